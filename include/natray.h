@@ -1,0 +1,349 @@
+/*
+ * natray.h - C ABI of the B200 simulation step of natray (a water balloon shot by bullets).
+ *
+ * This header is the drop-in boundary that replaces the wgpu dispatch layer of the reference
+ * (src/gpu.rs:60-214) and the `Sim` surface built on it (src/sim.rs:149-689). A Rust host
+ * binds it through a thin FFI crate; this repository binds it from Python through ctypes.
+ *
+ * Conventions
+ *   - Every call returns an ntr_status. Nothing aborts across the ABI; the message of the last
+ *     failure on the calling thread is available from ntr_last_error().
+ *   - Plain pointers and sizes only. Device pointers are lent by ntr_sim_buffer() and stay
+ *     valid until ntr_sim_destroy() or ntr_sim_restore().
+ *   - One ntr_sim per host thread at a time; each owns its own CUDA stream.
+ *
+ * World blob
+ *   A "world" is the complete description of a simulation: parameters, the static scene (mesh,
+ *   bullet surfaces) and all state that lives across steps. It is one contiguous byte blob: an
+ *   ntr_world_header followed by sections at the offsets the header lists. It is produced on the
+ *   CPU by ntr_world_build() (no GPU needed), consumed by ntr_sim_create_from_world(), and
+ *   written back by ntr_sim_snapshot(). The same format is the fixture format of the tests.
+ *   Block lists in a world are in canonical order: ascending block slot.
+ */
+#ifndef NATRAY_H
+#define NATRAY_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define NTR_API __declspec(dllexport)
+#else
+#define NTR_API __attribute__((visibility("default")))
+#endif
+
+/* Errors. The reference panics on these (src/sim.rs:635, src/gpu.rs:63-69, src/balloon.rs:225). */
+typedef enum ntr_status {
+    NTR_OK = 0,
+    NTR_E_INVALID = 1,     /* bad argument, bad parameter value, malformed world blob */
+    NTR_E_NOMEM = 2,       /* device or host allocation refused */
+    NTR_E_OVERFLOW = 3,    /* more grid blocks needed than the block capacity holds */
+    NTR_E_UNCONVERGED = 4, /* warning: a step ran out of solver iterations */
+    NTR_E_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+    NTR_E_CUDA = 6,        /* CUDA runtime error */
+    NTR_E_NODEVICE = 7,    /* no CUDA device, or the library was built without one */
+    NTR_E_BUSY = 8         /* admission refused for lack of free memory or slots */
+} ntr_status;
+
+#define NTR_MAX_SHOTS 4
+#define NTR_MAX_PATCHES 576
+#define NTR_N_SEC 32
+#define NTR_LOG_CAP 256
+#define NTR_OUTLINE 33
+#define NTR_HIT_FIELDS 13
+#define NTR_ACC_FIELDS 19
+#define NTR_CELL_FIELDS 11
+#define NTR_AIR_FIELDS 5
+#define NTR_LAYER_MODES 6
+
+/* One bullet fired at the balloon. Mirrors `Shot` (src/params.rs:205-264). `bullet` indexes
+ * the table of loads (src/params.rs:193-201): 0 .22 LR, 1 9 mm, 2 .45 ACP, 3 M855, 4 .308,
+ * 5 wadcutter, 6 BB. */
+typedef struct ntr_shot {
+    uint32_t bullet;
+    float speed;
+    float caliber_mm;
+    float mass_g;
+    float spin_rpm;
+    float range_m;
+    float muzzle_yaw_deg;
+    float azimuth_deg;
+    float elevation_deg;
+    float impact_offset_cm;
+    float impact_side_cm;
+    float delay_ms;
+} ntr_shot;
+
+/* Mirrors `SimParams` (src/params.rs:266-314), plus the knobs the reference hard-codes. */
+typedef struct ntr_sim_params {
+    uint32_t n_shots;
+    ntr_shot shots[NTR_MAX_SHOTS];
+    float balloon_diameter_cm;
+    float balloon_height;
+    float rubber_modulus_mpa;
+    float rubber_rest_diameter_cm;
+    float rubber_break_stretch;
+    float rubber_thickness_mm;
+    float gravity;
+    float spray_amount;
+    float mist_amount;
+    uint32_t resolution;
+    /* Hard-coded in the reference, exposed here. Defaults reproduce the reference. */
+    uint32_t mesh_level;  /* icosphere subdivisions (src/balloon.rs:357: 6) */
+    float dt_max;         /* longest step in s (src/sim.rs:19: 1e-3); 2e-6 gives a fixed step */
+    uint64_t seed;        /* 0: the reference jitter state 0x9E3779B97F4A7C15 (src/balloon.rs:359) */
+    uint32_t block_cap;   /* grid block capacity, 0 = sized from the particle count */
+    uint32_t spray_cap;   /* spray slots (src/sim.rs:13: 1,200,000) */
+    uint32_t max_iters;   /* solver iteration ceiling (src/sim.rs:21: 4096) */
+    float solve_tol;      /* relative residual (src/sim.rs:20: 1e-5) */
+} ntr_sim_params;
+
+/* The per-step uniform, field for field `Params` of src/sim.rs:49-64 / shaders/sim_defs.wgsl:8-21. */
+typedef struct ntr_gpu_params {
+    float origin[4];    /* domain corner, w = cell size h */
+    uint32_t dims[4];   /* domain size in cells, w = particle count */
+    uint32_t bdims[4];  /* domain size in 4^3 blocks, w = block capacity */
+    float gravity[4];   /* xyz, w = sound speed in water */
+    float fluid[4];     /* water density, CFL, longest step, particle spacing */
+    float wet[4];       /* x = wet map half size */
+    uint32_t limits[4]; /* wet map resolution, spray capacity, solver iterations, stop (ns) */
+    float solve[4];     /* x = relative tolerance */
+    uint32_t mem[4];    /* rubber verts, rubber substeps, air substeps, bullets */
+    float rubber[4];    /* Ogden moduli (Pa), uninflated thickness */
+    float rubber2[4];   /* ground friction, break stretch */
+    float knot[4];      /* where the neck is tied, w = neck radius */
+} ntr_gpu_params;
+
+/* The GPU clock and counters, word for word `State` of src/sim.rs:66-94 /
+ * shaders/sim_defs.wgsl:24-58. f32 fields that the device lowers with atomicMin are f32. */
+typedef struct ntr_state {
+    uint32_t t_ns;
+    uint32_t dt_ns;
+    uint32_t step;
+    uint32_t n_blocks;
+    float max_speed;
+    uint32_t n_blocks_prev;
+    uint32_t overflow;
+    uint32_t solve_iters;
+    float rz;
+    float alpha;
+    float b_norm;
+    float r_norm;
+    uint32_t free_dt_ns;
+    uint32_t iters_max;
+    uint32_t unconverged;
+    float beta;
+    uint32_t spray_count;
+    float mem_dt;
+    float cap_dt;
+    float mem_dt_seen;
+    float dt_flow;
+    float air_dt;
+    float air_dt_seen;
+    uint32_t mem_ticket;
+} ntr_state;
+
+/* Sections of a world blob. Element layouts (all little-endian, 4-byte words):
+ *   PARTICLES   n_particles x 20 f32: pos.xyzw, vel.xyz + alive (w), c0 (w = pressure Pa),
+ *               c1 (w = thin age s), c2 (w = scratch)           -- `Particle`, sim_defs.wgsl:61
+ *   MEM_X/V     n_verts x 4 f32 (v.w = 1 where a bullet holds it)
+ *   MEM_MASS    n_verts f32 (0 where the knot holds it)
+ *   MEM_WATER   n_verts x 4 f32 (water velocity, fill)
+ *   MEM_LAYER   n_verts x 6 x 4 f32 (Stokes-layer modes)
+ *   MEM_PUSH    n_verts x 2 f32 (push on the water N, area m^2)
+ *   TRIS        n_tris x (3 u32, rest_area f32, dm_inv 4 f32)    -- `GpuTri`, balloon.rs:23-29
+ *   ALIVE       n_tris u32
+ *   VTRI_OFF    (n_verts + 1) u32;  VTRI  n_vtri u32
+ *   BULLETS     4 x 28 words (`Bullet`, bullet.wgsl:16-34)
+ *   PATCHES     4 x 576 x 8 f32;  OUTLINES 4 x 33 x 2 f32;  SECTIONS 4 x 32 x 12 f32
+ *   BULLET_HIT  4 x 13 i32;  POSE_LOG 4 x 256 x 12 f32
+ *   BLOCKS_PREV n_blocks_prev u32 block slots, ascending
+ *   BLOCK_ACTIVE n_blocks_prev u32
+ *   AIR         5 fields x (64 n_blocks_prev) f32, field-major (rho, m.xyz, E)
+ *   SPRAY       n_spray x 12 f32 (pos + r, vel + weight, air);  LANDED n_spray x 4 f32
+ *   TOUCH       wet_res^2 u32 (f32 bits of the first wet time) */
+typedef enum ntr_section {
+    NTR_SEC_PARTICLES = 0,
+    NTR_SEC_MEM_X,
+    NTR_SEC_MEM_V,
+    NTR_SEC_MEM_MASS,
+    NTR_SEC_MEM_WATER,
+    NTR_SEC_MEM_LAYER,
+    NTR_SEC_MEM_PUSH,
+    NTR_SEC_TRIS,
+    NTR_SEC_ALIVE,
+    NTR_SEC_VTRI_OFF,
+    NTR_SEC_VTRI,
+    NTR_SEC_BULLETS,
+    NTR_SEC_PATCHES,
+    NTR_SEC_OUTLINES,
+    NTR_SEC_SECTIONS,
+    NTR_SEC_BULLET_HIT,
+    NTR_SEC_POSE_LOG,
+    NTR_SEC_BLOCKS_PREV,
+    NTR_SEC_BLOCK_ACTIVE,
+    NTR_SEC_AIR,
+    NTR_SEC_SPRAY,
+    NTR_SEC_LANDED,
+    NTR_SEC_TOUCH,
+    NTR_SEC_COUNT
+} ntr_section;
+
+#define NTR_WORLD_MAGIC 0x5752544Eu /* "NTRW" */
+#define NTR_WORLD_VERSION 1u
+
+typedef struct ntr_world_header {
+    uint32_t magic;
+    uint32_t version;
+    uint32_t n_particles;
+    uint32_t n_verts;
+    uint32_t n_tris;
+    uint32_t n_vtri;
+    uint32_t n_shots;
+    uint32_t n_blocks_prev;
+    uint32_t n_spray;
+    uint32_t wet_res;
+    uint32_t spray_cap;
+    uint32_t block_cap;
+    /* Host-side control that src/sim.rs:186-198 keeps between batches. */
+    uint32_t iters;
+    uint32_t substeps;
+    uint32_t air_substeps;
+    uint32_t unconverged;
+    uint32_t started;
+    uint32_t max_iters;
+    double t;
+    double t_start;
+    double t0;
+    double dx;
+    ntr_gpu_params params;
+    ntr_state state;
+    uint64_t offset[NTR_SEC_COUNT];
+    uint64_t bytes[NTR_SEC_COUNT];
+} ntr_world_header;
+
+/* Buffers a renderer or keyframe packer reads (src/sim.rs:149-205 pub fields). */
+typedef enum ntr_buf {
+    NTR_BUF_PARTICLES = 0, /* SoA: 5 arrays of n_particles float4 (pos, vel, c0, c1, c2) */
+    NTR_BUF_STATE,         /* one ntr_state */
+    NTR_BUF_MEM_POS,       /* n_verts float4 */
+    NTR_BUF_TRIS,
+    NTR_BUF_ALIVE,
+    NTR_BUF_VTRI_OFF,
+    NTR_BUF_VTRI,
+    NTR_BUF_SPRAY,         /* spray_cap x 48 B */
+    NTR_BUF_TOUCH,
+    NTR_BUF_LANDED,
+    NTR_BUF_BLOCK_LIST,    /* this step's block slots, ascending */
+    NTR_BUF_SORTED,        /* particle indices grouped by block, ascending within a block */
+    NTR_BUF_BLOCK_START,   /* n_blocks + 1 u32 */
+    NTR_BUF_ACC,           /* 19 fields x block_cap*64 i32, field-major */
+    NTR_BUF_CF,            /* 11 fields x block_cap*64 f32, field-major */
+    NTR_BUF_AIR,           /* 5 fields x block_cap*64 f32, field-major */
+    NTR_BUF_BLOCK_NB,      /* n_blocks x 27 u32 */
+    NTR_BUF_COUNT
+} ntr_buf;
+
+typedef struct ntr_sim_info {
+    uint32_t n_particles;
+    uint32_t n_verts;
+    uint32_t n_tris;
+    uint32_t n_shots;
+    uint32_t dims[3];
+    uint32_t block_cap;
+    uint32_t spray_cap;
+    uint32_t iters;
+    uint32_t substeps;
+    uint32_t air_substeps;
+    double dx;
+    double spacing;
+    float grid_origin[3];
+    float pad;
+    double t;
+    double t_start;
+    double t0;
+    uint64_t device_bytes;
+} ntr_sim_info;
+
+typedef struct ntr_sim ntr_sim;
+
+/* Message of the last failure on this thread (empty if none). Returns the message length. */
+NTR_API size_t ntr_last_error(char* buf, size_t cap);
+NTR_API const char* ntr_version(void);
+NTR_API void ntr_free(void* p);
+
+/* --- Parameters (CPU only) -------------------------------------------------------------- */
+/* SimParams::default (src/params.rs:297-314). */
+NTR_API ntr_status ntr_params_default(ntr_sim_params* p);
+/* A `key=value` override, `set_kv` of src/params.rs:361-423 (look keys are accepted and
+ * ignored: they only change the renderer). */
+NTR_API ntr_status ntr_params_set(ntr_sim_params* p, const char* key, const char* value);
+/* A named scene, `presets::named` of src/presets.rs:110-116. */
+NTR_API ntr_status ntr_params_preset(ntr_sim_params* p, const char* name);
+
+/* The filled balloon's axisymmetric shape, `Profile` of src/balloon.rs:73-110. */
+#define NTR_PROFILE_SAMPLES 402
+typedef struct ntr_profile {
+    uint32_t n_samples;
+    uint32_t pad;
+    double neck_angle;
+    double z_neck;
+    double neck_r;
+    double volume;
+    double z_centroid;
+    double stretch;
+    double r_max;
+    double samples[NTR_PROFILE_SAMPLES][3]; /* (angle on the uninflated sphere, r, z) */
+} ntr_profile;
+
+/* --- World construction (CPU only) ------------------------------------------------------- */
+/* `inflate` of src/balloon.rs:170-248: Ogden latex of the given small-strain shear modulus
+ * (Pa) and thickness (m), uninflated radius rest_radius (m), filled with `volume` (m^3) of
+ * water under rho*g = rho_g (Pa/m). */
+NTR_API ntr_status ntr_inflate(double shear_modulus, double thickness, double rest_radius, double volume, double rho_g,
+                               ntr_profile* out);
+/* Builds the scene and the initial state, as `Sim::new` does before its first dispatch
+ * (src/sim.rs:208-494, scene from src/balloon.rs:343-464 and src/bullet.rs:56-132), including
+ * the zero-length measuring substep of src/sim.rs:524-541. The blob is allocated here and
+ * released with ntr_free(). */
+NTR_API ntr_status ntr_world_build(const ntr_sim_params* p, void** blob, size_t* len);
+
+/* --- Simulation on one GPU ---------------------------------------------------------------- */
+/* Sim::new (src/sim.rs:208). */
+NTR_API ntr_status ntr_sim_create(const ntr_sim_params* p, int device, ntr_sim** out);
+/* A simulation from a world blob (a fixture, or a snapshot). */
+NTR_API ntr_status ntr_sim_create_from_world(const void* blob, size_t len, int device, ntr_sim** out);
+NTR_API ntr_status ntr_sim_destroy(ntr_sim* s);
+/* Sim::run (src/sim.rs:585-648): one batch of up to n steps that stops at stop_ns, one state
+ * read back, then the host's adaptation of solver iterations and substeps. */
+NTR_API ntr_status ntr_sim_step(ntr_sim* s, uint32_t n, uint32_t stop_ns, uint32_t* taken);
+/* Sim::advance (src/sim.rs:498-522). */
+NTR_API ntr_status ntr_sim_advance(ntr_sim* s, double t_target, uint32_t budget, uint32_t* taken);
+NTR_API ntr_status ntr_sim_read_state(ntr_sim* s, ntr_state* out);
+NTR_API ntr_status ntr_sim_info_get(ntr_sim* s, ntr_sim_info* out);
+/* Lends a device buffer. */
+NTR_API ntr_status ntr_sim_buffer(ntr_sim* s, ntr_buf which, void** dev_ptr, size_t* bytes);
+/* Copies a device buffer (or its first `bytes`) to host memory. */
+NTR_API ntr_status ntr_sim_download(ntr_sim* s, ntr_buf which, void* host, size_t bytes);
+/* The whole state as a world blob. With buf == NULL only *len is set. */
+NTR_API ntr_status ntr_sim_snapshot(ntr_sim* s, void* buf, size_t cap, size_t* len);
+/* Replaces the state with a world blob of the same scene sizes. */
+NTR_API ntr_status ntr_sim_restore(ntr_sim* s, const void* blob, size_t len);
+/* FP64 accumulation of the solver's inner products and residual (default on). */
+NTR_API ntr_status ntr_sim_set_precision(ntr_sim* s, int fp64_reductions);
+/* Kernel launches made by the last ntr_sim_step call, and its device time in ms. */
+NTR_API ntr_status ntr_sim_last_launches(ntr_sim* s, uint64_t* launches, double* device_ms);
+/* Conservation sums over live particles, accumulated in FP64 on the device:
+ * out[0] = live count, out[1..3] = momentum per particle mass, out[4] = kinetic energy per
+ * particle mass, out[5..7] = sum of positions. */
+NTR_API ntr_status ntr_sim_conservation(ntr_sim* s, double out[8]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NATRAY_H */

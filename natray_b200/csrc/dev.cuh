@@ -1,0 +1,406 @@
+// Device-side types and helpers of the B200 step: the device state, the pointer table every
+// kernel gets, vector arithmetic in the association the reference's WGSL writes it
+// (shaders/sim_defs.wgsl, common.wgsl), and the sparse-grid lookups.
+//
+// The sparse grid differs from the reference in how blocks are found. The reference keeps a
+// pointer per 4^3 block of the whole domain and hands out indices with atomicAdd
+// (fluid.wgsl:109-125). Here each step sets one bit per claimed block in a bitmask over the
+// domain; a scan of the bitmask's popcounts numbers the blocks in ascending slot order, and a
+// block's index is the prefix of its word plus the set bits below it in the word. That order
+// is canonical (deterministic), and nothing per slot has to be cleared between steps but the
+// bitmask itself (one bit per block).
+#pragma once
+
+#include <cstdint>
+
+#include "natray.h"
+
+namespace ntr {
+
+constexpr uint32_t NONE = 0xffffffffu;
+constexpr uint32_t TILE = 343;
+constexpr uint32_t FLT_MAX_BITS = 0x7f7fffffu;
+
+enum { A_WC = 6, A_PC = 7, A_N = 8, A_MF = 9, A_MA = 10, A_BU = 11, A_SRC = 14, A_MW = 15, A_MV = 16 };
+enum { F_U = 0, F_P = 3, F_R = 4, F_Z = 5, F_D = 6, F_Q = 8, F_DIAG = 9, F_TYPE = 10 };
+enum { F_EXT = 4, F_EXT_SET = 7 };
+
+#define GAS_T 0.0f
+#define WATER_T 1.0f
+#define SOLID_T 2.0f
+#define COVERED_T 3.0f
+#define RUBBER_T 4.0f
+
+// Fixed-point scales (sim_defs.wgsl:127-136, bullet.wgsl:76-80).
+#define FP_W 16777216.0f
+#define FP_M 65536.0f
+#define FP_P 65536.0f
+#define FP_F 4194304.0f
+#define FP_A 65536.0f
+#define FP_Q 16777216.0f
+#define FP_J 1073741824.0f
+#define FP_L 68719476736.0f
+#define FP_X 4096.0f
+
+#define RHO_AIR 1.2f
+#define MU_AIR 1.8e-5f
+#define SIGMA_W 0.072f
+#define PI_F 3.14159265358979f
+#define GAMMA_F 1.4f
+#define P_ATM 101325.0f
+#define P_VAPOUR 2339.0f
+#define RHO_ATM 1.204f
+#define RHO_VAPOUR 0.0278f
+#define CFL_AIR 0.9f
+#define CONTACT_F 0.05f
+#define MU_WATER 1.0e-3f
+#define MU_JACKET 0.8f
+#define LOGVINOVICH_K 2.0f
+#define R_HAND 1.5f
+#define CP_WAKE (-0.4f)
+#define CF_SKIN 0.003f
+#define EVAPORATION 1.3e-10f
+#define WE_CRIT 12.0f
+#define BIG_F 3.0e38f
+
+struct Tri {
+    uint32_t v0, v1, v2;
+    float rest_area;
+    float4 dm_inv;
+};
+static_assert(sizeof(Tri) == 32, "Tri");
+
+struct DBullet {
+    float4 x, v, q, l, shape, reach;
+    uint4 info;
+};
+static_assert(sizeof(DBullet) == 112, "Bullet");
+
+struct DSection {
+    float4 a, b, c;
+};
+
+// The device's copy of the step state. `s` is word for word the reference's State; the
+// solver scalars are also kept in double.
+struct DevState {
+    ntr_state s;
+    double rz, alpha, beta, b_norm, r_norm;
+    uint32_t solver_on;
+    uint32_t ticket[4];  // arrival counters of the last-block reductions
+    uint32_t nbrk;       // break-ups of this step
+    uint32_t err;        // bit 0: a bounded wait gave up
+    uint32_t pad[5];
+};
+
+// Every pointer and size a kernel may need. Passed by value.
+struct Dev {
+    const ntr_gpu_params* U;
+    DevState* st;
+    float4 *pos, *vel, *c0, *c1, *c2;
+    uint32_t Np, Nv, Nt, cap_blocks, cap_cells, nwords, spray_cap, wet_res;
+    uint32_t n_tiles, radix_passes, scan_ctas, fp64_dots;
+    uint32_t* mask[2];
+    uint32_t* prefix[2];
+    uint32_t* block_list[2];
+    uint32_t* cta_sum;
+    uint32_t *pslot, *key, *key_alt, *val_alt, *key_sorted, *sorted, *hist;
+    uint32_t *block_start, *block_nb, *block_active;
+    int32_t* acc;
+    float* cf;
+    float* air[2];
+    double *px, *py, *pz;
+    float4* mem_x[2];
+    float4* mem_v[2];
+    float4 *mem_water, *mem_layer;
+    float2* mem_push;
+    float* mem_mass;
+    const Tri* tris;
+    uint32_t *alive, *vtri_off, *vtri;
+    DBullet* bullets;
+    const float4* patches;
+    const float2* outlines;
+    DSection* sections;
+    int32_t* bullet_hit;
+    float4* pose_log;
+    float4* spray;  // 3 float4 per slot: pos + r, vel + weight, air
+    float4* landed;
+    uint32_t* touch;
+    float4 *brk_x, *brk_v;
+    uint32_t *brk_count, *brk_off;
+};
+
+// ---- vectors (association as written in the WGSL) ------------------------------------------
+struct V3 {
+    float x, y, z;
+    __device__ float& operator[](int i) { return i == 0 ? x : i == 1 ? y : z; }
+    __device__ float operator[](int i) const { return i == 0 ? x : i == 1 ? y : z; }
+};
+__device__ __forceinline__ V3 v3(float a, float b, float c) { return {a, b, c}; }
+__device__ __forceinline__ V3 xyz(float4 a) { return {a.x, a.y, a.z}; }
+__device__ __forceinline__ float4 f4(V3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
+__device__ __forceinline__ V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ V3 operator-(V3 a) { return {-a.x, -a.y, -a.z}; }
+__device__ __forceinline__ V3 operator*(V3 a, V3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+__device__ __forceinline__ V3 operator/(V3 a, V3 b) { return {a.x / b.x, a.y / b.y, a.z / b.z}; }
+__device__ __forceinline__ V3 operator*(V3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ V3 operator*(float s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ V3 operator/(V3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+__device__ __forceinline__ V3 operator+(V3 a, float s) { return {a.x + s, a.y + s, a.z + s}; }
+__device__ __forceinline__ V3 operator-(V3 a, float s) { return {a.x - s, a.y - s, a.z - s}; }
+__device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+__device__ __forceinline__ float length(V3 a) { return sqrtf(dot(a, a)); }
+__device__ __forceinline__ V3 normalize(V3 a) { return a * (1.0f / sqrtf(dot(a, a))); }
+__device__ __forceinline__ float distance(V3 a, V3 b) { return length(a - b); }
+__device__ __forceinline__ V3 vfloor(V3 a) { return {floorf(a.x), floorf(a.y), floorf(a.z)}; }
+// min / max with the operand order of the CPU restatement (`b < a ? b : a`).
+__device__ __forceinline__ float mn(float a, float b) { return b < a ? b : a; }
+__device__ __forceinline__ float mx(float a, float b) { return a < b ? b : a; }
+__device__ __forceinline__ float clampf_(float x, float lo, float hi) { return mn(mx(x, lo), hi); }
+
+struct I3 {
+    int32_t x, y, z;
+};
+__device__ __forceinline__ I3 operator+(I3 a, I3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ I3 operator-(I3 a, I3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ I3 operator*(I3 a, int32_t s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ I3 shr2(I3 a) { return {a.x >> 2, a.y >> 2, a.z >> 2}; }
+__device__ __forceinline__ I3 vi(V3 a) { return {__float2int_rz(a.x), __float2int_rz(a.y), __float2int_rz(a.z)}; }
+__device__ __forceinline__ V3 vf(I3 a) { return {(float)a.x, (float)a.y, (float)a.z}; }
+__device__ __forceinline__ uint32_t f2u(float x) { return __float2uint_rz(x); }
+
+// to_fp rounds half to even (sim_defs.wgsl:217-219).
+__device__ __forceinline__ int32_t to_fp(float x, float scale) { return __float2int_rn(clampf_(x * scale, -2e9f, 2e9f)); }
+__device__ __forceinline__ float from_fp(int32_t x, float scale) { return (float)x / scale; }
+
+__device__ __forceinline__ V3 axis_weights(float fx) {
+    return {0.5f * (1.5f - fx) * (1.5f - fx), 0.75f - (fx - 1.0f) * (fx - 1.0f), 0.5f * (fx - 0.5f) * (fx - 0.5f)};
+}
+
+// ---- float transcendentals ---------------------------------------------------------------------
+// exp, log, sin, cos, asin and pow of the step, written from the mathematics so that a CPU
+// evaluation of the same algorithms agrees with the device to the bit:
+//   exp       Cody-Waite reduction x = k ln2 + r, |r| <= ln2/2 (ln2 as a 16-bit head plus a
+//             tail), Taylor polynomial of e^r to r^7 in Horner form, times 2^k by exact
+//             power-of-two multiplications.
+//   log       x = m 2^e, m in [sqrt(1/2), sqrt(2)); ln m = 2 atanh s, s = (m - 1)/(m + 1), odd
+//             power series to s^11; ln x = e ln2_head + (ln m + e ln2_tail).
+//   sin, cos  x = k pi/2 + r (pi/2 in three parts), Taylor polynomials to r^9 and r^10, the
+//             quadrant from k mod 4.
+//   asin      Maclaurin series to x^27 on |x| <= 1/2, pi/2 - 2 asin(sqrt((1 - x)/2)) above.
+//   pow       exp(y ln x) for x > 0.
+// Built with -fmad=false, each line is the rounded IEEE operation written.
+__device__ __forceinline__ float nt_scale2(float p, int k) {
+    if (k > 127) {
+        p = p * 0x1p64f;
+        k -= 64;
+    }
+    if (k < -125) {
+        p = p * 0x1p-100f;
+        k += 100;
+    }
+    return p * __uint_as_float((uint32_t)(k + 127) << 23);
+}
+__device__ __forceinline__ float nt_exp(float x) {
+    if (x != x) return x;
+    if (x > 88.72284f) return __uint_as_float(0x7f800000u);
+    if (x < -103.972084f) return 0.0f;
+    float k = rintf(x * 1.442695f);
+    float r = (x - k * 0.693145751953125f) - k * 1.4286068e-06f;
+    float p = 0.0001984127f;
+    p = p * r + 0.0013888889f;
+    p = p * r + 0.008333334f;
+    p = p * r + 0.041666668f;
+    p = p * r + 0.16666667f;
+    p = p * r + 0.5f;
+    p = p * r + 1.0f;
+    p = p * r + 1.0f;
+    return nt_scale2(p, (int)k);
+}
+__device__ __forceinline__ float nt_log(float x) {
+    if (x != x) return x;
+    if (x < 0.0f) return __uint_as_float(0x7fc00000u);
+    if (x == 0.0f) return __uint_as_float(0xff800000u);
+    if (x == __uint_as_float(0x7f800000u)) return x;
+    int e = 0;
+    uint32_t u = __float_as_uint(x);
+    if ((u >> 23) == 0) {
+        x = x * 0x1p25f;
+        u = __float_as_uint(x);
+        e = -25;
+    }
+    e += (int)((u >> 23) & 0xffu) - 126;
+    float m = __uint_as_float((u & 0x007fffffu) | 0x3f000000u);
+    if (m < 0.70710677f) {
+        m = m * 2.0f;
+        e -= 1;
+    }
+    float s = (m - 1.0f) / (m + 1.0f);
+    float z = s * s;
+    float p = 0.09090909f;
+    p = p * z + 0.11111111f;
+    p = p * z + 0.14285715f;
+    p = p * z + 0.2f;
+    p = p * z + 0.33333334f;
+    p = p * z + 1.0f;
+    float lm = 2.0f * s * p;
+    float fe = (float)e;
+    return fe * 0.693145751953125f + (lm + fe * 1.4286068e-06f);
+}
+__device__ __forceinline__ void nt_sincos(float x, float* so, float* co) {
+    float k = rintf(x * 0.63661975f);
+    float r = ((x - k * 1.5703125f) - k * 0.0004838268f) - k * 2.563283e-12f;
+    float z = r * r;
+    float ps = 2.7557319e-06f;
+    ps = ps * z - 0.0001984127f;
+    ps = ps * z + 0.008333334f;
+    ps = ps * z - 0.16666667f;
+    float sr = r + r * z * ps;
+    float pc = -2.755732e-07f;
+    pc = pc * z + 2.4801588e-05f;
+    pc = pc * z - 0.0013888889f;
+    pc = pc * z + 0.041666668f;
+    pc = pc * z - 0.5f;
+    float cr = 1.0f + z * pc;
+    int q = ((int)k) & 3;
+    *so = q == 0 ? sr : q == 1 ? cr : q == 2 ? -sr : -cr;
+    *co = q == 0 ? cr : q == 1 ? -sr : q == 2 ? -cr : sr;
+}
+__device__ __forceinline__ float nt_sin(float x) {
+    float s, c;
+    nt_sincos(x, &s, &c);
+    return s;
+}
+__device__ __forceinline__ float nt_cos(float x) {
+    float s, c;
+    nt_sincos(x, &s, &c);
+    return c;
+}
+__device__ __forceinline__ float nt_asin_series(float t) {
+    float z = t * t;
+    float p = 0.0057400377f;
+    p = p * z + 0.0064472104f;
+    p = p * z + 0.007312526f;
+    p = p * z + 0.008390335f;
+    p = p * z + 0.009761609f;
+    p = p * z + 0.011551801f;
+    p = p * z + 0.013964844f;
+    p = p * z + 0.017352764f;
+    p = p * z + 0.022372158f;
+    p = p * z + 0.030381944f;
+    p = p * z + 0.04464286f;
+    p = p * z + 0.075f;
+    p = p * z + 0.16666667f;
+    return t + t * z * p;
+}
+__device__ __forceinline__ float nt_asin(float x) {
+    float a = fabsf(x);
+    if (!(a <= 1.0f)) return __uint_as_float(0x7fc00000u);
+    float r = a <= 0.5f ? nt_asin_series(a) : 1.5707964f - 2.0f * nt_asin_series(sqrtf((1.0f - a) * 0.5f));
+    return x < 0.0f ? -r : r;
+}
+__device__ __forceinline__ float nt_pow(float x, float y) {
+    if (x > 0.0f) return nt_exp(y * nt_log(x));
+    if (x == 0.0f) return y > 0.0f ? 0.0f : (y == 0.0f ? 1.0f : __uint_as_float(0x7f800000u));
+    return __uint_as_float(0x7fc00000u);
+}
+
+__device__ __forceinline__ uint32_t pcg(uint32_t v) {
+    uint32_t s = v * 747796405u + 2891336453u;
+    uint32_t w = ((s >> ((s >> 28u) + 4u)) ^ s) * 277803737u;
+    return (w >> 22u) ^ w;
+}
+__device__ __forceinline__ uint32_t hash3(uint32_t a, uint32_t b, uint32_t c) { return pcg(a ^ pcg(b ^ pcg(c))); }
+__device__ __forceinline__ float rnd(uint32_t& seed) {
+    seed = pcg(seed);
+    return (float)(seed >> 8u) * (1.0f / 16777216.0f);
+}
+__device__ __forceinline__ float rnd_gauss(uint32_t& seed) {
+    float u1 = mx(rnd(seed), 1e-7f);
+    float u2 = rnd(seed);
+    return sqrtf(-2.0f * nt_log(u1)) * nt_cos(2.0f * PI_F * u2);
+}
+
+// ---- the grid ------------------------------------------------------------------------------
+struct Grid {
+    float h;
+    V3 org;
+    uint32_t dims[3], bd[3];
+    uint32_t cap_blocks, cap_cells;
+    const uint32_t* mask;
+    const uint32_t* prefix;
+    const uint32_t* list;
+    const uint32_t* nb;
+};
+
+__device__ __forceinline__ Grid grid_of(const Dev& D, int cur) {
+    Grid g;
+    const ntr_gpu_params* U = D.U;
+    g.h = U->origin[3];
+    g.org = {U->origin[0], U->origin[1], U->origin[2]};
+    g.dims[0] = U->dims[0], g.dims[1] = U->dims[1], g.dims[2] = U->dims[2];
+    g.bd[0] = U->bdims[0], g.bd[1] = U->bdims[1], g.bd[2] = U->bdims[2];
+    g.cap_blocks = D.cap_blocks;
+    g.cap_cells = D.cap_cells;
+    g.mask = D.mask[cur];
+    g.prefix = D.prefix[cur];
+    g.list = D.block_list[cur];
+    g.nb = D.block_nb;
+    return g;
+}
+
+__device__ __forceinline__ uint32_t block_slot(const Grid& g, I3 b) {
+    return ((uint32_t)b.x * g.bd[1] + (uint32_t)b.y) * g.bd[2] + (uint32_t)b.z;
+}
+__device__ __forceinline__ I3 slot_coord(const Grid& g, uint32_t s) {
+    return {(int32_t)(s / (g.bd[2] * g.bd[1])), (int32_t)((s / g.bd[2]) % g.bd[1]), (int32_t)(s % g.bd[2])};
+}
+__device__ __forceinline__ bool in_bd(const Grid& g, I3 b) {
+    return b.x >= 0 && b.y >= 0 && b.z >= 0 && (uint32_t)b.x < g.bd[0] && (uint32_t)b.y < g.bd[1] && (uint32_t)b.z < g.bd[2];
+}
+// Index of the block at `slot` among this step's blocks, or NONE.
+__device__ __forceinline__ uint32_t lookup(const uint32_t* mask, const uint32_t* prefix, uint32_t slot, uint32_t cap) {
+    uint32_t m = __ldg(mask + (slot >> 5));
+    uint32_t bit = slot & 31u;
+    if (!((m >> bit) & 1u)) return NONE;
+    uint32_t idx = __ldg(prefix + (slot >> 5)) + __popc(m & ((1u << bit) - 1u));
+    return idx < cap ? idx : NONE;
+}
+__device__ __forceinline__ uint32_t block_at(const Grid& g, I3 b) {
+    if (!in_bd(g, b)) return NONE;
+    return lookup(g.mask, g.prefix, block_slot(g, b), g.cap_blocks);
+}
+__device__ __forceinline__ I3 local_coord(uint32_t i) {
+    uint32_t l = i % 64u;
+    return {(int32_t)(l / 16u), (int32_t)((l / 4u) % 4u), (int32_t)(l % 4u)};
+}
+__device__ __forceinline__ I3 cell_coord(const Grid& g, uint32_t i) { return slot_coord(g, g.list[i / 64u]) * 4 + local_coord(i); }
+__device__ __forceinline__ uint32_t neighbour(const Grid& g, uint32_t cell, I3 off) {
+    I3 q = local_coord(cell) + off;
+    I3 n = {(q.x >= 4) - (q.x < 0), (q.y >= 4) - (q.y < 0), (q.z >= 4) - (q.z < 0)};
+    uint32_t b = g.nb[(cell / 64u) * 27u + (uint32_t)((n.x + 1) * 9 + (n.y + 1) * 3 + n.z + 1)];
+    if (b == NONE) return NONE;
+    I3 l = q - n * 4;
+    return b * 64u + (uint32_t)l.x * 16u + (uint32_t)l.y * 4u + (uint32_t)l.z;
+}
+__device__ __forceinline__ uint32_t cell_at(const Grid& g, I3 c) {
+    if (c.x < 0 || c.y < 0 || c.z < 0 || (uint32_t)c.x >= g.dims[0] || (uint32_t)c.y >= g.dims[1] || (uint32_t)c.z >= g.dims[2]) return NONE;
+    uint32_t b = lookup(g.mask, g.prefix, block_slot(g, shr2(c)), g.cap_blocks);
+    if (b == NONE) return NONE;
+    return b * 64u + (uint32_t)(c.x & 3) * 16u + (uint32_t)(c.y & 3) * 4u + (uint32_t)(c.z & 3);
+}
+__device__ __forceinline__ I3 own_cell(const Grid& g, V3 p) { return vi(vfloor((p - g.org) / g.h)); }
+__device__ __forceinline__ V3 lattice_offset(uint32_t d) {
+    V3 o = {0.5f, 0.5f, 0.5f};
+    if (d == 0) o.x = 0.0f;
+    if (d == 1) o.y = 0.0f;
+    if (d == 2) o.z = 0.0f;
+    return o;
+}
+__device__ __forceinline__ uint32_t a_mom(uint32_t d) { return 2 * d; }
+__device__ __forceinline__ uint32_t a_wt(uint32_t d) { return 2 * d + 1; }
+
+__device__ __forceinline__ int cur_of(const DevState* st) { return (int)(st->s.step & 1u); }
+
+}  // namespace ntr

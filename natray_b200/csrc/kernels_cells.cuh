@@ -1,0 +1,711 @@
+// Per-cell and per-vertex kernels of the step: air carry/fill/substep (shaders/air.wgsl),
+// rubber splat/sample/substep (shaders/membrane.wgsl, bullet.wgsl:426-611), grid prep,
+// projection and velocity extension (shaders/fluid.wgsl:305-674), and the PCG solve
+// (fluid.wgsl:381-578).
+//
+// Cell kernels run a grid-stride loop over this step's cells (64 per block, field-major
+// storage, so a warp touches 128 contiguous bytes of a field). Kernels that need a block's 64
+// cells together (the block-local preconditioner and the per-block partial sums) run 4 blocks
+// per 256-thread CTA.
+#pragma once
+
+#include "dev.cuh"
+
+namespace ntr {
+
+#define CELL_LOOP(D, st)                                                                  \
+    const uint32_t n_cells_ = min((st)->s.n_blocks, (D).cap_blocks) * 64u;                \
+    for (uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x; cell < n_cells_; cell += gridDim.x * blockDim.x)
+
+__device__ __forceinline__ float* cfp(const Dev& D, uint32_t f, uint32_t cell) { return D.cf + (size_t)f * D.cap_cells + cell; }
+__device__ __forceinline__ float cfv(const Dev& D, uint32_t f, uint32_t cell) { return D.cf[(size_t)f * D.cap_cells + cell]; }
+__device__ __forceinline__ int32_t accv(const Dev& D, uint32_t f, uint32_t cell) { return D.acc[(size_t)f * D.cap_cells + cell]; }
+__device__ __forceinline__ int32_t* accp(const Dev& D, uint32_t f, uint32_t cell) { return D.acc + (size_t)f * D.cap_cells + cell; }
+__device__ __forceinline__ float cell_type(const Dev& D, uint32_t cell) { return cell == NONE ? GAS_T : cfv(D, F_TYPE, cell); }
+__device__ __forceinline__ float dt_of(const DevState* st) { return (float)st->s.dt_ns * 1e-9f; }
+__device__ __forceinline__ float now_of(const DevState* st) { return (float)st->s.t_ns * 1e-9f; }
+
+// ---- gas, air.wgsl:34-83, 150-235 ----------------------------------------------------------------
+struct Gas {
+    float rho;
+    V3 m;
+    float e;
+};
+__device__ __forceinline__ Gas read_gas(const Dev& D, int buf, uint32_t cell) {
+    const float* a = D.air[buf];
+    size_t cc = D.cap_cells;
+    return {a[cell], {a[cc + cell], a[2 * cc + cell], a[3 * cc + cell]}, a[4 * cc + cell]};
+}
+__device__ __forceinline__ void write_gas(const Dev& D, int buf, uint32_t cell, const Gas& g) {
+    float* a = D.air[buf];
+    size_t cc = D.cap_cells;
+    a[cell] = g.rho, a[cc + cell] = g.m.x, a[2 * cc + cell] = g.m.y, a[3 * cc + cell] = g.m.z, a[4 * cc + cell] = g.e;
+}
+__device__ __forceinline__ Gas gas_at_rest(float rho, float p) { return {rho, {0.0f, 0.0f, 0.0f}, p / (GAMMA_F - 1.0f)}; }
+__device__ __forceinline__ Gas ambient() { return gas_at_rest(RHO_ATM, P_ATM); }
+__device__ __forceinline__ Gas no_gas() { return {0.0f, {0.0f, 0.0f, 0.0f}, 0.0f}; }
+__device__ __forceinline__ float gas_p(const Gas& g) { return (GAMMA_F - 1.0f) * (g.e - 0.5f * dot(g.m, g.m) / g.rho); }
+__device__ __forceinline__ Gas floored(Gas o) {
+    o.rho = mx(o.rho, RHO_VAPOUR);
+    o.e = mx(o.e, P_VAPOUR / (GAMMA_F - 1.0f) + 0.5f * dot(o.m, o.m) / o.rho);
+    return o;
+}
+__device__ __forceinline__ bool free_gas(const Dev& D, uint32_t cell) { return cell == NONE || cfv(D, F_TYPE, cell) == GAS_T; }
+
+__device__ __forceinline__ Gas hll(const Gas& l, const Gas& r, uint32_t d) {
+    float pl = gas_p(l), pr = gas_p(r);
+    float ul = l.m[d] / l.rho, ur = r.m[d] / r.rho;
+    float cl = sqrtf(GAMMA_F * pl / l.rho), cr = sqrtf(GAMMA_F * pr / r.rho);
+    float sl = mn(ul - cl, ur - cr), sr = mx(ul + cl, ur + cr);
+    V3 ml = l.m * ul;
+    ml[d] += pl;
+    V3 mr = r.m * ur;
+    mr[d] += pr;
+    Gas fl = {l.rho * ul, ml, (l.e + pl) * ul};
+    Gas fr = {r.rho * ur, mr, (r.e + pr) * ur};
+    if (sl >= 0.0f) return fl;
+    if (sr <= 0.0f) return fr;
+    float k = 1.0f / (sr - sl);
+    float a = sr * k, b = -sl * k, c = sl * sr * k;
+    return {a * fl.rho + b * fr.rho + c * (r.rho - l.rho), a * fl.m + b * fr.m + c * (r.m - l.m), a * fl.e + b * fr.e + c * (r.e - l.e)};
+}
+
+__device__ __forceinline__ Gas across(const Dev& D, const Grid& g, int buf, uint32_t cell, const Gas& own, uint32_t d, bool hi) {
+    I3 e = {0, 0, 0};
+    int s = hi ? 1 : -1;
+    if (d == 0) e.x = s;
+    if (d == 1) e.y = s;
+    if (d == 2) e.z = s;
+    uint32_t nb = neighbour(g, cell, e);
+    if (nb == NONE) return ambient();
+    if (free_gas(D, nb)) return read_gas(D, buf, nb);
+    float w = cfv(D, F_U + d, hi ? nb : cell);
+    if (cfv(D, F_TYPE, nb) == RUBBER_T) w = from_fp(accv(D, A_MV + d, nb), FP_A) / from_fp(accv(D, A_MW, nb), FP_A);
+    Gas gg = own;
+    float u = own.m[d] / own.rho;
+    gg.m[d] = own.rho * (2.0f * w - u);
+    gg.e = own.e + 0.5f * (gg.m[d] * gg.m[d] - own.m[d] * own.m[d]) / own.rho;
+    return gg;
+}
+
+__device__ float gas_pressure_at(const Dev& D, const Grid& g, int buf, V3 x) {
+    I3 base = vi(vfloor((x - g.org) / g.h - 1.0f));
+    V3 fx = (x - g.org) / g.h - 0.5f - vf(base);
+    V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
+    float sx = 0.0f, sy = 0.0f;
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++)
+            for (int c = 0; c < 3; c++) {
+                uint32_t cell = cell_at(g, base + I3{a, b, c});
+                float w = wx[a] * wy[b] * wz[c];
+                if (cell == NONE) {
+                    sx = sx + w * P_ATM;
+                    sy = sy + w;
+                } else if (free_gas(D, cell)) {
+                    sx = sx + w * gas_p(read_gas(D, buf, cell));
+                    sy = sy + w;
+                }
+            }
+    return sy > 1e-6f ? sx / sy : P_ATM;
+}
+
+// ---- air_carry, air.wgsl:85-99 --------------------------------------------------------------------
+__global__ void k_air_carry(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const int cur = cur_of(st);
+    const uint32_t* list = D.block_list[cur];
+    CELL_LOOP(D, st) {
+        uint32_t b = cell >> 6, li = cell & 63u;
+        uint32_t o = lookup(D.mask[cur ^ 1], D.prefix[cur ^ 1], list[b], D.cap_blocks);
+        Gas g = ambient();
+        if (o != NONE && o < st->s.n_blocks_prev) g = read_gas(D, 0, o * 64u + li);
+        write_gas(D, 1, cell, g);
+        if (li == 0) D.block_active[b] = 0u;
+    }
+}
+
+// ---- mem_splat, membrane.wgsl:182-217 -------------------------------------------------------------
+__global__ void k_mem_splat(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const Grid g = grid_of(D, cur_of(st));
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.Nv || D.mem_mass[i] == 0.0f) return;
+    float2 pa = D.mem_push[i];
+    if (pa.y <= 0.0f) return;
+    float4 x4 = D.mem_x[0][i];
+    uint32_t own = cell_at(g, own_cell(g, xyz(x4)));
+    if (own != NONE) {
+        float a = pa.y * 1e6f;
+        atomicAdd(accp(D, A_MW, own), to_fp(a, FP_A));
+        float4 mv = D.mem_v[0][i];
+        atomicAdd(accp(D, A_MV + 0, own), to_fp(a * mv.x, FP_A));
+        atomicAdd(accp(D, A_MV + 1, own), to_fp(a * mv.y, FP_A));
+        atomicAdd(accp(D, A_MV + 2, own), to_fp(a * mv.z, FP_A));
+    }
+    bool on_water = D.mem_water[i].w >= CONTACT_F;
+    if (!on_water) return;
+    V3 x = (xyz(x4) - g.org) / g.h - 0.5f;
+    I3 base = vi(vfloor(x - 0.5f));
+    V3 fx = x - vf(base);
+    V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++)
+            for (int c = 0; c < 3; c++) {
+                uint32_t cell = cell_at(g, base + I3{a, b, c});
+                if (cell == NONE) continue;
+                float w = wx[a] * wy[b] * wz[c];
+                atomicAdd(accp(D, A_MF, cell), to_fp(w * pa.x, FP_F));
+                atomicAdd(accp(D, A_MA, cell), to_fp(w * pa.y * 1e6f, FP_A));
+            }
+}
+
+// ---- grid_prep, fluid.wgsl:305-356 -----------------------------------------------------------------
+__global__ void k_grid_prep(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const Grid g = grid_of(D, cur_of(st));
+    const ntr_gpu_params* U = D.U;
+    const float hh = g.h;
+    const V3 knot = {U->knot[0], U->knot[1], U->knot[2]};
+    const float kr = U->knot[3] + 0.5f * hh;
+    const float dt = dt_of(st);
+    const float grav[3] = {U->gravity[0], U->gravity[1], U->gravity[2]};
+    CELL_LOOP(D, st) {
+        float ty = GAS_T;
+        I3 c = cell_coord(g, cell);
+        bool ground = g.org.y + ((float)c.y + 0.5f) * hh < 0.0f;
+        V3 p = g.org + (vf(c) + 0.5f) * hh - knot;
+        bool knot_c = p.y > 0.0f && p.y < 2.0f * kr && sqrtf(p.x * p.x + p.z * p.z) < kr;
+        if (ground || knot_c)
+            ty = SOLID_T;
+        else if (accv(D, A_N, cell) > 0)
+            ty = WATER_T;
+#pragma unroll
+        for (uint32_t d = 0; d < 3; d++) {
+            float w = from_fp(accv(D, a_wt(d), cell), FP_W);
+            float u = 0.0f;
+            if (w > 1e-6f) u = from_fp(accv(D, a_mom(d), cell), FP_M) / w + dt * grav[d];
+            *cfp(D, F_U + d, cell) = u;
+        }
+        float wc = from_fp(accv(D, A_WC, cell), FP_W);
+        float ma = from_fp(accv(D, A_MA, cell), FP_A);
+        if (ty == GAS_T && accv(D, A_MW, cell) > 0) ty = RUBBER_T;
+        float pr = 0.0f;
+        if (ty == WATER_T && wc > 1e-6f) {
+            pr = from_fp(accv(D, A_PC, cell), FP_P) / wc * 1e6f;
+        } else if (ty != WATER_T && ty != SOLID_T && ma > 0.0f) {
+            ty = COVERED_T;
+            pr = from_fp(accv(D, A_MF, cell), FP_F) / ma * 1e6f;
+        }
+        *cfp(D, F_TYPE, cell) = ty;
+        *cfp(D, F_P, cell) = pr;
+    }
+}
+
+__constant__ int8_t E6[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+__device__ __forceinline__ I3 e6(int k) { return {E6[k][0], E6[k][1], E6[k][2]}; }
+__device__ __forceinline__ I3 ed(uint32_t d, int s) { return {d == 0 ? s : 0, d == 1 ? s : 0, d == 2 ? s : 0}; }
+
+// ---- air_fill (reads the second air buffer, writes the first), air.wgsl:101-148 ---------------
+__global__ void k_air_fill(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const Grid g = grid_of(D, cur_of(st));
+    CELL_LOOP(D, st) {
+        float ty = cfv(D, F_TYPE, cell);
+        if (ty == WATER_T || ty == SOLID_T) {
+            write_gas(D, 0, cell, no_gas());
+            continue;
+        }
+        Gas gg = read_gas(D, 1, cell);
+        if (gg.rho <= 0.0f) {
+            Gas sum = no_gas();
+            float cnt = 0.0f;
+            for (int k = 0; k < 6; k++) {
+                uint32_t nb = neighbour(g, cell, e6(k));
+                if (nb == NONE) continue;
+                Gas q = read_gas(D, 1, nb);
+                if (q.rho > 0.0f) {
+                    sum = {sum.rho + q.rho, sum.m + q.m, sum.e + q.e};
+                    cnt += 1.0f;
+                }
+            }
+            if (cnt > 0.0f)
+                gg = {sum.rho / cnt, sum.m / cnt, sum.e / cnt};
+            else
+                gg = gas_at_rest(RHO_VAPOUR, P_VAPOUR);
+        }
+        write_gas(D, 0, cell, gg);
+        if (ty == GAS_T) *cfp(D, F_P, cell) = gas_p(gg) - P_ATM;
+        if (ty == RUBBER_T) {
+            float p = BIG_F;
+            for (int k = 0; k < 6; k++) {
+                uint32_t nb = neighbour(g, cell, e6(k));
+                if (nb == NONE || !free_gas(D, nb)) continue;
+                Gas q = read_gas(D, 1, nb);
+                if (q.rho > 0.0f) p = mn(p, gas_p(q));
+            }
+            *cfp(D, F_P, cell) = (p < BIG_F ? p : gas_p(gg)) - P_ATM;
+        }
+    }
+}
+
+// ---- bullet_apply, bullet.wgsl:385-393 ---------------------------------------------------------------
+__global__ void k_bullet_apply(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    CELL_LOOP(D, st) {
+#pragma unroll
+        for (uint32_t d = 0; d < 3; d++) {
+            int32_t du = accv(D, A_BU + d, cell);
+            if (du != 0) *cfp(D, F_U + d, cell) = cfv(D, F_U + d, cell) + from_fp(du, FP_M);
+        }
+    }
+}
+
+// ---- the pressure solve -----------------------------------------------------------------------------
+__device__ __forceinline__ float bounded(float u, float hi, float lo) {
+    if (lo == SOLID_T && hi == SOLID_T) return 0.0f;
+    if (lo == SOLID_T) return mx(u, 0.0f);
+    if (hi == SOLID_T) return mn(u, 0.0f);
+    return u;
+}
+__device__ __forceinline__ float face_u(const Dev& D, uint32_t cell, uint32_t lo, uint32_t d) {
+    if (cell == NONE) return 0.0f;
+    return bounded(cfv(D, F_U + d, cell), cfv(D, F_TYPE, cell), cell_type(D, lo));
+}
+__device__ __forceinline__ float pressure_of(const Dev& D, uint32_t cell) {
+    if (cell == NONE) return 0.0f;
+    float p = cfv(D, F_P, cell);
+    return cfv(D, F_TYPE, cell) == WATER_T ? mx(p, P_VAPOUR - P_ATM) : p;
+}
+
+constexpr int SOLVE_T = 256;  // 4 blocks of 64 cells per CTA
+
+// Symmetric red-black Gauss-Seidel, two sweeps inside the block (fluid.wgsl:390-410). All
+// threads of the CTA call it.
+__device__ __forceinline__ float precondition(float (*zl)[64], uint8_t (*wl)[64], int j, int li, float r, float diag, bool water) {
+    zl[j][li] = 0.0f;
+    wl[j][li] = water ? 1 : 0;
+    __syncthreads();
+    const int lx = li / 16, ly = (li / 4) % 4, lz = li % 4;
+    const uint32_t colour = (uint32_t)(lx + ly + lz) % 2u;
+    for (uint32_t k = 0; k < 5; k++) {
+        if (water && colour == k % 2u) {
+            float s = r;
+            if (lx > 0 && wl[j][li - 16]) s += zl[j][li - 16];
+            if (lx < 3 && wl[j][li + 16]) s += zl[j][li + 16];
+            if (ly > 0 && wl[j][li - 4]) s += zl[j][li - 4];
+            if (ly < 3 && wl[j][li + 4]) s += zl[j][li + 4];
+            if (lz > 0 && wl[j][li - 1]) s += zl[j][li - 1];
+            if (lz < 3 && wl[j][li + 1]) s += zl[j][li + 1];
+            zl[j][li] = s / diag;
+        }
+        __syncthreads();
+    }
+    return zl[j][li];
+}
+
+// The 64-wide tree of block_sum (fluid.wgsl:414-422): red[li] += red[li + off], off = 32..1.
+// The last five levels run as shuffles, which pair the same elements.
+template <class A>
+__device__ __forceinline__ A tree64(A (*red)[64], int j, int li, A v) {
+    red[j][li] = v;
+    __syncthreads();
+    A out = A(0);
+    if (li < 32) {
+        A x = red[j][li] + red[j][li + 32];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, off);
+        out = x;
+    }
+    __syncthreads();
+    return out;  // valid in li == 0
+}
+
+// total(): 256 strided sums, then the 256-wide tree (fluid.wgsl:426-439). All 256 threads.
+template <class A>
+__device__ __forceinline__ A total256(const double* part, uint32_t n, A* red) {
+    A s = A(0);
+    for (uint32_t i = threadIdx.x; i < n; i += 256) s = s + (A)part[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = 128; off >= 32; off >>= 1) {
+        if ((int)threadIdx.x < off) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x < 32) {
+        A x = red[threadIdx.x];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, off);
+        if (threadIdx.x == 0) red[0] = x;
+    }
+    __syncthreads();
+    A r = red[0];
+    __syncthreads();
+    return r;
+}
+
+// Arrival at the end of a kernel whose per-block partials the last CTA sums. True in the last.
+__device__ __forceinline__ bool last_cta(DevState* st, int k) {
+    __shared__ uint32_t s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = atomicAdd(&st->ticket[k], 1u);
+        s_last = (t == gridDim.x - 1) ? 1u : 0u;
+    }
+    __syncthreads();
+    bool last = s_last != 0;
+    if (last) __threadfence();
+    return last;
+}
+
+__device__ __forceinline__ bool converged_fp64(const DevState* st, double rr, float tol) {
+    return sqrt(rr) <= (double)tol * fmax(st->b_norm, 1.0);
+}
+__device__ __forceinline__ bool converged_fp32(const DevState* st, float rr, float tol) {
+    return sqrtf(rr) <= tol * mx((float)st->b_norm, 1.0f);
+}
+
+template <bool FP64>
+__global__ void __launch_bounds__(SOLVE_T) k_solve_init(Dev D) {
+    using A = typename std::conditional<FP64, double, float>::type;
+    DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const Grid g = grid_of(D, cur_of(st));
+    const ntr_gpu_params* U = D.U;
+    const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
+    const int j = threadIdx.x >> 6, li = threadIdx.x & 63;
+    __shared__ float zl[4][64];
+    __shared__ uint8_t wl[4][64];
+    __shared__ A red[4][64];
+    const float hh = g.h, dt = dt_of(st);
+    const float rho = U->fluid[0];
+    for (uint32_t b0 = blockIdx.x * 4u; b0 < nb; b0 += gridDim.x * 4u) {
+        const uint32_t b = b0 + j;
+        const uint32_t cell = b * 64u + li;
+        const bool active = b < nb;
+        const bool water = active && cfv(D, F_TYPE, cell) == WATER_T;
+        float diag = 1.0f, r = 0.0f, bq = 0.0f;
+        if (water) {
+            float cs = U->gravity[3] * dt;
+            float kc = hh * hh / (cs * cs);
+            float div = 0.0f, off = 0.0f;
+            diag = kc;
+            bq = kc * cfv(D, F_P, cell);
+            for (uint32_t d = 0; d < 3; d++) {
+                div += face_u(D, neighbour(g, cell, ed(d, 1)), cell, d) - face_u(D, cell, neighbour(g, cell, ed(d, -1)), d);
+                for (int s = -1; s <= 1; s += 2) {
+                    uint32_t nbc = neighbour(g, cell, ed(d, s));
+                    float nt = cell_type(D, nbc);
+                    if (nt == SOLID_T) continue;
+                    diag += 1.0f;
+                    if (nt == WATER_T)
+                        off -= cfv(D, F_P, nbc);
+                    else
+                        bq += pressure_of(D, nbc);
+                }
+            }
+            div -= from_fp(accv(D, A_SRC, cell), FP_Q) / (hh * hh);
+            bq -= rho * hh / dt * div;
+            r = bq - diag * cfv(D, F_P, cell) - off;
+            *cfp(D, F_DIAG, cell) = diag;
+            *cfp(D, F_R, cell) = r;
+        }
+        float z = precondition(zl, wl, j, li, r, diag, water);
+        if (water) *cfp(D, F_Z, cell) = z;
+        A vx, vy, vz;
+        if (FP64) {
+            vx = (A)((double)r * (double)z), vy = (A)((double)r * (double)r), vz = (A)((double)bq * (double)bq);
+        } else {
+            vx = (A)(r * z), vy = (A)(r * r), vz = (A)(bq * bq);
+        }
+        A sx = tree64(red, j, li, vx);
+        A sy = tree64(red, j, li, vy);
+        A sz = tree64(red, j, li, vz);
+        if (li == 0 && active) D.px[b] = (double)sx, D.py[b] = (double)sy, D.pz[b] = (double)sz;
+    }
+    if (!last_cta(st, 0)) return;
+    __shared__ A tred[256];
+    A sx = total256<A>(D.px, nb, tred);
+    A sy = total256<A>(D.py, nb, tred);
+    A sz = total256<A>(D.pz, nb, tred);
+    if (threadIdx.x == 0) {
+        st->ticket[0] = 0;
+        const float tol = U->solve[0];
+        st->rz = (double)sx;
+        st->beta = 0.0;
+        bool conv;
+        if (FP64) {
+            st->b_norm = sqrt((double)sz);
+            st->r_norm = sqrt((double)sy);
+            conv = converged_fp64(st, (double)sy, tol);
+        } else {
+            st->b_norm = (double)sqrtf((float)sz);
+            st->r_norm = (double)sqrtf((float)sy);
+            conv = converged_fp32(st, (float)sy, tol);
+        }
+        st->s.solve_iters = 0;
+        st->solver_on = ((double)sx > 0.0 && !conv) ? 1u : 0u;
+        st->s.rz = (float)st->rz, st->s.beta = 0.0f, st->s.b_norm = (float)st->b_norm, st->s.r_norm = (float)st->r_norm;
+    }
+}
+
+template <bool FP64>
+__global__ void __launch_bounds__(SOLVE_T) k_solve_q(Dev D) {
+    using A = typename std::conditional<FP64, double, float>::type;
+    DevState* st = D.st;
+    if (st->s.dt_ns == 0 || st->solver_on == 0) return;
+    const Grid g = grid_of(D, cur_of(st));
+    const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
+    const int j = threadIdx.x >> 6, li = threadIdx.x & 63;
+    __shared__ A red[4][64];
+    const uint32_t old = st->s.solve_iters % 2u;
+    const float beta = (float)st->beta;
+    for (uint32_t b0 = blockIdx.x * 4u; b0 < nb; b0 += gridDim.x * 4u) {
+        const uint32_t b = b0 + j;
+        const uint32_t cell = b * 64u + li;
+        A v = A(0);
+        if (b < nb && cfv(D, F_TYPE, cell) == WATER_T) {
+            float dn = cfv(D, F_Z, cell) + beta * cfv(D, F_D + old, cell);
+            float q = cfv(D, F_DIAG, cell) * dn;
+            for (uint32_t d = 0; d < 3; d++)
+                for (int k = -1; k <= 1; k += 2) {
+                    uint32_t nbc = neighbour(g, cell, ed(d, k));
+                    if (cell_type(D, nbc) == WATER_T) q -= cfv(D, F_Z, nbc) + beta * cfv(D, F_D + old, nbc);
+                }
+            *cfp(D, F_D + 1 - old, cell) = dn;
+            *cfp(D, F_Q, cell) = q;
+            v = FP64 ? (A)((double)dn * (double)q) : (A)(dn * q);
+        }
+        A s = tree64(red, j, li, v);
+        if (li == 0 && b < nb) D.px[b] = (double)s;
+    }
+    if (!last_cta(st, 1)) return;
+    __shared__ A tred[256];
+    A s = total256<A>(D.px, nb, tred);
+    if (threadIdx.x == 0) {
+        st->ticket[1] = 0;
+        if (FP64)
+            st->alpha = (double)s > 0.0 ? st->rz / (double)s : 0.0;
+        else
+            st->alpha = (float)s > 0.0f ? (double)((float)st->rz / (float)s) : 0.0;
+        st->s.alpha = (float)st->alpha;
+    }
+}
+
+template <bool FP64>
+__global__ void __launch_bounds__(SOLVE_T) k_solve_update(Dev D) {
+    using A = typename std::conditional<FP64, double, float>::type;
+    DevState* st = D.st;
+    if (st->s.dt_ns == 0 || st->solver_on == 0) return;
+    const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
+    const int j = threadIdx.x >> 6, li = threadIdx.x & 63;
+    __shared__ float zl[4][64];
+    __shared__ uint8_t wl[4][64];
+    __shared__ A red[4][64];
+    const uint32_t old = st->s.solve_iters % 2u;
+    const float a = (float)st->alpha;
+    for (uint32_t b0 = blockIdx.x * 4u; b0 < nb; b0 += gridDim.x * 4u) {
+        const uint32_t b = b0 + j;
+        const uint32_t cell = b * 64u + li;
+        const bool water = b < nb && cfv(D, F_TYPE, cell) == WATER_T;
+        float diag = 1.0f, r = 0.0f;
+        if (water) {
+            *cfp(D, F_P, cell) = cfv(D, F_P, cell) + a * cfv(D, F_D + 1 - old, cell);
+            r = cfv(D, F_R, cell) - a * cfv(D, F_Q, cell);
+            *cfp(D, F_R, cell) = r;
+            diag = cfv(D, F_DIAG, cell);
+        }
+        float z = precondition(zl, wl, j, li, r, diag, water);
+        if (water) *cfp(D, F_Z, cell) = z;
+        A vx = FP64 ? (A)((double)r * (double)z) : (A)(r * z);
+        A vy = FP64 ? (A)((double)r * (double)r) : (A)(r * r);
+        A sx = tree64(red, j, li, vx);
+        A sy = tree64(red, j, li, vy);
+        if (li == 0 && b < nb) D.px[b] = (double)sx, D.py[b] = (double)sy;
+    }
+    if (!last_cta(st, 2)) return;
+    __shared__ A tred[256];
+    A sx = total256<A>(D.px, nb, tred);
+    A sy = total256<A>(D.py, nb, tred);
+    if (threadIdx.x == 0) {
+        st->ticket[2] = 0;
+        const float tol = D.U->solve[0];
+        st->s.solve_iters += 1;
+        bool done;
+        if (FP64) {
+            st->r_norm = sqrt((double)sy);
+            st->beta = st->rz > 0.0 ? (double)sx / st->rz : 0.0;
+            done = converged_fp64(st, (double)sy, tol);
+        } else {
+            st->r_norm = (double)sqrtf((float)sy);
+            st->beta = st->rz > 0.0 ? (double)((float)sx / (float)st->rz) : 0.0;
+            done = converged_fp32(st, (float)sy, tol);
+        }
+        st->rz = (double)sx;
+        if (done || st->s.solve_iters >= D.U->limits[2]) {
+            st->s.iters_max = max(st->s.iters_max, st->s.solve_iters);
+            st->s.unconverged += done ? 0u : 1u;
+            st->solver_on = 0u;
+        }
+        st->s.rz = (float)st->rz, st->s.beta = (float)st->beta, st->s.r_norm = (float)st->r_norm;
+    }
+}
+
+// ---- project, extend, fluid.wgsl:580-674 -------------------------------------------------------------
+__global__ void k_project(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const Grid g = grid_of(D, cur_of(st));
+    const float k = dt_of(st) / (D.U->fluid[0] * g.h);
+    CELL_LOOP(D, st) {
+        float ty = cfv(D, F_TYPE, cell);
+#pragma unroll
+        for (uint32_t d = 0; d < 3; d++) {
+            uint32_t nb = neighbour(g, cell, ed(d, -1));
+            float nt = cell_type(D, nb);
+            float u = bounded(cfv(D, F_U + d, cell), ty, nt);
+            if (ty != SOLID_T && nt != SOLID_T && (ty == WATER_T || nt == WATER_T)) u -= k * (pressure_of(D, cell) - pressure_of(D, nb));
+            *cfp(D, F_U + d, cell) = u;
+        }
+    }
+}
+
+__device__ __forceinline__ bool face_set(const Dev& D, const Grid& g, uint32_t cell, uint32_t d) {
+    if (cell == NONE) return false;
+    return cfv(D, F_TYPE, cell) == WATER_T || cell_type(D, neighbour(g, cell, ed(d, -1))) == WATER_T;
+}
+
+__global__ void k_extend_1(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const Grid g = grid_of(D, cur_of(st));
+    CELL_LOOP(D, st) {
+        uint32_t done = 0;
+        for (uint32_t d = 0; d < 3; d++) {
+            float u = cfv(D, F_U + d, cell);
+            if (face_set(D, g, cell, d)) {
+                done |= 1u << d;
+            } else {
+                float sum = 0.0f, cnt = 0.0f;
+                for (int k = 0; k < 6; k++) {
+                    uint32_t nb = neighbour(g, cell, e6(k));
+                    if (face_set(D, g, nb, d)) {
+                        sum += cfv(D, F_U + d, nb);
+                        cnt += 1.0f;
+                    }
+                }
+                if (cnt > 0.0f) {
+                    u = sum / cnt;
+                    done |= 1u << d;
+                }
+            }
+            *cfp(D, F_EXT + d, cell) = u;
+        }
+        *cfp(D, F_EXT_SET, cell) = (float)done;
+    }
+}
+
+__device__ __forceinline__ bool ext_set(const Dev& D, uint32_t cell, uint32_t d) {
+    return cell != NONE && ((f2u(cfv(D, F_EXT_SET, cell)) >> d) & 1u) != 0u;
+}
+
+__global__ void k_extend_2(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const Grid g = grid_of(D, cur_of(st));
+    CELL_LOOP(D, st) {
+        float ty = cfv(D, F_TYPE, cell);
+        for (uint32_t d = 0; d < 3; d++) {
+            float u = cfv(D, F_U + d, cell);
+            if (ext_set(D, cell, d)) {
+                u = cfv(D, F_EXT + d, cell);
+            } else {
+                float sum = 0.0f, cnt = 0.0f;
+                for (int k = 0; k < 6; k++) {
+                    uint32_t nb = neighbour(g, cell, e6(k));
+                    if (ext_set(D, nb, d)) {
+                        sum += cfv(D, F_EXT + d, nb);
+                        cnt += 1.0f;
+                    }
+                }
+                if (cnt > 0.0f) u = sum / cnt;
+            }
+            *cfp(D, F_U + d, cell) = bounded(u, ty, cell_type(D, neighbour(g, cell, ed(d, -1))));
+        }
+    }
+}
+
+// ---- sampling the grid at a point, membrane.wgsl:219-239, bullet.wgsl:113-158 ---------------------------
+__device__ __forceinline__ float2 sample_grid(const Dev& D, const Grid& g, V3 x, uint32_t fu, uint32_t fw) {
+    I3 base = vi(vfloor(x - 0.5f));
+    V3 fx = x - vf(base);
+    V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
+    float sx = 0.0f, sy = 0.0f;
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++)
+            for (int c = 0; c < 3; c++) {
+                uint32_t cell = cell_at(g, base + I3{a, b, c});
+                if (cell == NONE) continue;
+                float w = wx[a] * wy[b] * wz[c] * from_fp(accv(D, fw, cell), FP_W);
+                sx = sx + w * cfv(D, fu, cell);
+                sy = sy + w;
+            }
+    return make_float2(sx, sy);
+}
+
+__global__ void k_mem_sample(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const Grid g = grid_of(D, cur_of(st));
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.Nv || D.mem_mass[i] == 0.0f) return;
+    V3 x = (xyz(D.mem_x[0][i]) - g.org) / g.h;
+    V3 v = {0.0f, 0.0f, 0.0f};
+    for (uint32_t d = 0; d < 3; d++) {
+        float2 s = sample_grid(D, g, x - lattice_offset(d), F_U + d, a_wt(d));
+        v[d] = s.y > 1e-6f ? s.x / s.y : 0.0f;
+    }
+    float fill = sample_grid(D, g, x - 0.5f, F_TYPE, A_WC).y / 8.0f;
+    D.mem_water[i] = f4(v, fill);
+}
+
+// ---- air_substep, air.wgsl:237-269 --------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_air_substep(Dev D, int par) {
+    DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const Grid g = grid_of(D, cur_of(st));
+    const float hh = g.h;
+    const float k = dt_of(st) / (float)max(D.U->mem[2], 1u) / hh;
+    float lim = BIG_F;
+    CELL_LOOP(D, st) {
+        Gas gg = read_gas(D, par, cell);
+        if (!free_gas(D, cell)) {
+            write_gas(D, 1 - par, cell, gg);
+            continue;
+        }
+        Gas f = no_gas();
+        for (uint32_t d = 0; d < 3; d++) {
+            Gas lo = hll(across(D, g, par, cell, gg, d, false), gg, d);
+            Gas hi = hll(gg, across(D, g, par, cell, gg, d, true), d);
+            f = {f.rho + hi.rho - lo.rho, f.m + hi.m - lo.m, f.e + hi.e - lo.e};
+        }
+        Gas n = floored(Gas{gg.rho - k * f.rho, gg.m - k * f.m, gg.e - k * f.e});
+        write_gas(D, 1 - par, cell, n);
+        V3 u = n.m / n.rho;
+        float p = gas_p(n);
+        float c = sqrtf(GAMMA_F * p / n.rho);
+        float limit = CFL_AIR * hh / (fabsf(u.x) + fabsf(u.y) + fabsf(u.z) + 3.0f * c);
+        lim = mn(lim, limit);
+        if (fabsf(p - P_ATM) > 10.0f || length(u) > 0.05f) D.block_active[cell >> 6] = 1u;
+    }
+    for (int o = 16; o > 0; o >>= 1) lim = fminf(lim, __shfl_down_sync(0xffffffffu, lim, o));
+    // The reference lowers air_dt once per workgroup, so only when there are cells.
+    if ((threadIdx.x & 31) == 0 && n_cells_ > 0) atomicMin((unsigned int*)&st->s.air_dt, __float_as_uint(lim));
+}
+
+}  // namespace ntr

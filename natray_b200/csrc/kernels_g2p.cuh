@@ -1,0 +1,388 @@
+// Grid to particle and the spray (shaders/fluid.wgsl:676-901, bullet.wgsl:395-424).
+//
+// Break-ups get their spray slots in a canonical order: block by block, and in sorted order
+// within a block. g2p writes each block's break-ups, ranked in that order, into scratch at the
+// block's own range of sorted positions; a scan over the blocks' counts then gives every one
+// its slots, and k_spray_emit writes the drops. The reference hands slots out with atomicAdd
+// (fluid.wgsl:726), whose order is the hardware's.
+#pragma once
+
+#include "kernels_grid.cuh"
+#include "kernels_mem.cuh"
+
+namespace ntr {
+
+__device__ __forceinline__ float drag_cd(float re) {
+    if (re < 1e-4f) return 24.0f / 1e-4f;
+    return 24.0f / re * (1.0f + 0.15f * nt_pow(re, 0.687f)) + 0.42f / (1.0f + 42500.0f * nt_pow(re, -1.16f));
+}
+
+__global__ void k_spray_update(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const uint32_t n = min(st->s.spray_count, D.spray_cap);
+    const float step = dt_of(st), now = now_of(st);
+    const ntr_gpu_params* U = D.U;
+    const V3 grav = {U->gravity[0], U->gravity[1], U->gravity[2]};
+    const float rhow = U->fluid[0];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 pos = D.spray[3 * (size_t)i], vel = D.spray[3 * (size_t)i + 1];
+        float r = pos.w;
+        if (r <= 0.0f) continue;
+        float sp = length(xyz(vel));
+        float re = 2.0f * r * sp * RHO_AIR / MU_AIR;
+        float k = 3.0f * RHO_AIR * drag_cd(re) * sp / (8.0f * rhow * r);
+        V3 v = (xyz(vel) + step * grav) / (1.0f + k * step);
+        r = sqrtf(mx(r * r - EVAPORATION * step, 0.0f));
+        if (r < 2.5e-6f) r = 0.0f;
+        V3 p = xyz(pos) + step * v;
+        if (p.y <= r) {
+            D.landed[i] = make_float4(p.x, p.z, r * nt_pow(vel.w, 1.0f / 3.0f), now);
+            r = 0.0f;
+        }
+        D.spray[3 * (size_t)i] = f4(p, r);
+        D.spray[3 * (size_t)i + 1] = f4(v, vel.w);
+    }
+}
+
+__device__ __forceinline__ void ground_touch(const Dev& D, V3 p, float now) {
+    const float hw = D.U->wet[0];
+    const uint32_t res = D.U->limits[0];
+    float ux = (p.x + hw) / (2.0f * hw), uz = (p.z + hw) / (2.0f * hw);
+    if (ux < 0.0f || uz < 0.0f || ux >= 1.0f || uz >= 1.0f) return;
+    uint32_t cx = f2u(ux * (float)res), cz = f2u(uz * (float)res);
+    atomicMin(D.touch + (size_t)cz * res + cx, __float_as_uint(now));
+}
+
+__device__ void carve(const Dev& D, V3& x, V3& v, uint32_t id, float t, float hh, uint32_t step_no) {
+    const float hand2 = R_HAND * R_HAND * hh * hh;
+    for (uint32_t bi = 0; bi < D.U->mem[3]; bi++) {
+        float4 reach = D.bullets[bi].reach;
+        if (reach.w <= 0.0f || distance(x, xyz(reach)) > reach.w) continue;
+        for (uint32_t k = 0; k < NTR_N_SEC; k++) {
+            const DSection s = D.sections[bi * NTR_N_SEC + k];
+            float r2 = section_r2(s, t);
+            if (s.b.w <= 0.0f || r2 >= hand2) continue;
+            V3 ab = xyz(s.b) - xyz(s.a);
+            float f = dot(x - xyz(s.a), ab) / mx(dot(ab, ab), 1e-20f);
+            if (f < 0.0f || f > 1.0f) continue;
+            V3 on = xyz(s.a) + f * ab;
+            V3 d = x - on;
+            if (dot(d, d) >= r2) continue;
+            if (dot(d, d) < 1e-14f) {
+                uint32_t seed = hash3(id, step_no, k);
+                float g0 = rnd_gauss(seed);
+                float g1 = rnd_gauss(seed);
+                float g2 = rnd_gauss(seed);
+                d = cross(ab + 1e-9f, v3(g0, g1, g2));
+            }
+            V3 dir = normalize(d);
+            float r = sqrtf(r2);
+            x = on + dir * r;
+            float wall = s.b.w / (2.0f * r);
+            v = v + dir * mx(wall - dot(v, dir), 0.0f);
+        }
+    }
+}
+
+struct Gathered {
+    float s;
+    V3 g;
+    float w;
+};
+
+__device__ __forceinline__ Gathered gather(const float* tg, V3 X, V3 o, I3 corner, uint32_t fa, uint32_t fw, float hh) {
+    I3 base = vi(vfloor(X - o - 0.5f));
+    V3 fx = X - o - vf(base);
+    V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
+    I3 tq = base - corner;
+    uint32_t t0 = (uint32_t)tq.x * 49u + (uint32_t)tq.y * 7u + (uint32_t)tq.z;
+    Gathered r = {0.0f, {0.0f, 0.0f, 0.0f}, 0.0f};
+#pragma unroll
+    for (uint32_t a = 0; a < 3; a++)
+#pragma unroll
+        for (uint32_t b = 0; b < 3; b++)
+#pragma unroll
+            for (uint32_t c = 0; c < 3; c++) {
+                float weight = wx[a] * wy[b] * wz[c];
+                uint32_t t = t0 + a * 49u + b * 7u + c;
+                float u = weight * tg[fa * TILE + t];
+                r.s += u;
+                r.g = r.g + u * (v3((float)a, (float)b, (float)c) - fx);
+                r.w += weight * tg[fw * TILE + t];
+            }
+    r.g = r.g * hh;
+    return r;
+}
+
+constexpr int G2P_T = 256;
+
+__global__ void __launch_bounds__(G2P_T) k_g2p(Dev D) {
+    DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const Grid g = grid_of(D, cur_of(st));
+    const ntr_gpu_params* U = D.U;
+    const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
+    const float hh = g.h, step = dt_of(st), now = now_of(st);
+    const float spacing = U->fluid[3];
+    const V3 lo = g.org + 3.5f * hh;
+    const V3 hi = g.org + (v3((float)g.dims[0], (float)g.dims[1], (float)g.dims[2]) - 4.5f) * hh;
+    const float r_thin = 0.75f * spacing;
+    const float t_thin = 3.0f * sqrtf(U->fluid[0] * r_thin * r_thin * r_thin / SIGMA_W);
+    const float cs = 4.0f / (hh * hh);
+    const uint32_t step_no = st->s.step;
+    __shared__ float tg[8 * TILE];
+    __shared__ uint32_t links[27];
+    __shared__ uint32_t s_wcount[G2P_T / 32];
+    __shared__ uint32_t s_brk;
+    float fastest = 0.0f;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
+        const uint32_t first = D.block_start[b];
+        const uint32_t count = D.block_start[b + 1] - first;
+        if (count == 0) {
+            if (threadIdx.x == 0) D.brk_count[b] = 0;
+            continue;
+        }
+        if (threadIdx.x < 27) links[threadIdx.x] = D.block_nb[b * 27u + threadIdx.x];
+        if (threadIdx.x == 0) s_brk = 0;
+        __syncthreads();
+        for (uint32_t t = threadIdx.x; t < TILE; t += G2P_T) {
+            uint32_t cell = tile_cell(links, t);
+            bool water = cell != NONE && cfv(D, F_TYPE, cell) == WATER_T;
+#pragma unroll
+            for (uint32_t d = 0; d < 3; d++) {
+                float u = 0.0f, w = 0.0f;
+                if (cell != NONE) {
+                    u = cfv(D, F_U + d, cell);
+                    w = from_fp(accv(D, a_wt(d), cell), FP_W);
+                }
+                tg[a_mom(d) * TILE + t] = u;
+                tg[a_wt(d) * TILE + t] = w;
+            }
+            tg[A_PC * TILE + t] = water ? pressure_of(D, cell) : 0.0f;
+            tg[A_WC * TILE + t] = water ? 1.0f : 0.0f;
+        }
+        __syncthreads();
+        const I3 corner = slot_coord(g, g.list[b]) * 4 - I3{1, 1, 1};
+        // Rounds of 256 particles keep the sorted order for ranking the break-ups.
+        for (uint32_t base = 0; base < count; base += G2P_T) {
+            const uint32_t k = base + threadIdx.x;
+            bool brk = false;
+            V3 bx = {0.0f, 0.0f, 0.0f}, bv = bx;
+            uint32_t bid = 0;
+            if (k < count) {
+                const uint32_t i = D.sorted[first + k];
+                const float4 pos = D.pos[i];
+                const float c1w = D.c1[i].w;
+                V3 X = (xyz(pos) - g.org) / hh;
+                Gathered gu = gather(tg, X, v3(0.0f, 0.5f, 0.5f), corner, 0, 1, hh);
+                Gathered gv = gather(tg, X, v3(0.5f, 0.0f, 0.5f), corner, 2, 3, hh);
+                Gathered gw = gather(tg, X, v3(0.5f, 0.5f, 0.0f), corner, 4, 5, hh);
+                Gathered gp = gather(tg, X, v3(0.5f, 0.5f, 0.5f), corner, A_PC, A_WC, hh);
+                V3 v = {gu.s, gv.s, gw.s};
+                float m_near = gu.w + gv.w + gw.w;
+                V3 x = xyz(pos) + step * v;
+                if (U->mem[3] > 0u) carve(D, x, v, i, now, hh, step_no);
+                bool escaped = x.x < lo.x || x.z < lo.z || x.x > hi.x || x.z > hi.z || x.y > hi.y;
+                float fill = m_near / 24.0f;
+                bool on_ground = x.y < 1.5f * spacing;
+                I3 oc = vi(vfloor(X)) - corner;
+                uint32_t own_t = tile_cell(links, (uint32_t)oc.x * 49u + (uint32_t)oc.y * 7u + (uint32_t)oc.z);
+                bool covered = own_t != NONE && accv(D, A_MA, own_t) > 0;
+                float thin_age = (fill < 0.45f && !on_ground && !covered) ? c1w + step : 0.0f;
+                if (escaped || (!covered && fill < 0.2f) || thin_age > t_thin) {
+                    if (on_ground) {
+                        ground_touch(D, x, now);
+                    } else {
+                        brk = true;
+                        bx = x, bv = v, bid = i;
+                    }
+                    D.vel[i] = f4(v, 0.0f);
+                } else {
+                    V3 xx = x, vv = v;
+                    if (xx.y < 0.3f * spacing) {
+                        xx.y = 0.3f * spacing;
+                        vv.y = mx(vv.y, 0.0f);
+                    }
+                    if (xx.y < 0.7f * spacing) ground_touch(D, xx, now);
+                    D.pos[i] = f4(xx, pos.w);
+                    D.vel[i] = f4(vv, 1.0f);
+                    D.c0[i] = f4(gu.g * cs, gp.w > 1e-6f ? gp.s / gp.w : 0.0f);
+                    D.c1[i] = f4(gv.g * cs, thin_age);
+                    D.c2[i] = f4(gw.g * cs, 0.0f);
+                    fastest = mx(fastest, length(vv));
+                }
+            }
+            // Rank this round's break-ups in sorted order and put them after the earlier ones.
+            uint32_t bal = __ballot_sync(0xffffffffu, brk);
+            if (lane == 0) s_wcount[warp] = __popc(bal);
+            __syncthreads();
+            uint32_t before = s_brk;
+            for (uint32_t w = 0; w < warp; w++) before += s_wcount[w];
+            if (brk) {
+                uint32_t r = before + __popc(bal & ((1u << lane) - 1u));
+                D.brk_x[first + r] = f4(bx, __uint_as_float(bid));
+                D.brk_v[first + r] = f4(bv, 0.0f);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                uint32_t t = 0;
+                for (uint32_t w = 0; w < G2P_T / 32; w++) t += s_wcount[w];
+                s_brk += t;
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) D.brk_count[b] = s_brk;
+        __syncthreads();
+    }
+    for (int o = 16; o > 0; o >>= 1) fastest = fmaxf(fastest, __shfl_down_sync(0xffffffffu, fastest, o));
+    if (lane == 0 && fastest > 0.0f) atomicMax((unsigned int*)&st->s.max_speed, __float_as_uint(fastest));
+}
+
+// Exclusive scan of the blocks' break-up counts (one CTA); advances the spray count.
+__global__ void __launch_bounds__(1024) k_spray_scan(Dev D) {
+    DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const uint32_t n = min(st->s.n_blocks, D.cap_blocks);
+    const uint32_t per = (n + 1023u) / 1024u;
+    const uint32_t lo = min(threadIdx.x * per, n), hi = min(lo + per, n);
+    uint32_t s = 0;
+    for (uint32_t i = lo; i < hi; i++) s += D.brk_count[i];
+    __shared__ uint32_t ws[32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t inc = s;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= (uint32_t)o) inc += v;
+    }
+    if (lane == 31) ws[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t v = ws[lane], x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= (uint32_t)o) x += y;
+        }
+        ws[lane] = x;  // inclusive
+    }
+    __syncthreads();
+    uint32_t run = (warp > 0 ? ws[warp - 1] : 0u) + inc - s;
+    for (uint32_t i = lo; i < hi; i++) {
+        D.brk_off[i] = run;
+        run += D.brk_count[i];
+    }
+    if (threadIdx.x == 0) {
+        uint32_t total = ws[31];
+        st->nbrk = total;
+    }
+}
+
+// Writes the drops of every break-up (fluid.wgsl:718-765): 4 drops and a parcel of finer ones.
+__global__ void k_spray_emit(Dev D) {
+    DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
+    const uint32_t cap = D.spray_cap;
+    const uint32_t base_count = st->s.spray_count;
+    const float hs = D.U->fluid[3], rhow = D.U->fluid[0];
+    const float now = now_of(st);
+    const uint32_t step_no = st->s.step;
+    const float vol = hs * hs * hs;
+    // One warp per block, lanes over its break-ups.
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t b = gw; b < nb; b += nw) {
+        const uint32_t cnt = D.brk_count[b];
+        if (cnt == 0) continue;
+        const uint32_t first_pos = D.block_start[b];
+        for (uint32_t r = lane; r < cnt; r += 32) {
+            const uint32_t grank = D.brk_off[b] + r;
+            const uint32_t firsts = base_count + 5u * grank;
+            if (firsts >= cap) continue;
+            const float4 ex = D.brk_x[first_pos + r], ev = D.brk_v[first_pos + r];
+            const V3 x = xyz(ex), v = xyz(ev);
+            const uint32_t id = __float_as_uint(ex.w);
+            uint32_t seed = hash3(step_no, id, 0xb4eau);
+            float speed = length(v);
+            float bd2 = WE_CRIT * SIGMA_W / (RHO_AIR * mx(speed * speed, 1e-4f));
+            float d_med = mn(0.55f * hs, 0.5f * bd2);
+            float dd[4];
+            float used = 0.0f;
+            for (int k = 0; k < 4; k++) {
+                dd[k] = clampf_(d_med * nt_exp(0.5f * rnd_gauss(seed)), 2e-5f, 1.24f * hs);
+                used += 0.5236f * dd[k] * dd[k] * dd[k];
+            }
+            float df = 0.5f * d_med;
+            bool fine = df < 1e-4f;
+            float fit = nt_pow(vol / used, 1.0f / 3.0f);
+            float scale = fine ? mn(1.0f, fit) : fit;
+            bool stop = false;
+            for (uint32_t k = 0; k < 4; k++) {
+                uint32_t slot = firsts + k;
+                if (slot >= cap) {
+                    stop = true;
+                    break;
+                }
+                float dk = dd[k] * scale;
+                float spread = sqrtf(SIGMA_W / (rhow * dk)) + 0.05f * speed;
+                float g0 = rnd_gauss(seed);
+                float g1 = rnd_gauss(seed);
+                float g2 = rnd_gauss(seed);
+                V3 u = normalize(v3(g0, g1, g2) + 1e-6f);
+                float o0 = rnd(seed);
+                float o1 = rnd(seed);
+                float o2 = rnd(seed);
+                V3 off = (v3(o0, o1, o2) - 0.5f) * hs;
+                float rr = rnd(seed);
+                D.spray[3 * (size_t)slot] = f4(x + off, 0.5f * dk);
+                D.spray[3 * (size_t)slot + 1] = f4(v + u * spread * rr, 1.0f);
+                D.spray[3 * (size_t)slot + 2] = make_float4(0.0f, 0.0f, 0.0f, now);
+            }
+            if (stop) continue;
+            uint32_t slot = firsts + 4;
+            if (slot >= cap) continue;
+            float nn = (vol - used * scale * scale * scale) / (0.5236f * df * df * df);
+            D.spray[3 * (size_t)slot] = f4(x, (fine && nn >= 2.0f) ? 0.5f * df : 0.0f);
+            D.spray[3 * (size_t)slot + 1] = f4(v, mx(nn, 2.0f));
+            D.spray[3 * (size_t)slot + 2] = make_float4(0.0f, 0.0f, 0.0f, now);
+        }
+    }
+}
+
+// The spray count moves on by five slots per break-up, capacity or not (fluid.wgsl:726).
+__global__ void k_spray_commit(Dev D) {
+    DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    if (threadIdx.x == 0 && blockIdx.x == 0) st->s.spray_count += 5u * st->nbrk;
+}
+
+// ---- the zero-length measuring substep and diagnostics --------------------------------------------
+// Conservation sums over live particles in FP64: count, momentum, kinetic energy (per particle
+// mass) and the sum of positions.
+__global__ void k_conservation(Dev D, double* out) {
+    __shared__ double red[8][8];
+    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < D.Np; i += gridDim.x * blockDim.x) {
+        float4 v = D.vel[i];
+        if (v.w < 0.5f) continue;
+        float4 p = D.pos[i];
+        a[0] += 1.0;
+        a[1] += v.x, a[2] += v.y, a[3] += v.z;
+        a[4] += 0.5 * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+        a[5] += p.x, a[6] += p.y, a[7] += p.z;
+    }
+    for (int k = 0; k < 8; k++)
+        for (int o = 16; o > 0; o >>= 1) a[k] += __shfl_down_sync(0xffffffffu, a[k], o);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int k = 0; k < 8; k++) red[warp][k] = a[k];
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        double s = 0;
+        for (uint32_t w = 0; w < blockDim.x / 32; w++) s += red[w][threadIdx.x];
+        atomicAdd(out + threadIdx.x, s);
+    }
+}
+
+}  // namespace ntr

@@ -1,0 +1,433 @@
+// Kernels of the step up to the transfer to the grid: the step clock, block activation over a
+// bitmask, the stable radix sort of particles by block, and APIC P2G in a shared-memory tile.
+//
+// Reference: shaders/fluid.wgsl:33-303 (begin_step .. p2g), membrane.wgsl:164-180
+// (mark_rubber), air.wgsl:271-277 (keep_blocks).
+#pragma once
+
+#include "dev.cuh"
+
+namespace ntr {
+
+// ---- begin_step, fluid.wgsl:33-89 ------------------------------------------------------------
+__global__ void k_begin_step(Dev D) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const ntr_gpu_params* U = D.U;
+    ntr_state& s = D.st->s;
+    float vmax = s.max_speed;
+    uint32_t arrive = U->limits[3];
+    for (uint32_t k = 0; k < U->mem[3]; k++) {
+        const DBullet& b = D.bullets[k];
+        if (b.info.z == 1u) {
+            vmax = mx(vmax, b.l.w);
+        } else if (b.info.z == 0u) {
+            if (b.info.x > s.t_ns)
+                arrive = min(arrive, b.info.x);
+            else
+                vmax = mx(vmax, length(xyz(b.v)));
+        }
+    }
+    float mem_dt = s.mem_dt, air_dt = s.air_dt;
+    float dt_s = mn(U->fluid[2], s.cap_dt);
+    if (vmax > 0.0f) dt_s = mn(dt_s, U->fluid[1] * U->origin[3] / vmax);
+    s.dt_flow = dt_s;
+    s.mem_dt_seen = mem_dt;
+    s.air_dt_seen = air_dt;
+    dt_s = mn(dt_s, mn((float)U->mem[1] * mem_dt, (float)U->mem[2] * air_dt));
+    if (s.free_dt_ns > 0u) dt_s = mn(dt_s, 1.25f * (float)s.free_dt_ns * 1e-9f);
+    uint32_t free_ns = max(f2u(dt_s * 1e9f), 20u);
+    uint32_t stop = U->limits[3];
+    bool live = s.t_ns < stop;
+    uint32_t dt_ns = 0;
+    if (live) {
+        dt_ns = min(free_ns, min(stop, arrive) - s.t_ns);
+        s.free_dt_ns = free_ns;
+        s.t_ns += dt_ns;
+        s.step += 1;
+        s.max_speed = 0.0f;
+        s.mem_dt = __uint_as_float(FLT_MAX_BITS);
+        s.cap_dt = __uint_as_float(FLT_MAX_BITS);
+        s.air_dt = __uint_as_float(FLT_MAX_BITS);
+        s.mem_ticket = 0;
+        s.n_blocks_prev = min(s.n_blocks, U->bdims[3]);
+        s.n_blocks = 0;
+        D.st->nbrk = 0;
+    }
+    s.dt_ns = dt_ns;
+}
+
+// ---- clear: the last step's transfer sums, and this step's bitmask ----------------------------
+__global__ void k_clear(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const int cur = cur_of(st);
+    const uint32_t ncell = st->s.n_blocks_prev * 64u;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (size_t i = tid; i < (size_t)ncell * NTR_ACC_FIELDS; i += stride) {
+        size_t f = i / ncell, c = i - f * ncell;
+        D.acc[f * D.cap_cells + c] = 0;
+    }
+    uint32_t* m = D.mask[cur];
+    for (size_t w = tid; w < D.nwords; w += stride) m[w] = 0u;
+}
+
+// Sets the bit of block `slot` once per distinct slot of the warp.
+__device__ __forceinline__ void set_block_bit(uint32_t* mask, uint32_t slot, bool valid) {
+    uint32_t key = valid ? slot : NONE;
+    uint32_t peers = __match_any_sync(0xffffffffu, key);
+    if (valid && (__ffs(peers) - 1) == (int)(threadIdx.x & 31u)) atomicOr(mask + (slot >> 5), 1u << (slot & 31u));
+}
+
+// ---- mark: particles' stencils, active air, dry rubber (fluid.wgsl:131-150, air.wgsl:271-277,
+// membrane.wgsl:164-180). One thread per particle, then per last-step block, then per vertex.
+__global__ void k_mark(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const int cur = cur_of(st);
+    const Grid g = grid_of(D, cur);
+    const uint32_t n_prev = st->s.n_blocks_prev;
+    uint32_t* mask = D.mask[cur];
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const I3 bmax = {(int32_t)g.bd[0] - 1, (int32_t)g.bd[1] - 1, (int32_t)g.bd[2] - 1};
+    auto clampb = [&](I3 b) {
+        return I3{min(max(b.x, 0), bmax.x), min(max(b.y, 0), bmax.y), min(max(b.z, 0), bmax.z)};
+    };
+    {
+        // Every lane of the warp runs the loop over the up to 2x2x2 blocks of a particle's
+        // stencil (lanes without a live particle claim nothing), so the warp-wide match is
+        // taken by all 32 lanes.
+        const bool isp = i < D.Np;
+        bool alive = false;
+        I3 lo = {0, 0, 0}, hi = {-1, -1, -1};
+        if (isp) {
+            float4 p = D.pos[i];
+            alive = D.vel[i].w >= 0.5f;
+            I3 c = own_cell(g, xyz(p));
+            lo = clampb(shr2(c - I3{1, 1, 1}));
+            hi = clampb(shr2(c + I3{2, 2, 2}));
+            I3 ob = shr2(c);
+            D.pslot[i] = (alive && in_bd(g, ob)) ? block_slot(g, ob) : NONE;
+        }
+        for (int k = 0; k < 8; k++) {
+            I3 b = {lo.x + (k & 1), lo.y + ((k >> 1) & 1), lo.z + ((k >> 2) & 1)};
+            bool valid = alive && b.x <= hi.x && b.y <= hi.y && b.z <= hi.z;
+            set_block_bit(mask, valid ? block_slot(g, b) : 0u, valid);
+        }
+        if (isp) return;
+    }
+    uint32_t j = i - D.Np;
+    if (j < n_prev) {
+        if (D.block_active[j] != 0u) {
+            uint32_t s = D.block_list[cur ^ 1][j];
+            atomicOr(mask + (s >> 5), 1u << (s & 31u));
+        }
+        return;
+    }
+    j -= n_prev;
+    if (j < D.Nv) {
+        float2 push = D.mem_push[j];
+        bool on_water = D.mem_mass[j] > 0.0f && D.mem_water[j].w >= CONTACT_F;
+        if (push.y <= 0.0f || on_water) return;
+        I3 c = own_cell(g, xyz(D.mem_x[0][j]));
+        I3 lo = clampb(shr2(c - I3{2, 2, 2})), hi = clampb(shr2(c + I3{3, 3, 3}));
+        for (int x = lo.x; x <= hi.x; x++)
+            for (int y = lo.y; y <= hi.y; y++)
+                for (int z = lo.z; z <= hi.z; z++) {
+                    uint32_t s = block_slot(g, I3{x, y, z});
+                    atomicOr(mask + (s >> 5), 1u << (s & 31u));
+                }
+    }
+}
+
+// ---- compaction of the bitmask: blocks numbered in ascending slot order ----------------------
+constexpr int SCAN_T = 256, SCAN_W = 8;  // 2048 words per CTA
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_words_a(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const uint32_t* m = D.mask[cur_of(st)];
+    uint32_t base = blockIdx.x * SCAN_T * SCAN_W;
+    uint32_t s = 0;
+    for (int k = 0; k < SCAN_W; k++) {
+        uint32_t w = base + k * SCAN_T + threadIdx.x;
+        if (w < D.nwords) s += __popc(m[w]);
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    __shared__ uint32_t ws[SCAN_T / 32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int k = 0; k < SCAN_T / 32; k++) t += ws[k];
+        D.cta_sum[blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(SCAN_T) k_scan_words_b(Dev D) {
+    DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const int cur = cur_of(st);
+    const uint32_t* m = D.mask[cur];
+    uint32_t* prefix = D.prefix[cur];
+    uint32_t* list = D.block_list[cur];
+    __shared__ uint32_t s_base, ws[SCAN_T / 32];
+    if (threadIdx.x < 32) {
+        uint32_t t = 0;
+        for (uint32_t k = threadIdx.x; k < blockIdx.x; k += 32) t += D.cta_sum[k];
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (threadIdx.x == 0) s_base = t;
+    }
+    // Each thread owns SCAN_W consecutive words.
+    uint32_t w0 = blockIdx.x * SCAN_T * SCAN_W + threadIdx.x * SCAN_W;
+    uint32_t words[SCAN_W], cnt = 0;
+    for (int k = 0; k < SCAN_W; k++) {
+        words[k] = (w0 + k < D.nwords) ? m[w0 + k] : 0u;
+        cnt += __popc(words[k]);
+    }
+    uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t inc = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= (uint32_t)o) inc += v;
+    }
+    if (lane == 31) ws[warp] = inc;
+    __syncthreads();
+    uint32_t wbase = 0;
+    for (uint32_t k = 0; k < warp; k++) wbase += ws[k];
+    uint32_t run = s_base + wbase + inc - cnt;
+    const uint32_t cap = D.cap_blocks;
+    for (int k = 0; k < SCAN_W; k++) {
+        uint32_t w = w0 + k;
+        if (w >= D.nwords) break;
+        prefix[w] = run;
+        uint32_t bits = words[k];
+        while (bits) {
+            uint32_t b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            if (run < cap) list[run] = w * 32u + b;
+            run++;
+        }
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == SCAN_T - 1) {
+        st->s.n_blocks = run;
+        if (run > cap) st->s.overflow = 1u;
+    }
+}
+
+// ---- keys: each live particle's block index ---------------------------------------------------
+__global__ void k_keys(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const int cur = cur_of(st);
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.Np) return;
+    uint32_t s = D.pslot[i];
+    D.key[i] = s == NONE ? NONE : lookup(D.mask[cur], D.prefix[cur], s, D.cap_blocks);
+}
+
+// ---- stable LSD radix sort of (block index, particle index), 8 bits per pass ------------------
+// Pass p reads keys (and values, except in pass 0 where the value is the position) and writes
+// them in the stable order of digit (key >> 8p) & 255. Tiles of RADIX_TILE elements.
+constexpr int RADIX_T = 256, RADIX_ITEMS = 16, RADIX_TILE = RADIX_T * RADIX_ITEMS;
+
+__global__ void __launch_bounds__(RADIX_T) k_radix_hist(Dev D, const uint32_t* keys, uint32_t shift) {
+    if (D.st->s.dt_ns == 0) return;
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    uint32_t base = blockIdx.x * RADIX_TILE;
+    for (int r = 0; r < RADIX_ITEMS; r++) {
+        uint32_t i = base + r * RADIX_T + threadIdx.x;
+        // Lanes past the end match on 256, a digit no element has, and add nothing.
+        uint32_t d = i < D.Np ? (keys[i] >> shift) & 255u : 256u;
+        uint32_t peers = __match_any_sync(0xffffffffu, d);
+        if (d < 256u && (__ffs(peers) - 1) == (int)(threadIdx.x & 31u)) atomicAdd(&h[d], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    D.hist[threadIdx.x * D.n_tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of the digit-major histogram (256 x n_tiles), one CTA.
+__global__ void __launch_bounds__(1024) k_radix_scan(Dev D) {
+    if (D.st->s.dt_ns == 0) return;
+    const uint32_t n = 256u * D.n_tiles;
+    const uint32_t per = (n + 1023u) / 1024u;
+    uint32_t lo = threadIdx.x * per, hi = min(lo + per, n);
+    uint32_t s = 0;
+    for (uint32_t i = lo; i < hi; i++) s += D.hist[i];
+    __shared__ uint32_t ws[32];
+    uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t inc = s;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= (uint32_t)o) inc += v;
+    }
+    if (lane == 31) ws[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t v = ws[lane];
+        uint32_t x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= (uint32_t)o) x += y;
+        }
+        ws[lane] = x - v;
+    }
+    __syncthreads();
+    uint32_t run = ws[warp] + inc - s;
+    for (uint32_t i = lo; i < hi; i++) {
+        uint32_t c = D.hist[i];
+        D.hist[i] = run;
+        run += c;
+    }
+}
+
+__global__ void __launch_bounds__(RADIX_T) k_radix_scatter(Dev D, const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                                                           uint32_t* vals_out, uint32_t shift) {
+    if (D.st->s.dt_ns == 0) return;
+    __shared__ uint32_t s_base[256];
+    __shared__ uint32_t s_run[256];
+    __shared__ uint32_t s_wh[RADIX_T / 32][256];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    s_base[threadIdx.x] = D.hist[threadIdx.x * D.n_tiles + blockIdx.x];
+    s_run[threadIdx.x] = 0;
+    const uint32_t base = blockIdx.x * RADIX_TILE;
+    for (int r = 0; r < RADIX_ITEMS; r++) {
+        for (int w = 0; w < RADIX_T / 32; w++) s_wh[w][threadIdx.x] = 0;
+        __syncthreads();
+        uint32_t i = base + r * RADIX_T + threadIdx.x;
+        bool in = i < D.Np;
+        uint32_t key = in ? keys_in[i] : NONE;
+        uint32_t val = in ? (vals_in ? vals_in[i] : i) : 0u;
+        uint32_t d = in ? ((key >> shift) & 255u) : 256u;
+        uint32_t peers = __match_any_sync(0xffffffffu, d);
+        uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+        if (in && rank == 0) s_wh[warp][d] = __popc(peers);
+        __syncthreads();
+        // Per digit: exclusive offsets of the warps, after the elements of earlier rounds.
+        {
+            uint32_t dg = threadIdx.x;
+            uint32_t run = s_run[dg];
+            for (int w = 0; w < RADIX_T / 32; w++) {
+                uint32_t c = s_wh[w][dg];
+                s_wh[w][dg] = run;
+                run += c;
+            }
+            s_run[dg] = run;
+        }
+        __syncthreads();
+        if (in) {
+            uint32_t pos = s_base[d] + s_wh[warp][d] + rank;
+            keys_out[pos] = key;
+            vals_out[pos] = val;
+        }
+        __syncthreads();
+    }
+}
+
+// block_start from the sorted keys: block b starts at the first position whose key is >= b.
+__global__ void k_block_bounds(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
+    const uint32_t* ks = D.key_sorted;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p <= D.Np; p += gridDim.x * blockDim.x) {
+        int64_t k = p < D.Np ? (int64_t)min(ks[p], nb) : (int64_t)nb;
+        int64_t kp = p > 0 ? (int64_t)min(ks[p - 1], nb) : -1;
+        for (int64_t b = kp + 1; b <= k; b++) D.block_start[b] = p;
+    }
+}
+
+// ---- P2G, fluid.wgsl:198-303 -----------------------------------------------------------------
+// One block per iteration of a CTA: the block's particles add into a 7^3 x 8-field tile of i32
+// fixed-point sums in shared memory, which then goes out to the grid with one atomic add per
+// nonzero tile entry. Fixed-point sums do not depend on the order of the adds.
+constexpr int P2G_T = 256;
+
+__device__ __forceinline__ void splat(int32_t* tile, V3 x, V3 o, I3 corner, uint32_t fa, float val, V3 grad, uint32_t fw, float scale, float hh) {
+    I3 base = vi(vfloor(x - o - 0.5f));
+    V3 fx = x - o - vf(base);
+    V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
+    I3 t = base - corner;
+    uint32_t t0 = (uint32_t)t.x * 49u + (uint32_t)t.y * 7u + (uint32_t)t.z;
+    V3 hg = grad * hh;
+#pragma unroll
+    for (uint32_t a = 0; a < 3; a++)
+#pragma unroll
+        for (uint32_t b = 0; b < 3; b++)
+#pragma unroll
+            for (uint32_t c = 0; c < 3; c++) {
+                float weight = wx[a] * wy[b] * wz[c];
+                uint32_t tt = t0 + a * 49u + b * 7u + c;
+                float node = val + dot(hg, v3((float)a, (float)b, (float)c) - fx);
+                atomicAdd(&tile[fa * TILE + tt], to_fp(weight * node, scale));
+                atomicAdd(&tile[fw * TILE + tt], to_fp(weight, FP_W));
+            }
+}
+
+__device__ __forceinline__ uint32_t tile_cell(const uint32_t* links, uint32_t t) {
+    I3 rel = {(int32_t)(t / 49u) - 1, (int32_t)((t / 7u) % 7u) - 1, (int32_t)(t % 7u) - 1};
+    I3 nb = {(rel.x + 4) / 4 - 1, (rel.y + 4) / 4 - 1, (rel.z + 4) / 4 - 1};
+    uint32_t b = links[(uint32_t)((nb.x + 1) * 9 + (nb.y + 1) * 3 + nb.z + 1)];
+    if (b == NONE) return NONE;
+    I3 l = rel - nb * 4;
+    return b * 64u + (uint32_t)l.x * 16u + (uint32_t)l.y * 4u + (uint32_t)l.z;
+}
+
+__global__ void __launch_bounds__(P2G_T) k_p2g(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const Grid g = grid_of(D, cur_of(st));
+    const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
+    __shared__ int32_t tile[8 * TILE];
+    __shared__ uint32_t own[64];
+    __shared__ uint32_t links[27];
+    const float hh = g.h;
+    for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
+        const I3 bc = slot_coord(g, g.list[b]);
+        if (threadIdx.x < 27) {
+            uint32_t li = threadIdx.x;
+            I3 n = bc + I3{(int32_t)(li / 9u), (int32_t)((li / 3u) % 3u), (int32_t)(li % 3u)} - I3{1, 1, 1};
+            uint32_t idx = block_at(g, n);
+            links[li] = idx;
+            D.block_nb[b * 27u + li] = idx;
+        }
+        if (threadIdx.x < 64) own[threadIdx.x] = 0;
+        const uint32_t first = D.block_start[b];
+        const uint32_t count = D.block_start[b + 1] - first;
+        if (count == 0) {
+            if (threadIdx.x < 64) D.acc[(size_t)A_N * D.cap_cells + b * 64u + threadIdx.x] = 0;
+            __syncthreads();
+            continue;
+        }
+        for (uint32_t t = threadIdx.x; t < 8 * TILE; t += P2G_T) tile[t] = 0;
+        __syncthreads();
+        const I3 corner = bc * 4 - I3{1, 1, 1};
+        for (uint32_t k = threadIdx.x; k < count; k += P2G_T) {
+            uint32_t i = D.sorted[first + k];
+            float4 pos = D.pos[i], vel = D.vel[i], c0 = D.c0[i], c1 = D.c1[i], c2 = D.c2[i];
+            V3 x = (xyz(pos) - g.org) / hh;
+            splat(tile, x, v3(0.0f, 0.5f, 0.5f), corner, 0, vel.x, xyz(c0), 1, FP_M, hh);
+            splat(tile, x, v3(0.5f, 0.0f, 0.5f), corner, 2, vel.y, xyz(c1), 3, FP_M, hh);
+            splat(tile, x, v3(0.5f, 0.5f, 0.0f), corner, 4, vel.z, xyz(c2), 5, FP_M, hh);
+            splat(tile, x, v3(0.5f, 0.5f, 0.5f), corner, A_PC, c0.w * 1e-6f, v3(0.0f, 0.0f, 0.0f), A_WC, FP_P, hh);
+            I3 l = own_cell(g, xyz(pos)) - bc * 4;
+            atomicAdd(&own[l.x * 16 + l.y * 4 + l.z], 1u);
+        }
+        __syncthreads();
+        for (uint32_t t = threadIdx.x; t < TILE; t += P2G_T) {
+            uint32_t cell = tile_cell(links, t);
+            if (cell == NONE) continue;
+#pragma unroll
+            for (uint32_t f = 0; f < 8; f++) {
+                int32_t v = tile[f * TILE + t];
+                if (v != 0) atomicAdd(&D.acc[(size_t)f * D.cap_cells + cell], v);
+            }
+        }
+        if (threadIdx.x < 64) D.acc[(size_t)A_N * D.cap_cells + b * 64u + threadIdx.x] = (int32_t)own[threadIdx.x];
+        __syncthreads();
+    }
+}
+
+}  // namespace ntr

@@ -1,0 +1,637 @@
+// Rubber substep (shaders/membrane.wgsl:40-149, 258-400) with bullet contact
+// (shaders/bullet.wgsl:426-611), and the bullets' own step (bullet.wgsl:92-383).
+#pragma once
+
+#include "kernels_cells.cuh"
+
+namespace ntr {
+
+__device__ __forceinline__ V3 qrot(float4 q, V3 v) {
+    V3 qv = xyz(q);
+    V3 t = 2.0f * cross(qv, v);
+    return v + q.w * t + cross(qv, t);
+}
+__device__ __forceinline__ float4 qmul(float4 a, float4 b) {
+    V3 v = a.w * xyz(b) + b.w * xyz(a) + cross(xyz(a), xyz(b));
+    return make_float4(v.x, v.y, v.z, a.w * b.w - dot(xyz(a), xyz(b)));
+}
+__device__ __forceinline__ float4 normalize4(float4 q) {
+    float inv = 1.0f / sqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+    return make_float4(q.x * inv, q.y * inv, q.z * inv, q.w * inv);
+}
+
+struct Sheet {
+    float sx, sy, tangent;
+};
+
+// Ogden plane stress with wrinkling (membrane.wgsl:47-65).
+__device__ __forceinline__ Sheet sheet(const ntr_gpu_params* U, float major, float minor) {
+    if (major <= 1.0f) return {0.0f, 0.0f, 0.0f};
+    const V3 mu = {U->rubber[0], U->rubber[1], U->rubber[2]};
+    const V3 AL = {1.3f, 5.0f, -2.0f};
+    float la = nt_log(major);
+    V3 e1 = AL * la;
+    V3 pa = {nt_exp(e1.x), nt_exp(e1.y), nt_exp(e1.z)};
+    float tan_scale = 1.0f / (major * major);
+    if (minor * minor * major < 1.0f) {
+        V3 e2 = ((-0.5f) * AL) * la;
+        V3 pn = {nt_exp(e2.x), nt_exp(e2.y), nt_exp(e2.z)};
+        return {dot(mu, pa - pn), 0.0f, dot(mu * AL, pa + 0.5f * pn) * tan_scale};
+    }
+    float lb = nt_log(minor);
+    V3 e3 = AL * lb;
+    V3 pb = {nt_exp(e3.x), nt_exp(e3.y), nt_exp(e3.z)};
+    V3 e4 = (-AL) * (la + lb);
+    V3 p3 = {nt_exp(e4.x), nt_exp(e4.y), nt_exp(e4.z)};
+    return {dot(mu, pa - p3), dot(mu, pb - p3), dot(mu * AL, pa + p3) * tan_scale};
+}
+
+struct VertexForce {
+    V3 f, n;
+    float area, stiff, tension, reach, thick;
+};
+
+__device__ VertexForce vertex_force(const Dev& D, int par, uint32_t i) {
+    const ntr_gpu_params* U = D.U;
+    const float4* X = D.mem_x[par];
+    const float thick0 = U->rubber[3];
+    VertexForce o = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, 0.0f, 0.0f, 0.0f, 0.0f, thick0};
+    float rest = 0.0f;
+    const uint32_t k0 = D.vtri_off[i], k1 = D.vtri_off[i + 1];
+    for (uint32_t k = k0; k < k1; k++) {
+        uint32_t t = D.vtri[k];
+        if (*(volatile uint32_t*)&D.alive[t] == 0u) continue;
+        const Tri tri = D.tris[t];
+        V3 x0 = xyz(X[tri.v0]);
+        V3 e1 = xyz(X[tri.v1]) - x0;
+        V3 e2 = xyz(X[tri.v2]) - x0;
+        const float mxx = tri.dm_inv.x, myy = tri.dm_inv.y, mzz = tri.dm_inv.z, mww = tri.dm_inv.w;
+        o.reach = mx(o.reach, mx(length(e1), mx(length(e2), length(e2 - e1))));
+        V3 f0 = e1 * mxx + e2 * mzz;
+        V3 f1 = e1 * myy + e2 * mww;
+        float c00 = dot(f0, f0), c01 = dot(f0, f1), c11 = dot(f1, f1);
+        float mid = 0.5f * (c00 + c11);
+        float dev = sqrtf(0.25f * (c00 - c11) * (c00 - c11) + c01 * c01);
+        float lx = sqrtf(mid + dev), ly = sqrtf(mx(mid - dev, 1e-12f));
+        if (lx >= U->rubber2[1]) {
+            *(volatile uint32_t*)&D.alive[t] = 0u;
+            continue;
+        }
+        Sheet sh = sheet(U, lx, ly);
+        float ex = 1.0f, ey = 0.0f;
+        if (dev > 1e-6f * mid) {
+            float qx, qy;
+            if (c00 >= c11)
+                qx = mid + dev - c11, qy = c01;
+            else
+                qx = c01, qy = mid + dev - c00;
+            float inv = 1.0f / sqrtf(qx * qx + qy * qy);
+            ex = qx * inv, ey = qy * inv;
+        }
+        float sx = sh.sx / (lx * lx), sy = sh.sy / (ly * ly);
+        float ds = sx - sy;
+        float s00 = sy + ds * ex * ex;
+        float s01 = ds * ex * ey;
+        float s11 = sy + ds * ey * ey;
+        V3 p0 = f0 * s00 + f1 * s01;
+        V3 p1 = f0 * s01 + f1 * s11;
+        float vol = tri.rest_area * thick0;
+        V3 h1 = (-vol) * (p0 * mxx + p1 * myy);
+        V3 h2 = (-vol) * (p0 * mzz + p1 * mww);
+        float gx = mxx, gy = myy;
+        if (i == tri.v0) {
+            o.f = o.f - (h1 + h2);
+            gx = -(mxx + mzz), gy = -(myy + mww);
+        } else if (i == tri.v1) {
+            o.f = o.f + h1;
+        } else {
+            o.f = o.f + h2;
+            gx = mzz, gy = mww;
+        }
+        V3 cr = cross(e1, e2);
+        o.n = o.n + cr;
+        o.area += length(cr) / 6.0f;
+        rest += tri.rest_area / 3.0f;
+        o.stiff += vol * (gx * gx + gy * gy) * (sh.tangent + sx);
+        o.tension = mx(o.tension, sh.sx * thick0 / (lx * ly));
+    }
+    if (o.area > 0.0f) o.thick = thick0 * rest / o.area;
+    return o;
+}
+
+struct Near {
+    float ax, ay, nx, ny, depth;
+};
+
+// The nearest point of bullet `bi`'s outline to q = (z, r) of its body frame
+// (bullet.wgsl:438-472).
+__device__ Near nearest_surface(const Dev& D, uint32_t bi, float qx, float qy) {
+    const float2* ol = D.outlines + bi * NTR_OUTLINE;
+    float2 first = ol[0], last = ol[NTR_OUTLINE - 1];
+    Near o = {qx, qy, 0.0f, 0.0f, 0.0f};
+    float best = BIG_F;
+    for (uint32_t j = 0; j <= NTR_OUTLINE; j++) {
+        float2 p0 = make_float2(first.x, 0.0f), p1 = make_float2(last.x, 0.0f);
+        if (j > 0) p0 = ol[j - 1];
+        if (j < NTR_OUTLINE) p1 = ol[j];
+        float ex = p1.x - p0.x, ey = p1.y - p0.y;
+        float len2 = ex * ex + ey * ey;
+        if (len2 <= 0.0f) continue;
+        float tt = clampf_(((qx - p0.x) * ex + (qy - p0.y) * ey) / len2, 0.0f, 1.0f);
+        float onx = p0.x + ex * tt, ony = p0.y + ey * tt;
+        float dqx = qx - onx, dqy = qy - ony;
+        float d = sqrtf(dqx * dqx + dqy * dqy);
+        if (d < best) {
+            best = d;
+            o.ax = onx, o.ay = ony;
+            float nnx = -ey, nny = ex;
+            float inv = 1.0f / sqrtf(nnx * nnx + nny * nny);
+            o.nx = nnx * inv, o.ny = nny * inv;
+        }
+    }
+    bool inside = false;
+    if (qx > first.x && qx < last.x) {
+        uint32_t k = 1;
+        while (k < NTR_OUTLINE - 1 && ol[k].x < qx) k++;
+        float2 a = ol[k - 1], c = ol[k];
+        float f = (qx - a.x) / mx(c.x - a.x, 1e-12f);
+        inside = qy < a.y * (1.0f - f) + c.y * f;
+    }
+    o.depth = inside ? best : -best;
+    if (!inside && best > 0.0f) o.nx = (qx - o.ax) / best, o.ny = (qy - o.ay) / best;
+    return o;
+}
+
+__device__ float rubber_contact(const Dev& D, int par, uint32_t i, V3& x, V3& v, float m, V3 load, const VertexForce& vf, bool wet, bool& held,
+                                float t, float sub, float now, float dt) {
+    const float4* MX = D.mem_x[par];
+    const float4* MV = D.mem_v[par];
+    float limit = BIG_F;
+    float band = held ? 0.5f * vf.thick : 0.0f;
+    held = false;
+    const uint32_t nbu = D.U->mem[3];
+    for (uint32_t bi = 0; bi < nbu; bi++) {
+        const DBullet b = D.bullets[bi];
+        if (b.info.z != 1u) continue;
+        V3 xb = xyz(b.x) - xyz(b.v) * (now - t);
+        float closing = length(xyz(b.v) - v);
+        if (length(x - xb) > b.shape.z + vf.reach + 2.0f * closing * dt) continue;
+        limit = mn(limit, 0.25f * b.shape.w / mx(closing, 1e-6f));
+        float4 back = make_float4(-b.q.x, -b.q.y, -b.q.z, b.q.w);
+        V3 w = qrot(b.q, qrot(back, xyz(b.l)) / v3(b.shape.y, b.shape.y, b.shape.x));
+        float best = -band;
+        bool found = false;
+        V3 gap = {0.0f, 0.0f, 0.0f}, on_b = gap, nrm = gap, rel = gap;
+        float share = 0.0f;
+        const uint32_t k0 = D.vtri_off[i], k1 = D.vtri_off[i + 1];
+        for (uint32_t k = k0; k <= k1; k++) {
+            V3 p[3] = {x, x, x};
+            V3 pv[3] = {v, v, v};
+            uint32_t own = 0, n = 1;
+            if (k < k1) {
+                uint32_t tn = D.vtri[k];
+                if (*(volatile uint32_t*)&D.alive[tn] == 0u) continue;
+                const Tri tri = D.tris[tn];
+                uint32_t ids[3] = {tri.v0, tri.v1, tri.v2};
+                for (uint32_t c = 0; c < 3; c++) {
+                    if (ids[c] == i) {
+                        own = c;
+                    } else {
+                        pv[c] = xyz(MV[ids[c]]);
+                        p[c] = xyz(MX[ids[c]]) + sub * pv[c];
+                    }
+                }
+                float longest = mx(distance(p[0], p[1]), mx(distance(p[1], p[2]), distance(p[2], p[0])));
+                n = f2u(clampf_(ceilf(longest / b.shape.w), 1.0f, 8.0f));
+            }
+            for (uint32_t a = 0; a <= n; a++) {
+                for (uint32_t c = 0; c <= n - a; c++) {
+                    V3 bary = v3((float)a, (float)c, (float)(n - a - c)) / (float)n;
+                    float wi = bary[own];
+                    if (wi <= 0.0f) continue;
+                    V3 s = bary.x * p[0] + bary.y * p[1] + bary.z * p[2];
+                    V3 r = s - xb;
+                    if (length(r) >= b.shape.z + band) continue;
+                    V3 q = qrot(back, r);
+                    float rho = sqrtf(q.x * q.x + q.y * q.y);
+                    Near nr = nearest_surface(D, bi, q.z, rho);
+                    if (nr.depth <= best) continue;
+                    float rx = 1.0f, ry = 0.0f;
+                    if (rho > 1e-9f) rx = q.x / rho, ry = q.y / rho;
+                    best = nr.depth;
+                    found = true;
+                    on_b = qrot(b.q, v3(rx * nr.ay, ry * nr.ay, nr.ax));
+                    gap = on_b - r;
+                    nrm = qrot(b.q, v3(rx * nr.ny, ry * nr.ny, nr.nx));
+                    share = wi / dot(bary, bary);
+                    rel = bary.x * pv[0] + bary.y * pv[1] + bary.z * pv[2] - xyz(b.v) - cross(w, on_b);
+                }
+            }
+        }
+        if (!found) continue;
+        float vn = dot(rel, nrm);
+        V3 rel_t = rel - vn * nrm;
+        float slide = length(rel_t);
+        float dvn = 0.0f, jn = 0.0f;
+        V3 j = {0.0f, 0.0f, 0.0f};
+        bool holds = false;
+        if (!wet) {
+            dvn = mx(-vn, 0.0f);
+            jn = m * dvn;
+            j = -m * share * dvn * nrm;
+        } else {
+            float ln = dot(load, nrm);
+            if (ln < 0.0f) {
+                dvn = -vn;
+                jn = -ln * sub;
+                j = mn(share, 1.0f) * ln * sub * nrm;
+                holds = true;
+                held = true;
+            } else if (best > 0.0f) {
+                dvn = mx(-vn, 0.0f);
+            } else {
+                continue;
+            }
+        }
+        float stop = (slide > 1e-9f && m > 0.0f) ? mn(1.0f, MU_JACKET * jn / (m * slide)) : 0.0f;
+        V3 dvt = -share * stop * rel_t;
+        x = x + (share * gap + sub * dvt);
+        v = v + (share * dvn * nrm + dvt);
+        j = j - m * dvt;
+        float nl = length(vf.n);
+        int32_t* hit = D.bullet_hit + bi * NTR_HIT_FIELDS;
+        if (holds && nl > 0.0f) {
+            float a = vf.area * 1e6f;
+            V3 sx = (x - xb) * 1e3f * a;
+            for (int c = 0; c < 3; c++) {
+                atomicAdd(hit + 6 + c, to_fp(vf.n[c] / nl * a, FP_A));
+                atomicAdd(hit + 9 + c, to_fp(sx[c], FP_X));
+            }
+            atomicAdd(hit + 12, to_fp(a, FP_A));
+        }
+        V3 jl = cross(on_b, j);
+        for (int c = 0; c < 3; c++) {
+            atomicAdd(hit + c, to_fp(j[c], FP_J));
+            atomicAdd(hit + 3 + c, to_fp(jl[c], FP_L));
+        }
+    }
+    return limit;
+}
+
+// One explicit rubber substep (membrane.wgsl:283-400). `k` is which substep of the step this
+// is, `par` which pair of buffers it reads.
+__global__ void __launch_bounds__(256) k_mem_substep(Dev D, uint32_t k, int par) {
+    DevState* st = D.st;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    float lim_x = BIG_F, lim_y = BIG_F;
+    const ntr_gpu_params* U = D.U;
+    const float dt = dt_of(st), now = now_of(st);
+    if (i < D.Nv) {
+        const Grid g = grid_of(D, cur_of(st));
+        const float m = D.mem_mass[i];
+        const float4 x4 = D.mem_x[par][i];
+        float4* XO = D.mem_x[1 - par];
+        float4* VO = D.mem_v[1 - par];
+        if (m == 0.0f) {
+            XO[i] = x4;
+            VO[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        } else {
+            const float hh = g.h;
+            const float sub = dt / (float)max(U->mem[1], 1u);
+            const float t_sub = now - dt + (float)(k + 1u) * sub;
+            VertexForce vf = vertex_force(D, par, i);
+            lim_x = sqrtf(m / mx(vf.stiff, 1e-30f));
+            if (vf.tension > 0.0f) lim_y = sqrtf(U->fluid[0] * hh * hh * hh / (4.0f * PI_F * vf.tension));
+            V3 f = vf.f + m * v3(U->gravity[0], U->gravity[1], U->gravity[2]);
+            const float4 v4 = D.mem_v[par][i];
+            V3 v = xyz(v4);
+            float nl = length(vf.n);
+            const size_t first = (size_t)i * NTR_LAYER_MODES;
+            bool held = v4.w > 0.0f;
+            const float4 mw = D.mem_water[i];
+            const bool ow = mw.w >= CONTACT_F;
+            float push = (ow && nl > 0.0f) ? -dot(f, vf.n / mx(nl, 1e-30f)) : 0.0f;
+            D.mem_push[i] = make_float2(held ? 0.0f : push, vf.area);
+            if (sub <= 0.0f) {
+                XO[i] = x4;
+                VO[i] = v4;
+            } else {
+                if (ow && nl > 0.0f) {
+                    V3 n = vf.n / nl;
+                    V3 vw = xyz(mw);
+                    V3 rel = v - vw;
+                    V3 rel_t = rel - dot(rel, n) * n;
+                    V3 ft = f - dot(f, n) * n;
+                    float kk = sqrtf(U->fluid[0] * MU_WATER) * vf.area;
+                    const V3 TAU0 = {2.0e-6f, 3.170e-5f, 5.024e-4f}, TAU1 = {7.962e-3f, 1.262e-1f, 2.0f};
+                    const V3 LW0 = {573.42f, 158.41f, 38.750f}, LW1 = {10.049f, 2.2387f, 0.9494f};
+                    V3 x0 = v3(-sub, -sub, -sub) / TAU0, x1 = v3(-sub, -sub, -sub) / TAU1;
+                    V3 e0 = {nt_exp(x0.x), nt_exp(x0.y), nt_exp(x0.z)}, e1 = {nt_exp(x1.x), nt_exp(x1.y), nt_exp(x1.z)};
+                    V3 g0 = (v3(1.0f, 1.0f, 1.0f) - e0) * TAU0 / v3(sub, sub, sub);
+                    V3 g1 = (v3(1.0f, 1.0f, 1.0f) - e1) * TAU1 / v3(sub, sub, sub);
+                    float lhs = m / sub + kk * (dot(LW0, g0) + dot(LW1, g1));
+                    V3 rhs = m / sub * rel_t + ft;
+                    V3 z[6];
+                    for (int jj = 0; jj < 6; jj++) {
+                        z[jj] = xyz(D.mem_layer[first + jj]);
+                        z[jj] = z[jj] - dot(z[jj], n) * n;
+                    }
+                    for (int bb = 0; bb < 3; bb++) rhs = rhs - kk * LW0[bb] * (e0[bb] * z[bb] - g0[bb] * rel_t);
+                    for (int bb = 0; bb < 3; bb++) rhs = rhs - kk * LW1[bb] * (e1[bb] * z[3 + bb] - g1[bb] * rel_t);
+                    V3 rel_new = rhs / lhs;
+                    for (int bb = 0; bb < 3; bb++) D.mem_layer[first + bb] = f4(e0[bb] * z[bb] + g0[bb] * (rel_new - rel_t), 0.0f);
+                    for (int bb = 0; bb < 3; bb++) D.mem_layer[first + 3 + bb] = f4(e1[bb] * z[3 + bb] + g1[bb] * (rel_new - rel_t), 0.0f);
+                    v = vw + rel_new;
+                    if (held) v = v + dot(rel, n) * n;
+                } else if (ow) {
+                    v = xyz(mw);
+                } else {
+                    for (int jj = 0; jj < 6; jj++) D.mem_layer[first + jj] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    V3 fa = {0.0f, 0.0f, 0.0f};
+                    if (nl > 0.0f) {
+                        V3 n = vf.n / nl;
+                        fa = (gas_pressure_at(D, g, par, xyz(x4) - hh * n) - gas_pressure_at(D, g, par, xyz(x4) + hh * n)) * vf.area * n;
+                    }
+                    v = v + sub * (f + fa) / m;
+                }
+                V3 xx = xyz(x4) + sub * v;
+                held = held && ow;
+                lim_x = mn(lim_x, rubber_contact(D, par, i, xx, v, m, f, vf, ow, held, t_sub, sub, now, dt));
+                D.mem_push[i].x = held ? 0.0f : push;
+                if (xx.y < 0.0f) {
+                    float jj = mx(-v.y, 0.0f);
+                    xx.y = 0.0f;
+                    v.y = mx(v.y, 0.0f);
+                    float s = sqrtf(v.x * v.x + v.z * v.z);
+                    float keep = s > 1e-9f ? mx(0.0f, 1.0f - U->rubber2[0] * jj / s) : 0.0f;
+                    v = v3(v.x * keep, v.y, v.z * keep);
+                }
+                XO[i] = make_float4(xx.x, xx.y, xx.z, x4.w);
+                VO[i] = make_float4(v.x, v.y, v.z, held ? 1.0f : 0.0f);
+            }
+        }
+    }
+    // The longest stable substep and the capillary step, lowered with atomicMin on the bits.
+    for (int o = 16; o > 0; o >>= 1) {
+        lim_x = fminf(lim_x, __shfl_down_sync(0xffffffffu, lim_x, o));
+        lim_y = fminf(lim_y, __shfl_down_sync(0xffffffffu, lim_y, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin((unsigned int*)&st->s.mem_dt, __float_as_uint(lim_x));
+        atomicMin((unsigned int*)&st->s.cap_dt, __float_as_uint(lim_y));
+    }
+}
+
+// ---- the bullets' step, bullet.wgsl:101-383 ---------------------------------------------------
+__device__ __forceinline__ float cp_patch(float s) {
+    if (s < 0.0f) return CP_WAKE * s * s;
+    float beta = nt_asin(mn(s, 1.0f));
+    if (beta < PI_F / 12.0f) return 2.13f * s * s;
+    float x = beta / PI_F - 0.25f;
+    return 0.5f + 1.81f * x - 2.0f * x * x;
+}
+
+__device__ __forceinline__ float2 sample_pressure(const Dev& D, const Grid& g, V3 x, bool gas_only) {
+    I3 base = vi(vfloor(x - 0.5f));
+    V3 fx = x - vf(base);
+    V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
+    float sx = 0.0f, sy = 0.0f;
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++)
+            for (int c = 0; c < 3; c++) {
+                uint32_t cell = cell_at(g, base + I3{a, b, c});
+                if (cell == NONE) continue;
+                float ty = cfv(D, F_TYPE, cell);
+                if (ty == SOLID_T || (gas_only && ty == WATER_T)) continue;
+                float w = wx[a] * wy[b] * wz[c];
+                sx = sx + w * cfv(D, F_P, cell);
+                sy = sy + w;
+            }
+    return make_float2(sx, sy);
+}
+
+__device__ __forceinline__ float section_r2(const DSection& s, float t) { return s.c.x + s.b.w * mx(t - s.a.w, 0.0f); }
+
+__device__ bool in_cavity(const Dev& D, float hh, uint32_t b, V3 p, float t) {
+    float hand2 = R_HAND * R_HAND * hh * hh;
+    for (uint32_t k = 0; k < NTR_N_SEC; k++) {
+        const DSection s = D.sections[b * NTR_N_SEC + k];
+        if (s.b.w <= 0.0f || section_r2(s, t) >= hand2) continue;
+        V3 ab = xyz(s.b) - xyz(s.a);
+        float f = dot(p - xyz(s.a), ab) / mx(dot(ab, ab), 1e-20f);
+        if (f < 0.0f || f > 1.0f) continue;
+        V3 d = p - (xyz(s.a) + f * ab);
+        if (dot(d, d) < section_r2(s, t)) return true;
+    }
+    return false;
+}
+
+__device__ void push_water(const Dev& D, const Grid& g, V3 x, uint32_t d, float j, float sw) {
+    if (sw <= 1e-6f || j == 0.0f) return;
+    V3 lx = x - lattice_offset(d);
+    I3 base = vi(vfloor(lx - 0.5f));
+    V3 fx = lx - vf(base);
+    V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
+    float hs = D.U->fluid[3];
+    float k = j / (D.U->fluid[0] * hs * hs * hs * sw);
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++)
+            for (int c = 0; c < 3; c++) {
+                uint32_t cell = cell_at(g, base + I3{a, b, c});
+                if (cell == NONE || accv(D, a_wt(d), cell) <= 0) continue;
+                atomicAdd(accp(D, A_BU + d, cell), to_fp(k * wx[a] * wy[b] * wz[c], FP_M));
+            }
+}
+
+// One CTA of 256 threads per bullet. Patches are summed per thread (k = li, li + 256, ...) and
+// then by the 256-wide tree, the reference's order.
+__global__ void __launch_bounds__(256) k_bullet_step(Dev D) {
+    DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const uint32_t bi = blockIdx.x;
+    const Grid g = grid_of(D, cur_of(st));
+    const ntr_gpu_params* U = D.U;
+    const uint32_t li = threadIdx.x;
+    const DBullet b = D.bullets[bi];
+    const float step = dt_of(st), t_end = now_of(st), hh = g.h;
+    __shared__ uint32_t s_state;
+    __shared__ float s_pf;
+    __shared__ float4 s_side;
+    __shared__ float4 red_f[256], red_t[256], red_c[256];
+    int32_t* hit = D.bullet_hit + bi * NTR_HIT_FIELDS;
+    if (li == 0) {
+        uint32_t state = b.info.z;
+        if (state == 0u && st->s.t_ns - st->s.dt_ns >= b.info.x) state = 1u;
+        s_state = state;
+        V3 ahead = xyz(b.x) + normalize(xyz(b.v) + 1e-9f) * (b.shape.z + 3.0f * hh);
+        float2 s = sample_pressure(D, g, (ahead - g.org) / hh - 0.5f, false);
+        s_pf = s.y > 1e-6f ? s.x / s.y : 0.0f;
+        V3 sn, sx;
+        for (int c = 0; c < 3; c++) {
+            sn[c] = from_fp(atomicExch(hit + 6 + c, 0), FP_A);
+            sx[c] = from_fp(atomicExch(hit + 9 + c, 0), FP_X);
+        }
+        float sa = from_fp(atomicExch(hit + 12, 0), FP_A);
+        s_side = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (sa > 0.0f && length(sn) > 0.0f) {
+            V3 n = normalize(sn);
+            s_side = make_float4(n.x, n.y, n.z, dot(sx, n) / sa * 1e-3f);
+        }
+    }
+    __syncthreads();
+    const uint32_t state = s_state;
+    if (state != 1u) {
+        if (li == 0) {
+            D.bullets[bi].info.z = state;
+            D.pose_log[(bi * NTR_LOG_CAP + st->s.step % NTR_LOG_CAP) * 3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        return;
+    }
+    const float pf = s_pf;
+    const float4 side = s_side;
+    V3 lb = qrot(make_float4(-b.q.x, -b.q.y, -b.q.z, b.q.w), xyz(b.l));
+    V3 w = qrot(b.q, lb / v3(b.shape.y, b.shape.y, b.shape.x));
+    const float rho = U->fluid[0];
+    const V3 vhat = normalize(xyz(b.v) + 1e-9f);
+    V3 f = {0.0f, 0.0f, 0.0f}, tq = {0.0f, 0.0f, 0.0f};
+    float cavx = 0.0f, cavy = 0.0f;
+    float4 cen = make_float4(0.0f, 0.0f, 0.0f, BIG_F);
+    for (uint32_t k = li; k < b.info.y; k += 256u) {
+        const float4 pp = D.patches[(bi * NTR_MAX_PATCHES + k) * 2], pn = D.patches[(bi * NTR_MAX_PATCHES + k) * 2 + 1];
+        V3 r = qrot(b.q, xyz(pp));
+        V3 p = xyz(b.x) + r;
+        V3 n = qrot(b.q, xyz(pn));
+        float area = pp.w;
+        V3 X = (p - g.org) / hh;
+        V3 uw, sw;
+        for (uint32_t d = 0; d < 3; d++) {
+            float2 s = sample_grid(D, g, X - lattice_offset(d), F_U + d, a_wt(d));
+            uw[d] = s.y > 1e-6f ? s.x / s.y : 0.0f;
+            sw[d] = s.y;
+        }
+        float fill = clampf_(sample_grid(D, g, X - 0.5f, F_TYPE, A_WC).y / 8.0f, 0.0f, 1.0f);
+        if (in_cavity(D, hh, bi, p, t_end - step) || dot(r, xyz(side)) > side.w) fill = 0.0f;
+        float2 gs = sample_pressure(D, g, X - 0.5f, true);
+        float p_gas = gs.y > 1e-6f ? gs.x / gs.y : 0.0f;
+        V3 vp = xyz(b.v) + cross(w, r);
+        V3 rel = vp - uw;
+        float spd = length(rel);
+        float wn = dot(rel, n);
+        float q = 0.5f * rho * spd * spd;
+        float p_water = mx(P_VAPOUR - P_ATM, pf + q * cp_patch(wn / mx(spd, 1e-9f)));
+        V3 fw = -fill * p_water * area * n;
+        V3 rt = rel - wn * n;
+        float rtl = length(rt);
+        if (rtl > 1e-9f) fw = fw - fill * CF_SKIN * 0.5f * rho * rtl * rt * area;
+        V3 fp = fw - (1.0f - fill) * mx(p_gas, P_VAPOUR - P_ATM) * area * n;
+        f = f + fp;
+        tq = tq + cross(r, fp);
+        for (uint32_t d = 0; d < 3; d++) push_water(D, g, X, d, -fw[d] * step, sw[d]);
+        if (wn > 0.0f && fill > 0.0f) {
+            float face = fill * area * mx(dot(n, vhat), 0.0f);
+            cavx = cavx + -dot(fw, vhat);
+            cavy = cavy + face;
+            V3 cx = v3(cen.x, cen.y, cen.z) + p * face;
+            cen = make_float4(cx.x, cx.y, cx.z, mn(cen.w, dot(r, vhat)));
+        }
+    }
+    red_f[li] = make_float4(f.x, f.y, f.z, cavx);
+    red_t[li] = make_float4(tq.x, tq.y, tq.z, cavy);
+    red_c[li] = cen;
+    __syncthreads();
+    for (uint32_t off = 128; off > 0; off >>= 1) {
+        if (li < off) {
+            float4 a = red_f[li], o = red_f[li + off];
+            red_f[li] = make_float4(a.x + o.x, a.y + o.y, a.z + o.z, a.w + o.w);
+            a = red_t[li], o = red_t[li + off];
+            red_t[li] = make_float4(a.x + o.x, a.y + o.y, a.z + o.z, a.w + o.w);
+            a = red_c[li], o = red_c[li + off];
+            red_c[li] = make_float4(a.x + o.x, a.y + o.y, a.z + o.z, mn(a.w, o.w));
+        }
+        __syncthreads();
+    }
+    const float hand2 = R_HAND * R_HAND * hh * hh;
+    if (li == 0) {
+        V3 hitv, hit_l;
+        for (int c = 0; c < 3; c++) {
+            hitv[c] = from_fp(atomicExch(hit + c, 0), FP_J);
+            hit_l[c] = from_fp(atomicExch(hit + 3 + c, 0), FP_L);
+        }
+        const float4 rf = red_f[0], rt4 = red_t[0], rc = red_c[0];
+        V3 force = xyz(rf) + b.x.w * v3(U->gravity[0], U->gravity[1], U->gravity[2]);
+        float drag = rf.w, face = rt4.w;
+        V3 v = xyz(b.v) + (force * step + hitv) / b.x.w;
+        V3 x = xyz(b.x) + v * step;
+        V3 l = xyz(b.l) + xyz(rt4) * step + hit_l;
+        V3 axis0 = qrot(b.q, v3(0.0f, 0.0f, 1.0f));
+        float spin_extra = dot(l, axis0) * (1.0f / b.shape.x - 1.0f / b.shape.y) * step;
+        float cone = length(l) / b.shape.y * step;
+        float4 q = qmul(b.q, make_float4(0.0f, 0.0f, nt_sin(0.5f * spin_extra), nt_cos(0.5f * spin_extra)));
+        if (cone > 1e-12f) {
+            V3 ln = normalize(l) * nt_sin(0.5f * cone);
+            q = qmul(make_float4(ln.x, ln.y, ln.z, nt_cos(0.5f * cone)), q);
+        }
+        q = normalize4(q);
+        float roll = b.v.w + dot(l, axis0) / b.shape.x * step;
+        uint4 info = b.info;
+        info.z = 1u;
+        V3 hi = g.org + v3((float)g.dims[0], (float)g.dims[1], (float)g.dims[2]) * hh;
+        if (x.x < g.org.x || x.y < g.org.y || x.z < g.org.z || x.x > hi.x || x.y > hi.y || x.z > hi.z) info.z = 2u;
+        I3 c = shr2(own_cell(g, x));
+        bool nearb = false;
+        for (uint32_t k = 0; k < 27; k++) {
+            I3 nb = c + I3{(int32_t)(k / 9u), (int32_t)((k / 3u) % 3u), (int32_t)(k % 3u)} - I3{1, 1, 1};
+            if (block_at(g, nb) != NONE) nearb = true;
+        }
+        float pace = nearb ? length(v) : length(v) * U->fluid[1] / 4.0f;
+        if (drag > 0.0f && face > 0.0f) {
+            V3 mid = xyz(rc) / face;
+            V3 a = mid + vhat * (rc.w - dot(mid - xyz(b.x), vhat));
+            DSection s;
+            s.a = f4(a, t_end - 0.5f * step);
+            s.b = f4(a + v * step, 2.0f * sqrtf(drag / (PI_F * rho * LOGVINOVICH_K)));
+            s.c = make_float4(face / PI_F, 0.0f, 0.0f, 0.0f);
+            D.sections[bi * NTR_N_SEC + info.w % NTR_N_SEC] = s;
+            info.w += 1u;
+        }
+        float reach = 0.0f;
+        for (uint32_t k = 0; k < NTR_N_SEC; k++) {
+            const DSection s = D.sections[bi * NTR_N_SEC + k];
+            if (s.b.w <= 0.0f || section_r2(s, t_end) >= hand2) continue;
+            reach = mx(reach, mx(length(xyz(s.a) - x), length(xyz(s.b) - x)));
+        }
+        DBullet& o = D.bullets[bi];
+        o.x = f4(x, b.x.w);
+        o.v = f4(v, roll);
+        o.q = q;
+        o.l = f4(l, pace);
+        o.reach = f4(x, reach > 0.0f ? reach + R_HAND * hh : 0.0f);
+        o.info = info;
+        float4* e = D.pose_log + (bi * NTR_LOG_CAP + st->s.step % NTR_LOG_CAP) * 3;
+        e[0] = f4(x, __uint_as_float(st->s.t_ns));
+        e[1] = q;
+        e[2] = f4(v, roll);
+    }
+    __syncthreads();
+    // Sections thinner than the grid push the water out of the way as they open.
+    if (li < NTR_N_SEC) {
+        const DSection s = D.sections[bi * NTR_N_SEC + li];
+        float r2 = section_r2(s, t_end);
+        if (s.b.w > 0.0f && r2 < hand2) {
+            float qv = PI_F * s.b.w * length(xyz(s.b) - xyz(s.a));
+            V3 xx = (0.5f * (xyz(s.a) + xyz(s.b)) - g.org) / hh - 0.5f;
+            I3 base = vi(vfloor(xx - 0.5f));
+            V3 fx = xx - vf(base);
+            V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
+            for (int a = 0; a < 3; a++)
+                for (int bb = 0; bb < 3; bb++)
+                    for (int cc = 0; cc < 3; cc++) {
+                        uint32_t cell = cell_at(g, base + I3{a, bb, cc});
+                        if (cell == NONE) continue;
+                        atomicAdd(accp(D, A_SRC, cell), to_fp(qv * wx[a] * wy[bb] * wz[cc], FP_Q));
+                    }
+        }
+    }
+}
+
+}  // namespace ntr

@@ -1,0 +1,1279 @@
+// Scene construction on the CPU: the balloon's latex, the shape it takes filled with water and
+// hanging from its knot, its mesh, the water particles, the bullets' bodies and surfaces, and
+// the initial world of a simulation.
+//
+// Restates src/balloon.rs (build, inflate, shoot, icosphere, spatial_order), src/bullet.rs
+// (outline, surface, hull, initial), src/flight.rs (Body::new, profile), src/params.rs and
+// src/presets.rs, and the setup half of Sim::new (src/sim.rs:208-441). Arithmetic keeps the
+// reference's types: f64 for the inflation and the bullets, f32 where the reference uses glam's
+// Vec3 (the icosphere and its ordering).
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <optional>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "world.hpp"
+
+namespace ntr {
+namespace {
+
+constexpr double PI = 3.14159265358979323846;
+constexpr double TAU = 2.0 * PI;
+
+// ---- small vector types with the reference's arithmetic order -----------------------------
+struct V3f {
+    float x, y, z;
+};
+static inline V3f operator+(V3f a, V3f b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline V3f operator-(V3f a, V3f b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+static inline V3f operator*(V3f a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+static inline V3f operator/(V3f a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+static inline float dot(V3f a, V3f b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline V3f cross(V3f a, V3f b) {
+    return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y};
+}
+static inline V3f normalize(V3f a) {
+    float r = 1.0f / std::sqrt(dot(a, a));
+    return a * r;
+}
+static inline V3f normalize_or(V3f a, V3f fb) {
+    float r = 1.0f / std::sqrt(dot(a, a));
+    if (std::isfinite(r) && r > 0.0f) return a * r;
+    return fb;
+}
+// Duff et al., "Building an Orthonormal Basis, Revisited" (JCGT 2017): the second vector of
+// the basis around a unit `n`.
+static inline V3f any_orthonormal(V3f n) {
+    float sign = std::copysign(1.0f, n.z);
+    float a = -1.0f / (sign + n.z);
+    float b = n.x * n.y * a;
+    return {b, sign + n.y * n.y * a, -n.y};
+}
+
+struct V3d {
+    double x, y, z;
+};
+static inline V3d operator+(V3d a, V3d b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline V3d operator-(V3d a, V3d b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+static inline V3d operator*(V3d a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+static inline double dot(V3d a, V3d b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline V3d cross(V3d a, V3d b) {
+    return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y};
+}
+static inline double length(V3d a) { return std::sqrt(dot(a, a)); }
+static inline V3d normalize(V3d a) {
+    double r = 1.0 / std::sqrt(dot(a, a));
+    return a * r;
+}
+static inline V3d widen(V3f a) { return {a.x, a.y, a.z}; }
+
+// ---- latex (src/balloon.rs:13-71) --------------------------------------------------------
+constexpr double RHO_WATER = 1000.0;
+constexpr double RHO_RUBBER = 950.0;
+constexpr double OGDEN_MU[3] = {0.63e6, 0.0012e6, -0.01e6};
+constexpr double OGDEN_AL[3] = {1.3, 5.0, -2.0};
+constexpr double NECK = 0.25;
+
+struct Latex {
+    double mu[3];
+    double thickness;
+    Latex(double shear, double thick) : thickness(thick) {
+        double g0 = 0.0;
+        for (int i = 0; i < 3; i++) g0 += OGDEN_MU[i] * OGDEN_AL[i];
+        g0 /= 2.0;
+        for (int i = 0; i < 3; i++) mu[i] = OGDEN_MU[i] * shear / g0;
+    }
+    double sigma(double a, double b) const {
+        double s = 0.0;
+        for (int i = 0; i < 3; i++) s += mu[i] * (std::pow(a, OGDEN_AL[i]) - std::pow(b, OGDEN_AL[i]));
+        return s;
+    }
+    std::pair<double, double> stress(double l1, double l2) const {
+        double major = std::max(l1, l2), minor = std::min(l1, l2);
+        if (major <= 1.0) return {0.0, 0.0};
+        double natural = std::pow(major, -0.5);
+        if (minor < natural) {
+            double s = sigma(major, natural);
+            return l1 >= l2 ? std::make_pair(s, 0.0) : std::make_pair(0.0, s);
+        }
+        double l3 = 1.0 / (l1 * l2);
+        return {sigma(l1, l3), sigma(l2, l3)};
+    }
+    std::pair<double, double> tension(double l1, double l2) const {
+        auto s = stress(l1, l2);
+        double t = thickness / (l1 * l2);
+        return {s.first * t, s.second * t};
+    }
+};
+
+// ---- inflation (src/balloon.rs:73-248) ---------------------------------------------------
+struct Sample {
+    double angle, r, z;
+};
+struct Profile {
+    std::vector<Sample> samples;
+    double neck_angle = 0, z_neck = 0, neck_r = 0, volume = 0, z_centroid = 0, stretch = 0;
+    double z_top() const { return z_neck; }
+    double r_at(double z) const {
+        const auto& s = samples;
+        if (z <= 0.0 || z >= z_neck) return 0.0;
+        size_t i = std::partition_point(s.begin(), s.end(), [&](const Sample& p) { return p.z < z; }) - s.begin();
+        i = std::clamp<size_t>(i, 1, s.size() - 1);
+        const Sample &a = s[i - 1], &b = s[i];
+        return a.r + (b.r - a.r) * (z - a.z) / std::max(b.z - a.z, 1e-15);
+    }
+    std::pair<double, double> place(double angle) const {
+        const auto& s = samples;
+        size_t i = std::partition_point(s.begin(), s.end(), [&](const Sample& p) { return p.angle < angle; }) - s.begin();
+        i = std::clamp<size_t>(i, 1, s.size() - 1);
+        const Sample &a = s[i - 1], &b = s[i];
+        double f = std::clamp((angle - a.angle) / (b.angle - a.angle), 0.0, 1.0);
+        return {a.r + (b.r - a.r) * f, a.z + (b.z - a.z) * f};
+    }
+};
+
+constexpr int SHOOT_STEPS = 400;
+using Y5 = std::array<double, 5>;
+
+struct ShotResult {
+    std::vector<Sample> samples;
+    double volume;
+};
+
+std::optional<ShotResult> shoot(const Latex& latex, double rest_r, double apex_stretch, double apex_curv, double rho_g) {
+    const double neck_angle = PI - std::asin(NECK);
+    const double p_apex = 2.0 * latex.tension(apex_stretch, apex_stretch).first * apex_curv;
+    auto deriv = [&](double th, const Y5& y) -> std::optional<Y5> {
+        double r = y[0], z = y[1], psi = y[2], l1 = y[3];
+        double rr = rest_r * std::sin(th);
+        double l2 = r / rr;
+        if (!(r > 0.0 && l1 > 0.0)) return std::nullopt;
+        auto t = latex.tension(l1, l2);
+        double t1 = t.first, t2 = t.second;
+        if (t1 <= 0.0) return std::nullopt;
+        double e = 1e-6;
+        double t1_l1 = (latex.tension(l1 * (1.0 + e), l2).first - latex.tension(l1 * (1.0 - e), l2).first) / (2.0 * e * l1);
+        double t1_l2 = (latex.tension(l1, l2 * (1.0 + e)).first - latex.tension(l1, l2 * (1.0 - e)).first) / (2.0 * e * l2);
+        double p = p_apex - rho_g * z;
+        double dr = l1 * std::cos(psi);
+        double dz = l1 * std::sin(psi);
+        double dpsi = l1 * (p - t2 * std::sin(psi) / r) / t1;
+        double dl2 = (dr - l2 * std::cos(th)) / rr;
+        double dl1 = (dr * (t2 - t1) - r * t1_l2 * dl2) / (r * t1_l1);
+        Y5 d = {dr, dz, dpsi, dl1, PI * r * r * dz};
+        for (auto& v : d) v = v * rest_r;
+        return d;
+    };
+    const double th0 = 1e-3;
+    double r = apex_stretch * rest_r * std::sin(th0);
+    Y5 y = {r, 0.5 * apex_curv * r * r, apex_curv * r, apex_stretch, 0.0};
+    double h = (neck_angle - th0) / SHOOT_STEPS;
+    double th = th0;
+    ShotResult out;
+    out.samples.reserve(SHOOT_STEPS + 2);
+    out.samples.push_back({0.0, 0.0, 0.0});
+    out.samples.push_back({th, y[0], y[1]});
+    auto add = [](const Y5& a, const Y5& k, double s) {
+        Y5 o;
+        for (int i = 0; i < 5; i++) o[i] = a[i] + s * k[i];
+        return o;
+    };
+    for (int it = 0; it < SHOOT_STEPS; it++) {
+        auto k1 = deriv(th, y);
+        if (!k1) return std::nullopt;
+        auto k2 = deriv(th + 0.5 * h, add(y, *k1, 0.5 * h));
+        if (!k2) return std::nullopt;
+        auto k3 = deriv(th + 0.5 * h, add(y, *k2, 0.5 * h));
+        if (!k3) return std::nullopt;
+        auto k4 = deriv(th + h, add(y, *k3, h));
+        if (!k4) return std::nullopt;
+        Y5 n;
+        for (int i = 0; i < 5; i++) n[i] = y[i] + h / 6.0 * ((*k1)[i] + 2.0 * (*k2)[i] + 2.0 * (*k3)[i] + (*k4)[i]);
+        y = n;
+        th += h;
+        if (y[0] <= 0.0 || y[2] > 3.5) return std::nullopt;
+        out.samples.push_back({th, y[0], y[1]});
+    }
+    out.volume = y[4];
+    return out;
+}
+
+bool inflate(const Latex& latex, double rest_r, double volume, double rho_g, Profile& prof, std::string& err) {
+    const double neck_r = NECK * rest_r;
+    auto miss = [&](std::array<double, 2> x, double target) -> std::optional<std::array<double, 2>> {
+        auto s = shoot(latex, rest_r, x[0], std::exp(x[1]), rho_g);
+        if (!s) return std::nullopt;
+        return std::array<double, 2>{(s->samples.back().r - neck_r) / neck_r, std::log(s->volume) - target};
+    };
+    const double la0 = 1.2;
+    double lo = std::log(1e-3 / rest_r), hi = std::log(1e3 / rest_r);
+    for (int i = 0; i < 60; i++) {
+        double mid = 0.5 * (lo + hi);
+        auto s = shoot(latex, rest_r, la0, std::exp(mid), rho_g);
+        if (s && s->samples.back().r > neck_r)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    std::array<double, 2> x = {la0, lo};
+    auto s0 = shoot(latex, rest_r, x[0], std::exp(x[1]), rho_g);
+    if (!s0) {
+        err = "balloon doesn't inflate";
+        return false;
+    }
+    double v = std::log(s0->volume);
+    std::array<double, 2> prev = x;
+    size_t n_inc = (size_t)std::max(std::ceil(std::fabs(std::log(volume) - v) / 0.05), 1.0);
+    double inc = (std::log(volume) - v) / (double)n_inc;
+    for (size_t step = 0; step < n_inc; step++) {
+        double target = v + inc;
+        std::array<double, 2> y = step > 0 ? std::array<double, 2>{2.0 * x[0] - prev[0], 2.0 * x[1] - prev[1]} : x;
+        bool done = false;
+        for (int it = 0; it < 30; it++) {
+            auto f = miss(y, target);
+            if (!f) break;
+            double norm = std::hypot((*f)[0], (*f)[1]);
+            if (norm < 1e-9) {
+                done = true;
+                break;
+            }
+            double e = 1e-6;
+            auto fa = miss({y[0] + e, y[1]}, target);
+            auto fb = miss({y[0], y[1] + e}, target);
+            if (!fa || !fb) break;
+            double j00 = ((*fa)[0] - (*f)[0]) / e, j01 = ((*fb)[0] - (*f)[0]) / e;
+            double j10 = ((*fa)[1] - (*f)[1]) / e, j11 = ((*fb)[1] - (*f)[1]) / e;
+            double det = j00 * j11 - j01 * j10;
+            double d0 = (-(*f)[0] * j11 + (*f)[1] * j01) / det;
+            double d1 = (-(*f)[1] * j00 + (*f)[0] * j10) / det;
+            double a = 1.0;
+            while (a > 1e-4) {
+                std::array<double, 2> c = {y[0] + a * d0, y[1] + a * d1};
+                auto g = miss(c, target);
+                if (g && std::hypot((*g)[0], (*g)[1]) < norm) {
+                    y = c;
+                    break;
+                }
+                a *= 0.5;
+            }
+        }
+        if (!done) {
+            char buf[128];
+            snprintf(buf, sizeof buf, "the balloon shape didn't converge at %.3f L", std::exp(target) * 1e3);
+            err = buf;
+            return false;
+        }
+        prev = x;
+        x = y;
+        v = target;
+    }
+    auto fin = shoot(latex, rest_r, x[0], std::exp(x[1]), rho_g);
+    if (!fin) {
+        err = "final balloon shape failed";
+        return false;
+    }
+    double zmom = 0.0;
+    const auto& smp = fin->samples;
+    for (size_t i = 0; i + 1 < smp.size(); i++) {
+        const Sample &a = smp[i], &b = smp[i + 1];
+        zmom += PI * 0.5 * (a.r * a.r + b.r * b.r) * (b.z - a.z) * 0.5 * (a.z + b.z);
+    }
+    double stretch = 0.0;
+    for (size_t i = 1; i < smp.size(); i++) stretch = std::max(stretch, smp[i].r / std::max(rest_r * std::sin(smp[i].angle), 1e-12));
+    prof.samples = smp;
+    prof.neck_angle = smp.back().angle;
+    prof.z_neck = smp.back().z;
+    prof.neck_r = neck_r;
+    prof.volume = fin->volume;
+    prof.z_centroid = zmom / fin->volume;
+    prof.stretch = stretch;
+    return true;
+}
+
+// ---- mesh (src/balloon.rs:250-322) -------------------------------------------------------
+struct Rng {
+    uint64_t s;
+    double next() {
+        s ^= s << 13;
+        s ^= s >> 7;
+        s ^= s << 17;
+        return (double)(s >> 11) / (double)(1ull << 53);
+    }
+};
+
+void icosphere(uint32_t level, std::vector<V3f>& v, std::vector<std::array<uint32_t, 3>>& f) {
+    const float t = (1.0f + std::sqrt(5.0f)) / 2.0f;
+    const float base[12][3] = {{-1, t, 0}, {1, t, 0}, {-1, -t, 0}, {1, -t, 0}, {0, -1, t}, {0, 1, t},
+                               {0, -1, -t}, {0, 1, -t}, {t, 0, -1}, {t, 0, 1}, {-t, 0, -1}, {-t, 0, 1}};
+    v.clear();
+    for (auto& b : base) v.push_back(normalize(V3f{b[0], b[1], b[2]}));
+    f = {{0, 11, 5}, {0, 5, 1}, {0, 1, 7}, {0, 7, 10}, {0, 10, 11}, {1, 5, 9}, {5, 11, 4},
+         {11, 10, 2}, {10, 7, 6}, {7, 1, 8}, {3, 9, 4}, {3, 4, 2}, {3, 2, 6}, {3, 6, 8},
+         {3, 8, 9}, {4, 9, 5}, {2, 4, 11}, {6, 2, 10}, {8, 6, 7}, {9, 8, 1}};
+    for (uint32_t l = 0; l < level; l++) {
+        std::map<std::pair<uint32_t, uint32_t>, uint32_t> cache;
+        auto mid = [&](uint32_t a, uint32_t b) -> uint32_t {
+            auto key = std::make_pair(std::min(a, b), std::max(a, b));
+            auto it = cache.find(key);
+            if (it != cache.end()) return it->second;
+            v.push_back(normalize((v[a] + v[b]) * 0.5f));
+            uint32_t idx = (uint32_t)v.size() - 1;
+            cache.emplace(key, idx);
+            return idx;
+        };
+        std::vector<std::array<uint32_t, 3>> nf;
+        nf.reserve(f.size() * 4);
+        for (auto& tri : f) {
+            uint32_t a = tri[0], b = tri[1], c = tri[2];
+            uint32_t ab = mid(a, b);
+            uint32_t bc = mid(b, c);
+            uint32_t ca = mid(c, a);
+            nf.push_back({a, ab, ca});
+            nf.push_back({b, bc, ab});
+            nf.push_back({c, ca, bc});
+            nf.push_back({ab, bc, ca});
+        }
+        f.swap(nf);
+    }
+}
+
+static inline uint32_t spread10(uint32_t x) {
+    x &= 0x3ff;
+    x = (x | (x << 16)) & 0x030000ff;
+    x = (x | (x << 8)) & 0x0300f00f;
+    x = (x | (x << 4)) & 0x030c30c3;
+    return (x | (x << 2)) & 0x09249249;
+}
+static inline uint32_t sat_u32(float f) {
+    // Rust's `as u32` saturates and maps NaN to 0.
+    if (!(f > 0.0f)) return 0;
+    if (f >= 4294967296.0f) return 0xffffffffu;
+    return (uint32_t)f;
+}
+static inline uint32_t morton_key(V3f p) {
+    V3f q = (p * 0.5f + V3f{0.5f, 0.5f, 0.5f}) * 1023.0f;
+    return spread10(sat_u32(q.x)) | spread10(sat_u32(q.y)) << 1 | spread10(sat_u32(q.z)) << 2;
+}
+
+void spatial_order(std::vector<V3f>& v, std::vector<std::array<uint32_t, 3>>& f) {
+    std::vector<uint32_t> order(v.size());
+    for (uint32_t i = 0; i < v.size(); i++) order[i] = i;
+    std::vector<uint32_t> keys(v.size());
+    for (size_t i = 0; i < v.size(); i++) keys[i] = morton_key(v[i]);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return keys[a] < keys[b]; });
+    std::vector<uint32_t> new_index(v.size());
+    for (uint32_t n = 0; n < order.size(); n++) new_index[order[n]] = n;
+    std::vector<V3f> nv(v.size());
+    for (size_t n = 0; n < order.size(); n++) nv[n] = v[order[n]];
+    v.swap(nv);
+    for (auto& t : f)
+        for (auto& i : t) i = new_index[i];
+    std::vector<uint32_t> fk(f.size());
+    for (size_t i = 0; i < f.size(); i++) fk[i] = morton_key((v[f[i][0]] + v[f[i][1]] + v[f[i][2]]) / 3.0f);
+    std::vector<uint32_t> fo(f.size());
+    for (uint32_t i = 0; i < f.size(); i++) fo[i] = i;
+    std::stable_sort(fo.begin(), fo.end(), [&](uint32_t a, uint32_t b) { return fk[a] < fk[b]; });
+    std::vector<std::array<uint32_t, 3>> nf(f.size());
+    for (size_t i = 0; i < fo.size(); i++) nf[i] = f[fo[i]];
+    f.swap(nf);
+}
+
+struct GpuTri {
+    uint32_t v[3];
+    float rest_area;
+    float dm_inv[4];
+};
+static_assert(sizeof(GpuTri) == 32, "GpuTri is 32 bytes");
+
+struct Balloon {
+    Profile profile;
+    Latex latex{1, 1};
+    double bottom_y = 0;
+    V3f center{};
+    V3f knot{};
+    double radius_max = 0;
+    double spacing = 0;
+    std::vector<std::array<float, 4>> particles;
+    std::vector<std::array<float, 4>> mem_pos;
+    std::vector<float> mem_mass;
+    std::vector<GpuTri> tris;
+    std::vector<uint32_t> vtri_off, vtri;
+
+    // Where a straight line through `aim` along `dir` first meets the undisturbed balloon,
+    // src/balloon.rs:466-477.
+    std::optional<V3f> entry(V3f aim, V3f dir) const {
+        auto inside = [&](double s) {
+            V3f q = aim + dir * (float)s;
+            return std::hypot((double)q.x, (double)q.z) < profile.r_at((double)q.y - bottom_y);
+        };
+        double reach = 1.5 * (radius_max + profile.z_top());
+        const int steps = 8000;
+        for (int i = 0; i <= steps; i++) {
+            double s = -reach + 2.0 * reach * (double)i / (double)steps;
+            if (inside(s)) return aim + dir * (float)s;
+        }
+        return std::nullopt;
+    }
+};
+
+static uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+bool build_balloon(const ntr_sim_params& p, Balloon& out, std::string& err) {
+    double d = (double)p.balloon_diameter_cm * 0.01;
+    double volume = PI / 6.0 * d * d * d;
+    double t0 = (double)p.rubber_thickness_mm * 1e-3;
+    Latex latex((double)p.rubber_modulus_mpa * 1e6, t0);
+    double rest_r = (double)p.rubber_rest_diameter_cm * 0.005;
+    Profile profile;
+    if (!inflate(latex, rest_r, volume, RHO_WATER * (double)std::max(p.gravity, 0.0f), profile, err)) return false;
+    double bottom_y = (double)p.balloon_height - profile.z_centroid;
+    double radius_max = 0.0;
+    for (auto& q : profile.samples) radius_max = std::max(radius_max, q.r);
+    V3f center{0.0f, p.balloon_height, 0.0f};
+    V3f knot{0.0f, (float)(bottom_y + profile.z_neck + 0.5 * profile.neck_r), 0.0f};
+
+    std::vector<V3f> sphere;
+    std::vector<std::array<uint32_t, 3>> faces;
+    icosphere(p.mesh_level, sphere, faces);
+    spatial_order(sphere, faces);
+    Rng rng{p.seed == 0 ? 0x9E3779B97F4A7C15ull : splitmix64(p.seed)};
+    if (rng.s == 0) rng.s = 0x9E3779B97F4A7C15ull;
+    const float edge_angle = 1.1f / (float)(1u << p.mesh_level);
+    std::vector<V3d> rest;
+    std::vector<V3f> pos;
+    std::vector<bool> held;
+    rest.reserve(sphere.size());
+    pos.reserve(sphere.size());
+    for (const V3f& s : sphere) {
+        V3f t1 = any_orthonormal(s);
+        V3f t2 = cross(s, t1);
+        float r1 = (float)rng.next() - 0.5f;
+        V3f a = t1 * r1;
+        float r2 = (float)rng.next() - 0.5f;
+        V3f b = t2 * r2;
+        V3f j = ((a + b) * edge_angle) * 0.4f;
+        V3d dir = widen(normalize(s + j));
+        rest.push_back(dir * rest_r);
+        double angle = std::acos(std::clamp(-dir.y, -1.0, 1.0));
+        double az = std::atan2(dir.z, dir.x);
+        double r, z;
+        if (angle <= profile.neck_angle) {
+            auto pl = profile.place(angle);
+            r = pl.first;
+            z = pl.second;
+        } else {
+            double f = (angle - profile.neck_angle) / (PI - profile.neck_angle);
+            r = profile.neck_r * (1.0 - f);
+            z = profile.z_neck + 0.5 * profile.neck_r * f;
+        }
+        held.push_back(angle > profile.neck_angle);
+        pos.push_back({(float)(r * std::cos(az)), (float)(bottom_y + z), (float)(r * std::sin(az))});
+    }
+
+    std::vector<double> vmass(pos.size(), 0.0);
+    std::vector<GpuTri> tris;
+    tris.reserve(faces.size());
+    for (auto& f : faces) {
+        {
+            V3d a = rest[f[0]], b = rest[f[1]], c = rest[f[2]];
+            if (dot(cross(b - a, c - a), a + b + c) < 0.0) std::swap(f[1], f[2]);
+        }
+        V3d a = rest[f[0]], b = rest[f[1]], c = rest[f[2]];
+        V3d e1 = b - a, e2 = c - a;
+        V3d u = normalize(e1);
+        V3d w = cross(normalize(cross(e1, e2)), u);
+        double m00 = dot(e1, u), m01 = dot(e2, u), m10 = dot(e1, w), m11 = dot(e2, w);
+        double det = m00 * m11 - m01 * m10;
+        double area = 0.5 * std::fabs(det);
+        for (uint32_t vi : f) vmass[vi] += RHO_RUBBER * t0 * area / 3.0;
+        GpuTri t;
+        t.v[0] = f[0];
+        t.v[1] = f[1];
+        t.v[2] = f[2];
+        t.rest_area = (float)area;
+        t.dm_inv[0] = (float)(m11 / det);
+        t.dm_inv[1] = (float)(-m01 / det);
+        t.dm_inv[2] = (float)(-m10 / det);
+        t.dm_inv[3] = (float)(m00 / det);
+        tris.push_back(t);
+    }
+    out.mem_mass.resize(pos.size());
+    for (size_t i = 0; i < pos.size(); i++) out.mem_mass[i] = held[i] ? 0.0f : (float)vmass[i];
+    out.mem_pos.resize(pos.size());
+    for (size_t i = 0; i < pos.size(); i++) out.mem_pos[i] = {pos[i].x, pos[i].y, pos[i].z, 0.0f};
+
+    std::vector<std::vector<uint32_t>> vt(pos.size());
+    for (uint32_t ti = 0; ti < tris.size(); ti++)
+        for (uint32_t k = 0; k < 3; k++) vt[tris[ti].v[k]].push_back(ti);
+    out.vtri_off.assign(1, 0u);
+    out.vtri.clear();
+    for (auto& l : vt) {
+        out.vtri.insert(out.vtri.end(), l.begin(), l.end());
+        out.vtri_off.push_back((uint32_t)out.vtri.size());
+    }
+
+    // Water particles fill the membrane on a jittered lattice, src/balloon.rs:419-445.
+    double spacing = d / (double)std::max<uint32_t>(p.resolution, 16);
+    int n = (int)std::ceil(2.0 * radius_max / spacing) + 2;
+    int nz = (int)std::ceil(profile.z_neck / spacing) + 1;
+    out.particles.clear();
+    for (int iy = 0; iy < nz; iy++) {
+        double zl = ((double)iy + 0.5) * spacing;
+        if (zl > profile.z_neck - spacing) break;
+        double rmax = profile.r_at(zl) - 0.5 * spacing;
+        if (rmax <= 0.0) continue;
+        for (int ix = -n / 2; ix <= n / 2; ix++) {
+            for (int iz = -n / 2; iz <= n / 2; iz++) {
+                double x = ((double)ix + 0.5 * (double)(iy % 2)) * spacing;
+                double z = ((double)iz + 0.5 * (double)(iy % 2)) * spacing;
+                double jx = (rng.next() - 0.5) * 0.3 * spacing;
+                double jy = (rng.next() - 0.5) * 0.3 * spacing;
+                double jz = (rng.next() - 0.5) * 0.3 * spacing;
+                if (std::sqrt(x * x + z * z) < rmax)
+                    out.particles.push_back({(float)(x + jx), (float)(bottom_y + zl + jy), (float)(z + jz), 1.0f});
+            }
+        }
+    }
+    out.profile = std::move(profile);
+    out.latex = latex;
+    out.bottom_y = bottom_y;
+    out.center = center;
+    out.knot = knot;
+    out.radius_max = radius_max;
+    out.spacing = spacing;
+    out.tris = std::move(tris);
+    return true;
+}
+
+// ---- bullets (src/params.rs:155-201, src/flight.rs:41-192, src/bullet.rs) ----------------
+enum Nose { ROUND, SPITZER, FLAT, SPHERE };
+enum Metal { LEAD, COPPER, STEEL };
+struct BulletType {
+    const char* name;
+    float caliber_mm, mass_g, speed, twist_in;
+    Nose nose;
+    Metal metal;
+    float spin_rpm() const { return twist_in <= 0.0f ? 0.0f : speed / (twist_in * 0.0254f) * 60.0f; }
+};
+const BulletType BULLETS[7] = {
+    {".22 LR, 40 gr lead round nose", 5.7f, 2.59f, 330.0f, 16.0f, ROUND, LEAD},
+    {"9 mm Luger, 115 gr FMJ", 9.0f, 7.45f, 360.0f, 10.0f, ROUND, COPPER},
+    {".45 ACP, 230 gr FMJ", 11.5f, 14.9f, 255.0f, 16.0f, ROUND, COPPER},
+    {"5.56 NATO, 62 gr M855", 5.7f, 4.0f, 940.0f, 7.0f, SPITZER, COPPER},
+    {".308 Win, 150 gr spitzer", 7.8f, 9.72f, 860.0f, 10.0f, SPITZER, COPPER},
+    {".177 air rifle, 8.4 gr wadcutter", 4.5f, 0.54f, 240.0f, 16.0f, FLAT, LEAD},
+    {".177 steel BB", 4.4f, 0.34f, 150.0f, 0.0f, SPHERE, STEEL},
+};
+
+double body_share(Nose n) { return n == ROUND ? 0.55 : n == SPITZER ? 0.42 : 1.0; }
+
+double profile_r(Nose nose, double r, double len, double u) {
+    if (nose == SPHERE) return std::sqrt(std::max(r * r - (u - r) * (u - r), 0.0));
+    double body = body_share(nose) * len;
+    if (u <= body) return r;
+    double x = u - body, nl = len - body;
+    if (nose == SPITZER) {
+        double ro = (r * r + nl * nl) / (2.0 * r);
+        return std::max(std::sqrt(std::max(ro * ro - x * x, 0.0)) - (ro - r), 0.0);
+    }
+    double q = x / nl;
+    return r * std::sqrt(std::max(1.0 - q * q, 0.0));
+}
+
+struct Body {
+    Nose nose;
+    double radius, length, mass, u_cg, ix, iy;
+};
+
+Body body_new(const ntr_shot& s) {
+    Body b;
+    b.nose = BULLETS[s.bullet].nose;
+    Metal metal = BULLETS[s.bullet].metal;
+    double r = 0.5 * (double)s.caliber_mm * 1e-3;
+    double mass = (double)s.mass_g * 1e-3;
+    double density = metal == LEAD ? 11340.0 : metal == COPPER ? 10500.0 : 7850.0;
+    double fill = b.nose == ROUND ? 0.85 : b.nose == SPITZER ? 0.72 : b.nose == FLAT ? 0.95 : 1.0;
+    double length = b.nose == SPHERE ? 2.0 * r : mass / density / (PI * r * r) / fill;
+    const int fine = 2000;
+    double du = length / fine;
+    double vol = 0.0, mom = 0.0;
+    std::vector<std::pair<double, double>> rad(fine);
+    for (int i = 0; i < fine; i++) {
+        double u = ((double)i + 0.5) * du;
+        rad[i] = {u, profile_r(b.nose, r, length, u)};
+    }
+    for (auto& q : rad) vol += PI * q.second * q.second * du;
+    for (auto& q : rad) mom += PI * q.second * q.second * du * q.first;
+    double u_cg = mom / vol;
+    double rho = mass / vol;
+    double ix = 0.0, iy = 0.0;
+    for (auto& q : rad) {
+        double r2 = q.second * q.second;
+        ix += rho * PI * (r2 * r2) / 2.0 * du;
+    }
+    for (auto& q : rad) {
+        double dd = q.first - u_cg;
+        iy += rho * PI * q.second * q.second * du * (q.second * q.second / 4.0 + dd * dd);
+    }
+    b.radius = r;
+    b.length = length;
+    b.mass = mass;
+    b.u_cg = u_cg;
+    b.ix = ix;
+    b.iy = iy;
+    return b;
+}
+
+constexpr int SLICES = 32;
+constexpr int SECTORS = 16;
+
+std::vector<std::pair<double, double>> outline(const Body& b) {
+    const int fine = 4000;
+    std::vector<std::pair<double, double>> line(fine + 1);
+    for (int i = 0; i <= fine; i++) {
+        double u = b.length * (double)i / (double)fine;
+        line[i] = {u, profile_r(b.nose, b.radius, b.length, u)};
+    }
+    std::vector<double> s(1, 0.0);
+    for (int i = 0; i < fine; i++) s.push_back(s.back() + std::hypot(line[i + 1].first - line[i].first, line[i + 1].second - line[i].second));
+    double total = s.back();
+    std::vector<std::pair<double, double>> out;
+    for (int k = 0; k <= SLICES; k++) {
+        double target = total * (double)k / (double)SLICES;
+        size_t i = std::partition_point(s.begin(), s.end(), [&](double x) { return x < target; }) - s.begin();
+        i = std::clamp<size_t>(i, 1, fine);
+        double f = (target - s[i - 1]) / std::max(s[i] - s[i - 1], 1e-15);
+        auto a = line[i - 1], c = line[i];
+        out.push_back({a.first + (c.first - a.first) * f, a.second + (c.second - a.second) * f});
+    }
+    return out;
+}
+
+struct Patch {
+    float p[4];
+    float n[4];
+};
+
+std::vector<Patch> surface(const Body& b) {
+    std::vector<Patch> out;
+    auto ring = [&](double u, double r, double radial, double axial, double area) {
+        for (int j = 0; j < SECTORS; j++) {
+            double phi = ((double)j + 0.5) * TAU / (double)SECTORS;
+            double c = std::cos(phi), sn = std::sin(phi);
+            Patch pt;
+            pt.p[0] = (float)(r * c);
+            pt.p[1] = (float)(r * sn);
+            pt.p[2] = (float)(u - b.u_cg);
+            pt.p[3] = (float)(area / (double)SECTORS);
+            pt.n[0] = (float)(radial * c);
+            pt.n[1] = (float)(radial * sn);
+            pt.n[2] = (float)axial;
+            pt.n[3] = 0.0f;
+            out.push_back(pt);
+        }
+    };
+    auto ol = outline(b);
+    for (size_t i = 0; i + 1 < ol.size(); i++) {
+        double ua = ol[i].first, ra = ol[i].second, ub = ol[i + 1].first, rb = ol[i + 1].second;
+        double len = std::hypot(ub - ua, rb - ra);
+        if (len <= 0.0) continue;
+        double r = 0.5 * (ra + rb);
+        ring(0.5 * (ua + ub), r, (ub - ua) / len, -(rb - ra) / len, TAU * r * len);
+    }
+    const double ends[2][2] = {{0.0, -1.0}, {b.length, 1.0}};
+    for (auto& e : ends) {
+        double r = profile_r(b.nose, b.radius, b.length, e[0]);
+        if (r > 1e-9) ring(e[0], 2.0 / 3.0 * r, 0.0, e[1], PI * r * r);
+    }
+    return out;
+}
+
+double hull(const Body& b) {
+    double m = 0.0;
+    for (auto& q : outline(b)) m = std::max(m, std::hypot(q.first - b.u_cg, q.second));
+    return m;
+}
+
+// Body-to-world rotation taking +z onto `n`: the half-way quaternion (cross, 1 + dot),
+// normalised, with the two singular cases of glam's DQuat::from_rotation_arc.
+std::array<double, 4> rotation_arc_z(V3d n) {
+    const V3d from{0, 0, 1};
+    double one_minus_eps = 1.0 - 2.0 * 2.220446049250313e-16;
+    double d = dot(from, n);
+    if (d > one_minus_eps) return {0, 0, 0, 1};
+    if (d < -one_minus_eps) {
+        // Half a turn about the orthonormal vector Duff et al. give for +z: (0, 1, -0).
+        double s = std::sin(PI * 0.5), c = std::cos(PI * 0.5);
+        return {0.0 * s, 1.0 * s, -0.0 * s, c};
+    }
+    V3d c = cross(from, n);
+    double q[4] = {c.x, c.y, c.z, 1.0 + d};
+    double len = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    double inv = 1.0 / len;
+    return {q[0] * inv, q[1] * inv, q[2] * inv, q[3] * inv};
+}
+
+constexpr double LOOKAHEAD = 0.05;
+
+// The hand-over from the flight through the air, straight-line form: the bullet arrives
+// along the aim with its shot speed and the muzzle spin, its tip LOOKAHEAD short of where the
+// line meets the balloon (Flight::new, src/flight.rs:408-470, without the 6-DOF air drag).
+struct Handoff {
+    V3d x, u, n, h;
+    double roll;
+    double t_read;
+    double v_impact;
+};
+
+Handoff straight_handoff(const ntr_shot& s, const Body& b, V3d target, V3d dir, double t_hit) {
+    Handoff o;
+    double v_hit = std::max((double)s.speed, 1.0);
+    double p0 = (double)s.spin_rpm / 60.0 * TAU;
+    o.n = dir;
+    o.x = target - dir * LOOKAHEAD - dir * (b.length - b.u_cg);
+    o.u = dir * v_hit;
+    o.h = dir * (b.ix * p0);
+    o.roll = 0.0;
+    o.t_read = t_hit - LOOKAHEAD / v_hit;
+    o.v_impact = v_hit;
+    return o;
+}
+
+struct GpuBullet {
+    float x[4], v[4], q[4], l[4], shape[4], reach[4];
+    uint32_t info[4];
+};
+static_assert(sizeof(GpuBullet) == 112, "Bullet is 112 bytes");
+
+}  // namespace
+
+bool inflate_profile(double shear, double thick, double rest_r, double volume, double rho_g, ntr_profile& out, std::string& err) {
+    Latex latex(shear, thick);
+    Profile prof;
+    if (!inflate(latex, rest_r, volume, rho_g, prof, err)) return false;
+    std::memset(&out, 0, sizeof out);
+    out.n_samples = (uint32_t)std::min<size_t>(prof.samples.size(), NTR_PROFILE_SAMPLES);
+    out.neck_angle = prof.neck_angle;
+    out.z_neck = prof.z_neck;
+    out.neck_r = prof.neck_r;
+    out.volume = prof.volume;
+    out.z_centroid = prof.z_centroid;
+    out.stretch = prof.stretch;
+    for (auto& s : prof.samples) out.r_max = std::max(out.r_max, s.r);
+    for (uint32_t i = 0; i < out.n_samples; i++) {
+        out.samples[i][0] = prof.samples[i].angle;
+        out.samples[i][1] = prof.samples[i].r;
+        out.samples[i][2] = prof.samples[i].z;
+    }
+    return true;
+}
+
+// ---- params (src/params.rs, src/presets.rs) ---------------------------------------------
+static void shot_set_bullet(ntr_shot& s, uint32_t k) {
+    const BulletType& b = BULLETS[k];
+    s.bullet = k;
+    s.caliber_mm = b.caliber_mm;
+    s.mass_g = b.mass_g;
+    s.speed = b.speed;
+    s.spin_rpm = b.spin_rpm();
+}
+
+static ntr_shot shot_default() {
+    ntr_shot s{};
+    shot_set_bullet(s, 0);
+    s.range_m = 10.0f;
+    s.muzzle_yaw_deg = 0.5f;
+    return s;
+}
+
+void params_default(ntr_sim_params& p) {
+    std::memset(&p, 0, sizeof p);
+    p.n_shots = 1;
+    p.shots[0] = shot_default();
+    p.balloon_diameter_cm = 16.0f;
+    p.balloon_height = 0.55f;
+    p.rubber_modulus_mpa = 0.42f;
+    p.rubber_rest_diameter_cm = 6.0f;
+    p.rubber_break_stretch = 7.0f;
+    p.rubber_thickness_mm = 0.25f;
+    p.gravity = 9.81f;
+    p.spray_amount = 1.0f;
+    p.mist_amount = 1.0f;
+    p.resolution = 64;
+    p.mesh_level = 6;
+    p.dt_max = 1e-3f;
+    p.seed = 0;
+    p.block_cap = 0;
+    p.spray_cap = 1200000;
+    p.max_iters = 4096;
+    p.solve_tol = 1e-5f;
+}
+
+// A copy of the last shot, a quarter turn further round (SimParams::add_shot).
+static void add_shot(ntr_sim_params& p) {
+    ntr_shot s = p.n_shots > 0 ? p.shots[p.n_shots - 1] : shot_default();
+    s.azimuth_deg = std::fmod(s.azimuth_deg + 270.0f, 360.0f) - 180.0f;
+    p.shots[p.n_shots++] = s;
+}
+
+template <class T>
+static bool parse_num(const char* v, T& out) {
+    char* end = nullptr;
+    if constexpr (std::is_same<T, float>::value) {
+        out = std::strtof(v, &end);
+    } else if constexpr (std::is_same<T, uint64_t>::value) {
+        if (*v == '-') return false;
+        out = std::strtoull(v, &end, 10);
+    } else {
+        if (*v == '-') return false;
+        unsigned long long x = std::strtoull(v, &end, 10);
+        if (x > 0xffffffffull) return false;
+        out = (T)x;
+    }
+    return end && end != v && *end == 0;
+}
+
+bool params_set(ntr_sim_params& p, const char* key_c, const char* v, std::string& err) {
+    std::string key = key_c ? key_c : "";
+    if (!v) {
+        err = "missing value";
+        return false;
+    }
+    size_t idx = 0;
+    std::string name = key;
+    if (key.rfind("shot", 0) == 0) {
+        size_t dot = key.find('.');
+        if (dot != std::string::npos) {
+            uint32_t n = 0;
+            if (!parse_num(key.substr(4, dot - 4).c_str(), n)) {
+                err = "bad value '" + key.substr(4, dot - 4) + "'";
+                return false;
+            }
+            if (n == 0) {
+                err = "shots count from 1";
+                return false;
+            }
+            idx = n - 1;
+            name = key.substr(dot + 1);
+        }
+    }
+    if (idx >= NTR_MAX_SHOTS) {
+        err = "at most 4 shots";
+        return false;
+    }
+    size_t count = std::max<size_t>(p.n_shots, idx + 1);
+    if (name == "shots") {
+        uint32_t c = 0;
+        if (!parse_num(v, c)) {
+            err = std::string("bad value '") + v + "'";
+            return false;
+        }
+        count = c;
+    }
+    if (count < 1 || count > NTR_MAX_SHOTS) {
+        err = "shots 1..4";
+        return false;
+    }
+    ntr_sim_params q = p;
+    if (q.n_shots > count) q.n_shots = (uint32_t)count;
+    while (q.n_shots < count) add_shot(q);
+    ntr_shot& s = q.shots[idx];
+    auto bad = [&]() {
+        err = std::string("bad value '") + v + "'";
+        return false;
+    };
+    auto setf = [&](float& dst) { return parse_num(v, dst) ? true : bad(); };
+    auto setu = [&](uint32_t& dst) { return parse_num(v, dst) ? true : bad(); };
+    bool ok = true;
+    if (name == "shots") {
+    } else if (name == "bullet") {
+        uint32_t k = 0;
+        if (!parse_num(v, k)) return bad();
+        if (k >= 7) {
+            err = "bullet 0..6";
+            return false;
+        }
+        shot_set_bullet(s, k);
+    } else if (name == "bullet_speed") ok = setf(s.speed);
+    else if (name == "caliber") ok = setf(s.caliber_mm);
+    else if (name == "mass") ok = setf(s.mass_g);
+    else if (name == "spin") ok = setf(s.spin_rpm);
+    else if (name == "range") ok = setf(s.range_m);
+    else if (name == "yaw") ok = setf(s.muzzle_yaw_deg);
+    else if (name == "azimuth") ok = setf(s.azimuth_deg);
+    else if (name == "elevation") ok = setf(s.elevation_deg);
+    else if (name == "impact_offset") ok = setf(s.impact_offset_cm);
+    else if (name == "impact_side") ok = setf(s.impact_side_cm);
+    else if (name == "delay") ok = setf(s.delay_ms);
+    else if (name == "diameter") ok = setf(q.balloon_diameter_cm);
+    else if (name == "height") ok = setf(q.balloon_height);
+    else if (name == "modulus") ok = setf(q.rubber_modulus_mpa);
+    else if (name == "rest_diameter") ok = setf(q.rubber_rest_diameter_cm);
+    else if (name == "break_stretch") ok = setf(q.rubber_break_stretch);
+    else if (name == "thickness") ok = setf(q.rubber_thickness_mm);
+    else if (name == "gravity") ok = setf(q.gravity);
+    else if (name == "spray") ok = setf(q.spray_amount);
+    else if (name == "mist") ok = setf(q.mist_amount);
+    else if (name == "resolution") ok = setu(q.resolution);
+    else if (name == "mesh_level") {
+        ok = setu(q.mesh_level);
+        if (ok && q.mesh_level > 8) {
+            err = "mesh_level 0..8";
+            return false;
+        }
+    } else if (name == "dt_max") ok = setf(q.dt_max);
+    else if (name == "seed") {
+        ok = parse_num(v, q.seed) ? true : bad();
+    } else if (name == "block_cap") ok = setu(q.block_cap);
+    else if (name == "spray_cap") ok = setu(q.spray_cap);
+    else if (name == "max_iters") ok = setu(q.max_iters);
+    else if (name == "solve_tol") ok = setf(q.solve_tol);
+    else if (name == "sun" || name == "sky" || name == "env_rotation" || name == "exposure" || name == "dof" ||
+             name == "fstop" || name == "focal" || name == "bloom" || name == "caustics" || name == "mist_render" ||
+             name == "shutter" || name == "max_bounces" || name == "color") {
+        // Renderer-only look parameters: accepted, no effect on the simulation.
+    } else {
+        err = "unknown parameter '" + key + "'";
+        return false;
+    }
+    if (!ok) return false;
+    p = q;
+    return true;
+}
+
+static bool ieq(const char* a, const char* b) {
+    for (; *a && *b; a++, b++)
+        if (std::tolower((unsigned char)*a) != std::tolower((unsigned char)*b)) return false;
+    return *a == 0 && *b == 0;
+}
+
+bool params_preset(ntr_sim_params& p, const char* name, std::string& err) {
+    ntr_sim_params q;
+    params_default(q);
+    auto with_bullet = [](uint32_t k) {
+        ntr_shot s = shot_default();
+        shot_set_bullet(s, k);
+        return s;
+    };
+    if (ieq(name, "Backlit")) {
+    } else if (ieq(name, "Tumbling rifle round")) {
+        q.shots[0] = with_bullet(3);
+        q.shots[0].speed = 500.0f;
+        q.balloon_diameter_cm = 22.0f;
+        q.rubber_rest_diameter_cm = 8.0f;
+        q.rubber_thickness_mm = 0.5f;
+    } else if (ieq(name, "Crossfire")) {
+        q.n_shots = 2;
+        q.shots[0] = shot_default();
+        q.shots[0].impact_offset_cm = 1.5f;
+        q.shots[1] = shot_default();
+        q.shots[1].azimuth_deg = 90.0f;
+        q.shots[1].impact_offset_cm = -1.5f;
+    } else if (ieq(name, "Four sides")) {
+        const float ad[4][2] = {{0.0f, 0.0f}, {90.0f, 0.5f}, {-180.0f, 1.0f}, {-90.0f, 1.5f}};
+        q.n_shots = 4;
+        for (int i = 0; i < 4; i++) {
+            q.shots[i] = shot_default();
+            q.shots[i].azimuth_deg = ad[i][0];
+            q.shots[i].delay_ms = ad[i][1];
+        }
+    } else if (ieq(name, "Moon gravity")) {
+        q.gravity = 1.62f;
+        q.balloon_diameter_cm = 20.0f;
+    } else if (ieq(name, "Weightless")) {
+        q.gravity = 0.0f;
+    } else if (ieq(name, "Slow pellet")) {
+        q.shots[0] = with_bullet(5);
+        q.shots[0].speed = 120.0f;
+        q.balloon_diameter_cm = 12.0f;
+        q.rubber_rest_diameter_cm = 3.2f;
+    } else if (ieq(name, "Bounce")) {
+        q.shots[0] = with_bullet(6);
+        q.shots[0].speed = 40.0f;
+        q.rubber_thickness_mm = 1.5f;
+        q.rubber_modulus_mpa = 4.0f;
+    } else {
+        err = std::string("no preset '") + name +
+              "', try one of: Backlit, Tumbling rifle round, Crossfire, Four sides, Moon gravity, Weightless, Slow pellet, Bounce";
+        return false;
+    }
+    p = q;
+    return true;
+}
+
+uint32_t substeps_for(float dt, float sub_dt) {
+    float n = std::ceil(1.1f * dt / sub_dt);
+    if (!std::isfinite(n)) return 2;
+    uint32_t k = n <= 0.0f ? 0u : (n >= 4294967296.0f ? 0xffffffffu : (uint32_t)n);
+    k = std::clamp<uint32_t>(k, 2, 256);
+    return (k + 1) / 2 * 2;
+}
+
+void adapt_after_batch(ntr_world_header& h, const ntr_state& s) {
+    h.unconverged += s.unconverged;
+    uint32_t mx = h.max_iters ? h.max_iters : 4096;
+    if (s.unconverged > 0)
+        h.iters = std::min(h.iters * 2, mx);
+    else if (s.iters_max > 0)
+        h.iters = std::clamp(s.iters_max + s.iters_max / 4 + 2, std::min(8u, mx), mx);
+    h.substeps = substeps_for(s.dt_flow, s.mem_dt_seen);
+    h.air_substeps = substeps_for(s.dt_flow, s.air_dt_seen);
+}
+
+// ---- the world ---------------------------------------------------------------------------
+SectionShape section_shape(const ntr_world_header& h, int sec) {
+    size_t cells_prev = (size_t)h.n_blocks_prev * 64;
+    switch (sec) {
+        case NTR_SEC_PARTICLES: return {80, h.n_particles};
+        case NTR_SEC_MEM_X: return {16, h.n_verts};
+        case NTR_SEC_MEM_V: return {16, h.n_verts};
+        case NTR_SEC_MEM_MASS: return {4, h.n_verts};
+        case NTR_SEC_MEM_WATER: return {16, h.n_verts};
+        case NTR_SEC_MEM_LAYER: return {16 * NTR_LAYER_MODES, h.n_verts};
+        case NTR_SEC_MEM_PUSH: return {8, h.n_verts};
+        case NTR_SEC_TRIS: return {32, h.n_tris};
+        case NTR_SEC_ALIVE: return {4, h.n_tris};
+        case NTR_SEC_VTRI_OFF: return {4, (size_t)h.n_verts + 1};
+        case NTR_SEC_VTRI: return {4, h.n_vtri};
+        case NTR_SEC_BULLETS: return {112, NTR_MAX_SHOTS};
+        case NTR_SEC_PATCHES: return {32, NTR_MAX_SHOTS * NTR_MAX_PATCHES};
+        case NTR_SEC_OUTLINES: return {8, NTR_MAX_SHOTS * NTR_OUTLINE};
+        case NTR_SEC_SECTIONS: return {48, NTR_MAX_SHOTS * NTR_N_SEC};
+        case NTR_SEC_BULLET_HIT: return {4, NTR_MAX_SHOTS * NTR_HIT_FIELDS};
+        case NTR_SEC_POSE_LOG: return {48, NTR_MAX_SHOTS * NTR_LOG_CAP};
+        case NTR_SEC_BLOCKS_PREV: return {4, h.n_blocks_prev};
+        case NTR_SEC_BLOCK_ACTIVE: return {4, h.n_blocks_prev};
+        case NTR_SEC_AIR: return {4, NTR_AIR_FIELDS * cells_prev};
+        case NTR_SEC_SPRAY: return {48, h.n_spray};
+        case NTR_SEC_LANDED: return {16, h.n_spray};
+        case NTR_SEC_TOUCH: return {4, (size_t)h.wet_res * h.wet_res};
+    }
+    return {0, 0};
+}
+
+void World::shape_sections() {
+    for (int s = 0; s < NTR_SEC_COUNT; s++) {
+        SectionShape sh = section_shape(h, s);
+        sec[s].resize(sh.elem * sh.count);
+    }
+}
+
+std::vector<uint8_t> serialize(const World& w) {
+    ntr_world_header h = w.h;
+    size_t off = (sizeof(ntr_world_header) + 255) & ~size_t(255);
+    for (int s = 0; s < NTR_SEC_COUNT; s++) {
+        h.offset[s] = off;
+        h.bytes[s] = w.sec[s].size();
+        off += (w.sec[s].size() + 255) & ~size_t(255);
+    }
+    std::vector<uint8_t> out(off, 0);
+    std::memcpy(out.data(), &h, sizeof h);
+    for (int s = 0; s < NTR_SEC_COUNT; s++)
+        if (!w.sec[s].empty()) std::memcpy(out.data() + h.offset[s], w.sec[s].data(), w.sec[s].size());
+    return out;
+}
+
+bool deserialize(const void* blob, size_t len, World& w, std::string& err) {
+    if (!blob || len < sizeof(ntr_world_header)) {
+        err = "world blob too short";
+        return false;
+    }
+    std::memcpy(&w.h, blob, sizeof(ntr_world_header));
+    if (w.h.magic != NTR_WORLD_MAGIC || w.h.version != NTR_WORLD_VERSION) {
+        err = "not a world blob of this version";
+        return false;
+    }
+    if (w.h.n_shots > NTR_MAX_SHOTS || w.h.n_blocks_prev > w.h.block_cap || w.h.n_spray > w.h.spray_cap) {
+        err = "world blob counts out of range";
+        return false;
+    }
+    const uint8_t* b = (const uint8_t*)blob;
+    for (int s = 0; s < NTR_SEC_COUNT; s++) {
+        SectionShape sh = section_shape(w.h, s);
+        size_t need = sh.elem * sh.count;
+        if (w.h.bytes[s] != need || w.h.offset[s] > len || len - w.h.offset[s] < need) {
+            char buf[96];
+            snprintf(buf, sizeof buf, "world blob section %d has %llu bytes, expected %zu", s, (unsigned long long)w.h.bytes[s], need);
+            err = buf;
+            return false;
+        }
+        w.sec[s].assign(b + w.h.offset[s], b + w.h.offset[s] + need);
+    }
+    return true;
+}
+
+bool build_world(const ntr_sim_params& p, World& w, std::string& err) {
+    if (p.n_shots < 1 || p.n_shots > NTR_MAX_SHOTS) {
+        err = "shots 1..4";
+        return false;
+    }
+    for (uint32_t k = 0; k < p.n_shots; k++)
+        if (p.shots[k].bullet >= 7) {
+            err = "bullet 0..6";
+            return false;
+        }
+    if (!(p.balloon_diameter_cm > 0.0f) || !(p.rubber_rest_diameter_cm > 0.0f) || !(p.rubber_thickness_mm > 0.0f) ||
+        !(p.rubber_modulus_mpa > 0.0f) || !(p.dt_max > 0.0f) || p.mesh_level > 8 || p.resolution > 4096) {
+        err = "scene parameters out of range";
+        return false;
+    }
+    Balloon scene;
+    if (!build_balloon(p, scene, err)) return false;
+
+    const float WET_HALF = 1.2f;
+    const uint32_t WET_RES = 1024;
+    const float SOUND = 1480.0f, CFL = 0.8f;
+    const uint32_t n_particles = (uint32_t)scene.particles.size();
+    const uint32_t n_verts = (uint32_t)scene.mem_pos.size();
+    const uint32_t n_tris = (uint32_t)scene.tris.size();
+    const double dx = 2.0 * scene.spacing;
+
+    // The sparse grid covers everything the water could reach, src/sim.rs:215-226.
+    double top = scene.bottom_y + scene.profile.z_top() + 0.6;
+    auto mult4 = [](uint32_t x) { return (x + 3) / 4 * 4; };
+    uint32_t nxz = mult4((uint32_t)std::ceil(2.0 * (double)WET_HALF / dx));
+    uint32_t ny = mult4((uint32_t)std::ceil(top / dx) + 3);
+    float half = (float)((double)nxz * 0.5 * dx);
+    float origin[3] = {-half, (float)(-3.0 * dx), -half};
+    uint32_t block_cap = p.block_cap;
+    if (block_cap == 0) block_cap = std::max<uint32_t>(65535u, n_particles / 32u + 4096u);
+
+    ntr_world_header& h = w.h;
+    std::memset(&h, 0, sizeof h);
+    h.magic = NTR_WORLD_MAGIC;
+    h.version = NTR_WORLD_VERSION;
+    h.n_particles = n_particles;
+    h.n_verts = n_verts;
+    h.n_tris = n_tris;
+    h.n_vtri = (uint32_t)scene.vtri.size();
+    h.n_shots = p.n_shots;
+    h.n_blocks_prev = 0;
+    h.n_spray = 0;
+    h.wet_res = WET_RES;
+    h.spray_cap = p.spray_cap ? p.spray_cap : 1200000u;
+    h.block_cap = block_cap;
+    h.iters = 64;
+    h.substeps = 0;  // 0 = the zero-length measuring substep has not run yet
+    h.air_substeps = 0;
+    h.unconverged = 0;
+    h.started = 0;
+    h.max_iters = p.max_iters ? p.max_iters : 4096;
+    h.dx = dx;
+    w.shape_sections();
+
+    float* part = w.as<float>(NTR_SEC_PARTICLES);
+    for (uint32_t i = 0; i < n_particles; i++) {
+        float* a = part + (size_t)i * 20;
+        std::memset(a, 0, 80);
+        std::memcpy(a, scene.particles[i].data(), 16);
+        a[7] = 1.0f;
+    }
+    std::memcpy(w.as<float>(NTR_SEC_MEM_X), scene.mem_pos.data(), (size_t)n_verts * 16);
+    std::memcpy(w.as<float>(NTR_SEC_MEM_MASS), scene.mem_mass.data(), (size_t)n_verts * 4);
+    float* mw = w.as<float>(NTR_SEC_MEM_WATER);
+    for (uint32_t i = 0; i < n_verts; i++) mw[4 * i + 3] = 1.0f;  // the rubber starts on the water
+    std::memcpy(w.as<uint8_t>(NTR_SEC_TRIS), scene.tris.data(), (size_t)n_tris * 32);
+    uint32_t* alive = w.as<uint32_t>(NTR_SEC_ALIVE);
+    for (uint32_t t = 0; t < n_tris; t++) alive[t] = 1;
+    std::memcpy(w.as<uint32_t>(NTR_SEC_VTRI_OFF), scene.vtri_off.data(), scene.vtri_off.size() * 4);
+    std::memcpy(w.as<uint32_t>(NTR_SEC_VTRI), scene.vtri.data(), scene.vtri.size() * 4);
+    uint32_t* touch = w.as<uint32_t>(NTR_SEC_TOUCH);
+    for (size_t i = 0; i < (size_t)WET_RES * WET_RES; i++) touch[i] = 0xffffffffu;
+
+    // Shots, src/sim.rs:280-310.
+    float first = 3.4028235e38f;
+    for (uint32_t k = 0; k < p.n_shots; k++) first = std::min(first, p.shots[k].delay_ms);
+    const float RADS = 3.14159265358979323846f / 180.0f;
+    std::vector<Handoff> hand(p.n_shots);
+    std::vector<Body> bodies(p.n_shots);
+    for (uint32_t k = 0; k < p.n_shots; k++) {
+        const ntr_shot& s = p.shots[k];
+        float az = s.azimuth_deg * RADS, el = s.elevation_deg * RADS;
+        V3f dir{std::cos(az) * std::cos(el), -std::sin(el), std::sin(az) * std::cos(el)};
+        V3f side = normalize_or(cross(dir, V3f{0, 1, 0}), V3f{0, 0, 1});
+        V3f aim = (scene.center + V3f{0, 1, 0} * (s.impact_offset_cm * 0.01f)) + side * (s.impact_side_cm * 0.01f);
+        auto e = scene.entry(aim, dir);
+        V3f target = e ? *e : aim - dir * (float)scene.radius_max;
+        double t_hit = (double)(s.delay_ms - first) * 1e-3;
+        bodies[k] = body_new(s);
+        hand[k] = straight_handoff(s, bodies[k], widen(target), widen(dir), t_hit);
+    }
+    double t_start = 0.0, t0 = 0.0;
+    for (auto& hd : hand) {
+        t_start = std::min(t_start, hd.t_read - (0.3 - LOOKAHEAD) / hd.v_impact);
+        t0 = std::min(t0, hd.t_read);
+    }
+    GpuBullet* bl = w.as<GpuBullet>(NTR_SEC_BULLETS);
+    Patch* pat = w.as<Patch>(NTR_SEC_PATCHES);
+    float* ol = w.as<float>(NTR_SEC_OUTLINES);
+    for (uint32_t k = 0; k < p.n_shots; k++) {
+        const Body& b = bodies[k];
+        auto surf = surface(b);
+        if (surf.size() > NTR_MAX_PATCHES) {
+            err = "bullet surface has too many patches";
+            return false;
+        }
+        std::memcpy(pat + (size_t)k * NTR_MAX_PATCHES, surf.data(), surf.size() * sizeof(Patch));
+        auto line = outline(b);
+        for (int j = 0; j < NTR_OUTLINE; j++) {
+            ol[(k * NTR_OUTLINE + j) * 2 + 0] = (float)(line[j].first - b.u_cg);
+            ol[(k * NTR_OUTLINE + j) * 2 + 1] = (float)line[j].second;
+        }
+        const Handoff& hd = hand[k];
+        auto q = rotation_arc_z(normalize(hd.n));
+        GpuBullet g{};
+        g.x[0] = (float)hd.x.x, g.x[1] = (float)hd.x.y, g.x[2] = (float)hd.x.z, g.x[3] = (float)b.mass;
+        g.v[0] = (float)hd.u.x, g.v[1] = (float)hd.u.y, g.v[2] = (float)hd.u.z, g.v[3] = (float)hd.roll;
+        for (int c = 0; c < 4; c++) g.q[c] = (float)q[c];
+        g.l[0] = (float)hd.h.x, g.l[1] = (float)hd.h.y, g.l[2] = (float)hd.h.z, g.l[3] = (float)length(hd.u);
+        g.shape[0] = (float)b.ix, g.shape[1] = (float)b.iy, g.shape[2] = (float)b.length, g.shape[3] = (float)hull(b);
+        g.info[0] = (uint32_t)std::llround((hd.t_read - t0) * 1e9);
+        g.info[1] = (uint32_t)surf.size();
+        g.info[2] = 0;
+        g.info[3] = 0;
+        bl[k] = g;
+    }
+    h.t = t_start;
+    h.t_start = t_start;
+    h.t0 = t0;
+
+    // The uniform, src/sim.rs:428-441.
+    ntr_gpu_params& u = h.params;
+    u.origin[0] = origin[0], u.origin[1] = origin[1], u.origin[2] = origin[2], u.origin[3] = (float)dx;
+    u.dims[0] = nxz, u.dims[1] = ny, u.dims[2] = nxz, u.dims[3] = n_particles;
+    u.bdims[0] = nxz / 4, u.bdims[1] = ny / 4, u.bdims[2] = nxz / 4, u.bdims[3] = block_cap;
+    u.gravity[0] = 0.0f, u.gravity[1] = -p.gravity, u.gravity[2] = 0.0f, u.gravity[3] = SOUND;
+    u.fluid[0] = (float)RHO_WATER, u.fluid[1] = CFL, u.fluid[2] = p.dt_max, u.fluid[3] = (float)scene.spacing;
+    u.wet[0] = WET_HALF;
+    u.limits[0] = WET_RES, u.limits[1] = h.spray_cap, u.limits[2] = 0, u.limits[3] = 0;
+    u.solve[0] = p.solve_tol > 0.0f ? p.solve_tol : 1e-5f;
+    u.mem[0] = n_verts, u.mem[1] = 2, u.mem[2] = 2, u.mem[3] = p.n_shots;
+    u.rubber[0] = (float)scene.latex.mu[0], u.rubber[1] = (float)scene.latex.mu[1], u.rubber[2] = (float)scene.latex.mu[2];
+    u.rubber[3] = (float)scene.latex.thickness;
+    u.rubber2[0] = 0.8f, u.rubber2[1] = p.rubber_break_stretch;
+    u.knot[0] = 0.0f, u.knot[1] = (float)(scene.bottom_y + scene.profile.z_neck), u.knot[2] = 0.0f;
+    u.knot[3] = (float)scene.profile.neck_r;
+
+    // Nothing limits the first step until the rubber has measured itself; the air starts
+    // still at the stable substep of air.wgsl, src/sim.rs:238-241.
+    ntr_state& st = h.state;
+    std::memset(&st, 0, sizeof st);
+    float c_air = std::sqrt(1.4f * 101325.0f / 1.204f);
+    st.mem_dt = 3.4028235e38f;
+    st.cap_dt = 3.4028235e38f;
+    st.air_dt = 0.9f * (float)dx / (3.0f * c_air);
+    return true;
+}
+
+}  // namespace ntr

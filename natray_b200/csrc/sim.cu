@@ -1,0 +1,755 @@
+// The simulation on one B200: device state, the step as one CUDA graph, and the C ABI of
+// include/natray.h that replaces the reference's wgpu dispatch (src/gpu.rs:60-214, src/sim.rs:
+// 208-689).
+//
+// A step is ~30 kernels plus two per solver iteration and one or two per substep. The host
+// never synchronises inside a batch: the step length, the block set, the solver's convergence
+// and every dispatch size are decided on the device, as in the reference. The host captures
+// one step into a CUDA graph per (solver iterations, rubber substeps, air substeps, precision)
+// and launches it n times for a batch, then reads the state back once (src/sim.rs:585-648).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <type_traits>
+#include <vector>
+
+#include "capi_util.hpp"
+#include "kernels_g2p.cuh"
+#include "kernels_grid.cuh"
+#include "world.hpp"
+
+namespace ntr {
+
+#define CU(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) {                                                                   \
+            return fail(NTR_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));           \
+        }                                                                                          \
+    } while (0)
+
+struct GraphKey {
+    uint32_t iters, n_mem, n_air, fp64;
+    bool operator<(const GraphKey& o) const {
+        return std::tie(iters, n_mem, n_air, fp64) < std::tie(o.iters, o.n_mem, o.n_air, o.fp64);
+    }
+};
+
+struct StepGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t launches = 0;
+};
+
+struct Sim {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    World host;  // header (params, host control) of the world; sections are not kept
+    ntr_gpu_params U{};
+    Dev D{};
+    std::vector<void*> allocs;
+    size_t device_bytes = 0;
+    DevState* h_state = nullptr;  // pinned
+    std::map<GraphKey, StepGraph> graphs;
+    uint64_t last_launches = 0;
+    double last_ms = 0.0;
+    double step_ms = 0.0;
+    uint32_t fp64 = 1;
+
+    ~Sim() {
+        cudaSetDevice(device);
+        for (auto& kv : graphs) {
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+            if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+        }
+        for (void* p : allocs) cudaFree(p);
+        if (h_state) cudaFreeHost(h_state);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    template <class T>
+    ntr_status alloc(T*& p, size_t count) {
+        void* q = nullptr;
+        size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+        cudaError_t e = cudaMalloc(&q, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(NTR_E_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+        }
+        allocs.push_back(q);
+        device_bytes += bytes;
+        p = (T*)q;
+        return NTR_OK;
+    }
+};
+
+static ntr_status check_device(int device) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(NTR_E_NODEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= n) return fail(NTR_E_INVALID, "device index out of range");
+    return NTR_OK;
+}
+
+static uint32_t radix_passes_for(uint32_t cap) {
+    // The key NONE sorts as 2^(8p) - 1, which no valid block index may reach.
+    uint32_t p = 1;
+    while (p < 4 && (uint64_t)cap >= (1ull << (8 * p))) p++;
+    return p;
+}
+
+// ---- allocation and upload --------------------------------------------------------------------
+static ntr_status allocate(Sim& S) {
+    const ntr_world_header& h = S.host.h;
+    Dev& D = S.D;
+    D.Np = h.n_particles, D.Nv = h.n_verts, D.Nt = h.n_tris;
+    D.cap_blocks = h.block_cap;
+    D.cap_cells = h.block_cap * 64u;
+    D.spray_cap = h.spray_cap;
+    D.wet_res = h.wet_res;
+    const size_t slots = (size_t)h.params.bdims[0] * h.params.bdims[1] * h.params.bdims[2];
+    D.nwords = (uint32_t)((slots + 31) / 32);
+    D.scan_ctas = (D.nwords + SCAN_T * SCAN_W - 1) / (SCAN_T * SCAN_W);
+    D.n_tiles = (D.Np + RADIX_TILE - 1) / RADIX_TILE;
+    if (D.n_tiles == 0) D.n_tiles = 1;
+    D.radix_passes = radix_passes_for(D.cap_blocks);
+    D.fp64_dots = S.fp64;
+    ntr_status r;
+#define AL(p, n) \
+    if ((r = S.alloc(p, n)) != NTR_OK) return r
+    ntr_gpu_params* u;
+    AL(u, 1);
+    D.U = u;
+    AL(D.st, 1);
+    AL(D.pos, D.Np);
+    AL(D.vel, D.Np);
+    AL(D.c0, D.Np);
+    AL(D.c1, D.Np);
+    AL(D.c2, D.Np);
+    for (int k = 0; k < 2; k++) {
+        AL(D.mask[k], D.nwords);
+        AL(D.prefix[k], D.nwords + 1);
+        AL(D.block_list[k], D.cap_blocks);
+    }
+    AL(D.cta_sum, D.scan_ctas + 1);
+    AL(D.pslot, D.Np);
+    AL(D.key, D.Np);
+    AL(D.key_alt, D.Np);
+    AL(D.val_alt, D.Np);
+    AL(D.key_sorted, D.Np);
+    AL(D.sorted, D.Np);
+    AL(D.hist, 256u * D.n_tiles);
+    AL(D.block_start, D.cap_blocks + 1);
+    AL(D.block_nb, (size_t)D.cap_blocks * 27);
+    AL(D.block_active, D.cap_blocks);
+    AL(D.acc, (size_t)NTR_ACC_FIELDS * D.cap_cells);
+    AL(D.cf, (size_t)NTR_CELL_FIELDS * D.cap_cells);
+    AL(D.air[0], (size_t)NTR_AIR_FIELDS * D.cap_cells);
+    AL(D.air[1], (size_t)NTR_AIR_FIELDS * D.cap_cells);
+    AL(D.px, D.cap_blocks); AL(D.py, D.cap_blocks); AL(D.pz, D.cap_blocks);
+    for (int k = 0; k < 2; k++) {
+        AL(D.mem_x[k], D.Nv);
+        AL(D.mem_v[k], D.Nv);
+    }
+    AL(D.mem_water, D.Nv);
+    AL(D.mem_layer, (size_t)D.Nv * NTR_LAYER_MODES);
+    AL(D.mem_push, D.Nv);
+    AL(D.mem_mass, D.Nv);
+    Tri* tris;
+    AL(tris, D.Nt);
+    D.tris = tris;
+    AL(D.alive, D.Nt);
+    AL(D.vtri_off, D.Nv + 1);
+    AL(D.vtri, h.n_vtri);
+    AL(D.bullets, NTR_MAX_SHOTS);
+    float4* pat;
+    AL(pat, NTR_MAX_SHOTS * NTR_MAX_PATCHES * 2);
+    D.patches = pat;
+    float2* ol;
+    AL(ol, NTR_MAX_SHOTS * NTR_OUTLINE);
+    D.outlines = ol;
+    AL(D.sections, NTR_MAX_SHOTS * NTR_N_SEC);
+    AL(D.bullet_hit, NTR_MAX_SHOTS * NTR_HIT_FIELDS);
+    AL(D.pose_log, NTR_MAX_SHOTS * NTR_LOG_CAP * 3);
+    AL(D.spray, (size_t)D.spray_cap * 3);
+    AL(D.landed, D.spray_cap);
+    AL(D.touch, (size_t)D.wet_res * D.wet_res);
+    AL(D.brk_x, D.Np); AL(D.brk_v, D.Np);
+    AL(D.brk_count, D.cap_blocks); AL(D.brk_off, D.cap_blocks);
+#undef AL
+    return NTR_OK;
+}
+
+// Writes the world's state (not its static scene) to the device.
+static ntr_status upload_state(Sim& S, const World& w) {
+    const ntr_world_header& h = w.h;
+    Dev& D = S.D;
+    cudaStream_t st = S.stream;
+    // Particles: AoS of 20 floats to five float4 arrays.
+    {
+        std::vector<float4> a[5];
+        for (auto& v : a) v.resize(D.Np);
+        const float* p = w.as<float>(NTR_SEC_PARTICLES);
+        for (uint32_t i = 0; i < D.Np; i++)
+            for (int k = 0; k < 5; k++) a[k][i] = make_float4(p[20 * (size_t)i + 4 * k], p[20 * (size_t)i + 4 * k + 1], p[20 * (size_t)i + 4 * k + 2], p[20 * (size_t)i + 4 * k + 3]);
+        float4* dst[5] = {D.pos, D.vel, D.c0, D.c1, D.c2};
+        for (int k = 0; k < 5; k++) CU(cudaMemcpy(dst[k], a[k].data(), (size_t)D.Np * 16, cudaMemcpyHostToDevice));
+    }
+    CU(cudaMemcpy(D.mem_x[0], w.sec[NTR_SEC_MEM_X].data(), (size_t)D.Nv * 16, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(D.mem_x[1], w.sec[NTR_SEC_MEM_X].data(), (size_t)D.Nv * 16, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(D.mem_v[0], w.sec[NTR_SEC_MEM_V].data(), (size_t)D.Nv * 16, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(D.mem_v[1], w.sec[NTR_SEC_MEM_V].data(), (size_t)D.Nv * 16, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(D.mem_water, w.sec[NTR_SEC_MEM_WATER].data(), (size_t)D.Nv * 16, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(D.mem_layer, w.sec[NTR_SEC_MEM_LAYER].data(), (size_t)D.Nv * 96, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(D.mem_push, w.sec[NTR_SEC_MEM_PUSH].data(), (size_t)D.Nv * 8, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(D.alive, w.sec[NTR_SEC_ALIVE].data(), (size_t)D.Nt * 4, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(D.bullets, w.sec[NTR_SEC_BULLETS].data(), w.sec[NTR_SEC_BULLETS].size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(D.sections, w.sec[NTR_SEC_SECTIONS].data(), w.sec[NTR_SEC_SECTIONS].size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(D.bullet_hit, w.sec[NTR_SEC_BULLET_HIT].data(), w.sec[NTR_SEC_BULLET_HIT].size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(D.pose_log, w.sec[NTR_SEC_POSE_LOG].data(), w.sec[NTR_SEC_POSE_LOG].size(), cudaMemcpyHostToDevice));
+    CU(cudaMemset(D.spray, 0, (size_t)D.spray_cap * 48));
+    CU(cudaMemset(D.landed, 0, (size_t)D.spray_cap * 16));
+    if (h.n_spray) {
+        CU(cudaMemcpy(D.spray, w.sec[NTR_SEC_SPRAY].data(), (size_t)h.n_spray * 48, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(D.landed, w.sec[NTR_SEC_LANDED].data(), (size_t)h.n_spray * 16, cudaMemcpyHostToDevice));
+    }
+    CU(cudaMemcpy(D.touch, w.sec[NTR_SEC_TOUCH].data(), (size_t)D.wet_res * D.wet_res * 4, cudaMemcpyHostToDevice));
+    // Grid: the last step's blocks become the "current" ones of parity step & 1.
+    CU(cudaMemset(D.acc, 0, (size_t)NTR_ACC_FIELDS * D.cap_cells * 4));
+    CU(cudaMemset(D.cf, 0, (size_t)NTR_CELL_FIELDS * D.cap_cells * 4));
+    CU(cudaMemset(D.air[0], 0, (size_t)NTR_AIR_FIELDS * D.cap_cells * 4));
+    CU(cudaMemset(D.air[1], 0, (size_t)NTR_AIR_FIELDS * D.cap_cells * 4));
+    CU(cudaMemset(D.block_active, 0, (size_t)D.cap_blocks * 4));
+    const int cur = (int)(h.state.step & 1u);
+    const uint32_t nbp = h.n_blocks_prev;
+    {
+        std::vector<uint32_t> mask(D.nwords, 0u), prefix(D.nwords + 1, 0u);
+        const uint32_t* bl = w.as<uint32_t>(NTR_SEC_BLOCKS_PREV);
+        for (uint32_t b = 0; b < nbp; b++) {
+            if (b > 0 && bl[b] <= bl[b - 1]) return fail(NTR_E_INVALID, "world blob block list is not ascending");
+            if ((size_t)bl[b] >= (size_t)D.nwords * 32) return fail(NTR_E_INVALID, "world blob block slot out of range");
+            mask[bl[b] >> 5] |= 1u << (bl[b] & 31u);
+        }
+        uint32_t run = 0;
+        for (uint32_t k = 0; k < D.nwords; k++) {
+            prefix[k] = run;
+            run += __builtin_popcount(mask[k]);
+        }
+        prefix[D.nwords] = run;
+        CU(cudaMemcpy(D.mask[cur], mask.data(), (size_t)D.nwords * 4, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(D.prefix[cur], prefix.data(), ((size_t)D.nwords + 1) * 4, cudaMemcpyHostToDevice));
+        CU(cudaMemset(D.mask[cur ^ 1], 0, (size_t)D.nwords * 4));
+        CU(cudaMemset(D.prefix[cur ^ 1], 0, ((size_t)D.nwords + 1) * 4));
+        if (nbp) {
+            CU(cudaMemcpy(D.block_list[cur], bl, (size_t)nbp * 4, cudaMemcpyHostToDevice));
+            CU(cudaMemcpy(D.block_active, w.sec[NTR_SEC_BLOCK_ACTIVE].data(), (size_t)nbp * 4, cudaMemcpyHostToDevice));
+            const float* af = w.as<float>(NTR_SEC_AIR);
+            for (uint32_t f = 0; f < NTR_AIR_FIELDS; f++)
+                CU(cudaMemcpy(D.air[0] + (size_t)f * D.cap_cells, af + (size_t)f * nbp * 64, (size_t)nbp * 64 * 4, cudaMemcpyHostToDevice));
+        }
+    }
+    DevState ds;
+    std::memset(&ds, 0, sizeof ds);
+    ds.s = h.state;
+    ds.s.n_blocks = nbp;
+    ds.rz = h.state.rz, ds.alpha = h.state.alpha, ds.beta = h.state.beta, ds.b_norm = h.state.b_norm, ds.r_norm = h.state.r_norm;
+    CU(cudaMemcpy(D.st, &ds, sizeof ds, cudaMemcpyHostToDevice));
+    (void)st;
+    return NTR_OK;
+}
+
+static ntr_status upload_static(Sim& S, const World& w) {
+    Dev& D = S.D;
+    CU(cudaMemcpy((void*)D.tris, w.sec[NTR_SEC_TRIS].data(), (size_t)D.Nt * 32, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(D.vtri_off, w.sec[NTR_SEC_VTRI_OFF].data(), ((size_t)D.Nv + 1) * 4, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(D.vtri, w.sec[NTR_SEC_VTRI].data(), w.sec[NTR_SEC_VTRI].size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(D.mem_mass, w.sec[NTR_SEC_MEM_MASS].data(), (size_t)D.Nv * 4, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy((void*)D.patches, w.sec[NTR_SEC_PATCHES].data(), w.sec[NTR_SEC_PATCHES].size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy((void*)D.outlines, w.sec[NTR_SEC_OUTLINES].data(), w.sec[NTR_SEC_OUTLINES].size(), cudaMemcpyHostToDevice));
+    return NTR_OK;
+}
+
+static ntr_status push_params(Sim& S) {
+    CU(cudaMemcpyAsync((void*)S.D.U, &S.U, sizeof(ntr_gpu_params), cudaMemcpyHostToDevice, S.stream));
+    return NTR_OK;
+}
+
+static ntr_status read_state(Sim& S) {
+    CU(cudaMemcpyAsync(S.h_state, S.D.st, sizeof(DevState), cudaMemcpyDeviceToHost, S.stream));
+    CU(cudaStreamSynchronize(S.stream));
+    return NTR_OK;
+}
+
+// The zero-length rubber substep that sizes the first step (src/sim.rs:524-541).
+static ntr_status measure_rubber(Sim& S) {
+    Dev& D = S.D;
+    CU(cudaMemsetAsync(&D.st->s.dt_ns, 0, 4, S.stream));
+    k_mem_substep<<<(D.Nv + 255) / 256, 256, 0, S.stream>>>(D, 0, 0);
+    CU(cudaGetLastError());
+    ntr_status r = read_state(S);
+    if (r != NTR_OK) return r;
+    const ntr_state& s = S.h_state->s;
+    float dtm = std::min(S.U.fluid[2], s.cap_dt);
+    S.host.h.substeps = substeps_for(dtm, s.mem_dt);
+    S.host.h.air_substeps = substeps_for(dtm, s.air_dt);
+    return NTR_OK;
+}
+
+// ---- the step -----------------------------------------------------------------------------------
+static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t iters, uint32_t n_mem, uint32_t n_air, bool fp64) {
+    Dev& D = S.D;
+    uint64_t n = 0;
+    const uint32_t G_cell = (uint32_t)S.sms * 8;
+    const uint32_t G_blk = (uint32_t)S.sms * 8;
+    const uint32_t G_solve = (uint32_t)S.sms * 4;
+    const uint32_t g_part = (D.Np + 255) / 256 ? (D.Np + 255) / 256 : 1;
+    const uint32_t g_vert = (D.Nv + 255) / 256 ? (D.Nv + 255) / 256 : 1;
+    const uint32_t n_shots = S.U.mem[3] ? S.U.mem[3] : 1;
+#define L(kern, grid, block, ...)                       \
+    do {                                                \
+        kern<<<(grid), (block), 0, s>>>(__VA_ARGS__);   \
+        n++;                                            \
+    } while (0)
+    L(k_begin_step, 1, 32, D);
+    L(k_clear, G_cell, 256, D);
+    L(k_mark, (uint32_t)(((uint64_t)D.Np + D.cap_blocks + D.Nv + 255) / 256), 256, D);
+    L(k_scan_words_a, D.scan_ctas, SCAN_T, D);
+    L(k_scan_words_b, D.scan_ctas, SCAN_T, D);
+    L(k_keys, g_part, 256, D);
+    {
+        const uint32_t P = D.radix_passes;
+        const uint32_t* kin = D.key;
+        const uint32_t* vin = nullptr;
+        for (uint32_t p = 0; p < P; p++) {
+            bool to_final = ((P - 1 - p) % 2) == 0;
+            uint32_t* kout = to_final ? D.key_sorted : D.key_alt;
+            uint32_t* vout = to_final ? D.sorted : D.val_alt;
+            L(k_radix_hist, D.n_tiles, RADIX_T, D, kin, 8u * p);
+            L(k_radix_scan, 1, 1024, D);
+            L(k_radix_scatter, D.n_tiles, RADIX_T, D, kin, vin, kout, vout, 8u * p);
+            kin = kout;
+            vin = vout;
+        }
+    }
+    L(k_block_bounds, (D.Np + 1 + 255) / 256, 256, D);
+    L(k_p2g, G_blk, P2G_T, D);
+    L(k_mem_splat, g_vert, 256, D);
+    L(k_air_carry, G_cell, 256, D);
+    L(k_grid_prep, G_cell, 256, D);
+    L(k_air_fill, G_cell, 256, D);
+    L(k_bullet_step, n_shots, 256, D);
+    L(k_bullet_apply, G_cell, 256, D);
+    if (fp64) {
+        L(k_solve_init<true>, G_solve, SOLVE_T, D);
+        for (uint32_t it = 0; it < iters; it++) {
+            L(k_solve_q<true>, G_solve, SOLVE_T, D);
+            L(k_solve_update<true>, G_solve, SOLVE_T, D);
+        }
+    } else {
+        L(k_solve_init<false>, G_solve, SOLVE_T, D);
+        for (uint32_t it = 0; it < iters; it++) {
+            L(k_solve_q<false>, G_solve, SOLVE_T, D);
+            L(k_solve_update<false>, G_solve, SOLVE_T, D);
+        }
+    }
+    L(k_project, G_cell, 256, D);
+    L(k_extend_1, G_cell, 256, D);
+    L(k_extend_2, G_cell, 256, D);
+    L(k_mem_sample, g_vert, 256, D);
+    for (uint32_t i = 0; i < std::max(n_mem, n_air); i++) {
+        if (i < n_mem) L(k_mem_substep, g_vert, 256, D, i, (int)(i % 2));
+        if (i < n_air) L(k_air_substep, G_cell, 256, D, (int)(i % 2));
+    }
+    L(k_spray_update, G_cell, 256, D);
+    L(k_g2p, G_blk, G2P_T, D);
+    L(k_spray_scan, 1, 1024, D);
+    L(k_spray_emit, G_cell, 256, D);
+    L(k_spray_commit, 1, 32, D);
+#undef L
+    return n;
+}
+
+static ntr_status get_graph(Sim& S, StepGraph*& out) {
+    GraphKey key{S.host.h.iters, S.host.h.substeps, S.host.h.air_substeps, S.fp64};
+    auto it = S.graphs.find(key);
+    if (it != S.graphs.end()) {
+        out = &it->second;
+        return NTR_OK;
+    }
+    // Bound the cache: a new shape replaces the oldest when there are many.
+    if (S.graphs.size() >= 16) {
+        auto victim = S.graphs.begin();
+        cudaGraphExecDestroy(victim->second.exec);
+        cudaGraphDestroy(victim->second.graph);
+        S.graphs.erase(victim);
+    }
+    StepGraph g;
+    CU(cudaStreamBeginCapture(S.stream, cudaStreamCaptureModeThreadLocal));
+    g.launches = enqueue_step(S, S.stream, key.iters, key.n_mem, key.n_air, key.fp64 != 0);
+    cudaError_t le = cudaGetLastError();
+    cudaError_t ce = cudaStreamEndCapture(S.stream, &g.graph);
+    if (le != cudaSuccess) return fail(NTR_E_CUDA, std::string("kernel launch during capture: ") + cudaGetErrorString(le));
+    if (ce != cudaSuccess) return fail(NTR_E_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce));
+    CU(cudaGraphInstantiate(&g.exec, g.graph, 0));
+    auto res = S.graphs.emplace(key, g);
+    out = &res.first->second;
+    return NTR_OK;
+}
+
+// Sim::run (src/sim.rs:585-648).
+static ntr_status run_batch(Sim& S, uint32_t n, uint32_t stop, uint32_t* taken) {
+    ntr_world_header& h = S.host.h;
+    S.U.limits[2] = h.iters;
+    S.U.limits[3] = stop;
+    S.U.mem[1] = h.substeps;
+    S.U.mem[2] = h.air_substeps;
+    ntr_status r = push_params(S);
+    if (r != NTR_OK) return r;
+    // iters_max and unconverged count per batch.
+    CU(cudaMemsetAsync(&S.D.st->s.iters_max, 0, 8, S.stream));
+    StepGraph* g = nullptr;
+    if ((r = get_graph(S, g)) != NTR_OK) return r;
+    const uint32_t before = S.h_state->s.step;
+    CU(cudaEventRecord(S.ev0, S.stream));
+    for (uint32_t k = 0; k < n; k++) CU(cudaGraphLaunch(g->exec, S.stream));
+    CU(cudaEventRecord(S.ev1, S.stream));
+    if ((r = read_state(S)) != NTR_OK) return r;
+    float ms = 0.0f;
+    CU(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
+    S.last_ms = ms;
+    S.last_launches = g->launches * n;
+    S.step_ms = n ? ms / n : 0.0;
+    const ntr_state& s = S.h_state->s;
+    if (taken) *taken = s.step - before;
+    if (s.overflow) return fail(NTR_E_OVERFLOW, "the water needs more than " + std::to_string(h.block_cap) + " grid blocks");
+    if (S.h_state->err) return fail(NTR_E_TIMEOUT, "a bounded device-side wait gave up");
+    adapt_after_batch(h, s);
+    return NTR_OK;
+}
+
+static ntr_status create_from(const World& w, int device, Sim*& out) {
+    ntr_status r = check_device(device);
+    if (r != NTR_OK) return r;
+    CU(cudaSetDevice(device));
+    std::unique_ptr<Sim> S(new Sim);
+    S->device = device;
+    S->host.h = w.h;
+    S->U = w.h.params;
+    cudaDeviceProp prop;
+    CU(cudaGetDeviceProperties(&prop, device));
+    S->sms = prop.multiProcessorCount;
+    if (prop.major < 10) return fail(NTR_E_NODEVICE, "this library is built for sm_100a (B200); device is sm_" + std::to_string(prop.major * 10 + prop.minor));
+    CU(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    CU(cudaEventCreate(&S->ev0));
+    CU(cudaEventCreate(&S->ev1));
+    CU(cudaMallocHost((void**)&S->h_state, sizeof(DevState)));
+    if ((r = allocate(*S)) != NTR_OK) return r;
+    if ((r = upload_static(*S, w)) != NTR_OK) return r;
+    if ((r = upload_state(*S, w)) != NTR_OK) return r;
+    if ((r = push_params(*S)) != NTR_OK) return r;
+    if ((r = read_state(*S)) != NTR_OK) return r;
+    if (S->host.h.substeps == 0)
+        if ((r = measure_rubber(*S)) != NTR_OK) return r;
+    out = S.release();
+    return NTR_OK;
+}
+
+// ---- snapshot -------------------------------------------------------------------------------------
+static ntr_status snapshot(Sim& S, std::vector<uint8_t>& blob) {
+    Dev& D = S.D;
+    ntr_status r = read_state(S);
+    if (r != NTR_OK) return r;
+    World w;
+    w.h = S.host.h;
+    w.h.params = S.U;
+    const DevState& ds = *S.h_state;
+    w.h.state = ds.s;
+    w.h.state.rz = (float)ds.rz, w.h.state.alpha = (float)ds.alpha, w.h.state.beta = (float)ds.beta;
+    w.h.state.b_norm = (float)ds.b_norm, w.h.state.r_norm = (float)ds.r_norm;
+    const uint32_t nb = std::min(ds.s.n_blocks, D.cap_blocks);
+    w.h.n_blocks_prev = nb;
+    w.h.n_spray = std::min(ds.s.spray_count, D.spray_cap);
+    w.shape_sections();
+    {
+        std::vector<float4> a[5];
+        float4* src[5] = {D.pos, D.vel, D.c0, D.c1, D.c2};
+        for (int k = 0; k < 5; k++) {
+            a[k].resize(D.Np);
+            CU(cudaMemcpy(a[k].data(), src[k], (size_t)D.Np * 16, cudaMemcpyDeviceToHost));
+        }
+        float* p = w.as<float>(NTR_SEC_PARTICLES);
+        for (uint32_t i = 0; i < D.Np; i++)
+            for (int k = 0; k < 5; k++) std::memcpy(p + 20 * (size_t)i + 4 * k, &a[k][i], 16);
+    }
+    auto dl = [&](int sec, const void* src) -> ntr_status {
+        if (!w.sec[sec].empty()) CU(cudaMemcpy(w.sec[sec].data(), src, w.sec[sec].size(), cudaMemcpyDeviceToHost));
+        return NTR_OK;
+    };
+    if ((r = dl(NTR_SEC_MEM_X, D.mem_x[0])) || (r = dl(NTR_SEC_MEM_V, D.mem_v[0])) || (r = dl(NTR_SEC_MEM_MASS, D.mem_mass)) ||
+        (r = dl(NTR_SEC_MEM_WATER, D.mem_water)) || (r = dl(NTR_SEC_MEM_LAYER, D.mem_layer)) || (r = dl(NTR_SEC_MEM_PUSH, D.mem_push)) ||
+        (r = dl(NTR_SEC_TRIS, D.tris)) || (r = dl(NTR_SEC_ALIVE, D.alive)) || (r = dl(NTR_SEC_VTRI_OFF, D.vtri_off)) ||
+        (r = dl(NTR_SEC_VTRI, D.vtri)) || (r = dl(NTR_SEC_BULLETS, D.bullets)) || (r = dl(NTR_SEC_PATCHES, D.patches)) ||
+        (r = dl(NTR_SEC_OUTLINES, D.outlines)) || (r = dl(NTR_SEC_SECTIONS, D.sections)) || (r = dl(NTR_SEC_BULLET_HIT, D.bullet_hit)) ||
+        (r = dl(NTR_SEC_POSE_LOG, D.pose_log)) || (r = dl(NTR_SEC_SPRAY, D.spray)) || (r = dl(NTR_SEC_LANDED, D.landed)) ||
+        (r = dl(NTR_SEC_TOUCH, D.touch)))
+        return r;
+    const int cur = (int)(ds.s.step & 1u);
+    if (nb) {
+        CU(cudaMemcpy(w.sec[NTR_SEC_BLOCKS_PREV].data(), D.block_list[cur], (size_t)nb * 4, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(w.sec[NTR_SEC_BLOCK_ACTIVE].data(), D.block_active, (size_t)nb * 4, cudaMemcpyDeviceToHost));
+        float* af = w.as<float>(NTR_SEC_AIR);
+        for (uint32_t f = 0; f < NTR_AIR_FIELDS; f++)
+            CU(cudaMemcpy(af + (size_t)f * nb * 64, D.air[0] + (size_t)f * D.cap_cells, (size_t)nb * 64 * 4, cudaMemcpyDeviceToHost));
+    }
+    blob = serialize(w);
+    return NTR_OK;
+}
+
+}  // namespace ntr
+
+using namespace ntr;
+
+struct ntr_sim {
+    Sim* s;
+};
+
+#define GUARD(sim)                                             \
+    if (!(sim) || !(sim)->s) return fail(NTR_E_INVALID, "null simulation handle"); \
+    Sim& S = *(sim)->s;                                        \
+    if (cudaSetDevice(S.device) != cudaSuccess) return fail(NTR_E_CUDA, "cudaSetDevice failed")
+
+extern "C" {
+
+NTR_API ntr_status ntr_sim_create_from_world(const void* blob, size_t len, int device, ntr_sim** out) {
+    if (!blob || !out) return fail(NTR_E_INVALID, "null argument");
+    World w;
+    std::string err;
+    if (!deserialize(blob, len, w, err)) return fail(NTR_E_INVALID, err);
+    Sim* s = nullptr;
+    ntr_status r = create_from(w, device, s);
+    if (r != NTR_OK) return r;
+    *out = new ntr_sim{s};
+    clear_error();
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_sim_create(const ntr_sim_params* p, int device, ntr_sim** out) {
+    if (!p || !out) return fail(NTR_E_INVALID, "null argument");
+    ntr_status r = check_device(device);
+    if (r != NTR_OK) return r;
+    World w;
+    std::string err;
+    if (!build_world(*p, w, err)) return fail(NTR_E_INVALID, err);
+    Sim* s = nullptr;
+    if ((r = create_from(w, device, s)) != NTR_OK) return r;
+    *out = new ntr_sim{s};
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_sim_destroy(ntr_sim* sim) {
+    if (!sim) return NTR_OK;
+    delete sim->s;
+    delete sim;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_sim_step(ntr_sim* sim, uint32_t n, uint32_t stop_ns, uint32_t* taken) {
+    GUARD(sim);
+    if (n == 0) {
+        if (taken) *taken = 0;
+        return NTR_OK;
+    }
+    return run_batch(S, n, stop_ns, taken);
+}
+
+NTR_API ntr_status ntr_sim_advance(ntr_sim* sim, double t_target, uint32_t budget, uint32_t* taken_out) {
+    GUARD(sim);
+    ntr_world_header& h = S.host.h;
+    uint32_t taken = 0;
+    if (!h.started) {
+        if (t_target < h.t0) {
+            h.t = std::max(t_target, h.t_start);
+            if (taken_out) *taken_out = 0;
+            return NTR_OK;
+        }
+        h.started = 1;
+        h.t = h.t0;
+    }
+    const double span = std::min(t_target - h.t0, 4.0);
+    const uint32_t stop = (uint32_t)std::llround(std::max(span, 0.0) * 1e9);
+    ntr_status r = NTR_OK;
+    while (taken < budget && S.h_state->s.t_ns < stop) {
+        const ntr_state& s = S.h_state->s;
+        uint32_t dt = s.free_dt_ns > 0 ? s.free_dt_ns : (uint32_t)(S.U.fluid[2] * 1e9f);
+        if (dt == 0) dt = 1;
+        size_t fit = S.step_ms > 0.0 ? (size_t)(4.0 / S.step_ms) : 1;
+        size_t want = (size_t)((stop - s.t_ns + dt - 1) / dt);
+        size_t cap = std::min<size_t>(budget - taken, 256);
+        cap = std::min(cap, std::max<size_t>(fit, 1));
+        uint32_t n = (uint32_t)std::clamp<size_t>(want, 1, std::max<size_t>(cap, 1));
+        uint32_t got = 0;
+        if ((r = run_batch(S, n, stop, &got)) != NTR_OK) break;
+        taken += got;
+        if (got == 0) break;
+    }
+    h.t = h.t0 + (double)S.h_state->s.t_ns * 1e-9;
+    if (taken_out) *taken_out = taken;
+    return r;
+}
+
+NTR_API ntr_status ntr_sim_read_state(ntr_sim* sim, ntr_state* out) {
+    GUARD(sim);
+    if (!out) return fail(NTR_E_INVALID, "null argument");
+    ntr_status r = read_state(S);
+    if (r != NTR_OK) return r;
+    *out = S.h_state->s;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_sim_info_get(ntr_sim* sim, ntr_sim_info* out) {
+    GUARD(sim);
+    if (!out) return fail(NTR_E_INVALID, "null argument");
+    const ntr_world_header& h = S.host.h;
+    std::memset(out, 0, sizeof *out);
+    out->n_particles = h.n_particles, out->n_verts = h.n_verts, out->n_tris = h.n_tris, out->n_shots = h.n_shots;
+    for (int k = 0; k < 3; k++) out->dims[k] = S.U.dims[k], out->grid_origin[k] = S.U.origin[k];
+    out->block_cap = h.block_cap, out->spray_cap = h.spray_cap;
+    out->iters = h.iters, out->substeps = h.substeps, out->air_substeps = h.air_substeps;
+    out->dx = h.dx, out->spacing = S.U.fluid[3];
+    out->t = h.t, out->t_start = h.t_start, out->t0 = h.t0;
+    out->device_bytes = S.device_bytes;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_sim_buffer(ntr_sim* sim, ntr_buf which, void** dev_ptr, size_t* bytes) {
+    GUARD(sim);
+    Dev& D = S.D;
+    const int cur = (int)(S.h_state->s.step & 1u);
+    void* p = nullptr;
+    size_t b = 0;
+    switch (which) {
+        case NTR_BUF_PARTICLES: p = D.pos, b = (size_t)D.Np * 80; break;
+        case NTR_BUF_STATE: p = D.st, b = sizeof(ntr_state); break;
+        case NTR_BUF_MEM_POS: p = D.mem_x[0], b = (size_t)D.Nv * 16; break;
+        case NTR_BUF_TRIS: p = (void*)D.tris, b = (size_t)D.Nt * 32; break;
+        case NTR_BUF_ALIVE: p = D.alive, b = (size_t)D.Nt * 4; break;
+        case NTR_BUF_VTRI_OFF: p = D.vtri_off, b = ((size_t)D.Nv + 1) * 4; break;
+        case NTR_BUF_VTRI: p = D.vtri, b = (size_t)S.host.h.n_vtri * 4; break;
+        case NTR_BUF_SPRAY: p = D.spray, b = (size_t)D.spray_cap * 48; break;
+        case NTR_BUF_TOUCH: p = D.touch, b = (size_t)D.wet_res * D.wet_res * 4; break;
+        case NTR_BUF_LANDED: p = D.landed, b = (size_t)D.spray_cap * 16; break;
+        case NTR_BUF_BLOCK_LIST: p = D.block_list[cur], b = (size_t)D.cap_blocks * 4; break;
+        case NTR_BUF_SORTED: p = D.sorted, b = (size_t)D.Np * 4; break;
+        case NTR_BUF_BLOCK_START: p = D.block_start, b = ((size_t)D.cap_blocks + 1) * 4; break;
+        case NTR_BUF_ACC: p = D.acc, b = (size_t)NTR_ACC_FIELDS * D.cap_cells * 4; break;
+        case NTR_BUF_CF: p = D.cf, b = (size_t)NTR_CELL_FIELDS * D.cap_cells * 4; break;
+        case NTR_BUF_AIR: p = D.air[0], b = (size_t)NTR_AIR_FIELDS * D.cap_cells * 4; break;
+        case NTR_BUF_BLOCK_NB: p = D.block_nb, b = (size_t)D.cap_blocks * 27 * 4; break;
+        default: return fail(NTR_E_INVALID, "unknown buffer");
+    }
+    if (dev_ptr) *dev_ptr = p;
+    if (bytes) *bytes = b;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_sim_download(ntr_sim* sim, ntr_buf which, void* host, size_t bytes) {
+    GUARD(sim);
+    if (!host) return fail(NTR_E_INVALID, "null argument");
+    void* p = nullptr;
+    size_t b = 0;
+    ntr_status r = ntr_sim_buffer(sim, which, &p, &b);
+    if (r != NTR_OK) return r;
+    if (which == NTR_BUF_PARTICLES) {
+        // Five float4 arrays, each n_particles long.
+        Dev& D = S.D;
+        float4* src[5] = {D.pos, D.vel, D.c0, D.c1, D.c2};
+        size_t each = (size_t)D.Np * 16;
+        for (int k = 0; k < 5 && bytes > 0; k++) {
+            size_t n = std::min(bytes, each);
+            CU(cudaMemcpy((char*)host + k * each, src[k], n, cudaMemcpyDeviceToHost));
+            bytes -= n;
+        }
+        return NTR_OK;
+    }
+    CU(cudaStreamSynchronize(S.stream));
+    CU(cudaMemcpy(host, p, std::min(bytes, b), cudaMemcpyDeviceToHost));
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_sim_snapshot(ntr_sim* sim, void* buf, size_t cap, size_t* len) {
+    GUARD(sim);
+    std::vector<uint8_t> blob;
+    ntr_status r = snapshot(S, blob);
+    if (r != NTR_OK) return r;
+    if (len) *len = blob.size();
+    if (buf) {
+        if (cap < blob.size()) return fail(NTR_E_INVALID, "snapshot buffer too small");
+        std::memcpy(buf, blob.data(), blob.size());
+    }
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_sim_restore(ntr_sim* sim, const void* blob, size_t len) {
+    GUARD(sim);
+    World w;
+    std::string err;
+    if (!deserialize(blob, len, w, err)) return fail(NTR_E_INVALID, err);
+    const ntr_world_header& a = S.host.h;
+    if (w.h.n_particles != a.n_particles || w.h.n_verts != a.n_verts || w.h.n_tris != a.n_tris || w.h.block_cap != a.block_cap ||
+        w.h.spray_cap != a.spray_cap || w.h.wet_res != a.wet_res || std::memcmp(w.h.params.bdims, a.params.bdims, 16) != 0)
+        return fail(NTR_E_INVALID, "world blob is of a different scene size");
+    CU(cudaStreamSynchronize(S.stream));
+    S.host.h = w.h;
+    S.U = w.h.params;
+    ntr_status r;
+    if ((r = upload_static(S, w)) != NTR_OK) return r;
+    if ((r = upload_state(S, w)) != NTR_OK) return r;
+    if ((r = push_params(S)) != NTR_OK) return r;
+    if ((r = read_state(S)) != NTR_OK) return r;
+    if (S.host.h.substeps == 0)
+        if ((r = measure_rubber(S)) != NTR_OK) return r;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_sim_set_precision(ntr_sim* sim, int fp64_reductions) {
+    GUARD(sim);
+    S.fp64 = fp64_reductions ? 1u : 0u;
+    S.D.fp64_dots = S.fp64;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_sim_last_launches(ntr_sim* sim, uint64_t* launches, double* device_ms) {
+    GUARD(sim);
+    if (launches) *launches = S.last_launches;
+    if (device_ms) *device_ms = S.last_ms;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_sim_conservation(ntr_sim* sim, double out[8]) {
+    GUARD(sim);
+    if (!out) return fail(NTR_E_INVALID, "null argument");
+    double* d = nullptr;
+    CU(cudaMallocAsync((void**)&d, 64, S.stream));
+    CU(cudaMemsetAsync(d, 0, 64, S.stream));
+    k_conservation<<<S.sms * 4, 256, 0, S.stream>>>(S.D, d);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(out, d, 64, cudaMemcpyDeviceToHost, S.stream));
+    CU(cudaFreeAsync(d, S.stream));
+    CU(cudaStreamSynchronize(S.stream));
+    return NTR_OK;
+}
+
+}  // extern "C"

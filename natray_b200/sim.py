@@ -1,0 +1,130 @@
+"""`Sim`: the reference's simulation surface (src/sim.rs:149-522) on one B200, through the C ABI.
+
+    sim = Sim(Params(resolution=64))         # Sim::new
+    sim.advance(t_target=0.001, budget=64)   # Sim::advance
+    sim.step(n, stop_ns)                     # Sim::run: one batch
+    sim.state                                # the State read back after a batch
+
+The product path is the CUDA library only: there is no CPU fallback, and a machine without a
+B200 gets NatrayError(NTR_E_NODEVICE).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import BUF, check, lib
+from .world import Params, World, build_world
+
+
+class Sim:
+    def __init__(self, params: Params | None = None, *, world: World | bytes | None = None, device: int = 0,
+                 fp64_reductions: bool = True):
+        self._h = C.c_void_p()
+        if world is None:
+            world = build_world(params if params is not None else Params())
+        blob = bytes(world.blob) if isinstance(world, World) else bytes(world)
+        check(lib().ntr_sim_create_from_world(blob, len(blob), device, C.byref(self._h)))
+        if not fp64_reductions:
+            check(lib().ntr_sim_set_precision(self._h, 0))
+        self.info = self._info()
+
+    # -- lifetime ---------------------------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            lib().ntr_sim_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- stepping ---------------------------------------------------------------------------
+    def step(self, n: int, stop_ns: int = 0xFFFFFFFF) -> int:
+        """One batch of up to `n` steps that stops at `stop_ns` (Sim::run)."""
+        taken = C.c_uint32()
+        check(lib().ntr_sim_step(self._h, n, stop_ns, C.byref(taken)))
+        return taken.value
+
+    def advance(self, t_target: float, budget: int) -> int:
+        """Runs to `t_target` (s, the reference's timeline) in at most `budget` steps."""
+        taken = C.c_uint32()
+        check(lib().ntr_sim_advance(self._h, t_target, budget, C.byref(taken)))
+        return taken.value
+
+    # -- reading back -----------------------------------------------------------------------
+    @property
+    def state(self) -> dict:
+        s = _abi.State()
+        check(lib().ntr_sim_read_state(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def _info(self) -> _abi.SimInfo:
+        i = _abi.SimInfo()
+        check(lib().ntr_sim_info_get(self._h, C.byref(i)))
+        return i
+
+    def snapshot(self) -> World:
+        n = C.c_size_t()
+        check(lib().ntr_sim_snapshot(self._h, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        check(lib().ntr_sim_snapshot(self._h, buf, n.value, C.byref(n)))
+        return World(buf.raw[: n.value])
+
+    def restore(self, world: World | bytes) -> None:
+        blob = bytes(world.blob) if isinstance(world, World) else bytes(world)
+        check(lib().ntr_sim_restore(self._h, blob, len(blob)))
+
+    def buffer(self, name: str) -> tuple[int, int]:
+        """(device pointer, bytes) of a lent buffer."""
+        p, n = C.c_void_p(), C.c_size_t()
+        check(lib().ntr_sim_buffer(self._h, BUF[name], C.byref(p), C.byref(n)))
+        return p.value or 0, n.value
+
+    def download(self, name: str, dtype=np.uint32, count: int | None = None) -> np.ndarray:
+        _, n = self.buffer(name)
+        if count is not None:
+            n = min(n, count * np.dtype(dtype).itemsize)
+        out = np.empty(n // np.dtype(dtype).itemsize, dtype=dtype)
+        check(lib().ntr_sim_download(self._h, BUF[name], out.ctypes.data, out.nbytes))
+        return out
+
+    def grid(self) -> dict:
+        """This step's grid in the layouts the oracle reports: block list, sorted particles,
+        block starts, transfer sums and cell fields of the allocated blocks."""
+        st = self.state
+        nb = min(st["n_blocks"], self.info.block_cap)
+        cap_cells = self.info.block_cap * 64
+        cells = nb * 64
+        bl = self.download("BLOCK_LIST", np.uint32, nb)
+        bs = self.download("BLOCK_START", np.uint32, nb + 1)
+        srt = self.download("SORTED", np.uint32, int(bs[-1]) if nb else 0)
+        acc = self.download("ACC", np.int32).reshape(19, cap_cells)[:, :cells].copy()
+        cf = self.download("CF", np.float32).reshape(11, cap_cells)[:, :cells].copy()
+        nbt = self.download("BLOCK_NB", np.uint32, nb * 27)
+        air = self.download("AIR", np.float32).reshape(5, cap_cells)[:, :cells].copy()
+        return {"block_list": bl, "block_start": bs, "sorted": srt, "acc": acc.reshape(-1), "cf": cf.reshape(-1),
+                "block_nb": nbt, "air": air.reshape(-1)}
+
+    def last_launches(self) -> tuple[int, float]:
+        n, ms = C.c_uint64(), C.c_double()
+        check(lib().ntr_sim_last_launches(self._h, C.byref(n), C.byref(ms)))
+        return n.value, ms.value
+
+    def conservation(self) -> np.ndarray:
+        out = (C.c_double * 8)()
+        check(lib().ntr_sim_conservation(self._h, out))
+        return np.array(out[:])
+
+
+__all__ = ["Sim"]

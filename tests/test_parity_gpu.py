@@ -1,0 +1,154 @@
+"""Parity of the CUDA step with the oracle, through the C ABI, on the same seeded inputs.
+
+Both sides run the canonical form of the reference's step (blocks by ascending slot,
+particles by ascending index within a block, spray slots in that order), the same float
+expressions without contraction, fixed-point i32 transfer sums, the same tree shapes for
+the solver's inner products, and the same float transcendentals. So the comparison is bit for
+bit: block sets, sort order and fixed-point sums as integers, every float field by its bits.
+"""
+import numpy as np
+import pytest
+
+from natray_b200 import Params, World, build_world
+from natray_b200._abi import NatrayError
+from natray_b200.sim import Sim
+from oracle.py import Oracle
+
+pytestmark = pytest.mark.gpu
+
+SECTIONS_COMPARED = ["PARTICLES", "MEM_X", "MEM_V", "MEM_WATER", "MEM_LAYER", "MEM_PUSH", "ALIVE", "BULLETS",
+                     "SECTIONS", "BULLET_HIT", "POSE_LOG", "BLOCKS_PREV", "BLOCK_ACTIVE", "AIR", "SPRAY", "LANDED", "TOUCH"]
+
+
+def small(**kw):
+    base = dict(resolution=24, mesh_level=3, block_cap=4096, spray_cap=200000)
+    base.update(kw)
+    return build_world(Params(**base))
+
+
+def measured(w: World) -> World:
+    """The world after the zero-length measuring substep, taken on the CPU so that both sides
+    start from the same substep counts."""
+    return World(Oracle(w.blob).snapshot())
+
+
+def bits(a):
+    a = np.ascontiguousarray(a)
+    return a.view(np.uint32) if a.dtype == np.float32 else a
+
+
+def first_diff(a, b):
+    a, b = bits(a).reshape(-1), bits(b).reshape(-1)
+    if a.shape != b.shape:
+        return f"shape {a.shape} vs {b.shape}"
+    d = np.nonzero(a != b)[0]
+    if d.size == 0:
+        return None
+    return f"{d.size} of {a.size} differ, first at {d[:4]}"
+
+
+def assert_worlds_equal(a: World, b: World, where: str):
+    sa, sb = a.state, b.state
+    bad = {k: (sa[k], sb[k]) for k in sa if not (sa[k] == sb[k] or (np.isnan(sa[k]) and np.isnan(sb[k])))}
+    assert not bad, f"{where}: state differs {bad}"
+    for sec in SECTIONS_COMPARED:
+        d = first_diff(a.sec(sec), b.sec(sec))
+        assert d is None, f"{where}: section {sec}: {d}"
+    assert (a.h.iters, a.h.substeps, a.h.air_substeps) == (b.h.iters, b.h.substeps, b.h.air_substeps), where
+
+
+def assert_grids_equal(o: Oracle, s: Sim, where: str):
+    g = s.grid()
+    for k in ["block_list", "block_start", "sorted", "block_nb", "acc", "cf", "air"]:
+        d = first_diff(o.get(k), g[k])
+        assert d is None, f"{where}: {k}: {d}"
+
+
+@pytest.fixture(scope="module")
+def w_small():
+    return measured(small())
+
+
+def test_first_step_is_bit_exact(w_small):
+    o, s = Oracle(w_small.blob), Sim(world=w_small)
+    assert o.step(1) == s.step(1) == 1
+    assert_grids_equal(o, s, "step 1")
+    assert_worlds_equal(World(o.snapshot()), s.snapshot(), "step 1")
+
+
+def test_batches_stay_bit_exact(w_small):
+    # Free running, through the impact: the bullet starts 5 cm out at 330 m/s.
+    o, s = Oracle(w_small.blob), Sim(world=w_small)
+    for k in range(6):
+        assert o.step(4) == s.step(4)
+        assert_worlds_equal(World(o.snapshot()), s.snapshot(), f"batch {k}")
+    assert_grids_equal(o, s, "after 24 steps")
+    st = s.state
+    assert st["step"] == 24 and st["n_blocks"] > 0
+
+
+def test_fixed_step_bb_shot_bit_exact():
+    # The small fixed-step scene: d = 8 cm, a 5,120-triangle membrane, thickness 0.2 mm, a
+    # steel sphere of 8 mm at 300 m/s, dt = 2 us. Scaled down in particle count to run in
+    # seconds on the CPU side.
+    w = measured(small(diameter=8, resolution=24, mesh_level=4, thickness=0.2, bullet=6, caliber=8,
+                       bullet_speed=300, dt_max=2e-6))
+    o, s = Oracle(w.blob), Sim(world=w)
+    for k in range(5):
+        o.step(8)
+        s.step(8)
+    a, b = World(o.snapshot()), s.snapshot()
+    assert a.state["dt_ns"] == 2000
+    assert_worlds_equal(a, b, "fixed step")
+
+
+def test_reference_fp32_sums_bit_exact(w_small):
+    o = Oracle(w_small.blob, fp64_dots=False)
+    s = Sim(world=w_small, fp64_reductions=False)
+    for _ in range(3):
+        o.step(4)
+        s.step(4)
+    assert_worlds_equal(World(o.snapshot()), s.snapshot(), "FP32 sums")
+
+
+def test_snapshot_restore_roundtrip(w_small):
+    s = Sim(world=w_small)
+    s.step(5)
+    a = s.snapshot()
+    s2 = Sim(world=a)
+    assert_worlds_equal(a, s2.snapshot(), "restore")
+    s.step(3)
+    s2.step(3)
+    assert_worlds_equal(s.snapshot(), s2.snapshot(), "after restore")
+    # Restoring a different state into a live simulation.
+    s.restore(a)
+    assert_worlds_equal(a, s.snapshot(), "restore into live")
+
+
+def test_overflow_is_reported():
+    w = measured(small(block_cap=16))
+    s = Sim(world=w)
+    with pytest.raises(NatrayError) as e:
+        s.step(1)
+    assert e.value.status == 3  # NTR_E_OVERFLOW
+
+
+def test_advance_follows_the_reference_timeline(w_small):
+    s = Sim(world=w_small)
+    info = s.info
+    taken = s.advance(info.t0 + 2e-4, 1000)
+    st = s.state
+    assert taken == st["step"] > 0
+    assert st["t_ns"] == 200000  # lands exactly on the stop time
+    assert s.advance(info.t0 + 2e-4, 1000) == 0
+
+
+def test_conservation_sums(w_small):
+    s = Sim(world=w_small)
+    c = s.conservation()
+    assert c[0] == w_small.h.n_particles
+    p = w_small.particles.astype(np.float64)
+    assert np.allclose(c[5:8], p[:, :3].sum(0), rtol=1e-6)
+    s.step(2)
+    launches, ms = s.last_launches()
+    assert launches > 40 and ms > 0
