@@ -1,0 +1,307 @@
+"""Benchmark of natray's simulation step on B200: particle-substeps/s at ~1M particles.
+
+A "step" here is one water step of the reference (one `Sim::run` step: begin_step .. g2p with
+its rubber and air substeps and its pressure iterations, src/sim.rs:553-566), which the metric
+calls a particle-substep. The workload is the full single scene at 1M particles: a 16 cm water
+balloon on a lattice of resolution 124 (976,915 particles, spacing 1.29 mm, cell 2.58 mm), an
+icosphere(6) latex membrane (40,962 vertices, 81,920 triangles), a rigid 8 mm steel sphere at
+350 m/s, a fixed step of 2 us. Inputs are synthetic (the reference's seeded scene builder).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl native|reference]
+
+Prints one JSON line (rank 0). `--impl reference` times the CPU restatement of the reference's
+step (the reference's own wgpu/WGSL path needs a graphics adapter, which this machine does
+not have) on the same scene with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+MEASURED_PEAKS = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+METRIC = "particle-substeps/s @1M"
+SCENE = dict(resolution=124, mesh_level=6, dt_max=2e-6, bullet=6, caliber=8, bullet_speed=350)
+WORKLOAD = "single scene 1M particles: d=16 cm balloon, res 124 (976,915 particles), icosphere(6) 81,920 tris, 8 mm steel sphere at 350 m/s, dt=2 us"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def hbm_peak() -> tuple[float, str]:
+    try:
+        d = json.loads(MEASURED_PEAKS.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            if self.t:
+                self.t.join(timeout=2)
+
+    def summary(self) -> dict:
+        mhz, maxs, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                maxs.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not mhz:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": max(maxs), "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def algorithmic_bytes(kernel: str, st: dict, n_particles: int, iters: int) -> float:
+    """Bytes a launch of `kernel` must move at the least: the per-unit figures of the step
+    (particle 80 B read + 80 B written; P2G reads a particle's 80 B and writes its block's tile
+    sums; the solve reads d, z, diag, type, p, r, q and writes d', q, p, r, z per water cell
+    and iteration, 48 B)."""
+    nb = st["n_blocks"]
+    if kernel.startswith("k_solve"):
+        n_water = st.get("_n_water", nb * 64)
+        return 48.0 * n_water * max(iters, 1) + 40.0 * n_water
+    if kernel == "k_p2g":
+        return 84.0 * n_particles + 8 * 4 * 343 * nb
+    if kernel == "k_g2p":
+        return (32.0 + 80.0) * n_particles + 8 * 4 * 343 * nb
+    return 0.0
+
+
+def run_native(args, rank, world, local):
+    import numpy as np
+    from natray_b200 import Params, build_world
+    from natray_b200.sim import Sim
+
+    params = Params(**SCENE)
+    w = build_world(params)
+    n_particles = w.h.n_particles
+    sim = Sim(world=w, device=local)
+    info = sim.info
+    log(f"rank {rank}: {n_particles} particles, {info.n_verts} verts, {info.n_tris} tris, dx {info.dx*1e3:.3f} mm")
+    import torch
+    use_dist = world > 1
+    if use_dist:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    def barrier():
+        if use_dist:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize(local)
+
+    # Warm-up: the first batches size the solver's iterations and the substeps, and build the
+    # step's graph.
+    for _ in range(args.warmup):
+        sim.step(1)
+    sim.step(args.warmup)
+    barrier()
+    # Device-timed region: K steps in one batch, CUDA events on the simulation's stream.
+    with Clocks(local) as clk:
+        sim.step(args.steps)
+    barrier()
+    launches, ms = sim.last_launches()
+    st = sim.state
+    t_dev = ms * 1e-3
+    if use_dist:
+        import torch.distributed as dist
+        tt = torch.tensor([t_dev], device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_dev = float(tt.item())
+    value = n_particles * args.steps * world / t_dev
+
+    # End to end through the public API: one ntr_sim_step call per step, each uploading the
+    # step's parameters from host memory and reading the state back.
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sim.step(1)
+    t_e2e = time.perf_counter() - t0
+    if use_dist:
+        import torch.distributed as dist
+        tt = torch.tensor([t_e2e], device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    e2e = n_particles * args.steps * world / t_e2e
+
+    # Roofline of the dominant kernel: kernel-by-kernel event timing of a few steps.
+    prof_steps = min(10, args.steps)
+    prof = sim.profile(prof_steps)
+    tot = sum(v[1] for v in prof.values())
+    top, (cnt, kms) = max(prof.items(), key=lambda kv: kv[1][1])
+    per_launch_s = kms / cnt * 1e-3
+    st2 = sim.state
+    cf_type = sim.download("CF", np.float32).reshape(11, -1)[10, : st2["n_blocks"] * 64]
+    st2["_n_water"] = int((cf_type == 1.0).sum())
+    iters = max(st2["solve_iters"], 1)
+    alg = algorithmic_bytes(top, st2, n_particles, iters)
+    peak, peak_kind = hbm_peak()
+    achieved = alg / per_launch_s / 1e9 if alg > 0 else None
+    traffic = None
+    tf = ROOT / "profiles" / f"{top.split('<')[0]}.md"
+    if tf.exists():
+        for line in tf.read_text().splitlines():
+            if line.startswith("traffic_per_launch_bytes:"):
+                try:
+                    traffic = float(line.split(":", 1)[1].strip())
+                except ValueError:
+                    pass
+
+    result = None
+    if rank == 0:
+        h2d = 192  # the Params uniform per call
+        d2h = 176  # the device state read back per call
+        shares = {k: round(v[1] / tot, 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])[:8]}
+        result = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "particle-substeps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": t_dev * 1e3 / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded scene builder of the reference)",
+            "config": {
+                "workload": WORKLOAD,
+                "n_particles": n_particles,
+                "n_tris": int(info.n_tris),
+                "dt_ns": st["dt_ns"],
+                "n_blocks": st["n_blocks"],
+                "solver_iters_last": st["solve_iters"],
+                "substeps": [int(sim._info().substeps), int(sim._info().air_substeps)],
+                "parallelism": f"replicas x{world}",
+                "l2": "no flush: a step moves ~170 MB of particles, sort buffers, tiles and cell fields, above the 126 MB L2",
+                "reductions": "fp64",
+            },
+            "e2e": {"value": e2e, "unit": "particle-substeps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "note": "one ntr_sim_step call per step from the host"},
+            "gpu_launches": int(launches),
+            "roofline": {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": alg, "launch_ms": per_launch_s * 1e3, "share": round(kms / tot, 4)},
+            "kernel_shares": shares,
+            "clocks": clk.summary(),
+        }
+    sim.close()
+    if use_dist:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def cpu_baseline(sample_steps: int, threads: int | None = None) -> dict:
+    """The CPU restatement of the reference's step (FP32) on this host's cores, on a bounded
+    sample of the same workload: `sample_steps` steps of the 1M scene."""
+    from natray_b200 import Params, World, build_world
+    from oracle.py import Oracle, set_threads, threads as nthreads
+    cores = threads or os.cpu_count() or 1
+    set_threads(cores)
+    w = build_world(Params(**SCENE))
+    o = Oracle(w.blob, fp64_dots=False)
+    o.step(1)  # the first step (allocation and first-touch) outside the sample
+    t0 = time.perf_counter()
+    n = o.step(sample_steps)
+    dt = time.perf_counter() - t0
+    return {"value": w.h.n_particles * n / dt, "unit": "particle-substeps/s", "cores": nthreads(), "kind": "port",
+            "sample": f"{n} steps of the 1M-particle scene after one untimed step, oracle FP32 with the reference's FP32 sums, OpenMP"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--cpu-sample", type=int, default=30, help="steps of the CPU baseline sample")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local = dist_env()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        steps = max(1, min(args.steps, args.cpu_sample))
+        cb = cpu_baseline(steps)
+        line = {"metric": METRIC, "value": cb["value"], "unit": "particle-substeps/s", "n_gpus": args.gpus, "steps": steps,
+                "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded scene builder of the reference)", "impl": "reference",
+                "config": {"workload": WORKLOAD, "parallelism": "host cores", "n_particles": None},
+                "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "particle-substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "note": "the reference's wgpu/WGSL step needs a graphics adapter (none on this box, no Rust toolchain); this is the C++ restatement of its step kernels"}
+        print(json.dumps(line), flush=True)
+        return
+
+    res = run_native(args, rank, world, local)
+    if rank == 0 and res is not None:
+        if world == 1:
+            res["cpu_baseline"] = cpu_baseline(args.cpu_sample)
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -335,6 +335,11 @@ NTR_API ntr_status ntr_sim_snapshot(ntr_sim* s, void* buf, size_t cap, size_t* l
 NTR_API ntr_status ntr_sim_restore(ntr_sim* s, const void* blob, size_t len);
 /* FP64 accumulation of the solver's inner products and residual (default on). */
 NTR_API ntr_status ntr_sim_set_precision(ntr_sim* s, int fp64_reductions);
+/* One batch as ntr_sim_step runs it, but launched kernel by kernel outside the step's graph
+ * with an event after each, and a report of device time per kernel, one text line per kernel
+ * name "name,launches,total_ms" (the reference's NATRAY_PROF, src/sim.rs:594-614, 670-689).
+ * With report == NULL only *len (the report's length) is set. */
+NTR_API ntr_status ntr_sim_profile(ntr_sim* s, uint32_t n, uint32_t stop_ns, char* report, size_t cap, size_t* len);
 /* Kernel launches made by the last ntr_sim_step call, and its device time in ms. */
 NTR_API ntr_status ntr_sim_last_launches(ntr_sim* s, uint64_t* launches, double* device_ms);
 /* Conservation sums over live particles, accumulated in FP64 on the device:

@@ -88,8 +88,10 @@ struct DevState {
     uint32_t solver_on;
     uint32_t ticket[4];  // arrival counters of the last-block reductions
     uint32_t nbrk;       // break-ups of this step
-    uint32_t err;        // bit 0: a bounded wait gave up
-    uint32_t pad[5];
+    uint32_t err;        // bit 0: a bounded grid barrier gave up
+    uint32_t bar_count;  // grid barrier of the persistent solver: arrivals
+    uint32_t bar_gen;    // and generation
+    uint32_t pad[3];
 };
 
 // Every pointer and size a kernel may need. Passed by value.
@@ -108,7 +110,7 @@ struct Dev {
     int32_t* acc;
     float* cf;
     float* air[2];
-    double *px, *py, *pz;
+    double *px, *py, *pz, *pq;
     float4* mem_x[2];
     float4* mem_v[2];
     float4 *mem_water, *mem_layer;
@@ -127,6 +129,10 @@ struct Dev {
     uint32_t* touch;
     float4 *brk_x, *brk_v;
     uint32_t *brk_count, *brk_off;
+    int32_t* tiles;     // per block: the P2G tile, 8 fields x 343 i32
+    uint32_t* tile_ok;  // per block: 1 when its tile holds this step's sums
+    uint32_t* coltot;   // radix sort: per digit, the elements with that digit
+    uint32_t* wnb;      // solver: per cell, its 6 neighbours that are water (or NONE), 8 words
 };
 
 // ---- vectors (association as written in the WGSL) ------------------------------------------

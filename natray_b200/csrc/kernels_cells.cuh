@@ -282,280 +282,6 @@ __device__ __forceinline__ float pressure_of(const Dev& D, uint32_t cell) {
     return cfv(D, F_TYPE, cell) == WATER_T ? mx(p, P_VAPOUR - P_ATM) : p;
 }
 
-constexpr int SOLVE_T = 256;  // 4 blocks of 64 cells per CTA
-
-// Symmetric red-black Gauss-Seidel, two sweeps inside the block (fluid.wgsl:390-410). All
-// threads of the CTA call it.
-__device__ __forceinline__ float precondition(float (*zl)[64], uint8_t (*wl)[64], int j, int li, float r, float diag, bool water) {
-    zl[j][li] = 0.0f;
-    wl[j][li] = water ? 1 : 0;
-    __syncthreads();
-    const int lx = li / 16, ly = (li / 4) % 4, lz = li % 4;
-    const uint32_t colour = (uint32_t)(lx + ly + lz) % 2u;
-    for (uint32_t k = 0; k < 5; k++) {
-        if (water && colour == k % 2u) {
-            float s = r;
-            if (lx > 0 && wl[j][li - 16]) s += zl[j][li - 16];
-            if (lx < 3 && wl[j][li + 16]) s += zl[j][li + 16];
-            if (ly > 0 && wl[j][li - 4]) s += zl[j][li - 4];
-            if (ly < 3 && wl[j][li + 4]) s += zl[j][li + 4];
-            if (lz > 0 && wl[j][li - 1]) s += zl[j][li - 1];
-            if (lz < 3 && wl[j][li + 1]) s += zl[j][li + 1];
-            zl[j][li] = s / diag;
-        }
-        __syncthreads();
-    }
-    return zl[j][li];
-}
-
-// The 64-wide tree of block_sum (fluid.wgsl:414-422): red[li] += red[li + off], off = 32..1.
-// The last five levels run as shuffles, which pair the same elements.
-template <class A>
-__device__ __forceinline__ A tree64(A (*red)[64], int j, int li, A v) {
-    red[j][li] = v;
-    __syncthreads();
-    A out = A(0);
-    if (li < 32) {
-        A x = red[j][li] + red[j][li + 32];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, off);
-        out = x;
-    }
-    __syncthreads();
-    return out;  // valid in li == 0
-}
-
-// total(): 256 strided sums, then the 256-wide tree (fluid.wgsl:426-439). All 256 threads.
-template <class A>
-__device__ __forceinline__ A total256(const double* part, uint32_t n, A* red) {
-    A s = A(0);
-    for (uint32_t i = threadIdx.x; i < n; i += 256) s = s + (A)part[i];
-    red[threadIdx.x] = s;
-    __syncthreads();
-    for (int off = 128; off >= 32; off >>= 1) {
-        if ((int)threadIdx.x < off) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + off];
-        __syncthreads();
-    }
-    if (threadIdx.x < 32) {
-        A x = red[threadIdx.x];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, off);
-        if (threadIdx.x == 0) red[0] = x;
-    }
-    __syncthreads();
-    A r = red[0];
-    __syncthreads();
-    return r;
-}
-
-// Arrival at the end of a kernel whose per-block partials the last CTA sums. True in the last.
-__device__ __forceinline__ bool last_cta(DevState* st, int k) {
-    __shared__ uint32_t s_last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t t = atomicAdd(&st->ticket[k], 1u);
-        s_last = (t == gridDim.x - 1) ? 1u : 0u;
-    }
-    __syncthreads();
-    bool last = s_last != 0;
-    if (last) __threadfence();
-    return last;
-}
-
-__device__ __forceinline__ bool converged_fp64(const DevState* st, double rr, float tol) {
-    return sqrt(rr) <= (double)tol * fmax(st->b_norm, 1.0);
-}
-__device__ __forceinline__ bool converged_fp32(const DevState* st, float rr, float tol) {
-    return sqrtf(rr) <= tol * mx((float)st->b_norm, 1.0f);
-}
-
-template <bool FP64>
-__global__ void __launch_bounds__(SOLVE_T) k_solve_init(Dev D) {
-    using A = typename std::conditional<FP64, double, float>::type;
-    DevState* st = D.st;
-    if (st->s.dt_ns == 0) return;
-    const Grid g = grid_of(D, cur_of(st));
-    const ntr_gpu_params* U = D.U;
-    const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
-    const int j = threadIdx.x >> 6, li = threadIdx.x & 63;
-    __shared__ float zl[4][64];
-    __shared__ uint8_t wl[4][64];
-    __shared__ A red[4][64];
-    const float hh = g.h, dt = dt_of(st);
-    const float rho = U->fluid[0];
-    for (uint32_t b0 = blockIdx.x * 4u; b0 < nb; b0 += gridDim.x * 4u) {
-        const uint32_t b = b0 + j;
-        const uint32_t cell = b * 64u + li;
-        const bool active = b < nb;
-        const bool water = active && cfv(D, F_TYPE, cell) == WATER_T;
-        float diag = 1.0f, r = 0.0f, bq = 0.0f;
-        if (water) {
-            float cs = U->gravity[3] * dt;
-            float kc = hh * hh / (cs * cs);
-            float div = 0.0f, off = 0.0f;
-            diag = kc;
-            bq = kc * cfv(D, F_P, cell);
-            for (uint32_t d = 0; d < 3; d++) {
-                div += face_u(D, neighbour(g, cell, ed(d, 1)), cell, d) - face_u(D, cell, neighbour(g, cell, ed(d, -1)), d);
-                for (int s = -1; s <= 1; s += 2) {
-                    uint32_t nbc = neighbour(g, cell, ed(d, s));
-                    float nt = cell_type(D, nbc);
-                    if (nt == SOLID_T) continue;
-                    diag += 1.0f;
-                    if (nt == WATER_T)
-                        off -= cfv(D, F_P, nbc);
-                    else
-                        bq += pressure_of(D, nbc);
-                }
-            }
-            div -= from_fp(accv(D, A_SRC, cell), FP_Q) / (hh * hh);
-            bq -= rho * hh / dt * div;
-            r = bq - diag * cfv(D, F_P, cell) - off;
-            *cfp(D, F_DIAG, cell) = diag;
-            *cfp(D, F_R, cell) = r;
-        }
-        float z = precondition(zl, wl, j, li, r, diag, water);
-        if (water) *cfp(D, F_Z, cell) = z;
-        A vx, vy, vz;
-        if (FP64) {
-            vx = (A)((double)r * (double)z), vy = (A)((double)r * (double)r), vz = (A)((double)bq * (double)bq);
-        } else {
-            vx = (A)(r * z), vy = (A)(r * r), vz = (A)(bq * bq);
-        }
-        A sx = tree64(red, j, li, vx);
-        A sy = tree64(red, j, li, vy);
-        A sz = tree64(red, j, li, vz);
-        if (li == 0 && active) D.px[b] = (double)sx, D.py[b] = (double)sy, D.pz[b] = (double)sz;
-    }
-    if (!last_cta(st, 0)) return;
-    __shared__ A tred[256];
-    A sx = total256<A>(D.px, nb, tred);
-    A sy = total256<A>(D.py, nb, tred);
-    A sz = total256<A>(D.pz, nb, tred);
-    if (threadIdx.x == 0) {
-        st->ticket[0] = 0;
-        const float tol = U->solve[0];
-        st->rz = (double)sx;
-        st->beta = 0.0;
-        bool conv;
-        if (FP64) {
-            st->b_norm = sqrt((double)sz);
-            st->r_norm = sqrt((double)sy);
-            conv = converged_fp64(st, (double)sy, tol);
-        } else {
-            st->b_norm = (double)sqrtf((float)sz);
-            st->r_norm = (double)sqrtf((float)sy);
-            conv = converged_fp32(st, (float)sy, tol);
-        }
-        st->s.solve_iters = 0;
-        st->solver_on = ((double)sx > 0.0 && !conv) ? 1u : 0u;
-        st->s.rz = (float)st->rz, st->s.beta = 0.0f, st->s.b_norm = (float)st->b_norm, st->s.r_norm = (float)st->r_norm;
-    }
-}
-
-template <bool FP64>
-__global__ void __launch_bounds__(SOLVE_T) k_solve_q(Dev D) {
-    using A = typename std::conditional<FP64, double, float>::type;
-    DevState* st = D.st;
-    if (st->s.dt_ns == 0 || st->solver_on == 0) return;
-    const Grid g = grid_of(D, cur_of(st));
-    const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
-    const int j = threadIdx.x >> 6, li = threadIdx.x & 63;
-    __shared__ A red[4][64];
-    const uint32_t old = st->s.solve_iters % 2u;
-    const float beta = (float)st->beta;
-    for (uint32_t b0 = blockIdx.x * 4u; b0 < nb; b0 += gridDim.x * 4u) {
-        const uint32_t b = b0 + j;
-        const uint32_t cell = b * 64u + li;
-        A v = A(0);
-        if (b < nb && cfv(D, F_TYPE, cell) == WATER_T) {
-            float dn = cfv(D, F_Z, cell) + beta * cfv(D, F_D + old, cell);
-            float q = cfv(D, F_DIAG, cell) * dn;
-            for (uint32_t d = 0; d < 3; d++)
-                for (int k = -1; k <= 1; k += 2) {
-                    uint32_t nbc = neighbour(g, cell, ed(d, k));
-                    if (cell_type(D, nbc) == WATER_T) q -= cfv(D, F_Z, nbc) + beta * cfv(D, F_D + old, nbc);
-                }
-            *cfp(D, F_D + 1 - old, cell) = dn;
-            *cfp(D, F_Q, cell) = q;
-            v = FP64 ? (A)((double)dn * (double)q) : (A)(dn * q);
-        }
-        A s = tree64(red, j, li, v);
-        if (li == 0 && b < nb) D.px[b] = (double)s;
-    }
-    if (!last_cta(st, 1)) return;
-    __shared__ A tred[256];
-    A s = total256<A>(D.px, nb, tred);
-    if (threadIdx.x == 0) {
-        st->ticket[1] = 0;
-        if (FP64)
-            st->alpha = (double)s > 0.0 ? st->rz / (double)s : 0.0;
-        else
-            st->alpha = (float)s > 0.0f ? (double)((float)st->rz / (float)s) : 0.0;
-        st->s.alpha = (float)st->alpha;
-    }
-}
-
-template <bool FP64>
-__global__ void __launch_bounds__(SOLVE_T) k_solve_update(Dev D) {
-    using A = typename std::conditional<FP64, double, float>::type;
-    DevState* st = D.st;
-    if (st->s.dt_ns == 0 || st->solver_on == 0) return;
-    const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
-    const int j = threadIdx.x >> 6, li = threadIdx.x & 63;
-    __shared__ float zl[4][64];
-    __shared__ uint8_t wl[4][64];
-    __shared__ A red[4][64];
-    const uint32_t old = st->s.solve_iters % 2u;
-    const float a = (float)st->alpha;
-    for (uint32_t b0 = blockIdx.x * 4u; b0 < nb; b0 += gridDim.x * 4u) {
-        const uint32_t b = b0 + j;
-        const uint32_t cell = b * 64u + li;
-        const bool water = b < nb && cfv(D, F_TYPE, cell) == WATER_T;
-        float diag = 1.0f, r = 0.0f;
-        if (water) {
-            *cfp(D, F_P, cell) = cfv(D, F_P, cell) + a * cfv(D, F_D + 1 - old, cell);
-            r = cfv(D, F_R, cell) - a * cfv(D, F_Q, cell);
-            *cfp(D, F_R, cell) = r;
-            diag = cfv(D, F_DIAG, cell);
-        }
-        float z = precondition(zl, wl, j, li, r, diag, water);
-        if (water) *cfp(D, F_Z, cell) = z;
-        A vx = FP64 ? (A)((double)r * (double)z) : (A)(r * z);
-        A vy = FP64 ? (A)((double)r * (double)r) : (A)(r * r);
-        A sx = tree64(red, j, li, vx);
-        A sy = tree64(red, j, li, vy);
-        if (li == 0 && b < nb) D.px[b] = (double)sx, D.py[b] = (double)sy;
-    }
-    if (!last_cta(st, 2)) return;
-    __shared__ A tred[256];
-    A sx = total256<A>(D.px, nb, tred);
-    A sy = total256<A>(D.py, nb, tred);
-    if (threadIdx.x == 0) {
-        st->ticket[2] = 0;
-        const float tol = D.U->solve[0];
-        st->s.solve_iters += 1;
-        bool done;
-        if (FP64) {
-            st->r_norm = sqrt((double)sy);
-            st->beta = st->rz > 0.0 ? (double)sx / st->rz : 0.0;
-            done = converged_fp64(st, (double)sy, tol);
-        } else {
-            st->r_norm = (double)sqrtf((float)sy);
-            st->beta = st->rz > 0.0 ? (double)((float)sx / (float)st->rz) : 0.0;
-            done = converged_fp32(st, (float)sy, tol);
-        }
-        st->rz = (double)sx;
-        if (done || st->s.solve_iters >= D.U->limits[2]) {
-            st->s.iters_max = max(st->s.iters_max, st->s.solve_iters);
-            st->s.unconverged += done ? 0u : 1u;
-            st->solver_on = 0u;
-        }
-        st->s.rz = (float)st->rz, st->s.beta = (float)st->beta, st->s.r_norm = (float)st->r_norm;
-    }
-}
-
 // ---- project, extend, fluid.wgsl:580-674 -------------------------------------------------------------
 __global__ void k_project(Dev D) {
     const DevState* st = D.st;

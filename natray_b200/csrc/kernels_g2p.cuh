@@ -117,7 +117,7 @@ __device__ __forceinline__ Gathered gather(const float* tg, V3 X, V3 o, I3 corne
 
 constexpr int G2P_T = 256;
 
-__global__ void __launch_bounds__(G2P_T) k_g2p(Dev D) {
+__global__ void __launch_bounds__(G2P_T, 3) k_g2p(Dev D) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));

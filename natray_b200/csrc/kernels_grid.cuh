@@ -64,9 +64,12 @@ __global__ void k_clear(Dev D) {
     const uint32_t ncell = st->s.n_blocks_prev * 64u;
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    for (size_t i = tid; i < (size_t)ncell * NTR_ACC_FIELDS; i += stride) {
+    // Fields 0..7 are written whole by k_p2g_gather and A_N by k_p2g; the rest accumulate
+    // atomically and start from zero.
+    constexpr uint32_t F0 = A_MF, NF = NTR_ACC_FIELDS - A_MF;
+    for (size_t i = tid; i < (size_t)ncell * NF; i += stride) {
         size_t f = i / ncell, c = i - f * ncell;
-        D.acc[f * D.cap_cells + c] = 0;
+        D.acc[(F0 + f) * D.cap_cells + c] = 0;
     }
     uint32_t* m = D.mask[cur];
     for (size_t w = tid; w < D.nwords; w += stride) m[w] = 0u;
@@ -248,39 +251,44 @@ __global__ void __launch_bounds__(RADIX_T) k_radix_hist(Dev D, const uint32_t* k
     D.hist[threadIdx.x * D.n_tiles + blockIdx.x] = h[threadIdx.x];
 }
 
-// Exclusive scan of the digit-major histogram (256 x n_tiles), one CTA.
-__global__ void __launch_bounds__(1024) k_radix_scan(Dev D) {
-    if (D.st->s.dt_ns == 0) return;
-    const uint32_t n = 256u * D.n_tiles;
-    const uint32_t per = (n + 1023u) / 1024u;
-    uint32_t lo = threadIdx.x * per, hi = min(lo + per, n);
-    uint32_t s = 0;
-    for (uint32_t i = lo; i < hi; i++) s += D.hist[i];
-    __shared__ uint32_t ws[32];
-    uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    uint32_t inc = s;
+// Exclusive scan of 256 values held one per thread of a 256-thread CTA; returns the thread's
+// exclusive prefix and sets *total.
+__device__ __forceinline__ uint32_t cta_scan256(uint32_t v, uint32_t* total) {
+    __shared__ uint32_t ws[8];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t inc = v;
     for (int o = 1; o < 32; o <<= 1) {
-        uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= (uint32_t)o) inc += v;
+        uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= (uint32_t)o) inc += y;
     }
     if (lane == 31) ws[warp] = inc;
     __syncthreads();
-    if (warp == 0) {
-        uint32_t v = ws[lane];
-        uint32_t x = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= (uint32_t)o) x += y;
-        }
-        ws[lane] = x - v;
+    uint32_t before = 0, all = 0;
+    for (uint32_t w = 0; w < 8; w++) {
+        if (w < warp) before += ws[w];
+        all += ws[w];
     }
     __syncthreads();
-    uint32_t run = ws[warp] + inc - s;
-    for (uint32_t i = lo; i < hi; i++) {
-        uint32_t c = D.hist[i];
-        D.hist[i] = run;
-        run += c;
+    *total = all;
+    return before + inc - v;
+}
+
+// The digit-major histogram (digit, then tile): CTA d scans its digit's column of tile
+// counts into offsets within the digit, and records the digit's total.
+__global__ void __launch_bounds__(256) k_radix_scan(Dev D) {
+    if (D.st->s.dt_ns == 0) return;
+    const uint32_t d = blockIdx.x, nt = D.n_tiles;
+    uint32_t* col = D.hist + (size_t)d * nt;
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < nt; base += 256) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < nt ? col[i] : 0u;
+        uint32_t total;
+        const uint32_t ex = cta_scan256(v, &total);
+        if (i < nt) col[i] = carry + ex;
+        carry += total;
     }
+    if (threadIdx.x == 0) D.coltot[d] = carry;
 }
 
 __global__ void __launch_bounds__(RADIX_T) k_radix_scatter(Dev D, const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
@@ -290,7 +298,11 @@ __global__ void __launch_bounds__(RADIX_T) k_radix_scatter(Dev D, const uint32_t
     __shared__ uint32_t s_run[256];
     __shared__ uint32_t s_wh[RADIX_T / 32][256];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    s_base[threadIdx.x] = D.hist[threadIdx.x * D.n_tiles + blockIdx.x];
+    {
+        uint32_t total;
+        const uint32_t digit_base = cta_scan256(D.coltot[threadIdx.x], &total);
+        s_base[threadIdx.x] = digit_base + D.hist[threadIdx.x * D.n_tiles + blockIdx.x];
+    }
     s_run[threadIdx.x] = 0;
     const uint32_t base = blockIdx.x * RADIX_TILE;
     for (int r = 0; r < RADIX_ITEMS; r++) {
@@ -380,7 +392,7 @@ __global__ void __launch_bounds__(P2G_T) k_p2g(Dev D) {
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
     const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
-    __shared__ int32_t tile[8 * TILE];
+    __shared__ __align__(16) int32_t tile[8 * TILE];
     __shared__ uint32_t own[64];
     __shared__ uint32_t links[27];
     const float hh = g.h;
@@ -398,13 +410,20 @@ __global__ void __launch_bounds__(P2G_T) k_p2g(Dev D) {
         const uint32_t count = D.block_start[b + 1] - first;
         if (count == 0) {
             if (threadIdx.x < 64) D.acc[(size_t)A_N * D.cap_cells + b * 64u + threadIdx.x] = 0;
+            if (threadIdx.x == 0) D.tile_ok[b] = 0u;
             __syncthreads();
             continue;
         }
         for (uint32_t t = threadIdx.x; t < 8 * TILE; t += P2G_T) tile[t] = 0;
         __syncthreads();
         const I3 corner = bc * 4 - I3{1, 1, 1};
-        for (uint32_t k = threadIdx.x; k < count; k += P2G_T) {
+        // Within a round of 256, lane l of warp w takes particle 8 l + w: a block's particles
+        // are in lattice order, so consecutive ones share a cell and would add to the same
+        // tile entries; 8 apart they mostly do not. (Sums are integer: any order is the same.)
+        const uint32_t perm = (threadIdx.x & 31u) * 8u + (threadIdx.x >> 5);
+        for (uint32_t base = 0; base < count; base += P2G_T) {
+            const uint32_t k = base + perm;
+            if (k >= count) continue;
             uint32_t i = D.sorted[first + k];
             float4 pos = D.pos[i], vel = D.vel[i], c0 = D.c0[i], c1 = D.c1[i], c2 = D.c2[i];
             V3 x = (xyz(pos) - g.org) / hh;
@@ -416,17 +435,47 @@ __global__ void __launch_bounds__(P2G_T) k_p2g(Dev D) {
             atomicAdd(&own[l.x * 16 + l.y * 4 + l.z], 1u);
         }
         __syncthreads();
-        for (uint32_t t = threadIdx.x; t < TILE; t += P2G_T) {
-            uint32_t cell = tile_cell(links, t);
-            if (cell == NONE) continue;
+        // The tile goes out whole, with plain coalesced stores; k_p2g_gather sums the tiles
+        // that overlap each cell.
+        int4* dst = reinterpret_cast<int4*>(D.tiles + (size_t)b * 8 * TILE);
+        const int4* srcv = reinterpret_cast<const int4*>(tile);
+        for (uint32_t t = threadIdx.x; t < 2 * TILE; t += P2G_T) dst[t] = srcv[t];
+        if (threadIdx.x < 64) D.acc[(size_t)A_N * D.cap_cells + b * 64u + threadIdx.x] = (int32_t)own[threadIdx.x];
+        if (threadIdx.x == 0) D.tile_ok[b] = 1u;
+        __syncthreads();
+    }
+}
+
+// Sums of the P2G tiles at each cell: a cell with local coordinate l along an axis lies in
+// the tile of its own block (at l + 1), in the tile of the block below when l <= 1 (at l + 5)
+// and of the block above when l == 3 (at 0). Integer sums, so the same as adding every tile
+// entry atomically, in any order.
+__global__ void k_p2g_gather(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const uint32_t n_cells = min(st->s.n_blocks, D.cap_blocks) * 64u;
+    for (uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x; cell < n_cells; cell += gridDim.x * blockDim.x) {
+        const uint32_t b = cell >> 6;
+        const I3 l = local_coord(cell);
+        int32_t s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        const uint32_t* nbt = D.block_nb + (size_t)b * 27u;
+        for (int ox = -1; ox <= 1; ox++) {
+            if ((ox < 0 && l.x > 1) || (ox > 0 && l.x < 3)) continue;
+            for (int oy = -1; oy <= 1; oy++) {
+                if ((oy < 0 && l.y > 1) || (oy > 0 && l.y < 3)) continue;
+                for (int oz = -1; oz <= 1; oz++) {
+                    if ((oz < 0 && l.z > 1) || (oz > 0 && l.z < 3)) continue;
+                    const uint32_t src = nbt[(ox + 1) * 9 + (oy + 1) * 3 + oz + 1];
+                    if (src == NONE || D.tile_ok[src] == 0u) continue;
+                    const uint32_t t = (uint32_t)(l.x + 1 - 4 * ox) * 49u + (uint32_t)(l.y + 1 - 4 * oy) * 7u + (uint32_t)(l.z + 1 - 4 * oz);
+                    const int32_t* tp = D.tiles + (size_t)src * 8 * TILE + t;
 #pragma unroll
-            for (uint32_t f = 0; f < 8; f++) {
-                int32_t v = tile[f * TILE + t];
-                if (v != 0) atomicAdd(&D.acc[(size_t)f * D.cap_cells + cell], v);
+                    for (int f = 0; f < 8; f++) s[f] = (int32_t)((uint32_t)s[f] + (uint32_t)tp[f * TILE]);
+                }
             }
         }
-        if (threadIdx.x < 64) D.acc[(size_t)A_N * D.cap_cells + b * 64u + threadIdx.x] = (int32_t)own[threadIdx.x];
-        __syncthreads();
+#pragma unroll
+        for (int f = 0; f < 8; f++) D.acc[(size_t)f * D.cap_cells + cell] = s[f];
     }
 }
 

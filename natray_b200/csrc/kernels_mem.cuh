@@ -443,9 +443,12 @@ __device__ void push_water(const Dev& D, const Grid& g, V3 x, uint32_t d, float 
             }
 }
 
-// One CTA of 256 threads per bullet. Patches are summed per thread (k = li, li + 256, ...) and
-// then by the 256-wide tree, the reference's order.
-__global__ void __launch_bounds__(256) k_bullet_step(Dev D) {
+// One CTA per bullet, one thread per surface patch (up to 768). The reference sums the
+// patches per lane (lane l takes patches l, l + 256, l + 512 in turn) and then by a 256-wide
+// tree; here the 256 lanes' running sums are formed in three rounds in that order, so the
+// sums are the reference's.
+constexpr int BULLET_T = 768;
+__global__ void __launch_bounds__(BULLET_T) k_bullet_step(Dev D) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const uint32_t bi = blockIdx.x;
@@ -493,22 +496,24 @@ __global__ void __launch_bounds__(256) k_bullet_step(Dev D) {
     V3 w = qrot(b.q, lb / v3(b.shape.y, b.shape.y, b.shape.x));
     const float rho = U->fluid[0];
     const V3 vhat = normalize(xyz(b.v) + 1e-9f);
-    V3 f = {0.0f, 0.0f, 0.0f}, tq = {0.0f, 0.0f, 0.0f};
-    float cavx = 0.0f, cavy = 0.0f;
-    float4 cen = make_float4(0.0f, 0.0f, 0.0f, BIG_F);
-    for (uint32_t k = li; k < b.info.y; k += 256u) {
+    // This thread's patch: its force, torque, push on the water, and share of the wetted face.
+    const uint32_t n_patch = b.info.y;
+    V3 fp = {0.0f, 0.0f, 0.0f}, tqp = {0.0f, 0.0f, 0.0f}, cenp = {0.0f, 0.0f, 0.0f};
+    float cavxp = 0.0f, cavyp = 0.0f, cenwp = BIG_F;
+    bool has_cav = false;
+    if (li < n_patch) {
+        const uint32_t k = li;
         const float4 pp = D.patches[(bi * NTR_MAX_PATCHES + k) * 2], pn = D.patches[(bi * NTR_MAX_PATCHES + k) * 2 + 1];
         V3 r = qrot(b.q, xyz(pp));
         V3 p = xyz(b.x) + r;
         V3 n = qrot(b.q, xyz(pn));
         float area = pp.w;
         V3 X = (p - g.org) / hh;
-        V3 uw, sw;
-        for (uint32_t d = 0; d < 3; d++) {
-            float2 s = sample_grid(D, g, X - lattice_offset(d), F_U + d, a_wt(d));
-            uw[d] = s.y > 1e-6f ? s.x / s.y : 0.0f;
-            sw[d] = s.y;
-        }
+        float2 s0 = sample_grid(D, g, X - lattice_offset(0), F_U + 0, a_wt(0));
+        float2 s1 = sample_grid(D, g, X - lattice_offset(1), F_U + 1, a_wt(1));
+        float2 s2 = sample_grid(D, g, X - lattice_offset(2), F_U + 2, a_wt(2));
+        V3 uw = {s0.y > 1e-6f ? s0.x / s0.y : 0.0f, s1.y > 1e-6f ? s1.x / s1.y : 0.0f, s2.y > 1e-6f ? s2.x / s2.y : 0.0f};
+        V3 sw = {s0.y, s1.y, s2.y};
         float fill = clampf_(sample_grid(D, g, X - 0.5f, F_TYPE, A_WC).y / 8.0f, 0.0f, 1.0f);
         if (in_cavity(D, hh, bi, p, t_end - step) || dot(r, xyz(side)) > side.w) fill = 0.0f;
         float2 gs = sample_pressure(D, g, X - 0.5f, true);
@@ -523,21 +528,52 @@ __global__ void __launch_bounds__(256) k_bullet_step(Dev D) {
         V3 rt = rel - wn * n;
         float rtl = length(rt);
         if (rtl > 1e-9f) fw = fw - fill * CF_SKIN * 0.5f * rho * rtl * rt * area;
-        V3 fp = fw - (1.0f - fill) * mx(p_gas, P_VAPOUR - P_ATM) * area * n;
-        f = f + fp;
-        tq = tq + cross(r, fp);
-        for (uint32_t d = 0; d < 3; d++) push_water(D, g, X, d, -fw[d] * step, sw[d]);
+        fp = fw - (1.0f - fill) * mx(p_gas, P_VAPOUR - P_ATM) * area * n;
+        tqp = cross(r, fp);
+        push_water(D, g, X, 0, -fw.x * step, sw.x);
+        push_water(D, g, X, 1, -fw.y * step, sw.y);
+        push_water(D, g, X, 2, -fw.z * step, sw.z);
         if (wn > 0.0f && fill > 0.0f) {
             float face = fill * area * mx(dot(n, vhat), 0.0f);
-            cavx = cavx + -dot(fw, vhat);
-            cavy = cavy + face;
-            V3 cx = v3(cen.x, cen.y, cen.z) + p * face;
-            cen = make_float4(cx.x, cx.y, cx.z, mn(cen.w, dot(r, vhat)));
+            has_cav = true;
+            cavxp = -dot(fw, vhat);
+            cavyp = face;
+            cenp = p * face;
+            cenwp = dot(r, vhat);
         }
     }
-    red_f[li] = make_float4(f.x, f.y, f.z, cavx);
-    red_t[li] = make_float4(tq.x, tq.y, tq.z, cavy);
-    red_c[li] = cen;
+    // Lane l's running sums over patches l, l + 256, l + 512, in that order.
+    __shared__ uint8_t st_has[256];
+    V3 f = {0.0f, 0.0f, 0.0f}, tq = {0.0f, 0.0f, 0.0f};
+    float cavx = 0.0f, cavy = 0.0f;
+    float4 cen = make_float4(0.0f, 0.0f, 0.0f, BIG_F);
+    for (uint32_t round = 0; round < 3; round++) {
+        if (li >= round * 256u && li < round * 256u + 256u) {
+            const uint32_t l = li - round * 256u;
+            red_f[l] = f4(fp, cavxp);
+            red_t[l] = f4(tqp, cavyp);
+            red_c[l] = f4(cenp, cenwp);
+            st_has[l] = has_cav ? 1 : 0;
+        }
+        __syncthreads();
+        if (li < 256u && li + round * 256u < n_patch) {
+            const float4 a = red_f[li], t4 = red_t[li], c4 = red_c[li];
+            f = f + xyz(a);
+            tq = tq + xyz(t4);
+            if (st_has[li]) {
+                cavx = cavx + a.w;
+                cavy = cavy + t4.w;
+                V3 cx = v3(cen.x, cen.y, cen.z) + xyz(c4);
+                cen = make_float4(cx.x, cx.y, cx.z, mn(cen.w, c4.w));
+            }
+        }
+        __syncthreads();
+    }
+    if (li < 256u) {
+        red_f[li] = make_float4(f.x, f.y, f.z, cavx);
+        red_t[li] = make_float4(tq.x, tq.y, tq.z, cavy);
+        red_c[li] = cen;
+    }
     __syncthreads();
     for (uint32_t off = 128; off > 0; off >>= 1) {
         if (li < off) {

@@ -1147,7 +1147,11 @@ bool build_world(const ntr_sim_params& p, World& w, std::string& err) {
     float half = (float)((double)nxz * 0.5 * dx);
     float origin[3] = {-half, (float)(-3.0 * dx), -half};
     uint32_t block_cap = p.block_cap;
-    if (block_cap == 0) block_cap = std::max<uint32_t>(65535u, n_particles / 32u + 4096u);
+    if (block_cap == 0) block_cap = 65535u;  // MAX_BLOCKS, src/sim.rs:36
+    if (block_cap > 65535u) {
+        err = "block_cap is at most 65535";
+        return false;
+    }
 
     ntr_world_header& h = w.h;
     std::memset(&h, 0, sizeof h);

@@ -21,6 +21,7 @@
 
 #include "capi_util.hpp"
 #include "kernels_g2p.cuh"
+#include "kernels_solve.cuh"
 #include "kernels_grid.cuh"
 #include "world.hpp"
 
@@ -35,10 +36,8 @@ namespace ntr {
     } while (0)
 
 struct GraphKey {
-    uint32_t iters, n_mem, n_air, fp64;
-    bool operator<(const GraphKey& o) const {
-        return std::tie(iters, n_mem, n_air, fp64) < std::tie(o.iters, o.n_mem, o.n_air, o.fp64);
-    }
+    uint32_t n_mem, n_air, fp64;
+    bool operator<(const GraphKey& o) const { return std::tie(n_mem, n_air, fp64) < std::tie(o.n_mem, o.n_air, o.fp64); }
 };
 
 struct StepGraph {
@@ -50,6 +49,8 @@ struct StepGraph {
 struct Sim {
     int device = 0;
     int sms = 148;
+    uint32_t coop_ctas = 148;
+    cudaError_t launch_err = cudaSuccess;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     World host;  // header (params, host control) of the world; sections are not kept
@@ -159,7 +160,10 @@ static ntr_status allocate(Sim& S) {
     AL(D.cf, (size_t)NTR_CELL_FIELDS * D.cap_cells);
     AL(D.air[0], (size_t)NTR_AIR_FIELDS * D.cap_cells);
     AL(D.air[1], (size_t)NTR_AIR_FIELDS * D.cap_cells);
-    AL(D.px, D.cap_blocks); AL(D.py, D.cap_blocks); AL(D.pz, D.cap_blocks);
+    AL(D.px, D.cap_blocks);
+    AL(D.py, D.cap_blocks);
+    AL(D.pz, D.cap_blocks);
+    AL(D.pq, D.cap_blocks);
     for (int k = 0; k < 2; k++) {
         AL(D.mem_x[k], D.Nv);
         AL(D.mem_v[k], D.Nv);
@@ -188,7 +192,12 @@ static ntr_status allocate(Sim& S) {
     AL(D.landed, D.spray_cap);
     AL(D.touch, (size_t)D.wet_res * D.wet_res);
     AL(D.brk_x, D.Np); AL(D.brk_v, D.Np);
-    AL(D.brk_count, D.cap_blocks); AL(D.brk_off, D.cap_blocks);
+    AL(D.brk_count, D.cap_blocks);
+    AL(D.brk_off, D.cap_blocks);
+    AL(D.tiles, (size_t)D.cap_blocks * 8 * TILE);
+    AL(D.tile_ok, D.cap_blocks);
+    AL(D.coltot, 256);
+    AL(D.wnb, (size_t)D.cap_cells * 8);
 #undef AL
     return NTR_OK;
 }
@@ -309,12 +318,38 @@ static ntr_status measure_rubber(Sim& S) {
 }
 
 // ---- the step -----------------------------------------------------------------------------------
-static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t iters, uint32_t n_mem, uint32_t n_air, bool fp64) {
+// Per-kernel device timing of the profiling mode, the reference's NATRAY_PROF
+// (src/sim.rs:594-614, 670-689): an event after every launch of a step run outside the graph.
+struct Prof {
+    std::vector<cudaEvent_t> ev;
+    std::vector<const char*> name;
+    size_t next = 0;
+    cudaError_t err = cudaSuccess;
+    void mark(const char* n, cudaStream_t s) {
+        if (next == ev.size()) {
+            cudaEvent_t e;
+            cudaError_t r = cudaEventCreate(&e);
+            if (r != cudaSuccess) {
+                err = r;
+                return;
+            }
+            ev.push_back(e);
+            name.push_back(nullptr);
+        }
+        name[next] = n;
+        cudaError_t r = cudaEventRecord(ev[next++], s);
+        if (r != cudaSuccess) err = r;
+    }
+    ~Prof() {
+        for (auto e : ev) cudaEventDestroy(e);
+    }
+};
+
+static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_air, bool fp64, Prof* prof) {
     Dev& D = S.D;
     uint64_t n = 0;
     const uint32_t G_cell = (uint32_t)S.sms * 8;
     const uint32_t G_blk = (uint32_t)S.sms * 8;
-    const uint32_t G_solve = (uint32_t)S.sms * 4;
     const uint32_t g_part = (D.Np + 255) / 256 ? (D.Np + 255) / 256 : 1;
     const uint32_t g_vert = (D.Nv + 255) / 256 ? (D.Nv + 255) / 256 : 1;
     const uint32_t n_shots = S.U.mem[3] ? S.U.mem[3] : 1;
@@ -322,7 +357,9 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t iters, uint32_t n_
     do {                                                \
         kern<<<(grid), (block), 0, s>>>(__VA_ARGS__);   \
         n++;                                            \
+        if (prof) prof->mark(#kern, s);                 \
     } while (0)
+    if (prof) prof->mark("start", s);
     L(k_begin_step, 1, 32, D);
     L(k_clear, G_cell, 256, D);
     L(k_mark, (uint32_t)(((uint64_t)D.Np + D.cap_blocks + D.Nv + 255) / 256), 256, D);
@@ -338,7 +375,7 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t iters, uint32_t n_
             uint32_t* kout = to_final ? D.key_sorted : D.key_alt;
             uint32_t* vout = to_final ? D.sorted : D.val_alt;
             L(k_radix_hist, D.n_tiles, RADIX_T, D, kin, 8u * p);
-            L(k_radix_scan, 1, 1024, D);
+            L(k_radix_scan, 256, 256, D);
             L(k_radix_scatter, D.n_tiles, RADIX_T, D, kin, vin, kout, vout, 8u * p);
             kin = kout;
             vin = vout;
@@ -346,24 +383,30 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t iters, uint32_t n_
     }
     L(k_block_bounds, (D.Np + 1 + 255) / 256, 256, D);
     L(k_p2g, G_blk, P2G_T, D);
+    L(k_p2g_gather, G_cell, 256, D);
     L(k_mem_splat, g_vert, 256, D);
     L(k_air_carry, G_cell, 256, D);
     L(k_grid_prep, G_cell, 256, D);
     L(k_air_fill, G_cell, 256, D);
-    L(k_bullet_step, n_shots, 256, D);
+    L(k_bullet_step, n_shots, BULLET_T, D);
     L(k_bullet_apply, G_cell, 256, D);
-    if (fp64) {
-        L(k_solve_init<true>, G_solve, SOLVE_T, D);
-        for (uint32_t it = 0; it < iters; it++) {
-            L(k_solve_q<true>, G_solve, SOLVE_T, D);
-            L(k_solve_update<true>, G_solve, SOLVE_T, D);
-        }
-    } else {
-        L(k_solve_init<false>, G_solve, SOLVE_T, D);
-        for (uint32_t it = 0; it < iters; it++) {
-            L(k_solve_q<false>, G_solve, SOLVE_T, D);
-            L(k_solve_update<false>, G_solve, SOLVE_T, D);
-        }
+    // The whole pressure solve: one cooperative launch, its grid barrier reset first.
+    cudaMemsetAsync(&D.st->bar_count, 0, 4, s);
+    {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(S.coop_ctas);
+        cfg.blockDim = dim3(SOLVE_T);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        cudaError_t e = fp64 ? cudaLaunchKernelEx(&cfg, k_solve<true>, D) : cudaLaunchKernelEx(&cfg, k_solve<false>, D);
+        if (e != cudaSuccess) S.launch_err = e;
+        n++;
+        if (prof) prof->mark(fp64 ? "k_solve<true>" : "k_solve<false>", s);
     }
     L(k_project, G_cell, 256, D);
     L(k_extend_1, G_cell, 256, D);
@@ -383,7 +426,7 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t iters, uint32_t n_
 }
 
 static ntr_status get_graph(Sim& S, StepGraph*& out) {
-    GraphKey key{S.host.h.iters, S.host.h.substeps, S.host.h.air_substeps, S.fp64};
+    GraphKey key{S.host.h.substeps, S.host.h.air_substeps, S.fp64};
     auto it = S.graphs.find(key);
     if (it != S.graphs.end()) {
         out = &it->second;
@@ -397,11 +440,16 @@ static ntr_status get_graph(Sim& S, StepGraph*& out) {
         S.graphs.erase(victim);
     }
     StepGraph g;
+    S.launch_err = cudaSuccess;
     CU(cudaStreamBeginCapture(S.stream, cudaStreamCaptureModeThreadLocal));
-    g.launches = enqueue_step(S, S.stream, key.iters, key.n_mem, key.n_air, key.fp64 != 0);
+    g.launches = enqueue_step(S, S.stream, key.n_mem, key.n_air, key.fp64 != 0, nullptr);
     cudaError_t le = cudaGetLastError();
     cudaError_t ce = cudaStreamEndCapture(S.stream, &g.graph);
-    if (le != cudaSuccess) return fail(NTR_E_CUDA, std::string("kernel launch during capture: ") + cudaGetErrorString(le));
+    if (S.launch_err != cudaSuccess) le = S.launch_err;
+    if (le != cudaSuccess) {
+        if (g.graph) cudaGraphDestroy(g.graph);
+        return fail(NTR_E_CUDA, std::string("kernel launch during capture: ") + cudaGetErrorString(le));
+    }
     if (ce != cudaSuccess) return fail(NTR_E_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce));
     CU(cudaGraphInstantiate(&g.exec, g.graph, 0));
     auto res = S.graphs.emplace(key, g);
@@ -410,7 +458,7 @@ static ntr_status get_graph(Sim& S, StepGraph*& out) {
 }
 
 // Sim::run (src/sim.rs:585-648).
-static ntr_status run_batch(Sim& S, uint32_t n, uint32_t stop, uint32_t* taken) {
+static ntr_status run_batch(Sim& S, uint32_t n, uint32_t stop, uint32_t* taken, Prof* prof = nullptr) {
     ntr_world_header& h = S.host.h;
     S.U.limits[2] = h.iters;
     S.U.limits[3] = stop;
@@ -421,16 +469,27 @@ static ntr_status run_batch(Sim& S, uint32_t n, uint32_t stop, uint32_t* taken) 
     // iters_max and unconverged count per batch.
     CU(cudaMemsetAsync(&S.D.st->s.iters_max, 0, 8, S.stream));
     StepGraph* g = nullptr;
-    if ((r = get_graph(S, g)) != NTR_OK) return r;
+    if (!prof)
+        if ((r = get_graph(S, g)) != NTR_OK) return r;
     const uint32_t before = S.h_state->s.step;
+    uint64_t launches = 0;
     CU(cudaEventRecord(S.ev0, S.stream));
-    for (uint32_t k = 0; k < n; k++) CU(cudaGraphLaunch(g->exec, S.stream));
+    if (prof) {
+        S.launch_err = cudaSuccess;
+        for (uint32_t k = 0; k < n; k++) launches += enqueue_step(S, S.stream, h.substeps, h.air_substeps, S.fp64 != 0, prof);
+        CU(cudaGetLastError());
+        CU(S.launch_err);
+        CU(prof->err);
+    } else {
+        for (uint32_t k = 0; k < n; k++) CU(cudaGraphLaunch(g->exec, S.stream));
+        launches = g->launches * n;
+    }
     CU(cudaEventRecord(S.ev1, S.stream));
     if ((r = read_state(S)) != NTR_OK) return r;
     float ms = 0.0f;
     CU(cudaEventElapsedTime(&ms, S.ev0, S.ev1));
     S.last_ms = ms;
-    S.last_launches = g->launches * n;
+    S.last_launches = launches;
     S.step_ms = n ? ms / n : 0.0;
     const ntr_state& s = S.h_state->s;
     if (taken) *taken = s.step - before;
@@ -451,6 +510,17 @@ static ntr_status create_from(const World& w, int device, Sim*& out) {
     cudaDeviceProp prop;
     CU(cudaGetDeviceProperties(&prop, device));
     S->sms = prop.multiProcessorCount;
+    {
+        // The persistent solver's grid must be co-resident: at most what occupancy allows.
+        int occ_a = 0, occ_b = 0;
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_solve<true>, SOLVE_T, 0));
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_solve<false>, SOLVE_T, 0));
+        int occ = std::min(occ_a, occ_b);
+        // CTA c owns the blocks c (mod 256), so 128..256 CTAs.
+        S->coop_ctas = (uint32_t)std::min(256, S->sms * occ);
+        if (S->coop_ctas < 128) return fail(NTR_E_NODEVICE, "the device cannot hold 128 resident solver CTAs");
+    }
+    if (w.h.block_cap > 65535u) return fail(NTR_E_INVALID, "block_cap is at most 65535");
     if (prop.major < 10) return fail(NTR_E_NODEVICE, "this library is built for sm_100a (B200); device is sm_" + std::to_string(prop.major * 10 + prop.minor));
     CU(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
     CU(cudaEventCreate(&S->ev0));
@@ -721,6 +791,37 @@ NTR_API ntr_status ntr_sim_restore(ntr_sim* sim, const void* blob, size_t len) {
     if ((r = read_state(S)) != NTR_OK) return r;
     if (S.host.h.substeps == 0)
         if ((r = measure_rubber(S)) != NTR_OK) return r;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_sim_profile(ntr_sim* sim, uint32_t n, uint32_t stop_ns, char* report, size_t cap, size_t* len) {
+    GUARD(sim);
+    Prof prof;
+    uint32_t taken = 0;
+    ntr_status r = run_batch(S, n, stop_ns, &taken, &prof);
+    if (r != NTR_OK) return r;
+    std::vector<std::string> order;
+    std::map<std::string, std::pair<uint64_t, double>> acc;
+    for (size_t i = 1; i < prof.next; i++) {
+        if (std::strcmp(prof.name[i], "start") == 0) continue;
+        float ms = 0.0f;
+        CU(cudaEventElapsedTime(&ms, prof.ev[i - 1], prof.ev[i]));
+        std::string k = prof.name[i];
+        if (!acc.count(k)) order.push_back(k);
+        acc[k].first += 1;
+        acc[k].second += ms;
+    }
+    std::string out;
+    char line[256];
+    for (auto& k : order) {
+        snprintf(line, sizeof line, "%s,%llu,%.6f\n", k.c_str(), (unsigned long long)acc[k].first, acc[k].second);
+        out += line;
+    }
+    if (len) *len = out.size();
+    if (report) {
+        if (cap < out.size() + 1) return fail(NTR_E_INVALID, "report buffer too small");
+        std::memcpy(report, out.c_str(), out.size() + 1);
+    }
     return NTR_OK;
 }
 

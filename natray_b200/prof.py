@@ -1,0 +1,45 @@
+"""Per-kernel device time of the simulation step, the reference's NATRAY_PROF
+(src/sim.rs:594-614, 670-689) as a command:
+
+    python -m natray_b200.prof [--resolution 124] [--warmup 3] [--steps 5] [--graph-steps 10]
+
+Builds the 1M-particle scene of the benchmark (or another resolution), runs warm-up batches,
+times `--graph-steps` steps through the step's CUDA graph, then runs `--steps` steps kernel by
+kernel with events between them and prints each kernel's share.
+"""
+from __future__ import annotations
+
+import argparse
+
+from .sim import Sim
+from .world import Params, build_world
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--resolution", type=int, default=124)
+    ap.add_argument("--mesh-level", type=int, default=6)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--graph-steps", type=int, default=10)
+    ap.add_argument("--speed", type=float, default=350.0)
+    args = ap.parse_args()
+    w = build_world(Params(resolution=args.resolution, mesh_level=args.mesh_level, dt_max=2e-6, bullet=6, caliber=8,
+                           bullet_speed=args.speed))
+    s = Sim(world=w)
+    s.step(args.warmup)
+    n = s.step(args.graph_steps)
+    launches, ms = s.last_launches()
+    st = s.state
+    print(f"{w.h.n_particles} particles: graph {ms / max(n, 1):.3f} ms/step, {launches / max(n, 1):.0f} launches/step, "
+          f"{st['n_blocks']} blocks, {st['solve_iters']} solver iterations")
+    if args.steps:
+        p = s.profile(args.steps)
+        tot = sum(v[1] for v in p.values())
+        print(f"kernel by kernel: {tot / args.steps:.3f} ms/step")
+        for k, (c, t) in sorted(p.items(), key=lambda kv: -kv[1][1]):
+            print(f"  {k:24s} {c:5d} launches {t / args.steps * 1e3:9.1f} us/step {100 * t / tot:5.1f}%")
+
+
+if __name__ == "__main__":
+    main()

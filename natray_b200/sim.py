@@ -116,6 +116,18 @@ class Sim:
         return {"block_list": bl, "block_start": bs, "sorted": srt, "acc": acc.reshape(-1), "cf": cf.reshape(-1),
                 "block_nb": nbt, "air": air.reshape(-1)}
 
+    def profile(self, n: int, stop_ns: int = 0xFFFFFFFF) -> dict:
+        """One batch launched kernel by kernel with events between them: {kernel: (launches, ms)}
+        (the reference's NATRAY_PROF)."""
+        buf = C.create_string_buffer(1 << 16)
+        ln = C.c_size_t()
+        check(lib().ntr_sim_profile(self._h, n, stop_ns, buf, len(buf), C.byref(ln)))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, cnt, ms = line.rsplit(",", 2)
+            out[name] = (int(cnt), float(ms))
+        return out
+
     def last_launches(self) -> tuple[int, float]:
         n, ms = C.c_uint64(), C.c_double()
         check(lib().ntr_sim_last_launches(self._h, C.byref(n), C.byref(ms)))
