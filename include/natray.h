@@ -347,6 +347,31 @@ NTR_API ntr_status ntr_sim_last_launches(ntr_sim* s, uint64_t* launches, double*
  * particle mass, out[5..7] = sum of positions. */
 NTR_API ntr_status ntr_sim_conservation(ntr_sim* s, double out[8]);
 
+/* --- Sorting particles by block without allocating ------------------------------------------
+ * No counterpart in the reference: an addition for callers that cannot allocate device
+ * memory, such as a host application whose framework has reserved the GPU's memory for its
+ * own pool, or a frame loop that must not make the device-wide synchronising cudaMalloc and
+ * cudaFree calls. The same stable radix sort the step uses (particles grouped by block index,
+ * ascending particle index within a block), with its scratch in a fixed array inside this
+ * library: NTR_NOALLOC_MAX_KEYS keys, NTR_NOALLOC_MAX_BLOCKS blocks (about 13 MB, held on every
+ * GPU that loads the library until the process exits).
+ *
+ *   keys         device array of n block indices (< n_blocks), or 0xFFFFFFFF for a particle
+ *                that takes no part
+ *   sorted       device array of n: the particle indices, grouped by block; the first
+ *                block_start[n_blocks] entries are meaningful
+ *   block_start  device array of n_blocks + 1: where each block's particles start in sorted
+ *   stream       a cudaStream_t (NULL: the default stream); the call is asynchronous on it
+ *
+ * The first call on a device looks up the scratch array's device address for that device; make
+ * that first call before any stream capture. Every call shares the one scratch array, so calls
+ * whose work overlaps on the GPU (different streams, or different host threads) race: order
+ * them. n > NTR_NOALLOC_MAX_KEYS or n_blocks > NTR_NOALLOC_MAX_BLOCKS is NTR_E_INVALID. */
+#define NTR_NOALLOC_MAX_KEYS 1048576u
+#define NTR_NOALLOC_MAX_BLOCKS 65535u
+NTR_API ntr_status ntr_sort_by_block_noalloc(const uint32_t* keys, uint32_t n, uint32_t n_blocks, uint32_t* sorted,
+                                             uint32_t* block_start, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

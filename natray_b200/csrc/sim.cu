@@ -14,6 +14,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <type_traits>
@@ -854,3 +855,97 @@ NTR_API ntr_status ntr_sim_conservation(ntr_sim* sim, double out[8]) {
 }
 
 }  // extern "C"
+
+// ---- sorting by block without allocating (ntr_sort_by_block_noalloc) --------------------------
+// For callers that cannot allocate device memory (a framework that has reserved the GPU's
+// memory for its own pool, a frame loop that must not make the device-wide synchronising
+// cudaMalloc/cudaFree calls): the step's stable radix sort, with its scratch in the file-scope
+// device array below instead of a simulation's buffers. The array holds a small state record
+// (the kernels' early-exit check and block count), the digit totals, the digit-major
+// histogram, and the keys and values between passes. The kernels are the step's own, given a
+// pointer table into this array.
+namespace ntr {
+constexpr size_t NOALLOC_TILES = (NTR_NOALLOC_MAX_KEYS + RADIX_TILE - 1) / RADIX_TILE;
+constexpr size_t NOALLOC_STATE_WORDS = 64;
+constexpr size_t NOALLOC_OFF_COLTOT = NOALLOC_STATE_WORDS;
+constexpr size_t NOALLOC_OFF_HIST = NOALLOC_OFF_COLTOT + 256;
+constexpr size_t NOALLOC_OFF_KEY_ALT = NOALLOC_OFF_HIST + 256 * NOALLOC_TILES;
+constexpr size_t NOALLOC_OFF_VAL_ALT = NOALLOC_OFF_KEY_ALT + NTR_NOALLOC_MAX_KEYS;
+constexpr size_t NOALLOC_OFF_KEY_SORTED = NOALLOC_OFF_VAL_ALT + NTR_NOALLOC_MAX_KEYS;
+constexpr size_t NOALLOC_WORDS = NOALLOC_OFF_KEY_SORTED + NTR_NOALLOC_MAX_KEYS;
+static_assert(sizeof(DevState) <= NOALLOC_STATE_WORDS * 4, "the state record fits its slot");
+
+// About 13 MB, held on every GPU that loads the library until the process exits.
+static __device__ __align__(256) uint32_t g_noalloc_scratch[NOALLOC_WORDS];
+
+// Sets what the sort kernels read of the state: a live step (dt_ns != 0) and the block count.
+// Everything else of the scratch is written whole by every call before it is read.
+__global__ void k_noalloc_prepare(DevState* st, uint32_t n_blocks) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        st->s.dt_ns = 1u;
+        st->s.n_blocks = n_blocks;
+    }
+}
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[64];  // per device: the scratch array's device address
+}  // namespace ntr
+
+extern "C" NTR_API ntr_status ntr_sort_by_block_noalloc(const uint32_t* keys, uint32_t n, uint32_t n_blocks, uint32_t* sorted,
+                                                        uint32_t* block_start, void* stream) {
+    using namespace ntr;
+    if (n > NTR_NOALLOC_MAX_KEYS)
+        return fail(NTR_E_INVALID, "ntr_sort_by_block_noalloc: " + std::to_string(n) + " keys, at most " + std::to_string(NTR_NOALLOC_MAX_KEYS));
+    if (n_blocks > NTR_NOALLOC_MAX_BLOCKS)
+        return fail(NTR_E_INVALID, "ntr_sort_by_block_noalloc: " + std::to_string(n_blocks) + " blocks, at most " +
+                                       std::to_string(NTR_NOALLOC_MAX_BLOCKS));
+    if ((n > 0 && (!keys || !sorted)) || !block_start) return fail(NTR_E_INVALID, "ntr_sort_by_block_noalloc: null device array");
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(NTR_E_INVALID, "ntr_sort_by_block_noalloc: device index out of range");
+    void* base = nullptr;
+    {
+        // Once per device, with that device current. In host code the array's name is only a
+        // host-side stand-in; the kernels need its device address.
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            cudaError_t e = cudaGetSymbolAddress(&g_noalloc_addr[dev], g_noalloc_scratch);
+            if (e != cudaSuccess) {
+                g_noalloc_addr[dev] = nullptr;
+                return fail(NTR_E_CUDA, std::string("cudaGetSymbolAddress of the sort scratch: ") + cudaGetErrorString(e));
+            }
+        }
+        base = g_noalloc_addr[dev];
+    }
+    uint32_t* w = static_cast<uint32_t*>(base);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Dev D{};
+    D.st = reinterpret_cast<DevState*>(w);
+    D.Np = n;
+    D.cap_blocks = n_blocks;
+    D.n_tiles = std::max<uint32_t>(1u, (n + RADIX_TILE - 1) / RADIX_TILE);
+    D.coltot = w + NOALLOC_OFF_COLTOT;
+    D.hist = w + NOALLOC_OFF_HIST;
+    D.key_alt = w + NOALLOC_OFF_KEY_ALT;
+    D.val_alt = w + NOALLOC_OFF_VAL_ALT;
+    D.key_sorted = w + NOALLOC_OFF_KEY_SORTED;
+    D.sorted = sorted;
+    D.block_start = block_start;
+    const uint32_t P = radix_passes_for(std::max<uint32_t>(n_blocks, 1u));
+    k_noalloc_prepare<<<1, 32, 0, s>>>(D.st, n_blocks);
+    const uint32_t* kin = keys;
+    const uint32_t* vin = nullptr;
+    for (uint32_t p = 0; p < P && n > 0; p++) {
+        const bool to_final = ((P - 1 - p) % 2) == 0;
+        uint32_t* kout = to_final ? D.key_sorted : D.key_alt;
+        uint32_t* vout = to_final ? D.sorted : D.val_alt;
+        k_radix_hist<<<D.n_tiles, RADIX_T, 0, s>>>(D, kin, 8u * p);
+        k_radix_scan<<<256, 256, 0, s>>>(D);
+        k_radix_scatter<<<D.n_tiles, RADIX_T, 0, s>>>(D, kin, vin, kout, vout, 8u * p);
+        kin = kout;
+        vin = vout;
+    }
+    k_block_bounds<<<(n + 1 + 255) / 256, 256, 0, s>>>(D);
+    CU(cudaGetLastError());
+    return NTR_OK;
+}
