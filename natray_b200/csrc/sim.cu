@@ -53,7 +53,9 @@ struct Sim {
     uint32_t coop_ctas = 148;
     cudaError_t launch_err = cudaSuccess;
     cudaStream_t stream = nullptr;
+    cudaStream_t aux = nullptr;  // the second stream of the step's forks
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
     World host;  // header (params, host control) of the world; sections are not kept
     ntr_gpu_params U{};
     Dev D{};
@@ -76,6 +78,11 @@ struct Sim {
         if (h_state) cudaFreeHost(h_state);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        for (int k = 0; k < 2; k++) {
+            if (ev_fork[k]) cudaEventDestroy(ev_fork[k]);
+            if (ev_join[k]) cudaEventDestroy(ev_join[k]);
+        }
+        if (aux) cudaStreamDestroy(aux);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -383,10 +390,31 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
         }
     }
     L(k_block_bounds, (D.Np + 1 + 255) / 256, 256, D);
+    // Independent work on a second stream: the rubber's splat and the air's carry touch none
+    // of what P2G reads or writes. (In the profiling mode everything stays on one stream.)
+    cudaStream_t a = prof ? s : S.aux;
+    auto fork = [&](int k) {
+        if (a == s) return;
+        cudaEventRecord(S.ev_fork[k], s);
+        cudaStreamWaitEvent(a, S.ev_fork[k], 0);
+    };
+    auto join = [&](int k) {
+        if (a == s) return;
+        cudaEventRecord(S.ev_join[k], a);
+        cudaStreamWaitEvent(s, S.ev_join[k], 0);
+    };
+#define LA(kern, grid, block, ...)                      \
+    do {                                                \
+        kern<<<(grid), (block), 0, a>>>(__VA_ARGS__);   \
+        n++;                                            \
+        if (prof) prof->mark(#kern, a);                 \
+    } while (0)
+    fork(0);
+    LA(k_mem_splat, g_vert, 256, D);
+    LA(k_air_carry, G_cell, 256, D);
     L(k_p2g, G_blk, P2G_T, D);
     L(k_p2g_gather, G_cell, 256, D);
-    L(k_mem_splat, g_vert, 256, D);
-    L(k_air_carry, G_cell, 256, D);
+    join(0);
     L(k_grid_prep, G_cell, 256, D);
     L(k_air_fill, G_cell, 256, D);
     L(k_bullet_step, n_shots, BULLET_T, D);
@@ -412,17 +440,22 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     L(k_project, G_cell, 256, D);
     L(k_extend_1, G_cell, 256, D);
     L(k_extend_2, G_cell, 256, D);
-    L(k_mem_sample, g_vert, 256, D);
+    // G2P shares nothing with the rubber and air substeps or the spray's flight: they run
+    // side by side.
+    fork(1);
+    LA(k_mem_sample, g_vert, 256, D);
     for (uint32_t i = 0; i < std::max(n_mem, n_air); i++) {
-        if (i < n_mem) L(k_mem_substep, g_vert, 256, D, i, (int)(i % 2));
-        if (i < n_air) L(k_air_substep, G_cell, 256, D, (int)(i % 2));
+        if (i < n_mem) LA(k_mem_substep, g_vert, 256, D, i, (int)(i % 2));
+        if (i < n_air) LA(k_air_substep, G_cell, 256, D, (int)(i % 2));
     }
-    L(k_spray_update, G_cell, 256, D);
+    LA(k_spray_update, G_cell, 256, D);
     L(k_g2p, G_blk, G2P_T, D);
+    join(1);
     L(k_spray_scan, 1, 1024, D);
     L(k_spray_emit, G_cell, 256, D);
     L(k_spray_commit, 1, 32, D);
 #undef L
+#undef LA
     return n;
 }
 
@@ -524,6 +557,11 @@ static ntr_status create_from(const World& w, int device, Sim*& out) {
     if (w.h.block_cap > 65535u) return fail(NTR_E_INVALID, "block_cap is at most 65535");
     if (prop.major < 10) return fail(NTR_E_NODEVICE, "this library is built for sm_100a (B200); device is sm_" + std::to_string(prop.major * 10 + prop.minor));
     CU(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    CU(cudaStreamCreateWithFlags(&S->aux, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; k++) {
+        CU(cudaEventCreateWithFlags(&S->ev_fork[k], cudaEventDisableTiming));
+        CU(cudaEventCreateWithFlags(&S->ev_join[k], cudaEventDisableTiming));
+    }
     CU(cudaEventCreate(&S->ev0));
     CU(cudaEventCreate(&S->ev1));
     CU(cudaMallocHost((void**)&S->h_state, sizeof(DevState)));
