@@ -89,8 +89,8 @@ struct DevState {
     uint32_t ticket[4];  // arrival counters of the last-block reductions
     uint32_t nbrk;       // break-ups of this step
     uint32_t err;        // bit 0: a bounded grid barrier gave up
-    uint32_t bar_count;  // grid barrier of the persistent solver: arrivals
-    uint32_t bar_gen;    // and generation
+    uint32_t bar_count;  // grid barrier of the persistent solver: arrivals (reset per launch)
+    uint32_t bar_gen;    // unused
     uint32_t pad[3];
 };
 
@@ -110,7 +110,7 @@ struct Dev {
     int32_t* acc;
     float* cf;
     float* air[2];
-    double *px, *py, *pz, *pq;
+    double* xsum;  // the solver's running sums: 2 parities x 256 residues x 3 quantities
     float4* mem_x[2];
     float4* mem_v[2];
     float4 *mem_water, *mem_layer;
@@ -176,8 +176,25 @@ __device__ __forceinline__ I3 vi(V3 a) { return {__float2int_rz(a.x), __float2in
 __device__ __forceinline__ V3 vf(I3 a) { return {(float)a.x, (float)a.y, (float)a.z}; }
 __device__ __forceinline__ uint32_t f2u(float x) { return __float2uint_rz(x); }
 
-// to_fp rounds half to even (sim_defs.wgsl:217-219).
-__device__ __forceinline__ int32_t to_fp(float x, float scale) { return __float2int_rn(clampf_(x * scale, -2e9f, 2e9f)); }
+// to_fp rounds half to even (sim_defs.wgsl:217-219): rint(clamp(x * scale, -2e9, 2e9)).
+// The transfer kernels convert hundreds of values per particle, more than the conversion unit
+// keeps up with, so the common range goes through the adder instead: for |y| < 2^22,
+// y + 1.5 * 2^23 lies in [2^23, 2^24], where floats are the integers, so the addition rounds y
+// to the nearest integer, ties to even (1.5 * 2^23 is even), and the integer is the difference
+// of the bit patterns. Everything else (large magnitudes, infinities, NaN) is converted. The
+// result is the same as the conversion's for every input.
+__device__ __forceinline__ int32_t to_fp(float x, float scale) {
+    const float y = __fmul_rn(x, scale);  // never contracted into the addition below
+    if (fabsf(y) < 4194304.0f) return __float_as_int(__fadd_rn(y, 12582912.0f)) - 0x4B400000;
+    return __float2int_rn(clampf_(y, -2e9f, 2e9f));
+}
+// The same for values that are mostly in [0, 2^23) (B-spline weights times 2^24, at most
+// 0.75^3 * 2^24): y + 2^23 lies in [2^23, 2^24].
+__device__ __forceinline__ int32_t to_fp_pos(float x, float scale) {
+    const float y = __fmul_rn(x, scale);
+    if (y >= 0.0f && y < 8388608.0f) return __float_as_int(__fadd_rn(y, 8388608.0f)) - 0x4B000000;
+    return __float2int_rn(clampf_(y, -2e9f, 2e9f));
+}
 __device__ __forceinline__ float from_fp(int32_t x, float scale) { return (float)x / scale; }
 
 __device__ __forceinline__ V3 axis_weights(float fx) {

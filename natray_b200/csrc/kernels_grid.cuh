@@ -374,7 +374,7 @@ __device__ __forceinline__ void splat(int32_t* tile, V3 x, V3 o, I3 corner, uint
                 uint32_t tt = t0 + a * 49u + b * 7u + c;
                 float node = val + dot(hg, v3((float)a, (float)b, (float)c) - fx);
                 atomicAdd(&tile[fa * TILE + tt], to_fp(weight * node, scale));
-                atomicAdd(&tile[fw * TILE + tt], to_fp(weight, FP_W));
+                atomicAdd(&tile[fw * TILE + tt], to_fp_pos(weight, FP_W));
             }
 }
 

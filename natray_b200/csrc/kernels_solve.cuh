@@ -6,17 +6,24 @@
 // launch runs the whole solve and stops at convergence.
 //
 // Layout of the work:
-//   - one warp per 4^3 block, each lane two cells (l and l + 32, which have the same
-//     red-black colour), so the block-local Gauss-Seidel sweeps and the block's 64-wide sum
-//     tree need only warp synchronisation;
+//   - one warp per 4^3 block, each lane two cells of opposite red-black colour (solve_cell),
+//     so the block-local Gauss-Seidel sweeps and the block's 64-wide sum tree need only warp
+//     synchronisation, and every lane has a cell to update in every half-sweep;
 //   - the reference sums the per-block partials with 256 strided running sums (lane l adds
 //     blocks l, l + 256, ...) and then a 256-wide tree (fluid.wgsl:426-439). CTA c owns the
 //     blocks b = c (mod 256) (with fewer than 256 CTAs, several residues), so it forms lane
 //     c's running sum from its own blocks and publishes one value; after a grid barrier every
-//     CTA reads the 256 values and runs the same tree. All CTAs agree on alpha, beta and
-//     convergence bit for bit, and the result equals the reference's order of summation.
-// The grid barrier spins a bounded number of times; when it gives up it sets an error bit
-// that the host reports as NTR_E_TIMEOUT, and the kernel returns.
+//     warp reads the 256 values and runs the same tree. All CTAs agree on alpha, beta and
+//     convergence bit for bit, and the result equals the reference's order of summation;
+//   - a warp that owns at most SOLVE_R blocks keeps their cells' solver values (type, diagonal,
+//     water neighbours, p, r, z, d, q) in registers for the whole solve, and writes to memory
+//     only what other warps read (d and z, for their neighbours) and, at the end, the final
+//     fields. Otherwise it loads and stores them per phase. Either way every load of a phase is
+//     issued before its first store, so the latencies overlap;
+//   - the grid barrier is a counter that only grows during the launch (reset before it): the
+//     k-th barrier waits for k * (CTAs) arrivals. One atomic per CTA and a poll of the same word.
+// The barrier spins a bounded number of times; when it gives up it sets an error bit that the
+// host reports as NTR_E_TIMEOUT, and the kernel returns.
 #pragma once
 
 #include "kernels_cells.cuh"
@@ -25,54 +32,20 @@ namespace ntr {
 
 constexpr int SOLVE_W = 12;                 // warps per CTA
 constexpr int SOLVE_T = SOLVE_W * 32;       // 384 threads
+constexpr int SOLVE_R = 1;                  // blocks per warp kept in registers
 constexpr uint32_t SOLVE_MAX_M = 256;       // blocks per residue: 65536 blocks / 256
 constexpr uint32_t BARRIER_SPINS = 1u << 24;
+constexpr int SOLVE_XQ = 3;                 // quantities per exchange, at most
 
-// Grid-wide barrier of a cooperative launch. Returns false in every thread of the CTA if the
-// wait gave up; the error bit is then set in the state.
 __device__ __forceinline__ uint32_t atom_add_release(uint32_t* p, uint32_t v) {
     uint32_t old;
-    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
     return old;
-}
-__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
     uint32_t v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
-}
-
-// Thread 0 arrives with release semantics (after the CTA's barrier, so the whole CTA's writes
-// are ordered before it) and waits with acquire semantics; the last to arrive resets the
-// count and releases the next generation.
-__device__ __forceinline__ bool grid_sync(DevState* st, uint32_t& gen) {
-    __shared__ uint32_t s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const uint32_t target = gen + 1u;
-        uint32_t ok = 1u;
-        const uint32_t t = atom_add_release(&st->bar_count, 1u);
-        if (t == gridDim.x - 1) {
-            atomicExch(&st->bar_count, 0u);
-            st_release(&st->bar_gen, target);
-        } else {
-            uint32_t spins = 0;
-            while (ld_acquire(&st->bar_gen) != target) {
-                if (++spins > BARRIER_SPINS) {
-                    atomicOr(&st->err, 1u);
-                    ok = 0u;
-                    break;
-                }
-                if (spins > 64) __nanosleep(32);
-            }
-        }
-        s_ok = ok;
-    }
-    __syncthreads();
-    gen++;
-    return s_ok != 0;
 }
 
 template <bool FP64>
@@ -87,77 +60,141 @@ struct SolveMath {
     static __device__ __forceinline__ double ratio(double a, double b) { return FP64 ? a / b : (double)((float)a / (float)b); }
 };
 
-// The 64-wide tree of block_sum (fluid.wgsl:414-422) over a warp whose lane l holds cells l
-// and l + 32: the first level adds those two, the rest are shuffles. Valid in lane 0.
+// The 64-wide tree of block_sum (fluid.wgsl:414-422) over a warp whose lane l holds the
+// values of its cells (solve_cell): the first level adds cells l and l + 32 (the latter held by
+// lane l ^ 1), the rest are shuffles. Valid in lane 0.
 template <class A>
 __device__ __forceinline__ A warp_tree64(A v0, A v1) {
-    A x = v0 + v1;
+    A x = v0 + __shfl_xor_sync(0xffffffffu, v1, 1);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, off);
     return x;
 }
 
+// A lane's two cells of a block: cell `lane` and cell (lane ^ 1) + 32. They have opposite
+// red-black colours (the second is two layers up in x and one step over in z), so in every
+// half-sweep of the block's Gauss-Seidel each lane updates exactly one cell.
+__device__ __forceinline__ uint32_t solve_cell(int lane, int k) { return k == 0 ? (uint32_t)lane : (uint32_t)(lane ^ 1) + 32u; }
+
 // Symmetric red-black Gauss-Seidel, two sweeps inside the block (fluid.wgsl:390-410), by one
-// warp. zl, wl: the warp's 64 cells in shared memory.
+// warp. zl, wl: the warp's 64 cells in shared memory. The cells of one colour do not touch each
+// other, so the order in which a half-sweep visits them does not matter.
 __device__ __forceinline__ void warp_precondition(float* zl, uint8_t* wl, int lane, const float r[2], const float diag[2],
                                                   const bool water[2], float z[2]) {
-    zl[lane] = 0.0f, zl[lane + 32] = 0.0f;
-    wl[lane] = water[0], wl[lane + 32] = water[1];
+    const int li0 = (int)solve_cell(lane, 0), li1 = (int)solve_cell(lane, 1);
+    zl[li0] = 0.0f, zl[li1] = 0.0f;
+    wl[li0] = water[0], wl[li1] = water[1];
     __syncwarp();
-    const int ly = (lane / 4) % 4, lz = lane % 4;
-    const int lx0 = lane / 16;  // the second cell is at lx0 + 2
-    const uint32_t colour = (uint32_t)(lx0 + ly + lz) % 2u;
-    for (uint32_t k = 0; k < 5; k++) {
-        if (colour == k % 2u) {
+    // Which of the block's face neighbours are water, in the order the sum visits them:
+    // -x, +x, -y, +y, -z, +z (local index steps 16, 4, 1).
+    uint32_t nm[2];
 #pragma unroll
-            for (int c = 0; c < 2; c++) {
-                if (!water[c]) continue;
-                const int li = lane + 32 * c, lx = lx0 + 2 * c;
-                float s = r[c];
-                if (lx > 0 && wl[li - 16]) s += zl[li - 16];
-                if (lx < 3 && wl[li + 16]) s += zl[li + 16];
-                if (ly > 0 && wl[li - 4]) s += zl[li - 4];
-                if (ly < 3 && wl[li + 4]) s += zl[li + 4];
-                if (lz > 0 && wl[li - 1]) s += zl[li - 1];
-                if (lz < 3 && wl[li + 1]) s += zl[li + 1];
-                zl[li] = s / diag[c];
-            }
+    for (int c = 0; c < 2; c++) {
+        const int li = c ? li1 : li0;
+        const int lx = li >> 4, ly = (li >> 2) & 3, lz = li & 3;
+        nm[c] = (lx > 0 && wl[li - 16] ? 1u : 0u) | (lx < 3 && wl[li + 16] ? 2u : 0u) | (ly > 0 && wl[li - 4] ? 4u : 0u) |
+                (ly < 3 && wl[li + 4] ? 8u : 0u) | (lz > 0 && wl[li - 1] ? 16u : 0u) | (lz < 3 && wl[li + 1] ? 32u : 0u);
+    }
+    const uint32_t colour0 = (uint32_t)((li0 >> 4) + ((li0 >> 2) & 3) + (li0 & 3)) % 2u;
+    for (uint32_t k = 0; k < 5; k++) {
+        const bool first = colour0 == k % 2u;  // this half-sweep's cell is the lane's first
+        if (first ? water[0] : water[1]) {
+            const int li = first ? li0 : li1;
+            const uint32_t m = first ? nm[0] : nm[1];
+            float s = first ? r[0] : r[1];
+            if (m & 1u) s += zl[li - 16];
+            if (m & 2u) s += zl[li + 16];
+            if (m & 4u) s += zl[li - 4];
+            if (m & 8u) s += zl[li + 4];
+            if (m & 16u) s += zl[li - 1];
+            if (m & 32u) s += zl[li + 1];
+            zl[li] = s / (first ? diag[0] : diag[1]);
         }
         __syncwarp();
     }
-    z[0] = zl[lane], z[1] = zl[lane + 32];
+    z[0] = zl[li0], z[1] = zl[li1];
     __syncwarp();
 }
 
-// The 256-wide tree over the published running sums (fluid.wgsl:434-438). All threads of the
-// CTA call it; every CTA gets the same value.
+// The 256-wide tree over the running sums (fluid.wgsl:434-438) of one quantity, by one warp:
+// lane l loads sums l, l + 32, ..., l + 224, does the levels 128, 64 and 32 in registers and
+// the rest with shuffles. Valid in lane 0.
 template <class A>
-__device__ __forceinline__ A tree256(const double* rs, A* red) {
-    if (threadIdx.x < 256) red[threadIdx.x] = (A)__ldcg(rs + threadIdx.x);
-    __syncthreads();
-    for (int off = 128; off >= 32; off >>= 1) {
-        if ((int)threadIdx.x < off) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + off];
-        __syncthreads();
-    }
-    if (threadIdx.x < 32) {
-        A x = red[threadIdx.x];
+__device__ __forceinline__ A warp_tree256(const double* sums, int q, int lane) {
+    A v[8];
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, off);
-        if (threadIdx.x == 0) red[0] = x;
-    }
-    __syncthreads();
-    A r = red[0];
-    __syncthreads();
-    return r;
+    for (int i = 0; i < 8; i++) v[i] = (A)__ldcg(sums + (size_t)(lane + 32 * i) * SOLVE_XQ + q);
+    // Level 128: positions l, l + 32, l + 64, l + 96 add l + 128, ... ; level 64; level 32.
+    const A a0 = v[0] + v[4], a1 = v[1] + v[5], a2 = v[2] + v[6], a3 = v[3] + v[7];
+    const A b0 = a0 + a2, b1 = a1 + a3;
+    A x = b0 + b1;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, off);
+    return x;
 }
 
+// Publishes this CTA's running sums (fluid.wgsl:429-431) of quantities 0..NQ-1 of `part`, waits
+// at the grid barrier, and returns the 256-wide trees in `out`. The sums are double-buffered
+// by the barrier's parity: a CTA writes the next-but-one sums only after every CTA has passed
+// the next barrier, that is, has read these. False (in every thread) if the wait gave up.
+template <class A, int NQ>
+__device__ __forceinline__ bool exchange(const Dev& D, DevState* st, uint32_t& gen, A (*part)[2][SOLVE_MAX_M],
+                                         uint32_t c, uint32_t G, uint32_t n_res, uint32_t nb, A (&out)[NQ]) {
+    __shared__ uint32_t s_ok;
+    gen++;
+    double* sums = D.xsum + (size_t)(gen & 1u) * 256u * SOLVE_XQ;
+    __syncthreads();  // every warp's partials and cell writes of this phase are done
+    if (threadIdx.x < n_res * NQ) {
+        const uint32_t ri = threadIdx.x / NQ, q = threadIdx.x % NQ, r = c + ri * G;
+        const uint32_t cnt = r < nb ? (nb - r + 255u) / 256u : 0u;
+        A s = A(0);
+        for (uint32_t m = 0; m < cnt; m++) s = s + part[q][ri][m];
+        sums[r * SOLVE_XQ + q] = (double)s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // Release: this CTA's writes (ordered before by the barrier above) before the arrival.
+        const uint32_t target = gen * G;
+        atom_add_release(&st->bar_count, 1u);
+        uint32_t ok = 1u;
+        for (uint32_t spins = 0; ld_acquire(&st->bar_count) < target;)
+            if (++spins > BARRIER_SPINS) {
+                atomicOr(&st->err, 1u);
+                ok = 0u;
+                break;
+            }
+        s_ok = ok;
+    }
+    __syncthreads();
+    if (!s_ok) return false;
+    // One warp forms the trees; every CTA gets the same values.
+    __shared__ A s_out[SOLVE_XQ];
+    if (threadIdx.x < 32)
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+            const A x = warp_tree256<A>(sums, q, (int)threadIdx.x);
+            if (threadIdx.x == 0) s_out[q] = x;
+        }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NQ; q++) out[q] = s_out[q];
+    return true;
+}
+
+// A lane's two cells of one block (solve_cell): the solver's values for them.
+struct SolveCells {
+    float diag[2], z[2], d[2], r[2], p[2], q[2];
+    uint32_t wn[2][6];  // water neighbours in solve_q's order (-x, +x, -y, +y, -z, +z), or NONE
+    bool water[2];
+};
+
 template <bool FP64>
-__global__ void __launch_bounds__(SOLVE_T) k_solve(Dev D) {
+__global__ void __launch_bounds__(SOLVE_T, 2) k_solve(Dev D) {
     using M = SolveMath<FP64>;
     using A = typename M::A;
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
-    uint32_t gen = *(volatile uint32_t*)&st->bar_gen;
+    uint32_t gen = 0;
     const Grid g = grid_of(D, cur_of(st));
     const ntr_gpu_params* U = D.U;
     const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
@@ -171,7 +208,6 @@ __global__ void __launch_bounds__(SOLVE_T) k_solve(Dev D) {
     __shared__ A part[3][2][SOLVE_MAX_M];
     __shared__ float zl[SOLVE_W][64];
     __shared__ uint8_t wl[SOLVE_W][64];
-    __shared__ A red[256];
     // Read before the first barrier: CTA 0 writes them back at the end. alpha keeps the last
     // step's value when the solver does not run, as the reference's state does.
     uint32_t iters_max = st->s.iters_max, unconverged = st->s.unconverged;
@@ -179,165 +215,232 @@ __global__ void __launch_bounds__(SOLVE_T) k_solve(Dev D) {
     // Residues of this CTA: c, c + G (G >= 128 keeps it to two).
     const uint32_t n_res = (c + G < 256u) ? 2u : 1u;
     auto count_of = [&](uint32_t r) -> uint32_t { return r < nb ? (nb - r + 255u) / 256u : 0u; };
-
-    // Runs `body(b, ri, m)` for every block this CTA owns, one warp per block.
-    auto for_my_blocks = [&](auto&& body) {
-        uint32_t e = 0;
-        for (uint32_t ri = 0; ri < n_res; ri++) {
-            const uint32_t r = c + ri * G;
-            const uint32_t cnt = count_of(r);
-            for (uint32_t m = 0; m < cnt; m++, e++)
-                if ((int)(e % SOLVE_W) == warp) body(r + 256u * m, ri, m);
-        }
+    const uint32_t cnt0 = count_of(c), n_mine = cnt0 + (n_res > 1 ? count_of(c + G) : 0u);
+    // The warp's j-th block: the CTA's (warp + j * SOLVE_W)-th, residue by residue.
+    auto block_of = [&](uint32_t e, uint32_t& b, uint32_t& ri, uint32_t& m) {
+        ri = e < cnt0 ? 0u : 1u;
+        m = e - (ri ? cnt0 : 0u);
+        b = c + ri * G + 256u * m;
     };
-    // Lane r's running sum (fluid.wgsl:429-431) of quantity q, into rs[r].
-    auto publish = [&](int q, double* rs) {
-        __syncthreads();
-        if (threadIdx.x < n_res) {
-            const uint32_t ri = threadIdx.x, r = c + ri * G;
-            A s = A(0);
-            const uint32_t cnt = count_of(r);
-            for (uint32_t m = 0; m < cnt; m++) s = s + part[q][ri][m];
-            rs[r] = (double)s;
-        }
-    };
+    const uint32_t n_warp = n_mine > (uint32_t)warp ? (n_mine - 1u - (uint32_t)warp) / SOLVE_W + 1u : 0u;
+    const bool in_regs = (n_mine + SOLVE_W - 1) / SOLVE_W <= (uint32_t)SOLVE_R;
+    SolveCells R[SOLVE_R];
 
-    // solve_init (fluid.wgsl:445-491): diagonal, right-hand side, residual, preconditioned
+    // ---- solve_init (fluid.wgsl:445-491): diagonal, right-hand side, residual, preconditioned
     // residual, and the block's (r.z, r.r, b.b).
-    for_my_blocks([&](uint32_t b, uint32_t ri, uint32_t m) {
-        float r[2], diag[2], bq[2], z[2];
-        bool water[2];
+    auto init_block = [&](SolveCells& C, uint32_t b, uint32_t ri, uint32_t m) {
+        uint32_t cell[2];
+        float bq[2];
+        // One cell after the other (to bound the registers), each with all its loads first.
+#pragma unroll
         for (int k = 0; k < 2; k++) {
-            const uint32_t cell = b * 64u + lane + 32u * k;
-            water[k] = cfv(D, F_TYPE, cell) == WATER_T;
-            diag[k] = 1.0f, r[k] = 0.0f, bq[k] = 0.0f;
-            if (!water[k]) continue;
+            cell[k] = b * 64u + solve_cell(lane, k);
+            uint32_t nbr[6];
+            float nty[6], np[6], nu[3], uc[3];
+#pragma unroll
+            for (int j = 0; j < 6; j++) nbr[j] = neighbour(g, cell[k], ed(j >> 1, (j & 1) ? 1 : -1));
+            const float ty = cfv(D, F_TYPE, cell[k]);
+            const float pc = cfv(D, F_P, cell[k]);
+            const float dold = cfv(D, F_D, cell[k]);
+            const int32_t src = accv(D, A_SRC, cell[k]);
+#pragma unroll
+            for (int d = 0; d < 3; d++) uc[d] = cfv(D, F_U + d, cell[k]);
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                nty[j] = GAS_T, np[j] = 0.0f;
+                if (nbr[j] != NONE) nty[j] = cfv(D, F_TYPE, nbr[j]), np[j] = cfv(D, F_P, nbr[j]);
+            }
+#pragma unroll
+            for (int d = 0; d < 3; d++) nu[d] = nbr[2 * d + 1] != NONE ? cfv(D, F_U + d, nbr[2 * d + 1]) : 0.0f;
+            C.water[k] = ty == WATER_T;
+            C.diag[k] = 1.0f, C.r[k] = 0.0f, C.p[k] = pc, C.d[k] = dold, bq[k] = 0.0f;
+#pragma unroll
+            for (int j = 0; j < 6; j++) C.wn[k][j] = NONE;
+            if (!C.water[k]) continue;
             float cs = U->gravity[3] * dt;
             float kc = hh * hh / (cs * cs);
             float div = 0.0f, off = 0.0f;
-            float dg = kc, bb = kc * cfv(D, F_P, cell);
-            uint32_t wn[8] = {NONE, NONE, NONE, NONE, NONE, NONE, NONE, NONE};
-            for (uint32_t d = 0; d < 3; d++) {
-                div += face_u(D, neighbour(g, cell, ed(d, 1)), cell, d) - face_u(D, cell, neighbour(g, cell, ed(d, -1)), d);
-                for (int s = -1; s <= 1; s += 2) {
-                    uint32_t nbc = neighbour(g, cell, ed(d, s));
-                    float nt = cell_type(D, nbc);
-                    if (nt == SOLID_T) continue;
+            float dg = kc, bb = kc * pc;
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                // face_u of the face above (its cell the neighbour, below it this cell) minus
+                // the face below (this cell over the neighbour below).
+                const float fu_hi = nbr[2 * d + 1] == NONE ? 0.0f : bounded(nu[d], nty[2 * d + 1], ty);
+                const float fu_lo = bounded(uc[d], ty, nty[2 * d]);
+                div += fu_hi - fu_lo;
+#pragma unroll
+                for (int s = 0; s < 2; s++) {
+                    const int j = 2 * d + s;
+                    if (nty[j] == SOLID_T) continue;
                     dg += 1.0f;
-                    if (nt == WATER_T) {
-                        off -= cfv(D, F_P, nbc);
-                        wn[2 * d + (s > 0 ? 1 : 0)] = nbc;
+                    if (nty[j] == WATER_T) {
+                        off -= np[j];
+                        C.wn[k][j] = nbr[j];
                     } else {
-                        bb += pressure_of(D, nbc);
+                        bb += np[j];  // pressure_of: 0 outside the grid, p of a non-water cell
                     }
                 }
             }
-            // The water neighbours, in the order solve_q visits them, for the iterations.
-            uint4* wp = reinterpret_cast<uint4*>(D.wnb + (size_t)cell * 8);
-            wp[0] = make_uint4(wn[0], wn[1], wn[2], wn[3]);
-            wp[1] = make_uint4(wn[4], wn[5], NONE, NONE);
-            div -= from_fp(accv(D, A_SRC, cell), FP_Q) / (hh * hh);
+            div -= from_fp(src, FP_Q) / (hh * hh);
             bb -= rho * hh / dt * div;
-            float rr = bb - dg * cfv(D, F_P, cell) - off;
-            *cfp(D, F_DIAG, cell) = dg;
-            *cfp(D, F_R, cell) = rr;
-            diag[k] = dg, r[k] = rr, bq[k] = bb;
+            C.r[k] = bb - dg * pc - off;
+            C.diag[k] = dg, bq[k] = bb;
         }
-        warp_precondition(zl[warp], wl[warp], lane, r, diag, water, z);
+        for (int k = 0; k < 2; k++) {
+            if (!C.water[k]) continue;
+            *cfp(D, F_DIAG, cell[k]) = C.diag[k];
+            *cfp(D, F_R, cell[k]) = C.r[k];
+            if (!in_regs) {
+                uint4* wp = reinterpret_cast<uint4*>(D.wnb + (size_t)cell[k] * 8);
+                wp[0] = make_uint4(C.wn[k][0], C.wn[k][1], C.wn[k][2], C.wn[k][3]);
+                wp[1] = make_uint4(C.wn[k][4], C.wn[k][5], NONE, NONE);
+            }
+        }
+        warp_precondition(zl[warp], wl[warp], lane, C.r, C.diag, C.water, C.z);
         for (int k = 0; k < 2; k++)
-            if (water[k]) *cfp(D, F_Z, b * 64u + lane + 32u * k) = z[k];
-        A sx = warp_tree64(M::prod(r[0], z[0]), M::prod(r[1], z[1]));
-        A sy = warp_tree64(M::prod(r[0], r[0]), M::prod(r[1], r[1]));
+            if (C.water[k]) *cfp(D, F_Z, cell[k]) = C.z[k];
+        A sx = warp_tree64(M::prod(C.r[0], C.z[0]), M::prod(C.r[1], C.z[1]));
+        A sy = warp_tree64(M::prod(C.r[0], C.r[0]), M::prod(C.r[1], C.r[1]));
         A sz = warp_tree64(M::prod(bq[0], bq[0]), M::prod(bq[1], bq[1]));
         if (lane == 0) part[0][ri][m] = sx, part[1][ri][m] = sy, part[2][ri][m] = sz;
-    });
-    publish(0, D.px);
-    publish(1, D.py);
-    publish(2, D.pz);
-    if (!grid_sync(st, gen)) return;
+    };
+
+    // ---- solve_q (fluid.wgsl:513-534): the new search direction and A d. `old` is the parity
+    // of the direction field the last iteration wrote.
+    auto q_block = [&](SolveCells& C, uint32_t b, uint32_t ri, uint32_t m, uint32_t old, float fbeta) {
+        uint32_t cell[2];
+        for (int k = 0; k < 2; k++) cell[k] = b * 64u + solve_cell(lane, k);
+        if (!in_regs) {
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                C.water[k] = cfv(D, F_TYPE, cell[k]) == WATER_T;
+                C.z[k] = cfv(D, F_Z, cell[k]);
+                C.d[k] = cfv(D, F_D + old, cell[k]);
+                C.diag[k] = cfv(D, F_DIAG, cell[k]);
+                const uint4* wp = reinterpret_cast<const uint4*>(D.wnb + (size_t)cell[k] * 8);
+                const uint4 w0 = wp[0], w1 = wp[1];
+                C.wn[k][0] = w0.x, C.wn[k][1] = w0.y, C.wn[k][2] = w0.z, C.wn[k][3] = w0.w;
+                C.wn[k][4] = w1.x, C.wn[k][5] = w1.y;
+            }
+        }
+        // The neighbours' z and old d were written by other warps and CTAs earlier in this
+        // launch: read through L2.
+        float zn[2][6], dnb[2][6];
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+#pragma unroll
+            for (int j = 0; j < 6; j++) {
+                zn[k][j] = 0.0f, dnb[k][j] = 0.0f;
+                const uint32_t n = C.wn[k][j];
+                if (C.water[k] && n != NONE) zn[k][j] = __ldcg(cfp(D, F_Z, n)), dnb[k][j] = __ldcg(cfp(D, F_D + old, n));
+            }
+        A v[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            v[k] = A(0);
+            if (!C.water[k]) continue;
+            const float dn = C.z[k] + fbeta * C.d[k];
+            float q = C.diag[k] * dn;
+#pragma unroll
+            for (int j = 0; j < 6; j++)
+                if (C.wn[k][j] != NONE) q -= zn[k][j] + fbeta * dnb[k][j];
+            *cfp(D, F_D + 1 - old, cell[k]) = dn;
+            if (!in_regs) *cfp(D, F_Q, cell[k]) = q;
+            C.d[k] = dn, C.q[k] = q;
+            v[k] = M::prod(dn, q);
+        }
+        A s = warp_tree64(v[0], v[1]);
+        if (lane == 0) part[0][ri][m] = s;
+    };
+
+    // ---- solve_update (fluid.wgsl:543-559): p, r, and the preconditioned residual. `nw` is
+    // the parity of the direction field this iteration's solve_q wrote.
+    auto update_block = [&](SolveCells& C, uint32_t b, uint32_t ri, uint32_t m, uint32_t nw, float a) {
+        uint32_t cell[2];
+        for (int k = 0; k < 2; k++) cell[k] = b * 64u + solve_cell(lane, k);
+        if (!in_regs) {
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                C.water[k] = cfv(D, F_TYPE, cell[k]) == WATER_T;
+                C.p[k] = cfv(D, F_P, cell[k]);
+                C.d[k] = cfv(D, F_D + nw, cell[k]);
+                C.r[k] = cfv(D, F_R, cell[k]);
+                C.q[k] = cfv(D, F_Q, cell[k]);
+                C.diag[k] = cfv(D, F_DIAG, cell[k]);
+            }
+        }
+        float r[2], diag[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            diag[k] = 1.0f, r[k] = 0.0f;
+            if (!C.water[k]) continue;
+            C.p[k] = C.p[k] + a * C.d[k];
+            C.r[k] = C.r[k] - a * C.q[k];
+            if (!in_regs) {
+                *cfp(D, F_P, cell[k]) = C.p[k];
+                *cfp(D, F_R, cell[k]) = C.r[k];
+            }
+            r[k] = C.r[k], diag[k] = C.diag[k];
+        }
+        warp_precondition(zl[warp], wl[warp], lane, r, diag, C.water, C.z);
+        for (int k = 0; k < 2; k++)
+            if (C.water[k]) *cfp(D, F_Z, cell[k]) = C.z[k];
+        A sx = warp_tree64(M::prod(r[0], C.z[0]), M::prod(r[1], C.z[1]));
+        A sy = warp_tree64(M::prod(r[0], r[0]), M::prod(r[1], r[1]));
+        if (lane == 0) part[0][ri][m] = sx, part[1][ri][m] = sy;
+    };
+
+    // Runs `body(C, b, ri, m)` over the warp's blocks.
+    auto each_block = [&](auto&& body) {
+        if (in_regs) {
+#pragma unroll
+            for (int j = 0; j < SOLVE_R; j++)
+                if ((uint32_t)j < n_warp) {
+                    uint32_t b, ri, m;
+                    block_of((uint32_t)warp + (uint32_t)j * SOLVE_W, b, ri, m);
+                    body(R[j], b, ri, m);
+                }
+        } else {
+            for (uint32_t j = 0; j < n_warp; j++) {
+                uint32_t b, ri, m;
+                block_of((uint32_t)warp + j * SOLVE_W, b, ri, m);
+                body(R[0], b, ri, m);
+            }
+        }
+    };
+
+    each_block([&](SolveCells& C, uint32_t b, uint32_t ri, uint32_t m) { init_block(C, b, ri, m); });
 
     // solve_start (fluid.wgsl:493-506).
     double rz, beta = 0.0, b_norm, r_norm;
     uint32_t iters = 0;
     bool on;
     {
-        A sx = tree256<A>(D.px, red);
-        A sy = tree256<A>(D.py, red);
-        A sz = tree256<A>(D.pz, red);
+        A s3[3];
+        if (!exchange<A, 3>(D, st, gen, part, c, G, n_res, nb, s3)) return;
+        const A sx = s3[0], sy = s3[1], sz = s3[2];
         rz = (double)sx;
         b_norm = M::root((double)sz);
         r_norm = M::root((double)sy);
         on = (double)sx > 0.0 && !M::converged((double)sy, b_norm, tol);
     }
     while (on) {
-        // solve_q (fluid.wgsl:513-534): the new search direction and A d.
         const uint32_t old = iters % 2u;
         const float fbeta = (float)beta;
-        for_my_blocks([&](uint32_t b, uint32_t ri, uint32_t m) {
-            A v[2];
-            for (int k = 0; k < 2; k++) {
-                const uint32_t cell = b * 64u + lane + 32u * k;
-                v[k] = A(0);
-                if (cfv(D, F_TYPE, cell) != WATER_T) continue;
-                float dn = cfv(D, F_Z, cell) + fbeta * cfv(D, F_D + old, cell);
-                float q = cfv(D, F_DIAG, cell) * dn;
-                const uint4* wp = reinterpret_cast<const uint4*>(D.wnb + (size_t)cell * 8);
-                const uint4 w0 = wp[0], w1 = wp[1];
-                const uint32_t wn[6] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y};
-                // All neighbour loads first (written by other CTAs earlier in this launch:
-                // read through L2), then the sum in the reference's order.
-                float zn[6], dnb[6];
-#pragma unroll
-                for (int k = 0; k < 6; k++) {
-                    zn[k] = 0.0f, dnb[k] = 0.0f;
-                    if (wn[k] != NONE) zn[k] = __ldcg(cfp(D, F_Z, wn[k])), dnb[k] = __ldcg(cfp(D, F_D + old, wn[k]));
-                }
-#pragma unroll
-                for (int k = 0; k < 6; k++)
-                    if (wn[k] != NONE) q -= zn[k] + fbeta * dnb[k];
-                *cfp(D, F_D + 1 - old, cell) = dn;
-                *cfp(D, F_Q, cell) = q;
-                v[k] = M::prod(dn, q);
-            }
-            A s = warp_tree64(v[0], v[1]);
-            if (lane == 0) part[0][ri][m] = s;
-        });
-        publish(0, D.pq);
-        if (!grid_sync(st, gen)) return;
+        each_block([&](SolveCells& C, uint32_t b, uint32_t ri, uint32_t m) { q_block(C, b, ri, m, old, fbeta); });
         // solve_alpha (fluid.wgsl:536-541).
         {
-            A s = tree256<A>(D.pq, red);
-            alpha = (double)s > 0.0 ? M::ratio(rz, (double)s) : 0.0;
+            A s1[1];
+            if (!exchange<A, 1>(D, st, gen, part, c, G, n_res, nb, s1)) return;
+            alpha = (double)s1[0] > 0.0 ? M::ratio(rz, (double)s1[0]) : 0.0;
         }
-        // solve_update (fluid.wgsl:543-559): p, r, and the preconditioned residual.
         const float a = (float)alpha;
-        for_my_blocks([&](uint32_t b, uint32_t ri, uint32_t m) {
-            float r[2], diag[2], z[2];
-            bool water[2];
-            for (int k = 0; k < 2; k++) {
-                const uint32_t cell = b * 64u + lane + 32u * k;
-                water[k] = cfv(D, F_TYPE, cell) == WATER_T;
-                diag[k] = 1.0f, r[k] = 0.0f;
-                if (!water[k]) continue;
-                *cfp(D, F_P, cell) = cfv(D, F_P, cell) + a * cfv(D, F_D + 1 - old, cell);
-                r[k] = cfv(D, F_R, cell) - a * cfv(D, F_Q, cell);
-                *cfp(D, F_R, cell) = r[k];
-                diag[k] = cfv(D, F_DIAG, cell);
-            }
-            warp_precondition(zl[warp], wl[warp], lane, r, diag, water, z);
-            for (int k = 0; k < 2; k++)
-                if (water[k]) *cfp(D, F_Z, b * 64u + lane + 32u * k) = z[k];
-            A sx = warp_tree64(M::prod(r[0], z[0]), M::prod(r[1], z[1]));
-            A sy = warp_tree64(M::prod(r[0], r[0]), M::prod(r[1], r[1]));
-            if (lane == 0) part[0][ri][m] = sx, part[1][ri][m] = sy;
-        });
-        publish(0, D.px);
-        publish(1, D.py);
-        if (!grid_sync(st, gen)) return;
+        each_block([&](SolveCells& C, uint32_t b, uint32_t ri, uint32_t m) { update_block(C, b, ri, m, 1u - old, a); });
         // solve_beta (fluid.wgsl:561-578).
         {
-            A sx = tree256<A>(D.px, red);
-            A sy = tree256<A>(D.py, red);
+            A s2[2];
+            if (!exchange<A, 2>(D, st, gen, part, c, G, n_res, nb, s2)) return;
+            const A sx = s2[0], sy = s2[1];
             iters += 1;
             r_norm = M::root((double)sy);
             beta = rz > 0.0 ? M::ratio((double)sx, rz) : 0.0;
@@ -350,6 +453,17 @@ __global__ void __launch_bounds__(SOLVE_T) k_solve(Dev D) {
             }
         }
     }
+    // The fields kept in registers go to memory once, as the iterations would have left them.
+    if (in_regs && iters > 0)
+        each_block([&](SolveCells& C, uint32_t b, uint32_t, uint32_t) {
+            for (int k = 0; k < 2; k++) {
+                if (!C.water[k]) continue;
+                const uint32_t cell = b * 64u + solve_cell(lane, k);
+                *cfp(D, F_P, cell) = C.p[k];
+                *cfp(D, F_R, cell) = C.r[k];
+                *cfp(D, F_Q, cell) = C.q[k];
+            }
+        });
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         st->rz = rz, st->alpha = alpha, st->beta = beta, st->b_norm = b_norm, st->r_norm = r_norm;
         st->solver_on = 0u;

@@ -168,10 +168,7 @@ static ntr_status allocate(Sim& S) {
     AL(D.cf, (size_t)NTR_CELL_FIELDS * D.cap_cells);
     AL(D.air[0], (size_t)NTR_AIR_FIELDS * D.cap_cells);
     AL(D.air[1], (size_t)NTR_AIR_FIELDS * D.cap_cells);
-    AL(D.px, D.cap_blocks);
-    AL(D.py, D.cap_blocks);
-    AL(D.pz, D.cap_blocks);
-    AL(D.pq, D.cap_blocks);
+    AL(D.xsum, 2u * 256u * SOLVE_XQ);
     for (int k = 0; k < 2; k++) {
         AL(D.mem_x[k], D.Nv);
         AL(D.mem_v[k], D.Nv);
@@ -419,7 +416,7 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     L(k_air_fill, G_cell, 256, D);
     L(k_bullet_step, n_shots, BULLET_T, D);
     L(k_bullet_apply, G_cell, 256, D);
-    // The whole pressure solve: one cooperative launch, its grid barrier reset first.
+    // The whole pressure solve: one cooperative launch, its grid barrier's counter reset first.
     cudaMemsetAsync(&D.st->bar_count, 0, 4, s);
     {
         cudaLaunchConfig_t cfg = {};
