@@ -59,6 +59,7 @@ typedef enum ntr_status {
 #define NTR_CELL_FIELDS 11
 #define NTR_AIR_FIELDS 5
 #define NTR_LAYER_MODES 6
+#define NTR_MAX_VALENCE 64 /* triangles per membrane vertex, at most */
 
 /* One bullet fired at the balloon. Mirrors `Shot` (src/params.rs:205-264). `bullet` indexes
  * the table of loads (src/params.rs:193-201): 0 .22 LR, 1 9 mm, 2 .45 ACP, 3 M855, 4 .308,

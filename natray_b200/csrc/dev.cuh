@@ -118,6 +118,7 @@ struct Dev {
     float* mem_mass;
     const Tri* tris;
     uint32_t *alive, *vtri_off, *vtri;
+    float4* tri_rec;  // per triangle: what its vertices fold into their force sums, 4 float4
     DBullet* bullets;
     const float4* patches;
     const float2* outlines;
@@ -230,15 +231,15 @@ __device__ __forceinline__ float nt_exp(float x) {
     if (x > 88.72284f) return __uint_as_float(0x7f800000u);
     if (x < -103.972084f) return 0.0f;
     float k = rintf(x * 1.442695f);
-    float r = (x - k * 0.693145751953125f) - k * 1.4286068e-06f;
+    float r = __fmaf_rn(-k, 1.4286068e-06f, x - k * 0.693145751953125f);  // k * 0.693145751953125 is exact
     float p = 0.0001984127f;
-    p = p * r + 0.0013888889f;
-    p = p * r + 0.008333334f;
-    p = p * r + 0.041666668f;
-    p = p * r + 0.16666667f;
-    p = p * r + 0.5f;
-    p = p * r + 1.0f;
-    p = p * r + 1.0f;
+    p = __fmaf_rn(p, r, 0.0013888889f);
+    p = __fmaf_rn(p, r, 0.008333334f);
+    p = __fmaf_rn(p, r, 0.041666668f);
+    p = __fmaf_rn(p, r, 0.16666667f);
+    p = __fmaf_rn(p, r, 0.5f);
+    p = __fmaf_rn(p, r, 1.0f);
+    p = __fmaf_rn(p, r, 1.0f);
     return nt_scale2(p, (int)k);
 }
 __device__ __forceinline__ float nt_log(float x) {
@@ -262,11 +263,11 @@ __device__ __forceinline__ float nt_log(float x) {
     float s = (m - 1.0f) / (m + 1.0f);
     float z = s * s;
     float p = 0.09090909f;
-    p = p * z + 0.11111111f;
-    p = p * z + 0.14285715f;
-    p = p * z + 0.2f;
-    p = p * z + 0.33333334f;
-    p = p * z + 1.0f;
+    p = __fmaf_rn(p, z, 0.11111111f);
+    p = __fmaf_rn(p, z, 0.14285715f);
+    p = __fmaf_rn(p, z, 0.2f);
+    p = __fmaf_rn(p, z, 0.33333334f);
+    p = __fmaf_rn(p, z, 1.0f);
     float lm = 2.0f * s * p;
     float fe = (float)e;
     return fe * 0.693145751953125f + (lm + fe * 1.4286068e-06f);
@@ -276,16 +277,16 @@ __device__ __forceinline__ void nt_sincos(float x, float* so, float* co) {
     float r = ((x - k * 1.5703125f) - k * 0.0004838268f) - k * 2.563283e-12f;
     float z = r * r;
     float ps = 2.7557319e-06f;
-    ps = ps * z - 0.0001984127f;
-    ps = ps * z + 0.008333334f;
-    ps = ps * z - 0.16666667f;
-    float sr = r + r * z * ps;
+    ps = __fmaf_rn(ps, z, -0.0001984127f);
+    ps = __fmaf_rn(ps, z, 0.008333334f);
+    ps = __fmaf_rn(ps, z, -0.16666667f);
+    float sr = __fmaf_rn(r * z, ps, r);
     float pc = -2.755732e-07f;
-    pc = pc * z + 2.4801588e-05f;
-    pc = pc * z - 0.0013888889f;
-    pc = pc * z + 0.041666668f;
-    pc = pc * z - 0.5f;
-    float cr = 1.0f + z * pc;
+    pc = __fmaf_rn(pc, z, 2.4801588e-05f);
+    pc = __fmaf_rn(pc, z, -0.0013888889f);
+    pc = __fmaf_rn(pc, z, 0.041666668f);
+    pc = __fmaf_rn(pc, z, -0.5f);
+    float cr = __fmaf_rn(z, pc, 1.0f);
     int q = ((int)k) & 3;
     *so = q == 0 ? sr : q == 1 ? cr : q == 2 ? -sr : -cr;
     *co = q == 0 ? cr : q == 1 ? -sr : q == 2 ? -cr : sr;
@@ -303,19 +304,19 @@ __device__ __forceinline__ float nt_cos(float x) {
 __device__ __forceinline__ float nt_asin_series(float t) {
     float z = t * t;
     float p = 0.0057400377f;
-    p = p * z + 0.0064472104f;
-    p = p * z + 0.007312526f;
-    p = p * z + 0.008390335f;
-    p = p * z + 0.009761609f;
-    p = p * z + 0.011551801f;
-    p = p * z + 0.013964844f;
-    p = p * z + 0.017352764f;
-    p = p * z + 0.022372158f;
-    p = p * z + 0.030381944f;
-    p = p * z + 0.04464286f;
-    p = p * z + 0.075f;
-    p = p * z + 0.16666667f;
-    return t + t * z * p;
+    p = __fmaf_rn(p, z, 0.0064472104f);
+    p = __fmaf_rn(p, z, 0.007312526f);
+    p = __fmaf_rn(p, z, 0.008390335f);
+    p = __fmaf_rn(p, z, 0.009761609f);
+    p = __fmaf_rn(p, z, 0.011551801f);
+    p = __fmaf_rn(p, z, 0.013964844f);
+    p = __fmaf_rn(p, z, 0.017352764f);
+    p = __fmaf_rn(p, z, 0.022372158f);
+    p = __fmaf_rn(p, z, 0.030381944f);
+    p = __fmaf_rn(p, z, 0.04464286f);
+    p = __fmaf_rn(p, z, 0.075f);
+    p = __fmaf_rn(p, z, 0.16666667f);
+    return __fmaf_rn(t * z, p, t);
 }
 __device__ __forceinline__ float nt_asin(float x) {
     float a = fabsf(x);
@@ -410,6 +411,32 @@ __device__ __forceinline__ uint32_t neighbour(const Grid& g, uint32_t cell, I3 o
 __device__ __forceinline__ uint32_t cell_at(const Grid& g, I3 c) {
     if (c.x < 0 || c.y < 0 || c.z < 0 || (uint32_t)c.x >= g.dims[0] || (uint32_t)c.y >= g.dims[1] || (uint32_t)c.z >= g.dims[2]) return NONE;
     uint32_t b = lookup(g.mask, g.prefix, block_slot(g, shr2(c)), g.cap_blocks);
+    if (b == NONE) return NONE;
+    return b * 64u + (uint32_t)(c.x & 3) * 16u + (uint32_t)(c.y & 3) * 4u + (uint32_t)(c.z & 3);
+}
+// The cells of a 3^3 stencil with corner `base`: the up to 2 x 2 x 2 blocks that hold the cells
+// base .. base + 2 (per axis) are looked up once, all eight at the same time, instead of a
+// dependent lookup per cell. near_cell gives what cell_at gives, for cells of the stencil.
+struct CellsNear {
+    I3 b0;
+    uint32_t blk[8];  // blocks b0 + (x, y, z), x, y, z in {0, 1}, at x + 2 y + 4 z
+};
+__device__ __forceinline__ CellsNear near_of(const Grid& g, I3 base) {
+    CellsNear n;
+    n.b0 = shr2(base);
+#pragma unroll
+    for (int k = 0; k < 8; k++) n.blk[k] = block_at(g, n.b0 + I3{k & 1, (k >> 1) & 1, k >> 2});
+    return n;
+}
+// `c` is a cell of the stencil: base + (0..2, 0..2, 0..2), so its block is b0 or the next one
+// along each axis.
+__device__ __forceinline__ uint32_t near_cell(const Grid& g, const CellsNear& n, I3 c) {
+    if (c.x < 0 || c.y < 0 || c.z < 0 || (uint32_t)c.x >= g.dims[0] || (uint32_t)c.y >= g.dims[1] || (uint32_t)c.z >= g.dims[2]) return NONE;
+    const I3 d = shr2(c) - n.b0;
+    const uint32_t x0 = d.x ? n.blk[1] : n.blk[0], x1 = d.x ? n.blk[3] : n.blk[2];
+    const uint32_t x2 = d.x ? n.blk[5] : n.blk[4], x3 = d.x ? n.blk[7] : n.blk[6];
+    const uint32_t y0 = d.y ? x1 : x0, y1 = d.y ? x3 : x2;
+    const uint32_t b = d.z ? y1 : y0;
     if (b == NONE) return NONE;
     return b * 64u + (uint32_t)(c.x & 3) * 16u + (uint32_t)(c.y & 3) * 4u + (uint32_t)(c.z & 3);
 }

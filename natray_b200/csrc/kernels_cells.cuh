@@ -92,11 +92,12 @@ __device__ float gas_pressure_at(const Dev& D, const Grid& g, int buf, V3 x) {
     I3 base = vi(vfloor((x - g.org) / g.h - 1.0f));
     V3 fx = (x - g.org) / g.h - 0.5f - vf(base);
     V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
+    const CellsNear n = near_of(g, base);
     float sx = 0.0f, sy = 0.0f;
     for (int a = 0; a < 3; a++)
         for (int b = 0; b < 3; b++)
             for (int c = 0; c < 3; c++) {
-                uint32_t cell = cell_at(g, base + I3{a, b, c});
+                uint32_t cell = near_cell(g, n, base + I3{a, b, c});
                 float w = wx[a] * wy[b] * wz[c];
                 if (cell == NONE) {
                     sx = sx + w * P_ATM;
@@ -150,10 +151,11 @@ __global__ void k_mem_splat(Dev D) {
     I3 base = vi(vfloor(x - 0.5f));
     V3 fx = x - vf(base);
     V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
+    const CellsNear n = near_of(g, base);
     for (int a = 0; a < 3; a++)
         for (int b = 0; b < 3; b++)
             for (int c = 0; c < 3; c++) {
-                uint32_t cell = cell_at(g, base + I3{a, b, c});
+                uint32_t cell = near_cell(g, n, base + I3{a, b, c});
                 if (cell == NONE) continue;
                 float w = wx[a] * wy[b] * wz[c];
                 atomicAdd(accp(D, A_MF, cell), to_fp(w * pa.x, FP_F));
@@ -371,11 +373,12 @@ __device__ __forceinline__ float2 sample_grid(const Dev& D, const Grid& g, V3 x,
     I3 base = vi(vfloor(x - 0.5f));
     V3 fx = x - vf(base);
     V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
+    const CellsNear n = near_of(g, base);
     float sx = 0.0f, sy = 0.0f;
     for (int a = 0; a < 3; a++)
         for (int b = 0; b < 3; b++)
             for (int c = 0; c < 3; c++) {
-                uint32_t cell = cell_at(g, base + I3{a, b, c});
+                uint32_t cell = near_cell(g, n, base + I3{a, b, c});
                 if (cell == NONE) continue;
                 float w = wx[a] * wy[b] * wz[c] * from_fp(accv(D, fw, cell), FP_W);
                 sx = sx + w * cfv(D, fu, cell);
@@ -384,20 +387,28 @@ __device__ __forceinline__ float2 sample_grid(const Dev& D, const Grid& g, V3 x,
     return make_float2(sx, sy);
 }
 
+// Four lanes per vertex, one per stencil (the three velocity lattices and the cell centres).
 __global__ void k_mem_sample(Dev D) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= D.Nv || D.mem_mass[i] == 0.0f) return;
-    V3 x = (xyz(D.mem_x[0][i]) - g.org) / g.h;
-    V3 v = {0.0f, 0.0f, 0.0f};
-    for (uint32_t d = 0; d < 3; d++) {
-        float2 s = sample_grid(D, g, x - lattice_offset(d), F_U + d, a_wt(d));
-        v[d] = s.y > 1e-6f ? s.x / s.y : 0.0f;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = t >> 2, q = t & 3u;
+    const bool act = i < D.Nv && D.mem_mass[i] != 0.0f;
+    float r = 0.0f;
+    if (act) {
+        V3 x = (xyz(D.mem_x[0][i]) - g.org) / g.h;
+        if (q < 3u) {
+            float2 s = sample_grid(D, g, x - lattice_offset(q), F_U + q, a_wt(q));
+            r = s.y > 1e-6f ? s.x / s.y : 0.0f;
+        } else {
+            r = sample_grid(D, g, x - 0.5f, F_TYPE, A_WC).y / 8.0f;
+        }
     }
-    float fill = sample_grid(D, g, x - 0.5f, F_TYPE, A_WC).y / 8.0f;
-    D.mem_water[i] = f4(v, fill);
+    const int l0 = (int)(threadIdx.x & 28u);
+    const float v0 = __shfl_sync(0xffffffffu, r, l0), v1 = __shfl_sync(0xffffffffu, r, l0 + 1);
+    const float v2 = __shfl_sync(0xffffffffu, r, l0 + 2), v3 = __shfl_sync(0xffffffffu, r, l0 + 3);
+    if (act && q == 0u) D.mem_water[i] = make_float4(v0, v1, v2, v3);
 }
 
 // ---- air_substep, air.wgsl:237-269 --------------------------------------------------------------------

@@ -75,15 +75,21 @@ __global__ void k_clear(Dev D) {
     for (size_t w = tid; w < D.nwords; w += stride) m[w] = 0u;
 }
 
-// Sets the bit of block `slot` once per distinct slot of the warp.
-__device__ __forceinline__ void set_block_bit(uint32_t* mask, uint32_t slot, bool valid) {
-    uint32_t key = valid ? slot : NONE;
-    uint32_t peers = __match_any_sync(0xffffffffu, key);
-    if (valid && (__ffs(peers) - 1) == (int)(threadIdx.x & 31u)) atomicOr(mask + (slot >> 5), 1u << (slot & 31u));
+// Sets the bits of the blocks `slot` of the lanes where `valid`: one atomicOr per distinct
+// word of the bitmask in the warp, with the bits of all its lanes. All 32 lanes call it.
+__device__ __forceinline__ void set_block_bits(uint32_t* mask, uint32_t slot, bool valid) {
+    const uint32_t word = valid ? slot >> 5 : NONE;
+    const uint32_t peers = __match_any_sync(0xffffffffu, word);
+    const uint32_t bits = __reduce_or_sync(peers, valid ? 1u << (slot & 31u) : 0u);
+    if (valid && (__ffs(peers) - 1) == (int)(threadIdx.x & 31u)) atomicOr(mask + word, bits);
 }
 
+__host__ __device__ __forceinline__ uint32_t warp_round(uint32_t n) { return (n + 31u) & ~31u; }
+
 // ---- mark: particles' stencils, active air, dry rubber (fluid.wgsl:131-150, air.wgsl:271-277,
-// membrane.wgsl:164-180). One thread per particle, then per last-step block, then per vertex.
+// membrane.wgsl:164-180). Three ranges of threads, each a whole number of warps: one thread per
+// particle, per last-step block (up to the block capacity), per vertex. Every lane of a warp
+// runs the same loop, so the bits are merged per warp before they go out.
 __global__ void k_mark(Dev D) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
@@ -96,10 +102,9 @@ __global__ void k_mark(Dev D) {
     auto clampb = [&](I3 b) {
         return I3{min(max(b.x, 0), bmax.x), min(max(b.y, 0), bmax.y), min(max(b.z, 0), bmax.z)};
     };
-    {
-        // Every lane of the warp runs the loop over the up to 2x2x2 blocks of a particle's
-        // stencil (lanes without a live particle claim nothing), so the warp-wide match is
-        // taken by all 32 lanes.
+    const uint32_t np_w = warp_round(D.Np), nb_w = warp_round(D.cap_blocks);
+    if (i < np_w) {
+        // The up to 2x2x2 blocks of a particle's stencil.
         const bool isp = i < D.Np;
         bool alive = false;
         I3 lo = {0, 0, 0}, hi = {-1, -1, -1};
@@ -115,31 +120,36 @@ __global__ void k_mark(Dev D) {
         for (int k = 0; k < 8; k++) {
             I3 b = {lo.x + (k & 1), lo.y + ((k >> 1) & 1), lo.z + ((k >> 2) & 1)};
             bool valid = alive && b.x <= hi.x && b.y <= hi.y && b.z <= hi.z;
-            set_block_bit(mask, valid ? block_slot(g, b) : 0u, valid);
-        }
-        if (isp) return;
-    }
-    uint32_t j = i - D.Np;
-    if (j < n_prev) {
-        if (D.block_active[j] != 0u) {
-            uint32_t s = D.block_list[cur ^ 1][j];
-            atomicOr(mask + (s >> 5), 1u << (s & 31u));
+            set_block_bits(mask, valid ? block_slot(g, b) : 0u, valid);
         }
         return;
     }
-    j -= n_prev;
+    uint32_t j = i - np_w;
+    if (j < nb_w) {
+        const bool valid = j < n_prev && D.block_active[j] != 0u;
+        set_block_bits(mask, valid ? D.block_list[cur ^ 1][j] : 0u, valid);
+        return;
+    }
+    j -= nb_w;
+    if (j >= warp_round(D.Nv)) return;
+    // Dry rubber: the blocks within two cells of the vertex (at most 3 per axis).
+    bool dry = false;
+    I3 lo = {0, 0, 0}, hi = {-1, -1, -1};
     if (j < D.Nv) {
         float2 push = D.mem_push[j];
         bool on_water = D.mem_mass[j] > 0.0f && D.mem_water[j].w >= CONTACT_F;
-        if (push.y <= 0.0f || on_water) return;
-        I3 c = own_cell(g, xyz(D.mem_x[0][j]));
-        I3 lo = clampb(shr2(c - I3{2, 2, 2})), hi = clampb(shr2(c + I3{3, 3, 3}));
-        for (int x = lo.x; x <= hi.x; x++)
-            for (int y = lo.y; y <= hi.y; y++)
-                for (int z = lo.z; z <= hi.z; z++) {
-                    uint32_t s = block_slot(g, I3{x, y, z});
-                    atomicOr(mask + (s >> 5), 1u << (s & 31u));
-                }
+        dry = !(push.y <= 0.0f || on_water);
+        if (dry) {
+            I3 c = own_cell(g, xyz(D.mem_x[0][j]));
+            lo = clampb(shr2(c - I3{2, 2, 2}));
+            hi = clampb(shr2(c + I3{3, 3, 3}));
+        }
+    }
+    if (!__any_sync(0xffffffffu, dry)) return;
+    for (int k = 0; k < 27; k++) {
+        I3 b = {lo.x + k / 9, lo.y + (k / 3) % 3, lo.z + k % 3};
+        bool valid = dry && b.x <= hi.x && b.y <= hi.y && b.z <= hi.z;
+        set_block_bits(mask, valid ? block_slot(g, b) : 0u, valid);
     }
 }
 

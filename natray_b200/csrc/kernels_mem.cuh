@@ -51,22 +51,34 @@ struct VertexForce {
     float area, stiff, tension, reach, thick;
 };
 
-__device__ VertexForce vertex_force(const Dev& D, int par, uint32_t i) {
+// The rubber's triangles, once per substep (membrane.wgsl:67-149, the part of vertex_force that
+// does not depend on which of its vertices asks): the stretch, the Ogden stresses, and what the
+// vertices fold into their sums. One thread per triangle, so the stresses are computed once
+// instead of once per vertex. Per triangle four float4 in `tri_rec`:
+//   {h1, vol}, {h2, tangent + sx}, {e1 x e2, |e1 x e2| / 6}, {rest / 3, tension, reach, kind}
+// with kind 0: dead at the start of the substep (not counted), 1: tore now (counts for the
+// reach only), 2: counted.
+//
+// `alive` holds the state at the start of the substep until this kernel writes the tears, and
+// the vertices read the kind, so every vertex of a triangle sees the same thing. The reference
+// writes a tear into `alive` while the triangle's other vertices may still be reading it, and
+// whether they count it then depends on the threads' timing.
+__global__ void k_mem_tri(Dev D, int par) {
     const ntr_gpu_params* U = D.U;
     const float4* X = D.mem_x[par];
     const float thick0 = U->rubber[3];
-    VertexForce o = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, 0.0f, 0.0f, 0.0f, 0.0f, thick0};
-    float rest = 0.0f;
-    const uint32_t k0 = D.vtri_off[i], k1 = D.vtri_off[i + 1];
-    for (uint32_t k = k0; k < k1; k++) {
-        uint32_t t = D.vtri[k];
-        if (*(volatile uint32_t*)&D.alive[t] == 0u) continue;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < D.Nt; t += gridDim.x * blockDim.x) {
+        float4* rec = D.tri_rec + 4 * (size_t)t;
+        if (D.alive[t] == 0u) {
+            rec[3] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(0u));
+            continue;
+        }
         const Tri tri = D.tris[t];
         V3 x0 = xyz(X[tri.v0]);
         V3 e1 = xyz(X[tri.v1]) - x0;
         V3 e2 = xyz(X[tri.v2]) - x0;
         const float mxx = tri.dm_inv.x, myy = tri.dm_inv.y, mzz = tri.dm_inv.z, mww = tri.dm_inv.w;
-        o.reach = mx(o.reach, mx(length(e1), mx(length(e2), length(e2 - e1))));
+        const float reach = mx(length(e1), mx(length(e2), length(e2 - e1)));
         V3 f0 = e1 * mxx + e2 * mzz;
         V3 f1 = e1 * myy + e2 * mww;
         float c00 = dot(f0, f0), c01 = dot(f0, f1), c11 = dot(f1, f1);
@@ -74,7 +86,8 @@ __device__ VertexForce vertex_force(const Dev& D, int par, uint32_t i) {
         float dev = sqrtf(0.25f * (c00 - c11) * (c00 - c11) + c01 * c01);
         float lx = sqrtf(mid + dev), ly = sqrtf(mx(mid - dev, 1e-12f));
         if (lx >= U->rubber2[1]) {
-            *(volatile uint32_t*)&D.alive[t] = 0u;
+            D.alive[t] = 0u;
+            rec[3] = make_float4(0.0f, 0.0f, reach, __uint_as_float(1u));
             continue;
         }
         Sheet sh = sheet(U, lx, ly);
@@ -98,6 +111,32 @@ __device__ VertexForce vertex_force(const Dev& D, int par, uint32_t i) {
         float vol = tri.rest_area * thick0;
         V3 h1 = (-vol) * (p0 * mxx + p1 * myy);
         V3 h2 = (-vol) * (p0 * mzz + p1 * mww);
+        V3 cr = cross(e1, e2);
+        rec[0] = f4(h1, vol);
+        rec[1] = f4(h2, sh.tangent + sx);
+        rec[2] = f4(cr, length(cr) / 6.0f);
+        rec[3] = make_float4(tri.rest_area / 3.0f, sh.sx * thick0 / (lx * ly), reach, __uint_as_float(2u));
+    }
+}
+
+// vertex_force (membrane.wgsl:67-149): the vertex's triangles' records, folded in its order.
+__device__ VertexForce vertex_force(const Dev& D, uint32_t i) {
+    const float thick0 = D.U->rubber[3];
+    VertexForce o = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, 0.0f, 0.0f, 0.0f, 0.0f, thick0};
+    float rest = 0.0f;
+    const uint32_t k0 = D.vtri_off[i], k1 = D.vtri_off[i + 1];
+    for (uint32_t k = k0; k < k1; k++) {
+        const uint32_t t = D.vtri[k];
+        const float4* rec = D.tri_rec + 4 * (size_t)t;
+        const float4 r3 = rec[3];
+        const uint32_t kind = __float_as_uint(r3.w);
+        if (kind == 0u) continue;
+        o.reach = mx(o.reach, r3.z);
+        if (kind == 1u) continue;
+        const Tri tri = D.tris[t];
+        const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2];
+        const float mxx = tri.dm_inv.x, myy = tri.dm_inv.y, mzz = tri.dm_inv.z, mww = tri.dm_inv.w;
+        const V3 h1 = xyz(r0), h2 = xyz(r1);
         float gx = mxx, gy = myy;
         if (i == tri.v0) {
             o.f = o.f - (h1 + h2);
@@ -108,12 +147,11 @@ __device__ VertexForce vertex_force(const Dev& D, int par, uint32_t i) {
             o.f = o.f + h2;
             gx = mzz, gy = mww;
         }
-        V3 cr = cross(e1, e2);
-        o.n = o.n + cr;
-        o.area += length(cr) / 6.0f;
-        rest += tri.rest_area / 3.0f;
-        o.stiff += vol * (gx * gx + gy * gy) * (sh.tangent + sx);
-        o.tension = mx(o.tension, sh.sx * thick0 / (lx * ly));
+        o.n = o.n + xyz(r2);
+        o.area += r2.w;
+        rest += r3.x;
+        o.stiff += r0.w * (gx * gx + gy * gy) * r1.w;
+        o.tension = mx(o.tension, r3.y);
     }
     if (o.area > 0.0f) o.thick = thick0 * rest / o.area;
     return o;
@@ -190,7 +228,7 @@ __device__ float rubber_contact(const Dev& D, int par, uint32_t i, V3& x, V3& v,
             uint32_t own = 0, n = 1;
             if (k < k1) {
                 uint32_t tn = D.vtri[k];
-                if (*(volatile uint32_t*)&D.alive[tn] == 0u) continue;
+                if (D.alive[tn] == 0u) continue;  // dead, or tore in this substep (k_mem_tri)
                 const Tri tri = D.tris[tn];
                 uint32_t ids[3] = {tri.v0, tri.v1, tri.v2};
                 for (uint32_t c = 0; c < 3; c++) {
@@ -299,7 +337,7 @@ __global__ void __launch_bounds__(256) k_mem_substep(Dev D, uint32_t k, int par)
             const float hh = g.h;
             const float sub = dt / (float)max(U->mem[1], 1u);
             const float t_sub = now - dt + (float)(k + 1u) * sub;
-            VertexForce vf = vertex_force(D, par, i);
+            const VertexForce vf = vertex_force(D, i);
             lim_x = sqrtf(m / mx(vf.stiff, 1e-30f));
             if (vf.tension > 0.0f) lim_y = sqrtf(U->fluid[0] * hh * hh * hh / (4.0f * PI_F * vf.tension));
             V3 f = vf.f + m * v3(U->gravity[0], U->gravity[1], U->gravity[2]);
@@ -395,11 +433,12 @@ __device__ __forceinline__ float2 sample_pressure(const Dev& D, const Grid& g, V
     I3 base = vi(vfloor(x - 0.5f));
     V3 fx = x - vf(base);
     V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
+    const CellsNear n = near_of(g, base);
     float sx = 0.0f, sy = 0.0f;
     for (int a = 0; a < 3; a++)
         for (int b = 0; b < 3; b++)
             for (int c = 0; c < 3; c++) {
-                uint32_t cell = cell_at(g, base + I3{a, b, c});
+                uint32_t cell = near_cell(g, n, base + I3{a, b, c});
                 if (cell == NONE) continue;
                 float ty = cfv(D, F_TYPE, cell);
                 if (ty == SOLID_T || (gas_only && ty == WATER_T)) continue;
@@ -430,6 +469,7 @@ __device__ void push_water(const Dev& D, const Grid& g, V3 x, uint32_t d, float 
     if (sw <= 1e-6f || j == 0.0f) return;
     V3 lx = x - lattice_offset(d);
     I3 base = vi(vfloor(lx - 0.5f));
+    const CellsNear n = near_of(g, base);
     V3 fx = lx - vf(base);
     V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
     float hs = D.U->fluid[3];
@@ -437,7 +477,7 @@ __device__ void push_water(const Dev& D, const Grid& g, V3 x, uint32_t d, float 
     for (int a = 0; a < 3; a++)
         for (int b = 0; b < 3; b++)
             for (int c = 0; c < 3; c++) {
-                uint32_t cell = cell_at(g, base + I3{a, b, c});
+                uint32_t cell = near_cell(g, n, base + I3{a, b, c});
                 if (cell == NONE || accv(D, a_wt(d), cell) <= 0) continue;
                 atomicAdd(accp(D, A_BU + d, cell), to_fp(k * wx[a] * wy[b] * wz[c], FP_M));
             }
@@ -461,20 +501,26 @@ __global__ void __launch_bounds__(BULLET_T) k_bullet_step(Dev D) {
     __shared__ float s_pf;
     __shared__ float4 s_side;
     __shared__ float4 red_f[256], red_t[256], red_c[256];
+    __shared__ int32_t s_hit[NTR_HIT_FIELDS];
     int32_t* hit = D.bullet_hit + bi * NTR_HIT_FIELDS;
+    uint32_t state = b.info.z;
+    if (state == 0u && st->s.t_ns - st->s.dt_ns >= b.info.x) state = 1u;
+    // The membrane's contact sums since the last step, taken and cleared one word per thread:
+    // the wetted-side sums always, the impulses only when the bullet flies this step.
+    if (li < NTR_HIT_FIELDS) s_hit[li] = (li >= 6u || state == 1u) ? atomicExch(hit + li, 0) : 0;
+    __syncthreads();
     if (li == 0) {
-        uint32_t state = b.info.z;
-        if (state == 0u && st->s.t_ns - st->s.dt_ns >= b.info.x) state = 1u;
         s_state = state;
         V3 ahead = xyz(b.x) + normalize(xyz(b.v) + 1e-9f) * (b.shape.z + 3.0f * hh);
-        float2 s = sample_pressure(D, g, (ahead - g.org) / hh - 0.5f, false);
+        const V3 xa = (ahead - g.org) / hh - 0.5f;
+        float2 s = sample_pressure(D, g, xa, false);
         s_pf = s.y > 1e-6f ? s.x / s.y : 0.0f;
         V3 sn, sx;
         for (int c = 0; c < 3; c++) {
-            sn[c] = from_fp(atomicExch(hit + 6 + c, 0), FP_A);
-            sx[c] = from_fp(atomicExch(hit + 9 + c, 0), FP_X);
+            sn[c] = from_fp(s_hit[6 + c], FP_A);
+            sx[c] = from_fp(s_hit[9 + c], FP_X);
         }
-        float sa = from_fp(atomicExch(hit + 12, 0), FP_A);
+        float sa = from_fp(s_hit[12], FP_A);
         s_side = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (sa > 0.0f && length(sn) > 0.0f) {
             V3 n = normalize(sn);
@@ -482,7 +528,6 @@ __global__ void __launch_bounds__(BULLET_T) k_bullet_step(Dev D) {
         }
     }
     __syncthreads();
-    const uint32_t state = s_state;
     if (state != 1u) {
         if (li == 0) {
             D.bullets[bi].info.z = state;
@@ -587,17 +632,26 @@ __global__ void __launch_bounds__(BULLET_T) k_bullet_step(Dev D) {
         __syncthreads();
     }
     const float hand2 = R_HAND * R_HAND * hh * hh;
+    // The new velocity and position (every thread; the 27 blocks around it are looked up in
+    // parallel), then the rest by one thread.
+    V3 hitv, hit_l;
+    for (int c = 0; c < 3; c++) {
+        hitv[c] = from_fp(s_hit[c], FP_J);
+        hit_l[c] = from_fp(s_hit[3 + c], FP_L);
+    }
+    const float4 rf = red_f[0], rt4 = red_t[0], rc = red_c[0];
+    V3 force = xyz(rf) + b.x.w * v3(U->gravity[0], U->gravity[1], U->gravity[2]);
+    V3 v = xyz(b.v) + (force * step + hitv) / b.x.w;
+    V3 x = xyz(b.x) + v * step;
+    bool near_k = false;
+    if (li < 27u) {
+        const I3 c = shr2(own_cell(g, x));
+        const I3 nb = c + I3{(int32_t)(li / 9u), (int32_t)((li / 3u) % 3u), (int32_t)(li % 3u)} - I3{1, 1, 1};
+        near_k = block_at(g, nb) != NONE;
+    }
+    const bool nearb = __syncthreads_or(near_k) != 0;
     if (li == 0) {
-        V3 hitv, hit_l;
-        for (int c = 0; c < 3; c++) {
-            hitv[c] = from_fp(atomicExch(hit + c, 0), FP_J);
-            hit_l[c] = from_fp(atomicExch(hit + 3 + c, 0), FP_L);
-        }
-        const float4 rf = red_f[0], rt4 = red_t[0], rc = red_c[0];
-        V3 force = xyz(rf) + b.x.w * v3(U->gravity[0], U->gravity[1], U->gravity[2]);
         float drag = rf.w, face = rt4.w;
-        V3 v = xyz(b.v) + (force * step + hitv) / b.x.w;
-        V3 x = xyz(b.x) + v * step;
         V3 l = xyz(b.l) + xyz(rt4) * step + hit_l;
         V3 axis0 = qrot(b.q, v3(0.0f, 0.0f, 1.0f));
         float spin_extra = dot(l, axis0) * (1.0f / b.shape.x - 1.0f / b.shape.y) * step;
@@ -613,12 +667,6 @@ __global__ void __launch_bounds__(BULLET_T) k_bullet_step(Dev D) {
         info.z = 1u;
         V3 hi = g.org + v3((float)g.dims[0], (float)g.dims[1], (float)g.dims[2]) * hh;
         if (x.x < g.org.x || x.y < g.org.y || x.z < g.org.z || x.x > hi.x || x.y > hi.y || x.z > hi.z) info.z = 2u;
-        I3 c = shr2(own_cell(g, x));
-        bool nearb = false;
-        for (uint32_t k = 0; k < 27; k++) {
-            I3 nb = c + I3{(int32_t)(k / 9u), (int32_t)((k / 3u) % 3u), (int32_t)(k % 3u)} - I3{1, 1, 1};
-            if (block_at(g, nb) != NONE) nearb = true;
-        }
         float pace = nearb ? length(v) : length(v) * U->fluid[1] / 4.0f;
         if (drag > 0.0f && face > 0.0f) {
             V3 mid = xyz(rc) / face;
@@ -659,10 +707,11 @@ __global__ void __launch_bounds__(BULLET_T) k_bullet_step(Dev D) {
             I3 base = vi(vfloor(xx - 0.5f));
             V3 fx = xx - vf(base);
             V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
+            const CellsNear n = near_of(g, base);
             for (int a = 0; a < 3; a++)
                 for (int bb = 0; bb < 3; bb++)
                     for (int cc = 0; cc < 3; cc++) {
-                        uint32_t cell = cell_at(g, base + I3{a, bb, cc});
+                        uint32_t cell = near_cell(g, n, base + I3{a, bb, cc});
                         if (cell == NONE) continue;
                         atomicAdd(accp(D, A_SRC, cell), to_fp(qv * wx[a] * wy[bb] * wz[cc], FP_Q));
                     }

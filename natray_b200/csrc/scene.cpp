@@ -1110,6 +1110,30 @@ bool deserialize(const void* blob, size_t len, World& w, std::string& err) {
         }
         w.sec[s].assign(b + w.h.offset[s], b + w.h.offset[s] + need);
     }
+    // The mesh indexes device arrays: every index must be in range, and a vertex may be in at
+    // most NTR_MAX_VALENCE triangles (the rubber substep keeps one bit per triangle of a vertex).
+    const uint32_t* off = w.as<uint32_t>(NTR_SEC_VTRI_OFF);
+    const uint32_t* vt = w.as<uint32_t>(NTR_SEC_VTRI);
+    if (off[0] != 0u || off[w.h.n_verts] != w.h.n_vtri) {
+        err = "world blob vertex-triangle offsets out of range";
+        return false;
+    }
+    for (uint32_t i = 0; i < w.h.n_verts; i++)
+        if (off[i + 1] < off[i] || off[i + 1] - off[i] > NTR_MAX_VALENCE) {
+            err = "world blob vertex in more than " + std::to_string(NTR_MAX_VALENCE) + " triangles, or offsets decreasing";
+            return false;
+        }
+    for (uint32_t k = 0; k < w.h.n_vtri; k++)
+        if (vt[k] >= w.h.n_tris) {
+            err = "world blob vertex-triangle index out of range";
+            return false;
+        }
+    const uint32_t* tri = w.as<uint32_t>(NTR_SEC_TRIS);
+    for (uint32_t t = 0; t < w.h.n_tris; t++)
+        if (tri[8 * (size_t)t] >= w.h.n_verts || tri[8 * (size_t)t + 1] >= w.h.n_verts || tri[8 * (size_t)t + 2] >= w.h.n_verts) {
+            err = "world blob triangle vertex out of range";
+            return false;
+        }
     return true;
 }
 

@@ -181,6 +181,7 @@ static ntr_status allocate(Sim& S) {
     AL(tris, D.Nt);
     D.tris = tris;
     AL(D.alive, D.Nt);
+    AL(D.tri_rec, (size_t)D.Nt * 4);
     AL(D.vtri_off, D.Nv + 1);
     AL(D.vtri, h.n_vtri);
     AL(D.bullets, NTR_MAX_SHOTS);
@@ -311,6 +312,7 @@ static ntr_status read_state(Sim& S) {
 static ntr_status measure_rubber(Sim& S) {
     Dev& D = S.D;
     CU(cudaMemsetAsync(&D.st->s.dt_ns, 0, 4, S.stream));
+    k_mem_tri<<<std::max((D.Nt + 255) / 256, 1u), 256, 0, S.stream>>>(D, 0);
     k_mem_substep<<<(D.Nv + 255) / 256, 256, 0, S.stream>>>(D, 0, 0);
     CU(cudaGetLastError());
     ntr_status r = read_state(S);
@@ -357,6 +359,7 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     const uint32_t G_blk = (uint32_t)S.sms * 8;
     const uint32_t g_part = (D.Np + 255) / 256 ? (D.Np + 255) / 256 : 1;
     const uint32_t g_vert = (D.Nv + 255) / 256 ? (D.Nv + 255) / 256 : 1;
+    const uint32_t g_tri = std::max((D.Nt + 255) / 256, 1u);
     const uint32_t n_shots = S.U.mem[3] ? S.U.mem[3] : 1;
 #define L(kern, grid, block, ...)                       \
     do {                                                \
@@ -367,7 +370,7 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     if (prof) prof->mark("start", s);
     L(k_begin_step, 1, 32, D);
     L(k_clear, G_cell, 256, D);
-    L(k_mark, (uint32_t)(((uint64_t)D.Np + D.cap_blocks + D.Nv + 255) / 256), 256, D);
+    L(k_mark, (uint32_t)(((uint64_t)warp_round(D.Np) + warp_round(D.cap_blocks) + warp_round(D.Nv) + 255) / 256), 256, D);
     L(k_scan_words_a, D.scan_ctas, SCAN_T, D);
     L(k_scan_words_b, D.scan_ctas, SCAN_T, D);
     L(k_keys, g_part, 256, D);
@@ -440,9 +443,12 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     // G2P shares nothing with the rubber and air substeps or the spray's flight: they run
     // side by side.
     fork(1);
-    LA(k_mem_sample, g_vert, 256, D);
+    LA(k_mem_sample, (uint32_t)(((uint64_t)D.Nv * 4 + 255) / 256), 256, D);
     for (uint32_t i = 0; i < std::max(n_mem, n_air); i++) {
-        if (i < n_mem) LA(k_mem_substep, g_vert, 256, D, i, (int)(i % 2));
+        if (i < n_mem) {
+            LA(k_mem_tri, g_tri, 256, D, (int)(i % 2));
+            LA(k_mem_substep, g_vert, 256, D, i, (int)(i % 2));
+        }
         if (i < n_air) LA(k_air_substep, G_cell, 256, D, (int)(i % 2));
     }
     LA(k_spray_update, G_cell, 256, D);

@@ -173,15 +173,15 @@ static inline float exp_(float x) {
     if (x > 88.72284f) return INFINITY;
     if (x < -103.972084f) return 0.0f;
     float k = std::nearbyint(x * 1.442695f);
-    float r = (x - k * 0.693145751953125f) - k * 1.4286068e-06f;
+    float r = std::fmaf(-k, 1.4286068e-06f, x - k * 0.693145751953125f);  // k * 0.693145751953125 is exact
     float p = 0.0001984127f;
-    p = p * r + 0.0013888889f;
-    p = p * r + 0.008333334f;
-    p = p * r + 0.041666668f;
-    p = p * r + 0.16666667f;
-    p = p * r + 0.5f;
-    p = p * r + 1.0f;
-    p = p * r + 1.0f;
+    p = std::fmaf(p, r, 0.0013888889f);
+    p = std::fmaf(p, r, 0.008333334f);
+    p = std::fmaf(p, r, 0.041666668f);
+    p = std::fmaf(p, r, 0.16666667f);
+    p = std::fmaf(p, r, 0.5f);
+    p = std::fmaf(p, r, 1.0f);
+    p = std::fmaf(p, r, 1.0f);
     return scale2(p, (int)k);
 }
 static inline float log_(float x) {
@@ -205,11 +205,11 @@ static inline float log_(float x) {
     float s = (m - 1.0f) / (m + 1.0f);
     float z = s * s;
     float p = 0.09090909f;
-    p = p * z + 0.11111111f;
-    p = p * z + 0.14285715f;
-    p = p * z + 0.2f;
-    p = p * z + 0.33333334f;
-    p = p * z + 1.0f;
+    p = std::fmaf(p, z, 0.11111111f);
+    p = std::fmaf(p, z, 0.14285715f);
+    p = std::fmaf(p, z, 0.2f);
+    p = std::fmaf(p, z, 0.33333334f);
+    p = std::fmaf(p, z, 1.0f);
     float lm = 2.0f * s * p;
     float fe = (float)e;
     return fe * 0.693145751953125f + (lm + fe * 1.4286068e-06f);
@@ -219,16 +219,16 @@ static inline void sincos_(float x, float* so, float* co) {
     float r = ((x - k * 1.5703125f) - k * 0.0004838268f) - k * 2.563283e-12f;
     float z = r * r;
     float ps = 2.7557319e-06f;
-    ps = ps * z - 0.0001984127f;
-    ps = ps * z + 0.008333334f;
-    ps = ps * z - 0.16666667f;
-    float sr = r + r * z * ps;
+    ps = std::fmaf(ps, z, -0.0001984127f);
+    ps = std::fmaf(ps, z, 0.008333334f);
+    ps = std::fmaf(ps, z, -0.16666667f);
+    float sr = std::fmaf(r * z, ps, r);
     float pc = -2.755732e-07f;
-    pc = pc * z + 2.4801588e-05f;
-    pc = pc * z - 0.0013888889f;
-    pc = pc * z + 0.041666668f;
-    pc = pc * z - 0.5f;
-    float cr = 1.0f + z * pc;
+    pc = std::fmaf(pc, z, 2.4801588e-05f);
+    pc = std::fmaf(pc, z, -0.0013888889f);
+    pc = std::fmaf(pc, z, 0.041666668f);
+    pc = std::fmaf(pc, z, -0.5f);
+    float cr = std::fmaf(z, pc, 1.0f);
     int q = ((int)k) & 3;
     float s = q == 0 ? sr : q == 1 ? cr : q == 2 ? -sr : -cr;
     float c = q == 0 ? cr : q == 1 ? -sr : q == 2 ? -cr : sr;
@@ -250,8 +250,8 @@ static inline float asin_series(float t) {
                          0.011551801f, 0.009761609f, 0.008390335f, 0.007312526f, 0.0064472104f, 0.0057400377f};
     float z = t * t;
     float p = C[12];
-    for (int i = 11; i >= 0; i--) p = p * z + C[i];
-    return t + t * z * p;
+    for (int i = 11; i >= 0; i--) p = std::fmaf(p, z, C[i]);
+    return std::fmaf(t * z, p, t);
 }
 static inline float asin_(float x) {
     float a = std::fabs(x);
@@ -391,6 +391,7 @@ struct Sim {
     std::vector<R> mem_mass;
     std::vector<Tri> tris;
     std::vector<uint32_t> alive, vtri_off, vtri;
+    std::vector<uint8_t> torn;  // triangles torn during the current rubber substep
     // Bullets.
     Bullet<R> bullets[4];
     std::vector<V4<R>> patches;  // p, n pairs
@@ -552,6 +553,7 @@ struct Sim {
     struct VertexForce {
         V3<R> f, n;
         R area, stiff, tension, reach, thick;
+        uint64_t torn;  // bit j: the vertex's j-th triangle tore in this substep
     };
     struct Sheet {
         V2<R> sig;
@@ -689,6 +691,7 @@ bool Sim<R>::load(const void* blob, size_t len, std::string& err) {
     tris.resize(Nt);
     std::memcpy(tris.data(), b + hdr.offset[NTR_SEC_TRIS], (size_t)Nt * 32);
     alive.assign(secu(NTR_SEC_ALIVE), secu(NTR_SEC_ALIVE) + Nt);
+    torn.assign(Nt, 0u);
     vtri_off.assign(secu(NTR_SEC_VTRI_OFF), secu(NTR_SEC_VTRI_OFF) + Nv + 1);
     vtri.assign(secu(NTR_SEC_VTRI), secu(NTR_SEC_VTRI) + hdr.n_vtri);
     const float* bf = sec(NTR_SEC_BULLETS);
@@ -1853,15 +1856,16 @@ typename Sim<R>::Sheet Sim<R>::sheet(R major, R minor) const {
 template <class R>
 typename Sim<R>::VertexForce Sim<R>::vertex_force(int par, uint32_t i) {
     const auto& X = mem_x[par];
-    VertexForce o = {{R(0), R(0), R(0)}, {R(0), R(0), R(0)}, R(0), R(0), R(0), R(0), R(U.rubber[3])};
+    VertexForce o = {{R(0), R(0), R(0)}, {R(0), R(0), R(0)}, R(0), R(0), R(0), R(0), R(U.rubber[3]), 0u};
     R rest = R(0);
     const R thick0 = R(U.rubber[3]);
+    // `alive` holds the state at the start of the substep for the whole substep: every vertex
+    // of a triangle sees it alive, evaluates the same stretch and so the same tear (the
+    // reference writes the tear at once, and what the triangle's other vertices then see depends
+    // on the threads' timing). Tears are committed after the substep (mem_substep).
     for (uint32_t k = vtri_off[i]; k < vtri_off[i + 1]; k++) {
         uint32_t t = vtri[k];
-        uint32_t al;
-#pragma omp atomic read
-        al = alive[t];
-        if (al == 0u) continue;
+        if (alive[t] == 0u) continue;
         const Tri& tri = tris[t];
         V3<R> x0 = X[tri.v0].xyz();
         V3<R> e1 = X[tri.v1].xyz() - x0;
@@ -1876,7 +1880,8 @@ typename Sim<R>::VertexForce Sim<R>::vertex_force(int par, uint32_t i) {
         V2<R> l = {std::sqrt(mid + dev), std::sqrt(mx(mid - dev, R(1e-12)))};
         if (l.x >= R(U.rubber2[1])) {
 #pragma omp atomic write
-            alive[t] = 0u;
+            torn[t] = 1u;
+            o.torn |= 1ull << (k - vtri_off[i]);
             continue;
         }
         Sheet sh = sheet(l.x, l.y);
@@ -2042,10 +2047,7 @@ R Sim<R>::rubber_contact(int par, uint32_t i, V3<R>& x, V3<R>& v, R m, V3<R> loa
             uint32_t own = 0, n = 1;
             if (k < vtri_off[i + 1]) {
                 uint32_t tn = vtri[k];
-                uint32_t al;
-#pragma omp atomic read
-                al = alive[tn];
-                if (al == 0u) continue;
+                if (alive[tn] == 0u || ((vf.torn >> (k - vtri_off[i])) & 1u)) continue;
                 const Tri& tri = tris[tn];
                 uint32_t ids[3] = {tri.v0, tri.v1, tri.v2};
                 for (uint32_t c = 0; c < 3; c++) {
@@ -2238,6 +2240,8 @@ void Sim<R>::mem_substep(uint32_t k, int par) {
         lo_x = mn(lo_x, l.x);
         lo_y = mn(lo_y, l.y);
     }
+    for (uint32_t t = 0; t < Nt; t++)
+        if (torn[t]) alive[t] = 0u, torn[t] = 0u;
     st.mem_dt = mn(st.mem_dt, lo_x);
     st.cap_dt = mn(st.cap_dt, lo_y);
 }

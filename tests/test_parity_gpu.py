@@ -102,6 +102,17 @@ def test_fixed_step_bb_shot_bit_exact():
     assert_worlds_equal(a, b, "fixed step")
 
 
+def test_solver_from_memory_bit_exact(oracle_threads):
+    # More blocks than the persistent solver has warps (256 CTAs x 12): its warps own two blocks
+    # or more, and keep the solver's values in memory instead of registers.
+    w = measured(build_world(Params(resolution=132, mesh_level=4, block_cap=65535, spray_cap=100000)))
+    o, s = Oracle(w.blob), Sim(world=w)
+    assert o.step(2) == s.step(2) == 2
+    assert s.state["n_blocks"] > 256 * 12 and s.state["solve_iters"] > 0
+    assert_grids_equal(o, s, "step 2")
+    assert_worlds_equal(World(o.snapshot()), s.snapshot(), "step 2")
+
+
 def test_reference_fp32_sums_bit_exact(w_small):
     o = Oracle(w_small.blob, fp64_dots=False)
     s = Sim(world=w_small, fp64_reductions=False)
