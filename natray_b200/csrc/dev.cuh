@@ -124,6 +124,8 @@ struct Dev {
     const float2* outlines;
     DSection* sections;
     int32_t* bullet_hit;
+    float4* bullet_prep;   // per bullet 4 float4: state and pressure ahead, wetted side, impulses
+    float4* bullet_patch;  // per bullet and patch 4 float4: force, torque, cavity share
     float4* pose_log;
     float4* spray;  // 3 float4 per slot: pos + r, vel + weight, air
     float4* landed;

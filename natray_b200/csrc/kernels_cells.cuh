@@ -387,6 +387,41 @@ __device__ __forceinline__ float2 sample_grid(const Dev& D, const Grid& g, V3 x,
     return make_float2(sx, sy);
 }
 
+// ---- 3^3 stencils taken by a warp: lane c < 27 has cell base + (c / 9, (c / 3) % 3, c % 3) --------
+__device__ __forceinline__ float wsel(V3 w, int i) { return i == 0 ? w.x : (i == 1 ? w.y : w.z); }
+
+// The sums of the lanes' `vx` and `vy` where `present`, added in lane order, which is the order
+// of the single-thread stencil loops (a, b, c). Every lane gets them.
+__device__ __forceinline__ float2 fold27(bool present, float vx, float vy) {
+    const uint32_t pm = __ballot_sync(0xffffffffu, present);
+    float sx = 0.0f, sy = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 27; c++) {
+        const float a = __shfl_sync(0xffffffffu, vx, c), b = __shfl_sync(0xffffffffu, vy, c);
+        if ((pm >> c) & 1u) sx = sx + a, sy = sy + b;
+    }
+    return make_float2(sx, sy);
+}
+
+// sample_grid by a warp.
+__device__ __forceinline__ float2 warp_sample_grid(const Dev& D, const Grid& g, V3 x, uint32_t fu, uint32_t fw, int lane) {
+    I3 base = vi(vfloor(x - 0.5f));
+    V3 fx = x - vf(base);
+    V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
+    const int a = lane / 9, b = (lane / 3) % 3, c = lane % 3;
+    bool present = false;
+    float wu = 0.0f, w = 0.0f;
+    if (lane < 27) {
+        const uint32_t cell = cell_at(g, base + I3{a, b, c});
+        if (cell != NONE) {
+            present = true;
+            w = wsel(wx, a) * wsel(wy, b) * wsel(wz, c) * from_fp(accv(D, fw, cell), FP_W);
+            wu = w * cfv(D, fu, cell);
+        }
+    }
+    return fold27(present, wu, w);
+}
+
 // Four lanes per vertex, one per stencil (the three velocity lattices and the cell centres).
 __global__ void k_mem_sample(Dev D) {
     const DevState* st = D.st;

@@ -429,196 +429,223 @@ __device__ __forceinline__ float cp_patch(float s) {
     return 0.5f + 1.81f * x - 2.0f * x * x;
 }
 
-__device__ __forceinline__ float2 sample_pressure(const Dev& D, const Grid& g, V3 x, bool gas_only) {
+__device__ __forceinline__ float section_r2(const DSection& s, float t) { return s.c.x + s.b.w * mx(t - s.a.w, 0.0f); }
+
+// sample_pressure by a warp.
+__device__ __forceinline__ float2 warp_sample_pressure(const Dev& D, const Grid& g, V3 x, bool gas_only, int lane) {
     I3 base = vi(vfloor(x - 0.5f));
     V3 fx = x - vf(base);
     V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
-    const CellsNear n = near_of(g, base);
-    float sx = 0.0f, sy = 0.0f;
-    for (int a = 0; a < 3; a++)
-        for (int b = 0; b < 3; b++)
-            for (int c = 0; c < 3; c++) {
-                uint32_t cell = near_cell(g, n, base + I3{a, b, c});
-                if (cell == NONE) continue;
-                float ty = cfv(D, F_TYPE, cell);
-                if (ty == SOLID_T || (gas_only && ty == WATER_T)) continue;
-                float w = wx[a] * wy[b] * wz[c];
-                sx = sx + w * cfv(D, F_P, cell);
-                sy = sy + w;
+    const int a = lane / 9, b = (lane / 3) % 3, c = lane % 3;
+    bool present = false;
+    float wp = 0.0f, w = 0.0f;
+    if (lane < 27) {
+        const uint32_t cell = cell_at(g, base + I3{a, b, c});
+        if (cell != NONE) {
+            const float ty = cfv(D, F_TYPE, cell);
+            if (!(ty == SOLID_T || (gas_only && ty == WATER_T))) {
+                present = true;
+                w = wsel(wx, a) * wsel(wy, b) * wsel(wz, c);
+                wp = w * cfv(D, F_P, cell);
             }
-    return make_float2(sx, sy);
-}
-
-__device__ __forceinline__ float section_r2(const DSection& s, float t) { return s.c.x + s.b.w * mx(t - s.a.w, 0.0f); }
-
-__device__ bool in_cavity(const Dev& D, float hh, uint32_t b, V3 p, float t) {
-    float hand2 = R_HAND * R_HAND * hh * hh;
-    for (uint32_t k = 0; k < NTR_N_SEC; k++) {
-        const DSection s = D.sections[b * NTR_N_SEC + k];
-        if (s.b.w <= 0.0f || section_r2(s, t) >= hand2) continue;
-        V3 ab = xyz(s.b) - xyz(s.a);
-        float f = dot(p - xyz(s.a), ab) / mx(dot(ab, ab), 1e-20f);
-        if (f < 0.0f || f > 1.0f) continue;
-        V3 d = p - (xyz(s.a) + f * ab);
-        if (dot(d, d) < section_r2(s, t)) return true;
+        }
     }
-    return false;
+    return fold27(present, wp, w);
 }
 
-__device__ void push_water(const Dev& D, const Grid& g, V3 x, uint32_t d, float j, float sw) {
+// push_water by a warp (integer sums: the lanes add their cells' shares in any order).
+__device__ __forceinline__ void warp_push_water(const Dev& D, const Grid& g, V3 x, uint32_t d, float j, float sw, int lane) {
     if (sw <= 1e-6f || j == 0.0f) return;
     V3 lx = x - lattice_offset(d);
     I3 base = vi(vfloor(lx - 0.5f));
-    const CellsNear n = near_of(g, base);
     V3 fx = lx - vf(base);
     V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
     float hs = D.U->fluid[3];
     float k = j / (D.U->fluid[0] * hs * hs * hs * sw);
-    for (int a = 0; a < 3; a++)
-        for (int b = 0; b < 3; b++)
-            for (int c = 0; c < 3; c++) {
-                uint32_t cell = near_cell(g, n, base + I3{a, b, c});
-                if (cell == NONE || accv(D, a_wt(d), cell) <= 0) continue;
-                atomicAdd(accp(D, A_BU + d, cell), to_fp(k * wx[a] * wy[b] * wz[c], FP_M));
-            }
+    if (lane >= 27) return;
+    const int a = lane / 9, b = (lane / 3) % 3, c = lane % 3;
+    const uint32_t cell = cell_at(g, base + I3{a, b, c});
+    if (cell == NONE || accv(D, a_wt(d), cell) <= 0) return;
+    atomicAdd(accp(D, A_BU + d, cell), to_fp(k * wsel(wx, a) * wsel(wy, b) * wsel(wz, c), FP_M));
 }
 
-// One CTA per bullet, one thread per surface patch (up to 768). The reference sums the
-// patches per lane (lane l takes patches l, l + 256, l + 512 in turn) and then by a 256-wide
-// tree; here the 256 lanes' running sums are formed in three rounds in that order, so the
-// sums are the reference's.
-constexpr int BULLET_T = 768;
-__global__ void __launch_bounds__(BULLET_T) k_bullet_step(Dev D) {
+// in_cavity by a warp: lane k tests section k.
+__device__ __forceinline__ bool warp_in_cavity(const Dev& D, float hh, uint32_t bi, V3 p, float t, int lane) {
+    static_assert(NTR_N_SEC == 32, "one lane per section");
+    const float hand2 = R_HAND * R_HAND * hh * hh;
+    const DSection s = D.sections[bi * NTR_N_SEC + lane];
+    bool in = false;
+    if (!(s.b.w <= 0.0f || section_r2(s, t) >= hand2)) {
+        V3 ab = xyz(s.b) - xyz(s.a);
+        float f = dot(p - xyz(s.a), ab) / mx(dot(ab, ab), 1e-20f);
+        if (!(f < 0.0f || f > 1.0f)) {
+            V3 dd = p - (xyz(s.a) + f * ab);
+            in = dot(dd, dd) < section_r2(s, t);
+        }
+    }
+    return __any_sync(0xffffffffu, in);
+}
+
+// The bullets' step (bullet.wgsl:186-383) in three launches:
+//   k_bullet_prep, a warp per bullet: whether it flies this step, the water pressure ahead of
+//     it, the membrane's contact sums (taken and cleared), into `bullet_prep`;
+//   k_bullet_patch, a warp per surface patch: the patch's loads and its push on the water, into
+//     `bullet_patch`;
+//   k_bullet_finish, a CTA per bullet: the patches summed in the reference's order (lane l of
+//     256 takes patches l, l + 256, l + 512 in turn, then a 256-wide tree), the rigid body, the
+//     cavity sections.
+__global__ void k_bullet_prep(Dev D) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const uint32_t bi = blockIdx.x;
+    const int lane = (int)threadIdx.x;
+    const Grid g = grid_of(D, cur_of(st));
+    const DBullet b = D.bullets[bi];
+    const float hh = g.h;
+    int32_t* hit = D.bullet_hit + bi * NTR_HIT_FIELDS;
+    uint32_t state = b.info.z;
+    if (state == 0u && st->s.t_ns - st->s.dt_ns >= b.info.x) state = 1u;
+    // The wetted-side sums always, the impulses only when the bullet flies this step.
+    int32_t hv = 0;
+    if (lane < NTR_HIT_FIELDS) hv = ((uint32_t)lane >= 6u || state == 1u) ? atomicExch(hit + lane, 0) : 0;
+    int32_t h[NTR_HIT_FIELDS];
+#pragma unroll
+    for (int c = 0; c < NTR_HIT_FIELDS; c++) h[c] = __shfl_sync(0xffffffffu, hv, c);
+    V3 ahead = xyz(b.x) + normalize(xyz(b.v) + 1e-9f) * (b.shape.z + 3.0f * hh);
+    const V3 xa = (ahead - g.org) / hh - 0.5f;
+    const float2 s = warp_sample_pressure(D, g, xa, false, lane);
+    if (lane != 0) return;
+    const float pf = s.y > 1e-6f ? s.x / s.y : 0.0f;
+    V3 sn, sx;
+    for (int c = 0; c < 3; c++) {
+        sn[c] = from_fp(h[6 + c], FP_A);
+        sx[c] = from_fp(h[9 + c], FP_X);
+    }
+    float sa = from_fp(h[12], FP_A);
+    float4 side = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (sa > 0.0f && length(sn) > 0.0f) {
+        V3 n = normalize(sn);
+        side = make_float4(n.x, n.y, n.z, dot(sx, n) / sa * 1e-3f);
+    }
+    float4* o = D.bullet_prep + bi * 4;
+    o[0] = make_float4(__uint_as_float(state), pf, 0.0f, 0.0f);
+    o[1] = side;
+    o[2] = make_float4(__int_as_float(h[0]), __int_as_float(h[1]), __int_as_float(h[2]), __int_as_float(h[3]));
+    o[3] = make_float4(__int_as_float(h[4]), __int_as_float(h[5]), 0.0f, 0.0f);
+    if (state != 1u) {
+        D.bullets[bi].info.z = state;
+        D.pose_log[(bi * NTR_LOG_CAP + st->s.step % NTR_LOG_CAP) * 3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+constexpr int BULLET_PW = 8;  // patch warps per CTA
+
+__global__ void __launch_bounds__(BULLET_PW * 32) k_bullet_patch(Dev D) {
+    DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const uint32_t bi = blockIdx.y;
+    const float4 pr = D.bullet_prep[bi * 4];
+    if (__float_as_uint(pr.x) != 1u) return;
+    const DBullet b = D.bullets[bi];
+    const uint32_t k = blockIdx.x * BULLET_PW + (threadIdx.x >> 5);
+    if (k >= b.info.y) return;
+    const int lane = (int)(threadIdx.x & 31u);
+    const Grid g = grid_of(D, cur_of(st));
+    const ntr_gpu_params* U = D.U;
+    const float step = dt_of(st), t_end = now_of(st), hh = g.h;
+    const float pf = pr.y;
+    const float4 side = D.bullet_prep[bi * 4 + 1];
+    V3 lb = qrot(make_float4(-b.q.x, -b.q.y, -b.q.z, b.q.w), xyz(b.l));
+    V3 w = qrot(b.q, lb / v3(b.shape.y, b.shape.y, b.shape.x));
+    const float rho = U->fluid[0];
+    const V3 vhat = normalize(xyz(b.v) + 1e-9f);
+    // The patch's force, torque, push on the water, and share of the wetted face.
+    V3 fp = {0.0f, 0.0f, 0.0f}, tqp = {0.0f, 0.0f, 0.0f}, cenp = {0.0f, 0.0f, 0.0f};
+    float cavxp = 0.0f, cavyp = 0.0f, cenwp = BIG_F;
+    bool has_cav = false;
+    const float4 pp = D.patches[(bi * NTR_MAX_PATCHES + k) * 2], pn = D.patches[(bi * NTR_MAX_PATCHES + k) * 2 + 1];
+    V3 r = qrot(b.q, xyz(pp));
+    V3 p = xyz(b.x) + r;
+    V3 n = qrot(b.q, xyz(pn));
+    float area = pp.w;
+    V3 X = (p - g.org) / hh;
+    float2 s0 = warp_sample_grid(D, g, X - lattice_offset(0), F_U + 0, a_wt(0), lane);
+    float2 s1 = warp_sample_grid(D, g, X - lattice_offset(1), F_U + 1, a_wt(1), lane);
+    float2 s2 = warp_sample_grid(D, g, X - lattice_offset(2), F_U + 2, a_wt(2), lane);
+    V3 uw = {s0.y > 1e-6f ? s0.x / s0.y : 0.0f, s1.y > 1e-6f ? s1.x / s1.y : 0.0f, s2.y > 1e-6f ? s2.x / s2.y : 0.0f};
+    V3 sw = {s0.y, s1.y, s2.y};
+    float fill = clampf_(warp_sample_grid(D, g, X - 0.5f, F_TYPE, A_WC, lane).y / 8.0f, 0.0f, 1.0f);
+    if (warp_in_cavity(D, hh, bi, p, t_end - step, lane) || dot(r, xyz(side)) > side.w) fill = 0.0f;
+    float2 gs = warp_sample_pressure(D, g, X - 0.5f, true, lane);
+    float p_gas = gs.y > 1e-6f ? gs.x / gs.y : 0.0f;
+    V3 vp = xyz(b.v) + cross(w, r);
+    V3 rel = vp - uw;
+    float spd = length(rel);
+    float wn = dot(rel, n);
+    float q = 0.5f * rho * spd * spd;
+    float p_water = mx(P_VAPOUR - P_ATM, pf + q * cp_patch(wn / mx(spd, 1e-9f)));
+    V3 fw = -fill * p_water * area * n;
+    V3 rt = rel - wn * n;
+    float rtl = length(rt);
+    if (rtl > 1e-9f) fw = fw - fill * CF_SKIN * 0.5f * rho * rtl * rt * area;
+    fp = fw - (1.0f - fill) * mx(p_gas, P_VAPOUR - P_ATM) * area * n;
+    tqp = cross(r, fp);
+    warp_push_water(D, g, X, 0, -fw.x * step, sw.x, lane);
+    warp_push_water(D, g, X, 1, -fw.y * step, sw.y, lane);
+    warp_push_water(D, g, X, 2, -fw.z * step, sw.z, lane);
+    if (wn > 0.0f && fill > 0.0f) {
+        float face = fill * area * mx(dot(n, vhat), 0.0f);
+        has_cav = true;
+        cavxp = -dot(fw, vhat);
+        cavyp = face;
+        cenp = p * face;
+        cenwp = dot(r, vhat);
+    }
+    if (lane == 0) {
+        float4* o = D.bullet_patch + (bi * NTR_MAX_PATCHES + k) * 4;
+        o[0] = f4(fp, cavxp);
+        o[1] = f4(tqp, cavyp);
+        o[2] = f4(cenp, cenwp);
+        o[3] = make_float4(has_cav ? 1.0f : 0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_bullet_finish(Dev D) {
+    DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    const uint32_t bi = blockIdx.x;
+    if (__float_as_uint(D.bullet_prep[bi * 4].x) != 1u) return;
     const Grid g = grid_of(D, cur_of(st));
     const ntr_gpu_params* U = D.U;
     const uint32_t li = threadIdx.x;
     const DBullet b = D.bullets[bi];
     const float step = dt_of(st), t_end = now_of(st), hh = g.h;
-    __shared__ uint32_t s_state;
-    __shared__ float s_pf;
-    __shared__ float4 s_side;
-    __shared__ float4 red_f[256], red_t[256], red_c[256];
-    __shared__ int32_t s_hit[NTR_HIT_FIELDS];
-    int32_t* hit = D.bullet_hit + bi * NTR_HIT_FIELDS;
-    uint32_t state = b.info.z;
-    if (state == 0u && st->s.t_ns - st->s.dt_ns >= b.info.x) state = 1u;
-    // The membrane's contact sums since the last step, taken and cleared one word per thread:
-    // the wetted-side sums always, the impulses only when the bullet flies this step.
-    if (li < NTR_HIT_FIELDS) s_hit[li] = (li >= 6u || state == 1u) ? atomicExch(hit + li, 0) : 0;
-    __syncthreads();
-    if (li == 0) {
-        s_state = state;
-        V3 ahead = xyz(b.x) + normalize(xyz(b.v) + 1e-9f) * (b.shape.z + 3.0f * hh);
-        const V3 xa = (ahead - g.org) / hh - 0.5f;
-        float2 s = sample_pressure(D, g, xa, false);
-        s_pf = s.y > 1e-6f ? s.x / s.y : 0.0f;
-        V3 sn, sx;
-        for (int c = 0; c < 3; c++) {
-            sn[c] = from_fp(s_hit[6 + c], FP_A);
-            sx[c] = from_fp(s_hit[9 + c], FP_X);
-        }
-        float sa = from_fp(s_hit[12], FP_A);
-        s_side = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (sa > 0.0f && length(sn) > 0.0f) {
-            V3 n = normalize(sn);
-            s_side = make_float4(n.x, n.y, n.z, dot(sx, n) / sa * 1e-3f);
-        }
-    }
-    __syncthreads();
-    if (state != 1u) {
-        if (li == 0) {
-            D.bullets[bi].info.z = state;
-            D.pose_log[(bi * NTR_LOG_CAP + st->s.step % NTR_LOG_CAP) * 3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        }
-        return;
-    }
-    const float pf = s_pf;
-    const float4 side = s_side;
-    V3 lb = qrot(make_float4(-b.q.x, -b.q.y, -b.q.z, b.q.w), xyz(b.l));
-    V3 w = qrot(b.q, lb / v3(b.shape.y, b.shape.y, b.shape.x));
     const float rho = U->fluid[0];
     const V3 vhat = normalize(xyz(b.v) + 1e-9f);
-    // This thread's patch: its force, torque, push on the water, and share of the wetted face.
+    __shared__ float4 red_f[256], red_t[256], red_c[256];
     const uint32_t n_patch = b.info.y;
-    V3 fp = {0.0f, 0.0f, 0.0f}, tqp = {0.0f, 0.0f, 0.0f}, cenp = {0.0f, 0.0f, 0.0f};
-    float cavxp = 0.0f, cavyp = 0.0f, cenwp = BIG_F;
-    bool has_cav = false;
-    if (li < n_patch) {
-        const uint32_t k = li;
-        const float4 pp = D.patches[(bi * NTR_MAX_PATCHES + k) * 2], pn = D.patches[(bi * NTR_MAX_PATCHES + k) * 2 + 1];
-        V3 r = qrot(b.q, xyz(pp));
-        V3 p = xyz(b.x) + r;
-        V3 n = qrot(b.q, xyz(pn));
-        float area = pp.w;
-        V3 X = (p - g.org) / hh;
-        float2 s0 = sample_grid(D, g, X - lattice_offset(0), F_U + 0, a_wt(0));
-        float2 s1 = sample_grid(D, g, X - lattice_offset(1), F_U + 1, a_wt(1));
-        float2 s2 = sample_grid(D, g, X - lattice_offset(2), F_U + 2, a_wt(2));
-        V3 uw = {s0.y > 1e-6f ? s0.x / s0.y : 0.0f, s1.y > 1e-6f ? s1.x / s1.y : 0.0f, s2.y > 1e-6f ? s2.x / s2.y : 0.0f};
-        V3 sw = {s0.y, s1.y, s2.y};
-        float fill = clampf_(sample_grid(D, g, X - 0.5f, F_TYPE, A_WC).y / 8.0f, 0.0f, 1.0f);
-        if (in_cavity(D, hh, bi, p, t_end - step) || dot(r, xyz(side)) > side.w) fill = 0.0f;
-        float2 gs = sample_pressure(D, g, X - 0.5f, true);
-        float p_gas = gs.y > 1e-6f ? gs.x / gs.y : 0.0f;
-        V3 vp = xyz(b.v) + cross(w, r);
-        V3 rel = vp - uw;
-        float spd = length(rel);
-        float wn = dot(rel, n);
-        float q = 0.5f * rho * spd * spd;
-        float p_water = mx(P_VAPOUR - P_ATM, pf + q * cp_patch(wn / mx(spd, 1e-9f)));
-        V3 fw = -fill * p_water * area * n;
-        V3 rt = rel - wn * n;
-        float rtl = length(rt);
-        if (rtl > 1e-9f) fw = fw - fill * CF_SKIN * 0.5f * rho * rtl * rt * area;
-        fp = fw - (1.0f - fill) * mx(p_gas, P_VAPOUR - P_ATM) * area * n;
-        tqp = cross(r, fp);
-        push_water(D, g, X, 0, -fw.x * step, sw.x);
-        push_water(D, g, X, 1, -fw.y * step, sw.y);
-        push_water(D, g, X, 2, -fw.z * step, sw.z);
-        if (wn > 0.0f && fill > 0.0f) {
-            float face = fill * area * mx(dot(n, vhat), 0.0f);
-            has_cav = true;
-            cavxp = -dot(fw, vhat);
-            cavyp = face;
-            cenp = p * face;
-            cenwp = dot(r, vhat);
-        }
-    }
     // Lane l's running sums over patches l, l + 256, l + 512, in that order.
-    __shared__ uint8_t st_has[256];
     V3 f = {0.0f, 0.0f, 0.0f}, tq = {0.0f, 0.0f, 0.0f};
     float cavx = 0.0f, cavy = 0.0f;
     float4 cen = make_float4(0.0f, 0.0f, 0.0f, BIG_F);
     for (uint32_t round = 0; round < 3; round++) {
-        if (li >= round * 256u && li < round * 256u + 256u) {
-            const uint32_t l = li - round * 256u;
-            red_f[l] = f4(fp, cavxp);
-            red_t[l] = f4(tqp, cavyp);
-            red_c[l] = f4(cenp, cenwp);
-            st_has[l] = has_cav ? 1 : 0;
-        }
-        __syncthreads();
-        if (li < 256u && li + round * 256u < n_patch) {
-            const float4 a = red_f[li], t4 = red_t[li], c4 = red_c[li];
+        const uint32_t k = li + round * 256u;
+        if (k < n_patch) {
+            const float4* rec = D.bullet_patch + (bi * NTR_MAX_PATCHES + k) * 4;
+            const float4 a = rec[0], t4 = rec[1], c4 = rec[2];
             f = f + xyz(a);
             tq = tq + xyz(t4);
-            if (st_has[li]) {
+            if (rec[3].x != 0.0f) {
                 cavx = cavx + a.w;
                 cavy = cavy + t4.w;
                 V3 cx = v3(cen.x, cen.y, cen.z) + xyz(c4);
                 cen = make_float4(cx.x, cx.y, cx.z, mn(cen.w, c4.w));
             }
         }
-        __syncthreads();
     }
-    if (li < 256u) {
-        red_f[li] = make_float4(f.x, f.y, f.z, cavx);
-        red_t[li] = make_float4(tq.x, tq.y, tq.z, cavy);
-        red_c[li] = cen;
-    }
+    red_f[li] = make_float4(f.x, f.y, f.z, cavx);
+    red_t[li] = make_float4(tq.x, tq.y, tq.z, cavy);
+    red_c[li] = cen;
     __syncthreads();
     for (uint32_t off = 128; off > 0; off >>= 1) {
         if (li < off) {
@@ -630,6 +657,12 @@ __global__ void __launch_bounds__(BULLET_T) k_bullet_step(Dev D) {
             red_c[li] = make_float4(a.x + o.x, a.y + o.y, a.z + o.z, mn(a.w, o.w));
         }
         __syncthreads();
+    }
+    int32_t s_hit[6];
+    {
+        const float4 h0 = D.bullet_prep[bi * 4 + 2], h1 = D.bullet_prep[bi * 4 + 3];
+        s_hit[0] = __float_as_int(h0.x), s_hit[1] = __float_as_int(h0.y), s_hit[2] = __float_as_int(h0.z);
+        s_hit[3] = __float_as_int(h0.w), s_hit[4] = __float_as_int(h1.x), s_hit[5] = __float_as_int(h1.y);
     }
     const float hand2 = R_HAND * R_HAND * hh * hh;
     // The new velocity and position (every thread; the 27 blocks around it are looked up in

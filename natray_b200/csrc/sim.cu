@@ -193,6 +193,8 @@ static ntr_status allocate(Sim& S) {
     D.outlines = ol;
     AL(D.sections, NTR_MAX_SHOTS * NTR_N_SEC);
     AL(D.bullet_hit, NTR_MAX_SHOTS * NTR_HIT_FIELDS);
+    AL(D.bullet_prep, NTR_MAX_SHOTS * 4);
+    AL(D.bullet_patch, NTR_MAX_SHOTS * NTR_MAX_PATCHES * 4);
     AL(D.pose_log, NTR_MAX_SHOTS * NTR_LOG_CAP * 3);
     AL(D.spray, (size_t)D.spray_cap * 3);
     AL(D.landed, D.spray_cap);
@@ -417,7 +419,12 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     join(0);
     L(k_grid_prep, G_cell, 256, D);
     L(k_air_fill, G_cell, 256, D);
-    L(k_bullet_step, n_shots, BULLET_T, D);
+    L(k_bullet_prep, n_shots, 32, D);
+    {
+        const dim3 gp((NTR_MAX_PATCHES + BULLET_PW - 1) / BULLET_PW, n_shots);
+        L(k_bullet_patch, gp, BULLET_PW * 32, D);
+    }
+    L(k_bullet_finish, n_shots, 256, D);
     L(k_bullet_apply, G_cell, 256, D);
     // The whole pressure solve: one cooperative launch, its grid barrier's counter reset first.
     cudaMemsetAsync(&D.st->bar_count, 0, 4, s);
