@@ -180,24 +180,14 @@ __device__ __forceinline__ V3 vf(I3 a) { return {(float)a.x, (float)a.y, (float)
 __device__ __forceinline__ uint32_t f2u(float x) { return __float2uint_rz(x); }
 
 // to_fp rounds half to even (sim_defs.wgsl:217-219): rint(clamp(x * scale, -2e9, 2e9)).
-// The transfer kernels convert hundreds of values per particle, more than the conversion unit
-// keeps up with, so the common range goes through the adder instead: for |y| < 2^22,
-// y + 1.5 * 2^23 lies in [2^23, 2^24], where floats are the integers, so the addition rounds y
-// to the nearest integer, ties to even (1.5 * 2^23 is even), and the integer is the difference
-// of the bit patterns. Everything else (large magnitudes, infinities, NaN) is converted. The
-// result is the same as the conversion's for every input.
-__device__ __forceinline__ int32_t to_fp(float x, float scale) {
-    const float y = __fmul_rn(x, scale);  // never contracted into the addition below
-    if (fabsf(y) < 4194304.0f) return __float_as_int(__fadd_rn(y, 12582912.0f)) - 0x4B400000;
-    return __float2int_rn(clampf_(y, -2e9f, 2e9f));
-}
-// The same for values that are mostly in [0, 2^23) (B-spline weights times 2^24, at most
-// 0.75^3 * 2^24): y + 2^23 lies in [2^23, 2^24].
-__device__ __forceinline__ int32_t to_fp_pos(float x, float scale) {
-    const float y = __fmul_rn(x, scale);
-    if (y >= 0.0f && y < 8388608.0f) return __float_as_int(__fadd_rn(y, 8388608.0f)) - 0x4B000000;
-    return __float2int_rn(clampf_(y, -2e9f, 2e9f));
-}
+__device__ __forceinline__ int32_t to_fp(float x, float scale) { return __float2int_rn(clampf_(x * scale, -2e9f, 2e9f)); }
+// The same rounding by addition, for the transfer kernels, which convert hundreds of values per
+// particle (more than the conversion unit keeps up with): for |y| < 2^22, y + 1.5 * 2^23 lies
+// in [2^23, 2^24], where floats are the integers, so the addition rounds y to the nearest
+// integer, ties to even (1.5 * 2^23 is even), and the integer is the difference of the bit
+// patterns. fp_round_pos does the same for 0 <= y < 2^23 with 2^23. The caller shows the range.
+__device__ __forceinline__ int32_t fp_round(float y) { return __float_as_int(__fadd_rn(y, 12582912.0f)) - 0x4B400000; }
+__device__ __forceinline__ int32_t fp_round_pos(float y) { return __float_as_int(__fadd_rn(y, 8388608.0f)) - 0x4B000000; }
 __device__ __forceinline__ float from_fp(int32_t x, float scale) { return (float)x / scale; }
 
 __device__ __forceinline__ V3 axis_weights(float fx) {

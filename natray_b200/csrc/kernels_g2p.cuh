@@ -214,24 +214,27 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Dev D) {
                     fastest = mx(fastest, length(vv));
                 }
             }
-            // Rank this round's break-ups in sorted order and put them after the earlier ones.
-            uint32_t bal = __ballot_sync(0xffffffffu, brk);
-            if (lane == 0) s_wcount[warp] = __popc(bal);
-            __syncthreads();
-            uint32_t before = s_brk;
-            for (uint32_t w = 0; w < warp; w++) before += s_wcount[w];
-            if (brk) {
-                uint32_t r = before + __popc(bal & ((1u << lane) - 1u));
-                D.brk_x[first + r] = f4(bx, __uint_as_float(bid));
-                D.brk_v[first + r] = f4(bv, 0.0f);
+            // Rank this round's break-ups in sorted order and put them after the earlier ones
+            // (most rounds have none).
+            if (__syncthreads_or(brk)) {
+                uint32_t bal = __ballot_sync(0xffffffffu, brk);
+                if (lane == 0) s_wcount[warp] = __popc(bal);
+                __syncthreads();
+                uint32_t before = s_brk;
+                for (uint32_t w = 0; w < warp; w++) before += s_wcount[w];
+                if (brk) {
+                    uint32_t r = before + __popc(bal & ((1u << lane) - 1u));
+                    D.brk_x[first + r] = f4(bx, __uint_as_float(bid));
+                    D.brk_v[first + r] = f4(bv, 0.0f);
+                }
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    uint32_t t = 0;
+                    for (uint32_t w = 0; w < G2P_T / 32; w++) t += s_wcount[w];
+                    s_brk += t;
+                }
+                __syncthreads();
             }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                uint32_t t = 0;
-                for (uint32_t w = 0; w < G2P_T / 32; w++) t += s_wcount[w];
-                s_brk += t;
-            }
-            __syncthreads();
         }
         if (threadIdx.x == 0) D.brk_count[b] = s_brk;
         __syncthreads();

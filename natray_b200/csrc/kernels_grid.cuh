@@ -374,18 +374,36 @@ __device__ __forceinline__ void splat(int32_t* tile, V3 x, V3 o, I3 corner, uint
     I3 t = base - corner;
     uint32_t t0 = (uint32_t)t.x * 49u + (uint32_t)t.y * 7u + (uint32_t)t.z;
     V3 hg = grad * hh;
+    // The weights are products of three B-spline factors in [0, 0.75], and a node's value is at
+    // most |val| + 1.5 |hg|_1 in size (every node - fx is within 1.5 per axis). When that bound
+    // times the scale is well below 2^22 (and nothing is infinite or NaN), every to_fp of the
+    // stencil is the rounding by addition (weight * 2^24 < 2^23 as well); otherwise convert.
+    const float bound = fabsf(val) + 1.5f * (fabsf(hg.x) + fabsf(hg.y) + fabsf(hg.z));
+    if (bound * scale < 4.0e6f && fabsf(fx.x) + fabsf(fx.y) + fabsf(fx.z) < 8.0f) {
 #pragma unroll
-    for (uint32_t a = 0; a < 3; a++)
+        for (uint32_t a = 0; a < 3; a++)
 #pragma unroll
-        for (uint32_t b = 0; b < 3; b++)
+            for (uint32_t b = 0; b < 3; b++)
 #pragma unroll
-            for (uint32_t c = 0; c < 3; c++) {
-                float weight = wx[a] * wy[b] * wz[c];
-                uint32_t tt = t0 + a * 49u + b * 7u + c;
-                float node = val + dot(hg, v3((float)a, (float)b, (float)c) - fx);
-                atomicAdd(&tile[fa * TILE + tt], to_fp(weight * node, scale));
-                atomicAdd(&tile[fw * TILE + tt], to_fp_pos(weight, FP_W));
-            }
+                for (uint32_t c = 0; c < 3; c++) {
+                    float weight = wx[a] * wy[b] * wz[c];
+                    uint32_t tt = t0 + a * 49u + b * 7u + c;
+                    float node = val + dot(hg, v3((float)a, (float)b, (float)c) - fx);
+                    atomicAdd(&tile[fa * TILE + tt], fp_round(__fmul_rn(weight * node, scale)));
+                    atomicAdd(&tile[fw * TILE + tt], fp_round_pos(__fmul_rn(weight, FP_W)));
+                }
+    } else {
+#pragma unroll 1
+        for (uint32_t a = 0; a < 3; a++)
+            for (uint32_t b = 0; b < 3; b++)
+                for (uint32_t c = 0; c < 3; c++) {
+                    float weight = wx[a] * wy[b] * wz[c];
+                    uint32_t tt = t0 + a * 49u + b * 7u + c;
+                    float node = val + dot(hg, v3((float)a, (float)b, (float)c) - fx);
+                    atomicAdd(&tile[fa * TILE + tt], to_fp(weight * node, scale));
+                    atomicAdd(&tile[fw * TILE + tt], to_fp(weight, FP_W));
+                }
+    }
 }
 
 __device__ __forceinline__ uint32_t tile_cell(const uint32_t* links, uint32_t t) {
@@ -427,12 +445,13 @@ __global__ void __launch_bounds__(P2G_T) k_p2g(Dev D) {
         for (uint32_t t = threadIdx.x; t < 8 * TILE; t += P2G_T) tile[t] = 0;
         __syncthreads();
         const I3 corner = bc * 4 - I3{1, 1, 1};
-        // Within a round of 256, lane l of warp w takes particle 8 l + w: a block's particles
-        // are in lattice order, so consecutive ones share a cell and would add to the same
-        // tile entries; 8 apart they mostly do not. (Sums are integer: any order is the same.)
-        const uint32_t perm = (threadIdx.x & 31u) * 8u + (threadIdx.x >> 5);
-        for (uint32_t base = 0; base < count; base += P2G_T) {
-            const uint32_t k = base + perm;
+        // Thread (warp w, lane l) takes the particles R (8 l + w) .. R (8 l + w) + R - 1 (R =
+        // count / 256, rounded up): the 32 lanes of a warp are spread over the whole block, where
+        // they mostly add to different nodes and banks (a block's particles are in lattice
+        // order, so neighbours in the list share a cell). Integer sums: any order is the same.
+        const uint32_t R = (count + P2G_T - 1) / P2G_T;
+        const uint32_t k0 = ((threadIdx.x & 31u) * 8u + (threadIdx.x >> 5)) * R;
+        for (uint32_t k = k0; k < k0 + R; k++) {
             if (k >= count) continue;
             uint32_t i = D.sorted[first + k];
             float4 pos = D.pos[i], vel = D.vel[i], c0 = D.c0[i], c1 = D.c1[i], c2 = D.c2[i];
