@@ -271,6 +271,39 @@ def cpu_baseline(sample_steps: int, threads: int | None = None) -> dict:
             "sample": f"{n} steps of the 1M-particle scene after one untimed step, oracle FP32 with the reference's FP32 sums, OpenMP"}
 
 
+def batch_and_serve(args) -> dict:
+    """The batched workload (many mixed scenes stepped together, against the same scenes one at a
+    time) and the serving loop (Poisson arrivals, continuous batching, against one request at a
+    time in arrival order), on seeded synthetic scenes of the shapes the configs name, scaled
+    down in count and steps so that the run stays within minutes."""
+    from natray_b200 import serve as sv
+    out = {}
+    if args.batch_scenes:
+        ws = sv.build_worlds(sv.mixed_scenes(args.batch_scenes, 7))
+        b = sv.run_batched(ws, args.batch_steps, args.batch_chunk, max_scenes=max(64, args.batch_scenes))
+        q = sv.run_sequential(ws, args.batch_steps, args.batch_chunk)
+        out["batched"] = {
+            "workload": f"{len(ws)} scenes, particles log-uniform 16k-512k (seeded; {sum(w.h.n_particles for w in ws)} in all), "
+                        f"diameter 6.5-16 cm, 8 mm steel sphere at 150-400 m/s, membrane level 4-6 by size, "
+                        f"{args.batch_steps} steps each, dt 2 us, FP64 solver sums",
+            "scenes_per_s": b["scenes_per_s"], "particle_steps_per_s": b["particle_steps_per_s"], "seconds": b["seconds"],
+            "sequential_scenes_per_s": q["scenes_per_s"], "sequential_seconds": q["seconds"],
+            "speedup_vs_sequential": q["seconds"] / b["seconds"], "chunk": args.batch_chunk}
+    if args.serve_requests:
+        ps = sv.mixed_scenes(args.serve_requests, 11, lo=16_000, hi=2_000_000, lognormal_median=128_000)
+        ws = sv.build_worlds(ps)
+        arr = sv.poisson_arrivals(args.serve_requests, args.serve_rate, 11)
+        srv = sv.serve(ws, arr, args.serve_steps, args.batch_chunk, max_scenes=64)
+        q = sv.run_sequential(ws, args.serve_steps, args.batch_chunk)
+        seq = sv.sequential_timeline(arr, q["per_scene_seconds_with_setup"])
+        out["serving"] = {
+            "workload": f"{args.serve_requests} requests, Poisson arrivals at {args.serve_rate}/s (seeded), particles lognormal "
+                        f"median 128k clipped 16k-2M, {args.serve_steps} steps each, admission by free HBM, 64 slots",
+            "scenes_per_s": srv["scenes_per_s"], "p50_s": srv["p50_s"], "p99_s": srv["p99_s"], "seconds": srv["seconds"],
+            "sequential": {"scenes_per_s": seq["scenes_per_s"], "p50_s": seq["p50_s"], "p99_s": seq["p99_s"], "seconds": seq["seconds"]}}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -278,6 +311,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=30, help="steps of the CPU baseline sample")
+    ap.add_argument("--batch-scenes", type=int, default=64, help="scenes of the batched run (0: skip)")
+    ap.add_argument("--batch-steps", type=int, default=100)
+    ap.add_argument("--batch-chunk", type=int, default=8, help="steps per batch call (state read back between)")
+    ap.add_argument("--serve-requests", type=int, default=64, help="requests of the serving loop (0: skip)")
+    ap.add_argument("--serve-steps", type=int, default=100)
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="request arrivals per second")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_env()
@@ -299,6 +338,7 @@ def main():
     res = run_native(args, rank, world, local)
     if rank == 0 and res is not None:
         if world == 1:
+            res.update(batch_and_serve(args))
             res["cpu_baseline"] = cpu_baseline(args.cpu_sample)
         print(json.dumps(res), flush=True)
 

@@ -348,6 +348,68 @@ NTR_API ntr_status ntr_sim_last_launches(ntr_sim* s, uint64_t* launches, double*
  * particle mass, out[5..7] = sum of positions. */
 NTR_API ntr_status ntr_sim_conservation(ntr_sim* s, double out[8]);
 
+/* --- Launch shapes and their autotuner ----------------------------------------------------
+ * No counterpart in the reference (wgpu picks nothing of the kind). How many CTAs the step's
+ * kernels use; the results do not depend on it, bit for bit. Zero fields take the defaults.
+ * ntr_sim_autotune times `steps` steps of the simulation's own scene per candidate (restoring
+ * its state before each and at the end, so the simulation is where it was), keeps the fastest
+ * in the simulation and returns it. */
+typedef struct {
+    uint32_t solve_ctas;        /* CTAs of the cooperative pressure solve, 1..256 (default: all that fit, at most 256) */
+    uint32_t cell_ctas_per_sm;  /* CTAs of 256 threads per SM of the per-cell kernels (default 8) */
+    uint32_t block_ctas_per_sm; /* CTAs per SM of the per-block transfer kernels P2G and G2P (default 8) */
+    uint32_t pad;
+} ntr_tuning;
+NTR_API ntr_status ntr_sim_get_tuning(ntr_sim* s, ntr_tuning* out);
+NTR_API ntr_status ntr_sim_set_tuning(ntr_sim* s, const ntr_tuning* t);
+NTR_API ntr_status ntr_sim_autotune(ntr_sim* s, uint32_t steps, ntr_tuning* best, double* best_ms_per_step);
+
+/* --- Batches of independent scenes --------------------------------------------------------
+ * No counterpart in the reference (it runs one Sim at a time, src/sim.rs:149-205): a serving
+ * engine for many scenes of uneven size on one GPU. Each admitted scene keeps its state on the
+ * device in its own slot. ntr_batch_step advances every unfinished scene by n steps: per step
+ * each scene's work before and after the pressure solve runs on its own stream, overlapping
+ * the others', and the pressure systems of all of them are solved by ONE cooperative launch
+ * that splits the GPU over them. A scene's results are bit for bit those of the same scene run
+ * alone with ntr_sim_step(n) calls of the same n.
+ *
+ *   ntr_batch_create  max_scenes (at most NTR_BATCH_MAX) slots; hbm_budget bytes the batch may
+ *                     hold on the device (0: no limit but the free memory)
+ *   ntr_batch_admit   a world blob (ntr_world_build, ntr_sim_snapshot) into a free slot, to run
+ *                     n_steps steps; NTR_E_BUSY when no slot is free or the scene's device memory
+ *                     does not fit the budget or the free HBM (less a reserve): admit it later
+ *   ntr_batch_step    n steps of every unfinished scene (fewer for a scene that reaches its
+ *                     target); *active (may be NULL) = scenes that stepped
+ *   ntr_batch_poll    a slot's state and progress
+ *   ntr_batch_snapshot  a slot's world blob, as ntr_sim_snapshot
+ *   ntr_batch_retire  frees a slot; it keeps its device region for the next scene it takes, so
+ *                     admitting and retiring make no device-wide synchronising allocation calls
+ *                     unless a scene needs a bigger region */
+#define NTR_BATCH_MAX 128u
+typedef struct ntr_batch ntr_batch;
+typedef struct {
+    uint32_t in_use;      /* the slot holds a scene */
+    uint32_t finished;    /* it has taken its steps */
+    uint32_t steps_done, steps_target;
+    uint64_t device_bytes;
+    ntr_state state;
+} ntr_batch_slot;
+typedef struct {
+    uint32_t max_scenes, in_use, active, pad;
+    uint64_t held_bytes;   /* device memory the slots hold (a slot keeps its region for its next scene) */
+    uint64_t budget_bytes;
+    uint64_t free_bytes;   /* free device memory now */
+    uint64_t steps;        /* batch steps taken */
+} ntr_batch_info;
+NTR_API ntr_status ntr_batch_create(int device, uint32_t max_scenes, uint64_t hbm_budget, ntr_batch** out);
+NTR_API ntr_status ntr_batch_destroy(ntr_batch* b);
+NTR_API ntr_status ntr_batch_admit(ntr_batch* b, const void* world_blob, size_t len, uint32_t n_steps, uint32_t* slot);
+NTR_API ntr_status ntr_batch_step(ntr_batch* b, uint32_t n, uint32_t* active);
+NTR_API ntr_status ntr_batch_poll(ntr_batch* b, uint32_t slot, ntr_batch_slot* out);
+NTR_API ntr_status ntr_batch_snapshot(ntr_batch* b, uint32_t slot, void* buf, size_t cap, size_t* len);
+NTR_API ntr_status ntr_batch_retire(ntr_batch* b, uint32_t slot);
+NTR_API ntr_status ntr_batch_info_get(ntr_batch* b, ntr_batch_info* out);
+
 /* --- Sorting particles by block without allocating ------------------------------------------
  * No counterpart in the reference: an addition for callers that cannot allocate device
  * memory, such as a host application whose framework has reserved the GPU's memory for its

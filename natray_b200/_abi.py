@@ -105,6 +105,25 @@ class Profile(C.Structure):
                 ("r_max", C.c_double), ("samples", (C.c_double * 3) * PROFILE_SAMPLES)]
 
 
+BATCH_MAX = 128
+
+
+class Tuning(C.Structure):
+    _fields_ = [("solve_ctas", C.c_uint32), ("cell_ctas_per_sm", C.c_uint32), ("block_ctas_per_sm", C.c_uint32),
+                ("pad", C.c_uint32)]
+
+
+class BatchSlot(C.Structure):
+    _fields_ = [("in_use", C.c_uint32), ("finished", C.c_uint32), ("steps_done", C.c_uint32),
+                ("steps_target", C.c_uint32), ("device_bytes", C.c_uint64), ("state", State)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("max_scenes", C.c_uint32), ("in_use", C.c_uint32), ("active", C.c_uint32), ("pad", C.c_uint32),
+                ("held_bytes", C.c_uint64), ("budget_bytes", C.c_uint64), ("free_bytes", C.c_uint64),
+                ("steps", C.c_uint64)]
+
+
 # Every entry point include/natray.h declares, with its ctypes signature.
 _P = C.c_void_p
 _SIGS = {
@@ -132,6 +151,17 @@ _SIGS = {
     "ntr_sim_last_launches": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
     "ntr_sim_conservation": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "ntr_sort_by_block_noalloc": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P, _P]),
+    "ntr_sim_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "ntr_sim_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "ntr_sim_autotune": (C.c_int, [_P, C.c_uint32, C.POINTER(Tuning), C.POINTER(C.c_double)]),
+    "ntr_batch_create": (C.c_int, [C.c_int, C.c_uint32, C.c_uint64, C.POINTER(_P)]),
+    "ntr_batch_destroy": (C.c_int, [_P]),
+    "ntr_batch_admit": (C.c_int, [_P, _P, C.c_size_t, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "ntr_batch_step": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "ntr_batch_poll": (C.c_int, [_P, C.c_uint32, C.POINTER(BatchSlot)]),
+    "ntr_batch_snapshot": (C.c_int, [_P, C.c_uint32, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "ntr_batch_retire": (C.c_int, [_P, C.c_uint32]),
+    "ntr_batch_info_get": (C.c_int, [_P, C.POINTER(BatchInfo)]),
 }
 
 _lib = None

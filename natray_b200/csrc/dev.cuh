@@ -110,7 +110,8 @@ struct Dev {
     int32_t* acc;
     float* cf;
     float* air[2];
-    double* xsum;  // the solver's running sums: 2 parities x 256 residues x 3 quantities
+    double* xsum;   // the solver's running sums: 2 parities x 256 residues x 3 quantities
+    double* spart;  // the solver's per-block partial sums when a CTA has many blocks: 3 x cap_blocks
     float4* mem_x[2];
     float4* mem_v[2];
     float4 *mem_water, *mem_layer;

@@ -11,8 +11,8 @@
 //     synchronisation, and every lane has a cell to update in every half-sweep;
 //   - the reference sums the per-block partials with 256 strided running sums (lane l adds
 //     blocks l, l + 256, ...) and then a 256-wide tree (fluid.wgsl:426-439). CTA c owns the
-//     blocks b = c (mod 256) (with fewer than 256 CTAs, several residues), so it forms lane
-//     c's running sum from its own blocks and publishes one value; after a grid barrier every
+//     blocks b = c (mod 256) (with G < 256 CTAs, the residues c, c + G, ...), so it forms lane
+//     c's running sum from its own blocks and publishes it; after a grid barrier every
 //     warp reads the 256 values and runs the same tree. All CTAs agree on alpha, beta and
 //     convergence bit for bit, and the result equals the reference's order of summation;
 //   - a warp that owns at most SOLVE_R blocks keeps their cells' solver values (type, diagonal,
@@ -21,7 +21,9 @@
 //     fields. Otherwise it loads and stores them per phase. Either way every load of a phase is
 //     issued before its first store, so the latencies overlap;
 //   - the grid barrier is a counter that only grows during the launch (reset before it): the
-//     k-th barrier waits for k * (CTAs) arrivals. One atomic per CTA and a poll of the same word.
+//     k-th barrier waits for k * (CTAs) arrivals. One atomic per CTA and a poll of the same word;
+//   - one launch can solve several simulations' systems (a batch): the CTAs split over them
+//     (solve_split), each simulation's CTAs with their own barrier and sums.
 // The barrier spins a bounded number of times; when it gives up it sets an error bit that the
 // host reports as NTR_E_TIMEOUT, and the kernel returns.
 #pragma once
@@ -33,7 +35,6 @@ namespace ntr {
 constexpr int SOLVE_W = 12;                 // warps per CTA
 constexpr int SOLVE_T = SOLVE_W * 32;       // 384 threads
 constexpr int SOLVE_R = 1;                  // blocks per warp kept in registers
-constexpr uint32_t SOLVE_MAX_M = 256;       // blocks per residue: 65536 blocks / 256
 constexpr uint32_t BARRIER_SPINS = 1u << 24;
 constexpr int SOLVE_XQ = 3;                 // quantities per exchange, at most
 
@@ -133,22 +134,35 @@ __device__ __forceinline__ A warp_tree256(const double* sums, int q, int lane) {
     return x;
 }
 
-// Publishes this CTA's running sums (fluid.wgsl:429-431) of quantities 0..NQ-1 of `part`, waits
-// at the grid barrier, and returns the 256-wide trees in `out`. The sums are double-buffered
-// by the barrier's parity: a CTA writes the next-but-one sums only after every CTA has passed
-// the next barrier, that is, has read these. False (in every thread) if the wait gave up.
+// Where a CTA keeps its blocks' partial sums: its blocks are those of residues c, c + G,
+// c + 2 G, ... (below 256), in that order and by ascending block within a residue; residue k's
+// blocks are the CTA's E[k] .. E[k + 1] - 1. Quantity q of the CTA's e-th block, block b, is at
+// part[q * stride + e] in shared memory, or part[q * stride + b] in the job's global array.
+template <class A>
+struct SolveParts {
+    A* part;
+    uint32_t stride;
+    bool by_block;
+    const uint32_t* E;
+    uint32_t n_res;
+    __device__ __forceinline__ A& at(uint32_t q, uint32_t e, uint32_t b) const { return part[q * stride + (by_block ? b : e)]; }
+};
+
+// Publishes this CTA's running sums (fluid.wgsl:429-431) of quantities 0..NQ-1 of `P`, waits at
+// the grid barrier, and returns the 256-wide trees in `out`. The sums are double-buffered by
+// the barrier's parity: a CTA writes the next-but-one sums only after every CTA has passed the
+// next barrier, that is, has read these. False (in every thread) if the wait gave up.
 template <class A, int NQ>
-__device__ __forceinline__ bool exchange(const Dev& D, DevState* st, uint32_t& gen, A (*part)[2][SOLVE_MAX_M],
-                                         uint32_t c, uint32_t G, uint32_t n_res, uint32_t nb, A (&out)[NQ]) {
+__device__ __forceinline__ bool exchange(const Dev& D, DevState* st, uint32_t& gen, const SolveParts<A>& P, uint32_t c, uint32_t G,
+                                         A (&out)[NQ]) {
     __shared__ uint32_t s_ok;
     gen++;
     double* sums = D.xsum + (size_t)(gen & 1u) * 256u * SOLVE_XQ;
     __syncthreads();  // every warp's partials and cell writes of this phase are done
-    if (threadIdx.x < n_res * NQ) {
-        const uint32_t ri = threadIdx.x / NQ, q = threadIdx.x % NQ, r = c + ri * G;
-        const uint32_t cnt = r < nb ? (nb - r + 255u) / 256u : 0u;
+    for (uint32_t t = threadIdx.x; t < P.n_res * NQ; t += blockDim.x) {
+        const uint32_t k = t / NQ, q = t % NQ, r = c + k * G;
         A s = A(0);
-        for (uint32_t m = 0; m < cnt; m++) s = s + part[q][ri][m];
+        for (uint32_t e = P.E[k], b = r; e < P.E[k + 1]; e++, b += 256u) s = s + P.at(q, e, b);
         sums[r * SOLVE_XQ + q] = (double)s;
     }
     __syncthreads();
@@ -157,12 +171,14 @@ __device__ __forceinline__ bool exchange(const Dev& D, DevState* st, uint32_t& g
         const uint32_t target = gen * G;
         atom_add_release(&st->bar_count, 1u);
         uint32_t ok = 1u;
-        for (uint32_t spins = 0; ld_acquire(&st->bar_count) < target;)
-            if (++spins > BARRIER_SPINS) {
+        for (uint32_t spins = 0; ld_acquire(&st->bar_count) < target;) {
+            // Give up after a bounded wait, or at once when another CTA of the solve has.
+            if (++spins > BARRIER_SPINS || ((spins & 1023u) == 0u && *(volatile uint32_t*)&st->err != 0u)) {
                 atomicOr(&st->err, 1u);
                 ok = 0u;
                 break;
             }
+        }
         s_ok = ok;
     }
     __syncthreads();
@@ -188,10 +204,45 @@ struct SolveCells {
     bool water[2];
 };
 
+constexpr uint32_t SOLVE_MAX_JOBS = 128;  // systems solved by one launch, at most
+constexpr uint32_t SOLVE_PART_SH = 512;   // partial sums per quantity kept in shared memory
+
+// The CTAs of a launch split over its jobs (independent systems, each a simulation's step):
+// every job that steps gets one CTA and the rest go by block count, at most 256 each. Every CTA
+// computes the same split. c0[j] .. c0[j + 1] are job j's CTAs.
+__device__ __forceinline__ void solve_split(const Dev* jobs, uint32_t n_jobs, uint32_t* w, uint32_t* c0) {
+    for (uint32_t j = threadIdx.x; j < n_jobs; j += blockDim.x) {
+        const DevState* st = jobs[j].st;
+        w[j] = st->s.dt_ns == 0u ? NONE : min(st->s.n_blocks, jobs[j].cap_blocks);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t live = 0;
+        uint64_t total = 0;
+        for (uint32_t j = 0; j < n_jobs; j++)
+            if (w[j] != NONE) live++, total += w[j];
+        const uint32_t spare = gridDim.x > live ? gridDim.x - live : 0u;
+        uint32_t at = 0;
+        for (uint32_t j = 0; j < n_jobs; j++) {
+            c0[j] = at;
+            if (w[j] == NONE || at >= gridDim.x) continue;
+            const uint32_t extra = total ? (uint32_t)((uint64_t)spare * w[j] / total) : 0u;
+            at += min(1u + extra, min(256u, gridDim.x - at));
+        }
+        c0[n_jobs] = at;
+    }
+    __syncthreads();
+}
+
+// The solve of one system by CTAs c = 0 .. G - 1 of a cooperative launch (k_solve for one
+// simulation, k_solve_batch for several). A job's result does not depend on G: the sums are the
+// reference's 256 running sums and tree either way.
 template <bool FP64>
-__global__ void __launch_bounds__(SOLVE_T, 2) k_solve(Dev D) {
+__device__ __forceinline__ void solve_body(const Dev& D, uint32_t c, uint32_t G) {
     using M = SolveMath<FP64>;
     using A = typename M::A;
+    __shared__ uint32_t s_E[257];
+    __shared__ A s_part[3 * SOLVE_PART_SH];
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     uint32_t gen = 0;
@@ -199,28 +250,42 @@ __global__ void __launch_bounds__(SOLVE_T, 2) k_solve(Dev D) {
     const ntr_gpu_params* U = D.U;
     const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t G = gridDim.x, c = blockIdx.x;
     const float tol = U->solve[0];
     const uint32_t limit = U->limits[2];
     const float hh = g.h, dt = dt_of(st);
     const float rho = U->fluid[0];
-    // Per-block partial sums of this CTA's blocks, by (residue slot, m), three quantities.
-    __shared__ A part[3][2][SOLVE_MAX_M];
     __shared__ float zl[SOLVE_W][64];
     __shared__ uint8_t wl[SOLVE_W][64];
     // Read before the first barrier: CTA 0 writes them back at the end. alpha keeps the last
     // step's value when the solver does not run, as the reference's state does.
     uint32_t iters_max = st->s.iters_max, unconverged = st->s.unconverged;
     double alpha = st->alpha;
-    // Residues of this CTA: c, c + G (G >= 128 keeps it to two).
-    const uint32_t n_res = (c + G < 256u) ? 2u : 1u;
+    // This CTA's residues c, c + G, ... and their blocks.
     auto count_of = [&](uint32_t r) -> uint32_t { return r < nb ? (nb - r + 255u) / 256u : 0u; };
-    const uint32_t cnt0 = count_of(c), n_mine = cnt0 + (n_res > 1 ? count_of(c + G) : 0u);
-    // The warp's j-th block: the CTA's (warp + j * SOLVE_W)-th, residue by residue.
-    auto block_of = [&](uint32_t e, uint32_t& b, uint32_t& ri, uint32_t& m) {
-        ri = e < cnt0 ? 0u : 1u;
-        m = e - (ri ? cnt0 : 0u);
-        b = c + ri * G + 256u * m;
+    const uint32_t n_res = c < 256u ? (256u - c + G - 1u) / G : 0u;
+    if (threadIdx.x == 0) {
+        uint32_t e = 0;
+        for (uint32_t k = 0; k < n_res; k++) s_E[k] = e, e += count_of(c + k * G);
+        s_E[n_res] = e;
+    }
+    __syncthreads();
+    const uint32_t n_mine = s_E[n_res];
+    // The partial sums: in shared memory, or in the job's own array when the CTA has too many
+    // blocks for that.
+    SolveParts<A> P;
+    P.by_block = n_mine > SOLVE_PART_SH;
+    P.part = P.by_block ? reinterpret_cast<A*>(D.spart) : s_part;
+    P.stride = P.by_block ? D.cap_blocks : SOLVE_PART_SH;
+    P.E = s_E;
+    P.n_res = n_res;
+    // The CTA's e-th block: residue k (the last with E[k] <= e), its (e - E[k])-th block.
+    auto block_of = [&](uint32_t e) -> uint32_t {
+        uint32_t lo = 0, hi = n_res;  // E[lo] <= e < E[hi]
+        while (hi - lo > 1u) {
+            const uint32_t mid = (lo + hi) / 2u;
+            if (s_E[mid] <= e) lo = mid; else hi = mid;
+        }
+        return c + lo * G + 256u * (e - s_E[lo]);
     };
     const uint32_t n_warp = n_mine > (uint32_t)warp ? (n_mine - 1u - (uint32_t)warp) / SOLVE_W + 1u : 0u;
     const bool in_regs = (n_mine + SOLVE_W - 1) / SOLVE_W <= (uint32_t)SOLVE_R;
@@ -228,7 +293,7 @@ __global__ void __launch_bounds__(SOLVE_T, 2) k_solve(Dev D) {
 
     // ---- solve_init (fluid.wgsl:445-491): diagonal, right-hand side, residual, preconditioned
     // residual, and the block's (r.z, r.r, b.b).
-    auto init_block = [&](SolveCells& C, uint32_t b, uint32_t ri, uint32_t m) {
+    auto init_block = [&](SolveCells& C, uint32_t b, uint32_t e) {
         uint32_t cell[2];
         float bq[2];
         // One cell after the other (to bound the registers), each with all its loads first.
@@ -302,12 +367,12 @@ __global__ void __launch_bounds__(SOLVE_T, 2) k_solve(Dev D) {
         A sx = warp_tree64(M::prod(C.r[0], C.z[0]), M::prod(C.r[1], C.z[1]));
         A sy = warp_tree64(M::prod(C.r[0], C.r[0]), M::prod(C.r[1], C.r[1]));
         A sz = warp_tree64(M::prod(bq[0], bq[0]), M::prod(bq[1], bq[1]));
-        if (lane == 0) part[0][ri][m] = sx, part[1][ri][m] = sy, part[2][ri][m] = sz;
+        if (lane == 0) P.at(0, e, b) = sx, P.at(1, e, b) = sy, P.at(2, e, b) = sz;
     };
 
     // ---- solve_q (fluid.wgsl:513-534): the new search direction and A d. `old` is the parity
     // of the direction field the last iteration wrote.
-    auto q_block = [&](SolveCells& C, uint32_t b, uint32_t ri, uint32_t m, uint32_t old, float fbeta) {
+    auto q_block = [&](SolveCells& C, uint32_t b, uint32_t e, uint32_t old, float fbeta) {
         uint32_t cell[2];
         for (int k = 0; k < 2; k++) cell[k] = b * 64u + solve_cell(lane, k);
         if (!in_regs) {
@@ -350,12 +415,12 @@ __global__ void __launch_bounds__(SOLVE_T, 2) k_solve(Dev D) {
             v[k] = M::prod(dn, q);
         }
         A s = warp_tree64(v[0], v[1]);
-        if (lane == 0) part[0][ri][m] = s;
+        if (lane == 0) P.at(0, e, b) = s;
     };
 
     // ---- solve_update (fluid.wgsl:543-559): p, r, and the preconditioned residual. `nw` is
     // the parity of the direction field this iteration's solve_q wrote.
-    auto update_block = [&](SolveCells& C, uint32_t b, uint32_t ri, uint32_t m, uint32_t nw, float a) {
+    auto update_block = [&](SolveCells& C, uint32_t b, uint32_t e, uint32_t nw, float a) {
         uint32_t cell[2];
         for (int k = 0; k < 2; k++) cell[k] = b * 64u + solve_cell(lane, k);
         if (!in_regs) {
@@ -387,29 +452,27 @@ __global__ void __launch_bounds__(SOLVE_T, 2) k_solve(Dev D) {
             if (C.water[k]) *cfp(D, F_Z, cell[k]) = C.z[k];
         A sx = warp_tree64(M::prod(r[0], C.z[0]), M::prod(r[1], C.z[1]));
         A sy = warp_tree64(M::prod(r[0], r[0]), M::prod(r[1], r[1]));
-        if (lane == 0) part[0][ri][m] = sx, part[1][ri][m] = sy;
+        if (lane == 0) P.at(0, e, b) = sx, P.at(1, e, b) = sy;
     };
 
-    // Runs `body(C, b, ri, m)` over the warp's blocks.
+    // Runs `body(C, b, e)` over the warp's blocks (the CTA's warp-th, (warp + SOLVE_W)-th, ...).
     auto each_block = [&](auto&& body) {
         if (in_regs) {
 #pragma unroll
             for (int j = 0; j < SOLVE_R; j++)
                 if ((uint32_t)j < n_warp) {
-                    uint32_t b, ri, m;
-                    block_of((uint32_t)warp + (uint32_t)j * SOLVE_W, b, ri, m);
-                    body(R[j], b, ri, m);
+                    const uint32_t e = (uint32_t)warp + (uint32_t)j * SOLVE_W;
+                    body(R[j], block_of(e), e);
                 }
         } else {
             for (uint32_t j = 0; j < n_warp; j++) {
-                uint32_t b, ri, m;
-                block_of((uint32_t)warp + j * SOLVE_W, b, ri, m);
-                body(R[0], b, ri, m);
+                const uint32_t e = (uint32_t)warp + j * SOLVE_W;
+                body(R[0], block_of(e), e);
             }
         }
     };
 
-    each_block([&](SolveCells& C, uint32_t b, uint32_t ri, uint32_t m) { init_block(C, b, ri, m); });
+    each_block([&](SolveCells& C, uint32_t b, uint32_t e) { init_block(C, b, e); });
 
     // solve_start (fluid.wgsl:493-506).
     double rz, beta = 0.0, b_norm, r_norm;
@@ -417,7 +480,7 @@ __global__ void __launch_bounds__(SOLVE_T, 2) k_solve(Dev D) {
     bool on;
     {
         A s3[3];
-        if (!exchange<A, 3>(D, st, gen, part, c, G, n_res, nb, s3)) return;
+        if (!exchange<A, 3>(D, st, gen, P, c, G, s3)) return;
         const A sx = s3[0], sy = s3[1], sz = s3[2];
         rz = (double)sx;
         b_norm = M::root((double)sz);
@@ -427,19 +490,19 @@ __global__ void __launch_bounds__(SOLVE_T, 2) k_solve(Dev D) {
     while (on) {
         const uint32_t old = iters % 2u;
         const float fbeta = (float)beta;
-        each_block([&](SolveCells& C, uint32_t b, uint32_t ri, uint32_t m) { q_block(C, b, ri, m, old, fbeta); });
+        each_block([&](SolveCells& C, uint32_t b, uint32_t e) { q_block(C, b, e, old, fbeta); });
         // solve_alpha (fluid.wgsl:536-541).
         {
             A s1[1];
-            if (!exchange<A, 1>(D, st, gen, part, c, G, n_res, nb, s1)) return;
+            if (!exchange<A, 1>(D, st, gen, P, c, G, s1)) return;
             alpha = (double)s1[0] > 0.0 ? M::ratio(rz, (double)s1[0]) : 0.0;
         }
         const float a = (float)alpha;
-        each_block([&](SolveCells& C, uint32_t b, uint32_t ri, uint32_t m) { update_block(C, b, ri, m, 1u - old, a); });
+        each_block([&](SolveCells& C, uint32_t b, uint32_t e) { update_block(C, b, e, 1u - old, a); });
         // solve_beta (fluid.wgsl:561-578).
         {
             A s2[2];
-            if (!exchange<A, 2>(D, st, gen, part, c, G, n_res, nb, s2)) return;
+            if (!exchange<A, 2>(D, st, gen, P, c, G, s2)) return;
             const A sx = s2[0], sy = s2[1];
             iters += 1;
             r_norm = M::root((double)sy);
@@ -455,7 +518,7 @@ __global__ void __launch_bounds__(SOLVE_T, 2) k_solve(Dev D) {
     }
     // The fields kept in registers go to memory once, as the iterations would have left them.
     if (in_regs && iters > 0)
-        each_block([&](SolveCells& C, uint32_t b, uint32_t, uint32_t) {
+        each_block([&](SolveCells& C, uint32_t b, uint32_t) {
             for (int k = 0; k < 2; k++) {
                 if (!C.water[k]) continue;
                 const uint32_t cell = b * 64u + solve_cell(lane, k);
@@ -464,13 +527,35 @@ __global__ void __launch_bounds__(SOLVE_T, 2) k_solve(Dev D) {
                 *cfp(D, F_Q, cell) = C.q[k];
             }
         });
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (c == 0 && threadIdx.x == 0) {
         st->rz = rz, st->alpha = alpha, st->beta = beta, st->b_norm = b_norm, st->r_norm = r_norm;
         st->solver_on = 0u;
         st->s.solve_iters = iters, st->s.iters_max = iters_max, st->s.unconverged = unconverged;
         st->s.rz = (float)rz, st->s.alpha = (float)alpha, st->s.beta = (float)beta;
         st->s.b_norm = (float)b_norm, st->s.r_norm = (float)r_norm;
     }
+}
+
+template <bool FP64>
+__global__ void __launch_bounds__(SOLVE_T, 2) k_solve(Dev D) {
+    solve_body<FP64>(D, blockIdx.x, gridDim.x);
+}
+
+// One launch for the systems of `n_jobs` simulations (their pointer tables at `jobs`): the CTAs
+// split over them (solve_split) and each group solves its own.
+template <bool FP64>
+__global__ void __launch_bounds__(SOLVE_T, 2) k_solve_batch(const Dev* __restrict__ jobs, uint32_t n_jobs) {
+    __shared__ uint32_t s_w[SOLVE_MAX_JOBS], s_c0[SOLVE_MAX_JOBS + 1];
+    __shared__ Dev s_dev;
+    solve_split(jobs, n_jobs, s_w, s_c0);
+    uint32_t job = NONE;
+    for (uint32_t j = 0; j < n_jobs; j++)
+        if (blockIdx.x >= s_c0[j] && blockIdx.x < s_c0[j + 1]) job = j;
+    if (job == NONE) return;
+    for (uint32_t k = threadIdx.x; k < sizeof(Dev) / 4; k += blockDim.x)
+        reinterpret_cast<uint32_t*>(&s_dev)[k] = reinterpret_cast<const uint32_t*>(jobs + job)[k];
+    __syncthreads();
+    solve_body<FP64>(s_dev, blockIdx.x - s_c0[job], s_c0[job + 1] - s_c0[job]);
 }
 
 }  // namespace ntr

@@ -37,8 +37,8 @@ namespace ntr {
     } while (0)
 
 struct GraphKey {
-    uint32_t n_mem, n_air, fp64;
-    bool operator<(const GraphKey& o) const { return std::tie(n_mem, n_air, fp64) < std::tie(o.n_mem, o.n_air, o.fp64); }
+    uint32_t n_mem, n_air, fp64, part;
+    bool operator<(const GraphKey& o) const { return std::tie(n_mem, n_air, fp64, part) < std::tie(o.n_mem, o.n_air, o.fp64, o.part); }
 };
 
 struct StepGraph {
@@ -62,11 +62,13 @@ struct Sim {
     std::vector<void*> allocs;
     size_t device_bytes = 0;
     DevState* h_state = nullptr;  // pinned
+    bool own_h_state = true;      // false: a batch slot's, kept across its scenes
     std::map<GraphKey, StepGraph> graphs;
     uint64_t last_launches = 0;
     double last_ms = 0.0;
     double step_ms = 0.0;
     uint32_t fp64 = 1;
+    ntr_tuning tune{0u, 8u, 8u, 0u};  // launch shapes (ntr_sim_set_tuning)
 
     ~Sim() {
         cudaSetDevice(device);
@@ -75,7 +77,7 @@ struct Sim {
             if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
         }
         for (void* p : allocs) cudaFree(p);
-        if (h_state) cudaFreeHost(h_state);
+        if (h_state && own_h_state) cudaFreeHost(h_state);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         for (int k = 0; k < 2; k++) {
@@ -86,10 +88,29 @@ struct Sim {
         if (stream) cudaStreamDestroy(stream);
     }
 
+    bool dry = false;  // allocate() only counts the bytes
+    // When set, allocations are carved from this device region (a batch slot's, kept across the
+    // scenes it holds) instead of made one by one: no cudaMalloc or cudaFree, which synchronise
+    // the whole device, when a scene is admitted or retired.
+    uint8_t* arena = nullptr;
+    size_t arena_cap = 0, arena_used = 0;
+
     template <class T>
     ntr_status alloc(T*& p, size_t count) {
         void* q = nullptr;
-        size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+        size_t bytes = (std::max<size_t>(count * sizeof(T), 16) + 255) & ~(size_t)255;
+        if (dry) {
+            device_bytes += bytes;
+            p = nullptr;
+            return NTR_OK;
+        }
+        if (arena) {
+            if (arena_used + bytes > arena_cap) return fail(NTR_E_NOMEM, "the slot's device region is too small for the scene");
+            p = (T*)(arena + arena_used);
+            arena_used += bytes;
+            device_bytes += bytes;
+            return NTR_OK;
+        }
         cudaError_t e = cudaMalloc(&q, bytes);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -169,6 +190,7 @@ static ntr_status allocate(Sim& S) {
     AL(D.air[0], (size_t)NTR_AIR_FIELDS * D.cap_cells);
     AL(D.air[1], (size_t)NTR_AIR_FIELDS * D.cap_cells);
     AL(D.xsum, 2u * 256u * SOLVE_XQ);
+    AL(D.spart, 3u * (size_t)D.cap_blocks);
     for (int k = 0; k < 2; k++) {
         AL(D.mem_x[k], D.Nv);
         AL(D.mem_v[k], D.Nv);
@@ -354,11 +376,39 @@ struct Prof {
     }
 };
 
-static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_air, bool fp64, Prof* prof) {
+// The pressure solve as one cooperative launch of `ctas` CTAs on `s`: of S alone (jobs == NULL),
+// or of the `n_jobs` simulations whose pointer tables are at `jobs` on the device. Each job's
+// barrier counter must be zero (the pre-solve part resets it).
+static uint64_t enqueue_solve(Sim& S, cudaStream_t s, const Dev* jobs, uint32_t n_jobs, bool fp64, Prof* prof, uint32_t ctas) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ctas);
+    cfg.blockDim = dim3(SOLVE_T);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaError_t e;
+    if (!jobs)
+        e = fp64 ? cudaLaunchKernelEx(&cfg, k_solve<true>, S.D) : cudaLaunchKernelEx(&cfg, k_solve<false>, S.D);
+    else
+        e = fp64 ? cudaLaunchKernelEx(&cfg, k_solve_batch<true>, jobs, n_jobs) : cudaLaunchKernelEx(&cfg, k_solve_batch<false>, jobs, n_jobs);
+    if (e != cudaSuccess) S.launch_err = e;
+    if (prof) prof->mark(fp64 ? "k_solve<true>" : "k_solve<false>", s);
+    return 1;
+}
+
+enum { PART_PRE = 1, PART_POST = 2, PART_FULL = 3 };
+
+// The step on stream `s`: the part before the pressure solve (PART_PRE), the part after it
+// (PART_POST), or both with the solve between (PART_FULL).
+static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_air, bool fp64, Prof* prof, int part = PART_FULL) {
     Dev& D = S.D;
     uint64_t n = 0;
-    const uint32_t G_cell = (uint32_t)S.sms * 8;
-    const uint32_t G_blk = (uint32_t)S.sms * 8;
+    const uint32_t G_cell = (uint32_t)S.sms * S.tune.cell_ctas_per_sm;
+    const uint32_t G_blk = (uint32_t)S.sms * S.tune.block_ctas_per_sm;
     const uint32_t g_part = (D.Np + 255) / 256 ? (D.Np + 255) / 256 : 1;
     const uint32_t g_vert = (D.Nv + 255) / 256 ? (D.Nv + 255) / 256 : 1;
     const uint32_t g_tri = std::max((D.Nt + 255) / 256, 1u);
@@ -369,7 +419,26 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
         n++;                                            \
         if (prof) prof->mark(#kern, s);                 \
     } while (0)
-    if (prof) prof->mark("start", s);
+    // Independent work goes to a second stream: (in the profiling mode everything stays on one).
+    cudaStream_t a = prof ? s : S.aux;
+    auto fork = [&](int k) {
+        if (a == s) return;
+        cudaEventRecord(S.ev_fork[k], s);
+        cudaStreamWaitEvent(a, S.ev_fork[k], 0);
+    };
+    auto join = [&](int k) {
+        if (a == s) return;
+        cudaEventRecord(S.ev_join[k], a);
+        cudaStreamWaitEvent(s, S.ev_join[k], 0);
+    };
+#define LA(kern, grid, block, ...)                      \
+    do {                                                \
+        kern<<<(grid), (block), 0, a>>>(__VA_ARGS__);   \
+        n++;                                            \
+        if (prof) prof->mark(#kern, a);                 \
+    } while (0)
+    if (prof && (part & PART_PRE)) prof->mark("start", s);
+    if (part & PART_PRE) {
     L(k_begin_step, 1, 32, D);
     L(k_clear, G_cell, 256, D);
     L(k_mark, (uint32_t)(((uint64_t)warp_round(D.Np) + warp_round(D.cap_blocks) + warp_round(D.Nv) + 255) / 256), 256, D);
@@ -392,25 +461,7 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
         }
     }
     L(k_block_bounds, (D.Np + 1 + 255) / 256, 256, D);
-    // Independent work on a second stream: the rubber's splat and the air's carry touch none
-    // of what P2G reads or writes. (In the profiling mode everything stays on one stream.)
-    cudaStream_t a = prof ? s : S.aux;
-    auto fork = [&](int k) {
-        if (a == s) return;
-        cudaEventRecord(S.ev_fork[k], s);
-        cudaStreamWaitEvent(a, S.ev_fork[k], 0);
-    };
-    auto join = [&](int k) {
-        if (a == s) return;
-        cudaEventRecord(S.ev_join[k], a);
-        cudaStreamWaitEvent(s, S.ev_join[k], 0);
-    };
-#define LA(kern, grid, block, ...)                      \
-    do {                                                \
-        kern<<<(grid), (block), 0, a>>>(__VA_ARGS__);   \
-        n++;                                            \
-        if (prof) prof->mark(#kern, a);                 \
-    } while (0)
+    // The rubber's splat and the air's carry touch none of what P2G reads or writes.
     fork(0);
     LA(k_mem_splat, g_vert, 256, D);
     LA(k_air_carry, G_cell, 256, D);
@@ -426,24 +477,11 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     }
     L(k_bullet_finish, n_shots, 256, D);
     L(k_bullet_apply, G_cell, 256, D);
-    // The whole pressure solve: one cooperative launch, its grid barrier's counter reset first.
+    // The pressure solve's grid barrier counter starts from zero.
     cudaMemsetAsync(&D.st->bar_count, 0, 4, s);
-    {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(S.coop_ctas);
-        cfg.blockDim = dim3(SOLVE_T);
-        cfg.dynamicSmemBytes = 0;
-        cfg.stream = s;
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeCooperative;
-        at[0].val.cooperative = 1;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
-        cudaError_t e = fp64 ? cudaLaunchKernelEx(&cfg, k_solve<true>, D) : cudaLaunchKernelEx(&cfg, k_solve<false>, D);
-        if (e != cudaSuccess) S.launch_err = e;
-        n++;
-        if (prof) prof->mark(fp64 ? "k_solve<true>" : "k_solve<false>", s);
     }
+    if (part == PART_FULL) n += enqueue_solve(S, s, nullptr, 1u, fp64, prof, S.tune.solve_ctas ? S.tune.solve_ctas : S.coop_ctas);
+    if (part & PART_POST) {
     L(k_project, G_cell, 256, D);
     L(k_extend_1, G_cell, 256, D);
     L(k_extend_2, G_cell, 256, D);
@@ -464,13 +502,15 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     L(k_spray_scan, 1, 1024, D);
     L(k_spray_emit, G_cell, 256, D);
     L(k_spray_commit, 1, 32, D);
+    }
 #undef L
 #undef LA
     return n;
 }
 
-static ntr_status get_graph(Sim& S, StepGraph*& out) {
-    GraphKey key{S.host.h.substeps, S.host.h.air_substeps, S.fp64};
+// The step (or a part of it, for a batch) captured as a graph, cached by its shape.
+static ntr_status get_graph(Sim& S, StepGraph*& out, int part = 3) {
+    GraphKey key{part == 1 ? 0u : S.host.h.substeps, part == 1 ? 0u : S.host.h.air_substeps, S.fp64, (uint32_t)part};
     auto it = S.graphs.find(key);
     if (it != S.graphs.end()) {
         out = &it->second;
@@ -486,7 +526,7 @@ static ntr_status get_graph(Sim& S, StepGraph*& out) {
     StepGraph g;
     S.launch_err = cudaSuccess;
     CU(cudaStreamBeginCapture(S.stream, cudaStreamCaptureModeThreadLocal));
-    g.launches = enqueue_step(S, S.stream, key.n_mem, key.n_air, key.fp64 != 0, nullptr);
+    g.launches = enqueue_step(S, S.stream, key.n_mem, key.n_air, key.fp64 != 0, nullptr, part);
     cudaError_t le = cudaGetLastError();
     cudaError_t ce = cudaStreamEndCapture(S.stream, &g.graph);
     if (S.launch_err != cudaSuccess) le = S.launch_err;
@@ -543,7 +583,8 @@ static ntr_status run_batch(Sim& S, uint32_t n, uint32_t stop, uint32_t* taken, 
     return NTR_OK;
 }
 
-static ntr_status create_from(const World& w, int device, Sim*& out) {
+static ntr_status create_from(const World& w, int device, Sim*& out, uint8_t* arena = nullptr, size_t arena_cap = 0,
+                              DevState* h_state = nullptr) {
     ntr_status r = check_device(device);
     if (r != NTR_OK) return r;
     CU(cudaSetDevice(device));
@@ -560,9 +601,12 @@ static ntr_status create_from(const World& w, int device, Sim*& out) {
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_solve<true>, SOLVE_T, 0));
         CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_solve<false>, SOLVE_T, 0));
         int occ = std::min(occ_a, occ_b);
-        // CTA c owns the blocks c (mod 256), so 128..256 CTAs.
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_solve_batch<true>, SOLVE_T, 0));
+        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_solve_batch<false>, SOLVE_T, 0));
+        occ = std::min(occ, std::min(occ_a, occ_b));
+        // CTA c owns the blocks c (mod 256) (and c + G, ... with fewer CTAs): at most 256.
         S->coop_ctas = (uint32_t)std::min(256, S->sms * occ);
-        if (S->coop_ctas < 128) return fail(NTR_E_NODEVICE, "the device cannot hold 128 resident solver CTAs");
+        if (S->coop_ctas < 1) return fail(NTR_E_NODEVICE, "the device cannot hold a solver CTA");
     }
     if (w.h.block_cap > 65535u) return fail(NTR_E_INVALID, "block_cap is at most 65535");
     if (prop.major < 10) return fail(NTR_E_NODEVICE, "this library is built for sm_100a (B200); device is sm_" + std::to_string(prop.major * 10 + prop.minor));
@@ -574,7 +618,11 @@ static ntr_status create_from(const World& w, int device, Sim*& out) {
     }
     CU(cudaEventCreate(&S->ev0));
     CU(cudaEventCreate(&S->ev1));
-    CU(cudaMallocHost((void**)&S->h_state, sizeof(DevState)));
+    if (h_state)
+        S->h_state = h_state, S->own_h_state = false;
+    else
+        CU(cudaMallocHost((void**)&S->h_state, sizeof(DevState)));
+    S->arena = arena, S->arena_cap = arena_cap;
     if ((r = allocate(*S)) != NTR_OK) return r;
     if ((r = upload_static(*S, w)) != NTR_OK) return r;
     if ((r = upload_state(*S, w)) != NTR_OK) return r;
@@ -881,6 +929,86 @@ NTR_API ntr_status ntr_sim_set_precision(ntr_sim* sim, int fp64_reductions) {
     return NTR_OK;
 }
 
+NTR_API ntr_status ntr_sim_get_tuning(ntr_sim* sim, ntr_tuning* out) {
+    GUARD(sim);
+    if (!out) return fail(NTR_E_INVALID, "null argument");
+    *out = S.tune;
+    if (!out->solve_ctas) out->solve_ctas = S.coop_ctas;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_sim_set_tuning(ntr_sim* sim, const ntr_tuning* t) {
+    GUARD(sim);
+    if (!t) return fail(NTR_E_INVALID, "null argument");
+    ntr_tuning n = *t;
+    if (n.solve_ctas > S.coop_ctas) return fail(NTR_E_INVALID, "solve_ctas is at most " + std::to_string(S.coop_ctas) + " (co-resident) on this device");
+    if (n.cell_ctas_per_sm > 64 || n.block_ctas_per_sm > 64) return fail(NTR_E_INVALID, "at most 64 CTAs per SM");
+    if (!n.cell_ctas_per_sm) n.cell_ctas_per_sm = 8;
+    if (!n.block_ctas_per_sm) n.block_ctas_per_sm = 8;
+    n.pad = 0;
+    CU(cudaStreamSynchronize(S.stream));
+    S.tune = n;
+    for (auto& kv : S.graphs) {
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+    }
+    S.graphs.clear();
+    return NTR_OK;
+}
+
+// A coordinate search over the launch shapes: block kernels, then cell kernels, then the solve.
+// Each candidate starts from the same state and takes one untimed step (its graph) and `steps`
+// timed ones.
+NTR_API ntr_status ntr_sim_autotune(ntr_sim* sim, uint32_t steps, ntr_tuning* best, double* best_ms) {
+    GUARD(sim);
+    if (steps == 0) return fail(NTR_E_INVALID, "steps must be positive");
+    std::vector<uint8_t> blob;
+    ntr_status r = snapshot(S, blob);
+    if (r != NTR_OK) return r;
+    ntr_tuning cur = S.tune;
+    double cur_ms = 1e300;
+    auto trial = [&](const ntr_tuning& t, double& ms) -> ntr_status {
+        ntr_status q;
+        if ((q = ntr_sim_restore(sim, blob.data(), blob.size())) != NTR_OK) return q;
+        if ((q = ntr_sim_set_tuning(sim, &t)) != NTR_OK) return q;
+        uint32_t got = 0;
+        if ((q = run_batch(S, 1, 0xFFFFFFFFu, &got)) != NTR_OK) return q;
+        if ((q = run_batch(S, steps, 0xFFFFFFFFu, &got)) != NTR_OK) return q;
+        ms = got ? S.last_ms / got : 1e300;
+        return NTR_OK;
+    };
+    if ((r = trial(cur, cur_ms)) != NTR_OK) return r;
+    const uint32_t blocks[] = {4, 6, 12, 16}, cells[] = {4, 6, 12, 16};
+    const uint32_t solves[] = {S.coop_ctas, S.coop_ctas / 2, (uint32_t)S.sms};
+    for (uint32_t v : blocks) {
+        ntr_tuning t = cur;
+        t.block_ctas_per_sm = v;
+        double ms;
+        if ((r = trial(t, ms)) != NTR_OK) return r;
+        if (ms < cur_ms) cur = t, cur_ms = ms;
+    }
+    for (uint32_t v : cells) {
+        ntr_tuning t = cur;
+        t.cell_ctas_per_sm = v;
+        double ms;
+        if ((r = trial(t, ms)) != NTR_OK) return r;
+        if (ms < cur_ms) cur = t, cur_ms = ms;
+    }
+    for (uint32_t v : solves) {
+        if (v == 0 || v > S.coop_ctas) continue;
+        ntr_tuning t = cur;
+        t.solve_ctas = v;
+        double ms;
+        if ((r = trial(t, ms)) != NTR_OK) return r;
+        if (ms < cur_ms) cur = t, cur_ms = ms;
+    }
+    if ((r = ntr_sim_restore(sim, blob.data(), blob.size())) != NTR_OK) return r;
+    if ((r = ntr_sim_set_tuning(sim, &cur)) != NTR_OK) return r;
+    if (best) *best = cur;
+    if (best_ms) *best_ms = cur_ms;
+    return NTR_OK;
+}
+
 NTR_API ntr_status ntr_sim_last_launches(ntr_sim* sim, uint64_t* launches, double* device_ms) {
     GUARD(sim);
     if (launches) *launches = S.last_launches;
@@ -997,3 +1125,98 @@ extern "C" NTR_API ntr_status ntr_sort_by_block_noalloc(const uint32_t* keys, ui
     CU(cudaGetLastError());
     return NTR_OK;
 }
+
+// ---- batches of scenes (include/natray.h, ntr_batch_*) ------------------------------------------
+#include "batch.cuh"
+
+struct ntr_batch {
+    Batch* b;
+};
+
+#define BGUARD(batch)                                                                   \
+    if (!(batch) || !(batch)->b) return fail(NTR_E_INVALID, "null batch handle");        \
+    Batch& B = *(batch)->b;                                                             \
+    if (cudaSetDevice(B.device) != cudaSuccess) return fail(NTR_E_CUDA, "cudaSetDevice failed")
+
+extern "C" {
+
+NTR_API ntr_status ntr_batch_create(int device, uint32_t max_scenes, uint64_t hbm_budget, ntr_batch** out) {
+    if (!out) return fail(NTR_E_INVALID, "null argument");
+    Batch* b = nullptr;
+    ntr_status r = batch_create(device, max_scenes, hbm_budget, b);
+    if (r != NTR_OK) return r;
+    *out = new ntr_batch{b};
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_batch_destroy(ntr_batch* batch) {
+    if (!batch) return NTR_OK;
+    delete batch->b;
+    delete batch;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_batch_admit(ntr_batch* batch, const void* blob, size_t len, uint32_t n_steps, uint32_t* slot) {
+    BGUARD(batch);
+    if (!blob || !slot) return fail(NTR_E_INVALID, "null argument");
+    return batch_admit(B, blob, len, n_steps, *slot);
+}
+
+NTR_API ntr_status ntr_batch_step(ntr_batch* batch, uint32_t n, uint32_t* active) {
+    BGUARD(batch);
+    uint32_t a = 0;
+    ntr_status r = batch_step(B, n, a);
+    if (active) *active = a;
+    return r;
+}
+
+NTR_API ntr_status ntr_batch_poll(ntr_batch* batch, uint32_t slot, ntr_batch_slot* out) {
+    BGUARD(batch);
+    if (!out) return fail(NTR_E_INVALID, "null argument");
+    if (slot >= B.max_scenes) return fail(NTR_E_INVALID, "slot out of range");
+    std::memset(out, 0, sizeof *out);
+    const BatchSlot& sl = B.slots[slot];
+    if (!sl.sim) return NTR_OK;
+    out->in_use = 1;
+    out->finished = sl.done >= sl.target ? 1u : 0u;
+    out->steps_done = sl.done, out->steps_target = sl.target;
+    out->device_bytes = sl.sim->device_bytes;
+    out->state = sl.sim->h_state->s;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_batch_snapshot(ntr_batch* batch, uint32_t slot, void* buf, size_t cap, size_t* len) {
+    BGUARD(batch);
+    if (slot >= B.max_scenes || !B.slots[slot].sim) return fail(NTR_E_INVALID, "no scene in that slot");
+    std::vector<uint8_t> blob;
+    ntr_status r = snapshot(*B.slots[slot].sim, blob);
+    if (r != NTR_OK) return r;
+    if (len) *len = blob.size();
+    if (!buf) return NTR_OK;
+    if (cap < blob.size()) return fail(NTR_E_INVALID, "snapshot buffer too small");
+    std::memcpy(buf, blob.data(), blob.size());
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_batch_retire(ntr_batch* batch, uint32_t slot) {
+    BGUARD(batch);
+    return batch_retire(B, slot);
+}
+
+NTR_API ntr_status ntr_batch_info_get(ntr_batch* batch, ntr_batch_info* out) {
+    BGUARD(batch);
+    if (!out) return fail(NTR_E_INVALID, "null argument");
+    std::memset(out, 0, sizeof *out);
+    out->max_scenes = B.max_scenes;
+    for (const auto& sl : B.slots)
+        if (sl.sim) {
+            out->in_use++;
+            if (sl.done < sl.target) out->active++;
+        }
+    out->held_bytes = B.held, out->budget_bytes = B.budget, out->steps = B.steps;
+    size_t f = 0, t = 0;
+    if (cudaMemGetInfo(&f, &t) == cudaSuccess) out->free_bytes = f;
+    return NTR_OK;
+}
+
+}  // extern "C"

@@ -128,6 +128,25 @@ class Sim:
             out[name] = (int(cnt), float(ms))
         return out
 
+    @property
+    def tuning(self) -> dict:
+        """The launch shapes (CTAs of the solve, per SM of the cell and transfer kernels)."""
+        t = _abi.Tuning()
+        check(lib().ntr_sim_get_tuning(self._h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in t._fields_ if k != "pad"}
+
+    @tuning.setter
+    def tuning(self, v: dict) -> None:
+        t = _abi.Tuning(**{k: int(x) for k, x in v.items()})
+        check(lib().ntr_sim_set_tuning(self._h, C.byref(t)))
+
+    def autotune(self, steps: int = 4) -> tuple[dict, float]:
+        """Times candidate launch shapes on this scene (its state is kept) and keeps the fastest;
+        returns it and its ms per step."""
+        t, ms = _abi.Tuning(), C.c_double()
+        check(lib().ntr_sim_autotune(self._h, steps, C.byref(t), C.byref(ms)))
+        return {k: getattr(t, k) for k, _ in t._fields_ if k != "pad"}, ms.value
+
     def last_launches(self) -> tuple[int, float]:
         n, ms = C.c_uint64(), C.c_double()
         check(lib().ntr_sim_last_launches(self._h, C.byref(n), C.byref(ms)))

@@ -48,6 +48,19 @@ def test_no_silent_cpu_fallback():
     with pytest.raises(NatrayError) as e:
         Sim(Params(resolution=16, mesh_level=1))
     assert e.value.status == 7  # NTR_E_NODEVICE
+    from natray_b200.batch import Batch
+    with pytest.raises(NatrayError) as e:
+        Batch(max_scenes=4)
+    assert e.value.status == 7
+
+
+def test_batch_structs_and_null_handles():
+    assert C.sizeof(_abi.BatchSlot) == 24 + 96
+    assert C.sizeof(_abi.BatchInfo) == 48
+    for name, args in [("ntr_batch_step", (None, 1, None)), ("ntr_batch_retire", (None, 0)),
+                       ("ntr_batch_info_get", (None, None))]:
+        assert getattr(lib(), name)(*args) == 1  # NTR_E_INVALID
+    assert lib().ntr_batch_destroy(None) == 0
 
 
 def test_oracle_float_math_error_bounds():

@@ -1,0 +1,103 @@
+"""The batch engine (ntr_batch_*): scenes of uneven size stepped together, with one joint
+pressure solve per step, give bit for bit the results of each scene stepped alone with the same
+chunks of steps, also when scenes arrive and leave while others run (continuous batching)."""
+import numpy as np
+import pytest
+
+from natray_b200 import Params, World, build_world
+from natray_b200.batch import Batch
+from natray_b200.sim import Sim
+from oracle.py import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def scene(**kw):
+    base = dict(resolution=20, mesh_level=3, block_cap=4096, spray_cap=100000)
+    base.update(kw)
+    w = build_world(Params(**base))
+    return World(Oracle(w.blob).snapshot())  # the measuring substep taken once, on the CPU
+
+
+def solo(w: World, target: int, chunk: int) -> World:
+    s = Sim(world=w)
+    done = 0
+    while done < target:
+        done += s.step(min(chunk, target - done))
+    out = s.snapshot()
+    s.close()
+    return out
+
+
+def first_difference(a: World, b: World):
+    from natray_b200._abi import SECTIONS
+    if a.state != b.state:
+        return "state " + str({k: (a.state[k], b.state[k]) for k in a.state if a.state[k] != b.state[k]})
+    for name in SECTIONS:
+        x, y = a.sec(name), b.sec(name)
+        if x.tobytes() != y.tobytes():
+            return f"section {name}"
+    if bytes(a.blob) != bytes(b.blob):
+        return "header"
+    return None
+
+
+@pytest.fixture(scope="module")
+def worlds():
+    return [scene(resolution=20), scene(resolution=28, bullet_speed=250), scene(resolution=14, diameter=10)]
+
+
+def test_batch_equals_each_scene_alone(worlds):
+    targets = [12, 8, 16]
+    with Batch(max_scenes=4) as b:
+        slots = [b.admit(w, t) for w, t in zip(worlds, targets)]
+        assert None not in slots
+        while b.step(4):
+            pass
+        for w, t, sl in zip(worlds, targets, slots):
+            p = b.poll(sl)
+            assert p["finished"] and p["steps_done"] == t
+            d = first_difference(solo(w, t, 4), b.snapshot(sl))
+            assert d is None, f"slot {sl}: {d}"
+
+
+def test_scenes_arrive_and_leave(worlds):
+    # Two scenes start; a third arrives after two batch steps; the first leaves when done and a
+    # fourth takes its slot. Each ends as it would alone.
+    w4 = scene(resolution=18, bullet_speed=300)
+    with Batch(max_scenes=2) as b:
+        s0 = b.admit(worlds[0], 8)
+        s1 = b.admit(worlds[1], 16)
+        assert b.admit(worlds[2], 8) is None  # both slots taken
+        b.step(4)
+        b.step(4)
+        assert b.poll(s0)["finished"]
+        r0 = b.snapshot(s0)
+        b.retire(s0)
+        s2 = b.admit(worlds[2], 8)
+        assert s2 == s0
+        b.step(4)
+        b.step(4)
+        r1, r2 = b.snapshot(s1), b.snapshot(s2)
+        b.retire(s1)
+        s3 = b.admit(w4, 4)
+        b.step(4)
+        r3 = b.snapshot(s3)
+        info = b.info()
+        assert info["in_use"] == 2 and info["active"] == 0
+    for w, t, r in [(worlds[0], 8, r0), (worlds[1], 16, r1), (worlds[2], 8, r2), (w4, 4, r3)]:
+        d = first_difference(solo(w, t, 4), r)
+        assert d is None, d
+
+
+def test_admission_respects_the_budget(worlds):
+    with Batch(max_scenes=4, hbm_budget=1) as b:
+        assert b.admit(worlds[0], 4) is None
+        assert b.info()["in_use"] == 0
+
+
+def test_serving_loop_finishes_every_request(worlds):
+    from natray_b200.serve import poisson_arrivals, serve
+    ws = worlds * 2
+    out = serve(ws, poisson_arrivals(len(ws), 200.0, 3), steps=8, chunk=4, max_scenes=3)
+    assert out["requests"] == len(ws) and out["p99_s"] >= out["p50_s"] > 0.0

@@ -113,6 +113,33 @@ def test_solver_from_memory_bit_exact(oracle_threads):
     assert_worlds_equal(World(o.snapshot()), s.snapshot(), "step 2")
 
 
+def test_launch_shapes_do_not_change_results(oracle_threads):
+    # One solver CTA for ~600 blocks: it owns all 256 residues, and its partial sums go to global
+    # memory (more than fit in shared). Few and many CTAs for the other kernels. All bit-exact.
+    w = measured(build_world(Params(resolution=64, mesh_level=4, block_cap=8192, spray_cap=100000)))
+    o = Oracle(w.blob)
+    assert o.step(2) == 2
+    ref = World(o.snapshot())
+    for tune in [dict(solve_ctas=1, cell_ctas_per_sm=2, block_ctas_per_sm=3),
+                 dict(solve_ctas=37, cell_ctas_per_sm=16, block_ctas_per_sm=12)]:
+        s = Sim(world=w)
+        s.tuning = tune
+        assert s.tuning["solve_ctas"] == tune["solve_ctas"]
+        assert s.step(2) == 2
+        assert s.state["n_blocks"] > 512
+        assert_grids_equal(o, s, f"tuning {tune}")
+        assert_worlds_equal(ref, s.snapshot(), f"tuning {tune}")
+
+
+def test_autotune_keeps_the_state(w_small):
+    s = Sim(world=w_small)
+    s.step(2)
+    before = s.snapshot()
+    best, ms = s.autotune(steps=2)
+    assert ms > 0 and best["block_ctas_per_sm"] > 0
+    assert_worlds_equal(before, s.snapshot(), "after autotune")
+
+
 def test_reference_fp32_sums_bit_exact(w_small):
     o = Oracle(w_small.blob, fp64_dots=False)
     s = Sim(world=w_small, fp64_reductions=False)
