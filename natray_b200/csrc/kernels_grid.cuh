@@ -415,14 +415,31 @@ __device__ __forceinline__ uint32_t tile_cell(const uint32_t* links, uint32_t t)
     return b * 64u + (uint32_t)l.x * 16u + (uint32_t)l.y * 4u + (uint32_t)l.z;
 }
 
-__global__ void __launch_bounds__(P2G_T) k_p2g(Dev D) {
+constexpr uint32_t P2G_CAP = 1024;  // particles of a block ordered at a time
+constexpr uint32_t P2G_LAYERS = 64;  // ranks within a cell that get the interleaved order
+
+// One block per iteration of a CTA. Its particles add into a 7^3 x 8-field tile of i32 sums in
+// shared memory, in an order that spreads the 32 lanes of an atomic over 32 different cells:
+// a counting sort by cell gives each particle its rank in its cell, and the particles are
+// taken rank layer by rank layer, cell by cell within a layer (layer r holds the cells with
+// more than r particles). Lanes in different cells add to different nodes of the tile, mostly
+// in different banks; neighbours in the particle list share a cell and would collide. Integer
+// sums do not depend on the order of the adds. The tile is stored whole; k_p2g_gather sums the
+// tiles that overlap each cell.
+__global__ void __launch_bounds__(P2G_T, 3) k_p2g(Dev D) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
     const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
+    const uint32_t lane = threadIdx.x & 31u;
     __shared__ __align__(16) int32_t tile[8 * TILE];
-    __shared__ uint32_t own[64];
+    __shared__ uint32_t own[64], s_cnt[64];
     __shared__ uint32_t links[27];
+    __shared__ uint32_t s_pid[P2G_CAP];
+    __shared__ uint8_t s_cell[P2G_CAP];
+    __shared__ uint16_t s_rank[P2G_CAP];
+    __shared__ uint32_t s_mlo[P2G_LAYERS], s_mhi[P2G_LAYERS];  // layer r: cells 0-31, 32-63 with > r particles
+    __shared__ uint32_t s_start[P2G_LAYERS + 1], s_over;
     const float hh = g.h;
     for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
         const I3 bc = slot_coord(g, g.list[b]);
@@ -443,29 +460,68 @@ __global__ void __launch_bounds__(P2G_T) k_p2g(Dev D) {
             continue;
         }
         for (uint32_t t = threadIdx.x; t < 8 * TILE; t += P2G_T) tile[t] = 0;
-        __syncthreads();
         const I3 corner = bc * 4 - I3{1, 1, 1};
-        // Thread (warp w, lane l) takes the particles R (8 l + w) .. R (8 l + w) + R - 1 (R =
-        // count / 256, rounded up): the 32 lanes of a warp are spread over the whole block, where
-        // they mostly add to different nodes and banks (a block's particles are in lattice
-        // order, so neighbours in the list share a cell). Integer sums: any order is the same.
-        const uint32_t R = (count + P2G_T - 1) / P2G_T;
-        const uint32_t k0 = ((threadIdx.x & 31u) * 8u + (threadIdx.x >> 5)) * R;
-        for (uint32_t k = k0; k < k0 + R; k++) {
-            if (k >= count) continue;
-            uint32_t i = D.sorted[first + k];
-            float4 pos = D.pos[i], vel = D.vel[i], c0 = D.c0[i], c1 = D.c1[i], c2 = D.c2[i];
-            V3 x = (xyz(pos) - g.org) / hh;
-            splat(tile, x, v3(0.0f, 0.5f, 0.5f), corner, 0, vel.x, xyz(c0), 1, FP_M, hh);
-            splat(tile, x, v3(0.5f, 0.0f, 0.5f), corner, 2, vel.y, xyz(c1), 3, FP_M, hh);
-            splat(tile, x, v3(0.5f, 0.5f, 0.0f), corner, 4, vel.z, xyz(c2), 5, FP_M, hh);
-            splat(tile, x, v3(0.5f, 0.5f, 0.5f), corner, A_PC, c0.w * 1e-6f, v3(0.0f, 0.0f, 0.0f), A_WC, FP_P, hh);
-            I3 l = own_cell(g, xyz(pos)) - bc * 4;
-            atomicAdd(&own[l.x * 16 + l.y * 4 + l.z], 1u);
+        for (uint32_t chunk = 0; chunk < count; chunk += P2G_CAP) {
+            const uint32_t n = min(P2G_CAP, count - chunk);
+            if (threadIdx.x < 64) s_cnt[threadIdx.x] = 0, s_mlo[threadIdx.x] = 0u, s_mhi[threadIdx.x] = 0u;
+            if (threadIdx.x == 0) s_over = 0;
+            __syncthreads();
+            // Each particle's cell and rank in its cell.
+            for (uint32_t j = threadIdx.x; j < n; j += P2G_T) {
+                const uint32_t i = D.sorted[first + chunk + j];
+                const I3 l = own_cell(g, xyz(D.pos[i])) - bc * 4;
+                const uint32_t c = (uint32_t)(l.x * 16 + l.y * 4 + l.z);
+                s_cell[j] = (uint8_t)c;
+                s_rank[j] = (uint16_t)atomicAdd(&s_cnt[c], 1u);
+            }
+            __syncthreads();
+            // The layers' cell masks (a ballot per layer by the two warps of the 64 cells), then
+            // where each layer starts (a scan by one warp).
+            if (threadIdx.x < 64) {
+                const uint32_t cnt = s_cnt[threadIdx.x];
+                own[threadIdx.x] += cnt;
+                uint32_t* m = threadIdx.x < 32 ? s_mlo : s_mhi;
+                for (uint32_t r = 0; r < P2G_LAYERS; r++) {
+                    const uint32_t bits = __ballot_sync(0xffffffffu, cnt > r);
+                    if (bits == 0u) break;
+                    if (lane == 0) m[r] = bits;
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                const uint32_t p = __popc(s_mlo[2 * lane]) + __popc(s_mhi[2 * lane]);
+                const uint32_t q = __popc(s_mlo[2 * lane + 1]) + __popc(s_mhi[2 * lane + 1]);
+                uint32_t inc = p + q;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (lane >= (uint32_t)o) inc += v;
+                }
+                s_start[2 * lane] = inc - p - q, s_start[2 * lane + 1] = inc - q;
+                if (lane == 31) s_start[P2G_LAYERS] = inc;
+            }
+            __syncthreads();
+            for (uint32_t j = threadIdx.x; j < n; j += P2G_T) {
+                const uint32_t c = s_cell[j], r = s_rank[j];
+                uint32_t pos;
+                if (r < P2G_LAYERS)
+                    pos = s_start[r] + (c < 32u ? __popc(s_mlo[r] & ((1u << c) - 1u)) : __popc(s_mlo[r]) + __popc(s_mhi[r] & ((1u << (c - 32u)) - 1u)));
+                else
+                    pos = s_start[P2G_LAYERS] + atomicAdd(&s_over, 1u);
+                s_pid[pos] = D.sorted[first + chunk + j];
+            }
+            __syncthreads();
+            for (uint32_t j = threadIdx.x; j < n; j += P2G_T) {
+                const uint32_t i = s_pid[j];
+                float4 pos = D.pos[i], vel = D.vel[i], c0 = D.c0[i], c1 = D.c1[i], c2 = D.c2[i];
+                V3 x = (xyz(pos) - g.org) / hh;
+                splat(tile, x, v3(0.0f, 0.5f, 0.5f), corner, 0, vel.x, xyz(c0), 1, FP_M, hh);
+                splat(tile, x, v3(0.5f, 0.0f, 0.5f), corner, 2, vel.y, xyz(c1), 3, FP_M, hh);
+                splat(tile, x, v3(0.5f, 0.5f, 0.0f), corner, 4, vel.z, xyz(c2), 5, FP_M, hh);
+                splat(tile, x, v3(0.5f, 0.5f, 0.5f), corner, A_PC, c0.w * 1e-6f, v3(0.0f, 0.0f, 0.0f), A_WC, FP_P, hh);
+            }
+            __syncthreads();
         }
-        __syncthreads();
-        // The tile goes out whole, with plain coalesced stores; k_p2g_gather sums the tiles
-        // that overlap each cell.
         int4* dst = reinterpret_cast<int4*>(D.tiles + (size_t)b * 8 * TILE);
         const int4* srcv = reinterpret_cast<const int4*>(tile);
         for (uint32_t t = threadIdx.x; t < 2 * TILE; t += P2G_T) dst[t] = srcv[t];
