@@ -70,17 +70,14 @@ __device__ __forceinline__ Gas hll(const Gas& l, const Gas& r, uint32_t d) {
     return {a * fl.rho + b * fr.rho + c * (r.rho - l.rho), a * fl.m + b * fr.m + c * (r.m - l.m), a * fl.e + b * fr.e + c * (r.e - l.e)};
 }
 
-__device__ __forceinline__ Gas across(const Dev& D, const Grid& g, int buf, uint32_t cell, const Gas& own, uint32_t d, bool hi) {
-    I3 e = {0, 0, 0};
-    int s = hi ? 1 : -1;
-    if (d == 0) e.x = s;
-    if (d == 1) e.y = s;
-    if (d == 2) e.z = s;
-    uint32_t nb = neighbour(g, cell, e);
+// The state across face (d, hi) of `cell` (air.wgsl:150-200): the outside air, the neighbour's
+// gas, or a ghost mirrored at a moving wall. `nb` is the neighbour, `nty` its type and `ng` its
+// gas (loaded by the caller; meaningless when nb is NONE).
+__device__ __forceinline__ Gas across(const Dev& D, uint32_t cell, const Gas& own, uint32_t d, bool hi, uint32_t nb, float nty, const Gas& ng) {
     if (nb == NONE) return ambient();
-    if (free_gas(D, nb)) return read_gas(D, buf, nb);
+    if (nty == GAS_T) return ng;
     float w = cfv(D, F_U + d, hi ? nb : cell);
-    if (cfv(D, F_TYPE, nb) == RUBBER_T) w = from_fp(accv(D, A_MV + d, nb), FP_A) / from_fp(accv(D, A_MW, nb), FP_A);
+    if (nty == RUBBER_T) w = from_fp(accv(D, A_MV + d, nb), FP_A) / from_fp(accv(D, A_MW, nb), FP_A);
     Gas gg = own;
     float u = own.m[d] / own.rho;
     gg.m[d] = own.rho * (2.0f * w - u);
@@ -455,15 +452,30 @@ __global__ void __launch_bounds__(256) k_air_substep(Dev D, int par) {
     const float k = dt_of(st) / (float)max(D.U->mem[2], 1u) / hh;
     float lim = BIG_F;
     CELL_LOOP(D, st) {
+        // The cell's and its six neighbours' types and gas are loaded first, all in flight
+        // together (a missing neighbour loads this cell's and is not used).
+        uint32_t nbr[6];
+        float nty[6];
+        Gas ng[6];
+#pragma unroll
+        for (int j = 0; j < 6; j++) nbr[j] = neighbour(g, cell, ed((uint32_t)(j >> 1), (j & 1) ? 1 : -1));
+        const float ty = cfv(D, F_TYPE, cell);
         Gas gg = read_gas(D, par, cell);
-        if (!free_gas(D, cell)) {
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+            const uint32_t at = nbr[j] != NONE ? nbr[j] : cell;
+            nty[j] = cfv(D, F_TYPE, at);
+            ng[j] = read_gas(D, par, at);
+        }
+        if (ty != GAS_T) {
             write_gas(D, 1 - par, cell, gg);
             continue;
         }
         Gas f = no_gas();
+#pragma unroll
         for (uint32_t d = 0; d < 3; d++) {
-            Gas lo = hll(across(D, g, par, cell, gg, d, false), gg, d);
-            Gas hi = hll(gg, across(D, g, par, cell, gg, d, true), d);
+            Gas lo = hll(across(D, cell, gg, d, false, nbr[2 * d], nty[2 * d], ng[2 * d]), gg, d);
+            Gas hi = hll(gg, across(D, cell, gg, d, true, nbr[2 * d + 1], nty[2 * d + 1], ng[2 * d + 1]), d);
             f = {f.rho + hi.rho - lo.rho, f.m + hi.m - lo.m, f.e + hi.e - lo.e};
         }
         Gas n = floored(Gas{gg.rho - k * f.rho, gg.m - k * f.m, gg.e - k * f.e});
