@@ -300,27 +300,57 @@ __global__ void k_project(Dev D) {
     }
 }
 
-__device__ __forceinline__ bool face_set(const Dev& D, const Grid& g, uint32_t cell, uint32_t d) {
-    if (cell == NONE) return false;
-    return cfv(D, F_TYPE, cell) == WATER_T || cell_type(D, neighbour(g, cell, ed(d, -1))) == WATER_T;
-}
+// Velocity extension in two passes (fluid.wgsl:604-674). Each cell loads everything its pass
+// reads first, all loads in flight together, then decides in the reference's order.
+__device__ __forceinline__ uint32_t cube_at(int x, int y, int z) { return (uint32_t)((x + 1) * 9 + (y + 1) * 3 + (z + 1)); }
 
 __global__ void k_extend_1(Dev D) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
     CELL_LOOP(D, st) {
+        // Types of the 3^3 cells around (GAS outside the grid), of the cells two down each axis,
+        // and the face velocities of the cell and its six neighbours.
+        uint32_t nc[27], n2[3];
+#pragma unroll
+        for (int k = 0; k < 27; k++) nc[k] = k == 13 ? cell : neighbour(g, cell, I3{k / 9 - 1, (k / 3) % 3 - 1, k % 3 - 1});
+#pragma unroll
+        for (int d = 0; d < 3; d++) n2[d] = neighbour(g, cell, ed((uint32_t)d, -2));
+        float T[27], T2[3], un[6][3], uo[3];
+#pragma unroll
+        for (int k = 0; k < 27; k++) T[k] = nc[k] != NONE ? cfv(D, F_TYPE, nc[k]) : GAS_T;
+#pragma unroll
+        for (int d = 0; d < 3; d++) T2[d] = n2[d] != NONE ? cfv(D, F_TYPE, n2[d]) : GAS_T;
+#pragma unroll
+        for (int d = 0; d < 3; d++) uo[d] = cfv(D, F_U + d, cell);
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+            const I3 o = e6(j);
+            const uint32_t nb = nc[cube_at(o.x, o.y, o.z)];
+#pragma unroll
+            for (int d = 0; d < 3; d++) un[j][d] = nb != NONE ? cfv(D, F_U + d, nb) : 0.0f;
+        }
+        // face_set (fluid.wgsl:604-610) of the cell at offset o: it exists, and it or the cell
+        // below it along d is water.
+        auto face_set = [&](I3 o, int d) -> bool {
+            if (nc[cube_at(o.x, o.y, o.z)] == NONE) return false;
+            if (T[cube_at(o.x, o.y, o.z)] == WATER_T) return true;
+            const I3 b = o - ed((uint32_t)d, 1);
+            const float tb = (b.x < -1 || b.y < -1 || b.z < -1) ? T2[d] : T[cube_at(b.x, b.y, b.z)];
+            return tb == WATER_T;
+        };
         uint32_t done = 0;
-        for (uint32_t d = 0; d < 3; d++) {
-            float u = cfv(D, F_U + d, cell);
-            if (face_set(D, g, cell, d)) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            float u = uo[d];
+            if (face_set(I3{0, 0, 0}, d)) {
                 done |= 1u << d;
             } else {
                 float sum = 0.0f, cnt = 0.0f;
-                for (int k = 0; k < 6; k++) {
-                    uint32_t nb = neighbour(g, cell, e6(k));
-                    if (face_set(D, g, nb, d)) {
-                        sum += cfv(D, F_U + d, nb);
+#pragma unroll
+                for (int j = 0; j < 6; j++) {
+                    if (face_set(e6(j), d)) {
+                        sum += un[j][d];
                         cnt += 1.0f;
                     }
                 }
@@ -335,32 +365,49 @@ __global__ void k_extend_1(Dev D) {
     }
 }
 
-__device__ __forceinline__ bool ext_set(const Dev& D, uint32_t cell, uint32_t d) {
-    return cell != NONE && ((f2u(cfv(D, F_EXT_SET, cell)) >> d) & 1u) != 0u;
-}
-
 __global__ void k_extend_2(Dev D) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
     CELL_LOOP(D, st) {
-        float ty = cfv(D, F_TYPE, cell);
-        for (uint32_t d = 0; d < 3; d++) {
-            float u = cfv(D, F_U + d, cell);
-            if (ext_set(D, cell, d)) {
-                u = cfv(D, F_EXT + d, cell);
+        uint32_t nb[6], lo[3];
+#pragma unroll
+        for (int j = 0; j < 6; j++) nb[j] = neighbour(g, cell, e6(j));
+#pragma unroll
+        for (int d = 0; d < 3; d++) lo[d] = nb[2 * d];  // e6 order: -x, +x, -y, +y, -z, +z
+        const float ty = cfv(D, F_TYPE, cell);
+        const uint32_t set = f2u(cfv(D, F_EXT_SET, cell));
+        float uo[3], eo[3], tlo[3], en[6][3];
+        uint32_t sn[6];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            uo[d] = cfv(D, F_U + d, cell);
+            eo[d] = cfv(D, F_EXT + d, cell);
+            tlo[d] = lo[d] != NONE ? cfv(D, F_TYPE, lo[d]) : GAS_T;
+        }
+#pragma unroll
+        for (int j = 0; j < 6; j++) {
+            sn[j] = nb[j] != NONE ? f2u(cfv(D, F_EXT_SET, nb[j])) : 0u;
+#pragma unroll
+            for (int d = 0; d < 3; d++) en[j][d] = nb[j] != NONE ? cfv(D, F_EXT + d, nb[j]) : 0.0f;
+        }
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            float u = uo[d];
+            if ((set >> d) & 1u) {
+                u = eo[d];
             } else {
                 float sum = 0.0f, cnt = 0.0f;
-                for (int k = 0; k < 6; k++) {
-                    uint32_t nb = neighbour(g, cell, e6(k));
-                    if (ext_set(D, nb, d)) {
-                        sum += cfv(D, F_EXT + d, nb);
+#pragma unroll
+                for (int j = 0; j < 6; j++) {
+                    if (nb[j] != NONE && ((sn[j] >> d) & 1u)) {
+                        sum += en[j][d];
                         cnt += 1.0f;
                     }
                 }
                 if (cnt > 0.0f) u = sum / cnt;
             }
-            *cfp(D, F_U + d, cell) = bounded(u, ty, cell_type(D, neighbour(g, cell, ed(d, -1))));
+            *cfp(D, F_U + d, cell) = bounded(u, ty, tlo[d]);
         }
     }
 }
