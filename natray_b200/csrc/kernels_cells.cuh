@@ -419,15 +419,26 @@ __device__ __forceinline__ float2 sample_grid(const Dev& D, const Grid& g, V3 x,
     V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
     const CellsNear n = near_of(g, base);
     float sx = 0.0f, sy = 0.0f;
-    for (int a = 0; a < 3; a++)
-        for (int b = 0; b < 3; b++)
-            for (int c = 0; c < 3; c++) {
-                uint32_t cell = near_cell(g, n, base + I3{a, b, c});
-                if (cell == NONE) continue;
-                float w = wx[a] * wy[b] * wz[c] * from_fp(accv(D, fw, cell), FP_W);
-                sx = sx + w * cfv(D, fu, cell);
-                sy = sy + w;
-            }
+    // A plane of 9 cells at a time: its 18 loads go out together, then the sums in order.
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        uint32_t cells[9];
+        int32_t wv[9];
+        float uv[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            cells[k] = near_cell(g, n, base + I3{a, k / 3, k % 3});
+            wv[k] = cells[k] != NONE ? accv(D, fw, cells[k]) : 0;
+            uv[k] = cells[k] != NONE ? cfv(D, fu, cells[k]) : 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            if (cells[k] == NONE) continue;
+            float w = wx[a] * wy[k / 3] * wz[k % 3] * from_fp(wv[k], FP_W);
+            sx = sx + w * uv[k];
+            sy = sy + w;
+        }
+    }
     return make_float2(sx, sy);
 }
 

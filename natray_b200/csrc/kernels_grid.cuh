@@ -542,25 +542,33 @@ __global__ void k_p2g_gather(Dev D) {
     for (uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x; cell < n_cells; cell += gridDim.x * blockDim.x) {
         const uint32_t b = cell >> 6;
         const I3 l = local_coord(cell);
-        int32_t s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        // The up to 2 x 2 x 2 tiles over the cell: per axis its own block (offset 0) and the one
+        // below (l <= 1) or above (l == 3). Their indices, then whether they hold sums, then all
+        // their entries, each step's loads in flight together.
+        const int ax[2] = {0, l.x <= 1 ? -1 : 1}, ay[2] = {0, l.y <= 1 ? -1 : 1}, az[2] = {0, l.z <= 1 ? -1 : 1};
+        const int nx = l.x == 2 ? 1 : 2, ny = l.y == 2 ? 1 : 2, nz = l.z == 2 ? 1 : 2;
         const uint32_t* nbt = D.block_nb + (size_t)b * 27u;
-        for (int ox = -1; ox <= 1; ox++) {
-            if ((ox < 0 && l.x > 1) || (ox > 0 && l.x < 3)) continue;
-            for (int oy = -1; oy <= 1; oy++) {
-                if ((oy < 0 && l.y > 1) || (oy > 0 && l.y < 3)) continue;
-                for (int oz = -1; oz <= 1; oz++) {
-                    if ((oz < 0 && l.z > 1) || (oz > 0 && l.z < 3)) continue;
-                    const uint32_t src = nbt[(ox + 1) * 9 + (oy + 1) * 3 + oz + 1];
-                    if (src == NONE || D.tile_ok[src] == 0u) continue;
-                    const uint32_t t = (uint32_t)(l.x + 1 - 4 * ox) * 49u + (uint32_t)(l.y + 1 - 4 * oy) * 7u + (uint32_t)(l.z + 1 - 4 * oz);
-                    const int32_t* tp = D.tiles + (size_t)src * 8 * TILE + t;
+        uint32_t src[8], tix[8];
 #pragma unroll
-                    for (int f = 0; f < 8; f++) s[f] = (int32_t)((uint32_t)s[f] + (uint32_t)tp[f * TILE]);
-                }
-            }
+        for (int i = 0; i < 8; i++) {
+            const int ix = i & 1, iy = (i >> 1) & 1, iz = i >> 2;
+            const int ox = ax[ix], oy = ay[iy], oz = az[iz];
+            src[i] = (ix < nx && iy < ny && iz < nz) ? nbt[(ox + 1) * 9 + (oy + 1) * 3 + oz + 1] : NONE;
+            tix[i] = (uint32_t)(l.x + 1 - 4 * ox) * 49u + (uint32_t)(l.y + 1 - 4 * oy) * 7u + (uint32_t)(l.z + 1 - 4 * oz);
+        }
+        bool ok[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) ok[i] = src[i] != NONE && D.tile_ok[src[i] != NONE ? src[i] : b] != 0u;
+        // Integer sums: the same in any order.
+        uint32_t s[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const int32_t* tp = D.tiles + (size_t)(ok[i] ? src[i] : b) * 8 * TILE + (ok[i] ? tix[i] : 0u);
+#pragma unroll
+            for (int f = 0; f < 8; f++) s[f] += ok[i] ? (uint32_t)tp[f * TILE] : 0u;
         }
 #pragma unroll
-        for (int f = 0; f < 8; f++) D.acc[(size_t)f * D.cap_cells + cell] = s[f];
+        for (int f = 0; f < 8; f++) D.acc[(size_t)f * D.cap_cells + cell] = (int32_t)s[f];
     }
 }
 
