@@ -53,9 +53,11 @@ struct Sim {
     uint32_t coop_ctas = 148;
     cudaError_t launch_err = cudaSuccess;
     cudaStream_t stream = nullptr;
-    cudaStream_t aux = nullptr;  // the second stream of the step's forks
+    cudaStream_t aux = nullptr;   // the second stream of the step's forks
+    cudaStream_t aux2 = nullptr;  // and the third (the air substeps)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork[3] = {nullptr, nullptr, nullptr}, ev_join[3] = {nullptr, nullptr, nullptr};
+    std::vector<cudaEvent_t> ev_sub;  // per substep: the rubber's, the air's
     World host;  // header (params, host control) of the world; sections are not kept
     ntr_gpu_params U{};
     Dev D{};
@@ -80,10 +82,13 @@ struct Sim {
         if (h_state && own_h_state) cudaFreeHost(h_state);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
-        for (int k = 0; k < 2; k++) {
+        for (int k = 0; k < 3; k++) {
             if (ev_fork[k]) cudaEventDestroy(ev_fork[k]);
             if (ev_join[k]) cudaEventDestroy(ev_join[k]);
         }
+        for (cudaEvent_t e : ev_sub)
+            if (e) cudaEventDestroy(e);
+        if (aux2) cudaStreamDestroy(aux2);
         if (aux) cudaStreamDestroy(aux);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -487,18 +492,47 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     L(k_extend_2, G_cell, 256, D);
     // G2P shares nothing with the rubber and air substeps or the spray's flight: they run
     // side by side.
+    // The rubber substeps on one side stream and the air substeps on another: rubber substep i
+    // reads the air buffer that air substep i - 1 writes, and air substep i overwrites the one
+    // rubber substep i - 1 reads, so substep i of the two runs side by side and each waits for
+    // the other's substep i - 1.
+    cudaStream_t a2 = prof ? s : S.aux2;
+    const uint32_t n_sub = std::max(n_mem, n_air);
+    if (a != s && S.ev_sub.size() < 2 * (size_t)n_sub) {
+        while (S.ev_sub.size() < 2 * (size_t)n_sub) {
+            cudaEvent_t e = nullptr;
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) S.launch_err = cudaErrorMemoryAllocation;
+            S.ev_sub.push_back(e);
+        }
+    }
     fork(1);
+    if (a2 != s) {
+        cudaEventRecord(S.ev_fork[2], s);
+        cudaStreamWaitEvent(a2, S.ev_fork[2], 0);
+    }
     LA(k_mem_sample, (uint32_t)(((uint64_t)D.Nv * 4 + 255) / 256), 256, D);
-    for (uint32_t i = 0; i < std::max(n_mem, n_air); i++) {
+    for (uint32_t i = 0; i < n_sub; i++) {
         if (i < n_mem) {
+            if (a != s && i >= 1 && i - 1 < n_air) cudaStreamWaitEvent(a, S.ev_sub[2 * (i - 1) + 1], 0);
             LA(k_mem_tri, g_tri, 256, D, (int)(i % 2));
             LA(k_mem_substep, g_vert, 256, D, i, (int)(i % 2));
+            if (a != s) cudaEventRecord(S.ev_sub[2 * i], a);
         }
-        if (i < n_air) LA(k_air_substep, G_cell, 256, D, (int)(i % 2));
+        if (i < n_air) {
+            if (a2 != s && i >= 1 && i - 1 < n_mem) cudaStreamWaitEvent(a2, S.ev_sub[2 * (i - 1)], 0);
+            k_air_substep<<<G_cell, 256, 0, a2>>>(D, (int)(i % 2));
+            n++;
+            if (prof) prof->mark("k_air_substep", a2);
+            if (a2 != s) cudaEventRecord(S.ev_sub[2 * i + 1], a2);
+        }
     }
     LA(k_spray_update, G_cell, 256, D);
     L(k_g2p, G_blk, G2P_T, D);
     join(1);
+    if (a2 != s) {
+        cudaEventRecord(S.ev_join[2], a2);
+        cudaStreamWaitEvent(s, S.ev_join[2], 0);
+    }
     L(k_spray_scan, 1, 1024, D);
     L(k_spray_emit, G_cell, 256, D);
     L(k_spray_commit, 1, 32, D);
@@ -612,7 +646,8 @@ static ntr_status create_from(const World& w, int device, Sim*& out, uint8_t* ar
     if (prop.major < 10) return fail(NTR_E_NODEVICE, "this library is built for sm_100a (B200); device is sm_" + std::to_string(prop.major * 10 + prop.minor));
     CU(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
     CU(cudaStreamCreateWithFlags(&S->aux, cudaStreamNonBlocking));
-    for (int k = 0; k < 2; k++) {
+    CU(cudaStreamCreateWithFlags(&S->aux2, cudaStreamNonBlocking));
+    for (int k = 0; k < 3; k++) {
         CU(cudaEventCreateWithFlags(&S->ev_fork[k], cudaEventDisableTiming));
         CU(cudaEventCreateWithFlags(&S->ev_join[k], cudaEventDisableTiming));
     }
