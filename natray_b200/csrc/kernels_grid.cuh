@@ -57,22 +57,26 @@ __global__ void k_begin_step(Dev D) {
 }
 
 // ---- clear: the last step's transfer sums, and this step's bitmask ----------------------------
-__global__ void k_clear(Dev D) {
+// Fields 0..7 of the sums are written whole by k_p2g_gather and A_N by k_p2g; the rest
+// accumulate atomically and start from zero. The two clears run on different streams.
+__global__ void k_clear_acc(Dev D) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
-    const int cur = cur_of(st);
     const uint32_t ncell = st->s.n_blocks_prev * 64u;
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    // Fields 0..7 are written whole by k_p2g_gather and A_N by k_p2g; the rest accumulate
-    // atomically and start from zero.
     constexpr uint32_t F0 = A_MF, NF = NTR_ACC_FIELDS - A_MF;
     for (size_t i = tid; i < (size_t)ncell * NF; i += stride) {
         size_t f = i / ncell, c = i - f * ncell;
         D.acc[(F0 + f) * D.cap_cells + c] = 0;
     }
-    uint32_t* m = D.mask[cur];
-    for (size_t w = tid; w < D.nwords; w += stride) m[w] = 0u;
+}
+
+__global__ void k_clear_mask(Dev D) {
+    const DevState* st = D.st;
+    if (st->s.dt_ns == 0) return;
+    uint32_t* m = D.mask[cur_of(st)];
+    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < D.nwords; w += (size_t)gridDim.x * blockDim.x) m[w] = 0u;
 }
 
 // Sets the bits of the blocks `slot` of the lanes where `valid`: one atomicOr per distinct

@@ -445,10 +445,21 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     if (prof && (part & PART_PRE)) prof->mark("start", s);
     if (part & PART_PRE) {
     L(k_begin_step, 1, 32, D);
-    L(k_clear, G_cell, 256, D);
+    // The side stream clears the last step's sums while the blocks are found and the particles
+    // sorted; it then splats the rubber and carries the air (which need the block set but touch
+    // none of what the sort and P2G read or write).
+    fork(0);
+    LA(k_clear_acc, G_cell, 256, D);
+    L(k_clear_mask, std::max((D.nwords + 255) / 256, 1u), 256, D);
     L(k_mark, (uint32_t)(((uint64_t)warp_round(D.Np) + warp_round(D.cap_blocks) + warp_round(D.Nv) + 255) / 256), 256, D);
     L(k_scan_words_a, D.scan_ctas, SCAN_T, D);
     L(k_scan_words_b, D.scan_ctas, SCAN_T, D);
+    if (a != s) {
+        cudaEventRecord(S.ev_fork[1], s);
+        cudaStreamWaitEvent(a, S.ev_fork[1], 0);
+    }
+    LA(k_mem_splat, g_vert, 256, D);
+    LA(k_air_carry, G_cell, 256, D);
     L(k_keys, g_part, 256, D);
     {
         const uint32_t P = D.radix_passes;
@@ -466,10 +477,6 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
         }
     }
     L(k_block_bounds, (D.Np + 1 + 255) / 256, 256, D);
-    // The rubber's splat and the air's carry touch none of what P2G reads or writes.
-    fork(0);
-    LA(k_mem_splat, g_vert, 256, D);
-    LA(k_air_carry, G_cell, 256, D);
     L(k_p2g, G_blk, P2G_T, D);
     L(k_p2g_gather, G_cell, 256, D);
     join(0);
