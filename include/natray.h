@@ -435,6 +435,101 @@ NTR_API ntr_status ntr_batch_info_get(ntr_batch* b, ntr_batch_info* out);
 NTR_API ntr_status ntr_sort_by_block_noalloc(const uint32_t* keys, uint32_t n, uint32_t n_blocks, uint32_t* sorted,
                                              uint32_t* block_start, void* stream);
 
+/* --- Keyframe cache: `Cache` of src/cache.rs ------------------------------------------------
+ * The simulation runs ahead and stores compact keyframes in a fixed device pool; playback
+ * blends between two of them into the buffers a renderer reads. A keyframe is, in u32 words
+ * (shaders/keys.wgsl:1-10): the spray slot count, the live spray count and two zero words;
+ * two words per water particle and per membrane vertex (21 bits per axis inside the 8 m box
+ * [-4, 4] x [-0.5, 7.5] x [-4, 4], the top bit of the second word set for a live particle); one
+ * alive bit per triangle; then, for the spray, one live bit per slot, the live count before each
+ * word of bits, and three words (position, radius bits) per live slot in slot order. A
+ * keyframe is rounded up to 256 bytes and never spans two pool pages.
+ *
+ * The cache borrows the simulation: it steps it in ntr_cache_bake and reads its buffers, and
+ * the simulation must outlive the cache (or be replaced with ntr_cache_rebuild). Every device
+ * buffer is allocated in ntr_cache_create; bake and show never allocate. */
+#define NTR_KEY_HEAD 4u        /* header words (src/cache.rs:20) */
+#define NTR_KEY_SPRAY_WORDS 3u /* words per live spray slot (src/cache.rs:21) */
+#define NTR_KEY_Q_MAX 2097151u /* position steps per axis over the 8 m box (shaders/keys.wgsl:18-20) */
+
+typedef struct ntr_cache ntr_cache;
+
+typedef struct ntr_cache_params {
+    uint64_t page_bytes; /* 128 MiB (src/cache.rs:16) */
+    uint32_t pages;      /* 16 (src/cache.rs:17) */
+    uint32_t n_arrivals; /* entries of `arrivals` in use, at most NTR_MAX_SHOTS */
+    double t_end;        /* end of the timeline, 1 s (src/cache.rs:14) */
+    double arrivals[NTR_MAX_SHOTS]; /* each shot's arrival time `flight.t_hit` (src/cache.rs:257) */
+} ntr_cache_params;
+
+/* One stored keyframe (`Key`, src/cache.rs:58-66). */
+typedef struct ntr_key_info {
+    double t;        /* simulated time */
+    uint64_t offset; /* bytes into its page */
+    uint64_t bytes;  /* its size (ntr_key_bytes) */
+    uint32_t page;
+    uint32_t spray;  /* spray slots in use */
+    uint32_t live;   /* of those, live */
+    uint32_t pad;
+} ntr_key_info;
+
+typedef struct ntr_cache_info {
+    uint32_t keys, done, full, shown_spray;
+    uint64_t used_bytes, pool_bytes, shown_id;
+    double end;    /* time of the newest keyframe */
+    double next_t; /* when the next keyframe is due */
+    double shown;  /* time of the shown state; NaN until the first ntr_cache_show */
+} ntr_cache_info;
+
+/* The buffers ntr_cache_show fills (src/cache.rs:393-408), plus the spray weights. */
+typedef enum ntr_shown {
+    NTR_SHOWN_PARTICLES = 0, /* n_particles x 2 float4: position (w 1), velocity (w 1 live, 0 not) */
+    NTR_SHOWN_SPRAY,         /* spray_cap x 2 float4: position + radius, velocity + weight (negative
+                                while the drop is still part of the crown sheet) */
+    NTR_SHOWN_MEM_POS,       /* n_verts float4 (w 0) */
+    NTR_SHOWN_ALIVE,         /* n_tris u32, 1 for an intact triangle */
+    NTR_SHOWN_WET,           /* wet_res^2 u32: water on the ground, 1e-3 mm^3 per cell */
+    NTR_SHOWN_SPRAY_W,       /* spray_cap float2: weight, time the drop tears loose */
+    NTR_SHOWN_COUNT
+} ntr_shown;
+
+/* Cache parameters for a scene: the reference's pool and timeline, and the shots' arrival
+ * times as Sim::new computes them (src/sim.rs:280-291: delay minus the earliest delay). CPU only. */
+NTR_API ntr_status ntr_cache_params_default(const ntr_sim_params* p, ntr_cache_params* out);
+/* Bytes of a keyframe with `spray` slots of which `live` are in use (`key_bytes`,
+ * src/cache.rs:412-421). CPU only. */
+NTR_API uint64_t ntr_key_bytes(uint32_t n_particles, uint32_t n_verts, uint32_t n_tris, uint32_t spray, uint32_t live);
+/* When the keyframe after one stored at `t` is due (src/cache.rs:249-264): 2% of the time since
+ * the last arrival, between 10 us and 4 ms, stretched when the keys still to come at that
+ * spacing would overrun the free pool, and never past the next arrival or t_end. CPU only. */
+NTR_API double ntr_key_next_time(double t, const double* arrivals, uint32_t n_arrivals, double t_end,
+                                 uint64_t free_bytes, uint64_t key_bytes);
+
+/* Cache::new without the Sim::new: allocates the pool and the shown buffers, takes the
+ * simulation to its start (Sim::advance(0, 0)) and stores the first keyframe. */
+NTR_API ntr_status ntr_cache_create(ntr_sim* s, const ntr_cache_params* cp, ntr_cache** out);
+/* Cache::rebuild: starts over on another simulation (or the same one restored), reusing the
+ * pool. The shown buffers are reallocated when the scene sizes change. */
+NTR_API ntr_status ntr_cache_rebuild(ntr_cache* c, ntr_sim* s);
+NTR_API ntr_status ntr_cache_destroy(ntr_cache* c);
+/* Cache::bake: up to max_steps simulation steps, storing keyframes when they are due. */
+NTR_API ntr_status ntr_cache_bake(ntr_cache* c, uint32_t max_steps, uint32_t* steps);
+/* Stores a keyframe of the simulation's current state now (what bake does when one is due;
+ * the schedule of later keys follows from it). */
+NTR_API ntr_status ntr_cache_store(ntr_cache* c);
+/* Cache::show: fills the shown buffers for time t (clamped to what was simulated). *changed
+ * is 0 when t is what is shown already. Asynchronous on the simulation's stream. */
+NTR_API ntr_status ntr_cache_show(ntr_cache* c, double t, int* changed);
+NTR_API ntr_status ntr_cache_info_get(ntr_cache* c, ntr_cache_info* out);
+NTR_API ntr_status ntr_cache_key(ntr_cache* c, uint32_t k, ntr_key_info* out);
+/* Lends keyframe k's words (valid until the cache restarts or is destroyed). */
+NTR_API ntr_status ntr_cache_key_buffer(ntr_cache* c, uint32_t k, void** dev_ptr, size_t* bytes);
+/* Lends a shown buffer (valid until rebuild or destroy). */
+NTR_API ntr_status ntr_cache_buffer(ntr_cache* c, ntr_shown which, void** dev_ptr, size_t* bytes);
+/* Copies the first `bytes` of a shown buffer, or of keyframe k's words when which is
+ * NTR_SHOWN_COUNT + k, to host memory (synchronous). */
+NTR_API ntr_status ntr_cache_download(ntr_cache* c, uint32_t which, void* host, size_t bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -124,6 +124,27 @@ class BatchInfo(C.Structure):
                 ("steps", C.c_uint64)]
 
 
+MAX_SHOTS = 4
+SHOWN = {"PARTICLES": 0, "SPRAY": 1, "MEM_POS": 2, "ALIVE": 3, "WET": 4, "SPRAY_W": 5}
+SHOWN_COUNT = 6
+
+
+class CacheParams(C.Structure):
+    _fields_ = [("page_bytes", C.c_uint64), ("pages", C.c_uint32), ("n_arrivals", C.c_uint32), ("t_end", C.c_double),
+                ("arrivals", C.c_double * MAX_SHOTS)]
+
+
+class KeyInfo(C.Structure):
+    _fields_ = [("t", C.c_double), ("offset", C.c_uint64), ("bytes", C.c_uint64), ("page", C.c_uint32),
+                ("spray", C.c_uint32), ("live", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class CacheInfo(C.Structure):
+    _fields_ = [("keys", C.c_uint32), ("done", C.c_uint32), ("full", C.c_uint32), ("shown_spray", C.c_uint32),
+                ("used_bytes", C.c_uint64), ("pool_bytes", C.c_uint64), ("shown_id", C.c_uint64), ("end", C.c_double),
+                ("next_t", C.c_double), ("shown", C.c_double)]
+
+
 # Every entry point include/natray.h declares, with its ctypes signature.
 _P = C.c_void_p
 _SIGS = {
@@ -162,6 +183,21 @@ _SIGS = {
     "ntr_batch_snapshot": (C.c_int, [_P, C.c_uint32, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
     "ntr_batch_retire": (C.c_int, [_P, C.c_uint32]),
     "ntr_batch_info_get": (C.c_int, [_P, C.POINTER(BatchInfo)]),
+    "ntr_cache_params_default": (C.c_int, [C.POINTER(SimParams), C.POINTER(CacheParams)]),
+    "ntr_key_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]),
+    "ntr_key_next_time": (C.c_double, [C.c_double, C.POINTER(C.c_double), C.c_uint32, C.c_double, C.c_uint64,
+                                       C.c_uint64]),
+    "ntr_cache_create": (C.c_int, [_P, C.POINTER(CacheParams), C.POINTER(_P)]),
+    "ntr_cache_rebuild": (C.c_int, [_P, _P]),
+    "ntr_cache_destroy": (C.c_int, [_P]),
+    "ntr_cache_bake": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "ntr_cache_store": (C.c_int, [_P]),
+    "ntr_cache_show": (C.c_int, [_P, C.c_double, C.POINTER(C.c_int)]),
+    "ntr_cache_info_get": (C.c_int, [_P, C.POINTER(CacheInfo)]),
+    "ntr_cache_key": (C.c_int, [_P, C.c_uint32, C.POINTER(KeyInfo)]),
+    "ntr_cache_key_buffer": (C.c_int, [_P, C.c_uint32, C.POINTER(_P), C.POINTER(C.c_size_t)]),
+    "ntr_cache_buffer": (C.c_int, [_P, C.c_int, C.POINTER(_P), C.POINTER(C.c_size_t)]),
+    "ntr_cache_download": (C.c_int, [_P, C.c_uint32, _P, C.c_size_t]),
 }
 
 _lib = None

@@ -1262,3 +1262,173 @@ NTR_API ntr_status ntr_batch_info_get(ntr_batch* batch, ntr_batch_info* out) {
 }
 
 }  // extern "C"
+
+// ---- keyframe cache (include/natray.h, ntr_cache_*) ---------------------------------------------
+#include "cache.cuh"
+
+struct ntr_cache {
+    Cache* c;
+};
+
+#define CGUARD(cache)                                                                   \
+    if (!(cache) || !(cache)->c) return fail(NTR_E_INVALID, "null cache handle");        \
+    Cache& C = *(cache)->c;                                                             \
+    if (cudaSetDevice(C.device) != cudaSuccess) return fail(NTR_E_CUDA, "cudaSetDevice failed")
+
+extern "C" {
+
+NTR_API ntr_status ntr_cache_params_default(const ntr_sim_params* p, ntr_cache_params* out) {
+    if (!p || !out) return fail(NTR_E_INVALID, "null argument");
+    if (p->n_shots > NTR_MAX_SHOTS) return fail(NTR_E_INVALID, "too many shots");
+    std::memset(out, 0, sizeof *out);
+    out->page_bytes = 128ull << 20;
+    out->pages = 16;
+    out->t_end = 1.0;
+    // t_hit of src/sim.rs:280-291: each shot's delay after the earliest, f32 difference in ms.
+    float first = 3.4028235e38f;
+    for (uint32_t k = 0; k < p->n_shots; k++) first = std::min(first, p->shots[k].delay_ms);
+    out->n_arrivals = p->n_shots;
+    for (uint32_t k = 0; k < p->n_shots; k++) out->arrivals[k] = (double)(p->shots[k].delay_ms - first) * 1e-3;
+    return NTR_OK;
+}
+
+NTR_API uint64_t ntr_key_bytes(uint32_t n_particles, uint32_t n_verts, uint32_t n_tris, uint32_t spray, uint32_t live) {
+    return key_bytes_of(n_particles, n_verts, n_tris, spray, live);
+}
+
+NTR_API double ntr_key_next_time(double t, const double* arrivals, uint32_t n_arrivals, double t_end, uint64_t free_bytes,
+                                 uint64_t key_bytes) {
+    if (!arrivals) n_arrivals = 0;
+    return key_next_time(t, arrivals, n_arrivals, t_end, std::max<uint64_t>(free_bytes, 1), key_bytes);
+}
+
+static ntr_status cache_check_params(const ntr_cache_params* cp) {
+    if (cp->pages == 0 || cp->page_bytes < 256) return fail(NTR_E_INVALID, "the keyframe pool needs at least one page of 256 bytes");
+    if (cp->n_arrivals > NTR_MAX_SHOTS) return fail(NTR_E_INVALID, "too many arrivals");
+    if (cp->page_bytes > (1ull << 40) / cp->pages) return fail(NTR_E_INVALID, "keyframe pool too large");
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_cache_create(ntr_sim* sim, const ntr_cache_params* cp, ntr_cache** out) {
+    if (!out || !cp) return fail(NTR_E_INVALID, "null argument");
+    *out = nullptr;
+    GUARD(sim);
+    ntr_status r = cache_check_params(cp);
+    if (r != NTR_OK) return r;
+    std::unique_ptr<Cache> c(new Cache);
+    c->handle = sim, c->S = &S, c->device = S.device, c->P = *cp;
+    c->pool_bytes = cp->page_bytes * cp->pages;
+    if (cudaMalloc(&c->pool, c->pool_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        c->pool = nullptr;
+        return fail(NTR_E_NOMEM, "device allocation of the keyframe pool (" + std::to_string(c->pool_bytes) + " bytes) failed");
+    }
+    CU(cudaMallocHost(&c->h_counts, 16));
+    if ((r = cache_size_for(*c, S)) != NTR_OK) return r;
+    if ((r = cache_restart(*c)) != NTR_OK) return r;
+    *out = new ntr_cache{c.release()};
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_cache_rebuild(ntr_cache* cache, ntr_sim* sim) {
+    CGUARD(cache);
+    if (!sim || !sim->s) return fail(NTR_E_INVALID, "null simulation handle");
+    if (sim->s->device != C.device) return fail(NTR_E_INVALID, "the simulation is on another device than the cache");
+    C.handle = sim, C.S = sim->s;
+    ntr_status r = cache_size_for(C, *C.S);
+    if (r != NTR_OK) return r;
+    return cache_restart(C);
+}
+
+NTR_API ntr_status ntr_cache_destroy(ntr_cache* cache) {
+    if (!cache) return NTR_OK;
+    delete cache->c;
+    delete cache;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_cache_bake(ntr_cache* cache, uint32_t max_steps, uint32_t* steps) {
+    CGUARD(cache);
+    return cache_bake(C, max_steps, steps);
+}
+
+NTR_API ntr_status ntr_cache_store(ntr_cache* cache) {
+    CGUARD(cache);
+    if (C.done) return NTR_OK;
+    return cache_store(C);
+}
+
+NTR_API ntr_status ntr_cache_show(ntr_cache* cache, double t, int* changed) {
+    CGUARD(cache);
+    return cache_show(C, t, changed);
+}
+
+NTR_API ntr_status ntr_cache_info_get(ntr_cache* cache, ntr_cache_info* out) {
+    CGUARD(cache);
+    if (!out) return fail(NTR_E_INVALID, "null argument");
+    std::memset(out, 0, sizeof *out);
+    out->keys = (uint32_t)C.keys.size(), out->done = C.done, out->full = C.full, out->shown_spray = C.shown_spray;
+    out->used_bytes = C.used(), out->pool_bytes = C.pool_bytes, out->shown_id = C.shown_id;
+    out->end = C.end(), out->next_t = C.next_t, out->shown = C.shown;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_cache_key(ntr_cache* cache, uint32_t k, ntr_key_info* out) {
+    CGUARD(cache);
+    if (!out) return fail(NTR_E_INVALID, "null argument");
+    if (k >= C.keys.size()) return fail(NTR_E_INVALID, "keyframe index out of range");
+    const KeyRec& r = C.keys[k];
+    std::memset(out, 0, sizeof *out);
+    out->t = r.t, out->offset = r.offset, out->bytes = r.bytes, out->page = r.page, out->spray = r.spray, out->live = r.live;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_cache_key_buffer(ntr_cache* cache, uint32_t k, void** dev_ptr, size_t* bytes) {
+    CGUARD(cache);
+    if (k >= C.keys.size()) return fail(NTR_E_INVALID, "keyframe index out of range");
+    if (dev_ptr) *dev_ptr = C.key_ptr(C.keys[k]);
+    if (bytes) *bytes = C.keys[k].bytes;
+    return NTR_OK;
+}
+
+static ntr_status cache_buffer(Cache& C, uint32_t which, void** p, size_t* b) {
+    switch (which) {
+        case NTR_SHOWN_PARTICLES: *p = C.shown_p, *b = (size_t)C.np * 32; break;
+        case NTR_SHOWN_SPRAY: *p = C.shown_drops, *b = (size_t)C.spray_cap * 32; break;
+        case NTR_SHOWN_MEM_POS: *p = C.shown_mem, *b = (size_t)C.nv * 16; break;
+        case NTR_SHOWN_ALIVE: *p = C.shown_alive, *b = (size_t)C.nt * 4; break;
+        case NTR_SHOWN_WET: *p = C.shown_wet, *b = (size_t)C.wet_res * C.wet_res * 4; break;
+        case NTR_SHOWN_SPRAY_W: *p = C.spray_w, *b = (size_t)C.spray_cap * 8; break;
+        default:
+            if (which - NTR_SHOWN_COUNT >= C.keys.size()) return fail(NTR_E_INVALID, "unknown cache buffer");
+            *p = C.key_ptr(C.keys[which - NTR_SHOWN_COUNT]), *b = C.keys[which - NTR_SHOWN_COUNT].bytes;
+    }
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_cache_buffer(ntr_cache* cache, ntr_shown which, void** dev_ptr, size_t* bytes) {
+    CGUARD(cache);
+    if ((uint32_t)which >= NTR_SHOWN_COUNT) return fail(NTR_E_INVALID, "unknown shown buffer");
+    void* p = nullptr;
+    size_t b = 0;
+    ntr_status r = cache_buffer(C, (uint32_t)which, &p, &b);
+    if (r != NTR_OK) return r;
+    if (dev_ptr) *dev_ptr = p;
+    if (bytes) *bytes = b;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_cache_download(ntr_cache* cache, uint32_t which, void* host, size_t bytes) {
+    CGUARD(cache);
+    if (!host && bytes) return fail(NTR_E_INVALID, "null argument");
+    void* p = nullptr;
+    size_t b = 0;
+    ntr_status r = cache_buffer(C, which, &p, &b);
+    if (r != NTR_OK) return r;
+    if (bytes > b) return fail(NTR_E_INVALID, "download larger than the buffer");
+    CU(cudaStreamSynchronize(C.S->stream));
+    CU(cudaMemcpy(host, p, bytes, cudaMemcpyDeviceToHost));
+    return NTR_OK;
+}
+
+}  // extern "C"
