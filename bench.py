@@ -126,6 +126,60 @@ def algorithmic_bytes(kernel: str, st: dict, n_particles: int, iters: int) -> fl
     return 0.0
 
 
+def keyframe_bench(sim, reps: int, peak: float, wet_res: int) -> dict:
+    """Keyframe store and show (the reference's Cache::bake / Cache::show) on the bench scene:
+    `reps` keyframes 4 us of simulated time apart, then shows between them. A store's two device
+    parts (spray index, packing) are timed with events on the simulation's stream; the shows are
+    issued back to back (each call returns before its work is done) and timed as a run, so the
+    device stays busy and host launch gaps do not count."""
+    import numpy as np
+    from natray_b200.cache import Cache
+
+    info = sim.info
+    n_p, n_v, n_t = info.n_particles, info.n_verts, info.n_tris
+    c = Cache(sim)
+    idx, pk, call, st_bytes = [], [], [], []
+    for _ in range(reps):
+        sim.advance(sim._info().t + 4e-6, 16)
+        t0 = time.perf_counter()
+        c.store()
+        a, b, _ = c.last_times()
+        call.append(time.perf_counter() - t0)
+        idx.append(a * 1e-3)
+        pk.append(b * 1e-3)
+        k = c.keys()[-1]
+        n, live = k["spray"], k["live"]
+        # pack reads position (16 B) and the alive word (4 B) of a particle and writes 8 B; a vertex
+        # 16 + 8; a triangle 4 + 1/8; a spray slot is read by the index (4 B) and the pack (24 B)
+        # and its weights written (8 B); a live slot's 12 B and two words per 32 slots written.
+        st_bytes.append(28 * n_p + 24 * n_v + 4.125 * n_t + 36 * n + 12 * live + 8 * ((n + 31) // 32))
+    keys = c.keys()
+    times = [0.5 * (a["t"] + b["t"]) for a, b in zip(keys[1:-1], keys[2:])]
+    m = max(k["spray"] for k in keys)
+    # two keyframes' particle words read (16 B) and the shown particle written (32 B); a vertex
+    # 16 + 16; a triangle's flag written; a spray slot's words of both keys, its landing record
+    # and weights read and 32 B written; the wet map cleared and the ground touch times read.
+    sh_bytes = 48 * n_p + 32 * n_v + 4 * n_t + 80 * m + 8 * wet_res * wet_res
+    c.show(times[-1])
+    c.last_times()
+    t0 = time.perf_counter()
+    for tt in times[:-1]:
+        c.show(tt)
+    c.last_times()  # waits for the last show
+    show_s = (time.perf_counter() - t0) / max(len(times) - 1, 1)
+    c.close()
+    med = lambda v: float(np.median(v))
+    i_t, p_t, s_b = med(idx), med(pk), med(st_bytes)
+    return {"workload": f"{reps} keyframes of the {n_p}-particle scene, 4 us apart, and a show between each pair",
+            "key_bytes": int(keys[-1]["bytes"]), "spray_slots": int(keys[-1]["spray"]), "live_spray": int(keys[-1]["live"]),
+            "index_us": i_t * 1e6, "pack_us": p_t * 1e6, "store_call_us": med(call) * 1e6,
+            "pack_gbs": s_b / p_t / 1e9, "pack_frac": s_b / p_t / 1e9 / peak,
+            "show_us": show_s * 1e6, "show_gbs": sh_bytes / show_s / 1e9, "show_frac": sh_bytes / show_s / 1e9 / peak,
+            "peak_gbs": peak,
+            "note": "store: events on the simulation's stream around each of its two device parts; the host's read of the "
+                    "spray counts between them is in store_call_us only. show: back-to-back calls timed as a run"}
+
+
 def run_native(args, rank, world, local):
     import numpy as np
     from natray_b200 import Params, build_world
@@ -246,6 +300,8 @@ def run_native(args, rank, world, local):
             "kernel_shares": shares,
             "clocks": clk.summary(),
         }
+    if rank == 0 and world == 1 and args.keyframes:
+        result["keyframes"] = keyframe_bench(sim, args.keyframes, peak, int(w.h.wet_res))
     sim.close()
     if use_dist:
         import torch.distributed as dist
@@ -317,6 +373,7 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=64, help="requests of the serving loop (0: skip)")
     ap.add_argument("--serve-steps", type=int, default=100)
     ap.add_argument("--serve-rate", type=float, default=20.0, help="request arrivals per second")
+    ap.add_argument("--keyframes", type=int, default=16, help="keyframes stored and shown at the bench scene (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_env()

@@ -521,6 +521,11 @@ NTR_API ntr_status ntr_cache_store(ntr_cache* c);
  * is 0 when t is what is shown already. Asynchronous on the simulation's stream. */
 NTR_API ntr_status ntr_cache_show(ntr_cache* c, double t, int* changed);
 NTR_API ntr_status ntr_cache_info_get(ntr_cache* c, ntr_cache_info* out);
+/* Device time (ms) of the last keyframe store, in its two parts (the spray index, then the
+ * packing; the host's read of the spray counts between them is in neither), and of the last
+ * show, measured with events on the simulation's stream; 0 before the first. Any pointer may be
+ * NULL. Waits for the timed work to finish. */
+NTR_API ntr_status ntr_cache_last_times(ntr_cache* c, double* index_ms, double* pack_ms, double* show_ms);
 NTR_API ntr_status ntr_cache_key(ntr_cache* c, uint32_t k, ntr_key_info* out);
 /* Lends keyframe k's words (valid until the cache restarts or is destroyed). */
 NTR_API ntr_status ntr_cache_key_buffer(ntr_cache* c, uint32_t k, void** dev_ptr, size_t* bytes);

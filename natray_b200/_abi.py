@@ -194,6 +194,7 @@ _SIGS = {
     "ntr_cache_store": (C.c_int, [_P]),
     "ntr_cache_show": (C.c_int, [_P, C.c_double, C.POINTER(C.c_int)]),
     "ntr_cache_info_get": (C.c_int, [_P, C.POINTER(CacheInfo)]),
+    "ntr_cache_last_times": (C.c_int, [_P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "ntr_cache_key": (C.c_int, [_P, C.c_uint32, C.POINTER(KeyInfo)]),
     "ntr_cache_key_buffer": (C.c_int, [_P, C.c_uint32, C.POINTER(_P), C.POINTER(C.c_size_t)]),
     "ntr_cache_buffer": (C.c_int, [_P, C.c_int, C.POINTER(_P), C.POINTER(C.c_size_t)]),

@@ -104,6 +104,12 @@ class Cache:
         check(lib().ntr_cache_info_get(self._h, C.byref(i)))
         return {k: getattr(i, k) for k, _ in i._fields_}
 
+    def last_times(self) -> tuple[float, float, float]:
+        """Device ms of the last store's spray index and packing, and of the last show."""
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        check(lib().ntr_cache_last_times(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
     def end(self) -> float:
         return self.info["end"]
 

@@ -2,14 +2,15 @@
 // layout of shaders/keys.wgsl, the packing of shaders/pack.wgsl and the playback of
 // shaders/show.wgsl.
 //
-// Storing a keyframe is three launches on the simulation's stream and one 8-byte read back:
-// k_key_count (live spray slots per tile of 256, from one warp ballot per 32 slots),
-// k_key_scan (one CTA: the tiles' exclusive prefix, and the slot and live counts), the read
-// back that sizes and places the keyframe, then k_key_pack, one launch whose CTA ranges pack
+// Storing a keyframe is two launches on the simulation's stream and one 8-byte read back:
+// k_key_index (live spray slots per tile of 256, from one warp ballot per 32 slots; the CTA
+// that finishes last scans the tiles and writes the slot and live counts), the read back that
+// sizes and places the keyframe, then k_key_pack, one launch whose CTA ranges pack
 // the water particles, the membrane vertices, the triangles' alive bits (a ballot per 32) and
 // the spray (bits, per-word prefixes and the live slots' words). Showing one is a clear of the
-// wet map, k_key_show (ranges for water, vertices, triangles, spray and landed drops) and
-// k_key_touch, which must follow the drops' additions (a max over their sums).
+// wet map, k_key_drops (the landed drops' additions, when key b has spray) and k_key_show
+// (ranges for water, vertices, triangles, spray and the ground touch, a max over the drops'
+// sums, so after them).
 //
 // Every float operation is written as the reference's expression with one rounding per
 // operation (no contraction; this file is built with -fmad=false): `mix(a, b, f)` is
@@ -28,6 +29,7 @@ constexpr float Q_SIZE = 8.0f, Q_MAX = 2097151.0f;
 constexpr float Q_STEP = Q_SIZE / Q_MAX;  // the WGSL constant Q_SIZE / Q_MAX, one f32 division
 constexpr uint32_t KEY_T = 256;           // threads per CTA of the keyframe kernels
 constexpr uint32_t KEY_TILE = 256;        // spray slots per tile (8 words of live bits)
+constexpr uint32_t KEY_PER = 4;           // water particles per thread in the pack and show kernels
 
 // Word offsets of a keyframe's parts (shaders/keys.wgsl:38-54).
 struct KeyLayout {
@@ -67,60 +69,52 @@ __device__ __forceinline__ V3 mix3(V3 a, V3 b, float f) { return {mixf(a.x, b.x,
 
 // ---- storing ------------------------------------------------------------------------------------
 
-// Live spray slots (radius > 0) of the first n = min(spray_count, spray_cap), counted per tile
-// of KEY_TILE slots. The live bits themselves are taken again by k_key_pack from the same data.
-__global__ void __launch_bounds__(KEY_T) k_key_count(Dev D, uint32_t* tile_tot) {
-    __shared__ uint32_t s_cnt[KEY_T / 32];
+// The live spray index: live slots (radius > 0) of the first n = min(spray_count, spray_cap)
+// counted per tile of KEY_TILE slots (one ballot per 32), then, in the CTA that finishes last
+// (a counter taken after a fence; no CTA waits for another), the tiles' exclusive prefix and
+// counts = {n, live}. The live bits themselves are taken again by k_key_pack from the same data.
+// counts[2] is the finish counter: zero before the launch, zero again after it.
+__global__ void __launch_bounds__(KEY_T) k_key_index(Dev D, uint32_t* tile_tot, uint32_t* tile_pre, uint32_t* counts) {
+    __shared__ uint32_t s_w[KEY_T / 32];
+    __shared__ uint32_t s_last;
     const uint32_t n = min(D.st->s.spray_count, D.spray_cap);
+    const uint32_t nt = (n + KEY_TILE - 1) / KEY_TILE;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    for (uint32_t t = blockIdx.x; t * KEY_TILE < n; t += gridDim.x) {
+    for (uint32_t t = blockIdx.x; t < nt; t += gridDim.x) {
         const uint32_t i = t * KEY_TILE + threadIdx.x;
         const bool live = i < n && D.spray[3 * (size_t)i].w > 0.0f;
         const uint32_t bits = __ballot_sync(0xffffffffu, live);
-        if (lane == 0) s_cnt[warp] = __popc(bits);
+        if (lane == 0) s_w[warp] = __popc(bits);
         __syncthreads();
         if (threadIdx.x == 0) {
             uint32_t sum = 0;
-            for (uint32_t w = 0; w < KEY_T / 32; w++) sum += s_cnt[w];
+            for (uint32_t w = 0; w < KEY_T / 32; w++) sum += s_w[w];
             tile_tot[t] = sum;
         }
         __syncthreads();
     }
-}
-
-// One CTA of 1024: the tiles' exclusive prefix of live slots; counts = {n, live}.
-__global__ void __launch_bounds__(1024) k_key_scan(Dev D, const uint32_t* tile_tot, uint32_t* tile_pre, uint32_t* counts) {
-    __shared__ uint32_t s_w[32];
-    const uint32_t n = min(D.st->s.spray_count, D.spray_cap);
-    const uint32_t nt = (n + KEY_TILE - 1) / KEY_TILE;
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    __threadfence();
+    if (threadIdx.x == 0) s_last = atomicAdd(counts + 2, 1u) == gridDim.x - 1u;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
     uint32_t carry = 0;
-    for (uint32_t base = 0; base < nt; base += 1024) {
+    for (uint32_t base = 0; base < nt; base += KEY_T) {
         const uint32_t i = base + threadIdx.x;
-        const uint32_t v = i < nt ? tile_tot[i] : 0u;
-        uint32_t inc = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= (uint32_t)o) inc += y;
-        }
-        if (lane == 31) s_w[warp] = inc;
-        __syncthreads();
-        uint32_t before = 0, all = 0;
-        for (uint32_t w = 0; w < 32; w++) {
-            before += w < warp ? s_w[w] : 0u;
-            all += s_w[w];
-        }
-        if (i < nt) tile_pre[i] = carry + before + inc - v;
-        carry += all;
-        __syncthreads();
+        const uint32_t v = i < nt ? __ldcg(tile_tot + i) : 0u;
+        uint32_t total;
+        const uint32_t ex = cta_scan256(v, &total);
+        if (i < nt) tile_pre[i] = carry + ex;
+        carry += total;
     }
     if (threadIdx.x == 0) {
         counts[0] = n;
         counts[1] = carry;
+        counts[2] = 0u;
     }
 }
 
-// CTA ranges of k_key_pack: [0, b_mem) particles, [b_mem, b_alive) vertices, [b_alive, b_spray)
+// CTA ranges of k_key_pack: [0, b_mem) particles (KEY_PER a thread), [b_mem, b_alive) vertices, [b_alive, b_spray)
 // alive words (a warp per word), [b_spray, b_end) spray tiles.
 struct PackRanges {
     uint32_t b_mem, b_alive, b_spray, b_end;
@@ -133,13 +127,21 @@ __global__ void __launch_bounds__(KEY_T) k_key_pack(Dev D, uint32_t* __restrict_
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t b = blockIdx.x;
     if (b == 0 && threadIdx.x < KEY_HEAD) key[threadIdx.x] = threadIdx.x == 0 ? R.n : threadIdx.x == 1 ? R.live : 0u;
-    if (b < R.b_mem) {  // pack_water (shaders/pack.wgsl:38-44)
-        const uint32_t i = b * KEY_T + threadIdx.x;
-        if (i >= D.Np) return;
-        const float4 p = D.pos[i];
-        const float alive = D.vel[i].w;
-        const uint2 w = pack_pos(p.x, p.y, p.z, alive > 0.5f);
-        reinterpret_cast<uint2*>(key + KEY_HEAD)[i] = w;
+    if (b < R.b_mem) {  // pack_water (shaders/pack.wgsl:38-44), KEY_PER particles a thread
+        const uint32_t i0 = b * KEY_T * KEY_PER + threadIdx.x;
+        float4 p[KEY_PER];
+        float alive[KEY_PER];
+#pragma unroll
+        for (uint32_t k = 0; k < KEY_PER; k++) {  // every load first: KEY_PER in flight
+            const uint32_t i = i0 + k * KEY_T;
+            p[k] = i < D.Np ? D.pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+            alive[k] = i < D.Np ? D.vel[i].w : 0.f;
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < KEY_PER; k++) {
+            const uint32_t i = i0 + k * KEY_T;
+            if (i < D.Np) reinterpret_cast<uint2*>(key + KEY_HEAD)[i] = pack_pos(p[k].x, p[k].y, p[k].z, alive[k] > 0.5f);
+        }
         return;
     }
     if (b < R.b_alive) {  // pack_mem (:46-51)
@@ -224,25 +226,40 @@ __device__ __forceinline__ float4 spray_slot(const uint32_t* key, const KeyLayou
     return make_float4(p.x, p.y, p.z, __uint_as_float(key[base + 2]));
 }
 
+__device__ __forceinline__ void show_water_one(const ShowArgs& A, uint32_t i, uint2 wa, uint2 wb) {
+    const V3 pa = unpack_pos(wa), pb = unpack_pos(wb);
+    V3 pos = A.f < 0.5f ? pa : pb;
+    const bool live = A.f < 0.5f ? flagged(wa) : flagged(wb);
+    V3 vel{0.f, 0.f, 0.f};
+    if (flagged(wa) && flagged(wb)) {
+        pos = mix3(pa, pb, A.f);
+        vel = {__fmul_rn(__fsub_rn(pb.x, pa.x), A.inv), __fmul_rn(__fsub_rn(pb.y, pa.y), A.inv),
+               __fmul_rn(__fsub_rn(pb.z, pa.z), A.inv)};
+    }
+    A.out_p[2 * (size_t)i] = make_float4(pos.x, pos.y, pos.z, 1.0f);
+    A.out_p[2 * (size_t)i + 1] = make_float4(vel.x, vel.y, vel.z, live ? 1.0f : 0.0f);
+}
+
+// CTA ranges: [0, b_mem) water (KEY_PER particles a thread), [b_mem, b_alive) vertices,
+// [b_alive, b_spray) triangles, [b_spray, b_drops) spray slots, [b_drops, b_end) wet-map cells
+// (the ground touch, after k_key_drops has added the landed drops).
 __global__ void __launch_bounds__(KEY_T) k_key_show(Dev D, ShowArgs A) {
     const KeyLayout K{D.Np, D.Nv, D.Nt};
     const uint32_t b = blockIdx.x;
     if (b < A.b_mem) {  // show_water (shaders/show.wgsl:41-60)
-        const uint32_t i = b * KEY_T + threadIdx.x;
-        if (i >= D.Np) return;
-        const uint2 wa = reinterpret_cast<const uint2*>(A.ka + KEY_HEAD)[i];
-        const uint2 wb = reinterpret_cast<const uint2*>(A.kb + KEY_HEAD)[i];
-        const V3 pa = unpack_pos(wa), pb = unpack_pos(wb);
-        V3 pos = A.f < 0.5f ? pa : pb;
-        const bool live = A.f < 0.5f ? flagged(wa) : flagged(wb);
-        V3 vel{0.f, 0.f, 0.f};
-        if (flagged(wa) && flagged(wb)) {
-            pos = mix3(pa, pb, A.f);
-            vel = {__fmul_rn(__fsub_rn(pb.x, pa.x), A.inv), __fmul_rn(__fsub_rn(pb.y, pa.y), A.inv),
-                   __fmul_rn(__fsub_rn(pb.z, pa.z), A.inv)};
+        const uint32_t i0 = b * KEY_T * KEY_PER + threadIdx.x;
+        uint2 wa[KEY_PER], wb[KEY_PER];
+#pragma unroll
+        for (uint32_t k = 0; k < KEY_PER; k++) {  // every load first
+            const uint32_t i = i0 + k * KEY_T;
+            wa[k] = i < D.Np ? reinterpret_cast<const uint2*>(A.ka + KEY_HEAD)[i] : make_uint2(0u, 0u);
+            wb[k] = i < D.Np ? reinterpret_cast<const uint2*>(A.kb + KEY_HEAD)[i] : make_uint2(0u, 0u);
         }
-        A.out_p[2 * (size_t)i] = make_float4(pos.x, pos.y, pos.z, 1.0f);
-        A.out_p[2 * (size_t)i + 1] = make_float4(vel.x, vel.y, vel.z, live ? 1.0f : 0.0f);
+#pragma unroll
+        for (uint32_t k = 0; k < KEY_PER; k++) {
+            const uint32_t i = i0 + k * KEY_T;
+            if (i < D.Np) show_water_one(A, i, wa[k], wb[k]);
+        }
         return;
     }
     if (b < A.b_alive) {  // show_mem (:62-68)
@@ -292,42 +309,43 @@ __global__ void __launch_bounds__(KEY_T) k_key_show(Dev D, ShowArgs A) {
         A.out_spray[2 * (size_t)i + 1] = make_float4(vel.x, vel.y, vel.z, t < w.y ? -w.x : w.x);
         return;
     }
-    {  // show_wet_drops (:114-136): a landed drop spreads over up to 5 x 5 cells
+    {  // show_wet_touch (:138-146): where the water body touched down by now the ground is soaked
         const uint32_t i = (b - A.b_drops) * KEY_T + threadIdx.x;
-        if (i >= A.kb[0]) return;
-        const float4 l = D.landed[i];
-        if (l.z <= 0.0f || l.w > A.t) return;
-        const float h = A.wet_half;
         const uint32_t res = A.wet_res;
-        const float cell = __fdiv_rn(__fmul_rn(2.0f, h), (float)res);
-        const float r = l.z;
-        const int k = (int)fminf(fmaxf(__fdiv_rn(__fmul_rn(3.0f, r), cell), 0.0f), 2.0f);
-        const float n = (float)((2 * k + 1) * (2 * k + 1));
-        const uint32_t amount =
-            __float2uint_rz(__fdiv_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(4.18879f, r), r), r), 1e12f), n));
-        const float two_h = __fmul_rn(2.0f, h);
-        for (int y = -k; y <= k; y++) {
-            for (int x = -k; x <= k; x++) {
-                const float u = __fdiv_rn(__fadd_rn(__fadd_rn(l.x, __fmul_rn((float)x, cell)), h), two_h);
-                const float v = __fdiv_rn(__fadd_rn(__fadd_rn(l.y, __fmul_rn((float)y, cell)), h), two_h);
-                if (u < 0.0f || v < 0.0f || u >= 1.0f || v >= 1.0f) continue;
-                // u, v < 1 keep the cell inside the map for a power-of-two resolution (the
-                // reference's 1024); the min guards any other.
-                const uint32_t cx = min(__float2uint_rz(__fmul_rn(u, (float)res)), res - 1u);
-                const uint32_t cy = min(__float2uint_rz(__fmul_rn(v, (float)res)), res - 1u);
-                atomicAdd(A.out_wet + (size_t)cy * res + cx, amount);
-            }
-        }
+        if (i >= res * res || A.t < 0.0f) return;
+        if (D.touch[i] <= __float_as_uint(A.t)) atomicMax(A.out_wet + i, 4000000u);
     }
 }
 
-// show_wet_touch (shaders/show.wgsl:138-146): where the water body touched down by now the
-// ground is soaked. After k_key_show: a max over the drops' sums.
-__global__ void __launch_bounds__(KEY_T) k_key_touch(Dev D, ShowArgs A) {
+// show_wet_drops (shaders/show.wgsl:114-136): a landed drop spreads over up to 5 x 5 cells of
+// the cleared wet map. Runs before k_key_show, whose ground-touch range takes a max over these
+// sums; launched only when key b has spray slots.
+__global__ void __launch_bounds__(KEY_T) k_key_drops(Dev D, ShowArgs A) {
     const uint32_t i = blockIdx.x * KEY_T + threadIdx.x;
+    if (i >= A.kb[0]) return;
+    const float4 l = D.landed[i];
+    if (l.z <= 0.0f || l.w > A.t) return;
+    const float h = A.wet_half;
     const uint32_t res = A.wet_res;
-    if (i >= res * res || A.t < 0.0f) return;
-    if (D.touch[i] <= __float_as_uint(A.t)) atomicMax(A.out_wet + i, 4000000u);
+    const float cell = __fdiv_rn(__fmul_rn(2.0f, h), (float)res);
+    const float r = l.z;
+    const int k = (int)fminf(fmaxf(__fdiv_rn(__fmul_rn(3.0f, r), cell), 0.0f), 2.0f);
+    const float n = (float)((2 * k + 1) * (2 * k + 1));
+    const uint32_t amount =
+        __float2uint_rz(__fdiv_rn(__fmul_rn(__fmul_rn(__fmul_rn(__fmul_rn(4.18879f, r), r), r), 1e12f), n));
+    const float two_h = __fmul_rn(2.0f, h);
+    for (int y = -k; y <= k; y++) {
+        for (int x = -k; x <= k; x++) {
+            const float u = __fdiv_rn(__fadd_rn(__fadd_rn(l.x, __fmul_rn((float)x, cell)), h), two_h);
+            const float v = __fdiv_rn(__fadd_rn(__fadd_rn(l.y, __fmul_rn((float)y, cell)), h), two_h);
+            if (u < 0.0f || v < 0.0f || u >= 1.0f || v >= 1.0f) continue;
+            // u, v < 1 keep the cell inside the map for a power-of-two resolution (the
+            // reference's 1024); the min guards any other.
+            const uint32_t cx = min(__float2uint_rz(__fmul_rn(u, (float)res)), res - 1u);
+            const uint32_t cy = min(__float2uint_rz(__fmul_rn(v, (float)res)), res - 1u);
+            atomicAdd(A.out_wet + (size_t)cy * res + cx, amount);
+        }
+    }
 }
 
 // ---- host: sizes and the keyframe schedule (src/cache.rs:22-46, 249-264, 410-421) ---------------
@@ -414,6 +432,11 @@ struct Cache {
     double shown = std::numeric_limits<double>::quiet_NaN();
     uint64_t shown_id = 0;
     uint32_t shown_spray = 0;
+    // Device time of the last store (the index launches, then the pack launch: the host's read
+    // of the counts between them is not counted) and of the last show, from events on the
+    // simulation's stream.
+    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    bool stored = false, showed = false;
 
     void free_shown() {
         for (void* p : {(void*)shown_p, (void*)shown_drops, (void*)shown_mem, (void*)shown_alive, (void*)shown_wet,
@@ -425,6 +448,8 @@ struct Cache {
     }
     ~Cache() {
         cudaSetDevice(device);
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
         free_shown();
         if (pool) cudaFree(pool);
         if (h_counts) cudaFreeHost(h_counts);
@@ -472,11 +497,15 @@ static ntr_status cache_store(Cache& C) {
     Sim& S = *C.S;
     const Dev& D = S.D;
     cudaStream_t s = S.stream;
-    const uint32_t tiles = (D.spray_cap + KEY_TILE - 1) / KEY_TILE;
-    const uint32_t g_count = std::max(1u, std::min(tiles, (uint32_t)S.sms * 8u));
-    k_key_count<<<g_count, KEY_T, 0, s>>>(D, C.tile_tot);
-    k_key_scan<<<1, 1024, 0, s>>>(D, C.tile_tot, C.tile_pre, C.counts);
+    // The grid is sized from the host's copy of the spray count (read back with the state after
+    // every batch); the kernel strides over the device's own count, so a stale copy only changes
+    // how the work is spread.
+    const uint32_t hint = std::min(S.h_state->s.spray_count, D.spray_cap);
+    const uint32_t g_count = std::max(1u, std::min((hint + KEY_TILE - 1) / KEY_TILE, (uint32_t)S.sms * 8u));
+    CU(cudaEventRecord(C.ev[0], s));
+    k_key_index<<<g_count, KEY_T, 0, s>>>(D, C.tile_tot, C.tile_pre, C.counts);
     CU(cudaGetLastError());
+    CU(cudaEventRecord(C.ev[1], s));
     CU(cudaMemcpyAsync(C.h_counts, C.counts, 8, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     const uint32_t n = C.h_counts[0], live = C.h_counts[1];
@@ -488,13 +517,16 @@ static ntr_status cache_store(Cache& C) {
     }
     KeyRec k{S.host.h.t, C.cur_off, size, C.cur_page, n, live};
     PackRanges R{};
-    R.b_mem = (D.Np + KEY_T - 1) / KEY_T;
+    R.b_mem = (D.Np + KEY_T * KEY_PER - 1) / (KEY_T * KEY_PER);
     R.b_alive = R.b_mem + (D.Nv + KEY_T - 1) / KEY_T;
     R.b_spray = R.b_alive + (bit_words(D.Nt) + KEY_T / 32 - 1) / (KEY_T / 32);
     R.b_end = R.b_spray + (n + KEY_TILE - 1) / KEY_TILE;
     R.n = n, R.live = live;
+    CU(cudaEventRecord(C.ev[2], s));
     k_key_pack<<<std::max(R.b_end, 1u), KEY_T, 0, s>>>(D, C.key_ptr(k), C.spray_w, C.tile_pre, R);
     CU(cudaGetLastError());
+    CU(cudaEventRecord(C.ev[3], s));
+    C.stored = true;
     C.cur_off += size;
     C.keys.push_back(k);
     if (C.next_t >= C.P.t_end) {
@@ -569,17 +601,20 @@ static ntr_status cache_show(Cache& C, double t, int* changed) {
     A.out_p = C.shown_p, A.out_spray = C.shown_drops, A.out_mem = C.shown_mem, A.out_alive = C.shown_alive, A.out_wet = C.shown_wet;
     A.t = (float)t, A.f = (float)f, A.inv = (float)inv, A.ta = (float)ka.t, A.tb = (float)kb.t;
     A.wet_half = S.U.wet[0], A.wet_res = D.wet_res;
-    A.b_mem = (D.Np + KEY_T - 1) / KEY_T;
+    const size_t cells = (size_t)D.wet_res * D.wet_res;
+    A.b_mem = (D.Np + KEY_T * KEY_PER - 1) / (KEY_T * KEY_PER);
     A.b_alive = A.b_mem + (D.Nv + KEY_T - 1) / KEY_T;
     A.b_spray = A.b_alive + (D.Nt + KEY_T - 1) / KEY_T;
     A.b_drops = A.b_spray + (spray + KEY_T - 1) / KEY_T;
-    A.b_end = A.b_drops + (kb.spray + KEY_T - 1) / KEY_T;
+    A.b_end = A.b_drops + (uint32_t)((cells + KEY_T - 1) / KEY_T);
     cudaStream_t s = S.stream;
-    const size_t cells = (size_t)D.wet_res * D.wet_res;
+    CU(cudaEventRecord(C.ev[4], s));
     CU(cudaMemsetAsync(C.shown_wet, 0, cells * 4, s));
+    if (kb.spray > 0) k_key_drops<<<(kb.spray + KEY_T - 1) / KEY_T, KEY_T, 0, s>>>(D, A);
     k_key_show<<<std::max(A.b_end, 1u), KEY_T, 0, s>>>(D, A);
-    k_key_touch<<<(uint32_t)((cells + KEY_T - 1) / KEY_T), KEY_T, 0, s>>>(D, A);
     CU(cudaGetLastError());
+    CU(cudaEventRecord(C.ev[5], s));
+    C.showed = true;
     C.shown = t;
     C.shown_id++;
     C.shown_spray = spray;

@@ -1324,6 +1324,7 @@ NTR_API ntr_status ntr_cache_create(ntr_sim* sim, const ntr_cache_params* cp, nt
         return fail(NTR_E_NOMEM, "device allocation of the keyframe pool (" + std::to_string(c->pool_bytes) + " bytes) failed");
     }
     CU(cudaMallocHost(&c->h_counts, 16));
+    for (cudaEvent_t& e : c->ev) CU(cudaEventCreate(&e));
     if ((r = cache_size_for(*c, S)) != NTR_OK) return r;
     if ((r = cache_restart(*c)) != NTR_OK) return r;
     *out = new ntr_cache{c.release()};
@@ -1370,6 +1371,24 @@ NTR_API ntr_status ntr_cache_info_get(ntr_cache* cache, ntr_cache_info* out) {
     out->keys = (uint32_t)C.keys.size(), out->done = C.done, out->full = C.full, out->shown_spray = C.shown_spray;
     out->used_bytes = C.used(), out->pool_bytes = C.pool_bytes, out->shown_id = C.shown_id;
     out->end = C.end(), out->next_t = C.next_t, out->shown = C.shown;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_cache_last_times(ntr_cache* cache, double* index_ms, double* pack_ms, double* show_ms) {
+    CGUARD(cache);
+    float a = 0.f, b = 0.f, c = 0.f;
+    if (C.stored) {
+        CU(cudaEventSynchronize(C.ev[3]));
+        CU(cudaEventElapsedTime(&a, C.ev[0], C.ev[1]));
+        CU(cudaEventElapsedTime(&b, C.ev[2], C.ev[3]));
+    }
+    if (C.showed) {
+        CU(cudaEventSynchronize(C.ev[5]));
+        CU(cudaEventElapsedTime(&c, C.ev[4], C.ev[5]));
+    }
+    if (index_ms) *index_ms = a;
+    if (pack_ms) *pack_ms = b;
+    if (show_ms) *show_ms = c;
     return NTR_OK;
 }
 
