@@ -1,11 +1,13 @@
 """Per-kernel device time of the simulation step, the reference's NATRAY_PROF
 (src/sim.rs:594-614, 670-689) as a command:
 
-    python -m natray_b200.prof [--resolution 124] [--warmup 3] [--steps 5] [--graph-steps 10]
+    python -m natray_b200.prof [--resolution 124] [--warmup 3] [--steps 5] [--graph-steps 10] [--keyframes 0]
 
 Builds the 1M-particle scene of the benchmark (or another resolution), runs warm-up batches,
 times `--graph-steps` steps through the step's CUDA graph, then runs `--steps` steps kernel by
-kernel with events between them and prints each kernel's share.
+kernel with events between them and prints each kernel's share. With `--keyframes N` it then
+stores N keyframes (the reference's Cache, src/cache.rs) 4 us of simulated time apart and shows
+the midpoint of each pair, printing their device times.
 """
 from __future__ import annotations
 
@@ -23,6 +25,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--graph-steps", type=int, default=10)
     ap.add_argument("--speed", type=float, default=350.0)
+    ap.add_argument("--keyframes", type=int, default=0)
     args = ap.parse_args()
     w = build_world(Params(resolution=args.resolution, mesh_level=args.mesh_level, dt_max=2e-6, bullet=6, caliber=8,
                            bullet_speed=args.speed))
@@ -39,6 +42,21 @@ def main():
         print(f"kernel by kernel: {tot / args.steps:.3f} ms/step")
         for k, (c, t) in sorted(p.items(), key=lambda kv: -kv[1][1]):
             print(f"  {k:24s} {c:5d} launches {t / args.steps * 1e3:9.1f} us/step {100 * t / tot:5.1f}%")
+    if args.keyframes:
+        from .cache import Cache
+        c = Cache(s)
+        for _ in range(args.keyframes):
+            s.advance(s._info().t + 4e-6, 16)
+            c.store()
+            i_ms, p_ms, _ = c.last_times()
+            k = c.keys()[-1]
+            print(f"keyframe at {k['t'] * 1e3:.4f} ms: {k['bytes']} B, {k['spray']} spray slots ({k['live']} live); "
+                  f"index {i_ms * 1e3:.1f} us, pack {p_ms * 1e3:.1f} us")
+        keys = c.keys()
+        for a, b in zip(keys[1:], keys[2:]):
+            c.show(0.5 * (a["t"] + b["t"]))
+            print(f"show at {0.5 * (a['t'] + b['t']) * 1e3:.4f} ms: {c.last_times()[2] * 1e3:.1f} us")
+        c.close()
 
 
 if __name__ == "__main__":
