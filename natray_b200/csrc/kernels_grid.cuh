@@ -370,13 +370,19 @@ __global__ void k_block_bounds(Dev D) {
 // fixed-point sums in shared memory, which then goes out to the grid with one atomic add per
 // nonzero tile entry. Fixed-point sums do not depend on the order of the adds.
 constexpr int P2G_T = 256;
+// The P2G tile in shared memory: 7 x 7 x 7 nodes per field with strides (68, 8, 1) and 476
+// words per field instead of (49, 7, 1) and 343. The 32 lanes of an atomic are 32 particles in
+// 32 cells of one half of the block (the layered order below): with these strides their nodes
+// at any one stencil offset fall in 32 different banks (x strides 0, 4, 8, 12 mod 32, y 0, 8,
+// 16, 24, z 0-3), where the packed strides put pairs of them in one bank.
+constexpr uint32_t TPX = 68, TPY = 8, TPF = 7 * TPX;
 
 __device__ __forceinline__ void splat(int32_t* tile, V3 x, V3 o, I3 corner, uint32_t fa, float val, V3 grad, uint32_t fw, float scale, float hh) {
     I3 base = vi(vfloor(x - o - 0.5f));
     V3 fx = x - o - vf(base);
     V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
     I3 t = base - corner;
-    uint32_t t0 = (uint32_t)t.x * 49u + (uint32_t)t.y * 7u + (uint32_t)t.z;
+    uint32_t t0 = (uint32_t)t.x * TPX + (uint32_t)t.y * TPY + (uint32_t)t.z;
     V3 hg = grad * hh;
     // The weights are products of three B-spline factors in [0, 0.75], and a node's value is at
     // most |val| + 1.5 |hg|_1 in size (every node - fx is within 1.5 per axis). When that bound
@@ -391,10 +397,10 @@ __device__ __forceinline__ void splat(int32_t* tile, V3 x, V3 o, I3 corner, uint
 #pragma unroll
                 for (uint32_t c = 0; c < 3; c++) {
                     float weight = wx[a] * wy[b] * wz[c];
-                    uint32_t tt = t0 + a * 49u + b * 7u + c;
+                    uint32_t tt = t0 + a * TPX + b * TPY + c;
                     float node = val + dot(hg, v3((float)a, (float)b, (float)c) - fx);
-                    atomicAdd(&tile[fa * TILE + tt], fp_round(__fmul_rn(weight * node, scale)));
-                    atomicAdd(&tile[fw * TILE + tt], fp_round_pos(__fmul_rn(weight, FP_W)));
+                    atomicAdd(&tile[fa * TPF + tt], fp_round(__fmul_rn(weight * node, scale)));
+                    atomicAdd(&tile[fw * TPF + tt], fp_round_pos(__fmul_rn(weight, FP_W)));
                 }
     } else {
 #pragma unroll 1
@@ -402,10 +408,10 @@ __device__ __forceinline__ void splat(int32_t* tile, V3 x, V3 o, I3 corner, uint
             for (uint32_t b = 0; b < 3; b++)
                 for (uint32_t c = 0; c < 3; c++) {
                     float weight = wx[a] * wy[b] * wz[c];
-                    uint32_t tt = t0 + a * 49u + b * 7u + c;
+                    uint32_t tt = t0 + a * TPX + b * TPY + c;
                     float node = val + dot(hg, v3((float)a, (float)b, (float)c) - fx);
-                    atomicAdd(&tile[fa * TILE + tt], to_fp(weight * node, scale));
-                    atomicAdd(&tile[fw * TILE + tt], to_fp(weight, FP_W));
+                    atomicAdd(&tile[fa * TPF + tt], to_fp(weight * node, scale));
+                    atomicAdd(&tile[fw * TPF + tt], to_fp(weight, FP_W));
                 }
     }
 }
@@ -436,7 +442,7 @@ __global__ void __launch_bounds__(P2G_T, 3) k_p2g(Dev D) {
     const Grid g = grid_of(D, cur_of(st));
     const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
     const uint32_t lane = threadIdx.x & 31u;
-    __shared__ __align__(16) int32_t tile[8 * TILE];
+    __shared__ __align__(16) int32_t tile[8 * TPF];
     __shared__ uint32_t own[64], s_cnt[64];
     __shared__ uint32_t links[27];
     __shared__ uint32_t s_pid[P2G_CAP];
@@ -463,7 +469,7 @@ __global__ void __launch_bounds__(P2G_T, 3) k_p2g(Dev D) {
             __syncthreads();
             continue;
         }
-        for (uint32_t t = threadIdx.x; t < 8 * TILE; t += P2G_T) tile[t] = 0;
+        for (uint32_t t = threadIdx.x; t < 8 * TPF; t += P2G_T) tile[t] = 0;
         const I3 corner = bc * 4 - I3{1, 1, 1};
         for (uint32_t chunk = 0; chunk < count; chunk += P2G_CAP) {
             const uint32_t n = min(P2G_CAP, count - chunk);
@@ -526,9 +532,12 @@ __global__ void __launch_bounds__(P2G_T, 3) k_p2g(Dev D) {
             }
             __syncthreads();
         }
-        int4* dst = reinterpret_cast<int4*>(D.tiles + (size_t)b * 8 * TILE);
-        const int4* srcv = reinterpret_cast<const int4*>(tile);
-        for (uint32_t t = threadIdx.x; t < 2 * TILE; t += P2G_T) dst[t] = srcv[t];
+        // Stored in the packed layout (8 fields x 343, strides 49, 7, 1) k_p2g_gather reads.
+        int32_t* dst = D.tiles + (size_t)b * 8 * TILE;
+        for (uint32_t e = threadIdx.x; e < 8 * TILE; e += P2G_T) {
+            const uint32_t f = e / TILE, r = e - f * TILE, x = r / 49u, y = (r - x * 49u) / 7u, z = r - x * 49u - y * 7u;
+            dst[e] = tile[f * TPF + x * TPX + y * TPY + z];
+        }
         if (threadIdx.x < 64) D.acc[(size_t)A_N * D.cap_cells + b * 64u + threadIdx.x] = (int32_t)own[threadIdx.x];
         if (threadIdx.x == 0) D.tile_ok[b] = 1u;
         __syncthreads();
