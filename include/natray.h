@@ -336,6 +336,12 @@ NTR_API ntr_status ntr_sim_snapshot(ntr_sim* s, void* buf, size_t cap, size_t* l
 NTR_API ntr_status ntr_sim_restore(ntr_sim* s, const void* blob, size_t len);
 /* FP64 accumulation of the solver's inner products and residual (default on). */
 NTR_API ntr_status ntr_sim_set_precision(ntr_sim* s, int fp64_reductions);
+/* The number of steps ntr_sim_advance puts in one batch. 0 (the default) is the reference's
+ * rule: as many as fit in 4 ms of the measured step time, at most 256 (src/sim.rs:505-516).
+ * The host adapts the solver's iterations and the substeps between batches, so where batches
+ * end changes the results, and with the default that depends on the GPU's timing; a fixed
+ * count makes runs repeat bit for bit. */
+NTR_API ntr_status ntr_sim_set_batch_steps(ntr_sim* s, uint32_t n);
 /* One batch as ntr_sim_step runs it, but launched kernel by kernel outside the step's graph
  * with an event after each, and a report of device time per kernel, one text line per kernel
  * name "name,launches,total_ms" (the reference's NATRAY_PROF, src/sim.rs:594-614, 670-689).

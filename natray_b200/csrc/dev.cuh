@@ -106,6 +106,7 @@ struct Dev {
     uint32_t* block_list[2];
     uint32_t* cta_sum;
     uint32_t *pslot, *key, *key_alt, *val_alt, *key_sorted, *sorted, *hist;
+    uint32_t* hist2;  // the sort's second histogram (pass 1's, counted by pass 0's scatter)
     uint32_t *block_start, *block_nb, *block_active;
     int32_t* acc;
     float* cf;

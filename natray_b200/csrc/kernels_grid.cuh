@@ -233,36 +233,64 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_words_b(Dev D) {
 }
 
 // ---- keys: each live particle's block index ---------------------------------------------------
-__global__ void k_keys(Dev D) {
+// ---- stable LSD radix sort of (block index, particle index), 8 bits per pass ------------------
+// Pass p orders the elements stably by digit (key >> 8p) & 255, in tiles of RADIX_TILE: a
+// digit-major histogram of every tile's digits, a scan of it (each tile's offset in each
+// digit's run, and the digits' totals), then the scatter. The keys are each particle's block
+// index (NONE, a particle in no block, sorts last); pass 0's values are the particle indices.
+constexpr int RADIX_T = 256, RADIX_ITEMS = 16, RADIX_TILE = RADIX_T * RADIX_ITEMS;
+constexpr int RADIX_WARPS = RADIX_T / 32, RADIX_WARP_ITEMS = RADIX_TILE / RADIX_WARPS;
+
+// Adds one digit per lane to a tile's histogram in shared memory: the lanes holding a digit
+// agree on it (match) and the lowest of them adds their count. Digit 256: nothing.
+__device__ __forceinline__ void tile_hist_add(uint32_t* h, uint32_t d) {
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    if (d < 256u && (__ffs(peers) - 1) == (int)(threadIdx.x & 31u)) atomicAdd(&h[d], (uint32_t)__popc(peers));
+}
+
+// The sort keys and pass 0's histogram in one read of the particles' block slots: each
+// particle's block index (fluid.wgsl:109-125's claim, canonical: the slot's rank in the block
+// bitmask) and its tile's count of each low digit. Also zeroes the tile's column of pass 1's
+// histogram, which pass 0's scatter fills.
+__global__ void __launch_bounds__(RADIX_T) k_keys_hist(Dev D) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const int cur = cur_of(st);
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= D.Np) return;
-    uint32_t s = D.pslot[i];
-    D.key[i] = s == NONE ? NONE : lookup(D.mask[cur], D.prefix[cur], s, D.cap_blocks);
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    if (D.radix_passes > 1) D.hist2[threadIdx.x * D.n_tiles + blockIdx.x] = 0u;
+    __syncthreads();
+    const uint32_t base = blockIdx.x * RADIX_TILE;
+    uint32_t slot[RADIX_ITEMS];
+#pragma unroll
+    for (int r = 0; r < RADIX_ITEMS; r++) {  // every load first
+        const uint32_t i = base + r * RADIX_T + threadIdx.x;
+        slot[r] = i < D.Np ? D.pslot[i] : NONE;
+    }
+#pragma unroll 4
+    for (int r = 0; r < RADIX_ITEMS; r++) {
+        const uint32_t i = base + r * RADIX_T + threadIdx.x;
+        const uint32_t k = slot[r] == NONE ? NONE : lookup(D.mask[cur], D.prefix[cur], slot[r], D.cap_blocks);
+        if (i < D.Np) D.key[i] = k;
+        tile_hist_add(h, i < D.Np ? (k & 255u) : 256u);
+    }
+    __syncthreads();
+    D.hist[threadIdx.x * D.n_tiles + blockIdx.x] = h[threadIdx.x];
 }
 
-// ---- stable LSD radix sort of (block index, particle index), 8 bits per pass ------------------
-// Pass p reads keys (and values, except in pass 0 where the value is the position) and writes
-// them in the stable order of digit (key >> 8p) & 255. Tiles of RADIX_TILE elements.
-constexpr int RADIX_T = 256, RADIX_ITEMS = 16, RADIX_TILE = RADIX_T * RADIX_ITEMS;
-
-__global__ void __launch_bounds__(RADIX_T) k_radix_hist(Dev D, const uint32_t* keys, uint32_t shift) {
+// A pass's histogram from its input keys (the passes no earlier kernel counted).
+__global__ void __launch_bounds__(RADIX_T) k_radix_hist(Dev D, uint32_t* hist, const uint32_t* keys, uint32_t shift) {
     if (D.st->s.dt_ns == 0) return;
     __shared__ uint32_t h[256];
     h[threadIdx.x] = 0;
     __syncthreads();
-    uint32_t base = blockIdx.x * RADIX_TILE;
+    const uint32_t base = blockIdx.x * RADIX_TILE;
     for (int r = 0; r < RADIX_ITEMS; r++) {
-        uint32_t i = base + r * RADIX_T + threadIdx.x;
-        // Lanes past the end match on 256, a digit no element has, and add nothing.
-        uint32_t d = i < D.Np ? (keys[i] >> shift) & 255u : 256u;
-        uint32_t peers = __match_any_sync(0xffffffffu, d);
-        if (d < 256u && (__ffs(peers) - 1) == (int)(threadIdx.x & 31u)) atomicAdd(&h[d], (uint32_t)__popc(peers));
+        const uint32_t i = base + r * RADIX_T + threadIdx.x;
+        tile_hist_add(h, i < D.Np ? (keys[i] >> shift) & 255u : 256u);
     }
     __syncthreads();
-    D.hist[threadIdx.x * D.n_tiles + blockIdx.x] = h[threadIdx.x];
+    hist[threadIdx.x * D.n_tiles + blockIdx.x] = h[threadIdx.x];
 }
 
 // Exclusive scan of 256 values held one per thread of a 256-thread CTA; returns the thread's
@@ -289,10 +317,10 @@ __device__ __forceinline__ uint32_t cta_scan256(uint32_t v, uint32_t* total) {
 
 // The digit-major histogram (digit, then tile): CTA d scans its digit's column of tile
 // counts into offsets within the digit, and records the digit's total.
-__global__ void __launch_bounds__(256) k_radix_scan(Dev D) {
+__global__ void __launch_bounds__(256) k_radix_scan(Dev D, uint32_t* hist) {
     if (D.st->s.dt_ns == 0) return;
     const uint32_t d = blockIdx.x, nt = D.n_tiles;
-    uint32_t* col = D.hist + (size_t)d * nt;
+    uint32_t* col = hist + (size_t)d * nt;
     uint32_t carry = 0;
     for (uint32_t base = 0; base < nt; base += 256) {
         const uint32_t i = base + threadIdx.x;
@@ -305,50 +333,93 @@ __global__ void __launch_bounds__(256) k_radix_scan(Dev D) {
     if (threadIdx.x == 0) D.coltot[d] = carry;
 }
 
-__global__ void __launch_bounds__(RADIX_T) k_radix_scatter(Dev D, const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
-                                                           uint32_t* vals_out, uint32_t shift) {
+// One tile of a pass. Warp w takes the tile's elements [512 w, 512 w + 512) in 16 rounds of 32
+// and ranks each among the warp's earlier elements of its digit (a match per round and a
+// running count per digit in shared memory; no block-wide barrier in the loop). The warps'
+// offsets within each digit's run and the runs' starts give every element its place in the
+// tile's stable digit order; the tile is reordered in shared memory and written out run by
+// run, consecutive threads to consecutive addresses. With hist_next, the same write-out counts
+// the next pass's digit per destination tile (a match on (tile, digit) and one global atomic
+// per group), which spares that pass its histogram kernel; hist_next must be zero before.
+__global__ void __launch_bounds__(RADIX_T) k_radix_scatter(Dev D, const uint32_t* hist, const uint32_t* keys_in,
+                                                           const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
+                                                           uint32_t shift, uint32_t* hist_next) {
     if (D.st->s.dt_ns == 0) return;
-    __shared__ uint32_t s_base[256];
-    __shared__ uint32_t s_run[256];
-    __shared__ uint32_t s_wh[RADIX_T / 32][256];
+    __shared__ uint32_t s_wc[RADIX_WARPS][256];  // per warp and digit: the running count, then the warp's offset
+    __shared__ uint32_t s_dstart[256];           // where each digit's run starts in the tile
+    __shared__ uint32_t s_gbase[256];            // where it starts in the output
+    __shared__ uint32_t s_k[RADIX_TILE], s_v[RADIX_TILE];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    {
-        uint32_t total;
-        const uint32_t digit_base = cta_scan256(D.coltot[threadIdx.x], &total);
-        s_base[threadIdx.x] = digit_base + D.hist[threadIdx.x * D.n_tiles + blockIdx.x];
-    }
-    s_run[threadIdx.x] = 0;
     const uint32_t base = blockIdx.x * RADIX_TILE;
+    const uint32_t n_here = D.Np > base ? min((uint32_t)RADIX_TILE, D.Np - base) : 0u;
+#pragma unroll
+    for (int w = 0; w < RADIX_WARPS; w++) s_wc[w][threadIdx.x] = 0;
+    const uint32_t wbase = base + warp * RADIX_WARP_ITEMS;
+    uint32_t key[RADIX_ITEMS], val[RADIX_ITEMS], rank[RADIX_ITEMS];
+#pragma unroll
+    for (int r = 0; r < RADIX_ITEMS; r++) {  // every load first
+        const uint32_t i = wbase + r * 32 + lane;
+        const bool in = i < D.Np;
+        key[r] = in ? keys_in[i] : NONE;
+        val[r] = in ? (vals_in ? vals_in[i] : i) : 0u;
+    }
+    __syncthreads();
+    const uint32_t lower_mask = (1u << lane) - 1u;
+#pragma unroll
     for (int r = 0; r < RADIX_ITEMS; r++) {
-        for (int w = 0; w < RADIX_T / 32; w++) s_wh[w][threadIdx.x] = 0;
-        __syncthreads();
-        uint32_t i = base + r * RADIX_T + threadIdx.x;
-        bool in = i < D.Np;
-        uint32_t key = in ? keys_in[i] : NONE;
-        uint32_t val = in ? (vals_in ? vals_in[i] : i) : 0u;
-        uint32_t d = in ? ((key >> shift) & 255u) : 256u;
-        uint32_t peers = __match_any_sync(0xffffffffu, d);
-        uint32_t rank = __popc(peers & ((1u << lane) - 1u));
-        if (in && rank == 0) s_wh[warp][d] = __popc(peers);
-        __syncthreads();
-        // Per digit: exclusive offsets of the warps, after the elements of earlier rounds.
-        {
-            uint32_t dg = threadIdx.x;
-            uint32_t run = s_run[dg];
-            for (int w = 0; w < RADIX_T / 32; w++) {
-                uint32_t c = s_wh[w][dg];
-                s_wh[w][dg] = run;
-                run += c;
-            }
-            s_run[dg] = run;
+        const bool in = wbase + r * 32 + lane < D.Np;
+        const uint32_t d = in ? (key[r] >> shift) & 255u : 256u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t lower = __popc(peers & lower_mask);
+        const uint32_t cnt = in ? s_wc[warp][d] : 0u;
+        __syncwarp();
+        if (in && lower == 0) s_wc[warp][d] = cnt + __popc(peers);
+        __syncwarp();
+        rank[r] = cnt + lower;
+    }
+    __syncthreads();
+    {
+        const uint32_t d = threadIdx.x;
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < RADIX_WARPS; w++) {
+            const uint32_t c = s_wc[w][d];
+            s_wc[w][d] = run;
+            run += c;
         }
-        __syncthreads();
+        uint32_t total;
+        s_dstart[d] = cta_scan256(run, &total);
+        const uint32_t digit_base = cta_scan256(D.coltot[d], &total);
+        s_gbase[d] = digit_base + hist[d * D.n_tiles + blockIdx.x];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < RADIX_ITEMS; r++) {
+        if (wbase + r * 32 + lane >= D.Np) continue;
+        const uint32_t d = (key[r] >> shift) & 255u;
+        const uint32_t p = s_dstart[d] + s_wc[warp][d] + rank[r];
+        s_k[p] = key[r];
+        s_v[p] = val[r];
+    }
+    __syncthreads();
+    for (uint32_t j0 = 0; j0 < n_here; j0 += RADIX_T) {
+        const uint32_t j = j0 + threadIdx.x;
+        const bool in = j < n_here;
+        uint32_t k = 0u, g = 0u;
         if (in) {
-            uint32_t pos = s_base[d] + s_wh[warp][d] + rank;
-            keys_out[pos] = key;
-            vals_out[pos] = val;
+            k = s_k[j];
+            const uint32_t d = (k >> shift) & 255u;
+            g = s_gbase[d] + (j - s_dstart[d]);
+            keys_out[g] = k;
+            vals_out[g] = s_v[j];
         }
-        __syncthreads();
+        if (hist_next) {
+            const uint32_t dn = (k >> (shift + 8u)) & 255u;
+            const uint32_t combo = in ? ((g / (uint32_t)RADIX_TILE) << 8) | dn : 0xFFFFFFFFu;
+            const uint32_t peers = __match_any_sync(0xffffffffu, combo);
+            if (in && (__ffs(peers) - 1) == (int)lane)
+                atomicAdd(hist_next + dn * D.n_tiles + (g / (uint32_t)RADIX_TILE), (uint32_t)__popc(peers));
+        }
     }
 }
 

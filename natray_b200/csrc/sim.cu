@@ -69,6 +69,7 @@ struct Sim {
     uint64_t last_launches = 0;
     double last_ms = 0.0;
     double step_ms = 0.0;
+    uint32_t batch_steps = 0;  // ntr_sim_set_batch_steps: fixed steps per ntr_sim_advance batch (0: by time)
     uint32_t fp64 = 1;
     ntr_tuning tune{0u, 8u, 8u, 0u};  // launch shapes (ntr_sim_set_tuning)
 
@@ -187,6 +188,7 @@ static ntr_status allocate(Sim& S) {
     AL(D.key_sorted, D.Np);
     AL(D.sorted, D.Np);
     AL(D.hist, 256u * D.n_tiles);
+    AL(D.hist2, 256u * D.n_tiles);
     AL(D.block_start, D.cap_blocks + 1);
     AL(D.block_nb, (size_t)D.cap_blocks * 27);
     AL(D.block_active, D.cap_blocks);
@@ -460,7 +462,9 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     }
     LA(k_mem_splat, g_vert, 256, D);
     LA(k_air_carry, G_cell, 256, D);
-    L(k_keys, g_part, 256, D);
+    // The sort: the keys with pass 0's histogram, then per pass the scan and the scatter; pass
+    // 0's scatter counts pass 1's histogram, later passes (more than 65,535 blocks) count their own.
+    L(k_keys_hist, D.n_tiles, RADIX_T, D);
     {
         const uint32_t P = D.radix_passes;
         const uint32_t* kin = D.key;
@@ -469,9 +473,10 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
             bool to_final = ((P - 1 - p) % 2) == 0;
             uint32_t* kout = to_final ? D.key_sorted : D.key_alt;
             uint32_t* vout = to_final ? D.sorted : D.val_alt;
-            L(k_radix_hist, D.n_tiles, RADIX_T, D, kin, 8u * p);
-            L(k_radix_scan, 256, 256, D);
-            L(k_radix_scatter, D.n_tiles, RADIX_T, D, kin, vin, kout, vout, 8u * p);
+            uint32_t* h = (p % 2 == 0) ? D.hist : D.hist2;
+            if (p >= 2) L(k_radix_hist, D.n_tiles, RADIX_T, D, h, kin, 8u * p);
+            L(k_radix_scan, 256, 256, D, h);
+            L(k_radix_scatter, D.n_tiles, RADIX_T, D, h, kin, vin, kout, vout, 8u * p, (p == 0 && P > 1) ? D.hist2 : nullptr);
             kin = kout;
             vin = vout;
         }
@@ -805,6 +810,7 @@ NTR_API ntr_status ntr_sim_advance(ntr_sim* sim, double t_target, uint32_t budge
         uint32_t dt = s.free_dt_ns > 0 ? s.free_dt_ns : (uint32_t)(S.U.fluid[2] * 1e9f);
         if (dt == 0) dt = 1;
         size_t fit = S.step_ms > 0.0 ? (size_t)(4.0 / S.step_ms) : 1;
+        if (S.batch_steps) fit = S.batch_steps;
         size_t want = (size_t)((stop - s.t_ns + dt - 1) / dt);
         size_t cap = std::min<size_t>(budget - taken, 256);
         cap = std::min(cap, std::max<size_t>(fit, 1));
@@ -961,6 +967,12 @@ NTR_API ntr_status ntr_sim_profile(ntr_sim* sim, uint32_t n, uint32_t stop_ns, c
         if (cap < out.size() + 1) return fail(NTR_E_INVALID, "report buffer too small");
         std::memcpy(report, out.c_str(), out.size() + 1);
     }
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_sim_set_batch_steps(ntr_sim* sim, uint32_t n) {
+    GUARD(sim);
+    S.batch_steps = n;
     return NTR_OK;
 }
 
@@ -1157,9 +1169,9 @@ extern "C" NTR_API ntr_status ntr_sort_by_block_noalloc(const uint32_t* keys, ui
         const bool to_final = ((P - 1 - p) % 2) == 0;
         uint32_t* kout = to_final ? D.key_sorted : D.key_alt;
         uint32_t* vout = to_final ? D.sorted : D.val_alt;
-        k_radix_hist<<<D.n_tiles, RADIX_T, 0, s>>>(D, kin, 8u * p);
-        k_radix_scan<<<256, 256, 0, s>>>(D);
-        k_radix_scatter<<<D.n_tiles, RADIX_T, 0, s>>>(D, kin, vin, kout, vout, 8u * p);
+        k_radix_hist<<<D.n_tiles, RADIX_T, 0, s>>>(D, D.hist, kin, 8u * p);
+        k_radix_scan<<<256, 256, 0, s>>>(D, D.hist);
+        k_radix_scatter<<<D.n_tiles, RADIX_T, 0, s>>>(D, D.hist, kin, vin, kout, vout, 8u * p, nullptr);
         kin = kout;
         vin = vout;
     }

@@ -56,6 +56,11 @@ class Sim:
         check(lib().ntr_sim_step(self._h, n, stop_ns, C.byref(taken)))
         return taken.value
 
+    def set_batch_steps(self, n: int) -> None:
+        """Steps per batch of `advance` (0: the reference's 4 ms rule, which depends on the GPU's
+        timing; a fixed count makes runs repeat bit for bit)."""
+        check(lib().ntr_sim_set_batch_steps(self._h, n))
+
     def advance(self, t_target: float, budget: int) -> int:
         """Runs to `t_target` (s, the reference's timeline) in at most `budget` steps."""
         taken = C.c_uint32()
