@@ -239,7 +239,33 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_words_b(Dev D) {
 // digit's run, and the digits' totals), then the scatter. The keys are each particle's block
 // index (NONE, a particle in no block, sorts last); pass 0's values are the particle indices.
 constexpr int RADIX_T = 256, RADIX_ITEMS = 16, RADIX_TILE = RADIX_T * RADIX_ITEMS;
-constexpr int RADIX_WARPS = RADIX_T / 32, RADIX_WARP_ITEMS = RADIX_TILE / RADIX_WARPS;
+// Threads per tile of the keys-and-histogram kernel and of the scatter (more threads than the
+// histogram's 256 keep more of a tile's loads in flight).
+constexpr int KEYS_T = 1024, KEYS_ITEMS = RADIX_TILE / KEYS_T;
+constexpr int SCAT_T = 512, SCAT_WARPS = SCAT_T / 32, SCAT_ITEMS = RADIX_TILE / SCAT_T, SCAT_WARP_ITEMS = RADIX_TILE / SCAT_WARPS;
+
+// Exclusive scan over the first 256 threads of a CTA of NT >= 256 (every thread calls it; the
+// others pass 0). Returns the thread's exclusive prefix and sets *total.
+template <int NT>
+__device__ __forceinline__ uint32_t cta_scan_first256(uint32_t v, uint32_t* total) {
+    __shared__ uint32_t ws[NT / 32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= (uint32_t)o) inc += y;
+    }
+    if (lane == 31) ws[warp] = inc;
+    __syncthreads();
+    uint32_t before = 0, all = 0;
+    for (uint32_t w = 0; w < 8; w++) {
+        if (w < warp) before += ws[w];
+        all += ws[w];
+    }
+    __syncthreads();
+    *total = all;
+    return before + inc - v;
+}
 
 // Adds one digit per lane to a tile's histogram in shared memory: the lanes holding a digit
 // agree on it (match) and the lowest of them adds their count. Digit 256: nothing.
@@ -252,30 +278,35 @@ __device__ __forceinline__ void tile_hist_add(uint32_t* h, uint32_t d) {
 // particle's block index (fluid.wgsl:109-125's claim, canonical: the slot's rank in the block
 // bitmask) and its tile's count of each low digit. Also zeroes the tile's column of pass 1's
 // histogram, which pass 0's scatter fills.
-__global__ void __launch_bounds__(RADIX_T) k_keys_hist(Dev D) {
+__global__ void __launch_bounds__(KEYS_T) k_keys_hist(Dev D) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const int cur = cur_of(st);
     __shared__ uint32_t h[256];
-    h[threadIdx.x] = 0;
-    if (D.radix_passes > 1) D.hist2[threadIdx.x * D.n_tiles + blockIdx.x] = 0u;
+    if (threadIdx.x < 256) {
+        h[threadIdx.x] = 0;
+        if (D.radix_passes > 1) D.hist2[threadIdx.x * D.n_tiles + blockIdx.x] = 0u;
+    }
     __syncthreads();
     const uint32_t base = blockIdx.x * RADIX_TILE;
-    uint32_t slot[RADIX_ITEMS];
+    uint32_t slot[KEYS_ITEMS];
 #pragma unroll
-    for (int r = 0; r < RADIX_ITEMS; r++) {  // every load first
-        const uint32_t i = base + r * RADIX_T + threadIdx.x;
+    for (int r = 0; r < KEYS_ITEMS; r++) {  // every load first
+        const uint32_t i = base + r * KEYS_T + threadIdx.x;
         slot[r] = i < D.Np ? D.pslot[i] : NONE;
     }
-#pragma unroll 4
-    for (int r = 0; r < RADIX_ITEMS; r++) {
-        const uint32_t i = base + r * RADIX_T + threadIdx.x;
-        const uint32_t k = slot[r] == NONE ? NONE : lookup(D.mask[cur], D.prefix[cur], slot[r], D.cap_blocks);
-        if (i < D.Np) D.key[i] = k;
-        tile_hist_add(h, i < D.Np ? (k & 255u) : 256u);
+    uint32_t key[KEYS_ITEMS];
+#pragma unroll
+    for (int r = 0; r < KEYS_ITEMS; r++)
+        key[r] = slot[r] == NONE ? NONE : lookup(D.mask[cur], D.prefix[cur], slot[r], D.cap_blocks);
+#pragma unroll
+    for (int r = 0; r < KEYS_ITEMS; r++) {
+        const uint32_t i = base + r * KEYS_T + threadIdx.x;
+        if (i < D.Np) D.key[i] = key[r];
+        tile_hist_add(h, i < D.Np ? (key[r] & 255u) : 256u);
     }
     __syncthreads();
-    D.hist[threadIdx.x * D.n_tiles + blockIdx.x] = h[threadIdx.x];
+    if (threadIdx.x < 256) D.hist[threadIdx.x * D.n_tiles + blockIdx.x] = h[threadIdx.x];
 }
 
 // A pass's histogram from its input keys (the passes no earlier kernel counted).
@@ -341,23 +372,22 @@ __global__ void __launch_bounds__(256) k_radix_scan(Dev D, uint32_t* hist) {
 // run, consecutive threads to consecutive addresses. With hist_next, the same write-out counts
 // the next pass's digit per destination tile (a match on (tile, digit) and one global atomic
 // per group), which spares that pass its histogram kernel; hist_next must be zero before.
-__global__ void __launch_bounds__(RADIX_T) k_radix_scatter(Dev D, const uint32_t* hist, const uint32_t* keys_in,
-                                                           const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
-                                                           uint32_t shift, uint32_t* hist_next) {
+__global__ void __launch_bounds__(SCAT_T) k_radix_scatter(Dev D, const uint32_t* hist, const uint32_t* keys_in,
+                                                          const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
+                                                          uint32_t shift, uint32_t* hist_next) {
     if (D.st->s.dt_ns == 0) return;
-    __shared__ uint32_t s_wc[RADIX_WARPS][256];  // per warp and digit: the running count, then the warp's offset
-    __shared__ uint32_t s_dstart[256];           // where each digit's run starts in the tile
-    __shared__ uint32_t s_gbase[256];            // where it starts in the output
+    __shared__ uint16_t s_wc[SCAT_WARPS][256];  // per warp and digit: the running count, then the warp's offset
+    __shared__ uint32_t s_dstart[256];          // where each digit's run starts in the tile
+    __shared__ uint32_t s_gbase[256];           // where it starts in the output
     __shared__ uint32_t s_k[RADIX_TILE], s_v[RADIX_TILE];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t base = blockIdx.x * RADIX_TILE;
     const uint32_t n_here = D.Np > base ? min((uint32_t)RADIX_TILE, D.Np - base) : 0u;
+    for (uint32_t e = threadIdx.x; e < SCAT_WARPS * 256; e += SCAT_T) (&s_wc[0][0])[e] = 0;
+    const uint32_t wbase = base + warp * SCAT_WARP_ITEMS;
+    uint32_t key[SCAT_ITEMS], val[SCAT_ITEMS], rank[SCAT_ITEMS];
 #pragma unroll
-    for (int w = 0; w < RADIX_WARPS; w++) s_wc[w][threadIdx.x] = 0;
-    const uint32_t wbase = base + warp * RADIX_WARP_ITEMS;
-    uint32_t key[RADIX_ITEMS], val[RADIX_ITEMS], rank[RADIX_ITEMS];
-#pragma unroll
-    for (int r = 0; r < RADIX_ITEMS; r++) {  // every load first
+    for (int r = 0; r < SCAT_ITEMS; r++) {  // every load first
         const uint32_t i = wbase + r * 32 + lane;
         const bool in = i < D.Np;
         key[r] = in ? keys_in[i] : NONE;
@@ -366,35 +396,39 @@ __global__ void __launch_bounds__(RADIX_T) k_radix_scatter(Dev D, const uint32_t
     __syncthreads();
     const uint32_t lower_mask = (1u << lane) - 1u;
 #pragma unroll
-    for (int r = 0; r < RADIX_ITEMS; r++) {
+    for (int r = 0; r < SCAT_ITEMS; r++) {
         const bool in = wbase + r * 32 + lane < D.Np;
         const uint32_t d = in ? (key[r] >> shift) & 255u : 256u;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         const uint32_t lower = __popc(peers & lower_mask);
         const uint32_t cnt = in ? s_wc[warp][d] : 0u;
         __syncwarp();
-        if (in && lower == 0) s_wc[warp][d] = cnt + __popc(peers);
+        if (in && lower == 0) s_wc[warp][d] = (uint16_t)(cnt + __popc(peers));
         __syncwarp();
         rank[r] = cnt + lower;
     }
     __syncthreads();
-    {
+    uint32_t run = 0, cold = 0;
+    if (threadIdx.x < 256) {
         const uint32_t d = threadIdx.x;
-        uint32_t run = 0;
 #pragma unroll
-        for (int w = 0; w < RADIX_WARPS; w++) {
+        for (int w = 0; w < SCAT_WARPS; w++) {
             const uint32_t c = s_wc[w][d];
-            s_wc[w][d] = run;
+            s_wc[w][d] = (uint16_t)run;
             run += c;
         }
-        uint32_t total;
-        s_dstart[d] = cta_scan256(run, &total);
-        const uint32_t digit_base = cta_scan256(D.coltot[d], &total);
-        s_gbase[d] = digit_base + hist[d * D.n_tiles + blockIdx.x];
+        cold = D.coltot[d];
+    }
+    uint32_t total;
+    const uint32_t dstart = cta_scan_first256<SCAT_T>(run, &total);
+    const uint32_t digit_base = cta_scan_first256<SCAT_T>(cold, &total);
+    if (threadIdx.x < 256) {
+        s_dstart[threadIdx.x] = dstart;
+        s_gbase[threadIdx.x] = digit_base + hist[threadIdx.x * D.n_tiles + blockIdx.x];
     }
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < RADIX_ITEMS; r++) {
+    for (int r = 0; r < SCAT_ITEMS; r++) {
         if (wbase + r * 32 + lane >= D.Np) continue;
         const uint32_t d = (key[r] >> shift) & 255u;
         const uint32_t p = s_dstart[d] + s_wc[warp][d] + rank[r];
@@ -402,7 +436,7 @@ __global__ void __launch_bounds__(RADIX_T) k_radix_scatter(Dev D, const uint32_t
         s_v[p] = val[r];
     }
     __syncthreads();
-    for (uint32_t j0 = 0; j0 < n_here; j0 += RADIX_T) {
+    for (uint32_t j0 = 0; j0 < n_here; j0 += SCAT_T) {
         const uint32_t j = j0 + threadIdx.x;
         const bool in = j < n_here;
         uint32_t k = 0u, g = 0u;

@@ -464,7 +464,7 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     LA(k_air_carry, G_cell, 256, D);
     // The sort: the keys with pass 0's histogram, then per pass the scan and the scatter; pass
     // 0's scatter counts pass 1's histogram, later passes (more than 65,535 blocks) count their own.
-    L(k_keys_hist, D.n_tiles, RADIX_T, D);
+    L(k_keys_hist, D.n_tiles, KEYS_T, D);
     {
         const uint32_t P = D.radix_passes;
         const uint32_t* kin = D.key;
@@ -476,7 +476,7 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
             uint32_t* h = (p % 2 == 0) ? D.hist : D.hist2;
             if (p >= 2) L(k_radix_hist, D.n_tiles, RADIX_T, D, h, kin, 8u * p);
             L(k_radix_scan, 256, 256, D, h);
-            L(k_radix_scatter, D.n_tiles, RADIX_T, D, h, kin, vin, kout, vout, 8u * p, (p == 0 && P > 1) ? D.hist2 : nullptr);
+            L(k_radix_scatter, D.n_tiles, SCAT_T, D, h, kin, vin, kout, vout, 8u * p, (p == 0 && P > 1) ? D.hist2 : nullptr);
             kin = kout;
             vin = vout;
         }
@@ -1171,7 +1171,7 @@ extern "C" NTR_API ntr_status ntr_sort_by_block_noalloc(const uint32_t* keys, ui
         uint32_t* vout = to_final ? D.sorted : D.val_alt;
         k_radix_hist<<<D.n_tiles, RADIX_T, 0, s>>>(D, D.hist, kin, 8u * p);
         k_radix_scan<<<256, 256, 0, s>>>(D, D.hist);
-        k_radix_scatter<<<D.n_tiles, RADIX_T, 0, s>>>(D, D.hist, kin, vin, kout, vout, 8u * p, nullptr);
+        k_radix_scatter<<<D.n_tiles, SCAT_T, 0, s>>>(D, D.hist, kin, vin, kout, vout, 8u * p, nullptr);
         kin = kout;
         vin = vout;
     }
