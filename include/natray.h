@@ -313,6 +313,24 @@ NTR_API ntr_status ntr_inflate(double shear_modulus, double thickness, double re
  * released with ntr_free(). */
 NTR_API ntr_status ntr_world_build(const ntr_sim_params* p, void** blob, size_t* len);
 
+/* A shot's flight through still air to the balloon (Flight::new, src/flight.rs:404-471): the
+ * launch from the muzzle that puts the tip on the target at the shot's speed, the state at
+ * which the simulation takes the bullet over (LOOKAHEAD = 5 cm short of the balloon), and the
+ * report at impact. */
+typedef struct ntr_flight {
+    double x[3], u[3], n[3], h[3]; /* hand-over: centre of mass (m), velocity (m/s), nose axis, angular momentum */
+    double roll;
+    double t_read;         /* when the simulation takes over (s, reference timeline: 0 = first arrival) */
+    double t_hit;          /* when the tip reaches the balloon */
+    double v_impact;       /* speed there (m/s) */
+    double sg_air;         /* gyroscopic stability there (infinite for a ball) */
+    double yaw_impact_deg; /* angle between the axis and the velocity there */
+    double twist;          /* rifling turns per metre */
+    double muzzle_x[3], muzzle_u[3]; /* the launch */
+} ntr_flight;
+/* The flights of the scene's shots (as many as p->n_shots; the first `cap` are written). CPU only. */
+NTR_API ntr_status ntr_shot_flights(const ntr_sim_params* p, ntr_flight* out, uint32_t cap, uint32_t* n);
+
 /* --- Simulation on one GPU ---------------------------------------------------------------- */
 /* Sim::new (src/sim.rs:208). */
 NTR_API ntr_status ntr_sim_create(const ntr_sim_params* p, int device, ntr_sim** out);

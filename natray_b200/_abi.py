@@ -145,6 +145,13 @@ class CacheInfo(C.Structure):
                 ("next_t", C.c_double), ("shown", C.c_double)]
 
 
+class Flight(C.Structure):
+    _fields_ = [("x", C.c_double * 3), ("u", C.c_double * 3), ("n", C.c_double * 3), ("h", C.c_double * 3),
+                ("roll", C.c_double), ("t_read", C.c_double), ("t_hit", C.c_double), ("v_impact", C.c_double),
+                ("sg_air", C.c_double), ("yaw_impact_deg", C.c_double), ("twist", C.c_double),
+                ("muzzle_x", C.c_double * 3), ("muzzle_u", C.c_double * 3)]
+
+
 # Every entry point include/natray.h declares, with its ctypes signature.
 _P = C.c_void_p
 _SIGS = {
@@ -155,6 +162,7 @@ _SIGS = {
     "ntr_params_set": (C.c_int, [C.POINTER(SimParams), C.c_char_p, C.c_char_p]),
     "ntr_params_preset": (C.c_int, [C.POINTER(SimParams), C.c_char_p]),
     "ntr_world_build": (C.c_int, [C.POINTER(SimParams), C.POINTER(_P), C.POINTER(C.c_size_t)]),
+    "ntr_shot_flights": (C.c_int, [C.POINTER(SimParams), C.POINTER(Flight), C.c_uint32, C.POINTER(C.c_uint32)]),
     "ntr_inflate": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.POINTER(Profile)]),
     "ntr_sim_create": (C.c_int, [C.POINTER(SimParams), C.c_int, C.POINTER(_P)]),
     "ntr_sim_create_from_world": (C.c_int, [_P, C.c_size_t, C.c_int, C.POINTER(_P)]),

@@ -76,4 +76,14 @@ NTR_API ntr_status ntr_world_build(const ntr_sim_params* p, void** blob, size_t*
     return NTR_OK;
 }
 
+NTR_API ntr_status ntr_shot_flights(const ntr_sim_params* p, ntr_flight* out, uint32_t cap, uint32_t* n) {
+    if (!p || (!out && cap)) return fail(NTR_E_INVALID, "null argument");
+    std::vector<ntr_flight> v;
+    std::string err;
+    if (!flights(*p, v, err)) return fail(NTR_E_INVALID, err);
+    if (n) *n = (uint32_t)v.size();
+    for (uint32_t k = 0; k < v.size() && k < cap; k++) out[k] = v[k];
+    return NTR_OK;
+}
+
 }  // extern "C"

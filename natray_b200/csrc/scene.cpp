@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <optional>
 #include <string>
@@ -578,6 +579,8 @@ const BulletType BULLETS[7] = {
 
 double body_share(Nose n) { return n == ROUND ? 0.55 : n == SPITZER ? 0.42 : 1.0; }
 
+constexpr double RHO_AIR_FLIGHT = 1.2;  // src/flight.rs:20
+
 double profile_r(Nose nose, double r, double len, double u) {
     if (nose == SPHERE) return std::sqrt(std::max(r * r - (u - r) * (u - r), 0.0));
     double body = body_share(nose) * len;
@@ -591,10 +594,26 @@ double profile_r(Nose nose, double r, double len, double u) {
     return r * std::sqrt(std::max(1.0 - q * q, 0.0));
 }
 
+constexpr int FLIGHT_SLICES = 24;  // slices of the body in the flight's loads (src/flight.rs:21)
+
+// `Body` of src/flight.rs:78-101. Every u is along the axis from the base.
 struct Body {
     Nose nose;
     double radius, length, mass, u_cg, ix, iy;
+    double slices[FLIGHT_SLICES][3];  // centre, length and radius of each slice
+    double side_area;                 // silhouette area seen from the side
+    double u_shoulder, u_cp, u_drag;  // where the cavity leaves the nose; where its lift and drag act
+    double cd_water, cd_air, kappa_water, kappa_air;
 };
+
+// Miller's twist rule (src/flight.rs:68-76): gyroscopic stability of a bullet of mass m (kg)
+// and diameter d (m), l calibres long, one turn per t calibres, at speed v (m/s).
+double miller_sg(double m, double d, double l, double t, double v) {
+    double grains = m / 64.79891e-6;
+    double d_in = d / 0.0254;
+    double fps = v / 0.3048;
+    return 30.0 * grains / (t * t * (d_in * d_in * d_in) * l * (1.0 + l * l)) * std::cbrt(fps / 2800.0);
+}
 
 Body body_new(const ntr_shot& s) {
     Body b;
@@ -632,6 +651,37 @@ Body body_new(const ntr_shot& s) {
     b.u_cg = u_cg;
     b.ix = ix;
     b.iy = iy;
+    // The aerodynamic constants of src/flight.rs:133-169.
+    const double body = body_share(b.nose) * length;
+    double v_nose = 0.0;
+    for (auto& q : rad)
+        if (q.first > body) v_nose += PI * q.second * q.second * du;
+    b.u_cp = b.nose == SPHERE ? r : body + v_nose / (PI * r * r);
+    switch (b.nose) {
+        case SPITZER: b.u_shoulder = body, b.u_drag = b.u_cp; break;
+        case ROUND: b.u_shoulder = body, b.u_drag = length - r * r / (length - body); break;
+        case FLAT: b.u_shoulder = length, b.u_drag = length; break;
+        default: b.u_shoulder = r, b.u_drag = r; break;
+    }
+    b.cd_water = (b.nose == ROUND || b.nose == SPHERE) ? 0.30 : b.nose == SPITZER ? 0.20 : 0.82;
+    b.cd_air = (b.nose == ROUND || b.nose == SPITZER) ? 0.30 : b.nose == FLAT ? 0.9 : 0.47;
+    b.kappa_water = b.nose == SPITZER ? 1.0 : 0.0;
+    if (b.nose == SPHERE) {
+        b.kappa_air = 0.0;
+    } else {
+        // Scaled so that the stability is Miller's at the shot's speed with one turn in 30 calibres.
+        const double v = std::max((double)s.speed, 1.0), d = 2.0 * r, tw = 30.0;
+        const double p = TAU * v / (tw * d);
+        const double m_alpha = ix * ix * p * p / (4.0 * iy * miller_sg(mass, d, length / d, tw, v));
+        b.kappa_air = m_alpha / (RHO_AIR_FLIGHT * PI * r * r * v * v * (b.u_cp - u_cg));
+    }
+    for (int j = 0; j < FLIGHT_SLICES; j++) {
+        const double sdu = length / (double)FLIGHT_SLICES;
+        const double u = ((double)j + 0.5) * sdu;
+        b.slices[j][0] = u, b.slices[j][1] = sdu, b.slices[j][2] = profile_r(b.nose, r, length, u);
+    }
+    b.side_area = 0.0;
+    for (auto& q : rad) b.side_area += 2.0 * q.second * du;
     return b;
 }
 
@@ -726,27 +776,203 @@ std::array<double, 4> rotation_arc_z(V3d n) {
 
 constexpr double LOOKAHEAD = 0.05;
 
-// The hand-over from the flight through the air, straight-line form: the bullet arrives
-// along the aim with its shot speed and the muzzle spin, its tip LOOKAHEAD short of where the
-// line meets the balloon (Flight::new, src/flight.rs:408-470, without the 6-DOF air drag).
+// The hand-over from the flight through the air to the simulation (Flight::new and
+// Flight::handoff, src/flight.rs:404-471, 633-637), with the flight's report at impact.
 struct Handoff {
-    V3d x, u, n, h;
+    V3d x, u, n, h;  // where the simulation takes over: centre of mass, velocity, axis, angular momentum
     double roll;
-    double t_read;
-    double v_impact;
+    double t_read;    // when
+    double t_hit;     // when the tip reaches the balloon
+    double v_impact;  // the speed there
+    double sg_air;    // gyroscopic stability at impact (infinite for a ball)
+    double yaw_impact;  // yaw at impact, rad
+    double twist;       // rifling turns per metre
+    V3d muzzle_x, muzzle_u;  // the launch that lands on the target
 };
 
-Handoff straight_handoff(const ntr_shot& s, const Body& b, V3d target, V3d dir, double t_hit) {
+// ---- the bullet's flight through still air (src/flight.rs:264-292, 404-676) ------------------
+// Rigid body of revolution: state (x, u, n, h, roll), RK4 steps, loads of the leading end and
+// of the slices behind it. In still air the reference's water terms have no share (the empty
+// field's fill is 0), so only the air terms are restated.
+constexpr double CDC_AIR = 1.2, CD_BASE_AIR = 1.17, CF_SKIN = 0.003, CMQ_AIR = -10.0;
+
+struct FState {
+    V3d x, u, n, h;
+    double roll;
+    FState add(const FState& d, double k) const {
+        return {x + d.x * k, u + d.u * k, n + d.n * k, h + d.h * k, roll + d.roll * k};
+    }
+    FState lerp(const FState& o, double k) const {
+        FState s = add(o.add(*this, -1.0), k);
+        s.n = normalize(s.n);
+        return s;
+    }
+    double yaw() const {
+        const double l = length(u);
+        const double r = 1.0 / l;
+        const V3d uh = (std::isfinite(r) && r > 0.0) ? u * r : V3d{0.0, 0.0, 0.0};
+        return std::acos(std::clamp(dot(n, uh), -1.0, 1.0));
+    }
+};
+
+static inline V3d vdiv(V3d a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+static inline V3d normalize_or(V3d a, V3d fallback) {
+    const double r = 1.0 / std::sqrt(dot(a, a));
+    return (std::isfinite(r) && r > 0.0) ? a * r : fallback;
+}
+
+struct Flight {
+    Body b;
+    V3d gravity;
+    // Force and torque on the body in still air (src/flight.rs:486-598 with an empty field).
+    void loads(const FState& s, V3d& force, V3d& torque) const {
+        const V3d n = s.n;
+        const double p = dot(s.h, n) / b.ix;
+        const V3d w_perp = vdiv(s.h - n * dot(s.h, n), b.iy);
+        auto at = [&](double u) { return s.x + n * (u - b.u_cg); };
+        const double speed = std::max(length(s.u), 1e-6);
+        const V3d uhat = vdiv(s.u, speed);
+        const double cos_d = std::clamp(dot(n, uhat), -1.0, 1.0);
+        const bool nose_first = cos_d >= 0.0;
+        const double area = PI * b.radius * b.radius;
+        const double rho = RHO_AIR_FLIGHT;
+        force = gravity * b.mass;
+        torque = {0.0, 0.0, 0.0};
+        // The leading end.
+        const V3d lead = at(nose_first ? b.length : 0.0);
+        const V3d w = s.u + cross(w_perp, lead - s.x);
+        const double wl = length(w);
+        if (wl >= 1e-9) {
+            const double wn = dot(w, n);
+            auto axial = [&](double cd) { return n * (-0.5 * rho * cd * area * wn * std::fabs(wn)); };
+            V3d f[2] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+            double fu[2] = {0.0, 0.0};
+            int nf = 1;
+            if (!nose_first) {
+                f[0] = axial(CD_BASE_AIR), fu[0] = 0.0;
+            } else if (b.nose == FLAT) {
+                f[0] = axial(b.cd_air), fu[0] = b.length;
+            } else if (b.nose == SPHERE) {
+                f[0] = w * (-0.5 * rho * b.cd_air * area * wl), fu[0] = b.u_drag;
+            } else {
+                const double c = wn / wl;
+                f[0] = w * (-0.5 * rho * b.cd_air * area * c * c * wl), fu[0] = b.u_cg;
+                f[1] = (w - n * wn) * (-rho * area * b.kappa_air * wn), fu[1] = b.u_cp;
+                nf = 2;
+            }
+            for (int i = 0; i < nf; i++) {
+                force = force + f[i] * 1.0;
+                torque = torque + cross(at(fu[i]) - s.x, f[i]) * 1.0;
+            }
+        }
+        // The slices: cross-flow drag, Magnus lift, skin friction of the spin.
+        for (int j = 0; j < FLIGHT_SLICES; j++) {
+            const double u = b.slices[j][0], du = b.slices[j][1], r = b.slices[j][2];
+            const V3d xj = at(u);
+            const V3d wj = s.u + cross(w_perp, xj - s.x);
+            const double wa = dot(wj, n);
+            const V3d wc = wj - n * wa;
+            const double wcl = length(wc);
+            V3d f{0.0, 0.0, 0.0};
+            if (b.nose != SPHERE) f = f - wc * (0.5 * rho * CDC_AIR * 2.0 * r * du * wcl);
+            if (wcl > 1e-9 && p != 0.0) f = f + cross(n, wc) * (rho * r * r * p * du * std::min(wcl / (r * std::fabs(p)), 1.0));
+            const double spin = -0.5 * rho * CF_SKIN * (p * r) * std::fabs(p * r) * TAU * r * du * r;
+            force = force + f * 1.0;
+            torque = torque + (cross(xj - s.x, f) + n * spin) * 1.0;
+        }
+        // Pitch damping.
+        torque = torque + w_perp * (0.5 * RHO_AIR_FLIGHT * speed * area * 4.0 * b.radius * b.radius * CMQ_AIR * 1.0);
+    }
+    FState deriv(const FState& s) const {
+        V3d f, tq;
+        loads(s, f, tq);
+        const double p = dot(s.h, s.n) / b.ix;
+        const V3d w_perp = vdiv(s.h - s.n * dot(s.h, s.n), b.iy);
+        return {s.u, vdiv(f, b.mass), cross(w_perp, s.n), tq, p};
+    }
+    FState step(const FState& s, double dt) const {
+        const FState k1 = deriv(s);
+        const FState k2 = deriv(s.add(k1, 0.5 * dt));
+        const FState k3 = deriv(s.add(k2, 0.5 * dt));
+        const FState k4 = deriv(s.add(k3, dt));
+        FState o = s.add(k1, dt / 6.0).add(k2, dt / 3.0).add(k3, dt / 3.0).add(k4, dt / 6.0);
+        o.n = normalize(o.n);
+        return o;
+    }
+    // A twentieth of a radian per step at the fastest rotation (src/flight.rs:618-631), in air.
+    double dt_of(const FState& s) const {
+        const double speed = std::max(length(s.u), 1.0);
+        const double p = dot(s.h, s.n) / b.ix;
+        const double tumble = length(vdiv(s.h - s.n * dot(s.h, s.n), b.iy));
+        const double rho = RHO_AIR_FLIGHT + 0.0 * RHO_WATER;
+        const double pull = std::sqrt(rho * PI * b.radius * b.radius * speed * speed * b.length / b.iy);
+        return std::min(0.05 / (tumble + b.ix * std::fabs(p) / b.iy + pull), 0.02 / speed);
+    }
+    V3d tip(const FState& s) const { return s.x + s.n * (b.length - b.u_cg); }
+    // Flies until g turns non-negative; the state and time where it crossed zero.
+    template <class G>
+    std::pair<FState, double> fly(FState s, double t, G g) const {
+        double gv = g(s);
+        for (int it = 0; it < 2000000; it++) {
+            if (gv >= 0.0) break;
+            const double dt = dt_of(s);
+            const FState next = step(s, dt);
+            const double gn = g(next);
+            if (gn >= 0.0) {
+                const double k = -gv / (gn - gv);
+                return {s.lerp(next, k), t + dt * k};
+            }
+            s = next;
+            t += dt;
+            gv = gn;
+        }
+        return {s, t};
+    }
+};
+
+// Flight::new (src/flight.rs:404-471): aims the bullet from the muzzle, range_m up the line of
+// fire, so that its tip crosses the target's plane on the line at the shot's speed (eight
+// rounds correcting the aim for the drop and drift and the muzzle speed for the drag), then
+// flies it to LOOKAHEAD short of that plane, the simulation's start, and on to the plane.
+Handoff flight_handoff(const ntr_shot& s, const Body& b, V3d target, V3d dir, double t_hit, double gravity) {
+    Flight f{b, V3d{0.0, -gravity, 0.0}};
+    const double v_hit = std::max((double)s.speed, 1.0);
+    const double p0 = (double)s.spin_rpm / 60.0 * TAU;
+    const double yaw = (double)s.muzzle_yaw_deg * (PI / 180.0);
+    const double range = std::max((double)s.range_m, 0.5);
+    const V3d muzzle = target - dir * range;
+    auto launch = [&](V3d aim, double v) {
+        const V3d side = normalize_or(V3d{0.0, 1.0, 0.0} - aim * aim.y, V3d{0.0, 0.0, 1.0});
+        const V3d n = aim * std::cos(yaw) + side * std::sin(yaw);
+        return FState{muzzle - n * (b.length - b.u_cg), aim * v, n, n * (b.ix * p0), 0.0};
+    };
+    auto crossing = [&](const FState& st) { return dot(f.tip(st) - target, dir); };
+    V3d aim = dir;
+    double v_m = v_hit;
+    for (int it = 0; it < 8; it++) {
+        const FState st = f.fly(launch(aim, v_m), 0.0, crossing).first;
+        V3d miss = f.tip(st) - target;
+        miss = miss - dir * dot(miss, dir);
+        aim = normalize(aim - vdiv(miss, range));
+        v_m *= v_hit / length(st.u);
+        if (length(miss) < 1e-4 && std::fabs(length(st.u) - v_hit) < 0.01 * v_hit) break;
+    }
     Handoff o;
-    double v_hit = std::max((double)s.speed, 1.0);
-    double p0 = (double)s.spin_rpm / 60.0 * TAU;
-    o.n = dir;
-    o.x = target - dir * LOOKAHEAD - dir * (b.length - b.u_cg);
-    o.u = dir * v_hit;
-    o.h = dir * (b.ix * p0);
-    o.roll = 0.0;
-    o.t_read = t_hit - LOOKAHEAD / v_hit;
-    o.v_impact = v_hit;
+    o.twist = p0 / (TAU * v_m);
+    const FState start = launch(aim, v_m);
+    o.muzzle_x = start.x, o.muzzle_u = start.u;
+    const auto [hand, t_hand] = f.fly(start, 0.0, [&](const FState& st) { return crossing(st) + LOOKAHEAD; });
+    const auto [hit, t_c] = f.fly(hand, t_hand, crossing);
+    const double shift = t_hit - t_c;
+    o.x = hand.x, o.u = hand.u, o.n = hand.n, o.h = hand.h, o.roll = hand.roll;
+    o.t_read = t_hand + shift;
+    o.t_hit = t_hit;
+    const double v = length(hit.u);
+    const double p = dot(hit.h, hit.n) / b.ix;
+    const double m_alpha = b.kappa_air * RHO_AIR_FLIGHT * PI * b.radius * b.radius * v * v * (b.u_cp - b.u_cg);
+    o.sg_air = m_alpha > 0.0 ? b.ix * b.ix * p * p / (4.0 * b.iy * m_alpha) : std::numeric_limits<double>::infinity();
+    o.yaw_impact = hit.yaw();
+    o.v_impact = v;
     return o;
 }
 
@@ -1137,7 +1363,54 @@ bool deserialize(const void* blob, size_t len, World& w, std::string& err) {
     return true;
 }
 
-bool build_world(const ntr_sim_params& p, World& w, std::string& err) {
+// Each shot's body and its flight to the balloon (src/sim.rs:280-295): the line of fire from
+// the azimuth and elevation, aimed at the impact offsets; the target where that line enters the
+// balloon (a radius short of the aim when it misses); the tip's arrival the shot's delay after
+// the earliest shot's.
+static void shot_flights(const ntr_sim_params& p, const Balloon& scene, std::vector<Handoff>& hand, std::vector<Body>& bodies) {
+    float first = 3.4028235e38f;
+    for (uint32_t k = 0; k < p.n_shots; k++) first = std::min(first, p.shots[k].delay_ms);
+    const float RADS = 3.14159265358979323846f / 180.0f;
+    hand.assign(p.n_shots, Handoff{});
+    bodies.assign(p.n_shots, Body{});
+    for (uint32_t k = 0; k < p.n_shots; k++) {
+        const ntr_shot& s = p.shots[k];
+        float az = s.azimuth_deg * RADS, el = s.elevation_deg * RADS;
+        V3f dir{std::cos(az) * std::cos(el), -std::sin(el), std::sin(az) * std::cos(el)};
+        V3f side = normalize_or(cross(dir, V3f{0, 1, 0}), V3f{0, 0, 1});
+        V3f aim = (scene.center + V3f{0, 1, 0} * (s.impact_offset_cm * 0.01f)) + side * (s.impact_side_cm * 0.01f);
+        auto e = scene.entry(aim, dir);
+        V3f target = e ? *e : aim - dir * (float)scene.radius_max;
+        double t_hit = (double)(s.delay_ms - first) * 1e-3;
+        bodies[k] = body_new(s);
+        hand[k] = flight_handoff(s, bodies[k], widen(target), widen(dir), t_hit, (double)p.gravity);
+    }
+}
+
+static bool check_params(const ntr_sim_params& p, std::string& err);
+
+bool flights(const ntr_sim_params& p, std::vector<ntr_flight>& out, std::string& err) {
+    if (!check_params(p, err)) return false;
+    Balloon scene;
+    if (!build_balloon(p, scene, err)) return false;
+    std::vector<Handoff> hand;
+    std::vector<Body> bodies;
+    shot_flights(p, scene, hand, bodies);
+    out.assign(p.n_shots, ntr_flight{});
+    for (uint32_t k = 0; k < p.n_shots; k++) {
+        const Handoff& h = hand[k];
+        ntr_flight& f = out[k];
+        const V3d* v[6] = {&h.x, &h.u, &h.n, &h.h, &h.muzzle_x, &h.muzzle_u};
+        double* d[6] = {f.x, f.u, f.n, f.h, f.muzzle_x, f.muzzle_u};
+        for (int i = 0; i < 6; i++) d[i][0] = v[i]->x, d[i][1] = v[i]->y, d[i][2] = v[i]->z;
+        f.roll = h.roll, f.t_read = h.t_read, f.t_hit = h.t_hit, f.v_impact = h.v_impact, f.sg_air = h.sg_air;
+        f.yaw_impact_deg = h.yaw_impact * (180.0 / PI);
+        f.twist = h.twist;
+    }
+    return true;
+}
+
+static bool check_params(const ntr_sim_params& p, std::string& err) {
     if (p.n_shots < 1 || p.n_shots > NTR_MAX_SHOTS) {
         err = "shots 1..4";
         return false;
@@ -1152,6 +1425,11 @@ bool build_world(const ntr_sim_params& p, World& w, std::string& err) {
         err = "scene parameters out of range";
         return false;
     }
+    return true;
+}
+
+bool build_world(const ntr_sim_params& p, World& w, std::string& err) {
+    if (!check_params(p, err)) return false;
     Balloon scene;
     if (!build_balloon(p, scene, err)) return false;
 
@@ -1220,23 +1498,9 @@ bool build_world(const ntr_sim_params& p, World& w, std::string& err) {
     for (size_t i = 0; i < (size_t)WET_RES * WET_RES; i++) touch[i] = 0xffffffffu;
 
     // Shots, src/sim.rs:280-310.
-    float first = 3.4028235e38f;
-    for (uint32_t k = 0; k < p.n_shots; k++) first = std::min(first, p.shots[k].delay_ms);
-    const float RADS = 3.14159265358979323846f / 180.0f;
-    std::vector<Handoff> hand(p.n_shots);
-    std::vector<Body> bodies(p.n_shots);
-    for (uint32_t k = 0; k < p.n_shots; k++) {
-        const ntr_shot& s = p.shots[k];
-        float az = s.azimuth_deg * RADS, el = s.elevation_deg * RADS;
-        V3f dir{std::cos(az) * std::cos(el), -std::sin(el), std::sin(az) * std::cos(el)};
-        V3f side = normalize_or(cross(dir, V3f{0, 1, 0}), V3f{0, 0, 1});
-        V3f aim = (scene.center + V3f{0, 1, 0} * (s.impact_offset_cm * 0.01f)) + side * (s.impact_side_cm * 0.01f);
-        auto e = scene.entry(aim, dir);
-        V3f target = e ? *e : aim - dir * (float)scene.radius_max;
-        double t_hit = (double)(s.delay_ms - first) * 1e-3;
-        bodies[k] = body_new(s);
-        hand[k] = straight_handoff(s, bodies[k], widen(target), widen(dir), t_hit);
-    }
+    std::vector<Handoff> hand;
+    std::vector<Body> bodies;
+    shot_flights(p, scene, hand, bodies);
     double t_start = 0.0, t0 = 0.0;
     for (auto& hd : hand) {
         t_start = std::min(t_start, hd.t_read - (0.3 - LOOKAHEAD) / hd.v_impact);

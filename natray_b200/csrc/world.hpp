@@ -37,6 +37,7 @@ bool deserialize(const void* blob, size_t len, World& w, std::string& err);
 // Scene construction, src/balloon.rs:343-464 and src/sim.rs:208-441 (before the measuring
 // substep, which the creator of the simulation runs).
 bool build_world(const ntr_sim_params& p, World& w, std::string& err);
+bool flights(const ntr_sim_params& p, std::vector<ntr_flight>& out, std::string& err);
 
 // `inflate` of src/balloon.rs:170-248 with `Latex::new(shear, thick)`.
 bool inflate_profile(double shear, double thick, double rest_r, double volume, double rho_g, ntr_profile& out, std::string& err);

@@ -51,6 +51,22 @@ class Params:
         return getattr(self.c, name)
 
 
+def flights(params: Params) -> list[dict]:
+    """Each shot's flight through the air to the balloon (the reference's Flight::new): the
+    hand-over state, its time, and the speed, stability and yaw at impact. CPU only."""
+    out = (_abi.Flight * _abi.MAX_SHOTS)()
+    n = C.c_uint32()
+    check(lib().ntr_shot_flights(C.byref(params.c), out, _abi.MAX_SHOTS, C.byref(n)))
+    res = []
+    for f in out[: n.value]:
+        d = {}
+        for k, _ in f._fields_:
+            v = getattr(f, k)
+            d[k] = list(v) if not isinstance(v, float) else v
+        res.append(d)
+    return res
+
+
 def sized_for(n_particles: int, diameter_cm: float = 16.0) -> int:
     """Lattice resolution that fills a sphere of `diameter_cm` with about `n_particles`:
     N ~ pi/6 res^3 (src/balloon.rs:420 spacing = d / res)."""
