@@ -14,6 +14,7 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <mutex>
 #include <optional>
 #include <string>
 #include <utility>
@@ -205,7 +206,39 @@ std::optional<ShotResult> shoot(const Latex& latex, double rest_r, double apex_s
     return out;
 }
 
+bool inflate_solve(const Latex& latex, double rest_r, double volume, double rho_g, Profile& prof, std::string& err);
+
+// Inflation depends only on the latex, the rest radius, the volume and the water's weight, and
+// takes about a second (hundreds of shooting integrations); the reference redoes it whenever a
+// scene is rebuilt, also when only the shots or the resolution changed. Results are kept per
+// exact inputs (their bits), so a rebuild of the same balloon gets the same profile at once.
 bool inflate(const Latex& latex, double rest_r, double volume, double rho_g, Profile& prof, std::string& err) {
+    using Key = std::array<uint64_t, 7>;
+    static std::mutex mu;
+    static std::map<Key, Profile> memo;
+    auto bits = [](double d) {
+        uint64_t u;
+        std::memcpy(&u, &d, 8);
+        return u;
+    };
+    const Key k = {bits(latex.mu[0]), bits(latex.mu[1]), bits(latex.mu[2]), bits(latex.thickness), bits(rest_r), bits(volume),
+                   bits(rho_g)};
+    {
+        std::lock_guard<std::mutex> g(mu);
+        auto it = memo.find(k);
+        if (it != memo.end()) {
+            prof = it->second;
+            return true;
+        }
+    }
+    if (!inflate_solve(latex, rest_r, volume, rho_g, prof, err)) return false;
+    std::lock_guard<std::mutex> g(mu);
+    if (memo.size() >= 256) memo.erase(memo.begin());
+    memo.emplace(k, prof);
+    return true;
+}
+
+bool inflate_solve(const Latex& latex, double rest_r, double volume, double rho_g, Profile& prof, std::string& err) {
     const double neck_r = NECK * rest_r;
     auto miss = [&](std::array<double, 2> x, double target) -> std::optional<std::array<double, 2>> {
         auto s = shoot(latex, rest_r, x[0], std::exp(x[1]), rho_g);
