@@ -354,6 +354,47 @@ NTR_API ntr_status ntr_sim_snapshot(ntr_sim* s, void* buf, size_t cap, size_t* l
 NTR_API ntr_status ntr_sim_restore(ntr_sim* s, const void* blob, size_t len);
 /* FP64 accumulation of the solver's inner products and residual (default on). */
 NTR_API ntr_status ntr_sim_set_precision(ntr_sim* s, int fp64_reductions);
+/* What `Sim::debug_stats` (src/sim.rs:691-863) prints, computed on the device (ntr_sim_stats).
+ * Sums are FP64 (the reference's means are sequential FP32 sums); counts, minima and maxima are
+ * exact. The clock, block count, solver and substep figures the reference prints beside these
+ * are in ntr_state and ntr_sim_info. */
+typedef struct ntr_stats_bullet {
+    uint32_t state;    /* the bullet's phase (Bullet.info[2]) */
+    uint32_t sections; /* cavity sections recorded (Bullet.info[3]) */
+    float x[3];
+    float speed;       /* m/s */
+    float yaw_deg;     /* angle between the axis and the velocity */
+    float spin_rev_s;
+    double kinetic_j;
+} ntr_stats_bullet;
+typedef struct ntr_stats {
+    /* water: particles with vel.w > 0.5 */
+    uint32_t water, n_particles;
+    float lo[3], hi[3];
+    double mean[3], vmean[3];
+    float vmax, fastest[3];     /* the fastest particle's speed and position (the first of equals) */
+    double volume_l;            /* cells holding 4 or more particles, times their volume, litres */
+    /* rubber */
+    double inside_l;            /* volume the membrane encloses, litres */
+    float mem_lo[3], mem_hi[3];
+    uint32_t free_verts, on_water, torn, n_tension;
+    float fill_min, fill_mean, rubber_vmax, pad0;
+    double tension[3];          /* N/m, the most tense intact triangles, most tense first */
+    uint32_t tension_tri[3], pad1;
+    float stretch[3][2];        /* their principal stretches */
+    /* air of the step's cells typed air */
+    uint32_t air_cells, vapour_cells;  /* vapour: gauge below -90 kPa */
+    float gauge_lo, gauge_hi, air_umax, pad2;
+    /* energies */
+    double water_j, bullets_j, vapour_cm3, vapour_j;
+    uint32_t n_bullets, pad3;
+    ntr_stats_bullet bullets[NTR_MAX_SHOTS];
+} ntr_stats;
+/* The statistics of the simulation's current state. The first call allocates its scratch on
+ * the device (4 bytes per cell of the block capacity, and a few KB); it synchronises with the
+ * simulation's stream. */
+NTR_API ntr_status ntr_sim_stats(ntr_sim* s, ntr_stats* out);
+
 /* The number of steps ntr_sim_advance puts in one batch. 0 (the default) is the reference's
  * rule: as many as fit in 4 ms of the measured step time, at most 256 (src/sim.rs:505-516).
  * The host adapts the solver's iterations and the substeps between batches, so where batches

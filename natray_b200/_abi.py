@@ -152,6 +152,25 @@ class Flight(C.Structure):
                 ("muzzle_x", C.c_double * 3), ("muzzle_u", C.c_double * 3)]
 
 
+class StatsBullet(C.Structure):
+    _fields_ = [("state", C.c_uint32), ("sections", C.c_uint32), ("x", C.c_float * 3), ("speed", C.c_float),
+                ("yaw_deg", C.c_float), ("spin_rev_s", C.c_float), ("kinetic_j", C.c_double)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("water", C.c_uint32), ("n_particles", C.c_uint32), ("lo", C.c_float * 3), ("hi", C.c_float * 3),
+                ("mean", C.c_double * 3), ("vmean", C.c_double * 3), ("vmax", C.c_float), ("fastest", C.c_float * 3),
+                ("volume_l", C.c_double), ("inside_l", C.c_double), ("mem_lo", C.c_float * 3),
+                ("mem_hi", C.c_float * 3), ("free_verts", C.c_uint32), ("on_water", C.c_uint32), ("torn", C.c_uint32),
+                ("n_tension", C.c_uint32), ("fill_min", C.c_float), ("fill_mean", C.c_float),
+                ("rubber_vmax", C.c_float), ("pad0", C.c_float), ("tension", C.c_double * 3),
+                ("tension_tri", C.c_uint32 * 3), ("pad1", C.c_uint32), ("stretch", (C.c_float * 2) * 3),
+                ("air_cells", C.c_uint32), ("vapour_cells", C.c_uint32), ("gauge_lo", C.c_float),
+                ("gauge_hi", C.c_float), ("air_umax", C.c_float), ("pad2", C.c_float), ("water_j", C.c_double),
+                ("bullets_j", C.c_double), ("vapour_cm3", C.c_double), ("vapour_j", C.c_double),
+                ("n_bullets", C.c_uint32), ("pad3", C.c_uint32), ("bullets", StatsBullet * MAX_SHOTS)]
+
+
 # Every entry point include/natray.h declares, with its ctypes signature.
 _P = C.c_void_p
 _SIGS = {
@@ -177,6 +196,7 @@ _SIGS = {
     "ntr_sim_restore": (C.c_int, [_P, _P, C.c_size_t]),
     "ntr_sim_set_precision": (C.c_int, [_P, C.c_int]),
     "ntr_sim_set_batch_steps": (C.c_int, [_P, C.c_uint32]),
+    "ntr_sim_stats": (C.c_int, [_P, C.POINTER(Stats)]),
     "ntr_sim_profile": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "ntr_sim_last_launches": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
     "ntr_sim_conservation": (C.c_int, [_P, C.POINTER(C.c_double)]),

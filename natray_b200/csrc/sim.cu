@@ -69,6 +69,7 @@ struct Sim {
     uint64_t last_launches = 0;
     double last_ms = 0.0;
     double step_ms = 0.0;
+    void* stats_mem = nullptr;  // ntr_sim_stats' scratch, allocated at its first call
     uint32_t batch_steps = 0;  // ntr_sim_set_batch_steps: fixed steps per ntr_sim_advance batch (0: by time)
     uint32_t fp64 = 1;
     ntr_tuning tune{0u, 8u, 8u, 0u};  // launch shapes (ntr_sim_set_tuning)
@@ -80,6 +81,7 @@ struct Sim {
             if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
         }
         for (void* p : allocs) cudaFree(p);
+        if (stats_mem) cudaFree(stats_mem);
         if (h_state && own_h_state) cudaFreeHost(h_state);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -1463,3 +1465,108 @@ NTR_API ntr_status ntr_cache_download(ntr_cache* cache, uint32_t which, void* ho
 }
 
 }  // extern "C"
+
+// ---- debug statistics (include/natray.h, ntr_sim_stats) -----------------------------------------
+#include "stats.cuh"
+
+extern "C" NTR_API ntr_status ntr_sim_stats(ntr_sim* sim, ntr_stats* out) {
+    GUARD(sim);
+    if (!out) return fail(NTR_E_INVALID, "null argument");
+    Dev& D = S.D;
+    cudaStream_t s = S.stream;
+    const uint32_t n_cta_tri = std::max((D.Nt + 255u) / 256u, 1u);
+    const size_t acc_bytes = (sizeof(StatsAcc) + 255) & ~(size_t)255;
+    const size_t cand_bytes = ((size_t)n_cta_tri * 3 * sizeof(TensionCand) + 255) & ~(size_t)255;
+    const size_t cell_bytes = (size_t)D.cap_cells * 4;
+    if (!S.stats_mem) {
+        if (cudaMalloc(&S.stats_mem, acc_bytes + cand_bytes + cell_bytes) != cudaSuccess) {
+            cudaGetLastError();
+            S.stats_mem = nullptr;
+            return fail(NTR_E_NOMEM, "device allocation of the statistics' scratch failed");
+        }
+    }
+    StatsAcc* A = (StatsAcc*)S.stats_mem;
+    TensionCand* cand = (TensionCand*)((uint8_t*)S.stats_mem + acc_bytes);
+    uint32_t* cells = (uint32_t*)((uint8_t*)S.stats_mem + acc_bytes + cand_bytes);
+    ntr_status r = read_state(S);
+    if (r != NTR_OK) return r;
+    const uint32_t nb = std::min(S.h_state->s.n_blocks, D.cap_blocks);
+    StatsAcc init{};
+    for (int k = 0; k < 3; k++) init.lo[k] = init.mlo[k] = 0xffffffffu, init.hi[k] = init.mhi[k] = 0u;
+    init.fill_min = init.plo = 0xffffffffu;
+    CU(cudaMemcpyAsync(A, &init, sizeof init, cudaMemcpyHostToDevice, s));
+    CU(cudaMemsetAsync(cells, 0, (size_t)nb * 64 * 4, s));
+    k_stats_particles<<<std::max((D.Np + 255u) / 256u, 1u), 256, 0, s>>>(D, A, cells);
+    k_stats_cells<<<std::max((nb * 64u + 255u) / 256u, 1u), 256, 0, s>>>(D, A, cells);
+    k_stats_verts<<<std::max((D.Nv + 255u) / 256u, 1u), 256, 0, s>>>(D, A);
+    k_stats_tris<<<n_cta_tri, 256, 0, s>>>(D, A, cand);
+    CU(cudaGetLastError());
+    StatsAcc a{};
+    std::vector<TensionCand> c((size_t)n_cta_tri * 3);
+    std::vector<DBullet> bl(NTR_MAX_SHOTS);
+    CU(cudaMemcpyAsync(&a, A, sizeof a, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(c.data(), cand, c.size() * sizeof(TensionCand), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(bl.data(), D.bullets, bl.size() * sizeof(DBullet), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    float4 fast_p = make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint32_t fast_i = ~(uint32_t)(a.fastest & 0xffffffffull);
+    if (a.water && fast_i < D.Np) CU(cudaMemcpy(&fast_p, D.pos + fast_i, 16, cudaMemcpyDeviceToHost));
+
+    std::memset(out, 0, sizeof *out);
+    const double dx = S.host.h.dx, dx3 = dx * dx * dx, spacing = 0.5 * dx;
+    out->water = a.water, out->n_particles = D.Np;
+    const double n = (double)std::max(a.water, 1u);
+    for (int k = 0; k < 3; k++) {
+        out->lo[k] = a.water ? fkey_inv(a.lo[k]) : 0.f, out->hi[k] = a.water ? fkey_inv(a.hi[k]) : 0.f;
+        out->mean[k] = a.sum_x[k] / n, out->vmean[k] = a.sum_v[k] / n;
+        out->mem_lo[k] = D.Nv ? fkey_inv(a.mlo[k]) : 0.f, out->mem_hi[k] = D.Nv ? fkey_inv(a.mhi[k]) : 0.f;
+    }
+    out->vmax = a.water ? fkey_inv((uint32_t)(a.fastest >> 32)) : 0.f;
+    out->fastest[0] = fast_p.x, out->fastest[1] = fast_p.y, out->fastest[2] = fast_p.z;
+    out->volume_l = (double)a.full_cells * dx3 * 1e3;
+    out->inside_l = a.inside * 1e3;
+    out->free_verts = a.free_verts, out->on_water = a.on_water, out->torn = a.torn;
+    out->fill_min = a.free_verts ? fkey_inv(a.fill_min) : 0.f;
+    out->fill_mean = a.free_verts ? (float)(a.fill_sum / (double)a.free_verts) : 0.f;
+    out->rubber_vmax = D.Nv ? fkey_inv(a.rubber_vmax) : 0.f;
+    // The three most tense over all CTAs' candidates: by tension, then by triangle.
+    std::vector<TensionCand> best;
+    for (const TensionCand& q : c)
+        if (q.tri != NONE && q.tension >= 0.0) best.push_back(q);
+    std::sort(best.begin(), best.end(), [](const TensionCand& x, const TensionCand& y) {
+        return x.tension > y.tension || (x.tension == y.tension && x.tri < y.tri);
+    });
+    out->n_tension = (uint32_t)std::min<size_t>(best.size(), 3);
+    for (uint32_t k = 0; k < out->n_tension; k++) {
+        out->tension[k] = best[k].tension, out->tension_tri[k] = best[k].tri;
+        out->stretch[k][0] = best[k].l1, out->stretch[k][1] = best[k].l2;
+    }
+    out->air_cells = a.air_cells, out->vapour_cells = a.vapour;
+    out->gauge_lo = a.air_cells ? fkey_inv(a.plo) : 0.f, out->gauge_hi = a.air_cells ? fkey_inv(a.phi) : 0.f;
+    out->air_umax = a.air_cells ? fkey_inv(a.umax) : 0.f;
+    // Energies (src/sim.rs:847-857): a particle's mass is the water in its spacing cube.
+    out->water_j = a.ke * (1000.0 * (spacing * spacing * spacing));
+    const double cavity = (double)a.vapour * dx3;
+    out->vapour_cm3 = cavity * 1e6, out->vapour_j = cavity * 101325.0;
+    out->n_bullets = std::min<uint32_t>(S.U.mem[3], NTR_MAX_SHOTS);
+    for (uint32_t k = 0; k < out->n_bullets; k++) {
+        const DBullet& b = bl[k];
+        ntr_stats_bullet& o = out->bullets[k];
+        o.state = b.info.z, o.sections = b.info.w;
+        o.x[0] = b.x.x, o.x[1] = b.x.y, o.x[2] = b.x.z;
+        const float vx = b.v.x, vy = b.v.y, vz = b.v.z;
+        const float vsq = vx * vx + vy * vy + vz * vz;
+        o.speed = std::sqrt(vsq);
+        // The axis: the body's z rotated by its orientation quaternion (x, y, z, w).
+        const double qx = b.q.x, qy = b.q.y, qz = b.q.z, qw = b.q.w;
+        const double ax = 2.0 * (qx * qz + qw * qy), ay = 2.0 * (qy * qz - qw * qx), az = 1.0 - 2.0 * (qx * qx + qy * qy);
+        const double al = std::sqrt(ax * ax + ay * ay + az * az), vl = std::sqrt((double)vsq);
+        const double cs = al > 0.0 && vl > 0.0 ? std::clamp((ax * vx + ay * vy + az * vz) / (al * vl), -1.0, 1.0) : 1.0;
+        o.yaw_deg = (float)(std::acos(cs) * (180.0 / 3.14159265358979323846));
+        const double spin = (ax * b.l.x + ay * b.l.y + az * b.l.z) / (double)b.shape.x;
+        o.spin_rev_s = (float)(spin / (2.0 * 3.14159265358979323846));
+        o.kinetic_j = 0.5 * (double)b.x.w * (double)vsq;
+        out->bullets_j += o.kinetic_j;
+    }
+    return NTR_OK;
+}

@@ -56,6 +56,27 @@ class Sim:
         check(lib().ntr_sim_step(self._h, n, stop_ns, C.byref(taken)))
         return taken.value
 
+    def stats(self) -> dict:
+        """What the reference's debug_stats prints (src/sim.rs:691-863), computed on the device:
+        see `natray_b200.sim.format_stats` for the printed form."""
+        st = _abi.Stats()
+        check(lib().ntr_sim_stats(self._h, C.byref(st)))
+        out = {}
+        for k, _ in st._fields_:
+            if k.startswith("pad"):
+                continue
+            v = getattr(st, k)
+            if k == "bullets":
+                out[k] = [{f: (list(getattr(b, f)) if f == "x" else getattr(b, f)) for f, _ in b._fields_}
+                          for b in v[: st.n_bullets]]
+            elif k == "stretch":
+                out[k] = [list(r) for r in v]
+            elif hasattr(v, "__len__"):
+                out[k] = list(v)
+            else:
+                out[k] = v
+        return out
+
     def set_batch_steps(self, n: int) -> None:
         """Steps per batch of `advance` (0: the reference's 4 ms rule, which depends on the GPU's
         timing; a fixed count makes runs repeat bit for bit)."""
@@ -164,3 +185,31 @@ class Sim:
 
 
 __all__ = ["Sim"]
+
+
+def format_stats(sim: Sim) -> str:
+    """The lines the reference's Sim::debug_stats prints, from ntr_sim_stats and the state."""
+    s, st, i = sim.stats(), sim.state, sim._info()
+    f3 = lambda v, d=3: "[" + ", ".join(f"{x:.{d}f}" for x in v) + "]"
+    lines = [
+        f"t={i.t:.6f} dt={st['dt_ns']}ns steps {st['step']} | water {s['water']}/{s['n_particles']} bbox {f3(s['lo'])}.."
+        f"{f3(s['hi'])} mean {f3(s['mean'], 4)} v {f3(s['vmean'])} vmax {s['vmax']:.2f} at {f3(s['fastest'], 4)} volume "
+        f"{s['volume_l']:.3f} L | blocks {st['n_blocks']} solver {st['solve_iters']} iters (encoded {i.iters}) r "
+        f"{st['r_norm']:.2e} of {st['b_norm']:.2e} | spray {st['spray_count']}"]
+    for k in range(s["n_tension"]):
+        l1, l2 = s["stretch"][k]
+        lines.append(f"  tension {s['tension'][k]:.0f} N/m stretch {l1:.2f} x {l2:.3f} (triangle {s['tension_tri'][k]})")
+    lines.append(
+        f"  rubber: inside {s['inside_l']:.4f} L bbox {f3(s['mem_lo'], 4)}..{f3(s['mem_hi'], 4)} on water {s['on_water']}/"
+        f"{s['free_verts']} fill min {s['fill_min']:.2f} mean {s['fill_mean']:.2f} torn {s['torn']} fastest "
+        f"{s['rubber_vmax']:.1f} m/s | substep {st['mem_dt_seen'] * 1e6:.2f}us x{i.substeps} (step could be "
+        f"{st['dt_flow'] * 1e6:.1f}us) capillary {st['cap_dt'] * 1e6:.1f}us")
+    for k, b in enumerate(s["bullets"]):
+        lines.append(f"  bullet {k}: state {b['state']} at {f3(b['x'], 4)} v {b['speed']:.1f} m/s yaw {b['yaw_deg']:.1f} deg "
+                     f"spin {b['spin_rev_s']:.0f} rev/s, {b['sections']} sections")
+    lines.append(f"  energy: water {s['water_j']:.2f} J, bullets {s['bullets_j']:.2f} J, vapour {s['vapour_cm3']:.1f} cm^3 "
+                 f"(x 1 atm = {s['vapour_j']:.2f} J)")
+    lines.append(f"  air: {s['air_cells']} cells, {s['vapour_cells']} of them vapour, gauge {s['gauge_lo']:.1f}.."
+                 f"{s['gauge_hi']:.1f} Pa, fastest {s['air_umax']:.2f} m/s | substep {st['air_dt_seen'] * 1e6:.2f}us x"
+                 f"{i.air_substeps}")
+    return "\n".join(lines)
