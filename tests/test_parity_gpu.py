@@ -190,3 +190,36 @@ def test_conservation_sums(w_small):
     s.step(2)
     launches, ms = s.last_launches()
     assert launches > 40 and ms > 0
+
+
+def test_four_bullets_bit_exact(oracle_threads):
+    # A 5.56 mm spitzer, a flat-nosed pellet, a .45 round nose and a steel BB from four sides,
+    # 50 us apart (the reference's `shotN.key` parameters): every bullet branch of the step in
+    # one scene, through their impacts, the tearing and the first spray.
+    p = Params(resolution=24, mesh_level=3, block_cap=4096, spray_cap=200000)
+    for k, (b, az, delay) in enumerate([(3, 0, 0.0), (5, 90, 0.05), (2, 180, 0.1), (6, 270, 0.15)], start=1):
+        p.set(f"shot{k}.bullet", b)
+        p.set(f"shot{k}.azimuth", az)
+        p.set(f"shot{k}.delay", delay)
+    w = measured(build_world(p))
+    assert w.h.n_shots == 4
+    o, s = Oracle(w.blob), Sim(world=w)
+    for k in range(10):
+        assert o.step(10) == s.step(10) == 10
+        assert_worlds_equal(World(o.snapshot()), s.snapshot(), f"batch {k}")
+    end = s.snapshot()
+    assert end.state["spray_count"] > 0 and int((end.sec("ALIVE") == 0).sum()) > 0
+
+
+def test_long_run_to_the_ground_bit_exact(oracle_threads):
+    # A low balloon (0.12 m) run for 1200 steps of the reference's adaptive dt, about 0.45 s:
+    # the water and its spray fall, drops land (LANDED) and the ground gets wet (TOUCH), and
+    # both sides still agree bit for bit.
+    w = measured(build_world(Params(resolution=16, mesh_level=3, block_cap=4096, spray_cap=100000, height=0.12)))
+    o, s = Oracle(w.blob), Sim(world=w)
+    for k in range(12):
+        assert o.step(100) == s.step(100) == 100
+        if k % 4 == 3:
+            assert_worlds_equal(World(o.snapshot()), s.snapshot(), f"after {100 * (k + 1)} steps")
+    end = s.snapshot()
+    assert int((end.sec("LANDED")[:, 3] > 0).sum()) > 100 and int((end.sec("TOUCH") != 0xFFFFFFFF).sum()) > 100
