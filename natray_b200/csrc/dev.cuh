@@ -434,6 +434,50 @@ __device__ __forceinline__ uint32_t near_cell(const Grid& g, const CellsNear& n,
     if (b == NONE) return NONE;
     return b * 64u + (uint32_t)(c.x & 3) * 16u + (uint32_t)(c.y & 3) * 4u + (uint32_t)(c.z & 3);
 }
+// The 27 cells of the stencil base + (0..2, 0..2, 0..2), with the work of near_cell shared:
+// per axis each coordinate's block step from base's block, offset in the block and whether it
+// lies in the domain; per (a, b) the two blocks the z step chooses from. cell(a, b, c) is
+// near_cell(g, near_of(g, base), base + (a, b, c)).
+struct Stencil27 {
+    uint32_t blk[9][2];  // per a * 3 + b: the block for z step 0 and 1
+    uint32_t off[9];     // per a * 3 + b: the cells' x and y offsets in the block
+    uint32_t lz[3];
+    bool ok[9], okz[3], zs[3];
+    __device__ __forceinline__ uint32_t cell(int a, int b, int c) const {
+        const int ab = a * 3 + b;
+        const uint32_t bk = zs[c] ? blk[ab][1] : blk[ab][0];
+        return (ok[ab] && okz[c] && bk != NONE) ? bk * 64u + off[ab] + lz[c] : NONE;
+    }
+};
+__device__ __forceinline__ Stencil27 stencil_of(const Grid& g, const CellsNear& n, I3 base) {
+    Stencil27 s;
+    bool sx[3], sy[3], okx[3], oky[3];
+    uint32_t lx[3], ly[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const int cx = base.x + a, cy = base.y + a, cz = base.z + a;
+        okx[a] = cx >= 0 && (uint32_t)cx < g.dims[0];
+        oky[a] = cy >= 0 && (uint32_t)cy < g.dims[1];
+        s.okz[a] = cz >= 0 && (uint32_t)cz < g.dims[2];
+        sx[a] = (cx >> 2) != n.b0.x, sy[a] = (cy >> 2) != n.b0.y, s.zs[a] = (cz >> 2) != n.b0.z;
+        lx[a] = (uint32_t)(cx & 3), ly[a] = (uint32_t)(cy & 3), s.lz[a] = (uint32_t)(cz & 3);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        // blocks b0 + (sx, y, z) for (y, z) = (0,0), (1,0), (0,1), (1,1)
+        const uint32_t x0 = sx[a] ? n.blk[1] : n.blk[0], x1 = sx[a] ? n.blk[3] : n.blk[2];
+        const uint32_t x2 = sx[a] ? n.blk[5] : n.blk[4], x3 = sx[a] ? n.blk[7] : n.blk[6];
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            const int ab = a * 3 + b;
+            s.blk[ab][0] = sy[b] ? x1 : x0;
+            s.blk[ab][1] = sy[b] ? x3 : x2;
+            s.off[ab] = lx[a] * 16u + ly[b] * 4u;
+            s.ok[ab] = okx[a] && oky[b];
+        }
+    }
+    return s;
+}
 __device__ __forceinline__ I3 own_cell(const Grid& g, V3 p) { return vi(vfloor((p - g.org) / g.h)); }
 __device__ __forceinline__ V3 lattice_offset(uint32_t d) {
     V3 o = {0.5f, 0.5f, 0.5f};

@@ -89,12 +89,15 @@ __device__ float gas_pressure_at(const Dev& D, const Grid& g, int buf, V3 x) {
     I3 base = vi(vfloor((x - g.org) / g.h - 1.0f));
     V3 fx = (x - g.org) / g.h - 0.5f - vf(base);
     V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
-    const CellsNear n = near_of(g, base);
+    const Stencil27 sc = stencil_of(g, near_of(g, base), base);
     float sx = 0.0f, sy = 0.0f;
+#pragma unroll
     for (int a = 0; a < 3; a++)
+#pragma unroll
         for (int b = 0; b < 3; b++)
+#pragma unroll
             for (int c = 0; c < 3; c++) {
-                uint32_t cell = near_cell(g, n, base + I3{a, b, c});
+                uint32_t cell = sc.cell(a, b, c);
                 float w = wx[a] * wy[b] * wz[c];
                 if (cell == NONE) {
                     sx = sx + w * P_ATM;
@@ -148,11 +151,14 @@ __global__ void k_mem_splat(Dev D) {
     I3 base = vi(vfloor(x - 0.5f));
     V3 fx = x - vf(base);
     V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
-    const CellsNear n = near_of(g, base);
+    const Stencil27 sc = stencil_of(g, near_of(g, base), base);
+#pragma unroll
     for (int a = 0; a < 3; a++)
+#pragma unroll
         for (int b = 0; b < 3; b++)
+#pragma unroll
             for (int c = 0; c < 3; c++) {
-                uint32_t cell = near_cell(g, n, base + I3{a, b, c});
+                uint32_t cell = sc.cell(a, b, c);
                 if (cell == NONE) continue;
                 float w = wx[a] * wy[b] * wz[c];
                 atomicAdd(accp(D, A_MF, cell), to_fp(w * pa.x, FP_F));
@@ -417,7 +423,7 @@ __device__ __forceinline__ float2 sample_grid(const Dev& D, const Grid& g, V3 x,
     I3 base = vi(vfloor(x - 0.5f));
     V3 fx = x - vf(base);
     V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
-    const CellsNear n = near_of(g, base);
+    const Stencil27 sc = stencil_of(g, near_of(g, base), base);
     float sx = 0.0f, sy = 0.0f;
     // A plane of 9 cells at a time: its 18 loads go out together, then the sums in order.
 #pragma unroll
@@ -427,7 +433,7 @@ __device__ __forceinline__ float2 sample_grid(const Dev& D, const Grid& g, V3 x,
         float uv[9];
 #pragma unroll
         for (int k = 0; k < 9; k++) {
-            cells[k] = near_cell(g, n, base + I3{a, k / 3, k % 3});
+            cells[k] = sc.cell(a, k / 3, k % 3);
             wv[k] = cells[k] != NONE ? accv(D, fw, cells[k]) : 0;
             uv[k] = cells[k] != NONE ? cfv(D, fu, cells[k]) : 0.0f;
         }
