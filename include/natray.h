@@ -408,6 +408,13 @@ NTR_API ntr_status ntr_sim_set_batch_steps(ntr_sim* s, uint32_t n);
 NTR_API ntr_status ntr_sim_profile(ntr_sim* s, uint32_t n, uint32_t stop_ns, char* report, size_t cap, size_t* len);
 /* Kernel launches made by the last ntr_sim_step call, and its device time in ms. */
 NTR_API ntr_status ntr_sim_last_launches(ntr_sim* s, uint64_t* launches, double* device_ms);
+/* The particles in the reference's layout (`Particle`, sim_defs.wgsl:61: 20 f32 each, pos.xyzw,
+ * vel.xyz + alive, c0, c1, c2), written into a device buffer the caller owns (16-byte aligned,
+ * at least n_particles * 80 bytes): for a renderer or packer written against that layout, which
+ * this library keeps as five arrays. Ordered after the simulation's work so far. With
+ * stream != NULL (a cudaStream_t) the call is asynchronous and that stream's later work sees the
+ * result; with NULL it returns once the buffer is written. */
+NTR_API ntr_status ntr_sim_pack_particles(ntr_sim* s, void* dst_device, size_t bytes, void* stream);
 /* Conservation sums over live particles, accumulated in FP64 on the device:
  * out[0] = live count, out[1..3] = momentum per particle mass, out[4] = kinetic energy per
  * particle mass, out[5..7] = sum of positions. */

@@ -197,6 +197,7 @@ _SIGS = {
     "ntr_sim_set_precision": (C.c_int, [_P, C.c_int]),
     "ntr_sim_set_batch_steps": (C.c_int, [_P, C.c_uint32]),
     "ntr_sim_stats": (C.c_int, [_P, C.POINTER(Stats)]),
+    "ntr_sim_pack_particles": (C.c_int, [_P, _P, C.c_size_t, _P]),
     "ntr_sim_profile": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "ntr_sim_last_launches": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
     "ntr_sim_conservation": (C.c_int, [_P, C.POINTER(C.c_double)]),

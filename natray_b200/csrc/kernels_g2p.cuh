@@ -363,6 +363,18 @@ __global__ void k_spray_commit(Dev D) {
 // ---- the zero-length measuring substep and diagnostics --------------------------------------------
 // Conservation sums over live particles in FP64: count, momentum, kinetic energy (per particle
 // mass) and the sum of positions.
+// The particles in the reference's layout (`Particle`, sim_defs.wgsl:61): 20 floats each, the
+// five float4 of the SoA arrays in order. One thread per output float4: coalesced writes.
+__global__ void k_pack_particles(Dev D, float4* __restrict__ dst) {
+    const size_t n = (size_t)D.Np * 5;
+    for (size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+        const size_t i = o / 5;
+        const uint32_t k = (uint32_t)(o - i * 5);
+        const float4* src = k == 0 ? D.pos : k == 1 ? D.vel : k == 2 ? D.c0 : k == 3 ? D.c1 : D.c2;
+        dst[o] = src[i];
+    }
+}
+
 __global__ void k_conservation(Dev D, double* out) {
     __shared__ double red[8][8];
     double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};

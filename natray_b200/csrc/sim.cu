@@ -70,6 +70,7 @@ struct Sim {
     double last_ms = 0.0;
     double step_ms = 0.0;
     void* stats_mem = nullptr;  // ntr_sim_stats' scratch, allocated at its first call
+    cudaEvent_t ev_out = nullptr;  // ntr_sim_pack_particles: the caller's stream waits on it
     uint32_t batch_steps = 0;  // ntr_sim_set_batch_steps: fixed steps per ntr_sim_advance batch (0: by time)
     uint32_t fp64 = 1;
     ntr_tuning tune{0u, 8u, 8u, 0u};  // launch shapes (ntr_sim_set_tuning)
@@ -82,6 +83,7 @@ struct Sim {
         }
         for (void* p : allocs) cudaFree(p);
         if (stats_mem) cudaFree(stats_mem);
+        if (ev_out) cudaEventDestroy(ev_out);
         if (h_state && own_h_state) cudaFreeHost(h_state);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -1069,6 +1071,24 @@ NTR_API ntr_status ntr_sim_last_launches(ntr_sim* sim, uint64_t* launches, doubl
     GUARD(sim);
     if (launches) *launches = S.last_launches;
     if (device_ms) *device_ms = S.last_ms;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_sim_pack_particles(ntr_sim* sim, void* dst, size_t bytes, void* stream) {
+    GUARD(sim);
+    if (!dst) return fail(NTR_E_INVALID, "null argument");
+    if (bytes < (size_t)S.D.Np * 80) return fail(NTR_E_INVALID, "destination smaller than 80 bytes per particle");
+    if ((uintptr_t)dst % 16) return fail(NTR_E_INVALID, "destination not 16-byte aligned");
+    const uint32_t grid = (uint32_t)std::min<size_t>(((size_t)S.D.Np * 5 + 255) / 256, (size_t)S.sms * 16);
+    k_pack_particles<<<std::max(grid, 1u), 256, 0, S.stream>>>(S.D, (float4*)dst);
+    CU(cudaGetLastError());
+    if (stream) {
+        if (!S.ev_out) CU(cudaEventCreateWithFlags(&S.ev_out, cudaEventDisableTiming));
+        CU(cudaEventRecord(S.ev_out, S.stream));
+        CU(cudaStreamWaitEvent((cudaStream_t)stream, S.ev_out, 0));
+    } else {
+        CU(cudaStreamSynchronize(S.stream));
+    }
     return NTR_OK;
 }
 

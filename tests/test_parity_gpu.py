@@ -223,3 +223,27 @@ def test_long_run_to_the_ground_bit_exact(oracle_threads):
             assert_worlds_equal(World(o.snapshot()), s.snapshot(), f"after {100 * (k + 1)} steps")
     end = s.snapshot()
     assert int((end.sec("LANDED")[:, 3] > 0).sum()) > 100 and int((end.sec("TOUCH") != 0xFFFFFFFF).sum()) > 100
+
+
+def test_pack_particles_gives_the_reference_layout(w_small):
+    # ntr_sim_pack_particles: the five SoA arrays written as the reference's 20-float records
+    # into a device buffer the caller owns (here torch's), on the caller's stream or not.
+    import ctypes as C
+
+    import torch
+    from natray_b200._abi import lib
+    s = Sim(world=w_small)
+    s.step(6)
+    want = s.snapshot().sec("PARTICLES")
+    n = want.shape[0]
+    buf = torch.zeros(n * 80, dtype=torch.uint8, device="cuda:0")
+    stream = torch.cuda.current_stream().cuda_stream
+    assert lib().ntr_sim_pack_particles(s._h, C.c_void_p(buf.data_ptr()), n * 80, C.c_void_p(stream)) == 0
+    got = buf.cpu().numpy().view(np.float32).reshape(n, 20)
+    assert np.array_equal(bits(got), bits(want))
+    buf.zero_()
+    torch.cuda.synchronize()
+    assert lib().ntr_sim_pack_particles(s._h, C.c_void_p(buf.data_ptr()), n * 80, None) == 0
+    assert np.array_equal(bits(buf.cpu().numpy().view(np.float32).reshape(n, 20)), bits(want))
+    assert lib().ntr_sim_pack_particles(s._h, C.c_void_p(buf.data_ptr()), n * 80 - 16, None) == 1  # too small
+    s.close()
