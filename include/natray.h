@@ -481,6 +481,15 @@ NTR_API ntr_status ntr_batch_poll(ntr_batch* b, uint32_t slot, ntr_batch_slot* o
 NTR_API ntr_status ntr_batch_snapshot(ntr_batch* b, uint32_t slot, void* buf, size_t cap, size_t* len);
 NTR_API ntr_status ntr_batch_retire(ntr_batch* b, uint32_t slot);
 NTR_API ntr_status ntr_batch_info_get(ntr_batch* b, ntr_batch_info* out);
+/* Admission from any thread. Every ntr_batch_* call holds the batch's lock, so calls from
+ * several host threads take turns (a call waits at most for the one in progress, such as a
+ * batch step). ntr_batch_enqueue checks the world blob, queues a copy and returns a ticket; the
+ * queued scenes are admitted in order at the start of the next ntr_batch_step, as far as slots
+ * and memory allow (a scene that does not fit yet stays at the head of the queue).
+ * ntr_batch_ticket gives the ticket's slot once admitted, NTR_BATCH_MAX while it waits, and
+ * NTR_E_INVALID if its admission failed. */
+NTR_API ntr_status ntr_batch_enqueue(ntr_batch* b, const void* world_blob, size_t len, uint32_t n_steps, uint64_t* ticket);
+NTR_API ntr_status ntr_batch_ticket(ntr_batch* b, uint64_t ticket, uint32_t* slot);
 
 /* --- Sorting particles by block without allocating ------------------------------------------
  * No counterpart in the reference: an addition for callers that cannot allocate device

@@ -53,6 +53,20 @@ class Batch:
         check(st)
         return slot.value
 
+    def enqueue(self, world: World | bytes, n_steps: int) -> int:
+        """Queues the scene from any thread; the stepping thread admits it at its next step.
+        Returns the ticket."""
+        blob = bytes(world.blob) if isinstance(world, World) else bytes(world)
+        ticket = C.c_uint64()
+        check(lib().ntr_batch_enqueue(self._h, blob, len(blob), n_steps, C.byref(ticket)))
+        return ticket.value
+
+    def ticket(self, ticket: int) -> int | None:
+        """The queued scene's slot once admitted, None while it waits."""
+        slot = C.c_uint32()
+        check(lib().ntr_batch_ticket(self._h, ticket, C.byref(slot)))
+        return None if slot.value == _abi.BATCH_MAX else slot.value
+
     def step(self, n: int) -> int:
         """n steps of every unfinished scene; returns how many scenes stepped."""
         active = C.c_uint32()

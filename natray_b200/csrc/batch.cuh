@@ -12,6 +12,7 @@
 #pragma once
 
 #include <chrono>
+#include <deque>
 
 namespace ntr {
 
@@ -39,6 +40,18 @@ struct Batch {
     cudaEvent_t ev_solve = nullptr;
     Dev* d_jobs = nullptr;  // the pointer tables of the scenes in the current step's order
     uint32_t n_jobs_cap = 0;
+    // Every call on the batch holds this lock: calls from several host threads take turns.
+    std::mutex mu;
+    // Scenes queued by any thread (ntr_batch_enqueue), admitted in order at the start of the
+    // next ntr_batch_step; where each ticket went (a slot, or BATCH_REJECTED).
+    struct Queued {
+        uint64_t ticket;
+        std::vector<uint8_t> blob;
+        uint32_t n_steps;
+    };
+    std::deque<Queued> queue;
+    uint64_t next_ticket = 1;
+    std::map<uint64_t, uint32_t> placed;
 
     ~Batch() {
         cudaSetDevice(device);

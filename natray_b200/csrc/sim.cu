@@ -1212,7 +1212,10 @@ struct ntr_batch {
 #define BGUARD(batch)                                                                   \
     if (!(batch) || !(batch)->b) return fail(NTR_E_INVALID, "null batch handle");        \
     Batch& B = *(batch)->b;                                                             \
+    std::lock_guard<std::mutex> batch_lock_(B.mu);                                      \
     if (cudaSetDevice(B.device) != cudaSuccess) return fail(NTR_E_CUDA, "cudaSetDevice failed")
+
+constexpr uint32_t BATCH_REJECTED = 0xfffffffeu;
 
 extern "C" {
 
@@ -1238,8 +1241,46 @@ NTR_API ntr_status ntr_batch_admit(ntr_batch* batch, const void* blob, size_t le
     return batch_admit(B, blob, len, n_steps, *slot);
 }
 
+NTR_API ntr_status ntr_batch_enqueue(ntr_batch* batch, const void* blob, size_t len, uint32_t n_steps, uint64_t* ticket) {
+    BGUARD(batch);
+    if (!blob || !ticket) return fail(NTR_E_INVALID, "null argument");
+    World w;
+    std::string err;
+    if (!deserialize(blob, len, w, err)) return fail(NTR_E_INVALID, err);
+    const uint8_t* p = static_cast<const uint8_t*>(blob);
+    B.queue.push_back(Batch::Queued{B.next_ticket, std::vector<uint8_t>(p, p + len), n_steps});
+    *ticket = B.next_ticket++;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_batch_ticket(ntr_batch* batch, uint64_t ticket, uint32_t* slot) {
+    BGUARD(batch);
+    if (!slot) return fail(NTR_E_INVALID, "null argument");
+    auto it = B.placed.find(ticket);
+    if (it != B.placed.end()) {
+        if (it->second == BATCH_REJECTED) return fail(NTR_E_INVALID, "the queued scene could not be admitted");
+        *slot = it->second;
+        return NTR_OK;
+    }
+    for (const auto& q : B.queue)
+        if (q.ticket == ticket) {
+            *slot = NTR_BATCH_MAX;
+            return NTR_OK;
+        }
+    return fail(NTR_E_INVALID, "unknown ticket");
+}
+
 NTR_API ntr_status ntr_batch_step(ntr_batch* batch, uint32_t n, uint32_t* active) {
     BGUARD(batch);
+    // Queued scenes first, in order, as far as slots and memory allow.
+    while (!B.queue.empty()) {
+        Batch::Queued& q = B.queue.front();
+        uint32_t slot = 0;
+        const ntr_status r = batch_admit(B, q.blob.data(), q.blob.size(), q.n_steps, slot);
+        if (r == NTR_E_BUSY) break;
+        B.placed[q.ticket] = r == NTR_OK ? slot : BATCH_REJECTED;
+        B.queue.pop_front();
+    }
     uint32_t a = 0;
     ntr_status r = batch_step(B, n, a);
     if (active) *active = a;

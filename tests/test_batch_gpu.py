@@ -101,3 +101,37 @@ def test_serving_loop_finishes_every_request(worlds):
     ws = worlds * 2
     out = serve(ws, poisson_arrivals(len(ws), 200.0, 3), steps=8, chunk=4, max_scenes=3)
     assert out["requests"] == len(ws) and out["p99_s"] >= out["p50_s"] > 0.0
+
+
+def test_queue_from_other_threads(worlds):
+    # Three host threads queue scenes while the main thread steps the batch (every call takes
+    # the batch's lock); each scene is admitted at a step in queue order and ends as it would
+    # alone.
+    import threading
+    with Batch(max_scenes=2) as b:
+        tickets = {}
+
+        def submit(k):
+            tickets[k] = b.enqueue(worlds[k], 8)
+
+        threads = [threading.Thread(target=submit, args=(k,)) for k in range(3)]
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
+        assert sorted(tickets.values()) == [1, 2, 3]
+        order = sorted(tickets, key=tickets.get)
+        got = {}
+        for _ in range(12):
+            b.step(4)
+            for k in order:
+                sl = b.ticket(tickets[k])
+                if sl is not None and k not in got and b.poll(sl)["finished"]:
+                    got[k] = b.snapshot(sl)
+                    b.retire(sl)
+            if len(got) == 3:
+                break
+        assert len(got) == 3
+    for k, r in got.items():
+        d = first_difference(solo(worlds[k], 8, 4), r)
+        assert d is None, f"scene {k}: {d}"
