@@ -216,12 +216,8 @@ def run_native(args, rank, world, local):
     barrier()
     launches, ms = sim.last_launches()
     st = sim.state
-    t_dev = ms * 1e-3
-    if use_dist:
-        import torch.distributed as dist
-        tt = torch.tensor([t_dev], device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_dev = float(tt.item())
+    from natray_b200.replicas import max_over_ranks
+    t_dev = max_over_ranks(ms * 1e-3)
     value = n_particles * args.steps * world / t_dev
 
     # End to end through the public API: one ntr_sim_step call per step, each uploading the
@@ -230,12 +226,7 @@ def run_native(args, rank, world, local):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         sim.step(1)
-    t_e2e = time.perf_counter() - t0
-    if use_dist:
-        import torch.distributed as dist
-        tt = torch.tensor([t_e2e], device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt.item())
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
     e2e = n_particles * args.steps * world / t_e2e
 
     # Roofline of the dominant kernel: kernel-by-kernel event timing of a few steps.

@@ -481,6 +481,9 @@ NTR_API ntr_status ntr_batch_poll(ntr_batch* b, uint32_t slot, ntr_batch_slot* o
 NTR_API ntr_status ntr_batch_snapshot(ntr_batch* b, uint32_t slot, void* buf, size_t cap, size_t* len);
 NTR_API ntr_status ntr_batch_retire(ntr_batch* b, uint32_t slot);
 NTR_API ntr_status ntr_batch_info_get(ntr_batch* b, ntr_batch_info* out);
+/* The device memory a simulation of this world takes (what admission to a batch checks against
+ * its budget and the free memory; a server placing scenes on GPUs uses it). CPU only. */
+NTR_API ntr_status ntr_world_device_bytes(const void* world_blob, size_t len, uint64_t* bytes);
 /* Admission from any thread. Every ntr_batch_* call holds the batch's lock, so calls from
  * several host threads take turns (a call waits at most for the one in progress, such as a
  * batch step). ntr_batch_enqueue checks the world blob, queues a copy and returns a ticket; the

@@ -214,6 +214,7 @@ _SIGS = {
     "ntr_batch_retire": (C.c_int, [_P, C.c_uint32]),
     "ntr_batch_info_get": (C.c_int, [_P, C.POINTER(BatchInfo)]),
     "ntr_batch_enqueue": (C.c_int, [_P, _P, C.c_size_t, C.c_uint32, C.POINTER(C.c_uint64)]),
+    "ntr_world_device_bytes": (C.c_int, [_P, C.c_size_t, C.POINTER(C.c_uint64)]),
     "ntr_batch_ticket": (C.c_int, [_P, C.c_uint64, C.POINTER(C.c_uint32)]),
     "ntr_cache_params_default": (C.c_int, [C.POINTER(SimParams), C.POINTER(CacheParams)]),
     "ntr_key_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]),

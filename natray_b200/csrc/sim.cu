@@ -1241,6 +1241,14 @@ NTR_API ntr_status ntr_batch_admit(ntr_batch* batch, const void* blob, size_t le
     return batch_admit(B, blob, len, n_steps, *slot);
 }
 
+NTR_API ntr_status ntr_world_device_bytes(const void* blob, size_t len, uint64_t* bytes) {
+    if (!blob || !bytes) return fail(NTR_E_INVALID, "null argument");
+    World w;
+    std::string err;
+    if (!deserialize(blob, len, w, err)) return fail(NTR_E_INVALID, err);
+    return world_device_bytes(w, *bytes);
+}
+
 NTR_API ntr_status ntr_batch_enqueue(ntr_batch* batch, const void* blob, size_t len, uint32_t n_steps, uint64_t* ticket) {
     BGUARD(batch);
     if (!blob || !ticket) return fail(NTR_E_INVALID, "null argument");

@@ -126,7 +126,7 @@ def serve(worlds: list[World], arrivals: list[float], steps: int, chunk: int = 4
         makespan = time.perf_counter() - t0
     lat = np.array([f - a for f, a in zip(finish, arrivals)])
     return {"requests": n, "seconds": makespan, "scenes_per_s": n / makespan, "p50_s": float(np.percentile(lat, 50)),
-            "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean())}
+            "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()), "latencies": [float(x) for x in lat]}
 
 
 def sequential_timeline(arrivals: list[float], durations: list[float]) -> dict:
@@ -155,6 +155,24 @@ def main():
     ap.add_argument("--rate", type=float, default=40.0, help="requests per second")
     ap.add_argument("--seed", type=int, default=7)
     args = ap.parse_args()
+    import os
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        # Under torchrun: one process per GPU, the request stream shared out by free device
+        # memory (natray_b200.replicas), the results merged on rank 0.
+        import torch
+        import torch.distributed as dist
+        from .replicas import serve_replicas
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl")
+        n = args.serve or args.scenes
+        ps = mixed_scenes(n, args.seed, lo=16_000, hi=2_000_000, lognormal_median=128_000)
+        worlds = build_worlds(ps)
+        res = serve_replicas(worlds, poisson_arrivals(n, args.rate, args.seed), args.steps, args.chunk)
+        if res is not None:
+            res.pop("plan", None)
+            print(json.dumps({"served": res}))
+        dist.destroy_process_group()
+        return
     if args.serve:
         ps = mixed_scenes(args.serve, args.seed, lo=16_000, hi=2_000_000, lognormal_median=128_000)
         worlds = build_worlds(ps)
