@@ -3,7 +3,9 @@
 Every CUDA source is compiled by nvcc for `-gencode arch=compute_100a,code=sm_100a` only; host
 C++ sources by g++. Floating-point contraction is off in both (`-fmad=false`,
 `-ffp-contract=off`) so that the fixed-point transfer sums are bit-identical to a CPU
-evaluation of the same expressions. Usage: `python -m natray_b200.build`.
+evaluation of the same expressions. Host code also takes `-fno-math-errno`: math functions
+leave errno alone, so the compiler may treat them as pure (their values do not change). Usage:
+`python -m natray_b200.build`.
 """
 from __future__ import annotations
 
@@ -19,7 +21,7 @@ OBJ = PKG / "_build"
 LIB = PKG / "libnatray.so"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CXXFLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fvisibility=hidden", "-Wall", "-Wno-unused-function"]
+CXXFLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-math-errno", "-fvisibility=hidden", "-Wall", "-Wno-unused-function"]
 NVFLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-fvisibility=hidden,-ffp-contract=off",
                   "-Xptxas", "-warn-spills", "--expt-relaxed-constexpr"]
 

@@ -67,12 +67,12 @@ NTR_API ntr_status ntr_world_build(const ntr_sim_params* p, void** blob, size_t*
     World w;
     std::string err;
     if (!build_world(*p, w, err)) return fail(NTR_E_INVALID, err);
-    std::vector<uint8_t> v = serialize(w);
-    void* out = std::malloc(v.size());
+    const size_t n = serialize_into(w, nullptr);
+    void* out = std::malloc(n);
     if (!out) return fail(NTR_E_NOMEM, "host allocation of the world blob failed");
-    std::memcpy(out, v.data(), v.size());
+    serialize_into(w, out);
     *blob = out;
-    *len = v.size();
+    *len = n;
     return NTR_OK;
 }
 

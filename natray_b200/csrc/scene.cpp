@@ -11,12 +11,16 @@
 #include <array>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
+#include <condition_variable>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <optional>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -82,6 +86,42 @@ constexpr double OGDEN_MU[3] = {0.63e6, 0.0012e6, -0.01e6};
 constexpr double OGDEN_AL[3] = {1.3, 5.0, -2.0};
 constexpr double NECK = 0.25;
 
+// pow(x, alpha) for the three Ogden exponents and pow(x, -0.5), for the few distinct stretches
+// one evaluation of the shape's ODE asks for (its finite differences share most of them). Kept
+// by the bits of x, so every value is the one pow returns.
+class Powers {
+   public:
+    using P3 = std::array<double, 3>;
+    P3 ogden(double x) {
+        const uint64_t b = bits(x);
+        for (int i = 0; i < n3_; i++)
+            if (k3_[i] == b) return v3_[i];
+        P3 v = {std::pow(x, OGDEN_AL[0]), std::pow(x, OGDEN_AL[1]), std::pow(x, OGDEN_AL[2])};
+        if (n3_ < CAP) k3_[n3_] = b, v3_[n3_++] = v;
+        return v;
+    }
+    double inv_sqrt(double x) {
+        const uint64_t b = bits(x);
+        for (int i = 0; i < nh_; i++)
+            if (kh_[i] == b) return vh_[i];
+        double v = std::pow(x, -0.5);
+        if (nh_ < CAP) kh_[nh_] = b, vh_[nh_++] = v;
+        return v;
+    }
+
+   private:
+    static constexpr int CAP = 16;
+    static uint64_t bits(double x) {
+        uint64_t u;
+        std::memcpy(&u, &x, 8);
+        return u;
+    }
+    uint64_t k3_[CAP], kh_[CAP];
+    P3 v3_[CAP];
+    double vh_[CAP];
+    int n3_ = 0, nh_ = 0;
+};
+
 struct Latex {
     double mu[3];
     double thickness;
@@ -91,26 +131,31 @@ struct Latex {
         g0 /= 2.0;
         for (int i = 0; i < 3; i++) mu[i] = OGDEN_MU[i] * shear / g0;
     }
-    double sigma(double a, double b) const {
+    // sum_i mu_i (a^alpha_i - b^alpha_i), from the powers of a and b.
+    double sigma(const Powers::P3& a, const Powers::P3& b) const {
         double s = 0.0;
-        for (int i = 0; i < 3; i++) s += mu[i] * (std::pow(a, OGDEN_AL[i]) - std::pow(b, OGDEN_AL[i]));
+        for (int i = 0; i < 3; i++) s += mu[i] * (a[i] - b[i]);
         return s;
     }
-    std::pair<double, double> stress(double l1, double l2) const {
+    // Principal tensions (stress times deformed thickness) at stretches l1, l2; with `both`
+    // false only the first is computed (the second is returned as 0 times the thickness factor).
+    std::pair<double, double> tension(double l1, double l2, Powers& pw, bool both = true) const {
         double major = std::max(l1, l2), minor = std::min(l1, l2);
-        if (major <= 1.0) return {0.0, 0.0};
-        double natural = std::pow(major, -0.5);
-        if (minor < natural) {
-            double s = sigma(major, natural);
-            return l1 >= l2 ? std::make_pair(s, 0.0) : std::make_pair(0.0, s);
+        double s1 = 0.0, s2 = 0.0;
+        if (major > 1.0) {
+            double natural = pw.inv_sqrt(major);
+            if (minor < natural) {
+                double s = sigma(pw.ogden(major), pw.ogden(natural));
+                (l1 >= l2 ? s1 : s2) = s;
+            } else {
+                double l3 = 1.0 / (l1 * l2);
+                const Powers::P3 p3 = pw.ogden(l3);
+                s1 = sigma(pw.ogden(l1), p3);
+                if (both) s2 = sigma(pw.ogden(l2), p3);
+            }
         }
-        double l3 = 1.0 / (l1 * l2);
-        return {sigma(l1, l3), sigma(l2, l3)};
-    }
-    std::pair<double, double> tension(double l1, double l2) const {
-        auto s = stress(l1, l2);
         double t = thickness / (l1 * l2);
-        return {s.first * t, s.second * t};
+        return {s1 * t, s2 * t};
     }
 };
 
@@ -150,18 +195,22 @@ struct ShotResult {
 
 std::optional<ShotResult> shoot(const Latex& latex, double rest_r, double apex_stretch, double apex_curv, double rho_g) {
     const double neck_angle = PI - std::asin(NECK);
-    const double p_apex = 2.0 * latex.tension(apex_stretch, apex_stretch).first * apex_curv;
+    Powers apex;
+    const double p_apex = 2.0 * latex.tension(apex_stretch, apex_stretch, apex).first * apex_curv;
     auto deriv = [&](double th, const Y5& y) -> std::optional<Y5> {
         double r = y[0], z = y[1], psi = y[2], l1 = y[3];
         double rr = rest_r * std::sin(th);
         double l2 = r / rr;
         if (!(r > 0.0 && l1 > 0.0)) return std::nullopt;
-        auto t = latex.tension(l1, l2);
+        Powers pw;
+        auto t = latex.tension(l1, l2, pw);
         double t1 = t.first, t2 = t.second;
         if (t1 <= 0.0) return std::nullopt;
         double e = 1e-6;
-        double t1_l1 = (latex.tension(l1 * (1.0 + e), l2).first - latex.tension(l1 * (1.0 - e), l2).first) / (2.0 * e * l1);
-        double t1_l2 = (latex.tension(l1, l2 * (1.0 + e)).first - latex.tension(l1, l2 * (1.0 - e)).first) / (2.0 * e * l2);
+        double t1_l1 =
+            (latex.tension(l1 * (1.0 + e), l2, pw, false).first - latex.tension(l1 * (1.0 - e), l2, pw, false).first) / (2.0 * e * l1);
+        double t1_l2 =
+            (latex.tension(l1, l2 * (1.0 + e), pw, false).first - latex.tension(l1, l2 * (1.0 - e), pw, false).first) / (2.0 * e * l2);
         double p = p_apex - rho_g * z;
         double dr = l1 * std::cos(psi);
         double dz = l1 * std::sin(psi);
@@ -238,38 +287,184 @@ bool inflate(const Latex& latex, double rest_r, double volume, double rho_g, Pro
     return true;
 }
 
+// A few threads that run a batch of independent jobs together; the calling thread takes part,
+// so a pool of n runs n jobs at a time.
+class Pool {
+   public:
+    explicit Pool(unsigned n) {
+        for (unsigned i = 1; i < n; i++) th_.emplace_back([this] { work(); });
+    }
+    ~Pool() {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            stop_ = true;
+        }
+        wake_.notify_all();
+        for (auto& t : th_) t.join();
+    }
+    unsigned size() const { return (unsigned)th_.size() + 1; }
+    // Runs fn(i) for every i in [0, n) and returns when all have run.
+    void run(size_t n, const std::function<void(size_t)>& fn) {
+        if (n == 0) return;
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            fn_ = &fn, n_ = n, next_ = 0, left_ = n, gen_++;
+        }
+        wake_.notify_all();
+        drain();
+        std::unique_lock<std::mutex> lk(mu_);
+        done_.wait(lk, [&] { return left_ == 0; });
+        fn_ = nullptr;
+    }
+
+   private:
+    void drain() {
+        for (;;) {
+            size_t i;
+            const std::function<void(size_t)>* f;
+            {
+                std::lock_guard<std::mutex> g(mu_);
+                if (!fn_ || next_ >= n_) return;
+                i = next_++, f = fn_;
+            }
+            (*f)(i);
+            std::lock_guard<std::mutex> g(mu_);
+            if (--left_ == 0) done_.notify_all();
+        }
+    }
+    void work() {
+        uint64_t seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                wake_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+            }
+            drain();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex mu_;
+    std::condition_variable wake_, done_;
+    const std::function<void(size_t)>* fn_ = nullptr;
+    size_t n_ = 0, next_ = 0, left_ = 0;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+};
+
+// The outcome of one shot (its end radius and volume), kept per exact inputs (apex stretch and
+// log apex curvature, as bits). The search below is the reference's sequential one and reads its
+// shots from here; before each of its steps the shots that step and the next are likely to need
+// are run together on the pool. A shot is a pure function of its inputs, so the profile is
+// bit-identical to one computed shot by shot, whatever was run ahead and on which thread.
+class Shots {
+   public:
+    struct End {
+        bool ok;
+        double r, volume;
+    };
+    using X = std::array<double, 2>;
+    Shots(const Latex& latex, double rest_r, double rho_g, unsigned threads)
+        : latex_(latex), rest_r_(rest_r), rho_g_(rho_g), pool_(threads) {}
+    unsigned width() const { return pool_.size(); }
+    const End& get(X x) {
+        auto it = memo_.find(key(x));
+        if (it != memo_.end()) return it->second;
+        return memo_.emplace(key(x), one(x)).first->second;
+    }
+    // Runs the shots not run yet, all at once (nothing on a pool of one: get() runs them then).
+    void ahead(const std::vector<X>& xs) {
+        if (pool_.size() < 2) return;
+        std::vector<X> todo;
+        for (const X& x : xs)
+            if (!memo_.count(key(x)) &&
+                std::none_of(todo.begin(), todo.end(), [&](const X& t) { return key(t) == key(x); }))
+                todo.push_back(x);
+        std::vector<End> out(todo.size());
+        pool_.run(todo.size(), [&](size_t i) { out[i] = one(todo[i]); });
+        for (size_t i = 0; i < todo.size(); i++) memo_.emplace(key(todo[i]), out[i]);
+    }
+
+   private:
+    static std::pair<uint64_t, uint64_t> key(X x) {
+        uint64_t a, b;
+        std::memcpy(&a, &x[0], 8);
+        std::memcpy(&b, &x[1], 8);
+        return {a, b};
+    }
+    End one(X x) const {
+        auto s = shoot(latex_, rest_r_, x[0], std::exp(x[1]), rho_g_);
+        if (!s) return {false, 0.0, 0.0};
+        return {true, s->samples.back().r, s->volume};
+    }
+    const Latex& latex_;
+    double rest_r_, rho_g_;
+    Pool pool_;
+    std::map<std::pair<uint64_t, uint64_t>, End> memo_;
+};
+
+// Threads for the inflation's shots: NATRAY_BUILD_THREADS when set (1 runs them one by one, in
+// the reference's order), else the host's, at most 8 (the search runs at most 8 ahead).
+static unsigned build_threads() {
+    if (const char* e = std::getenv("NATRAY_BUILD_THREADS")) {
+        long n = std::strtol(e, nullptr, 10);
+        if (n >= 1) return (unsigned)std::min(n, 64L);
+    }
+    return std::clamp(std::thread::hardware_concurrency(), 1u, 8u);
+}
+
 bool inflate_solve(const Latex& latex, double rest_r, double volume, double rho_g, Profile& prof, std::string& err) {
     const double neck_r = NECK * rest_r;
+    Shots shots(latex, rest_r, rho_g, build_threads());
+    const unsigned width = shots.width();
     auto miss = [&](std::array<double, 2> x, double target) -> std::optional<std::array<double, 2>> {
-        auto s = shoot(latex, rest_r, x[0], std::exp(x[1]), rho_g);
-        if (!s) return std::nullopt;
-        return std::array<double, 2>{(s->samples.back().r - neck_r) / neck_r, std::log(s->volume) - target};
+        const Shots::End& s = shots.get(x);
+        if (!s.ok) return std::nullopt;
+        return std::array<double, 2>{(s.r - neck_r) / neck_r, std::log(s.volume) - target};
     };
     const double la0 = 1.2;
     double lo = std::log(1e-3 / rest_r), hi = std::log(1e3 / rest_r);
-    for (int i = 0; i < 60; i++) {
-        double mid = 0.5 * (lo + hi);
-        auto s = shoot(latex, rest_r, la0, std::exp(mid), rho_g);
-        if (s && s->samples.back().r > neck_r)
-            lo = mid;
-        else
-            hi = mid;
+    // 60 halvings of the apex curvature; `depth` of them at a time read shots run together, all
+    // 2^depth - 1 midpoints the next `depth` halvings can reach.
+    int depth = 1;
+    while ((2u << depth) - 1 <= width) depth++;
+    for (int i = 0; i < 60;) {
+        const int k = std::min(depth, 60 - i);
+        std::vector<std::pair<double, double>> tree(size_t(1) << k);
+        std::vector<Shots::X> mids;
+        tree[1] = {lo, hi};
+        for (size_t j = 1; j < tree.size(); j++) {
+            double mid = 0.5 * (tree[j].first + tree[j].second);
+            mids.push_back({la0, mid});
+            if (2 * j < tree.size()) tree[2 * j] = {tree[j].first, mid}, tree[2 * j + 1] = {mid, tree[j].second};
+        }
+        shots.ahead(mids);
+        for (int m = 0; m < k; m++, i++) {
+            double mid = 0.5 * (lo + hi);
+            const Shots::End& s = shots.get({la0, mid});
+            if (s.ok && s.r > neck_r)
+                lo = mid;
+            else
+                hi = mid;
+        }
     }
     std::array<double, 2> x = {la0, lo};
-    auto s0 = shoot(latex, rest_r, x[0], std::exp(x[1]), rho_g);
-    if (!s0) {
+    if (!shots.get(x).ok) {
         err = "balloon doesn't inflate";
         return false;
     }
-    double v = std::log(s0->volume);
+    double v = std::log(shots.get(x).volume);
     std::array<double, 2> prev = x;
     size_t n_inc = (size_t)std::max(std::ceil(std::fabs(std::log(volume) - v) / 0.05), 1.0);
     double inc = (std::log(volume) - v) / (double)n_inc;
+    const double e = 1e-6;
     for (size_t step = 0; step < n_inc; step++) {
         double target = v + inc;
         std::array<double, 2> y = step > 0 ? std::array<double, 2>{2.0 * x[0] - prev[0], 2.0 * x[1] - prev[1]} : x;
         bool done = false;
         for (int it = 0; it < 30; it++) {
+            shots.ahead({y, {y[0] + e, y[1]}, {y[0], y[1] + e}});
             auto f = miss(y, target);
             if (!f) break;
             double norm = std::hypot((*f)[0], (*f)[1]);
@@ -277,7 +472,6 @@ bool inflate_solve(const Latex& latex, double rest_r, double volume, double rho_
                 done = true;
                 break;
             }
-            double e = 1e-6;
             auto fa = miss({y[0] + e, y[1]}, target);
             auto fb = miss({y[0], y[1] + e}, target);
             if (!fa || !fb) break;
@@ -286,16 +480,31 @@ bool inflate_solve(const Latex& latex, double rest_r, double volume, double rho_
             double det = j00 * j11 - j01 * j10;
             double d0 = (-(*f)[0] * j11 + (*f)[1] * j01) / det;
             double d1 = (-(*f)[1] * j00 + (*f)[0] * j10) / det;
+            // Ahead: the full Newton step with the Jacobian around it; if the full step converges,
+            // the first shots of the next continuation step (extrapolated from it); shorter steps
+            // of the line search with what room is left.
+            const std::array<double, 2> c1 = {y[0] + 1.0 * d0, y[1] + 1.0 * d1};
+            std::vector<Shots::X> next = {c1, {c1[0] + e, c1[1]}, {c1[0], c1[1] + e}};
+            if (step + 1 < n_inc) {
+                const Shots::X y2 = {2.0 * c1[0] - x[0], 2.0 * c1[1] - x[1]};
+                next.insert(next.end(), {y2, {y2[0] + e, y2[1]}, {y2[0], y2[1] + e}});
+            }
+            for (double a = 0.5; a > 1e-4 && next.size() < width; a *= 0.5) next.push_back({y[0] + a * d0, y[1] + a * d1});
+            shots.ahead(next);
             double a = 1.0;
+            bool moved = false;
             while (a > 1e-4) {
                 std::array<double, 2> c = {y[0] + a * d0, y[1] + a * d1};
                 auto g = miss(c, target);
                 if (g && std::hypot((*g)[0], (*g)[1]) < norm) {
                     y = c;
+                    moved = true;
                     break;
                 }
                 a *= 0.5;
             }
+            // Where the line search finds nothing, every later iteration repeats this one exactly.
+            if (!moved) break;
         }
         if (!done) {
             char buf[128];
@@ -1328,7 +1537,7 @@ void World::shape_sections() {
     }
 }
 
-std::vector<uint8_t> serialize(const World& w) {
+size_t serialize_into(const World& w, void* out) {
     ntr_world_header h = w.h;
     size_t off = (sizeof(ntr_world_header) + 255) & ~size_t(255);
     for (int s = 0; s < NTR_SEC_COUNT; s++) {
@@ -1336,10 +1545,22 @@ std::vector<uint8_t> serialize(const World& w) {
         h.bytes[s] = w.sec[s].size();
         off += (w.sec[s].size() + 255) & ~size_t(255);
     }
-    std::vector<uint8_t> out(off, 0);
-    std::memcpy(out.data(), &h, sizeof h);
-    for (int s = 0; s < NTR_SEC_COUNT; s++)
-        if (!w.sec[s].empty()) std::memcpy(out.data() + h.offset[s], w.sec[s].data(), w.sec[s].size());
+    if (!out) return off;
+    uint8_t* b = static_cast<uint8_t*>(out);
+    std::memcpy(b, &h, sizeof h);
+    size_t end = sizeof h;  // everything before `end` is written; the gaps are zeroed
+    for (int s = 0; s < NTR_SEC_COUNT; s++) {
+        std::memset(b + end, 0, h.offset[s] - end);
+        if (!w.sec[s].empty()) std::memcpy(b + h.offset[s], w.sec[s].data(), w.sec[s].size());
+        end = h.offset[s] + w.sec[s].size();
+    }
+    std::memset(b + end, 0, off - end);
+    return off;
+}
+
+std::vector<uint8_t> serialize(const World& w) {
+    std::vector<uint8_t> out(serialize_into(w, nullptr));
+    serialize_into(w, out.data());
     return out;
 }
 

@@ -31,6 +31,8 @@ struct World {
 };
 
 std::vector<uint8_t> serialize(const World& w);
+// Writes the blob into `out` (when not null) and returns its size in bytes.
+size_t serialize_into(const World& w, void* out);
 // Returns false with a message on a malformed blob.
 bool deserialize(const void* blob, size_t len, World& w, std::string& err);
 

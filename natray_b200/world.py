@@ -76,8 +76,8 @@ def sized_for(n_particles: int, diameter_cm: float = 16.0) -> int:
 class World:
     """A world blob and numpy views of its header and sections."""
 
-    def __init__(self, blob: bytes):
-        self.blob = bytearray(blob)
+    def __init__(self, blob: bytes | bytearray, copy: bool = True):
+        self.blob = blob if not copy and isinstance(blob, bytearray) else bytearray(blob)
         self.h = _abi.WorldHeader.from_buffer_copy(bytes(self.blob[: C.sizeof(_abi.WorldHeader)]))
         if self.h.magic != _abi.WORLD_MAGIC:
             raise ValueError("not a world blob")
@@ -117,10 +117,11 @@ def build_world(params: Params) -> World:
     n = C.c_size_t()
     check(lib().ntr_world_build(C.byref(params.c), C.byref(p), C.byref(n)))
     try:
-        blob = C.string_at(p, n.value)
+        blob = bytearray(n.value)  # one copy, out of the library's buffer
+        C.memmove((C.c_char * n.value).from_buffer(blob), p, n.value)
     finally:
         lib().ntr_free(p)
-    return World(blob)
+    return World(blob, copy=False)
 
 
 __all__ = ["Params", "World", "build_world", "sized_for", "SECTIONS"]

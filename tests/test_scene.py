@@ -151,3 +151,34 @@ def test_fixed_step_configs_build():
     w = build_world(p)
     assert 60000 < w.h.n_particles < 80000 and w.h.n_tris == 5120
     assert abs(w.h.params.fluid[2] - 2e-6) < 1e-12
+
+
+_PROFILE_BITS = """
+import ctypes as C, hashlib, math, sys
+sys.path.insert(0, sys.argv[1])
+from natray_b200._abi import Profile, check, lib
+h = hashlib.sha256()
+for d, g in ((0.065, 9.81), (0.16, 9.81), (0.12, 0.0)):
+    p = Profile()
+    check(lib().ntr_inflate(0.42e6, 0.25e-3, 0.03, math.pi / 6.0 * d ** 3, 1000.0 * g, C.byref(p)))
+    h.update(bytes(p))
+print(h.hexdigest())
+"""
+
+
+def test_inflation_on_threads_is_bit_identical_to_one_by_one():
+    # The search runs its likely next shots together on a pool; with NATRAY_BUILD_THREADS=1 it
+    # runs them one at a time in the reference's order. The profiles must agree to the bit.
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    root = str(Path(__file__).resolve().parents[1])
+    out = []
+    for n in ("1", "8"):
+        env = dict(os.environ, NATRAY_BUILD_THREADS=n)
+        r = subprocess.run([sys.executable, "-c", _PROFILE_BITS, root], env=env, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        out.append(r.stdout.strip())
+    assert out[0] == out[1] and len(out[0]) == 64
