@@ -115,9 +115,11 @@ __device__ __forceinline__ Gathered gather(const float* tg, V3 X, V3 o, I3 corne
     return r;
 }
 
-constexpr int G2P_T = 256;
+// 128 threads a CTA, 6 CTAs an SM: a block's few hundred particles take 3 rounds with a short
+// last one, and the SM has more CTAs to switch to while one waits on its loads or barriers.
+constexpr int G2P_T = 128;
 
-__global__ void __launch_bounds__(G2P_T, 3) k_g2p(Dev D) {
+__global__ void __launch_bounds__(G2P_T, 6) k_g2p(Dev D) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
@@ -133,6 +135,7 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Dev D) {
     const uint32_t step_no = st->s.step;
     __shared__ float tg[8 * TILE];
     __shared__ uint32_t links[27];
+    __shared__ uint8_t s_cov[64];  // the block's own cells: rubber over them (A_MA > 0)
     __shared__ uint32_t s_wcount[G2P_T / 32];
     __shared__ uint32_t s_brk;
     float fastest = 0.0f;
@@ -145,6 +148,7 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Dev D) {
             continue;
         }
         if (threadIdx.x < 27) links[threadIdx.x] = D.block_nb[b * 27u + threadIdx.x];
+        if (threadIdx.x < 64) s_cov[threadIdx.x] = accv(D, A_MA, b * 64u + threadIdx.x) > 0 ? 1 : 0;
         if (threadIdx.x == 0) s_brk = 0;
         __syncthreads();
         for (uint32_t t = threadIdx.x; t < TILE; t += G2P_T) {
@@ -187,9 +191,16 @@ __global__ void __launch_bounds__(G2P_T, 3) k_g2p(Dev D) {
                 bool escaped = x.x < lo.x || x.z < lo.z || x.x > hi.x || x.z > hi.z || x.y > hi.y;
                 float fill = m_near / 24.0f;
                 bool on_ground = x.y < 1.5f * spacing;
-                I3 oc = vi(vfloor(X)) - corner;
-                uint32_t own_t = tile_cell(links, (uint32_t)oc.x * 49u + (uint32_t)oc.y * 7u + (uint32_t)oc.z);
-                bool covered = own_t != NONE && accv(D, A_MA, own_t) > 0;
+                // The particle's own cell, in this block (tile coordinates 1-4) as a rule: its rubber
+                // flag is in shared memory; elsewhere it is looked up.
+                const I3 oc = vi(vfloor(X)) - corner;
+                bool covered;
+                if ((uint32_t)(oc.x - 1) < 4u && (uint32_t)(oc.y - 1) < 4u && (uint32_t)(oc.z - 1) < 4u) {
+                    covered = s_cov[(oc.x - 1) * 16 + (oc.y - 1) * 4 + (oc.z - 1)] != 0;
+                } else {
+                    const uint32_t own_t = tile_cell(links, (uint32_t)oc.x * 49u + (uint32_t)oc.y * 7u + (uint32_t)oc.z);
+                    covered = own_t != NONE && accv(D, A_MA, own_t) > 0;
+                }
                 float thin_age = (fill < 0.45f && !on_ground && !covered) ? c1w + step : 0.0f;
                 if (escaped || (!covered && fill < 0.2f) || thin_age > t_thin) {
                     if (on_ground) {
