@@ -147,6 +147,16 @@ __global__ void __launch_bounds__(G2P_T, 6) k_g2p(Dev D) {
             if (threadIdx.x == 0) D.brk_count[b] = 0;
             continue;
         }
+        // This thread's particle of the first round, loaded before the tile so that the two
+        // waits overlap; each round then loads the next round's particle before its gathers.
+        uint32_t i_next = 0u;
+        float4 pos_next = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        float c1w_next = 0.0f;
+        if (threadIdx.x < count) {
+            i_next = D.sorted[first + threadIdx.x];
+            pos_next = D.pos[i_next];
+            c1w_next = D.c1[i_next].w;
+        }
         if (threadIdx.x < 27) links[threadIdx.x] = D.block_nb[b * 27u + threadIdx.x];
         if (threadIdx.x < 64) s_cov[threadIdx.x] = accv(D, A_MA, b * 64u + threadIdx.x) > 0 ? 1 : 0;
         if (threadIdx.x == 0) s_brk = 0;
@@ -169,16 +179,21 @@ __global__ void __launch_bounds__(G2P_T, 6) k_g2p(Dev D) {
         }
         __syncthreads();
         const I3 corner = slot_coord(g, g.list[b]) * 4 - I3{1, 1, 1};
-        // Rounds of 256 particles keep the sorted order for ranking the break-ups.
+        // Rounds of G2P_T particles keep the sorted order for ranking the break-ups.
         for (uint32_t base = 0; base < count; base += G2P_T) {
             const uint32_t k = base + threadIdx.x;
             bool brk = false;
             V3 bx = {0.0f, 0.0f, 0.0f}, bv = bx;
             uint32_t bid = 0;
+            const uint32_t i = i_next;
+            const float4 pos = pos_next;
+            const float c1w = c1w_next;
+            if (k + G2P_T < count) {
+                i_next = D.sorted[first + k + G2P_T];
+                pos_next = D.pos[i_next];
+                c1w_next = D.c1[i_next].w;
+            }
             if (k < count) {
-                const uint32_t i = D.sorted[first + k];
-                const float4 pos = D.pos[i];
-                const float c1w = D.c1[i].w;
                 V3 X = (xyz(pos) - g.org) / hh;
                 Gathered gu = gather(tg, X, v3(0.0f, 0.5f, 0.5f), corner, 0, 1, hh);
                 Gathered gv = gather(tg, X, v3(0.5f, 0.0f, 0.5f), corner, 2, 3, hh);
