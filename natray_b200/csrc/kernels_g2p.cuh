@@ -108,8 +108,11 @@ __device__ __forceinline__ Gathered gather(const float* tg, V3 X, V3 o, I3 corne
                 uint32_t t = t0 + a * 49u + b * 7u + c;
                 float u = weight * tg[fa * TILE + t];
                 r.s += u;
-                r.g = r.g + u * (v3((float)a, (float)b, (float)c) - fx);
-                r.w += weight * tg[fw * TILE + t];
+                // The gradient's and the weight's sums are fused multiply-adds (the oracle's
+                // gather does the same), one rounding a term instead of two.
+                const V3 d = v3((float)a, (float)b, (float)c) - fx;
+                r.g = {__fmaf_rn(u, d.x, r.g.x), __fmaf_rn(u, d.y, r.g.y), __fmaf_rn(u, d.z, r.g.z)};
+                r.w = __fmaf_rn(weight, tg[fw * TILE + t], r.w);
             }
     r.g = r.g * hh;
     return r;

@@ -2405,8 +2405,10 @@ void Sim<R>::g2p() {
                                 uint32_t t = t0 + a * 49u + bq * 7u + c;
                                 R u = weight * tg[fa * TILE + t];
                                 r.s += u;
-                                r.g = r.g + u * (v3(R(a), R(bq), R(c)) - fx);
-                                r.w += weight * tg[fw * TILE + t];
+                                // Fused multiply-adds, as the CUDA gather.
+                                V3<R> d = v3(R(a), R(bq), R(c)) - fx;
+                                r.g = {std::fma(u, d.x, r.g.x), std::fma(u, d.y, r.g.y), std::fma(u, d.z, r.g.z)};
+                                r.w = std::fma(weight, tg[fw * TILE + t], r.w);
                             }
                     r.g = r.g * hh;
                     return r;
