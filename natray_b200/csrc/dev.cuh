@@ -120,6 +120,7 @@ struct Dev {
     float* mem_mass;
     const Tri* tris;
     uint32_t *alive, *vtri_off, *vtri;
+    uint8_t* vtri_c;  // per entry of vtri: which corner (0-2) of the triangle the vertex is
     float4* tri_rec;  // per triangle: what its vertices fold into their force sums, 4 float4
     DBullet* bullets;
     const float4* patches;

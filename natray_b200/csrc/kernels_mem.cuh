@@ -52,12 +52,16 @@ struct VertexForce {
 };
 
 // The rubber's triangles, once per substep (membrane.wgsl:67-149, the part of vertex_force that
-// does not depend on which of its vertices asks): the stretch, the Ogden stresses, and what the
-// vertices fold into their sums. One thread per triangle, so the stresses are computed once
-// instead of once per vertex. Per triangle four float4 in `tri_rec`:
-//   {h1, vol}, {h2, tangent + sx}, {e1 x e2, |e1 x e2| / 6}, {rest / 3, tension, reach, kind}
-// with kind 0: dead at the start of the substep (not counted), 1: tore now (counts for the
-// reach only), 2: counted.
+// does not depend on which of its vertices asks): the stretch, the Ogden stresses, and what each
+// of its three vertices folds into its sums. One thread per triangle, so the stresses are
+// computed once instead of once per vertex. Per triangle five float4 in `tri_rec`:
+//   {-(h1 + h2), stiffness at v0}, {h1, at v1}, {h2, at v2}, {e1 x e2, |e1 x e2| / 6},
+//   {rest / 3, tension, reach, kind}
+// with the stiffness at a corner vol * (gx^2 + gy^2) * (tangent + sx), (gx, gy) the corner's
+// shape gradient, and kind 0: dead at the start of the substep (not counted), 1: tore now
+// (counts for the reach only), 2: counted. A vertex adds its corner's record, so it reads two
+// records of each of its triangles at once, with no dependent lookups (the corner comes from
+// `vtri_c`); adding -(h1 + h2) is the same as subtracting h1 + h2.
 //
 // `alive` holds the state at the start of the substep until this kernel writes the tears, and
 // the vertices read the kind, so every vertex of a triangle sees the same thing. The reference
@@ -68,9 +72,9 @@ __global__ void k_mem_tri(Dev D, int par) {
     const float4* X = D.mem_x[par];
     const float thick0 = U->rubber[3];
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < D.Nt; t += gridDim.x * blockDim.x) {
-        float4* rec = D.tri_rec + 4 * (size_t)t;
+        float4* rec = D.tri_rec + 5 * (size_t)t;
         if (D.alive[t] == 0u) {
-            rec[3] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(0u));
+            rec[4] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(0u));
             continue;
         }
         const Tri tri = D.tris[t];
@@ -87,7 +91,7 @@ __global__ void k_mem_tri(Dev D, int par) {
         float lx = sqrtf(mid + dev), ly = sqrtf(mx(mid - dev, 1e-12f));
         if (lx >= U->rubber2[1]) {
             D.alive[t] = 0u;
-            rec[3] = make_float4(0.0f, 0.0f, reach, __uint_as_float(1u));
+            rec[4] = make_float4(0.0f, 0.0f, reach, __uint_as_float(1u));
             continue;
         }
         Sheet sh = sheet(U, lx, ly);
@@ -112,46 +116,59 @@ __global__ void k_mem_tri(Dev D, int par) {
         V3 h1 = (-vol) * (p0 * mxx + p1 * myy);
         V3 h2 = (-vol) * (p0 * mzz + p1 * mww);
         V3 cr = cross(e1, e2);
-        rec[0] = f4(h1, vol);
-        rec[1] = f4(h2, sh.tangent + sx);
-        rec[2] = f4(cr, length(cr) / 6.0f);
-        rec[3] = make_float4(tri.rest_area / 3.0f, sh.sx * thick0 / (lx * ly), reach, __uint_as_float(2u));
+        const float tan_sx = sh.tangent + sx;
+        auto stiff = [&](float gx, float gy) { return vol * (gx * gx + gy * gy) * tan_sx; };
+        rec[0] = f4(-(h1 + h2), stiff(-(mxx + mzz), -(myy + mww)));
+        rec[1] = f4(h1, stiff(mxx, myy));
+        rec[2] = f4(h2, stiff(mzz, mww));
+        rec[3] = f4(cr, length(cr) / 6.0f);
+        rec[4] = make_float4(tri.rest_area / 3.0f, sh.sx * thick0 / (lx * ly), reach, __uint_as_float(2u));
     }
 }
 
 // vertex_force (membrane.wgsl:67-149): the vertex's triangles' records, folded in its order.
+// Eight triangles at a time: their indices and corners, then their records, each group of
+// loads issued together; the sums then run in the vertex's order.
+constexpr uint32_t VF_BATCH = 8;
+
 __device__ VertexForce vertex_force(const Dev& D, uint32_t i) {
     const float thick0 = D.U->rubber[3];
     VertexForce o = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, 0.0f, 0.0f, 0.0f, 0.0f, thick0};
     float rest = 0.0f;
     const uint32_t k0 = D.vtri_off[i], k1 = D.vtri_off[i + 1];
-    for (uint32_t k = k0; k < k1; k++) {
-        const uint32_t t = D.vtri[k];
-        const float4* rec = D.tri_rec + 4 * (size_t)t;
-        const float4 r3 = rec[3];
-        const uint32_t kind = __float_as_uint(r3.w);
-        if (kind == 0u) continue;
-        o.reach = mx(o.reach, r3.z);
-        if (kind == 1u) continue;
-        const Tri tri = D.tris[t];
-        const float4 r0 = rec[0], r1 = rec[1], r2 = rec[2];
-        const float mxx = tri.dm_inv.x, myy = tri.dm_inv.y, mzz = tri.dm_inv.z, mww = tri.dm_inv.w;
-        const V3 h1 = xyz(r0), h2 = xyz(r1);
-        float gx = mxx, gy = myy;
-        if (i == tri.v0) {
-            o.f = o.f - (h1 + h2);
-            gx = -(mxx + mzz), gy = -(myy + mww);
-        } else if (i == tri.v1) {
-            o.f = o.f + h1;
-        } else {
-            o.f = o.f + h2;
-            gx = mzz, gy = mww;
+    for (uint32_t kb = k0; kb < k1; kb += VF_BATCH) {
+        uint32_t t[VF_BATCH], c[VF_BATCH];
+#pragma unroll
+        for (uint32_t j = 0; j < VF_BATCH; j++) {
+            const bool in = kb + j < k1;
+            t[j] = in ? D.vtri[kb + j] : 0u;
+            c[j] = in ? (uint32_t)D.vtri_c[kb + j] : 0u;
         }
-        o.n = o.n + xyz(r2);
-        o.area += r2.w;
-        rest += r3.x;
-        o.stiff += r0.w * (gx * gx + gy * gy) * r1.w;
-        o.tension = mx(o.tension, r3.y);
+        float4 own[VF_BATCH], nrm[VF_BATCH], info[VF_BATCH];
+#pragma unroll
+        for (uint32_t j = 0; j < VF_BATCH; j++) {
+            own[j] = nrm[j] = info[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (kb + j < k1) {
+                const float4* rec = D.tri_rec + 5 * (size_t)t[j];
+                own[j] = rec[c[j]];
+                nrm[j] = rec[3];
+                info[j] = rec[4];
+            }
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < VF_BATCH; j++) {
+            if (kb + j >= k1) break;
+            const uint32_t kind = __float_as_uint(info[j].w);
+            if (kind == 0u) continue;
+            o.reach = mx(o.reach, info[j].z);
+            if (kind == 1u) continue;
+            o.f = o.f + xyz(own[j]);
+            o.n = o.n + xyz(nrm[j]);
+            o.area += nrm[j].w;
+            rest += info[j].x;
+            o.stiff += own[j].w;
+            o.tension = mx(o.tension, info[j].y);
+        }
     }
     if (o.area > 0.0f) o.thick = thick0 * rest / o.area;
     return o;

@@ -214,9 +214,10 @@ static ntr_status allocate(Sim& S) {
     AL(tris, D.Nt);
     D.tris = tris;
     AL(D.alive, D.Nt);
-    AL(D.tri_rec, (size_t)D.Nt * 4);
+    AL(D.tri_rec, (size_t)D.Nt * 5);
     AL(D.vtri_off, D.Nv + 1);
     AL(D.vtri, h.n_vtri);
+    AL(D.vtri_c, h.n_vtri);
     AL(D.bullets, NTR_MAX_SHOTS);
     float4* pat;
     AL(pat, NTR_MAX_SHOTS * NTR_MAX_PATCHES * 2);
@@ -326,6 +327,21 @@ static ntr_status upload_static(Sim& S, const World& w) {
     CU(cudaMemcpy((void*)D.tris, w.sec[NTR_SEC_TRIS].data(), (size_t)D.Nt * 32, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(D.vtri_off, w.sec[NTR_SEC_VTRI_OFF].data(), ((size_t)D.Nv + 1) * 4, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(D.vtri, w.sec[NTR_SEC_VTRI].data(), w.sec[NTR_SEC_VTRI].size(), cudaMemcpyHostToDevice));
+    {
+        // Which corner of each of its triangles a vertex is: the first of v0, v1, v2 that it
+        // equals (the order in which membrane.wgsl's vertex_force tests them).
+        const uint32_t* off = w.as<uint32_t>(NTR_SEC_VTRI_OFF);
+        const uint32_t* vt = w.as<uint32_t>(NTR_SEC_VTRI);
+        const Tri* tr = w.as<Tri>(NTR_SEC_TRIS);
+        const size_t n_vt = w.sec[NTR_SEC_VTRI].size() / 4;
+        std::vector<uint8_t> corner(n_vt, 2);
+        for (uint32_t i = 0; i < D.Nv; i++)
+            for (uint32_t k = off[i]; k < off[i + 1] && k < n_vt; k++) {
+                const uint32_t t = vt[k];
+                if (t < D.Nt) corner[k] = tr[t].v0 == i ? 0 : tr[t].v1 == i ? 1 : 2;
+            }
+        if (n_vt) CU(cudaMemcpy(D.vtri_c, corner.data(), n_vt, cudaMemcpyHostToDevice));
+    }
     CU(cudaMemcpy(D.mem_mass, w.sec[NTR_SEC_MEM_MASS].data(), (size_t)D.Nv * 4, cudaMemcpyHostToDevice));
     CU(cudaMemcpy((void*)D.patches, w.sec[NTR_SEC_PATCHES].data(), w.sec[NTR_SEC_PATCHES].size(), cudaMemcpyHostToDevice));
     CU(cudaMemcpy((void*)D.outlines, w.sec[NTR_SEC_OUTLINES].data(), w.sec[NTR_SEC_OUTLINES].size(), cudaMemcpyHostToDevice));
