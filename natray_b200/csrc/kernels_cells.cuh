@@ -494,12 +494,11 @@ __global__ void k_mem_sample(Dev D) {
     float r = 0.0f;
     if (act) {
         V3 x = (xyz(D.mem_x[0][i]) - g.org) / g.h;
-        if (q < 3u) {
-            float2 s = sample_grid(D, g, x - lattice_offset(q), F_U + q, a_wt(q));
-            r = s.y > 1e-6f ? s.x / s.y : 0.0f;
-        } else {
-            r = sample_grid(D, g, x - 0.5f, F_TYPE, A_WC).y / 8.0f;
-        }
+        // One call for the four lanes of a vertex (three face lattices and the fill, whose
+        // lattice offset is 0.5 on every axis), so that they do not run one after the other.
+        const bool fill = q == 3u;
+        const float2 s = sample_grid(D, g, x - lattice_offset(q), fill ? (uint32_t)F_TYPE : F_U + q, fill ? (uint32_t)A_WC : a_wt(q));
+        r = fill ? s.y / 8.0f : (s.y > 1e-6f ? s.x / s.y : 0.0f);
     }
     const int l0 = (int)(threadIdx.x & 28u);
     const float v0 = __shfl_sync(0xffffffffu, r, l0), v1 = __shfl_sync(0xffffffffu, r, l0 + 1);
