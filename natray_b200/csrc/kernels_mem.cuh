@@ -728,18 +728,11 @@ __global__ void __launch_bounds__(256) k_bullet_finish(Dev D) {
             D.sections[bi * NTR_N_SEC + info.w % NTR_N_SEC] = s;
             info.w += 1u;
         }
-        float reach = 0.0f;
-        for (uint32_t k = 0; k < NTR_N_SEC; k++) {
-            const DSection s = D.sections[bi * NTR_N_SEC + k];
-            if (s.b.w <= 0.0f || section_r2(s, t_end) >= hand2) continue;
-            reach = mx(reach, mx(length(xyz(s.a) - x), length(xyz(s.b) - x)));
-        }
         DBullet& o = D.bullets[bi];
         o.x = f4(x, b.x.w);
         o.v = f4(v, roll);
         o.q = q;
         o.l = f4(l, pace);
-        o.reach = f4(x, reach > 0.0f ? reach + R_HAND * hh : 0.0f);
         o.info = info;
         float4* e = D.pose_log + (bi * NTR_LOG_CAP + st->s.step % NTR_LOG_CAP) * 3;
         e[0] = f4(x, __uint_as_float(st->s.t_ns));
@@ -747,6 +740,19 @@ __global__ void __launch_bounds__(256) k_bullet_finish(Dev D) {
         e[2] = f4(v, roll);
     }
     __syncthreads();
+    // The reach of the open sections around the new position: a lane per section (with the one
+    // opened above), then the largest. A maximum of lengths (none negative; a NaN one is passed
+    // over, as by the reference's running maximum) does not depend on the order.
+    if (li < 32u) {
+        static_assert(NTR_N_SEC == 32, "one lane per section");
+        const DSection s = D.sections[bi * NTR_N_SEC + li];
+        float r = 0.0f;
+        if (!(s.b.w <= 0.0f || section_r2(s, t_end) >= hand2)) r = mx(length(xyz(s.a) - x), length(xyz(s.b) - x));
+        if (!(r >= 0.0f)) r = 0.0f;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r = mx(r, __shfl_xor_sync(0xffffffffu, r, o));
+        if (li == 0) D.bullets[bi].reach = f4(x, r > 0.0f ? r + R_HAND * hh : 0.0f);
+    }
     // Sections thinner than the grid push the water out of the way as they open.
     if (li < NTR_N_SEC) {
         const DSection s = D.sections[bi * NTR_N_SEC + li];
