@@ -315,6 +315,14 @@ __global__ void k_extend_1(Dev D) {
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
     CELL_LOOP(D, st) {
+        // A water cell has all three of its faces set (face_set at offset 0 is true on every
+        // axis): it keeps its velocities and needs nothing around it.
+        if (cfv(D, F_TYPE, cell) == WATER_T) {
+#pragma unroll
+            for (int d = 0; d < 3; d++) *cfp(D, F_EXT + d, cell) = cfv(D, F_U + d, cell);
+            *cfp(D, F_EXT_SET, cell) = 7.0f;
+            continue;
+        }
         // Types of the 3^3 cells around (GAS outside the grid), of the cells two down each axis,
         // and the face velocities of the cell and its six neighbours.
         uint32_t nc[27], n2[3];
@@ -376,13 +384,23 @@ __global__ void k_extend_2(Dev D) {
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
     CELL_LOOP(D, st) {
+        const float ty = cfv(D, F_TYPE, cell);
+        const uint32_t set = f2u(cfv(D, F_EXT_SET, cell));
+        // All three faces set (water cells among them): each takes its extended value, bounded
+        // by the types of the cell and the one below it; the neighbours' values are not needed.
+        if (set == 7u) {
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const uint32_t lo = neighbour(g, cell, ed((uint32_t)d, -1));
+                *cfp(D, F_U + d, cell) = bounded(cfv(D, F_EXT + d, cell), ty, lo != NONE ? cfv(D, F_TYPE, lo) : GAS_T);
+            }
+            continue;
+        }
         uint32_t nb[6], lo[3];
 #pragma unroll
         for (int j = 0; j < 6; j++) nb[j] = neighbour(g, cell, e6(j));
 #pragma unroll
         for (int d = 0; d < 3; d++) lo[d] = nb[2 * d];  // e6 order: -x, +x, -y, +y, -z, +z
-        const float ty = cfv(D, F_TYPE, cell);
-        const uint32_t set = f2u(cfv(D, F_EXT_SET, cell));
         float uo[3], eo[3], tlo[3], en[6][3];
         uint32_t sn[6];
 #pragma unroll
@@ -515,24 +533,25 @@ __global__ void __launch_bounds__(256) k_air_substep(Dev D, int par) {
     const float k = dt_of(st) / (float)max(D.U->mem[2], 1u) / hh;
     float lim = BIG_F;
     CELL_LOOP(D, st) {
-        // The cell's and its six neighbours' types and gas are loaded first, all in flight
-        // together (a missing neighbour loads this cell's and is not used).
+        // A cell that is not gas only carries its gas over (most cells of the active blocks are
+        // water). A gas cell loads its six neighbours' types and gas, all in flight together (a
+        // missing neighbour loads this cell's and is not used).
+        const float ty = cfv(D, F_TYPE, cell);
+        Gas gg = read_gas(D, par, cell);
+        if (ty != GAS_T) {
+            write_gas(D, 1 - par, cell, gg);
+            continue;
+        }
         uint32_t nbr[6];
         float nty[6];
         Gas ng[6];
 #pragma unroll
         for (int j = 0; j < 6; j++) nbr[j] = neighbour(g, cell, ed((uint32_t)(j >> 1), (j & 1) ? 1 : -1));
-        const float ty = cfv(D, F_TYPE, cell);
-        Gas gg = read_gas(D, par, cell);
 #pragma unroll
         for (int j = 0; j < 6; j++) {
             const uint32_t at = nbr[j] != NONE ? nbr[j] : cell;
             nty[j] = cfv(D, F_TYPE, at);
             ng[j] = read_gas(D, par, at);
-        }
-        if (ty != GAS_T) {
-            write_gas(D, 1 - par, cell, gg);
-            continue;
         }
         Gas f = no_gas();
 #pragma unroll
