@@ -179,9 +179,8 @@ struct Near {
 };
 
 // The nearest point of bullet `bi`'s outline to q = (z, r) of its body frame
-// (bullet.wgsl:438-472).
-__device__ Near nearest_surface(const Dev& D, uint32_t bi, float qx, float qy) {
-    const float2* ol = D.outlines + bi * NTR_OUTLINE;
+// (bullet.wgsl:438-472). `ol` is the bullet's outline (in shared memory).
+__device__ Near nearest_surface(const float2* __restrict__ ol, float qx, float qy) {
     float2 first = ol[0], last = ol[NTR_OUTLINE - 1];
     Near o = {qx, qy, 0.0f, 0.0f, 0.0f};
     float best = BIG_F;
@@ -217,130 +216,280 @@ __device__ Near nearest_surface(const Dev& D, uint32_t bi, float qx, float qy) {
     return o;
 }
 
-__device__ float rubber_contact(const Dev& D, int par, uint32_t i, V3& x, V3& v, float m, V3 load, const VertexForce& vf, bool wet, bool& held,
-                                float t, float sub, float now, float dt) {
+// The response to the best sample (bullet.wgsl:426-611): the rubber pushed out of the bullet and
+// slowed along it, the impulses and, for a held wet vertex, the wetted-side sums into the
+// bullet's fixed-point sums.
+__device__ __forceinline__ void contact_response(const Dev& D, uint32_t bi, V3& x, V3& v, float m, V3 load, const VertexForce& vf, bool wet, bool& held,
+                                                 float sub, V3 xb, float best, V3 on_b, V3 gap, V3 nrm, V3 rel, float share) {
+    float vn = dot(rel, nrm);
+    V3 rel_t = rel - vn * nrm;
+    float slide = length(rel_t);
+    float dvn = 0.0f, jn = 0.0f;
+    V3 j = {0.0f, 0.0f, 0.0f};
+    bool holds = false;
+    if (!wet) {
+        dvn = mx(-vn, 0.0f);
+        jn = m * dvn;
+        j = -m * share * dvn * nrm;
+    } else {
+        float ln = dot(load, nrm);
+        if (ln < 0.0f) {
+            dvn = -vn;
+            jn = -ln * sub;
+            j = mn(share, 1.0f) * ln * sub * nrm;
+            holds = true;
+            held = true;
+        } else if (best > 0.0f) {
+            dvn = mx(-vn, 0.0f);
+        } else {
+            return;
+        }
+    }
+    float stop = (slide > 1e-9f && m > 0.0f) ? mn(1.0f, MU_JACKET * jn / (m * slide)) : 0.0f;
+    V3 dvt = -share * stop * rel_t;
+    x = x + (share * gap + sub * dvt);
+    v = v + (share * dvn * nrm + dvt);
+    j = j - m * dvt;
+    float nl = length(vf.n);
+    int32_t* hit = D.bullet_hit + bi * NTR_HIT_FIELDS;
+    if (holds && nl > 0.0f) {
+        float a = vf.area * 1e6f;
+        V3 sx = (x - xb) * 1e3f * a;
+        for (int c = 0; c < 3; c++) {
+            atomicAdd(hit + 6 + c, to_fp(vf.n[c] / nl * a, FP_A));
+            atomicAdd(hit + 9 + c, to_fp(sx[c], FP_X));
+        }
+        atomicAdd(hit + 12, to_fp(a, FP_A));
+    }
+    V3 jl = cross(on_b, j);
+    for (int c = 0; c < 3; c++) {
+        atomicAdd(hit + c, to_fp(j[c], FP_J));
+        atomicAdd(hit + 3 + c, to_fp(jl[c], FP_L));
+    }
+}
+
+// A triangle of vertex i's contact search (or, for k == k1, the vertex alone): its corners as
+// they will be after the substep, their velocities, which corner i is, and its subdivision.
+struct ContactTri {
+    V3 p[3], pv[3];
+    uint32_t own, n;
+    bool ok;
+};
+
+__device__ __forceinline__ ContactTri contact_tri(const Dev& D, int par, uint32_t i, uint32_t k, uint32_t k1, V3 x, V3 v, float sub, float hull) {
     const float4* MX = D.mem_x[par];
     const float4* MV = D.mem_v[par];
+    ContactTri t;
+    for (int c = 0; c < 3; c++) t.p[c] = x, t.pv[c] = v;
+    t.own = 0, t.n = 1, t.ok = true;
+    if (k < k1) {
+        const uint32_t tn = D.vtri[k];
+        if (D.alive[tn] == 0u) {  // dead, or tore in this substep (k_mem_tri)
+            t.ok = false;
+            return t;
+        }
+        const Tri tri = D.tris[tn];
+        const uint32_t ids[3] = {tri.v0, tri.v1, tri.v2};
+        for (uint32_t c = 0; c < 3; c++) {
+            if (ids[c] == i) {
+                t.own = c;
+            } else {
+                t.pv[c] = xyz(MV[ids[c]]);
+                t.p[c] = xyz(MX[ids[c]]) + sub * t.pv[c];
+            }
+        }
+        const float longest = mx(distance(t.p[0], t.p[1]), mx(distance(t.p[1], t.p[2]), distance(t.p[2], t.p[0])));
+        t.n = f2u(clampf_(ceilf(longest / hull), 1.0f, 8.0f));
+    }
+    return t;
+}
+
+// Sample m of a triangle subdivided n times: barycentric (a, c, n - a - c) / n in the order
+// a = 0..n, c = 0..n - a.
+__device__ __forceinline__ void contact_sample_ac(uint32_t m, uint32_t n, uint32_t& a, uint32_t& c) {
+    a = 0;
+    while (m > n - a) m -= n - a + 1, a++;
+    c = m;
+}
+
+// What the search keeps of its best sample.
+struct ContactHit {
+    V3 on_b, gap, nrm, rel;
+    float share, depth;
+};
+
+// One sample against bullet `bi` (membrane.wgsl's contact search, bullet.wgsl:426-611): false if
+// it does not count (no weight on this vertex, or beyond the bullet's reach). With `hit`, also
+// what the response needs.
+__device__ __forceinline__ bool contact_sample(const float2* ol, const ContactTri& t, uint32_t a, uint32_t c, const DBullet& b, V3 xb,
+                                               float4 back, V3 w, float band, float& depth, ContactHit* hit) {
+    const uint32_t n = t.n;
+    V3 bary = v3((float)a, (float)c, (float)(n - a - c)) / (float)n;
+    float wi = bary[t.own];
+    if (wi <= 0.0f) return false;
+    V3 s = bary.x * t.p[0] + bary.y * t.p[1] + bary.z * t.p[2];
+    V3 r = s - xb;
+    if (length(r) >= b.shape.z + band) return false;
+    V3 q = qrot(back, r);
+    float rho = sqrtf(q.x * q.x + q.y * q.y);
+    Near nr = nearest_surface(ol, q.z, rho);
+    depth = nr.depth;
+    if (hit) {
+        float rx = 1.0f, ry = 0.0f;
+        if (rho > 1e-9f) rx = q.x / rho, ry = q.y / rho;
+        hit->depth = nr.depth;
+        hit->on_b = qrot(b.q, v3(rx * nr.ay, ry * nr.ay, nr.ax));
+        hit->gap = hit->on_b - r;
+        hit->nrm = qrot(b.q, v3(rx * nr.ny, ry * nr.ny, nr.nx));
+        hit->share = wi / dot(bary, bary);
+        hit->rel = bary.x * t.pv[0] + bary.y * t.pv[1] + bary.z * t.pv[2] - xyz(b.v) - cross(w, hit->on_b);
+    }
+    return true;
+}
+
+// Lane `src`'s contact search against bullet `bi`, by the whole warp: the samples of its
+// vertex's triangles (and of the vertex alone) shared out over the lanes, each lane keeping the
+// first of its samples of greatest depth, then the warp's: the greatest depth, the earliest in
+// the reference's order among equals. That is the sample the reference's sequential search
+// ends on (it takes a sample only when deeper than the best so far, from -band): found when its
+// depth is above -band. Returns the sample's triangle slot and index. All 32 lanes call it.
+__device__ bool contact_search_warp(const Dev& D, int par, int src, uint32_t i_l, V3 x_l, V3 v_l, float band_l, float sub, const DBullet& b,
+                                    V3 xb, float4 back, V3 w, const float2* ol, uint32_t& k_best, uint32_t& m_best) {
+    const uint32_t full = 0xffffffffu, lane = threadIdx.x & 31u;
+    const uint32_t i = __shfl_sync(full, i_l, src);
+    const V3 x = {__shfl_sync(full, x_l.x, src), __shfl_sync(full, x_l.y, src), __shfl_sync(full, x_l.z, src)};
+    const V3 v = {__shfl_sync(full, v_l.x, src), __shfl_sync(full, v_l.y, src), __shfl_sync(full, v_l.z, src)};
+    const float band = __shfl_sync(full, band_l, src);
+    const uint32_t k0 = D.vtri_off[i], k1 = D.vtri_off[i + 1];
+    bool have = false;
+    float bd = 0.0f;
+    uint32_t bo = 0u;  // (k - k0) * 64 + sample: the reference's order
+    // The triangles (and the vertex alone, last), 32 at a time: lane j loads the j-th, so their
+    // loads go out together. Their samples, numbered triangle by triangle in the reference's
+    // order, are then shared out over the lanes: sample p of the round goes to lane p % 32, which
+    // takes its triangle's corners from the lane that loaded them.
+    for (uint32_t kb = k0; kb <= k1; kb += 32u) {
+        const uint32_t kl = kb + lane;
+        const ContactTri mine = kl <= k1 ? contact_tri(D, par, i, kl, k1, x, v, sub, b.shape.w) : ContactTri{};
+        const uint32_t nk = min(32u, k1 + 1u - kb);
+        // Where each triangle's samples start; a dead triangle has none.
+        const uint32_t my_ns = (kl <= k1 && mine.ok) ? (mine.n + 1u) * (mine.n + 2u) / 2u : 0u;
+        uint32_t start = my_ns;  // inclusive scan, then exclusive
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(full, start, o);
+            if ((int)lane >= o) start += y;
+        }
+        const uint32_t total = __shfl_sync(full, start, nk - 1u);
+        start -= my_ns;
+        for (uint32_t p0 = 0; p0 < total; p0 += 32u) {
+            const uint32_t p = p0 + lane;
+            // The triangle of sample p: the last with start <= p (lanes past the end take 0).
+            uint32_t j = 0;
+            for (uint32_t q = 1; q < nk; q++)
+                if (__shfl_sync(full, start, q) <= p) j = q;
+            ContactTri t;
+            for (int c = 0; c < 3; c++) {
+                t.p[c] = {__shfl_sync(full, mine.p[c].x, j), __shfl_sync(full, mine.p[c].y, j), __shfl_sync(full, mine.p[c].z, j)};
+                t.pv[c] = {__shfl_sync(full, mine.pv[c].x, j), __shfl_sync(full, mine.pv[c].y, j), __shfl_sync(full, mine.pv[c].z, j)};
+            }
+            t.own = __shfl_sync(full, mine.own, j);
+            t.n = __shfl_sync(full, mine.n, j);
+            t.ok = true;
+            const uint32_t m = p - __shfl_sync(full, start, j);
+            if (p >= total) continue;
+            uint32_t a, c;
+            contact_sample_ac(m, t.n, a, c);
+            float depth;
+            if (contact_sample(ol, t, a, c, b, xb, back, w, band, depth, nullptr) && (!have || depth > bd)) {
+                have = true;
+                bd = depth;
+                bo = (kb + j - k0) * 64u + m;
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const bool oh = __shfl_xor_sync(full, have, o);
+        const float od = __shfl_xor_sync(full, bd, o);
+        const uint32_t oo = __shfl_xor_sync(full, bo, o);
+        if (oh && (!have || od > bd || (od == bd && oo < bo))) have = true, bd = od, bo = oo;
+    }
+    if (!have || !(bd > -band)) return false;
+    k_best = k0 + bo / 64u;
+    m_best = bo % 64u;
+    return true;
+}
+
+// Contact of the rubber with the bullets (bullet.wgsl:426-611), for the lanes with `act`; every
+// lane of the warp calls it. Per bullet in turn: the lanes near it, one after the other, have
+// their search run by the whole warp (contact_search_warp), then take the response themselves.
+__device__ float rubber_contact(const Dev& D, const float2* outlines, int par, uint32_t i, bool act, V3& x, V3& v, float m, V3 load,
+                                const VertexForce& vf, bool wet, bool& held, float t, float sub, float now, float dt) {
+    const uint32_t full = 0xffffffffu, lane = threadIdx.x & 31u;
     float limit = BIG_F;
-    float band = held ? 0.5f * vf.thick : 0.0f;
-    held = false;
+    const float band = held ? 0.5f * vf.thick : 0.0f;
+    if (act) held = false;
     const uint32_t nbu = D.U->mem[3];
     for (uint32_t bi = 0; bi < nbu; bi++) {
         const DBullet b = D.bullets[bi];
         if (b.info.z != 1u) continue;
+        const float2* ol = outlines + bi * NTR_OUTLINE;
         V3 xb = xyz(b.x) - xyz(b.v) * (now - t);
         float closing = length(xyz(b.v) - v);
-        if (length(x - xb) > b.shape.z + vf.reach + 2.0f * closing * dt) continue;
-        limit = mn(limit, 0.25f * b.shape.w / mx(closing, 1e-6f));
+        const bool near = act && !(length(x - xb) > b.shape.z + vf.reach + 2.0f * closing * dt);
+        if (near) limit = mn(limit, 0.25f * b.shape.w / mx(closing, 1e-6f));
         float4 back = make_float4(-b.q.x, -b.q.y, -b.q.z, b.q.w);
         V3 w = qrot(b.q, qrot(back, xyz(b.l)) / v3(b.shape.y, b.shape.y, b.shape.x));
-        float best = -band;
-        bool found = false;
-        V3 gap = {0.0f, 0.0f, 0.0f}, on_b = gap, nrm = gap, rel = gap;
-        float share = 0.0f;
-        const uint32_t k0 = D.vtri_off[i], k1 = D.vtri_off[i + 1];
-        for (uint32_t k = k0; k <= k1; k++) {
-            V3 p[3] = {x, x, x};
-            V3 pv[3] = {v, v, v};
-            uint32_t own = 0, n = 1;
-            if (k < k1) {
-                uint32_t tn = D.vtri[k];
-                if (D.alive[tn] == 0u) continue;  // dead, or tore in this substep (k_mem_tri)
-                const Tri tri = D.tris[tn];
-                uint32_t ids[3] = {tri.v0, tri.v1, tri.v2};
-                for (uint32_t c = 0; c < 3; c++) {
-                    if (ids[c] == i) {
-                        own = c;
-                    } else {
-                        pv[c] = xyz(MV[ids[c]]);
-                        p[c] = xyz(MX[ids[c]]) + sub * pv[c];
-                    }
-                }
-                float longest = mx(distance(p[0], p[1]), mx(distance(p[1], p[2]), distance(p[2], p[0])));
-                n = f2u(clampf_(ceilf(longest / b.shape.w), 1.0f, 8.0f));
-            }
-            for (uint32_t a = 0; a <= n; a++) {
-                for (uint32_t c = 0; c <= n - a; c++) {
-                    V3 bary = v3((float)a, (float)c, (float)(n - a - c)) / (float)n;
-                    float wi = bary[own];
-                    if (wi <= 0.0f) continue;
-                    V3 s = bary.x * p[0] + bary.y * p[1] + bary.z * p[2];
-                    V3 r = s - xb;
-                    if (length(r) >= b.shape.z + band) continue;
-                    V3 q = qrot(back, r);
-                    float rho = sqrtf(q.x * q.x + q.y * q.y);
-                    Near nr = nearest_surface(D, bi, q.z, rho);
-                    if (nr.depth <= best) continue;
-                    float rx = 1.0f, ry = 0.0f;
-                    if (rho > 1e-9f) rx = q.x / rho, ry = q.y / rho;
-                    best = nr.depth;
-                    found = true;
-                    on_b = qrot(b.q, v3(rx * nr.ay, ry * nr.ay, nr.ax));
-                    gap = on_b - r;
-                    nrm = qrot(b.q, v3(rx * nr.ny, ry * nr.ny, nr.nx));
-                    share = wi / dot(bary, bary);
-                    rel = bary.x * pv[0] + bary.y * pv[1] + bary.z * pv[2] - xyz(b.v) - cross(w, on_b);
-                }
-            }
-        }
-        if (!found) continue;
-        float vn = dot(rel, nrm);
-        V3 rel_t = rel - vn * nrm;
-        float slide = length(rel_t);
-        float dvn = 0.0f, jn = 0.0f;
-        V3 j = {0.0f, 0.0f, 0.0f};
-        bool holds = false;
-        if (!wet) {
-            dvn = mx(-vn, 0.0f);
-            jn = m * dvn;
-            j = -m * share * dvn * nrm;
-        } else {
-            float ln = dot(load, nrm);
-            if (ln < 0.0f) {
-                dvn = -vn;
-                jn = -ln * sub;
-                j = mn(share, 1.0f) * ln * sub * nrm;
-                holds = true;
-                held = true;
-            } else if (best > 0.0f) {
-                dvn = mx(-vn, 0.0f);
-            } else {
-                continue;
-            }
-        }
-        float stop = (slide > 1e-9f && m > 0.0f) ? mn(1.0f, MU_JACKET * jn / (m * slide)) : 0.0f;
-        V3 dvt = -share * stop * rel_t;
-        x = x + (share * gap + sub * dvt);
-        v = v + (share * dvn * nrm + dvt);
-        j = j - m * dvt;
-        float nl = length(vf.n);
-        int32_t* hit = D.bullet_hit + bi * NTR_HIT_FIELDS;
-        if (holds && nl > 0.0f) {
-            float a = vf.area * 1e6f;
-            V3 sx = (x - xb) * 1e3f * a;
-            for (int c = 0; c < 3; c++) {
-                atomicAdd(hit + 6 + c, to_fp(vf.n[c] / nl * a, FP_A));
-                atomicAdd(hit + 9 + c, to_fp(sx[c], FP_X));
-            }
-            atomicAdd(hit + 12, to_fp(a, FP_A));
-        }
-        V3 jl = cross(on_b, j);
-        for (int c = 0; c < 3; c++) {
-            atomicAdd(hit + c, to_fp(j[c], FP_J));
-            atomicAdd(hit + 3 + c, to_fp(jl[c], FP_L));
+        for (uint32_t todo = __ballot_sync(full, near); todo; todo &= todo - 1u) {
+            const int src = __ffs(todo) - 1;
+            uint32_t kb = 0, mb = 0;
+            const bool found = contact_search_warp(D, par, src, i, x, v, band, sub, b, xb, back, w, ol, kb, mb);
+            if ((int)lane != src || !found) continue;
+            // The best sample again, with what the response needs.
+            const uint32_t k1 = D.vtri_off[i + 1];
+            const ContactTri tb = contact_tri(D, par, i, kb, k1, x, v, sub, b.shape.w);
+            uint32_t a, c;
+            contact_sample_ac(mb, tb.n, a, c);
+            ContactHit hit;
+            float depth_again;
+            contact_sample(ol, tb, a, c, b, xb, back, w, band, depth_again, &hit);
+            const float best = hit.depth;
+            const V3 on_b = hit.on_b, gap = hit.gap, nrm = hit.nrm, rel = hit.rel;
+            const float share = hit.share;
+            contact_response(D, bi, x, v, m, load, vf, wet, held, sub, xb, best, on_b, gap, nrm, rel, share);
         }
     }
     return limit;
+}
+
+// The vertex of a thread of k_mem_substep: groups of 4 consecutive vertices, the 8 groups of a
+// warp an eighth of the launch's vertices apart (a bijection of the launch's threads). The
+// vertices near a bullet lie together in the mesh's spatial order: so their contact searches,
+// the substep's only heavy work, fall to many warps (and SMs) instead of a few, and each warp
+// shares its few among its lanes.
+__device__ __forceinline__ uint32_t substep_vertex(uint32_t block, uint32_t thread, uint32_t n_blocks) {
+    const uint32_t t = block * blockDim.x + thread;
+    const uint32_t span = n_blocks * blockDim.x / 32u;  // groups in an eighth
+    const uint32_t gi = t >> 2;
+    return (((gi & 7u) * span + (gi >> 3)) << 2) | (t & 3u);
 }
 
 // One explicit rubber substep (membrane.wgsl:283-400). `k` is which substep of the step this
 // is, `par` which pair of buffers it reads.
 __global__ void __launch_bounds__(256) k_mem_substep(Dev D, uint32_t k, int par) {
     DevState* st = D.st;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = substep_vertex(blockIdx.x, threadIdx.x, gridDim.x);
     float lim_x = BIG_F, lim_y = BIG_F;
     const ntr_gpu_params* U = D.U;
     const float dt = dt_of(st), now = now_of(st);
+    const float sub = dt / (float)max(U->mem[1], 1u);
+    const float t_sub = now - dt + (float)(k + 1u) * sub;
+    // What the contact with the bullets needs of this vertex; `act` when it takes part.
+    bool act = false, c_held = false, c_ow = false;
+    V3 c_x = {0.0f, 0.0f, 0.0f}, c_v = c_x, c_f = c_x;
+    float c_m = 0.0f, c_push = 0.0f, c_w = 0.0f;
+    VertexForce c_vf = {{0.0f, 0.0f, 0.0f}, {0.0f, 0.0f, 0.0f}, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     if (i < D.Nv) {
         const Grid g = grid_of(D, cur_of(st));
         const float m = D.mem_mass[i];
@@ -352,8 +501,6 @@ __global__ void __launch_bounds__(256) k_mem_substep(Dev D, uint32_t k, int par)
             VO[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         } else {
             const float hh = g.h;
-            const float sub = dt / (float)max(U->mem[1], 1u);
-            const float t_sub = now - dt + (float)(k + 1u) * sub;
             const VertexForce vf = vertex_force(D, i);
             lim_x = sqrtf(m / mx(vf.stiff, 1e-30f));
             if (vf.tension > 0.0f) lim_y = sqrtf(U->fluid[0] * hh * hh * hh / (4.0f * PI_F * vf.tension));
@@ -409,22 +556,34 @@ __global__ void __launch_bounds__(256) k_mem_substep(Dev D, uint32_t k, int par)
                     }
                     v = v + sub * (f + fa) / m;
                 }
-                V3 xx = xyz(x4) + sub * v;
-                held = held && ow;
-                lim_x = mn(lim_x, rubber_contact(D, par, i, xx, v, m, f, vf, ow, held, t_sub, sub, now, dt));
-                D.mem_push[i].x = held ? 0.0f : push;
-                if (xx.y < 0.0f) {
-                    float jj = mx(-v.y, 0.0f);
-                    xx.y = 0.0f;
-                    v.y = mx(v.y, 0.0f);
-                    float s = sqrtf(v.x * v.x + v.z * v.z);
-                    float keep = s > 1e-9f ? mx(0.0f, 1.0f - U->rubber2[0] * jj / s) : 0.0f;
-                    v = v3(v.x * keep, v.y, v.z * keep);
-                }
-                XO[i] = make_float4(xx.x, xx.y, xx.z, x4.w);
-                VO[i] = make_float4(v.x, v.y, v.z, held ? 1.0f : 0.0f);
+                act = true;
+                c_x = xyz(x4) + sub * v;
+                c_v = v, c_f = f, c_m = m, c_vf = vf, c_ow = ow, c_push = push, c_w = x4.w;
+                c_held = held && ow;
             }
         }
+    }
+    // The contact with the bullets, with every lane of the warp (rubber_contact shares a
+    // vertex's search among them), then the rest of the vertex's substep.
+    // The bullets' outlines, which every contact sample walks, in shared memory.
+    __shared__ float2 s_outline[NTR_MAX_SHOTS * NTR_OUTLINE];
+    for (uint32_t j = threadIdx.x; j < U->mem[3] * NTR_OUTLINE && j < NTR_MAX_SHOTS * NTR_OUTLINE; j += blockDim.x) s_outline[j] = D.outlines[j];
+    __syncthreads();
+    const float lim_c = rubber_contact(D, s_outline, par, i, act, c_x, c_v, c_m, c_f, c_vf, c_ow, c_held, t_sub, sub, now, dt);
+    if (act) {
+        lim_x = mn(lim_x, lim_c);
+        D.mem_push[i].x = c_held ? 0.0f : c_push;
+        V3 xx = c_x, v = c_v;
+        if (xx.y < 0.0f) {
+            float jj = mx(-v.y, 0.0f);
+            xx.y = 0.0f;
+            v.y = mx(v.y, 0.0f);
+            float s = sqrtf(v.x * v.x + v.z * v.z);
+            float keep = s > 1e-9f ? mx(0.0f, 1.0f - U->rubber2[0] * jj / s) : 0.0f;
+            v = v3(v.x * keep, v.y, v.z * keep);
+        }
+        D.mem_x[1 - par][i] = make_float4(xx.x, xx.y, xx.z, c_w);
+        D.mem_v[1 - par][i] = make_float4(v.x, v.y, v.z, c_held ? 1.0f : 0.0f);
     }
     // The longest stable substep and the capillary step, lowered with atomicMin on the bits.
     for (int o = 16; o > 0; o >>= 1) {
