@@ -525,7 +525,8 @@ __global__ void k_mem_sample(Dev D) {
 }
 
 // ---- air_substep, air.wgsl:237-269 --------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_air_substep(Dev D, int par) {
+// Three CTAs an SM (80 registers, from 84 and two CTAs): 38.5 -> 34.8 us a step at 1M particles.
+__global__ void __launch_bounds__(256, 3) k_air_substep(Dev D, int par) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
