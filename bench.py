@@ -121,7 +121,7 @@ def algorithmic_bytes(kernel: str, st: dict, n_particles: int, iters: int) -> fl
         return 48.0 * n_water * max(iters, 1) + 40.0 * n_water
     if kernel == "k_p2g":
         return 84.0 * n_particles + 8 * 4 * 343 * nb
-    if kernel == "k_g2p":
+    if kernel.startswith("k_g2p"):
         return (32.0 + 80.0) * n_particles + 8 * 4 * 343 * nb
     return 0.0
 

@@ -118,11 +118,13 @@ __device__ __forceinline__ Gathered gather(const float* tg, V3 X, V3 o, I3 corne
     return r;
 }
 
-// 128 threads a CTA, 6 CTAs an SM: a block's few hundred particles take 3 rounds with a short
-// last one, and the SM has more CTAs to switch to while one waits on its loads or barriers.
-constexpr int G2P_T = 128;
-
-__global__ void __launch_bounds__(G2P_T, 6) k_g2p(Dev D) {
+// G2P_T threads a CTA, 768 / G2P_T CTAs an SM. With many blocks (the 1M-particle scene: 128
+// threads, six CTAs an SM) a block's few hundred particles take 3 rounds with a short last one,
+// and the SM has more CTAs to switch to while one waits on its loads or barriers. With few
+// blocks (small scenes: 256 threads) every block runs at once and its chain of rounds is the
+// time. The result does not depend on the CTA's size.
+template <int G2P_T>
+__global__ void __launch_bounds__(G2P_T, 768 / G2P_T) k_g2p(Dev D) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));

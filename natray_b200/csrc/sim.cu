@@ -559,7 +559,11 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
         }
     }
     LA(k_spray_update, G_cell, 256, D);
-    L(k_g2p, G_blk, G2P_T, D);
+    // Past 300k particles the blocks outnumber the resident CTAs: smaller CTAs, more of them.
+    if (D.Np >= 300000u)
+        L(k_g2p<128>, G_blk, 128, D);
+    else
+        L(k_g2p<256>, G_blk, 256, D);
     join(1);
     if (a2 != s) {
         cudaEventRecord(S.ev_join[2], a2);
