@@ -549,7 +549,6 @@ __global__ void __launch_bounds__(P2G_T, 3) k_p2g(Dev D) {
     const uint32_t lane = threadIdx.x & 31u;
     __shared__ __align__(16) int32_t tile[8 * TPF];
     __shared__ uint32_t own[64], s_cnt[64];
-    __shared__ uint32_t links[27];
     __shared__ uint32_t s_pid[P2G_CAP];
     __shared__ uint8_t s_cell[P2G_CAP];
     __shared__ uint16_t s_rank[P2G_CAP];
@@ -561,9 +560,7 @@ __global__ void __launch_bounds__(P2G_T, 3) k_p2g(Dev D) {
         if (threadIdx.x < 27) {
             uint32_t li = threadIdx.x;
             I3 n = bc + I3{(int32_t)(li / 9u), (int32_t)((li / 3u) % 3u), (int32_t)(li % 3u)} - I3{1, 1, 1};
-            uint32_t idx = block_at(g, n);
-            links[li] = idx;
-            D.block_nb[b * 27u + li] = idx;
+            D.block_nb[b * 27u + li] = block_at(g, n);
         }
         if (threadIdx.x < 64) own[threadIdx.x] = 0;
         const uint32_t first = D.block_start[b];

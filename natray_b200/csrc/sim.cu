@@ -248,7 +248,6 @@ static ntr_status allocate(Sim& S) {
 static ntr_status upload_state(Sim& S, const World& w) {
     const ntr_world_header& h = w.h;
     Dev& D = S.D;
-    cudaStream_t st = S.stream;
     // Particles: AoS of 20 floats to five float4 arrays.
     {
         std::vector<float4> a[5];
@@ -318,7 +317,6 @@ static ntr_status upload_state(Sim& S, const World& w) {
     ds.s.n_blocks = nbp;
     ds.rz = h.state.rz, ds.alpha = h.state.alpha, ds.beta = h.state.beta, ds.b_norm = h.state.b_norm, ds.r_norm = h.state.r_norm;
     CU(cudaMemcpy(D.st, &ds, sizeof ds, cudaMemcpyHostToDevice));
-    (void)st;
     return NTR_OK;
 }
 
@@ -436,7 +434,6 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     uint64_t n = 0;
     const uint32_t G_cell = (uint32_t)S.sms * S.tune.cell_ctas_per_sm;
     const uint32_t G_blk = (uint32_t)S.sms * S.tune.block_ctas_per_sm;
-    const uint32_t g_part = (D.Np + 255) / 256 ? (D.Np + 255) / 256 : 1;
     const uint32_t g_vert = (D.Nv + 255) / 256 ? (D.Nv + 255) / 256 : 1;
     const uint32_t g_tri = std::max((D.Nt + 255) / 256, 1u);
     const uint32_t n_shots = S.U.mem[3] ? S.U.mem[3] : 1;
