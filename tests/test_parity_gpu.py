@@ -211,6 +211,18 @@ def test_four_bullets_bit_exact(oracle_threads):
     assert end.state["spray_count"] > 0 and int((end.sec("ALIVE") == 0).sum()) > 0
 
 
+def test_large_scene_bit_exact(oracle_threads):
+    # From 300k particles G2P runs its many-block form (CTAs of 128 threads, six an SM), the one
+    # the 1M-particle workload takes; the smaller scenes of the other tests take the 256-thread
+    # form.
+    w = measured(build_world(Params(resolution=88, mesh_level=5, block_cap=4096, spray_cap=200000)))
+    assert w.h.n_particles >= 300000
+    o, s = Oracle(w.blob), Sim(world=w)
+    for k in range(2):
+        assert o.step(2) == s.step(2) == 2
+        assert_worlds_equal(World(o.snapshot()), s.snapshot(), f"batch {k}")
+
+
 def test_long_run_to_the_ground_bit_exact(oracle_threads):
     # A low balloon (0.12 m) run for 1200 steps of the reference's adaptive dt, about 0.45 s:
     # the water and its spray fall, drops land (LANDED) and the ground gets wet (TOUCH), and
