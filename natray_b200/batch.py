@@ -15,7 +15,7 @@ import ctypes as C
 
 from . import _abi
 from ._abi import NatrayError, check, lib
-from .world import World
+from .world import World, blob_arg
 
 NTR_E_BUSY = 8
 
@@ -45,9 +45,9 @@ class Batch:
 
     def admit(self, world: World | bytes, n_steps: int) -> int | None:
         """The scene's slot, or None when the batch has no room for it now."""
-        blob = bytes(world.blob) if isinstance(world, World) else bytes(world)
+        blob, n = blob_arg(world)
         slot = C.c_uint32()
-        st = lib().ntr_batch_admit(self._h, blob, len(blob), n_steps, C.byref(slot))
+        st = lib().ntr_batch_admit(self._h, blob, n, n_steps, C.byref(slot))
         if st == NTR_E_BUSY:
             return None
         check(st)
@@ -56,9 +56,9 @@ class Batch:
     def enqueue(self, world: World | bytes, n_steps: int) -> int:
         """Queues the scene from any thread; the stepping thread admits it at its next step.
         Returns the ticket."""
-        blob = bytes(world.blob) if isinstance(world, World) else bytes(world)
+        blob, n = blob_arg(world)
         ticket = C.c_uint64()
-        check(lib().ntr_batch_enqueue(self._h, blob, len(blob), n_steps, C.byref(ticket)))
+        check(lib().ntr_batch_enqueue(self._h, blob, n, n_steps, C.byref(ticket)))
         return ticket.value
 
     def ticket(self, ticket: int) -> int | None:

@@ -19,14 +19,14 @@ import ctypes as C
 import numpy as np
 
 from ._abi import check, lib
-from .world import World
+from .world import World, blob_arg
 
 
 def device_bytes(world: World | bytes) -> int:
     """The device memory a simulation of the world takes (ntr_world_device_bytes)."""
-    blob = bytes(world.blob) if isinstance(world, World) else bytes(world)
+    blob, size = blob_arg(world)
     n = C.c_uint64()
-    check(lib().ntr_world_device_bytes(blob, len(blob), C.byref(n)))
+    check(lib().ntr_world_device_bytes(blob, size, C.byref(n)))
     return n.value
 
 

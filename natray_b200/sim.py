@@ -16,7 +16,7 @@ import numpy as np
 
 from . import _abi
 from ._abi import BUF, check, lib
-from .world import Params, World, build_world
+from .world import Params, World, blob_arg, build_world
 
 
 class Sim:
@@ -25,8 +25,8 @@ class Sim:
         self._h = C.c_void_p()
         if world is None:
             world = build_world(params if params is not None else Params())
-        blob = bytes(world.blob) if isinstance(world, World) else bytes(world)
-        check(lib().ntr_sim_create_from_world(blob, len(blob), device, C.byref(self._h)))
+        blob, n = blob_arg(world)
+        check(lib().ntr_sim_create_from_world(blob, n, device, C.byref(self._h)))
         if not fp64_reductions:
             check(lib().ntr_sim_set_precision(self._h, 0))
         self.info = self._info()
@@ -108,8 +108,8 @@ class Sim:
         return World(buf.raw[: n.value])
 
     def restore(self, world: World | bytes) -> None:
-        blob = bytes(world.blob) if isinstance(world, World) else bytes(world)
-        check(lib().ntr_sim_restore(self._h, blob, len(blob)))
+        blob, n = blob_arg(world)
+        check(lib().ntr_sim_restore(self._h, blob, n))
 
     def buffer(self, name: str) -> tuple[int, int]:
         """(device pointer, bytes) of a lent buffer."""

@@ -111,6 +111,18 @@ class World:
                 "n_shots": h.n_shots, "bytes": len(self.blob)}
 
 
+def blob_arg(world: "World | bytes | bytearray") -> tuple[object, int]:
+    """A world blob as the library's (pointer, length) arguments. A World's bytearray is passed
+    in place, not copied (93 MB at 1M particles): every entry point taking a blob reads it
+    during the call and copies what it keeps."""
+    if isinstance(world, World):
+        world = world.blob
+    if isinstance(world, bytearray):
+        return (C.c_char * len(world)).from_buffer(world), len(world)
+    b = bytes(world)
+    return b, len(b)
+
+
 def build_world(params: Params) -> World:
     """The initial world of `params`, built on the CPU."""
     p = C.c_void_p()
@@ -124,4 +136,4 @@ def build_world(params: Params) -> World:
     return World(blob, copy=False)
 
 
-__all__ = ["Params", "World", "build_world", "sized_for", "SECTIONS"]
+__all__ = ["Params", "World", "blob_arg", "build_world", "sized_for", "SECTIONS"]
