@@ -1732,10 +1732,11 @@ bool build_world(const ntr_sim_params& p, World& w, std::string& err) {
     h.dx = dx;
     w.shape_sections();
 
+    // The sections come zeroed from shape_sections(): each particle needs its position and its
+    // alive flag only.
     float* part = w.as<float>(NTR_SEC_PARTICLES);
     for (uint32_t i = 0; i < n_particles; i++) {
         float* a = part + (size_t)i * 20;
-        std::memset(a, 0, 80);
         std::memcpy(a, scene.particles[i].data(), 16);
         a[7] = 1.0f;
     }
