@@ -318,9 +318,9 @@ struct ContactHit {
     float share, depth;
 };
 
-// One sample against bullet `bi` (membrane.wgsl's contact search, bullet.wgsl:426-611): false if
-// it does not count (no weight on this vertex, or beyond the bullet's reach). With `hit`, also
-// what the response needs.
+// One sample against a bullet, `ol` its outline (the contact search of bullet.wgsl:426-611):
+// false if it does not count (no weight on this vertex, or beyond the bullet's reach). With
+// `hit`, also what the response needs.
 __device__ __forceinline__ bool contact_sample(const float2* ol, const ContactTri& t, uint32_t a, uint32_t c, const DBullet& b, V3 xb,
                                                float4 back, V3 w, float band, float& depth, ContactHit* hit) {
     const uint32_t n = t.n;
@@ -347,12 +347,13 @@ __device__ __forceinline__ bool contact_sample(const float2* ol, const ContactTr
     return true;
 }
 
-// Lane `src`'s contact search against bullet `bi`, by the whole warp: the samples of its
-// vertex's triangles (and of the vertex alone) shared out over the lanes, each lane keeping the
-// first of its samples of greatest depth, then the warp's: the greatest depth, the earliest in
-// the reference's order among equals. That is the sample the reference's sequential search
-// ends on (it takes a sample only when deeper than the best so far, from -band): found when its
-// depth is above -band. Returns the sample's triangle slot and index. All 32 lanes call it.
+// Lane `src`'s contact search against a bullet (`ol` its outline), by the whole warp: the
+// samples of its vertex's triangles (and of the vertex alone) shared out over the lanes, each
+// lane keeping the first of its samples of greatest depth, then the warp's: the greatest depth,
+// the earliest in the reference's order among equals. For finite depths that is the sample the
+// reference's sequential search ends on (it takes a sample only when deeper than the best so
+// far, from -band): found when its depth is above -band. Returns the sample's triangle slot and
+// index. All 32 lanes call it.
 __device__ bool contact_search_warp(const Dev& D, int par, int src, uint32_t i_l, V3 x_l, V3 v_l, float band_l, float sub, const DBullet& b,
                                     V3 xb, float4 back, V3 w, const float2* ol, uint32_t& k_best, uint32_t& m_best) {
     const uint32_t full = 0xffffffffu, lane = threadIdx.x & 31u;
