@@ -182,3 +182,19 @@ def test_inflation_on_threads_is_bit_identical_to_one_by_one():
         assert r.returncode == 0, r.stderr
         out.append(r.stdout.strip())
     assert out[0] == out[1] and len(out[0]) == 64
+
+
+def test_world_blob_is_passed_in_place():
+    # A World's bytearray reaches the library without a copy; bytes are passed as they are.
+    import ctypes as C
+
+    from natray_b200.replicas import device_bytes
+    from natray_b200.world import blob_arg
+
+    w = build_world(Params(resolution=20, mesh_level=2))
+    arg, n = blob_arg(w)
+    assert n == len(w.blob)
+    assert C.addressof(arg) == C.addressof((C.c_char * n).from_buffer(w.blob))
+    raw, n2 = blob_arg(bytes(w.blob))
+    assert isinstance(raw, bytes) and n2 == n
+    assert device_bytes(w) == device_bytes(bytes(w.blob)) > 0
