@@ -54,7 +54,7 @@ struct Batch {
     std::map<uint64_t, uint32_t> placed;
 
     ~Batch() {
-        cudaSetDevice(device);
+        DeviceScope scope(device);
         for (auto& s : slots) {
             s.sim.reset();
             if (s.ev_pre) cudaEventDestroy(s.ev_pre);
@@ -83,7 +83,8 @@ static ntr_status batch_create(int device, uint32_t max_scenes, uint64_t budget,
     ntr_status r = check_device(device);
     if (r != NTR_OK) return r;
     if (max_scenes == 0 || max_scenes > NTR_BATCH_MAX) return fail(NTR_E_INVALID, "max_scenes is 1.." + std::to_string(NTR_BATCH_MAX));
-    CU(cudaSetDevice(device));
+    DeviceScope scope(device);
+    if (!scope.ok) return fail(NTR_E_CUDA, "cudaSetDevice failed");
     cudaDeviceProp prop;
     CU(cudaGetDeviceProperties(&prop, device));
     if (prop.major < 10) return fail(NTR_E_NODEVICE, "this library is built for sm_100a (B200)");

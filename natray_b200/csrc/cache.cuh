@@ -447,7 +447,7 @@ struct Cache {
         spray_w = nullptr;
     }
     ~Cache() {
-        cudaSetDevice(device);
+        DeviceScope scope(device);
         for (cudaEvent_t e : ev)
             if (e) cudaEventDestroy(e);
         free_shown();

@@ -913,7 +913,9 @@ __global__ void __launch_bounds__(256) k_bullet_finish(Dev D) {
         for (int o = 16; o > 0; o >>= 1) r = mx(r, __shfl_xor_sync(0xffffffffu, r, o));
         if (li == 0) D.bullets[bi].reach = f4(x, r > 0.0f ? r + R_HAND * hh : 0.0f);
     }
-    // Sections thinner than the grid push the water out of the way as they open.
+    // A cavity section still narrower than the hand-over radius is a volume source: the rate at
+    // which its cylinder opens goes into A_SRC of the 27 cells around its middle, with the
+    // B-spline weights of a particle there, and the pressure solve makes room for it.
     if (li < NTR_N_SEC) {
         const DSection s = D.sections[bi * NTR_N_SEC + li];
         float r2 = section_r2(s, t_end);

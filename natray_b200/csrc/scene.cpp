@@ -1533,7 +1533,7 @@ SectionShape section_shape(const ntr_world_header& h, int sec) {
 void World::shape_sections() {
     for (int s = 0; s < NTR_SEC_COUNT; s++) {
         SectionShape sh = section_shape(h, s);
-        sec[s].resize(sh.elem * sh.count);
+        sec[s].assign(sh.elem * sh.count, 0);  // zeroed whatever the World held before
     }
 }
 

@@ -47,6 +47,22 @@ struct StepGraph {
     uint64_t launches = 0;
 };
 
+// Makes `device` current for the rest of the calling scope and puts the thread's own current
+// device back when the scope ends, so a call on a simulation or batch of another GPU leaves the
+// caller's CUDA (or torch) context where it was.
+struct DeviceScope {
+    int saved = -1;
+    bool ok = false;
+    explicit DeviceScope(int device) {
+        if (cudaGetDevice(&saved) != cudaSuccess) saved = -1;
+        ok = saved == device || cudaSetDevice(device) == cudaSuccess;
+    }
+    ~DeviceScope() {
+        int now = -1;
+        if (saved >= 0 && cudaGetDevice(&now) == cudaSuccess && now != saved) cudaSetDevice(saved);
+    }
+};
+
 struct Sim {
     int device = 0;
     int sms = 148;
@@ -76,7 +92,7 @@ struct Sim {
     ntr_tuning tune{0u, 8u, 8u, 0u};  // launch shapes (ntr_sim_set_tuning)
 
     ~Sim() {
-        cudaSetDevice(device);
+        DeviceScope scope(device);
         for (auto& kv : graphs) {
             if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
             if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
@@ -617,7 +633,7 @@ static ntr_status run_batch(Sim& S, uint32_t n, uint32_t stop, uint32_t* taken, 
     S.U.mem[2] = h.air_substeps;
     ntr_status r = push_params(S);
     if (r != NTR_OK) return r;
-    // iters_max and unconverged count per batch.
+    // The solver's most-iterations and out-of-iterations counters start from zero in every batch.
     CU(cudaMemsetAsync(&S.D.st->s.iters_max, 0, 8, S.stream));
     StepGraph* g = nullptr;
     if (!prof)
@@ -654,7 +670,8 @@ static ntr_status create_from(const World& w, int device, Sim*& out, uint8_t* ar
                               DevState* h_state = nullptr) {
     ntr_status r = check_device(device);
     if (r != NTR_OK) return r;
-    CU(cudaSetDevice(device));
+    DeviceScope scope(device);
+    if (!scope.ok) return fail(NTR_E_CUDA, "cudaSetDevice failed");
     std::unique_ptr<Sim> S(new Sim);
     S->device = device;
     S->host.h = w.h;
@@ -764,7 +781,8 @@ struct ntr_sim {
 #define GUARD(sim)                                             \
     if (!(sim) || !(sim)->s) return fail(NTR_E_INVALID, "null simulation handle"); \
     Sim& S = *(sim)->s;                                        \
-    if (cudaSetDevice(S.device) != cudaSuccess) return fail(NTR_E_CUDA, "cudaSetDevice failed")
+    DeviceScope device_scope_(S.device);                       \
+    if (!device_scope_.ok) return fail(NTR_E_CUDA, "cudaSetDevice failed")
 
 extern "C" {
 
@@ -1230,7 +1248,8 @@ struct ntr_batch {
     if (!(batch) || !(batch)->b) return fail(NTR_E_INVALID, "null batch handle");        \
     Batch& B = *(batch)->b;                                                             \
     std::lock_guard<std::mutex> batch_lock_(B.mu);                                      \
-    if (cudaSetDevice(B.device) != cudaSuccess) return fail(NTR_E_CUDA, "cudaSetDevice failed")
+    DeviceScope device_scope_(B.device);                                                \
+    if (!device_scope_.ok) return fail(NTR_E_CUDA, "cudaSetDevice failed")
 
 constexpr uint32_t BATCH_REJECTED = 0xfffffffeu;
 
@@ -1267,13 +1286,20 @@ NTR_API ntr_status ntr_world_device_bytes(const void* blob, size_t len, uint64_t
 }
 
 NTR_API ntr_status ntr_batch_enqueue(ntr_batch* batch, const void* blob, size_t len, uint32_t n_steps, uint64_t* ticket) {
-    BGUARD(batch);
+    if (!batch || !batch->b) return fail(NTR_E_INVALID, "null batch handle");
     if (!blob || !ticket) return fail(NTR_E_INVALID, "null argument");
-    World w;
-    std::string err;
-    if (!deserialize(blob, len, w, err)) return fail(NTR_E_INVALID, err);
+    // The blob is checked and copied before the batch's lock is taken (a 1M-particle world is
+    // about 93 MB), so a producer thread holds up the stepping thread only for the queue's push.
+    {
+        World w;
+        std::string err;
+        if (!deserialize(blob, len, w, err)) return fail(NTR_E_INVALID, err);
+    }
     const uint8_t* p = static_cast<const uint8_t*>(blob);
-    B.queue.push_back(Batch::Queued{B.next_ticket, std::vector<uint8_t>(p, p + len), n_steps});
+    std::vector<uint8_t> copy(p, p + len);
+    Batch& B = *batch->b;
+    std::lock_guard<std::mutex> lock(B.mu);
+    B.queue.push_back(Batch::Queued{B.next_ticket, std::move(copy), n_steps});
     *ticket = B.next_ticket++;
     return NTR_OK;
 }
@@ -1373,7 +1399,8 @@ struct ntr_cache {
 #define CGUARD(cache)                                                                   \
     if (!(cache) || !(cache)->c) return fail(NTR_E_INVALID, "null cache handle");        \
     Cache& C = *(cache)->c;                                                             \
-    if (cudaSetDevice(C.device) != cudaSuccess) return fail(NTR_E_CUDA, "cudaSetDevice failed")
+    DeviceScope device_scope_(C.device);                                                \
+    if (!device_scope_.ok) return fail(NTR_E_CUDA, "cudaSetDevice failed")
 
 extern "C" {
 

@@ -26,7 +26,7 @@ struct World {
     T* as(int s) { return reinterpret_cast<T*>(sec[s].data()); }
     template <class T>
     const T* as(int s) const { return reinterpret_cast<const T*>(sec[s].data()); }
-    // Resizes every section to what the header's counts say.
+    // Resizes every section to what the header's counts say, every byte zero.
     void shape_sections();
 };
 
