@@ -675,6 +675,12 @@ __global__ void k_bullet_prep(Dev D) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const uint32_t bi = blockIdx.x;
+    // A scene without bullets still launches one CTA; it has nothing to do (and the patch and
+    // finish kernels skip a bullet whose prep flag is not set).
+    if (bi >= D.U->mem[3]) {
+        if (threadIdx.x == 0) D.bullet_prep[bi * 4].x = 0.0f;
+        return;
+    }
     const int lane = (int)threadIdx.x;
     const Grid g = grid_of(D, cur_of(st));
     const DBullet b = D.bullets[bi];
