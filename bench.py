@@ -55,18 +55,35 @@ def hbm_peak() -> tuple[float, str]:
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and throttle reasons sampled during the timed region: NVML every millisecond
+    from a thread (the region can be a few ms long), nvidia-smi every 25 ms if NVML is missing."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits (nvml.h: nvmlClocksEventReason*).
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown"}
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
         self.lines: list[str] = []
+        self.samples: list[tuple[float, float, int]] = []
         self.t = None
+        self.stop = threading.Event()
+        self.nvml = None
 
     def __enter__(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.nvml = (nv, h)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                           "-lms", "25"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
@@ -76,53 +93,75 @@ class Clocks:
             self.proc = None
         return self
 
+    def _poll(self):
+        nv, h = self.nvml
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop.is_set():
+            try:
+                self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), self.max_mhz, int(get_reasons(h))))
+            except Exception:
+                pass
+            time.sleep(0.001)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
-            if self.t:
-                self.t.join(timeout=2)
+        if self.t:
+            self.t.join(timeout=2)
 
     def summary(self) -> dict:
         mhz, maxs, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                mhz.append(float(f[1]))
-                maxs.append(float(f[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
+        if self.nvml:
+            for m, mx, r in self.samples:
+                mhz.append(m)
+                maxs.append(mx)
+                reasons.update(n for bit, n in self.REASONS.items() if r & bit)
+            src = "nvml, 1 ms"
+        else:
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for ln in self.lines:
+                f = [x.strip() for x in ln.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    mhz.append(float(f[1]))
+                    maxs.append(float(f[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+            src = "nvidia-smi, 25 ms"
         if not mhz:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": max(maxs), "reasons": sorted(reasons), "samples": len(mhz)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "source": src}
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": max(maxs), "reasons": sorted(reasons), "samples": len(mhz),
+                "source": src}
 
 
 def algorithmic_bytes(kernel: str, st: dict, n_particles: int, iters: int) -> float:
-    """Bytes a launch of `kernel` must move at the least: the per-unit figures of the step
-    (particle 80 B read + 80 B written; P2G reads a particle's 80 B and writes its block's tile
-    sums; the solve reads d, z, diag, type, p, r, q and writes d', q, p, r, z per water cell
-    and iteration, 48 B)."""
-    nb = st["n_blocks"]
+    """Bytes a launch of `kernel` must move at the least, from the per-unit figures of the step:
+    P2G reads a particle's 80 B and its index and writes its cells' particle counts (its tile of
+    sums is this implementation's, not the algorithm's: the cells' sums are written by the tile
+    gather); the solve reads d, z, diag, type, p, r, q and writes d', q, p, r, z per water cell
+    and iteration (48 B) and sets up with 40 B per water cell; G2P reads a particle's 80 B, its
+    index and its cells' 8 fields once (32 B per cell) and writes the particle's 80 B."""
+    cells = st["n_blocks"] * 64
     if kernel.startswith("k_solve"):
-        n_water = st.get("_n_water", nb * 64)
+        n_water = st.get("_n_water", cells)
         return 48.0 * n_water * max(iters, 1) + 40.0 * n_water
     if kernel == "k_p2g":
-        return 84.0 * n_particles + 8 * 4 * 343 * nb
+        return 84.0 * n_particles + 4.0 * cells
     if kernel.startswith("k_g2p"):
-        return (32.0 + 80.0) * n_particles + 8 * 4 * 343 * nb
+        return 164.0 * n_particles + 32.0 * cells
     return 0.0
 
 
@@ -204,21 +243,26 @@ def run_native(args, rank, world, local):
             dist.barrier()
         torch.cuda.synchronize(local)
 
-    # Warm-up: the first batches size the solver's iterations and the substeps, and build the
-    # step's graph.
+    # Warm-up: W steps, one a batch: they size the solver's iterations and the substeps, and
+    # build the step's graph. The timed steps are W + 1 .. W + K, as in the reference arm.
     for _ in range(args.warmup):
         sim.step(1)
-    sim.step(args.warmup)
     barrier()
+    sim.work(reset=True)
     # Device-timed region: K steps in one batch, CUDA events on the simulation's stream.
     with Clocks(local) as clk:
         sim.step(args.steps)
     barrier()
     launches, ms = sim.last_launches()
     st = sim.state
+    work = sim.work(reset=True)
     from natray_b200.replicas import max_over_ranks
     t_dev = max_over_ranks(ms * 1e-3)
     value = n_particles * args.steps * world / t_dev
+    # The step-level roofline: the algorithmic bytes of the K timed steps, from the work the
+    # steps counted on the device (blocks, water cells x iterations, gas cells x air substeps,
+    # rubber substeps, spray), over their device time.
+    step_bytes = sim.algorithmic_bytes(work)
 
     # End to end through the public API: one ntr_sim_step call per step, each uploading the
     # step's parameters from host memory and reading the state back.
@@ -242,13 +286,16 @@ def run_native(args, rank, world, local):
     alg = algorithmic_bytes(top, st2, n_particles, iters)
     peak, peak_kind = hbm_peak()
     achieved = alg / per_launch_s / 1e9 if alg > 0 else None
-    traffic = None
+    # DRAM traffic of one launch of that kernel, from the ncu capture summarised in profiles/
+    # (the file gives the command that made it; ncu's figures cannot be taken inside this run).
+    traffic, traffic_src = None, None
     tf = ROOT / "profiles" / f"{top.split('<')[0]}.md"
     if tf.exists():
         for line in tf.read_text().splitlines():
             if line.startswith("traffic_per_launch_bytes:"):
                 try:
                     traffic = float(line.split(":", 1)[1].strip())
+                    traffic_src = f"profiles/{tf.name}"
                 except ValueError:
                     pass
 
@@ -287,23 +334,16 @@ def run_native(args, rank, world, local):
             "gpu_launches": int(launches),
             "roofline": {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": alg, "launch_ms": per_launch_s * 1e3, "share": round(kms / tot, 4)},
+                         "traffic_source": traffic_src, "algorithmic_bytes_per_launch": alg,
+                         "launch_ms": per_launch_s * 1e3, "share": round(kms / tot, 4)},
+            "step_roofline": {"bound": "hbm", "achieved": step_bytes / t_dev / 1e9 * world, "peak": peak, "unit": "GB/s",
+                              "frac": step_bytes / t_dev / 1e9 / peak, "peak_kind": peak_kind,
+                              "algorithmic_bytes_per_step": step_bytes / max(work["steps"], 1), "work": work,
+                              "note": "sum over the timed steps of 160 Np + 160 cells + 48 K Nw + (256 Nv + 32 Nt) Sm "
+                                      "+ 44 Sa Na + 48 Nspray, counted on the device by the steps, over their device time"},
             "kernel_shares": shares,
             "clocks": clk.summary(),
         }
-        if top == "k_p2g":
-            # P2G's limit is not HBM but its shared-memory atomics: 4 lattices x 27 nodes x
-            # (value, weight) per particle. Their rate, in warp-wide atomics per SM cycle.
-            atomics = 216 * n_particles
-            sm_hz = (result["clocks"].get("sm_mhz") or 1965.0) * 1e6
-            n_sms = torch.cuda.get_device_properties(0).multi_processor_count
-            result["roofline"]["limit"] = {
-                "kind": "shared-memory atomics",
-                "atomics_per_launch": atomics,
-                "warp_atomics_per_sm_cycle": atomics / 32 / (per_launch_s * sm_hz * n_sms),
-                "note": "timing copies of the kernel: 126 us as built, 20 us with plain shared stores in place of the "
-                        "atomics, 114 us with no two lanes of a warp on one node",
-            }
     if rank == 0 and world == 1 and args.keyframes:
         result["keyframes"] = keyframe_bench(sim, args.keyframes, peak, int(w.h.wet_res))
     sim.close()
@@ -314,21 +354,27 @@ def run_native(args, rank, world, local):
     return result
 
 
-def cpu_baseline(sample_steps: int, threads: int | None = None) -> dict:
+def cpu_baseline(sample_steps: int, threads: int | None = None, warmup: int = 1) -> dict:
     """The CPU restatement of the reference's step (FP32) on this host's cores, on a bounded
-    sample of the same workload: `sample_steps` steps of the 1M scene."""
+    sample of the same workload: `sample_steps` steps of the 1M scene after `warmup` untimed
+    steps taken one a batch, as the native arm takes its warm-up. The world comes from the
+    library's scene builder (CPU code, the reference's balloon.rs/bullet.rs/flight.rs restated):
+    the only part of libnatray.so this arm uses, and it runs before the timed steps."""
     from natray_b200 import Params, World, build_world
     from oracle.py import Oracle, set_threads, threads as nthreads
     cores = threads or os.cpu_count() or 1
     set_threads(cores)
     w = build_world(Params(**SCENE))
     o = Oracle(w.blob, fp64_dots=False)
-    o.step(1)  # the first step (allocation and first-touch) outside the sample
+    for _ in range(max(warmup, 1)):
+        o.step(1)
     t0 = time.perf_counter()
     n = o.step(sample_steps)
     dt = time.perf_counter() - t0
     return {"value": w.h.n_particles * n / dt, "unit": "particle-substeps/s", "cores": nthreads(), "kind": "port",
-            "sample": f"{n} steps of the 1M-particle scene after one untimed step, oracle FP32 with the reference's FP32 sums, OpenMP"}
+            "sample": f"steps {max(warmup, 1) + 1}-{max(warmup, 1) + n} of the 1M-particle scene (after {max(warmup, 1)} untimed "
+                      f"steps), oracle FP32 with the reference's FP32 sums, OpenMP; the scene built by the library's CPU "
+                      f"scene builder before timing"}
 
 
 def batch_and_serve(args) -> dict:
@@ -386,9 +432,9 @@ def main():
         if rank != 0:
             return
         steps = max(1, min(args.steps, args.cpu_sample))
-        cb = cpu_baseline(steps)
+        cb = cpu_baseline(steps, warmup=args.warmup)
         line = {"metric": METRIC, "value": cb["value"], "unit": "particle-substeps/s", "n_gpus": args.gpus, "steps": steps,
-                "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded scene builder of the reference)", "impl": "reference",
                 "config": {"workload": WORKLOAD, "parallelism": "host cores", "n_particles": None},
                 "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "particle-substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -400,7 +446,7 @@ def main():
     if rank == 0 and res is not None:
         if world == 1:
             res.update(batch_and_serve(args))
-            res["cpu_baseline"] = cpu_baseline(args.cpu_sample)
+            res["cpu_baseline"] = cpu_baseline(args.cpu_sample, warmup=args.warmup)
         print(json.dumps(res), flush=True)
 
 

@@ -406,6 +406,17 @@ NTR_API ntr_status ntr_sim_set_batch_steps(ntr_sim* s, uint32_t n);
  * name "name,launches,total_ms" (the reference's NATRAY_PROF, src/sim.rs:594-614, 670-689).
  * With report == NULL only *len (the report's length) is set. */
 NTR_API ntr_status ntr_sim_profile(ntr_sim* s, uint32_t n, uint32_t stop_ns, char* report, size_t cap, size_t* len);
+/* The work the steps did since the simulation was created or restored, or since the last call
+ * with reset != 0, counted on the device by the steps themselves (out[k] for NTR_WORK_*): steps
+ * taken; cells of their blocks (64 per block, summed over the steps); water cells times solver
+ * iterations; rubber substeps; free-gas cells times air substeps; spray slots in use. The
+ * algorithmic bytes of those steps follow from them (160 per particle and step, 160 per cell,
+ * 48 per water cell and iteration, 256 per vertex and 32 per triangle and rubber substep, 44 per
+ * gas cell and air substep, 48 per spray slot): the per-step quantities the reference's
+ * profiler sees through its State readback (src/sim.rs:594-689). Waits for the stream. */
+#define NTR_WORK_FIELDS 6
+enum { NTR_WORK_STEPS = 0, NTR_WORK_CELLS, NTR_WORK_WATER_ITERS, NTR_WORK_MEM_SUBSTEPS, NTR_WORK_GAS_SUBSTEPS, NTR_WORK_SPRAY };
+NTR_API ntr_status ntr_sim_work(ntr_sim* s, uint64_t out[NTR_WORK_FIELDS], int reset);
 /* Kernel launches made by the last ntr_sim_step call, and its device time in ms. */
 NTR_API ntr_status ntr_sim_last_launches(ntr_sim* s, uint64_t* launches, double* device_ms);
 /* The particles in the reference's layout (`Particle`, sim_defs.wgsl:61: 20 f32 each, pos.xyzw,

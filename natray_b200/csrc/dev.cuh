@@ -92,6 +92,11 @@ struct DevState {
     uint32_t bar_count;  // grid barrier of the persistent solver: arrivals (reset per launch)
     uint32_t bar_gen;    // unused
     uint32_t pad[3];
+    // The step's work, for its algorithmic bytes: this step's water and free-gas cells (counted
+    // by k_project), and totals since ntr_sim_work last cleared them (added by the step's last
+    // kernel): NTR_WORK_STEPS .. NTR_WORK_SPRAY of include/natray.h.
+    uint32_t n_water, n_gas;
+    unsigned long long work[6];
 };
 
 // Every pointer and size a kernel may need. Passed by value.

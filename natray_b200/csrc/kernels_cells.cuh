@@ -289,12 +289,18 @@ __device__ __forceinline__ float pressure_of(const Dev& D, uint32_t cell) {
 
 // ---- project, extend, fluid.wgsl:580-674 -------------------------------------------------------------
 __global__ void k_project(Dev D) {
-    const DevState* st = D.st;
+    DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
     const float k = dt_of(st) / (D.U->fluid[0] * g.h);
+    __shared__ uint32_t s_cnt[2];
+    if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    uint32_t n_water = 0, n_gas = 0;  // the step's cells by type, for its work counts
     CELL_LOOP(D, st) {
         float ty = cfv(D, F_TYPE, cell);
+        n_water += ty == WATER_T;
+        n_gas += ty == GAS_T;
 #pragma unroll
         for (uint32_t d = 0; d < 3; d++) {
             uint32_t nb = neighbour(g, cell, ed(d, -1));
@@ -303,6 +309,17 @@ __global__ void k_project(Dev D) {
             if (ty != SOLID_T && nt != SOLID_T && (ty == WATER_T || nt == WATER_T)) u -= k * (pressure_of(D, cell) - pressure_of(D, nb));
             *cfp(D, F_U + d, cell) = u;
         }
+    }
+    n_water = __reduce_add_sync(0xffffffffu, n_water);
+    n_gas = __reduce_add_sync(0xffffffffu, n_gas);
+    if ((threadIdx.x & 31u) == 0) {
+        atomicAdd(&s_cnt[0], n_water);
+        atomicAdd(&s_cnt[1], n_gas);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        atomicAdd(&st->n_water, s_cnt[0]);
+        atomicAdd(&st->n_gas, s_cnt[1]);
     }
 }
 

@@ -388,7 +388,20 @@ __global__ void k_spray_emit(Dev D) {
 __global__ void k_spray_commit(Dev D) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
-    if (threadIdx.x == 0 && blockIdx.x == 0) st->s.spray_count += 5u * st->nbrk;
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        st->s.spray_count += 5u * st->nbrk;
+        // The step's work (its algorithmic bytes are counted from these): blocks, water cells
+        // times solver iterations, rubber substeps, free-gas cells times air substeps, spray
+        // slots in use.
+        const ntr_gpu_params* U = D.U;
+        st->work[0] += 1ull;
+        st->work[1] += 64ull * min(st->s.n_blocks, D.cap_blocks);
+        st->work[2] += (unsigned long long)st->n_water * st->s.solve_iters;
+        st->work[3] += U->mem[1];
+        st->work[4] += (unsigned long long)st->n_gas * U->mem[2];
+        st->work[5] += min(st->s.spray_count, D.spray_cap);
+        st->n_water = st->n_gas = 0u;
+    }
 }
 
 // ---- the zero-length measuring substep and diagnostics --------------------------------------------

@@ -1108,6 +1108,16 @@ NTR_API ntr_status ntr_sim_autotune(ntr_sim* sim, uint32_t steps, ntr_tuning* be
     return NTR_OK;
 }
 
+NTR_API ntr_status ntr_sim_work(ntr_sim* sim, uint64_t out[NTR_WORK_FIELDS], int reset) {
+    GUARD(sim);
+    if (!out) return fail(NTR_E_INVALID, "null argument");
+    static_assert(sizeof(DevState::work) == NTR_WORK_FIELDS * sizeof(uint64_t), "work counters");
+    CU(cudaMemcpyAsync(out, &S.D.st->work[0], sizeof(DevState::work), cudaMemcpyDeviceToHost, S.stream));
+    if (reset) CU(cudaMemsetAsync(&S.D.st->work[0], 0, sizeof(DevState::work), S.stream));
+    CU(cudaStreamSynchronize(S.stream));
+    return NTR_OK;
+}
+
 NTR_API ntr_status ntr_sim_last_launches(ntr_sim* sim, uint64_t* launches, double* device_ms) {
     GUARD(sim);
     if (launches) *launches = S.last_launches;

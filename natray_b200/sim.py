@@ -173,6 +173,26 @@ class Sim:
         check(lib().ntr_sim_autotune(self._h, steps, C.byref(t), C.byref(ms)))
         return {k: getattr(t, k) for k, _ in t._fields_ if k != "pad"}, ms.value
 
+    WORK = ("steps", "cells", "water_iters", "mem_substeps", "gas_substeps", "spray")
+
+    def work(self, reset: bool = False) -> dict:
+        """The steps' work counted on the device since creation, a restore or the last reset:
+        steps, block cells, water cells x solver iterations, rubber substeps, gas cells x air
+        substeps, spray slots (each summed over the steps)."""
+        out = (C.c_uint64 * 6)()
+        check(lib().ntr_sim_work(self._h, out, int(reset)))
+        return dict(zip(self.WORK, list(out)))
+
+    def algorithmic_bytes(self, work: dict) -> float:
+        """Bytes the steps counted in `work` must move at the least: 160 per particle and step
+        (its state read and written), 160 per block cell (transfer sums, cell fields, projection,
+        the G2P read, the clear), 48 per water cell and solver iteration, 256 per vertex and 32
+        per triangle and rubber substep, 44 per gas cell and air substep, 48 per spray slot."""
+        i = self.info
+        return (160.0 * i.n_particles * work["steps"] + 160.0 * work["cells"] + 48.0 * work["water_iters"]
+                + (256.0 * i.n_verts + 32.0 * i.n_tris) * work["mem_substeps"] + 44.0 * work["gas_substeps"]
+                + 48.0 * work["spray"])
+
     def last_launches(self) -> tuple[int, float]:
         n, ms = C.c_uint64(), C.c_double()
         check(lib().ntr_sim_last_launches(self._h, C.byref(n), C.byref(ms)))
