@@ -417,6 +417,13 @@ NTR_API ntr_status ntr_sim_profile(ntr_sim* s, uint32_t n, uint32_t stop_ns, cha
 #define NTR_WORK_FIELDS 6
 enum { NTR_WORK_STEPS = 0, NTR_WORK_CELLS, NTR_WORK_WATER_ITERS, NTR_WORK_MEM_SUBSTEPS, NTR_WORK_GAS_SUBSTEPS, NTR_WORK_SPRAY };
 NTR_API ntr_status ntr_sim_work(ntr_sim* s, uint64_t out[NTR_WORK_FIELDS], int reset);
+/* For tests of the failure path; no counterpart in the reference (whose solver loop is host
+ * dispatches, fluid.wgsl:572-577, src/sim.rs:634-647). The persistent pressure solve's grid
+ * barriers give up after `spins` polls (0: the default, 2^24), setting an error that the step
+ * reports as NTR_E_TIMEOUT, and CTA `skip_cta` of the solve (0xFFFFFFFF: none) skips its first
+ * arrival, so that every other CTA's wait runs out. Every CTA then returns: the kernel ends, the
+ * context stays usable, and the state is that of a failed step (restore a snapshot). */
+NTR_API ntr_status ntr_sim_test_barrier(ntr_sim* s, uint32_t spins, uint32_t skip_cta);
 /* Kernel launches made by the last ntr_sim_step call, and its device time in ms. */
 NTR_API ntr_status ntr_sim_last_launches(ntr_sim* s, uint64_t* launches, double* device_ms);
 /* The particles in the reference's layout (`Particle`, sim_defs.wgsl:61: 20 f32 each, pos.xyzw,

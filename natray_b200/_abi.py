@@ -201,6 +201,7 @@ _SIGS = {
     "ntr_sim_profile": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "ntr_sim_last_launches": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
     "ntr_sim_work": (C.c_int, [_P, C.POINTER(C.c_uint64), C.c_int]),
+    "ntr_sim_test_barrier": (C.c_int, [_P, C.c_uint32, C.c_uint32]),
     "ntr_sim_conservation": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "ntr_sort_by_block_noalloc": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P, _P]),
     "ntr_sim_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),

@@ -106,6 +106,9 @@ struct Dev {
     float4 *pos, *vel, *c0, *c1, *c2;
     uint32_t Np, Nv, Nt, cap_blocks, cap_cells, nwords, spray_cap, wet_res;
     uint32_t n_tiles, radix_passes, scan_ctas, fp64_dots;
+    // The solver's grid barriers: polls before a wait gives up, and a CTA that skips its first
+    // arrival (NONE: none) so that the others' waits run out (ntr_sim_test_barrier).
+    uint32_t bar_spins, bar_skip;
     uint32_t* mask[2];
     uint32_t* prefix[2];
     uint32_t* block_list[2];

@@ -169,11 +169,11 @@ __device__ __forceinline__ bool exchange(const Dev& D, DevState* st, uint32_t& g
     if (threadIdx.x == 0) {
         // Release: this CTA's writes (ordered before by the barrier above) before the arrival.
         const uint32_t target = gen * G;
-        atom_add_release(&st->bar_count, 1u);
+        if (!(gen == 1u && c == D.bar_skip)) atom_add_release(&st->bar_count, 1u);
         uint32_t ok = 1u;
         for (uint32_t spins = 0; ld_acquire(&st->bar_count) < target;) {
             // Give up after a bounded wait, or at once when another CTA of the solve has.
-            if (++spins > BARRIER_SPINS || ((spins & 1023u) == 0u && *(volatile uint32_t*)&st->err != 0u)) {
+            if (++spins > D.bar_spins || ((spins & 1023u) == 0u && *(volatile uint32_t*)&st->err != 0u)) {
                 atomicOr(&st->err, 1u);
                 ok = 0u;
                 break;

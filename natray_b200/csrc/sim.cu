@@ -37,8 +37,10 @@ namespace ntr {
     } while (0)
 
 struct GraphKey {
-    uint32_t n_mem, n_air, fp64, part;
-    bool operator<(const GraphKey& o) const { return std::tie(n_mem, n_air, fp64, part) < std::tie(o.n_mem, o.n_air, o.fp64, o.part); }
+    uint32_t n_mem, n_air, fp64, part, size;
+    bool operator<(const GraphKey& o) const {
+        return std::tie(n_mem, n_air, fp64, part, size) < std::tie(o.n_mem, o.n_air, o.fp64, o.part, o.size);
+    }
 };
 
 struct StepGraph {
@@ -67,6 +69,9 @@ struct Sim {
     int device = 0;
     int sms = 148;
     uint32_t coop_ctas = 148;
+    // The scene's size class for its launch grids: its block count at the last read-back with a
+    // quarter to spare, rounded up to a power of two (0: not known yet, full grids).
+    uint32_t size_class = 0;
     cudaError_t launch_err = cudaSuccess;
     cudaStream_t stream = nullptr;
     cudaStream_t aux = nullptr;   // the second stream of the step's forks
@@ -183,6 +188,8 @@ static ntr_status allocate(Sim& S) {
     if (D.n_tiles == 0) D.n_tiles = 1;
     D.radix_passes = radix_passes_for(D.cap_blocks);
     D.fp64_dots = S.fp64;
+    D.bar_spins = BARRIER_SPINS;
+    D.bar_skip = NONE;
     ntr_status r;
 #define AL(p, n) \
     if ((r = S.alloc(p, n)) != NTR_OK) return r
@@ -443,13 +450,39 @@ static uint64_t enqueue_solve(Sim& S, cudaStream_t s, const Dev* jobs, uint32_t 
 
 enum { PART_PRE = 1, PART_POST = 2, PART_FULL = 3 };
 
+// Launch grids sized to the scene. The per-cell, per-block and solver kernels loop over their
+// work, so any grid gives the same results, bit for bit; a scene of a few hundred blocks gets as
+// many CTAs as its cells and blocks can use (a cell a thread, a block a CTA, a block a solver
+// warp) instead of the GPU's worth its kernels would otherwise spend launching CTAs with nothing
+// to do. The launch-shape tuning (ntr_sim_set_tuning) caps them.
+struct Grids {
+    uint32_t cell, blk, solve;
+};
+static Grids launch_grids(const Sim& S) {
+    Grids g{(uint32_t)S.sms * S.tune.cell_ctas_per_sm, (uint32_t)S.sms * S.tune.block_ctas_per_sm,
+            S.tune.solve_ctas ? S.tune.solve_ctas : S.coop_ctas};
+    const uint32_t nb = S.size_class;
+    if (nb) {
+        g.cell = std::max(1u, std::min(g.cell, (nb * 64u + 255u) / 256u));
+        g.blk = std::max(1u, std::min(g.blk, nb));
+        if (!S.tune.solve_ctas) g.solve = std::max(1u, std::min(g.solve, (nb + SOLVE_T / 32 - 1) / (SOLVE_T / 32)));
+    }
+    return g;
+}
+static uint32_t size_class_of(uint32_t n_blocks) {
+    if (n_blocks == 0) return 0;
+    uint32_t want = n_blocks + n_blocks / 4 + 1, c = 64;
+    while (c < want && c < (1u << 30)) c <<= 1;
+    return c;
+}
+
 // The step on stream `s`: the part before the pressure solve (PART_PRE), the part after it
 // (PART_POST), or both with the solve between (PART_FULL).
 static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_air, bool fp64, Prof* prof, int part = PART_FULL) {
     Dev& D = S.D;
     uint64_t n = 0;
-    const uint32_t G_cell = (uint32_t)S.sms * S.tune.cell_ctas_per_sm;
-    const uint32_t G_blk = (uint32_t)S.sms * S.tune.block_ctas_per_sm;
+    const Grids grids = launch_grids(S);
+    const uint32_t G_cell = grids.cell, G_blk = grids.blk;
     const uint32_t g_vert = (D.Nv + 255) / 256 ? (D.Nv + 255) / 256 : 1;
     const uint32_t g_tri = std::max((D.Nt + 255) / 256, 1u);
     const uint32_t n_shots = S.U.mem[3] ? S.U.mem[3] : 1;
@@ -533,7 +566,7 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     // The pressure solve's grid barrier counter starts from zero.
     cudaMemsetAsync(&D.st->bar_count, 0, 4, s);
     }
-    if (part == PART_FULL) n += enqueue_solve(S, s, nullptr, 1u, fp64, prof, S.tune.solve_ctas ? S.tune.solve_ctas : S.coop_ctas);
+    if (part == PART_FULL) n += enqueue_solve(S, s, nullptr, 1u, fp64, prof, grids.solve);
     if (part & PART_POST) {
     L(k_project, G_cell, 256, D);
     L(k_extend_1, G_cell, 256, D);
@@ -596,7 +629,9 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
 
 // The step (or a part of it, for a batch) captured as a graph, cached by its shape.
 static ntr_status get_graph(Sim& S, StepGraph*& out, int part = 3) {
-    GraphKey key{part == 1 ? 0u : S.host.h.substeps, part == 1 ? 0u : S.host.h.air_substeps, S.fp64, (uint32_t)part};
+    // The size class follows the block count the last read-back saw.
+    if (S.h_state) S.size_class = size_class_of(std::max(S.h_state->s.n_blocks, S.h_state->s.n_blocks_prev));
+    GraphKey key{part == 1 ? 0u : S.host.h.substeps, part == 1 ? 0u : S.host.h.air_substeps, S.fp64, (uint32_t)part, S.size_class};
     auto it = S.graphs.find(key);
     if (it != S.graphs.end()) {
         out = &it->second;
@@ -639,8 +674,11 @@ static ntr_status run_batch(Sim& S, uint32_t n, uint32_t stop, uint32_t* taken, 
     // The solver's most-iterations and out-of-iterations counters start from zero in every batch.
     CU(cudaMemsetAsync(&S.D.st->s.iters_max, 0, 8, S.stream));
     StepGraph* g = nullptr;
-    if (!prof)
+    if (!prof) {
         if ((r = get_graph(S, g)) != NTR_OK) return r;
+    } else {
+        S.size_class = size_class_of(std::max(S.h_state->s.n_blocks, S.h_state->s.n_blocks_prev));
+    }
     const uint32_t before = S.h_state->s.step;
     uint64_t launches = 0;
     CU(cudaEventRecord(S.ev0, S.stream));
@@ -1105,6 +1143,20 @@ NTR_API ntr_status ntr_sim_autotune(ntr_sim* sim, uint32_t steps, ntr_tuning* be
     if ((r = ntr_sim_set_tuning(sim, &cur)) != NTR_OK) return r;
     if (best) *best = cur;
     if (best_ms) *best_ms = cur_ms;
+    return NTR_OK;
+}
+
+NTR_API ntr_status ntr_sim_test_barrier(ntr_sim* sim, uint32_t spins, uint32_t skip_cta) {
+    GUARD(sim);
+    CU(cudaStreamSynchronize(S.stream));
+    S.D.bar_spins = spins ? spins : BARRIER_SPINS;
+    S.D.bar_skip = skip_cta;
+    // The kernels take the pointer table by value: the captured step graphs hold the old one.
+    for (auto& kv : S.graphs) {
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+    }
+    S.graphs.clear();
     return NTR_OK;
 }
 
