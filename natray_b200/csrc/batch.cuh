@@ -1,12 +1,18 @@
 // Batches of independent scenes on one GPU (include/natray.h, ntr_batch_*): the serving engine.
 //
-// Every admitted scene is a Sim of its own (device-resident state, its own streams and cached
-// graphs). A batch step runs, per scene, the step's part before the pressure solve on the
-// scene's stream; then ONE cooperative launch solves every scene's system, the GPU's CTAs split
-// over the scenes by their block counts (k_solve, solve_split); then each scene's part after the
-// solve, again on its own stream, so the scenes' work overlaps on the device. The host reads the
-// scenes' states back once per ntr_batch_step call and adapts each one's solver iterations and
-// substeps as ntr_sim_step does, so a scene's results are those of the scene run alone.
+// Every admitted scene keeps its own device-resident state (a Sim in a slot's memory region).
+// A batch step runs the step of EVERY scene with one launch per kernel: each launch gives each
+// scene a contiguous range of its CTAs (the scene's own grid for that kernel, sized to the
+// scene), and every CTA finds its scene's pointer table through a prefix table of first CTAs
+// (Multi, multi_cta). The pressure systems of all scenes are solved by ONE cooperative launch
+// that splits the GPU's CTAs over the scenes by their block counts (k_solve_batch). The launch
+// sequence is the one-scene step's, on the same three streams, captured once as a CUDA graph
+// for the batch's current scenes and shapes and replayed per step; scenes differ in their
+// rubber and air substep counts (each scene's kernels skip the substeps past its own) and in
+// how many steps they take in a call (each scene's step budget stops it, as a stop time would).
+// The host reads the scenes' states back once per ntr_batch_step call and adapts each one's
+// solver iterations and substeps as ntr_sim_step does, so a scene's results are those of the
+// scene run alone with the same chunks of steps.
 //
 // Included at the end of sim.cu (it uses the Sim internals there).
 #pragma once
@@ -15,6 +21,10 @@
 #include <deque>
 
 namespace ntr {
+
+// The kinds of per-scene grids a step's launches use (enqueue_step's grid expressions).
+enum GridKind { GK_ONE, GK_CELL, GK_WORDS, GK_MARK, GK_SCAN, GK_TILES, GK_RSCAN, GK_BOUNDS, GK_BLK, GK_SHOTS, GK_PATCH,
+                GK_VERT, GK_VERT4, GK_TRI, GK_COUNT };
 
 struct BatchSlot {
     std::unique_ptr<Sim> sim;
@@ -36,10 +46,18 @@ struct Batch {
     uint64_t steps = 0;
     uint32_t ctas = 0;  // CTAs of the joint solve
     std::vector<BatchSlot> slots;
-    cudaStream_t solve_stream = nullptr;
+    cudaStream_t solve_stream = nullptr;  // the batch step's main stream
+    cudaStream_t aux = nullptr, aux2 = nullptr;  // its side streams (as a one-scene step's)
     cudaEvent_t ev_solve = nullptr;
+    cudaEvent_t ev_fork[3] = {nullptr, nullptr, nullptr}, ev_join[3] = {nullptr, nullptr, nullptr};
+    std::vector<cudaEvent_t> ev_sub;
     Dev* d_jobs = nullptr;  // the pointer tables of the scenes in the current step's order
+    uint32_t* d_first = nullptr;  // per kind of grid, the scenes' first CTAs (GK_COUNT x (max_scenes + 1))
     uint32_t n_jobs_cap = 0;
+    // The captured step of the current scenes and shapes, and what it was captured for.
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uint32_t> graph_key;
     // Every call on the batch holds this lock: calls from several host threads take turns.
     std::mutex mu;
     // Scenes queued by any thread (ntr_batch_enqueue), admitted in order at the start of the
@@ -55,6 +73,17 @@ struct Batch {
 
     ~Batch() {
         DeviceScope scope(device);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (int k = 0; k < 3; k++) {
+            if (ev_fork[k]) cudaEventDestroy(ev_fork[k]);
+            if (ev_join[k]) cudaEventDestroy(ev_join[k]);
+        }
+        for (cudaEvent_t e : ev_sub)
+            if (e) cudaEventDestroy(e);
+        if (aux) cudaStreamDestroy(aux);
+        if (aux2) cudaStreamDestroy(aux2);
+        if (d_first) cudaFree(d_first);
         for (auto& s : slots) {
             s.sim.reset();
             if (s.ev_pre) cudaEventDestroy(s.ev_pre);
@@ -102,12 +131,20 @@ static ntr_status batch_create(int device, uint32_t max_scenes, uint64_t budget,
     B->reserve = (uint64_t)1 << 30;
     B->slots.resize(max_scenes);
     CU(cudaStreamCreateWithFlags(&B->solve_stream, cudaStreamNonBlocking));
+    CU(cudaStreamCreateWithFlags(&B->aux, cudaStreamNonBlocking));
+    CU(cudaStreamCreateWithFlags(&B->aux2, cudaStreamNonBlocking));
     CU(cudaEventCreateWithFlags(&B->ev_solve, cudaEventDisableTiming));
+    for (int k = 0; k < 3; k++) {
+        CU(cudaEventCreateWithFlags(&B->ev_fork[k], cudaEventDisableTiming));
+        CU(cudaEventCreateWithFlags(&B->ev_join[k], cudaEventDisableTiming));
+    }
+    CU(cudaFuncSetAttribute(k_p2g_m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2G_SMEM));
     for (auto& s : B->slots) {
         CU(cudaEventCreateWithFlags(&s.ev_pre, cudaEventDisableTiming));
         CU(cudaMallocHost((void**)&s.h_state, sizeof(DevState)));
     }
     CU(cudaMalloc((void**)&B->d_jobs, sizeof(Dev) * max_scenes));
+    CU(cudaMalloc((void**)&B->d_first, sizeof(uint32_t) * GK_COUNT * (max_scenes + 1)));
     B->n_jobs_cap = max_scenes;
     out = B.release();
     return NTR_OK;
@@ -163,11 +200,120 @@ static ntr_status batch_retire(Batch& B, uint32_t slot) {
     return NTR_OK;
 }
 
-// n steps of every unfinished scene. The scenes are ordered by the steps they take in this call,
-// longest first, so the scenes that still step at step k are a prefix of the jobs table, and
-// one table serves every step of the call.
+
+static void scene_grids(const Sim& S, uint32_t g[GK_COUNT]) {
+    const Dev& D = S.D;
+    const Grids gr = launch_grids(S);
+    g[GK_ONE] = 1;
+    g[GK_CELL] = gr.cell;
+    g[GK_WORDS] = std::max((D.nwords + 255) / 256, 1u);
+    g[GK_MARK] = (uint32_t)(((uint64_t)warp_round(D.Np) + warp_round(D.cap_blocks) + warp_round(D.Nv) + 255) / 256);
+    g[GK_SCAN] = D.scan_ctas;
+    g[GK_TILES] = D.n_tiles;
+    g[GK_RSCAN] = 256;
+    g[GK_BOUNDS] = (D.Np + 1 + 255) / 256;
+    g[GK_BLK] = gr.blk;
+    g[GK_SHOTS] = S.U.mem[3] ? S.U.mem[3] : 1;
+    g[GK_PATCH] = (NTR_MAX_PATCHES + BULLET_PW - 1) / BULLET_PW;
+    g[GK_VERT] = (D.Nv + 255) / 256 ? (D.Nv + 255) / 256 : 1;
+    g[GK_VERT4] = (uint32_t)(((uint64_t)D.Nv * 4 + 255) / 256);
+    g[GK_TRI] = std::max((D.Nt + 255) / 256, 1u);
+}
+
+// The step of every scene of the batch, one launch per kernel over all of them: the launch
+// sequence of enqueue_step (on the same three streams), with each scene's own grid within each
+// launch. `tot` is each kind's CTAs over all scenes.
+static uint64_t enqueue_step_multi(Batch& B, uint32_t n_jobs, const uint32_t* tot, uint32_t max_shots, uint32_t n_mem,
+                                   uint32_t n_air, bool fp64, Sim& S0) {
+    cudaStream_t s = B.solve_stream, a = B.aux, a2 = B.aux2;
+    uint64_t nl = 0;
+    auto M = [&](int kind) { return Multi{B.d_jobs, B.d_first + (size_t)kind * (B.max_scenes + 1), n_jobs}; };
+#define LM(kern, kind, threads, strm, ...)                                              \
+    do {                                                                                \
+        if (tot[kind]) kern<<<tot[kind], (threads), 0, (strm)>>>(M(kind), ##__VA_ARGS__); \
+        nl++;                                                                           \
+    } while (0)
+    auto fork = [&](int k, cudaStream_t to) {
+        cudaEventRecord(B.ev_fork[k], s);
+        cudaStreamWaitEvent(to, B.ev_fork[k], 0);
+    };
+    auto join = [&](int k, cudaStream_t from) {
+        cudaEventRecord(B.ev_join[k], from);
+        cudaStreamWaitEvent(s, B.ev_join[k], 0);
+    };
+    LM(k_begin_step_m, GK_ONE, 32, s);
+    fork(0, a);
+    LM(k_clear_acc_m, GK_CELL, 256, a);
+    LM(k_clear_mask_m, GK_WORDS, 256, s);
+    LM(k_mark_m, GK_MARK, 256, s);
+    LM(k_scan_words_a_m, GK_SCAN, SCAN_T, s);
+    LM(k_scan_words_b_m, GK_SCAN, SCAN_T, s);
+    cudaEventRecord(B.ev_fork[1], s);
+    cudaStreamWaitEvent(a, B.ev_fork[1], 0);
+    LM(k_mem_splat_m, GK_VERT, 256, a);
+    LM(k_air_carry_m, GK_CELL, 256, a);
+    LM(k_keys_hist_m, GK_TILES, KEYS_T, s);
+    for (uint32_t p = 0; p < 2; p++) {  // at most two passes below 65,536 blocks
+        if (p >= 2) LM(k_radix_hist_m, GK_TILES, RADIX_T, s, p);
+        LM(k_radix_scan_m, GK_RSCAN, 256, s, p);
+        LM(k_radix_scatter_m, GK_TILES, SCAT_T, s, p);
+    }
+    LM(k_block_bounds_m, GK_BOUNDS, 256, s);
+    if (tot[GK_BLK]) k_p2g_m<<<tot[GK_BLK], P2G_T, P2G_SMEM, s>>>(M(GK_BLK));
+    nl++;
+    LM(k_p2g_gather_m, GK_CELL, 256, s);
+    join(0, a);
+    LM(k_grid_prep_m, GK_CELL, 256, s);
+    LM(k_air_fill_m, GK_CELL, 256, s);
+    LM(k_bullet_prep_m, GK_SHOTS, 32, s);
+    if (tot[GK_PATCH]) k_bullet_patch_m<<<dim3(tot[GK_PATCH], max_shots), BULLET_PW * 32, 0, s>>>(M(GK_PATCH));
+    nl++;
+    LM(k_bullet_finish_m, GK_SHOTS, 256, s);
+    LM(k_bullet_apply_m, GK_CELL, 256, s);
+    // Every scene's grid barrier counter starts from zero (k_solve_batch keeps one per scene).
+    LM(k_solve_reset_m, GK_ONE, 32, s);
+    nl += enqueue_solve(S0, s, B.d_jobs, n_jobs, fp64, nullptr, B.ctas);
+    LM(k_project_m, GK_CELL, 256, s);
+    LM(k_extend_1_m, GK_CELL, 256, s);
+    LM(k_extend_2_m, GK_CELL, 256, s);
+    const uint32_t n_sub = std::max(n_mem, n_air);
+    while (B.ev_sub.size() < 2 * (size_t)n_sub) {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) S0.launch_err = cudaErrorMemoryAllocation;
+        B.ev_sub.push_back(e);
+    }
+    fork(1, a);
+    cudaEventRecord(B.ev_fork[2], s);
+    cudaStreamWaitEvent(a2, B.ev_fork[2], 0);
+    LM(k_mem_sample_m, GK_VERT4, 256, a);
+    for (uint32_t i = 0; i < n_sub; i++) {
+        if (i < n_mem) {
+            if (i >= 1 && i - 1 < n_air) cudaStreamWaitEvent(a, B.ev_sub[2 * (i - 1) + 1], 0);
+            LM(k_mem_tri_m, GK_TRI, 256, a, i, (int)(i % 2));
+            LM(k_mem_substep_m, GK_VERT, 256, a, i, (int)(i % 2));
+            cudaEventRecord(B.ev_sub[2 * i], a);
+        }
+        if (i < n_air) {
+            if (i >= 1 && i - 1 < n_mem) cudaStreamWaitEvent(a2, B.ev_sub[2 * (i - 1)], 0);
+            LM(k_air_substep_m, GK_CELL, 256, a2, i, (int)(i % 2));
+            cudaEventRecord(B.ev_sub[2 * i + 1], a2);
+        }
+    }
+    LM(k_spray_update_m, GK_CELL, 256, a);
+    LM(k_g2p_m<128>, GK_BLK, 128, s);
+    join(1, a);
+    cudaEventRecord(B.ev_join[2], a2);
+    cudaStreamWaitEvent(s, B.ev_join[2], 0);
+    LM(k_spray_scan_m, GK_ONE, 1024, s);
+    LM(k_spray_emit_m, GK_CELL, 256, s);
+    LM(k_spray_commit_m, GK_ONE, 32, s);
+#undef LM
+    return nl;
+}
+
+// n steps of every unfinished scene: each scene takes min(n, its steps left) (its step budget
+// stops it after those), all of them in the same replays of the batch's step graph.
 static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active) {
-    CU(cudaSetDevice(B.device));
     std::vector<uint32_t> order;
     std::vector<uint32_t> todo(B.max_scenes, 0u);
     for (uint32_t i = 0; i < B.max_scenes; i++) {
@@ -178,72 +324,94 @@ static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active) {
     }
     active = (uint32_t)order.size();
     if (order.empty() || n == 0) return NTR_OK;
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return todo[a] > todo[b]; });
-    // The scenes' pointer tables, and each scene's parameters for this call (Sim::run).
-    std::vector<Dev> jobs(order.size());
+    const uint32_t n_jobs = (uint32_t)order.size();
+    cudaStream_t s = B.solve_stream;
+    // Each scene's parameters for this call (Sim::run) and its step budget, then the pointer
+    // tables and the grids of the scenes in order.
+    std::vector<Dev> jobs(n_jobs);
+    std::vector<uint32_t> first((size_t)GK_COUNT * (B.max_scenes + 1), 0u), tot(GK_COUNT, 0u);
+    std::vector<uint32_t> key;
+    uint32_t fp64 = B.slots[order[0]].sim->fp64, max_shots = 1, n_mem = 0, n_air = 0, steps = 0;
     ntr_status r;
-    uint32_t fp64 = B.slots[order[0]].sim->fp64;
-    for (size_t j = 0; j < order.size(); j++) {
+    for (uint32_t j = 0; j < n_jobs; j++) {
         Sim& S = *B.slots[order[j]].sim;
         if (S.fp64 != fp64) return fail(NTR_E_INVALID, "the scenes of a batch step must use the same solver precision");
-        jobs[j] = S.D;
         ntr_world_header& h = S.host.h;
         S.U.limits[2] = h.iters;
         S.U.limits[3] = 0xFFFFFFFFu;
         S.U.mem[1] = h.substeps;
         S.U.mem[2] = h.air_substeps;
-        if ((r = push_params(S)) != NTR_OK) return r;
-        CU(cudaMemsetAsync(&S.D.st->s.iters_max, 0, 8, S.stream));
+        CU(cudaMemcpyAsync((void*)S.D.U, &S.U, sizeof(ntr_gpu_params), cudaMemcpyHostToDevice, s));
+        CU(cudaMemsetAsync(&S.D.st->s.iters_max, 0, 8, s));
+        CU(cudaMemcpyAsync(&S.D.st->step_budget, &todo[order[j]], 4, cudaMemcpyHostToDevice, s));
+        S.size_class = size_class_of(std::max(S.h_state->s.n_blocks, S.h_state->s.n_blocks_prev));
+        jobs[j] = S.D;
+        uint32_t g[GK_COUNT];
+        scene_grids(S, g);
+        for (int k = 0; k < GK_COUNT; k++) {
+            first[(size_t)k * (B.max_scenes + 1) + j] = tot[k];
+            tot[k] += g[k];
+        }
+        max_shots = std::max(max_shots, g[GK_SHOTS]);
+        n_mem = std::max(n_mem, h.substeps);
+        n_air = std::max(n_air, h.air_substeps);
+        steps = std::max(steps, todo[order[j]]);
+        key.push_back(order[j]);
+        key.push_back(S.size_class);
     }
-    CU(cudaMemcpyAsync(B.d_jobs, jobs.data(), sizeof(Dev) * jobs.size(), cudaMemcpyHostToDevice, B.solve_stream));
-    std::vector<StepGraph*> pre(order.size()), post(order.size());
-    for (size_t j = 0; j < order.size(); j++) {
-        Sim& S = *B.slots[order[j]].sim;
-        if ((r = get_graph(S, pre[j], PART_PRE)) != NTR_OK) return r;
-        if ((r = get_graph(S, post[j], PART_POST)) != NTR_OK) return r;
-    }
-    std::vector<uint32_t> before(order.size());
-    for (size_t j = 0; j < order.size(); j++) before[j] = B.slots[order[j]].sim->h_state->s.step;
+    for (int k = 0; k < GK_COUNT; k++) first[(size_t)k * (B.max_scenes + 1) + n_jobs] = tot[k];
+    key.insert(key.end(), {n_jobs, fp64, max_shots, n_mem, n_air});
+    CU(cudaMemcpyAsync(B.d_jobs, jobs.data(), sizeof(Dev) * n_jobs, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(B.d_first, first.data(), sizeof(uint32_t) * first.size(), cudaMemcpyHostToDevice, s));
+    // The step graph of these scenes and shapes (captured again when they change).
     Sim& S0 = *B.slots[order[0]].sim;
-    S0.launch_err = cudaSuccess;
-    for (uint32_t k = 0; k < todo[order[0]]; k++) {
-        uint32_t n_k = 0;  // scenes that take step k
-        for (size_t j = 0; j < order.size(); j++) {
-            if (todo[order[j]] <= k) break;
-            Sim& S = *B.slots[order[j]].sim;
-            CU(cudaGraphLaunch(pre[j]->exec, S.stream));
-            CU(cudaEventRecord(B.slots[order[j]].ev_pre, S.stream));
-            CU(cudaStreamWaitEvent(B.solve_stream, B.slots[order[j]].ev_pre, 0));
-            n_k++;
+    if (!B.exec || key != B.graph_key) {
+        if (B.exec) cudaGraphExecDestroy(B.exec), B.exec = nullptr;
+        if (B.graph) cudaGraphDestroy(B.graph), B.graph = nullptr;
+        CU(cudaStreamSynchronize(s));
+        S0.launch_err = cudaSuccess;
+        CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        enqueue_step_multi(B, n_jobs, tot.data(), max_shots, n_mem, n_air, fp64 != 0, S0);
+        cudaError_t le = cudaGetLastError();
+        cudaError_t ce = cudaStreamEndCapture(s, &B.graph);
+        if (S0.launch_err != cudaSuccess) le = S0.launch_err;
+        if (le != cudaSuccess) {
+            if (B.graph) cudaGraphDestroy(B.graph), B.graph = nullptr;
+            return fail(NTR_E_CUDA, std::string("kernel launch during capture: ") + cudaGetErrorString(le));
         }
-        enqueue_solve(S0, B.solve_stream, B.d_jobs, n_k, fp64 != 0, nullptr, B.ctas);
-        CU(S0.launch_err);
-        CU(cudaEventRecord(B.ev_solve, B.solve_stream));
-        for (uint32_t j = 0; j < n_k; j++) {
-            Sim& S = *B.slots[order[j]].sim;
-            CU(cudaStreamWaitEvent(S.stream, B.ev_solve, 0));
-            CU(cudaGraphLaunch(post[j]->exec, S.stream));
-        }
+        if (ce != cudaSuccess) return fail(NTR_E_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce));
+        CU(cudaGraphInstantiate(&B.exec, B.graph, 0));
+        B.graph_key = key;
     }
-    B.steps += todo[order[0]];
-    // States back, one copy per scene, then the host control of each (Sim::run).
-    for (size_t j = 0; j < order.size(); j++) {
+    std::vector<uint32_t> before(n_jobs);
+    for (uint32_t j = 0; j < n_jobs; j++) before[j] = B.slots[order[j]].sim->h_state->s.step;
+    for (uint32_t k = 0; k < steps; k++) CU(cudaGraphLaunch(B.exec, s));
+    B.steps += steps;
+    // States back, then the host control of each scene (Sim::run).
+    for (uint32_t j = 0; j < n_jobs; j++) {
         Sim& S = *B.slots[order[j]].sim;
-        CU(cudaMemcpyAsync(S.h_state, S.D.st, sizeof(DevState), cudaMemcpyDeviceToHost, S.stream));
+        CU(cudaMemcpyAsync(S.h_state, S.D.st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
     }
-    ntr_status first = NTR_OK;
-    for (size_t j = 0; j < order.size(); j++) {
+    CU(cudaStreamSynchronize(s));
+    ntr_status first_err = NTR_OK;
+    for (uint32_t j = 0; j < n_jobs; j++) {
         BatchSlot& sl = B.slots[order[j]];
         Sim& S = *sl.sim;
-        CU(cudaStreamSynchronize(S.stream));
         const ntr_state& st = S.h_state->s;
         sl.done += st.step - before[j];
-        if (st.overflow && first == NTR_OK)
-            first = fail(NTR_E_OVERFLOW, "a scene needs more than " + std::to_string(S.host.h.block_cap) + " grid blocks");
-        if (S.h_state->err && first == NTR_OK) first = fail(NTR_E_TIMEOUT, "a bounded device-side wait gave up");
+        if (st.overflow && first_err == NTR_OK)
+            first_err = fail(NTR_E_OVERFLOW, "a scene needs more than " + std::to_string(S.host.h.block_cap) + " grid blocks");
+        if (S.h_state->err && first_err == NTR_OK) first_err = fail(NTR_E_TIMEOUT, "a bounded device-side wait gave up");
         if (!st.overflow && !S.h_state->err) adapt_after_batch(S.host.h, st);
     }
-    return first;
+    // Each scene's budget back to no limit, for its own calls (snapshots keep their own state).
+    const uint32_t unlimited = 0xFFFFFFFFu;
+    for (uint32_t j = 0; j < n_jobs; j++) {
+        Sim& S = *B.slots[order[j]].sim;
+        CU(cudaMemcpy(&S.D.st->step_budget, &unlimited, 4, cudaMemcpyHostToDevice));
+    }
+    (void)r;
+    return first_err;
 }
 
 }  // namespace ntr

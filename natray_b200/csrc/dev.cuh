@@ -97,6 +97,9 @@ struct DevState {
     // kernel): NTR_WORK_STEPS .. NTR_WORK_SPRAY of include/natray.h.
     uint32_t n_water, n_gas;
     unsigned long long work[6];
+    // Steps this scene may still take in the current batch call (0xFFFFFFFF: no limit); a
+    // batch of scenes stepped together gives each its own count (k_begin_step).
+    uint32_t step_budget;
 };
 
 // Every pointer and size a kernel may need. Passed by value.
@@ -148,6 +151,53 @@ struct Dev {
     uint32_t* coltot;   // radix sort: per digit, the elements with that digit
     uint32_t* wnb;      // solver: per cell, its 6 neighbours that are water (or NONE), 8 words
 };
+
+// Where a CTA is in its scene's grid: x() and nx() as blockIdx.x and gridDim.x of a launch for
+// one scene, y() as blockIdx.y. Every step kernel's body takes its place from one of these, so
+// that the same body runs in a launch for one scene (HwCta: the hardware's indices, read where
+// used) and in one launch for many scenes (Cta: a batch, where each scene owns a contiguous
+// range of the launch's CTAs).
+struct HwCta {
+    __device__ __forceinline__ uint32_t x() const { return blockIdx.x; }
+    __device__ __forceinline__ uint32_t nx() const { return gridDim.x; }
+    __device__ __forceinline__ uint32_t y() const { return blockIdx.y; }
+};
+struct Cta {
+    uint32_t x_, nx_, y_;
+    __device__ __forceinline__ uint32_t x() const { return x_; }
+    __device__ __forceinline__ uint32_t nx() const { return nx_; }
+    __device__ __forceinline__ uint32_t y() const { return y_; }
+};
+
+// A launch over many scenes: scene s owns CTAs first[s] .. first[s + 1] - 1 of the launch (its
+// grid for this kernel, possibly none), with the pointer table jobs[s].
+struct Multi {
+    const Dev* jobs;
+    const uint32_t* first;  // n + 1 entries
+    uint32_t n;
+};
+
+// The CTA's scene in a launch over many scenes: its pointer table and its place in the
+// scene's grid, written to shared memory (`sD`, `sC`) so that they cost no registers. Every
+// thread of the CTA calls it (it has a barrier).
+__device__ __forceinline__ void multi_cta(const Multi& M, Dev& sD, Cta& sC) {
+    const uint32_t b = blockIdx.x;
+    uint32_t lo = 0, hi = M.n;  // the last scene whose first CTA is at or before b
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(M.first + mid) <= b) lo = mid;
+        else hi = mid;
+    }
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(M.jobs + lo);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&sD);
+    static_assert(sizeof(Dev) % 4 == 0, "the pointer table copies in words");
+    for (uint32_t k = threadIdx.x; k < sizeof(Dev) / 4; k += blockDim.x) dst[k] = __ldg(src + k);
+    if (threadIdx.x == 0) {
+        const uint32_t f = __ldg(M.first + lo);
+        sC = Cta{b - f, __ldg(M.first + lo + 1) - f, blockIdx.y};
+    }
+    __syncthreads();
+}
 
 // ---- vectors (association as written in the WGSL) ------------------------------------------
 struct V3 {

@@ -111,7 +111,8 @@ __device__ float gas_pressure_at(const Dev& D, const Grid& g, int buf, V3 x) {
 }
 
 // ---- air_carry, air.wgsl:85-99 --------------------------------------------------------------------
-__global__ void k_air_carry(Dev D) {
+template <class CT>
+__device__ __forceinline__ void air_carry_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const int cur = cur_of(st);
@@ -125,13 +126,21 @@ __global__ void k_air_carry(Dev D) {
         if (li == 0) D.block_active[b] = 0u;
     }
 }
+__global__ void k_air_carry(Dev D) { air_carry_body(D, HwCta{}); }
+__global__ void k_air_carry_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    air_carry_body(sD, c);
+}
 
 // ---- mem_splat, membrane.wgsl:182-217 -------------------------------------------------------------
-__global__ void k_mem_splat(Dev D) {
+template <class CT>
+__device__ __forceinline__ void mem_splat_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = C.x() * blockDim.x + threadIdx.x;
     if (i >= D.Nv || D.mem_mass[i] == 0.0f) return;
     float2 pa = D.mem_push[i];
     if (pa.y <= 0.0f) return;
@@ -165,9 +174,17 @@ __global__ void k_mem_splat(Dev D) {
                 atomicAdd(accp(D, A_MA, cell), to_fp(w * pa.y * 1e6f, FP_A));
             }
 }
+__global__ void k_mem_splat(Dev D) { mem_splat_body(D, HwCta{}); }
+__global__ void k_mem_splat_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    mem_splat_body(sD, c);
+}
 
 // ---- grid_prep, fluid.wgsl:305-356 -----------------------------------------------------------------
-__global__ void k_grid_prep(Dev D) {
+template <class CT>
+__device__ __forceinline__ void grid_prep_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
@@ -208,13 +225,21 @@ __global__ void k_grid_prep(Dev D) {
         *cfp(D, F_P, cell) = pr;
     }
 }
+__global__ void k_grid_prep(Dev D) { grid_prep_body(D, HwCta{}); }
+__global__ void k_grid_prep_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    grid_prep_body(sD, c);
+}
 
 __constant__ int8_t E6[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
 __device__ __forceinline__ I3 e6(int k) { return {E6[k][0], E6[k][1], E6[k][2]}; }
 __device__ __forceinline__ I3 ed(uint32_t d, int s) { return {d == 0 ? s : 0, d == 1 ? s : 0, d == 2 ? s : 0}; }
 
 // ---- air_fill (reads the second air buffer, writes the first), air.wgsl:101-148 ---------------
-__global__ void k_air_fill(Dev D) {
+template <class CT>
+__device__ __forceinline__ void air_fill_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
@@ -256,9 +281,17 @@ __global__ void k_air_fill(Dev D) {
         }
     }
 }
+__global__ void k_air_fill(Dev D) { air_fill_body(D, HwCta{}); }
+__global__ void k_air_fill_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    air_fill_body(sD, c);
+}
 
 // ---- bullet_apply, bullet.wgsl:385-393 ---------------------------------------------------------------
-__global__ void k_bullet_apply(Dev D) {
+template <class CT>
+__device__ __forceinline__ void bullet_apply_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     CELL_LOOP(D, st) {
@@ -268,6 +301,13 @@ __global__ void k_bullet_apply(Dev D) {
             if (du != 0) *cfp(D, F_U + d, cell) = cfv(D, F_U + d, cell) + from_fp(du, FP_M);
         }
     }
+}
+__global__ void k_bullet_apply(Dev D) { bullet_apply_body(D, HwCta{}); }
+__global__ void k_bullet_apply_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    bullet_apply_body(sD, c);
 }
 
 // ---- the pressure solve -----------------------------------------------------------------------------
@@ -288,7 +328,8 @@ __device__ __forceinline__ float pressure_of(const Dev& D, uint32_t cell) {
 }
 
 // ---- project, extend, fluid.wgsl:580-674 -------------------------------------------------------------
-__global__ void k_project(Dev D) {
+template <class CT>
+__device__ __forceinline__ void project_body(const Dev& D, const CT& C) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
@@ -322,12 +363,20 @@ __global__ void k_project(Dev D) {
         atomicAdd(&st->n_gas, s_cnt[1]);
     }
 }
+__global__ void k_project(Dev D) { project_body(D, HwCta{}); }
+__global__ void k_project_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    project_body(sD, c);
+}
 
 // Velocity extension in two passes (fluid.wgsl:604-674). Each cell loads everything its pass
 // reads first, all loads in flight together, then decides in the reference's order.
 __device__ __forceinline__ uint32_t cube_at(int x, int y, int z) { return (uint32_t)((x + 1) * 9 + (y + 1) * 3 + (z + 1)); }
 
-__global__ void k_extend_1(Dev D) {
+template <class CT>
+__device__ __forceinline__ void extend_1_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
@@ -395,8 +444,16 @@ __global__ void k_extend_1(Dev D) {
         *cfp(D, F_EXT_SET, cell) = (float)done;
     }
 }
+__global__ void k_extend_1(Dev D) { extend_1_body(D, HwCta{}); }
+__global__ void k_extend_1_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    extend_1_body(sD, c);
+}
 
-__global__ void k_extend_2(Dev D) {
+template <class CT>
+__device__ __forceinline__ void extend_2_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
@@ -451,6 +508,13 @@ __global__ void k_extend_2(Dev D) {
             *cfp(D, F_U + d, cell) = bounded(u, ty, tlo[d]);
         }
     }
+}
+__global__ void k_extend_2(Dev D) { extend_2_body(D, HwCta{}); }
+__global__ void k_extend_2_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    extend_2_body(sD, c);
 }
 
 // ---- sampling the grid at a point, membrane.wgsl:219-239, bullet.wgsl:113-158 ---------------------------
@@ -519,11 +583,12 @@ __device__ __forceinline__ float2 warp_sample_grid(const Dev& D, const Grid& g, 
 }
 
 // Four lanes per vertex, one per stencil (the three velocity lattices and the cell centres).
-__global__ void k_mem_sample(Dev D) {
+template <class CT>
+__device__ __forceinline__ void mem_sample_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t t = C.x() * blockDim.x + threadIdx.x;
     const uint32_t i = t >> 2, q = t & 3u;
     const bool act = i < D.Nv && D.mem_mass[i] != 0.0f;
     float r = 0.0f;
@@ -540,10 +605,18 @@ __global__ void k_mem_sample(Dev D) {
     const float v2 = __shfl_sync(0xffffffffu, r, l0 + 2), v3 = __shfl_sync(0xffffffffu, r, l0 + 3);
     if (act && q == 0u) D.mem_water[i] = make_float4(v0, v1, v2, v3);
 }
+__global__ void k_mem_sample(Dev D) { mem_sample_body(D, HwCta{}); }
+__global__ void k_mem_sample_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    mem_sample_body(sD, c);
+}
 
 // ---- air_substep, air.wgsl:237-269 --------------------------------------------------------------------
 // Three CTAs an SM (80 registers, from 84 and two CTAs): 38.5 -> 34.8 us a step at 1M particles.
-__global__ void __launch_bounds__(256, 3) k_air_substep(Dev D, int par) {
+template <class CT>
+__device__ __forceinline__ void air_substep_body(const Dev& D, const CT& C, int par) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
@@ -590,6 +663,16 @@ __global__ void __launch_bounds__(256, 3) k_air_substep(Dev D, int par) {
     for (int o = 16; o > 0; o >>= 1) lim = fminf(lim, __shfl_down_sync(0xffffffffu, lim, o));
     // The reference lowers air_dt once per workgroup, so only when there are cells.
     if ((threadIdx.x & 31) == 0 && n_cells_ > 0) atomicMin((unsigned int*)&st->s.air_dt, __float_as_uint(lim));
+}
+__global__ void __launch_bounds__(256, 3) k_air_substep(Dev D, int par) { air_substep_body(D, HwCta{}, par); }
+
+// The air's substep over many scenes: substep i, for the scenes whose step has that many.
+__global__ void __launch_bounds__(256, 3) k_air_substep_m(Multi M, uint32_t i, int par) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    if (i >= sD.U->mem[2]) return;
+    air_substep_body(sD, c, par);
 }
 
 }  // namespace ntr

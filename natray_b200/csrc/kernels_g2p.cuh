@@ -17,7 +17,8 @@ __device__ __forceinline__ float drag_cd(float re) {
     return 24.0f / re * (1.0f + 0.15f * nt_pow(re, 0.687f)) + 0.42f / (1.0f + 42500.0f * nt_pow(re, -1.16f));
 }
 
-__global__ void k_spray_update(Dev D) {
+template <class CT>
+__device__ __forceinline__ void spray_update_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const uint32_t n = min(st->s.spray_count, D.spray_cap);
@@ -25,7 +26,7 @@ __global__ void k_spray_update(Dev D) {
     const ntr_gpu_params* U = D.U;
     const V3 grav = {U->gravity[0], U->gravity[1], U->gravity[2]};
     const float rhow = U->fluid[0];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (uint32_t i = C.x() * blockDim.x + threadIdx.x; i < n; i += C.nx() * blockDim.x) {
         float4 pos = D.spray[3 * (size_t)i], vel = D.spray[3 * (size_t)i + 1];
         float r = pos.w;
         if (r <= 0.0f) continue;
@@ -43,6 +44,13 @@ __global__ void k_spray_update(Dev D) {
         D.spray[3 * (size_t)i] = f4(p, r);
         D.spray[3 * (size_t)i + 1] = f4(v, vel.w);
     }
+}
+__global__ void k_spray_update(Dev D) { spray_update_body(D, HwCta{}); }
+__global__ void k_spray_update_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    spray_update_body(sD, c);
 }
 
 __device__ __forceinline__ void ground_touch(const Dev& D, V3 p, float now) {
@@ -123,8 +131,8 @@ __device__ __forceinline__ Gathered gather(const float* tg, V3 X, V3 o, I3 corne
 // and the SM has more CTAs to switch to while one waits on its loads or barriers. With few
 // blocks (small scenes: 256 threads) every block runs at once and its chain of rounds is the
 // time. The result does not depend on the CTA's size.
-template <int G2P_T>
-__global__ void __launch_bounds__(G2P_T, 768 / G2P_T) k_g2p(Dev D) {
+template <int G2P_T, class CT>
+__device__ __forceinline__ void g2p_body(const Dev& D, const CT& C) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
@@ -145,7 +153,7 @@ __global__ void __launch_bounds__(G2P_T, 768 / G2P_T) k_g2p(Dev D) {
     __shared__ uint32_t s_brk;
     float fastest = 0.0f;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
+    for (uint32_t b = C.x(); b < nb; b += C.nx()) {
         const uint32_t first = D.block_start[b];
         const uint32_t count = D.block_start[b + 1] - first;
         if (count == 0) {
@@ -273,9 +281,19 @@ __global__ void __launch_bounds__(G2P_T, 768 / G2P_T) k_g2p(Dev D) {
     for (int o = 16; o > 0; o >>= 1) fastest = fmaxf(fastest, __shfl_down_sync(0xffffffffu, fastest, o));
     if (lane == 0 && fastest > 0.0f) atomicMax((unsigned int*)&st->s.max_speed, __float_as_uint(fastest));
 }
+template <int G2P_T>
+__global__ void __launch_bounds__(G2P_T, 768 / G2P_T) k_g2p(Dev D) { g2p_body<G2P_T>(D, HwCta{}); }
+template <int G2P_T>
+__global__ void __launch_bounds__(G2P_T, 768 / G2P_T) k_g2p_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    g2p_body<G2P_T>(sD, c);
+}
 
 // Exclusive scan of the blocks' break-up counts (one CTA); advances the spray count.
-__global__ void __launch_bounds__(1024) k_spray_scan(Dev D) {
+template <class CT>
+__device__ __forceinline__ void spray_scan_body(const Dev& D, const CT& C) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const uint32_t n = min(st->s.n_blocks, D.cap_blocks);
@@ -311,9 +329,17 @@ __global__ void __launch_bounds__(1024) k_spray_scan(Dev D) {
         st->nbrk = total;
     }
 }
+__global__ void __launch_bounds__(1024) k_spray_scan(Dev D) { spray_scan_body(D, HwCta{}); }
+__global__ void __launch_bounds__(1024) k_spray_scan_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    spray_scan_body(sD, c);
+}
 
 // Writes the drops of every break-up (fluid.wgsl:718-765): 4 drops and a parcel of finer ones.
-__global__ void k_spray_emit(Dev D) {
+template <class CT>
+__device__ __forceinline__ void spray_emit_body(const Dev& D, const CT& C) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
@@ -325,7 +351,7 @@ __global__ void k_spray_emit(Dev D) {
     const float vol = hs * hs * hs;
     // One warp per block, lanes over its break-ups.
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t gw = (C.x() * blockDim.x + threadIdx.x) >> 5, nw = (C.nx() * blockDim.x) >> 5;
     for (uint32_t b = gw; b < nb; b += nw) {
         const uint32_t cnt = D.brk_count[b];
         if (cnt == 0) continue;
@@ -383,12 +409,20 @@ __global__ void k_spray_emit(Dev D) {
         }
     }
 }
+__global__ void k_spray_emit(Dev D) { spray_emit_body(D, HwCta{}); }
+__global__ void k_spray_emit_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    spray_emit_body(sD, c);
+}
 
 // The spray count moves on by five slots per break-up, capacity or not (fluid.wgsl:726).
-__global__ void k_spray_commit(Dev D) {
+template <class CT>
+__device__ __forceinline__ void spray_commit_body(const Dev& D, const CT& C) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
+    if (threadIdx.x == 0 && C.x() == 0) {
         st->s.spray_count += 5u * st->nbrk;
         // The step's work (its algorithmic bytes are counted from these): blocks, water cells
         // times solver iterations, rubber substeps, free-gas cells times air substeps, spray
@@ -402,6 +436,13 @@ __global__ void k_spray_commit(Dev D) {
         st->work[5] += min(st->s.spray_count, D.spray_cap);
         st->n_water = st->n_gas = 0u;
     }
+}
+__global__ void k_spray_commit(Dev D) { spray_commit_body(D, HwCta{}); }
+__global__ void k_spray_commit_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    spray_commit_body(sD, c);
 }
 
 // ---- the zero-length measuring substep and diagnostics --------------------------------------------

@@ -10,8 +10,9 @@
 namespace ntr {
 
 // ---- begin_step, fluid.wgsl:33-89 ------------------------------------------------------------
-__global__ void k_begin_step(Dev D) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+template <class CT>
+__device__ __forceinline__ void begin_step_body(const Dev& D, const CT& C) {
+    if (threadIdx.x != 0 || C.x() != 0) return;
     const ntr_gpu_params* U = D.U;
     ntr_state& s = D.st->s;
     float vmax = s.max_speed;
@@ -37,9 +38,12 @@ __global__ void k_begin_step(Dev D) {
     if (s.free_dt_ns > 0u) dt_s = mn(dt_s, 1.25f * (float)s.free_dt_ns * 1e-9f);
     uint32_t free_ns = max(f2u(dt_s * 1e9f), 20u);
     uint32_t stop = U->limits[3];
-    bool live = s.t_ns < stop;
+    // A scene of a batch that has taken its steps of the call waits like one past its stop.
+    const uint32_t budget = D.st->step_budget;
+    bool live = s.t_ns < stop && budget != 0u;
     uint32_t dt_ns = 0;
     if (live) {
+        if (budget != 0xFFFFFFFFu) D.st->step_budget = budget - 1u;
         dt_ns = min(free_ns, min(stop, arrive) - s.t_ns);
         s.free_dt_ns = free_ns;
         s.t_ns += dt_ns;
@@ -55,28 +59,51 @@ __global__ void k_begin_step(Dev D) {
     }
     s.dt_ns = dt_ns;
 }
+__global__ void k_begin_step(Dev D) { begin_step_body(D, HwCta{}); }
+__global__ void k_begin_step_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    begin_step_body(sD, c);
+}
 
 // ---- clear: the last step's transfer sums, and this step's bitmask ----------------------------
 // Fields 0..7 of the sums are written whole by k_p2g_gather and A_N by k_p2g; the rest
 // accumulate atomically and start from zero. The two clears run on different streams.
-__global__ void k_clear_acc(Dev D) {
+template <class CT>
+__device__ __forceinline__ void clear_acc_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const uint32_t ncell = st->s.n_blocks_prev * 64u;
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t stride = (size_t)C.nx() * blockDim.x;
+    const size_t tid = (size_t)C.x() * blockDim.x + threadIdx.x;
     constexpr uint32_t F0 = A_MF, NF = NTR_ACC_FIELDS - A_MF;
     for (size_t i = tid; i < (size_t)ncell * NF; i += stride) {
         size_t f = i / ncell, c = i - f * ncell;
         D.acc[(F0 + f) * D.cap_cells + c] = 0;
     }
 }
+__global__ void k_clear_acc(Dev D) { clear_acc_body(D, HwCta{}); }
+__global__ void k_clear_acc_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    clear_acc_body(sD, c);
+}
 
-__global__ void k_clear_mask(Dev D) {
+template <class CT>
+__device__ __forceinline__ void clear_mask_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     uint32_t* m = D.mask[cur_of(st)];
-    for (size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x; w < D.nwords; w += (size_t)gridDim.x * blockDim.x) m[w] = 0u;
+    for (size_t w = (size_t)C.x() * blockDim.x + threadIdx.x; w < D.nwords; w += (size_t)C.nx() * blockDim.x) m[w] = 0u;
+}
+__global__ void k_clear_mask(Dev D) { clear_mask_body(D, HwCta{}); }
+__global__ void k_clear_mask_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    clear_mask_body(sD, c);
 }
 
 // Sets the bits of the blocks `slot` of the lanes where `valid`: one atomicOr per distinct
@@ -94,14 +121,15 @@ __host__ __device__ __forceinline__ uint32_t warp_round(uint32_t n) { return (n 
 // membrane.wgsl:164-180). Three ranges of threads, each a whole number of warps: one thread per
 // particle, per last-step block (up to the block capacity), per vertex. Every lane of a warp
 // runs the same loop, so the bits are merged per warp before they go out.
-__global__ void k_mark(Dev D) {
+template <class CT>
+__device__ __forceinline__ void mark_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const int cur = cur_of(st);
     const Grid g = grid_of(D, cur);
     const uint32_t n_prev = st->s.n_blocks_prev;
     uint32_t* mask = D.mask[cur];
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = C.x() * blockDim.x + threadIdx.x;
     const I3 bmax = {(int32_t)g.bd[0] - 1, (int32_t)g.bd[1] - 1, (int32_t)g.bd[2] - 1};
     auto clampb = [&](I3 b) {
         return I3{min(max(b.x, 0), bmax.x), min(max(b.y, 0), bmax.y), min(max(b.z, 0), bmax.z)};
@@ -156,15 +184,23 @@ __global__ void k_mark(Dev D) {
         set_block_bits(mask, valid ? block_slot(g, b) : 0u, valid);
     }
 }
+__global__ void k_mark(Dev D) { mark_body(D, HwCta{}); }
+__global__ void k_mark_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    mark_body(sD, c);
+}
 
 // ---- compaction of the bitmask: blocks numbered in ascending slot order ----------------------
 constexpr int SCAN_T = 256, SCAN_W = 8;  // 2048 words per CTA
 
-__global__ void __launch_bounds__(SCAN_T) k_scan_words_a(Dev D) {
+template <class CT>
+__device__ __forceinline__ void scan_words_a_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const uint32_t* m = D.mask[cur_of(st)];
-    uint32_t base = blockIdx.x * SCAN_T * SCAN_W;
+    uint32_t base = C.x() * SCAN_T * SCAN_W;
     uint32_t s = 0;
     for (int k = 0; k < SCAN_W; k++) {
         uint32_t w = base + k * SCAN_T + threadIdx.x;
@@ -177,11 +213,19 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_words_a(Dev D) {
     if (threadIdx.x == 0) {
         uint32_t t = 0;
         for (int k = 0; k < SCAN_T / 32; k++) t += ws[k];
-        D.cta_sum[blockIdx.x] = t;
+        D.cta_sum[C.x()] = t;
     }
 }
+__global__ void __launch_bounds__(SCAN_T) k_scan_words_a(Dev D) { scan_words_a_body(D, HwCta{}); }
+__global__ void __launch_bounds__(SCAN_T) k_scan_words_a_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    scan_words_a_body(sD, c);
+}
 
-__global__ void __launch_bounds__(SCAN_T) k_scan_words_b(Dev D) {
+template <class CT>
+__device__ __forceinline__ void scan_words_b_body(const Dev& D, const CT& C) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const int cur = cur_of(st);
@@ -191,12 +235,12 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_words_b(Dev D) {
     __shared__ uint32_t s_base, ws[SCAN_T / 32];
     if (threadIdx.x < 32) {
         uint32_t t = 0;
-        for (uint32_t k = threadIdx.x; k < blockIdx.x; k += 32) t += D.cta_sum[k];
+        for (uint32_t k = threadIdx.x; k < C.x(); k += 32) t += D.cta_sum[k];
         for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
         if (threadIdx.x == 0) s_base = t;
     }
     // Each thread owns SCAN_W consecutive words.
-    uint32_t w0 = blockIdx.x * SCAN_T * SCAN_W + threadIdx.x * SCAN_W;
+    uint32_t w0 = C.x() * SCAN_T * SCAN_W + threadIdx.x * SCAN_W;
     uint32_t words[SCAN_W], cnt = 0;
     for (int k = 0; k < SCAN_W; k++) {
         words[k] = (w0 + k < D.nwords) ? m[w0 + k] : 0u;
@@ -226,10 +270,17 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_words_b(Dev D) {
             run++;
         }
     }
-    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == SCAN_T - 1) {
+    if (C.x() == C.nx() - 1 && threadIdx.x == SCAN_T - 1) {
         st->s.n_blocks = run;
         if (run > cap) st->s.overflow = 1u;
     }
+}
+__global__ void __launch_bounds__(SCAN_T) k_scan_words_b(Dev D) { scan_words_b_body(D, HwCta{}); }
+__global__ void __launch_bounds__(SCAN_T) k_scan_words_b_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    scan_words_b_body(sD, c);
 }
 
 // ---- keys: each live particle's block index ---------------------------------------------------
@@ -278,17 +329,18 @@ __device__ __forceinline__ void tile_hist_add(uint32_t* h, uint32_t d) {
 // particle's block index (fluid.wgsl:109-125's claim, canonical: the slot's rank in the block
 // bitmask) and its tile's count of each low digit. Also zeroes the tile's column of pass 1's
 // histogram, which pass 0's scatter fills.
-__global__ void __launch_bounds__(KEYS_T) k_keys_hist(Dev D) {
+template <class CT>
+__device__ __forceinline__ void keys_hist_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const int cur = cur_of(st);
     __shared__ uint32_t h[256];
     if (threadIdx.x < 256) {
         h[threadIdx.x] = 0;
-        if (D.radix_passes > 1) D.hist2[threadIdx.x * D.n_tiles + blockIdx.x] = 0u;
+        if (D.radix_passes > 1) D.hist2[threadIdx.x * D.n_tiles + C.x()] = 0u;
     }
     __syncthreads();
-    const uint32_t base = blockIdx.x * RADIX_TILE;
+    const uint32_t base = C.x() * RADIX_TILE;
     uint32_t slot[KEYS_ITEMS];
 #pragma unroll
     for (int r = 0; r < KEYS_ITEMS; r++) {  // every load first
@@ -306,23 +358,32 @@ __global__ void __launch_bounds__(KEYS_T) k_keys_hist(Dev D) {
         tile_hist_add(h, i < D.Np ? (key[r] & 255u) : 256u);
     }
     __syncthreads();
-    if (threadIdx.x < 256) D.hist[threadIdx.x * D.n_tiles + blockIdx.x] = h[threadIdx.x];
+    if (threadIdx.x < 256) D.hist[threadIdx.x * D.n_tiles + C.x()] = h[threadIdx.x];
+}
+__global__ void __launch_bounds__(KEYS_T) k_keys_hist(Dev D) { keys_hist_body(D, HwCta{}); }
+__global__ void __launch_bounds__(KEYS_T) k_keys_hist_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    keys_hist_body(sD, c);
 }
 
 // A pass's histogram from its input keys (the passes no earlier kernel counted).
-__global__ void __launch_bounds__(RADIX_T) k_radix_hist(Dev D, uint32_t* hist, const uint32_t* keys, uint32_t shift) {
+template <class CT>
+__device__ __forceinline__ void radix_hist_body(const Dev& D, const CT& C, uint32_t* hist, const uint32_t* keys, uint32_t shift) {
     if (D.st->s.dt_ns == 0) return;
     __shared__ uint32_t h[256];
     h[threadIdx.x] = 0;
     __syncthreads();
-    const uint32_t base = blockIdx.x * RADIX_TILE;
+    const uint32_t base = C.x() * RADIX_TILE;
     for (int r = 0; r < RADIX_ITEMS; r++) {
         const uint32_t i = base + r * RADIX_T + threadIdx.x;
         tile_hist_add(h, i < D.Np ? (keys[i] >> shift) & 255u : 256u);
     }
     __syncthreads();
-    hist[threadIdx.x * D.n_tiles + blockIdx.x] = h[threadIdx.x];
+    hist[threadIdx.x * D.n_tiles + C.x()] = h[threadIdx.x];
 }
+__global__ void __launch_bounds__(RADIX_T) k_radix_hist(Dev D, uint32_t* hist, const uint32_t* keys, uint32_t shift) { radix_hist_body(D, HwCta{}, hist, keys, shift); }
 
 // Exclusive scan of 256 values held one per thread of a 256-thread CTA; returns the thread's
 // exclusive prefix and sets *total.
@@ -348,9 +409,10 @@ __device__ __forceinline__ uint32_t cta_scan256(uint32_t v, uint32_t* total) {
 
 // The digit-major histogram (digit, then tile): CTA d scans its digit's column of tile
 // counts into offsets within the digit, and records the digit's total.
-__global__ void __launch_bounds__(256) k_radix_scan(Dev D, uint32_t* hist) {
+template <class CT>
+__device__ __forceinline__ void radix_scan_body(const Dev& D, const CT& C, uint32_t* hist) {
     if (D.st->s.dt_ns == 0) return;
-    const uint32_t d = blockIdx.x, nt = D.n_tiles;
+    const uint32_t d = C.x(), nt = D.n_tiles;
     uint32_t* col = hist + (size_t)d * nt;
     uint32_t carry = 0;
     for (uint32_t base = 0; base < nt; base += 256) {
@@ -363,6 +425,7 @@ __global__ void __launch_bounds__(256) k_radix_scan(Dev D, uint32_t* hist) {
     }
     if (threadIdx.x == 0) D.coltot[d] = carry;
 }
+__global__ void __launch_bounds__(256) k_radix_scan(Dev D, uint32_t* hist) { radix_scan_body(D, HwCta{}, hist); }
 
 // One tile of a pass. Warp w takes the tile's elements [512 w, 512 w + 512) in 16 rounds of 32
 // and ranks each among the warp's earlier elements of its digit (a match per round and a
@@ -372,16 +435,15 @@ __global__ void __launch_bounds__(256) k_radix_scan(Dev D, uint32_t* hist) {
 // run, consecutive threads to consecutive addresses. With hist_next, the same write-out counts
 // the next pass's digit per destination tile (a match on (tile, digit) and one global atomic
 // per group), which spares that pass its histogram kernel; hist_next must be zero before.
-__global__ void __launch_bounds__(SCAT_T) k_radix_scatter(Dev D, const uint32_t* hist, const uint32_t* keys_in,
-                                                          const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
-                                                          uint32_t shift, uint32_t* hist_next) {
+template <class CT>
+__device__ __forceinline__ void radix_scatter_body(const Dev& D, const CT& C, const uint32_t* hist, const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out, uint32_t shift, uint32_t* hist_next) {
     if (D.st->s.dt_ns == 0) return;
     __shared__ uint16_t s_wc[SCAT_WARPS][256];  // per warp and digit: the running count, then the warp's offset
     __shared__ uint32_t s_dstart[256];          // where each digit's run starts in the tile
     __shared__ uint32_t s_gbase[256];           // where it starts in the output
     __shared__ uint32_t s_k[RADIX_TILE], s_v[RADIX_TILE];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint32_t base = blockIdx.x * RADIX_TILE;
+    const uint32_t base = C.x() * RADIX_TILE;
     const uint32_t n_here = D.Np > base ? min((uint32_t)RADIX_TILE, D.Np - base) : 0u;
     for (uint32_t e = threadIdx.x; e < SCAT_WARPS * 256; e += SCAT_T) (&s_wc[0][0])[e] = 0;
     const uint32_t wbase = base + warp * SCAT_WARP_ITEMS;
@@ -424,7 +486,7 @@ __global__ void __launch_bounds__(SCAT_T) k_radix_scatter(Dev D, const uint32_t*
     const uint32_t digit_base = cta_scan_first256<SCAT_T>(cold, &total);
     if (threadIdx.x < 256) {
         s_dstart[threadIdx.x] = dstart;
-        s_gbase[threadIdx.x] = digit_base + hist[threadIdx.x * D.n_tiles + blockIdx.x];
+        s_gbase[threadIdx.x] = digit_base + hist[threadIdx.x * D.n_tiles + C.x()];
     }
     __syncthreads();
 #pragma unroll
@@ -456,18 +518,72 @@ __global__ void __launch_bounds__(SCAT_T) k_radix_scatter(Dev D, const uint32_t*
         }
     }
 }
+__global__ void __launch_bounds__(SCAT_T) k_radix_scatter(Dev D, const uint32_t* hist, const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out, uint32_t shift, uint32_t* hist_next) { radix_scatter_body(D, HwCta{}, hist, keys_in, vals_in, keys_out, vals_out, shift, hist_next); }
+
+// The buffers of pass p of the step's sort, as the host's loop of a one-scene step passes
+// them: keys and values in (the particle indices on pass 0) and out (the last pass writes the
+// final arrays), the pass's histogram, and the next pass's when this pass's scatter counts it.
+struct RadixPass {
+    const uint32_t *kin, *vin;
+    uint32_t *kout, *vout, *hist, *next;
+    uint32_t shift;
+};
+__device__ __forceinline__ bool radix_to_final(const Dev& D, uint32_t p) { return ((D.radix_passes - 1u - p) % 2u) == 0u; }
+__device__ __forceinline__ RadixPass radix_pass(const Dev& D, uint32_t p) {
+    RadixPass r;
+    r.kin = p == 0 ? D.key : (radix_to_final(D, p - 1) ? D.key_sorted : D.key_alt);
+    r.vin = p == 0 ? nullptr : (radix_to_final(D, p - 1) ? D.sorted : D.val_alt);
+    r.kout = radix_to_final(D, p) ? D.key_sorted : D.key_alt;
+    r.vout = radix_to_final(D, p) ? D.sorted : D.val_alt;
+    r.hist = (p % 2u == 0u) ? D.hist : D.hist2;
+    r.next = (p == 0 && D.radix_passes > 1) ? D.hist2 : nullptr;
+    r.shift = 8u * p;
+    return r;
+}
+// The sort's kernels over many scenes, pass p (a scene with fewer passes skips it).
+__global__ void __launch_bounds__(RADIX_T) k_radix_hist_m(Multi M, uint32_t p) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    if (p >= sD.radix_passes) return;
+    const RadixPass r = radix_pass(sD, p);
+    radix_hist_body(sD, c, r.hist, r.kin, r.shift);
+}
+__global__ void __launch_bounds__(256) k_radix_scan_m(Multi M, uint32_t p) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    if (p >= sD.radix_passes) return;
+    radix_scan_body(sD, c, radix_pass(sD, p).hist);
+}
+__global__ void __launch_bounds__(SCAT_T) k_radix_scatter_m(Multi M, uint32_t p) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    if (p >= sD.radix_passes) return;
+    const RadixPass r = radix_pass(sD, p);
+    radix_scatter_body(sD, c, r.hist, r.kin, r.vin, r.kout, r.vout, r.shift, r.next);
+}
 
 // block_start from the sorted keys: block b starts at the first position whose key is >= b.
-__global__ void k_block_bounds(Dev D) {
+template <class CT>
+__device__ __forceinline__ void block_bounds_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
     const uint32_t* ks = D.key_sorted;
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p <= D.Np; p += gridDim.x * blockDim.x) {
+    for (uint32_t p = C.x() * blockDim.x + threadIdx.x; p <= D.Np; p += C.nx() * blockDim.x) {
         int64_t k = p < D.Np ? (int64_t)min(ks[p], nb) : (int64_t)nb;
         int64_t kp = p > 0 ? (int64_t)min(ks[p - 1], nb) : -1;
         for (int64_t b = kp + 1; b <= k; b++) D.block_start[b] = p;
     }
+}
+__global__ void k_block_bounds(Dev D) { block_bounds_body(D, HwCta{}); }
+__global__ void k_block_bounds_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    block_bounds_body(sD, c);
 }
 
 // ---- P2G, fluid.wgsl:198-303 -----------------------------------------------------------------
@@ -650,7 +766,8 @@ __device__ __forceinline__ void p2g_group(P2GShared& S, uint32_t k0, uint32_t bi
 
 // One block per iteration of a CTA; the tile is stored whole and k_p2g_gather sums the tiles
 // that overlap each cell.
-__global__ void __launch_bounds__(P2G_T, 2) k_p2g(Dev D) {
+template <class CT>
+__device__ __forceinline__ void p2g_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     extern __shared__ __align__(16) unsigned char p2g_smem[];
@@ -659,7 +776,7 @@ __global__ void __launch_bounds__(P2G_T, 2) k_p2g(Dev D) {
     const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const float hh = g.h;
-    for (uint32_t b = blockIdx.x; b < nb; b += gridDim.x) {
+    for (uint32_t b = C.x(); b < nb; b += C.nx()) {
         const I3 bc = slot_coord(g, g.list[b]);
         if (tid < 27) {
             I3 n = bc + I3{(int32_t)(tid / 9u), (int32_t)((tid / 3u) % 3u), (int32_t)(tid % 3u)} - I3{1, 1, 1};
@@ -802,16 +919,24 @@ __global__ void __launch_bounds__(P2G_T, 2) k_p2g(Dev D) {
         __syncthreads();
     }
 }
+__global__ void __launch_bounds__(P2G_T, 2) k_p2g(Dev D) { p2g_body(D, HwCta{}); }
+__global__ void __launch_bounds__(P2G_T, 2) k_p2g_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    p2g_body(sD, c);
+}
 
 // Sums of the P2G tiles at each cell: a cell with local coordinate l along an axis lies in
 // the tile of its own block (at l + 1), in the tile of the block below when l <= 1 (at l + 5)
 // and of the block above when l == 3 (at 0). Integer sums, so the same as adding every tile
 // entry atomically, in any order.
-__global__ void k_p2g_gather(Dev D) {
+template <class CT>
+__device__ __forceinline__ void p2g_gather_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const uint32_t n_cells = min(st->s.n_blocks, D.cap_blocks) * 64u;
-    for (uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x; cell < n_cells; cell += gridDim.x * blockDim.x) {
+    for (uint32_t cell = C.x() * blockDim.x + threadIdx.x; cell < n_cells; cell += C.nx() * blockDim.x) {
         const uint32_t b = cell >> 6;
         const I3 l = local_coord(cell);
         // The up to 2 x 2 x 2 tiles over the cell: per axis its own block (offset 0) and the one
@@ -842,6 +967,13 @@ __global__ void k_p2g_gather(Dev D) {
 #pragma unroll
         for (int f = 0; f < 8; f++) D.acc[(size_t)f * D.cap_cells + cell] = (int32_t)s[f];
     }
+}
+__global__ void k_p2g_gather(Dev D) { p2g_gather_body(D, HwCta{}); }
+__global__ void k_p2g_gather_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    p2g_gather_body(sD, c);
 }
 
 }  // namespace ntr

@@ -67,11 +67,12 @@ struct VertexForce {
 // the vertices read the kind, so every vertex of a triangle sees the same thing. The reference
 // writes a tear into `alive` while the triangle's other vertices may still be reading it, and
 // whether they count it then depends on the threads' timing.
-__global__ void k_mem_tri(Dev D, int par) {
+template <class CT>
+__device__ __forceinline__ void mem_tri_body(const Dev& D, const CT& C, int par) {
     const ntr_gpu_params* U = D.U;
     const float4* X = D.mem_x[par];
     const float thick0 = U->rubber[3];
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < D.Nt; t += gridDim.x * blockDim.x) {
+    for (uint32_t t = C.x() * blockDim.x + threadIdx.x; t < D.Nt; t += C.nx() * blockDim.x) {
         float4* rec = D.tri_rec + 5 * (size_t)t;
         if (D.alive[t] == 0u) {
             rec[4] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(0u));
@@ -125,6 +126,7 @@ __global__ void k_mem_tri(Dev D, int par) {
         rec[4] = make_float4(tri.rest_area / 3.0f, sh.sx * thick0 / (lx * ly), reach, __uint_as_float(2u));
     }
 }
+__global__ void k_mem_tri(Dev D, int par) { mem_tri_body(D, HwCta{}, par); }
 
 // vertex_force (membrane.wgsl:67-149): the vertex's triangles' records, folded in its order.
 // Eight triangles at a time: their indices and corners, then their records, each group of
@@ -478,9 +480,10 @@ __device__ __forceinline__ uint32_t substep_vertex(uint32_t block, uint32_t thre
 
 // One explicit rubber substep (membrane.wgsl:283-400). `k` is which substep of the step this
 // is, `par` which pair of buffers it reads.
-__global__ void __launch_bounds__(256) k_mem_substep(Dev D, uint32_t k, int par) {
+template <class CT>
+__device__ __forceinline__ void mem_substep_body(const Dev& D, const CT& C, uint32_t k, int par) {
     DevState* st = D.st;
-    const uint32_t i = substep_vertex(blockIdx.x, threadIdx.x, gridDim.x);
+    const uint32_t i = substep_vertex(C.x(), threadIdx.x, C.nx());
     float lim_x = BIG_F, lim_y = BIG_F;
     const ntr_gpu_params* U = D.U;
     const float dt = dt_of(st), now = now_of(st);
@@ -596,6 +599,7 @@ __global__ void __launch_bounds__(256) k_mem_substep(Dev D, uint32_t k, int par)
         atomicMin((unsigned int*)&st->s.cap_dt, __float_as_uint(lim_y));
     }
 }
+__global__ void __launch_bounds__(256) k_mem_substep(Dev D, uint32_t k, int par) { mem_substep_body(D, HwCta{}, k, par); }
 
 // ---- the bullets' step, bullet.wgsl:101-383 ---------------------------------------------------
 __device__ __forceinline__ float cp_patch(float s) {
@@ -671,10 +675,11 @@ __device__ __forceinline__ bool warp_in_cavity(const Dev& D, float hh, uint32_t 
 //   k_bullet_finish, a CTA per bullet: the patches summed in the reference's order (lane l of
 //     256 takes patches l, l + 256, l + 512 in turn, then a 256-wide tree), the rigid body, the
 //     cavity sections.
-__global__ void k_bullet_prep(Dev D) {
+template <class CT>
+__device__ __forceinline__ void bullet_prep_body(const Dev& D, const CT& C) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
-    const uint32_t bi = blockIdx.x;
+    const uint32_t bi = C.x();
     // A scene without bullets still launches one CTA; it has nothing to do (and the patch and
     // finish kernels skip a bullet whose prep flag is not set).
     if (bi >= D.U->mem[3]) {
@@ -720,17 +725,25 @@ __global__ void k_bullet_prep(Dev D) {
         D.pose_log[(bi * NTR_LOG_CAP + st->s.step % NTR_LOG_CAP) * 3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
 }
+__global__ void k_bullet_prep(Dev D) { bullet_prep_body(D, HwCta{}); }
+__global__ void k_bullet_prep_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    bullet_prep_body(sD, c);
+}
 
 constexpr int BULLET_PW = 8;  // patch warps per CTA
 
-__global__ void __launch_bounds__(BULLET_PW * 32) k_bullet_patch(Dev D) {
+template <class CT>
+__device__ __forceinline__ void bullet_patch_body(const Dev& D, const CT& C) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
-    const uint32_t bi = blockIdx.y;
+    const uint32_t bi = C.y();
     const float4 pr = D.bullet_prep[bi * 4];
     if (__float_as_uint(pr.x) != 1u) return;
     const DBullet b = D.bullets[bi];
-    const uint32_t k = blockIdx.x * BULLET_PW + (threadIdx.x >> 5);
+    const uint32_t k = C.x() * BULLET_PW + (threadIdx.x >> 5);
     if (k >= b.info.y) return;
     const int lane = (int)(threadIdx.x & 31u);
     const Grid g = grid_of(D, cur_of(st));
@@ -792,11 +805,19 @@ __global__ void __launch_bounds__(BULLET_PW * 32) k_bullet_patch(Dev D) {
         o[3] = make_float4(has_cav ? 1.0f : 0.0f, 0.0f, 0.0f, 0.0f);
     }
 }
+__global__ void __launch_bounds__(BULLET_PW * 32) k_bullet_patch(Dev D) { bullet_patch_body(D, HwCta{}); }
+__global__ void __launch_bounds__(BULLET_PW * 32) k_bullet_patch_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    bullet_patch_body(sD, c);
+}
 
-__global__ void __launch_bounds__(256) k_bullet_finish(Dev D) {
+template <class CT>
+__device__ __forceinline__ void bullet_finish_body(const Dev& D, const CT& C) {
     DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
-    const uint32_t bi = blockIdx.x;
+    const uint32_t bi = C.x();
     if (__float_as_uint(D.bullet_prep[bi * 4].x) != 1u) return;
     const Grid g = grid_of(D, cur_of(st));
     const ntr_gpu_params* U = D.U;
@@ -941,6 +962,30 @@ __global__ void __launch_bounds__(256) k_bullet_finish(Dev D) {
                     }
         }
     }
+}
+__global__ void __launch_bounds__(256) k_bullet_finish(Dev D) { bullet_finish_body(D, HwCta{}); }
+__global__ void __launch_bounds__(256) k_bullet_finish_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    bullet_finish_body(sD, c);
+}
+
+// The rubber's substep kernels over many scenes: substep i of the step, for the scenes whose
+// step has that many rubber substeps (each scene's count is its own).
+__global__ void k_mem_tri_m(Multi M, uint32_t i, int par) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    if (i >= sD.U->mem[1]) return;
+    mem_tri_body(sD, c, par);
+}
+__global__ void __launch_bounds__(256) k_mem_substep_m(Multi M, uint32_t k, int par) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    if (k >= sD.U->mem[1]) return;
+    mem_substep_body(sD, c, k, par);
 }
 
 }  // namespace ntr

@@ -558,4 +558,13 @@ __global__ void __launch_bounds__(SOLVE_T, 2) k_solve_batch(const Dev* __restric
     solve_body<FP64>(s_dev, blockIdx.x - s_c0[job], s_c0[job + 1] - s_c0[job]);
 }
 
+// Every scene's grid barrier counter back to zero before the joint solve (a one-scene step
+// clears its own with a memset).
+__global__ void k_solve_reset_m(Multi M) {
+    __shared__ Dev sD;
+    __shared__ Cta c;
+    multi_cta(M, sD, c);
+    if (threadIdx.x == 0) sD.st->bar_count = 0u;
+}
+
 }  // namespace ntr

@@ -336,6 +336,7 @@ static ntr_status upload_state(Sim& S, const World& w) {
     }
     DevState ds;
     std::memset(&ds, 0, sizeof ds);
+    ds.step_budget = 0xFFFFFFFFu;
     ds.s = h.state;
     ds.s.n_blocks = nbp;
     ds.rz = h.state.rz, ds.alpha = h.state.alpha, ds.beta = h.state.beta, ds.b_norm = h.state.b_norm, ds.r_norm = h.state.r_norm;
