@@ -332,7 +332,6 @@ static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active) {
     std::vector<uint32_t> first((size_t)GK_COUNT * (B.max_scenes + 1), 0u), tot(GK_COUNT, 0u);
     std::vector<uint32_t> key;
     uint32_t fp64 = B.slots[order[0]].sim->fp64, max_shots = 1, n_mem = 0, n_air = 0, steps = 0;
-    ntr_status r;
     for (uint32_t j = 0; j < n_jobs; j++) {
         Sim& S = *B.slots[order[j]].sim;
         if (S.fp64 != fp64) return fail(NTR_E_INVALID, "the scenes of a batch step must use the same solver precision");
@@ -397,6 +396,14 @@ static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active) {
     for (uint32_t j = 0; j < n_jobs; j++) {
         BatchSlot& sl = B.slots[order[j]];
         Sim& S = *sl.sim;
+        // A scene parked for the end of the call gets its last step length back: its state is
+        // what its own last step left, as after ntr_sim_step of its steps.
+        if (S.h_state->parked) {
+            S.h_state->s.dt_ns = S.h_state->parked_dt;
+            S.h_state->parked = 0u;
+            CU(cudaMemcpyAsync(&S.D.st->s.dt_ns, &S.h_state->s.dt_ns, 4, cudaMemcpyHostToDevice, s));
+            CU(cudaMemcpyAsync(&S.D.st->parked, &S.h_state->parked, 4, cudaMemcpyHostToDevice, s));
+        }
         const ntr_state& st = S.h_state->s;
         sl.done += st.step - before[j];
         if (st.overflow && first_err == NTR_OK)
@@ -404,13 +411,13 @@ static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active) {
         if (S.h_state->err && first_err == NTR_OK) first_err = fail(NTR_E_TIMEOUT, "a bounded device-side wait gave up");
         if (!st.overflow && !S.h_state->err) adapt_after_batch(S.host.h, st);
     }
-    // Each scene's budget back to no limit, for its own calls (snapshots keep their own state).
+    // Each scene's budget back to no limit, for its own calls.
     const uint32_t unlimited = 0xFFFFFFFFu;
     for (uint32_t j = 0; j < n_jobs; j++) {
         Sim& S = *B.slots[order[j]].sim;
-        CU(cudaMemcpy(&S.D.st->step_budget, &unlimited, 4, cudaMemcpyHostToDevice));
+        CU(cudaMemcpyAsync(&S.D.st->step_budget, &unlimited, 4, cudaMemcpyHostToDevice, s));
     }
-    (void)r;
+    CU(cudaStreamSynchronize(s));
     return first_err;
 }
 

@@ -98,8 +98,11 @@ struct DevState {
     uint32_t n_water, n_gas;
     unsigned long long work[6];
     // Steps this scene may still take in the current batch call (0xFFFFFFFF: no limit); a
-    // batch of scenes stepped together gives each its own count (k_begin_step).
-    uint32_t step_budget;
+    // batch of scenes stepped together gives each its own count (k_begin_step). A scene whose
+    // budget has run out is parked for the rest of the call: its begin_step keeps the last
+    // step length aside and sets none, and its kernels in the batch's launches skip it, so its
+    // state stays as its last step left it (the host puts the step length back).
+    uint32_t step_budget, parked, parked_dt;
 };
 
 // Every pointer and size a kernel may need. Passed by value.

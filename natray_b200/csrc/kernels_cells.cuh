@@ -15,7 +15,7 @@ namespace ntr {
 
 #define CELL_LOOP(D, st)                                                                  \
     const uint32_t n_cells_ = min((st)->s.n_blocks, (D).cap_blocks) * 64u;                \
-    for (uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x; cell < n_cells_; cell += gridDim.x * blockDim.x)
+    for (uint32_t cell = C.x() * blockDim.x + threadIdx.x; cell < n_cells_; cell += C.nx() * blockDim.x)
 
 __device__ __forceinline__ float* cfp(const Dev& D, uint32_t f, uint32_t cell) { return D.cf + (size_t)f * D.cap_cells + cell; }
 __device__ __forceinline__ float cfv(const Dev& D, uint32_t f, uint32_t cell) { return D.cf[(size_t)f * D.cap_cells + cell]; }
@@ -131,6 +131,7 @@ __global__ void k_air_carry_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     air_carry_body(sD, c);
 }
 
@@ -179,6 +180,7 @@ __global__ void k_mem_splat_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     mem_splat_body(sD, c);
 }
 
@@ -230,6 +232,7 @@ __global__ void k_grid_prep_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     grid_prep_body(sD, c);
 }
 
@@ -286,6 +289,7 @@ __global__ void k_air_fill_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     air_fill_body(sD, c);
 }
 
@@ -307,6 +311,7 @@ __global__ void k_bullet_apply_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     bullet_apply_body(sD, c);
 }
 
@@ -368,6 +373,7 @@ __global__ void k_project_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     project_body(sD, c);
 }
 
@@ -449,6 +455,7 @@ __global__ void k_extend_1_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     extend_1_body(sD, c);
 }
 
@@ -514,6 +521,7 @@ __global__ void k_extend_2_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     extend_2_body(sD, c);
 }
 
@@ -610,6 +618,7 @@ __global__ void k_mem_sample_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     mem_sample_body(sD, c);
 }
 
@@ -671,6 +680,7 @@ __global__ void __launch_bounds__(256, 3) k_air_substep_m(Multi M, uint32_t i, i
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     if (i >= sD.U->mem[2]) return;
     air_substep_body(sD, c, par);
 }

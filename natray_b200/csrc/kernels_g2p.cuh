@@ -50,6 +50,7 @@ __global__ void k_spray_update_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     spray_update_body(sD, c);
 }
 
@@ -288,6 +289,7 @@ __global__ void __launch_bounds__(G2P_T, 768 / G2P_T) k_g2p_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     g2p_body<G2P_T>(sD, c);
 }
 
@@ -334,6 +336,7 @@ __global__ void __launch_bounds__(1024) k_spray_scan_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     spray_scan_body(sD, c);
 }
 
@@ -414,6 +417,7 @@ __global__ void k_spray_emit_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     spray_emit_body(sD, c);
 }
 
@@ -442,6 +446,7 @@ __global__ void k_spray_commit_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     spray_commit_body(sD, c);
 }
 

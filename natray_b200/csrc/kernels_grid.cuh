@@ -15,6 +15,11 @@ __device__ __forceinline__ void begin_step_body(const Dev& D, const CT& C) {
     if (threadIdx.x != 0 || C.x() != 0) return;
     const ntr_gpu_params* U = D.U;
     ntr_state& s = D.st->s;
+    if (D.st->step_budget == 0u) {  // a batch scene that has taken its steps of the call
+        if (!D.st->parked) D.st->parked = 1u, D.st->parked_dt = s.dt_ns;
+        s.dt_ns = 0;
+        return;
+    }
     float vmax = s.max_speed;
     uint32_t arrive = U->limits[3];
     for (uint32_t k = 0; k < U->mem[3]; k++) {
@@ -38,9 +43,8 @@ __device__ __forceinline__ void begin_step_body(const Dev& D, const CT& C) {
     if (s.free_dt_ns > 0u) dt_s = mn(dt_s, 1.25f * (float)s.free_dt_ns * 1e-9f);
     uint32_t free_ns = max(f2u(dt_s * 1e9f), 20u);
     uint32_t stop = U->limits[3];
-    // A scene of a batch that has taken its steps of the call waits like one past its stop.
     const uint32_t budget = D.st->step_budget;
-    bool live = s.t_ns < stop && budget != 0u;
+    bool live = s.t_ns < stop;
     uint32_t dt_ns = 0;
     if (live) {
         if (budget != 0xFFFFFFFFu) D.st->step_budget = budget - 1u;
@@ -88,6 +92,7 @@ __global__ void k_clear_acc_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     clear_acc_body(sD, c);
 }
 
@@ -103,6 +108,7 @@ __global__ void k_clear_mask_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     clear_mask_body(sD, c);
 }
 
@@ -189,6 +195,7 @@ __global__ void k_mark_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     mark_body(sD, c);
 }
 
@@ -221,6 +228,7 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_words_a_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     scan_words_a_body(sD, c);
 }
 
@@ -280,6 +288,7 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_words_b_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     scan_words_b_body(sD, c);
 }
 
@@ -365,6 +374,7 @@ __global__ void __launch_bounds__(KEYS_T) k_keys_hist_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     keys_hist_body(sD, c);
 }
 
@@ -545,6 +555,7 @@ __global__ void __launch_bounds__(RADIX_T) k_radix_hist_m(Multi M, uint32_t p) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     if (p >= sD.radix_passes) return;
     const RadixPass r = radix_pass(sD, p);
     radix_hist_body(sD, c, r.hist, r.kin, r.shift);
@@ -553,6 +564,7 @@ __global__ void __launch_bounds__(256) k_radix_scan_m(Multi M, uint32_t p) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     if (p >= sD.radix_passes) return;
     radix_scan_body(sD, c, radix_pass(sD, p).hist);
 }
@@ -560,6 +572,7 @@ __global__ void __launch_bounds__(SCAT_T) k_radix_scatter_m(Multi M, uint32_t p)
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     if (p >= sD.radix_passes) return;
     const RadixPass r = radix_pass(sD, p);
     radix_scatter_body(sD, c, r.hist, r.kin, r.vin, r.kout, r.vout, r.shift, r.next);
@@ -583,6 +596,7 @@ __global__ void k_block_bounds_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     block_bounds_body(sD, c);
 }
 
@@ -924,6 +938,7 @@ __global__ void __launch_bounds__(P2G_T, 2) k_p2g_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     p2g_body(sD, c);
 }
 
@@ -973,6 +988,7 @@ __global__ void k_p2g_gather_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     p2g_gather_body(sD, c);
 }
 

@@ -730,6 +730,7 @@ __global__ void k_bullet_prep_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     bullet_prep_body(sD, c);
 }
 
@@ -810,6 +811,7 @@ __global__ void __launch_bounds__(BULLET_PW * 32) k_bullet_patch_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     bullet_patch_body(sD, c);
 }
 
@@ -968,6 +970,7 @@ __global__ void __launch_bounds__(256) k_bullet_finish_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     bullet_finish_body(sD, c);
 }
 
@@ -977,6 +980,7 @@ __global__ void k_mem_tri_m(Multi M, uint32_t i, int par) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     if (i >= sD.U->mem[1]) return;
     mem_tri_body(sD, c, par);
 }
@@ -984,6 +988,7 @@ __global__ void __launch_bounds__(256) k_mem_substep_m(Multi M, uint32_t k, int 
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
+    if (sD.st->parked) return;
     if (k >= sD.U->mem[1]) return;
     mem_substep_body(sD, c, k, par);
 }

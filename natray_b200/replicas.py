@@ -3,14 +3,14 @@ with its own batch, and no collective on the data path. A scene is one coupled s
 global reductions per solver iteration; the membrane, air and block set are global every step)
 that fits one B200, so the GPUs share out whole scenes: replicas, not a split scene.
 
-    partition_requests   the request stream shared out across the ranks, least loaded first
-                         (the rank with the most free device memory left takes the next request)
+    serve_replicas       the serving loop on every rank, the requests dispatched as the ranks'
+                         slots free up (each claims the next request in arrival order from a
+                         counter in a shared store when it has room), the results gathered
     merge_results        the ranks' serving results as one (throughput, p50/p99 latency)
-    serve_replicas       the serving loop on every rank over its share, the results gathered
     max_over_ranks       a device time as the maximum over the ranks (the bench's clock)
 
-Only host objects cross between the ranks (free memory, the plan is computed alike on every
-rank, and the results at the end), with gloo or NCCL alike.
+Only host objects cross between the ranks: the claim counter (an atomic add on a TCP store),
+and the results at the end, with gloo or NCCL alike.
 """
 from __future__ import annotations
 
@@ -30,20 +30,6 @@ def device_bytes(world: World | bytes) -> int:
     return n.value
 
 
-def partition_requests(need: list[int], free: list[int]) -> list[list[int]]:
-    """Requests (in arrival order, each needing `need[i]` bytes) to ranks (with `free[r]` bytes
-    free): each goes to the rank with the most free memory left (the lowest rank among equals),
-    which is then charged for it. A request larger than every rank's remainder still goes to the
-    rank with the most left, where it waits for memory in that rank's batch."""
-    left = [int(f) for f in free]
-    plan: list[list[int]] = [[] for _ in free]
-    for i, b in enumerate(need):
-        r = max(range(len(left)), key=lambda k: (left[k], -k))
-        plan[r].append(i)
-        left[r] -= int(b)
-    return plan
-
-
 def merge_results(results: list[dict]) -> dict:
     """One serving result from the ranks': requests summed, the makespan the longest, the
     latency percentiles over every request."""
@@ -57,34 +43,42 @@ def merge_results(results: list[dict]) -> dict:
     return out
 
 
-def serve_replicas(worlds: list[World], arrivals: list[float], steps: int, chunk: int = 4, max_scenes: int = 64,
-                   serve_fn=None, free: int | None = None) -> dict | None:
-    """The serving loop on every rank of the initialised process group, over the rank's share of
-    the requests (partition_requests on every rank's free device memory). Returns the merged
-    result on rank 0, None on the others. `serve_fn(worlds, arrivals, steps, chunk, max_scenes)`
-    defaults to natray_b200.serve.serve; `free` to this rank's free device memory."""
+def request_store(rank: int, world_size: int, port: int | None = None, host: str | None = None):
+    """The store the ranks share the request counter through: a TCP store on MASTER_ADDR, one
+    port above MASTER_PORT (rank 0 hosts it)."""
+    import os
+    from datetime import timedelta
+
     import torch.distributed as dist
 
-    if serve_fn is None:
-        from .serve import serve as serve_fn
-    if free is None:
-        import torch
-        free = int(torch.cuda.mem_get_info()[0])
+    host = host or os.environ.get("MASTER_ADDR", "127.0.0.1")
+    port = port or int(os.environ.get("MASTER_PORT", "29500")) + 1
+    return dist.TCPStore(host, port, world_size, rank == 0, timeout=timedelta(seconds=120))
+
+
+def serve_replicas(worlds, arrivals: list[float], steps: int, chunk: int = 4, max_scenes: int = 64, serve_fn=None,
+                   store=None, build=None, batch_factory=None) -> dict | None:
+    """The serving loop on every rank of the initialised process group, the requests dispatched
+    as slots free up (natray_b200.serve.SharedRequests on `store`, request_store by default).
+    `worlds` are the requests' worlds, or their parameters with `build` (each rank builds what it
+    takes, on its arrival). Returns the merged result on rank 0, None on the others."""
+    import torch.distributed as dist
+
+    from .serve import SharedRequests, serve
+
+    serve_fn = serve_fn or serve
     rank, size = dist.get_rank(), dist.get_world_size()
-    frees: list = [None] * size
-    dist.all_gather_object(frees, int(free))
-    plan = partition_requests([device_bytes(w) for w in worlds], frees)
-    mine = plan[rank]
+    if store is None:
+        store = request_store(rank, size)
     dist.barrier()  # a common start for the arrival clock
-    res = serve_fn([worlds[i] for i in mine], [arrivals[i] for i in mine], steps, chunk, max_scenes) if mine else \
-        {"requests": 0, "seconds": 0.0, "latencies": []}
-    res["requests_served"] = list(mine)
+    res = serve_fn(worlds, arrivals, steps, chunk, max_scenes, requests=SharedRequests(store, arrivals), build=build,
+                   batch_factory=batch_factory)
     gathered: list = [None] * size
     dist.all_gather_object(gathered, res)
     if rank != 0:
         return None
     out = merge_results(gathered)
-    out["plan"] = plan
+    out["served_by_rank"] = [r.get("requests_served", []) for r in gathered]
     return out
 
 

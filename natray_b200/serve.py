@@ -4,8 +4,9 @@
     python -m natray_b200.serve --serve 200 --steps 200 --rate 40 # Poisson arrivals, continuous batching
 
 `mixed_scenes` draws seeded scenes of uneven size: particle counts log-uniform (or log-normal),
-balloon diameter, projectile speed, and a membrane that is finer for bigger balloons. Worlds are
-built on the host before timing; the timed part is the GPU work and the host loop around it.
+balloon diameter, projectile speed, and a membrane that is finer for bigger balloons. The batched
+run builds its worlds before timing; the serving loop builds each request's world on a host
+thread when the request arrives, so that its latency includes the build.
 """
 from __future__ import annotations
 
@@ -68,13 +69,16 @@ def run_batched(worlds: list[World], steps: int, chunk: int = 4, max_scenes: int
     return {"seconds": wall, "scenes_per_s": len(worlds) / wall, "particle_steps_per_s": n_ps / wall}
 
 
-def run_sequential(worlds: list[World], steps: int, chunk: int = 4) -> dict:
-    """The same scenes one after the other, each a Sim of its own."""
+def run_sequential(worlds, steps: int, chunk: int = 4, build=None) -> dict:
+    """The same scenes one after the other, each a Sim of its own. With `build`, `worlds` are the
+    scenes' parameters and each is built just before it runs (its time counts with its setup)."""
     times, with_setup = [], []
     t_all = time.perf_counter()
     n_ps = 0
     for w in worlds:
         t_setup = time.perf_counter()
+        if build:
+            w = build(w)
         s = Sim(world=w)
         t0 = time.perf_counter()
         done = 0
@@ -93,40 +97,121 @@ def run_sequential(worlds: list[World], steps: int, chunk: int = 4) -> dict:
             "per_scene_seconds": times, "per_scene_seconds_with_setup": with_setup}
 
 
-def serve(worlds: list[World], arrivals: list[float], steps: int, chunk: int = 4, max_scenes: int = 64) -> dict:
-    """Continuous batching: a request enters the batch at its arrival time or as soon as a slot
-    and the device memory free up, runs `steps` steps, and leaves. Latency = completion - arrival."""
-    n = len(worlds)
-    finish = [0.0] * n
-    queue: list[int] = []
-    nxt = 0
+class LocalRequests:
+    """The requests of one server: each can be taken once it has arrived, in arrival order."""
+
+    def __init__(self, arrivals: list[float]):
+        self.arrivals = list(arrivals)
+        self.next = 0
+
+    def claim(self, now: float) -> int | None:
+        if self.next < len(self.arrivals) and self.arrivals[self.next] <= now:
+            self.next += 1
+            return self.next - 1
+        return None
+
+    def exhausted(self) -> bool:
+        return self.next >= len(self.arrivals)
+
+    def wait_hint(self, now: float) -> float:
+        """Seconds until the next request arrives (0 if one has, or none is left)."""
+        return max(0.0, self.arrivals[self.next] - now) if self.next < len(self.arrivals) else 0.0
+
+
+class SharedRequests:
+    """The requests of several servers (one per GPU), dispatched as their slots free up: a server
+    with room claims the next request in arrival order from a counter that every server shares
+    (an atomic add on a torch.distributed store), and takes it when it arrives. Each request goes
+    to exactly one server, the first to have room for it."""
+
+    def __init__(self, store, arrivals: list[float], key: str = "ntr/serve/next"):
+        self.store, self.key = store, key
+        self.arrivals = list(arrivals)
+        self.pending: int | None = None
+        self.out = False
+
+    def claim(self, now: float) -> int | None:
+        if self.pending is None and not self.out:
+            i = int(self.store.add(self.key, 1)) - 1
+            if i >= len(self.arrivals):
+                self.out = True
+            else:
+                self.pending = i
+        if self.pending is not None and self.arrivals[self.pending] <= now:
+            i, self.pending = self.pending, None
+            return i
+        return None
+
+    def exhausted(self) -> bool:
+        return self.out and self.pending is None
+
+    def wait_hint(self, now: float) -> float:
+        return max(0.0, self.arrivals[self.pending] - now) if self.pending is not None else 0.0
+
+
+def serve(worlds, arrivals: list[float], steps: int, chunk: int = 4, max_scenes: int = 64, *, requests=None,
+          build=None, build_threads: int = 8, batch_factory=None, clock=None) -> dict:
+    """Continuous batching: a request enters the batch when it has arrived (and, with `build`,
+    its scene has been built on a host thread, which its latency includes) and a slot and the
+    device memory are free, runs `steps` steps among the others, and leaves. Latency = completion
+    - arrival.
+
+    worlds         the requests' worlds, or their parameters when `build` (a function of them
+                   returning a World, natray_b200.build_world) builds each on its arrival
+    requests       where requests come from: LocalRequests(arrivals) by default, SharedRequests
+                   when several servers share one stream
+    batch_factory  makes the batch (natray_b200.batch.Batch); tests pass a stand-in"""
+    from concurrent.futures import ThreadPoolExecutor
+
+    requests = requests or LocalRequests(arrivals)
+    batch_factory = batch_factory or (lambda: Batch(max_scenes=max_scenes))
+    clock = clock or time.perf_counter
+    finish: dict[int, float] = {}
+    queue: list[tuple[int, object]] = []  # (request, its world or the future building it)
     slot_req: dict[int, int] = {}
-    with Batch(max_scenes=max_scenes) as b:
-        t0 = time.perf_counter()
-        while nxt < n or queue or slot_req:
-            now = time.perf_counter() - t0
-            while nxt < n and arrivals[nxt] <= now:
-                queue.append(nxt)
-                nxt += 1
-            while queue:
-                sl = b.admit(worlds[queue[0]], steps)
-                if sl is None:
-                    break
-                slot_req[sl] = queue.pop(0)
-            if not slot_req:
-                if nxt < n:
-                    time.sleep(max(0.0, arrivals[nxt] - (time.perf_counter() - t0)))
-                continue
-            b.step(chunk)
-            now = time.perf_counter() - t0
-            for sl in list(slot_req):
-                if b.poll(sl)["finished"]:
-                    finish[slot_req.pop(sl)] = now
-                    b.retire(sl)
-        makespan = time.perf_counter() - t0
-    lat = np.array([f - a for f, a in zip(finish, arrivals)])
-    return {"requests": n, "seconds": makespan, "scenes_per_s": n / makespan, "p50_s": float(np.percentile(lat, 50)),
-            "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()), "latencies": [float(x) for x in lat]}
+    pool = ThreadPoolExecutor(max_workers=max(1, build_threads)) if build else None
+    try:
+        with batch_factory() as b:
+            t0 = clock()
+            while not requests.exhausted() or queue or slot_req:
+                now = clock() - t0
+                # Take requests while the batch has room for them (queued ones count).
+                while len(slot_req) + len(queue) < max_scenes:
+                    i = requests.claim(now)
+                    if i is None:
+                        break
+                    queue.append((i, pool.submit(build, worlds[i]) if build else worlds[i]))
+                while queue:
+                    i, w = queue[0]
+                    if build:
+                        if not w.done():
+                            break
+                        w = w.result()
+                    sl = b.admit(w, steps)
+                    if sl is None:
+                        break
+                    slot_req[sl] = i
+                    queue.pop(0)
+                if not slot_req:
+                    time.sleep(min(requests.wait_hint(clock() - t0), 0.002) if not queue else 0.0005)
+                    continue
+                b.step(chunk)
+                now = clock() - t0
+                for sl in list(slot_req):
+                    if b.poll(sl)["finished"]:
+                        finish[slot_req.pop(sl)] = now
+                        b.retire(sl)
+            makespan = clock() - t0
+    finally:
+        if pool:
+            pool.shutdown(wait=True)
+    served = sorted(finish)
+    lat = np.array([finish[i] - arrivals[i] for i in served])
+    out = {"requests": len(served), "seconds": makespan, "scenes_per_s": len(served) / makespan if makespan > 0 else 0.0,
+           "latencies": [float(x) for x in lat], "requests_served": served}
+    if lat.size:
+        out.update({"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean())})
+    return out
 
 
 def sequential_timeline(arrivals: list[float], durations: list[float]) -> dict:
@@ -157,8 +242,9 @@ def main():
     args = ap.parse_args()
     import os
     if int(os.environ.get("WORLD_SIZE", "1")) > 1:
-        # Under torchrun: one process per GPU, the request stream shared out by free device
-        # memory (natray_b200.replicas), the results merged on rank 0.
+        # Under torchrun: one process per GPU, each with its own batch; the requests go to the
+        # ranks as their slots free up (natray_b200.replicas), each built by the rank that takes
+        # it when it arrives, and the results are merged on rank 0.
         import torch
         import torch.distributed as dist
         from .replicas import serve_replicas
@@ -166,20 +252,20 @@ def main():
         dist.init_process_group("nccl")
         n = args.serve or args.scenes
         ps = mixed_scenes(n, args.seed, lo=16_000, hi=2_000_000, lognormal_median=128_000)
-        worlds = build_worlds(ps)
-        res = serve_replicas(worlds, poisson_arrivals(n, args.rate, args.seed), args.steps, args.chunk)
+        res = serve_replicas(ps, poisson_arrivals(n, args.rate, args.seed), args.steps, args.chunk, build=build_world)
         if res is not None:
-            res.pop("plan", None)
+            res.pop("latencies", None)
             print(json.dumps({"served": res}))
         dist.destroy_process_group()
         return
     if args.serve:
         ps = mixed_scenes(args.serve, args.seed, lo=16_000, hi=2_000_000, lognormal_median=128_000)
-        worlds = build_worlds(ps)
         arr = poisson_arrivals(args.serve, args.rate, args.seed)
-        out = {"served": serve(worlds, arr, args.steps, args.chunk)}
-        seq = run_sequential(worlds, args.steps, args.chunk)
-        # A request served alone pays for its simulation's creation too, as in the batch.
+        # Each request's scene is built when it arrives: its latency includes the build.
+        out = {"served": serve(ps, arr, args.steps, args.chunk, build=build_world)}
+        out["served"].pop("latencies", None)
+        seq = run_sequential(ps, args.steps, args.chunk, build=build_world)
+        # A request served alone pays for its scene's build and its simulation's creation too.
         out["sequential"] = sequential_timeline(arr, seq["per_scene_seconds_with_setup"])
     else:
         worlds = build_worlds(mixed_scenes(args.scenes, args.seed))

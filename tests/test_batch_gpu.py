@@ -61,6 +61,21 @@ def test_batch_equals_each_scene_alone(worlds):
             assert d is None, f"slot {sl}: {d}"
 
 
+def test_uneven_targets_end_as_alone(worlds):
+    # Targets that are not multiples of the call's steps: in a scene's last call it takes fewer
+    # steps than the others and is parked for the rest of the call; its state is that of the
+    # scene alone after the same chunks.
+    targets = [10, 6, 13]
+    with Batch(max_scenes=4) as b:
+        slots = [b.admit(w, t) for w, t in zip(worlds, targets)]
+        while b.step(4):
+            pass
+        for w, t, sl in zip(worlds, targets, slots):
+            assert b.poll(sl)["steps_done"] == t
+            d = first_difference(solo(w, t, 4), b.snapshot(sl))
+            assert d is None, f"slot {sl}: {d}"
+
+
 def test_scenes_arrive_and_leave(worlds):
     # Two scenes start; a third arrives after two batch steps; the first leaves when done and a
     # fourth takes its slot. Each ends as it would alone.
@@ -101,6 +116,16 @@ def test_serving_loop_finishes_every_request(worlds):
     ws = worlds * 2
     out = serve(ws, poisson_arrivals(len(ws), 200.0, 3), steps=8, chunk=4, max_scenes=3)
     assert out["requests"] == len(ws) and out["p99_s"] >= out["p50_s"] > 0.0
+
+
+def test_serving_builds_each_scene_on_arrival():
+    # The requests are parameters; each scene is built on a host thread when its request
+    # arrives, and its latency includes the build.
+    from natray_b200.serve import poisson_arrivals, serve
+    ps = [Params(resolution=r, mesh_level=3, block_cap=4096, spray_cap=100000) for r in (14, 16, 18, 16)]
+    out = serve(ps, poisson_arrivals(len(ps), 100.0, 5), steps=6, chunk=3, max_scenes=2, build=build_world)
+    assert out["requests"] == len(ps) and sorted(out["requests_served"]) == list(range(len(ps)))
+    assert out["p99_s"] >= out["p50_s"] > 0.0
 
 
 def test_queue_from_other_threads(worlds):

@@ -1,6 +1,6 @@
-"""Scenes across GPUs (natray_b200.replicas), the host side, on the CPU: the request stream
-shared out by free device memory, the ranks' results merged, and the two-rank path through
-torch.distributed with the gloo backend (world size 2, one process per rank)."""
+"""Scenes across GPUs (natray_b200.replicas), the host side, on the CPU: the request dispatch as
+slots free up (a claim counter every server shares), the ranks' results merged, and the two-rank
+path through torch.distributed with the gloo backend (world size 2, one process per rank)."""
 import json
 import socket
 import sys
@@ -8,18 +8,36 @@ from pathlib import Path
 
 import numpy as np
 
-from natray_b200 import Params, build_world
-from natray_b200.replicas import device_bytes, merge_results, partition_requests
+from natray_b200.replicas import merge_results
+from natray_b200.serve import LocalRequests, SharedRequests
 
 
-def test_partition_is_least_loaded_first():
-    # rank 0 has 10 units free, rank 1 has 7: the 4-unit requests alternate as the free memory
-    # left says, ties to the lower rank
-    plan = partition_requests([4, 4, 4, 4, 1], [10, 7])
-    assert plan == [[0, 2, 4], [1, 3]]  # left: 10,7 -> 6,7 -> 6,3 -> 2,3 -> 2,-1 -> 1,-1
-    assert partition_requests([5, 5, 5], [0, 0]) == [[0, 2], [1]]  # nothing fits: still least loaded
-    p = partition_requests([1] * 6, [3, 3, 3])
-    assert sorted(sum(p, [])) == list(range(6)) and [len(x) for x in p] == [2, 2, 2]
+class DictStore:
+    """The add() of a torch.distributed store, in one process."""
+
+    def __init__(self):
+        self.v = {}
+
+    def add(self, key, n):
+        self.v[key] = self.v.get(key, 0) + n
+        return self.v[key]
+
+
+def test_local_requests_come_in_arrival_order():
+    r = LocalRequests([0.0, 0.5, 1.0])
+    assert r.claim(0.1) == 0 and r.claim(0.1) is None and r.wait_hint(0.1) == 0.4
+    assert r.claim(1.0) == 1 and r.claim(1.0) == 2 and r.exhausted()
+
+
+def test_shared_requests_go_to_one_server_each():
+    store = DictStore()
+    arr = [0.0, 0.0, 0.2, 0.3]
+    a, b = SharedRequests(store, arr), SharedRequests(store, arr)
+    got = [a.claim(0.0), b.claim(0.0), a.claim(0.0), b.claim(0.0)]
+    assert got[:2] == [0, 1] and got[2:] == [None, None]  # 2 and 3 are claimed but not arrived
+    assert a.wait_hint(0.0) == 0.2 and b.wait_hint(0.0) == 0.3
+    assert a.claim(0.25) == 2 and b.claim(0.25) is None and b.claim(0.3) == 3
+    assert a.claim(1.0) is None and b.claim(1.0) is None and a.exhausted() and b.exhausted()
 
 
 def test_merge_results():
@@ -37,21 +55,22 @@ def free_port() -> int:
 
 
 def test_two_ranks_over_gloo(tmp_path):
+    # 40 requests arriving over 0.2 s, 2 slots a rank, rank 1's steps four times slower: every
+    # request is served exactly once, by the rank that had room first, so rank 1 serves fewer.
     import torch.multiprocessing as mp
     sys.path.insert(0, str(Path(__file__).parent))
     import replica_worker
 
-    worlds = [build_world(Params(resolution=r, mesh_level=2, block_cap=b)) for r, b in
-              [(12, 512), (12, 2048), (14, 512), (12, 1024), (14, 4096)]]
-    blobs = [bytes(w.blob) for w in worlds]
-    arrivals = [0.0, 0.01, 0.02, 0.03, 0.04]
-    frees = [300_000_000, 200_000_000]  # about three and two of these scenes
-    mp.spawn(replica_worker.run, args=(free_port(), blobs, arrivals, frees, str(tmp_path)), nprocs=2, join=True)
+    n = 40
+    arrivals = [0.005 * i for i in range(n)]
+    port = free_port()
+    mp.spawn(replica_worker.run, args=(port, n, arrivals, [2.0, 8.0], 2, str(tmp_path)), nprocs=2, join=True)
     r0 = json.loads((tmp_path / "rank0.json").read_text())
     r1 = json.loads((tmp_path / "rank1.json").read_text())
     assert r1["merged"] is None and r0["max"] == r1["max"] == 2.5
     m = r0["merged"]
-    want = partition_requests([device_bytes(w) for w in worlds], frees)
-    assert m["plan"] == want and m["requests"] == 5 and m["per_rank"] == [len(x) for x in want]
-    assert m["p50_s"] == 0.01 and m["p99_s"] == 0.01
-    assert len(want[0]) > len(want[1]) > 0  # the rank with more memory takes more
+    a, b = m["served_by_rank"]
+    assert sorted(a + b) == list(range(n)) and not set(a) & set(b)
+    assert m["requests"] == n and m["per_rank"] == [len(a), len(b)]
+    assert len(a) > len(b) > 0
+    assert m["p50_s"] > 0 and m["p99_s"] >= m["p50_s"]
