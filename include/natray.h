@@ -495,6 +495,11 @@ NTR_API ntr_status ntr_batch_create(int device, uint32_t max_scenes, uint64_t hb
 NTR_API ntr_status ntr_batch_destroy(ntr_batch* b);
 NTR_API ntr_status ntr_batch_admit(ntr_batch* b, const void* world_blob, size_t len, uint32_t n_steps, uint32_t* slot);
 NTR_API ntr_status ntr_batch_step(ntr_batch* b, uint32_t n, uint32_t* active);
+/* ntr_batch_step's n steps launched kernel by kernel outside the batch's graph, one stream, an
+ * event after each, and a report of device time per kernel, "name,launches,total_ms" a line (as
+ * ntr_sim_profile; the reference's NATRAY_PROF, src/sim.rs:594-614, for one scene). With
+ * report == NULL only *len is set. The scenes advance as with ntr_batch_step. */
+NTR_API ntr_status ntr_batch_profile(ntr_batch* b, uint32_t n, char* report, size_t cap, size_t* len);
 NTR_API ntr_status ntr_batch_poll(ntr_batch* b, uint32_t slot, ntr_batch_slot* out);
 NTR_API ntr_status ntr_batch_snapshot(ntr_batch* b, uint32_t slot, void* buf, size_t cap, size_t* len);
 NTR_API ntr_status ntr_batch_retire(ntr_batch* b, uint32_t slot);

@@ -211,6 +211,7 @@ _SIGS = {
     "ntr_batch_destroy": (C.c_int, [_P]),
     "ntr_batch_admit": (C.c_int, [_P, _P, C.c_size_t, C.c_uint32, C.POINTER(C.c_uint32)]),
     "ntr_batch_step": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "ntr_batch_profile": (C.c_int, [_P, C.c_uint32, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     "ntr_batch_poll": (C.c_int, [_P, C.c_uint32, C.POINTER(BatchSlot)]),
     "ntr_batch_snapshot": (C.c_int, [_P, C.c_uint32, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
     "ntr_batch_retire": (C.c_int, [_P, C.c_uint32]),

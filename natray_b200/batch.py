@@ -73,6 +73,18 @@ class Batch:
         check(lib().ntr_batch_step(self._h, n, C.byref(active)))
         return active.value
 
+    def profile(self, n: int) -> dict:
+        """n steps of every unfinished scene launched kernel by kernel with events between them:
+        {kernel: (launches, ms)} (ntr_batch_profile)."""
+        buf = C.create_string_buffer(1 << 16)
+        ln = C.c_size_t()
+        check(lib().ntr_batch_profile(self._h, n, buf, len(buf), C.byref(ln)))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, cnt, ms = line.rsplit(",", 2)
+            out[name] = (int(cnt), float(ms))
+        return out
+
     def poll(self, slot: int) -> dict:
         s = _abi.BatchSlot()
         check(lib().ntr_batch_poll(self._h, slot, C.byref(s)))

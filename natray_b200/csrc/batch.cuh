@@ -223,21 +223,27 @@ static void scene_grids(const Sim& S, uint32_t g[GK_COUNT]) {
 // The step of every scene of the batch, one launch per kernel over all of them: the launch
 // sequence of enqueue_step (on the same three streams), with each scene's own grid within each
 // launch. `tot` is each kind's CTAs over all scenes.
+// With `prof`, every launch goes to the main stream in order with an event after it (the batch's
+// kernel-by-kernel profile, ntr_batch_profile).
 static uint64_t enqueue_step_multi(Batch& B, uint32_t n_jobs, const uint32_t* tot, uint32_t max_shots, uint32_t n_mem,
-                                   uint32_t n_air, bool fp64, Sim& S0) {
-    cudaStream_t s = B.solve_stream, a = B.aux, a2 = B.aux2;
+                                   uint32_t n_air, bool fp64, Sim& S0, Prof* prof = nullptr) {
+    cudaStream_t s = B.solve_stream, a = prof ? s : B.aux, a2 = prof ? s : B.aux2;
     uint64_t nl = 0;
     auto M = [&](int kind) { return Multi{B.d_jobs, B.d_first + (size_t)kind * (B.max_scenes + 1), n_jobs}; };
 #define LM(kern, kind, threads, strm, ...)                                              \
     do {                                                                                \
         if (tot[kind]) kern<<<tot[kind], (threads), 0, (strm)>>>(M(kind), ##__VA_ARGS__); \
         nl++;                                                                           \
+        if (prof) prof->mark(#kern, s);                                                 \
     } while (0)
+    if (prof) prof->mark("start", s);
     auto fork = [&](int k, cudaStream_t to) {
+        if (to == s) return;
         cudaEventRecord(B.ev_fork[k], s);
         cudaStreamWaitEvent(to, B.ev_fork[k], 0);
     };
     auto join = [&](int k, cudaStream_t from) {
+        if (from == s) return;
         cudaEventRecord(B.ev_join[k], from);
         cudaStreamWaitEvent(s, B.ev_join[k], 0);
     };
@@ -261,6 +267,7 @@ static uint64_t enqueue_step_multi(Batch& B, uint32_t n_jobs, const uint32_t* to
     LM(k_block_bounds_m, GK_BOUNDS, 256, s);
     if (tot[GK_BLK]) k_p2g_m<<<tot[GK_BLK], P2G_T, P2G_SMEM, s>>>(M(GK_BLK));
     nl++;
+    if (prof) prof->mark("k_p2g_m", s);
     LM(k_p2g_gather_m, GK_CELL, 256, s);
     join(0, a);
     LM(k_grid_prep_m, GK_CELL, 256, s);
@@ -268,11 +275,12 @@ static uint64_t enqueue_step_multi(Batch& B, uint32_t n_jobs, const uint32_t* to
     LM(k_bullet_prep_m, GK_SHOTS, 32, s);
     if (tot[GK_PATCH]) k_bullet_patch_m<<<dim3(tot[GK_PATCH], max_shots), BULLET_PW * 32, 0, s>>>(M(GK_PATCH));
     nl++;
+    if (prof) prof->mark("k_bullet_patch_m", s);
     LM(k_bullet_finish_m, GK_SHOTS, 256, s);
     LM(k_bullet_apply_m, GK_CELL, 256, s);
     // Every scene's grid barrier counter starts from zero (k_solve_batch keeps one per scene).
     LM(k_solve_reset_m, GK_ONE, 32, s);
-    nl += enqueue_solve(S0, s, B.d_jobs, n_jobs, fp64, nullptr, B.ctas);
+    nl += enqueue_solve(S0, s, B.d_jobs, n_jobs, fp64, prof, B.ctas);
     LM(k_project_m, GK_CELL, 256, s);
     LM(k_extend_1_m, GK_CELL, 256, s);
     LM(k_extend_2_m, GK_CELL, 256, s);
@@ -283,27 +291,25 @@ static uint64_t enqueue_step_multi(Batch& B, uint32_t n_jobs, const uint32_t* to
         B.ev_sub.push_back(e);
     }
     fork(1, a);
-    cudaEventRecord(B.ev_fork[2], s);
-    cudaStreamWaitEvent(a2, B.ev_fork[2], 0);
+    fork(2, a2);
     LM(k_mem_sample_m, GK_VERT4, 256, a);
     for (uint32_t i = 0; i < n_sub; i++) {
         if (i < n_mem) {
-            if (i >= 1 && i - 1 < n_air) cudaStreamWaitEvent(a, B.ev_sub[2 * (i - 1) + 1], 0);
+            if (a != s && i >= 1 && i - 1 < n_air) cudaStreamWaitEvent(a, B.ev_sub[2 * (i - 1) + 1], 0);
             LM(k_mem_tri_m, GK_TRI, 256, a, i, (int)(i % 2));
             LM(k_mem_substep_m, GK_VERT, 256, a, i, (int)(i % 2));
-            cudaEventRecord(B.ev_sub[2 * i], a);
+            if (a != s) cudaEventRecord(B.ev_sub[2 * i], a);
         }
         if (i < n_air) {
-            if (i >= 1 && i - 1 < n_mem) cudaStreamWaitEvent(a2, B.ev_sub[2 * (i - 1)], 0);
+            if (a2 != s && i >= 1 && i - 1 < n_mem) cudaStreamWaitEvent(a2, B.ev_sub[2 * (i - 1)], 0);
             LM(k_air_substep_m, GK_CELL, 256, a2, i, (int)(i % 2));
-            cudaEventRecord(B.ev_sub[2 * i + 1], a2);
+            if (a2 != s) cudaEventRecord(B.ev_sub[2 * i + 1], a2);
         }
     }
     LM(k_spray_update_m, GK_CELL, 256, a);
     LM(k_g2p_m<128>, GK_BLK, 128, s);
     join(1, a);
-    cudaEventRecord(B.ev_join[2], a2);
-    cudaStreamWaitEvent(s, B.ev_join[2], 0);
+    join(2, a2);
     LM(k_spray_scan_m, GK_ONE, 1024, s);
     LM(k_spray_emit_m, GK_CELL, 256, s);
     LM(k_spray_commit_m, GK_ONE, 32, s);
@@ -313,7 +319,7 @@ static uint64_t enqueue_step_multi(Batch& B, uint32_t n_jobs, const uint32_t* to
 
 // n steps of every unfinished scene: each scene takes min(n, its steps left) (its step budget
 // stops it after those), all of them in the same replays of the batch's step graph.
-static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active) {
+static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active, Prof* prof = nullptr) {
     std::vector<uint32_t> order;
     std::vector<uint32_t> todo(B.max_scenes, 0u);
     for (uint32_t i = 0; i < B.max_scenes; i++) {
@@ -364,7 +370,7 @@ static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active) {
     CU(cudaMemcpyAsync(B.d_first, first.data(), sizeof(uint32_t) * first.size(), cudaMemcpyHostToDevice, s));
     // The step graph of these scenes and shapes (captured again when they change).
     Sim& S0 = *B.slots[order[0]].sim;
-    if (!B.exec || key != B.graph_key) {
+    if (!prof && (!B.exec || key != B.graph_key)) {
         if (B.exec) cudaGraphExecDestroy(B.exec), B.exec = nullptr;
         if (B.graph) cudaGraphDestroy(B.graph), B.graph = nullptr;
         CU(cudaStreamSynchronize(s));
@@ -384,7 +390,15 @@ static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active) {
     }
     std::vector<uint32_t> before(n_jobs);
     for (uint32_t j = 0; j < n_jobs; j++) before[j] = B.slots[order[j]].sim->h_state->s.step;
-    for (uint32_t k = 0; k < steps; k++) CU(cudaGraphLaunch(B.exec, s));
+    if (prof) {
+        S0.launch_err = cudaSuccess;
+        for (uint32_t k = 0; k < steps; k++) enqueue_step_multi(B, n_jobs, tot.data(), max_shots, n_mem, n_air, fp64 != 0, S0, prof);
+        CU(cudaGetLastError());
+        CU(S0.launch_err);
+        CU(prof->err);
+    } else {
+        for (uint32_t k = 0; k < steps; k++) CU(cudaGraphLaunch(B.exec, s));
+    }
     B.steps += steps;
     // States back, then the host control of each scene (Sim::run).
     for (uint32_t j = 0; j < n_jobs; j++) {

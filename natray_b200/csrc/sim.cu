@@ -424,6 +424,7 @@ struct Prof {
         for (auto e : ev) cudaEventDestroy(e);
     }
 };
+static ntr_status prof_report(Prof& prof, char* report, size_t cap, size_t* len);
 
 // The pressure solve as one cooperative launch of `ctas` CTAs on `s`: of S alone (jobs == NULL),
 // or of the `n_jobs` simulations whose pointer tables are at `jobs` on the device. Each job's
@@ -1029,6 +1030,14 @@ NTR_API ntr_status ntr_sim_profile(ntr_sim* sim, uint32_t n, uint32_t stop_ns, c
     uint32_t taken = 0;
     ntr_status r = run_batch(S, n, stop_ns, &taken, &prof);
     if (r != NTR_OK) return r;
+    return prof_report(prof, report, cap, len);
+}
+
+}  // extern "C"
+
+namespace ntr {
+// The profile's events as a report: per kernel name, its launches and device time.
+static ntr_status prof_report(Prof& prof, char* report, size_t cap, size_t* len) {
     std::vector<std::string> order;
     std::map<std::string, std::pair<uint64_t, double>> acc;
     for (size_t i = 1; i < prof.next; i++) {
@@ -1053,6 +1062,9 @@ NTR_API ntr_status ntr_sim_profile(ntr_sim* sim, uint32_t n, uint32_t stop_ns, c
     }
     return NTR_OK;
 }
+}  // namespace ntr
+
+extern "C" {
 
 NTR_API ntr_status ntr_sim_set_batch_steps(ntr_sim* sim, uint32_t n) {
     GUARD(sim);
@@ -1388,6 +1400,15 @@ NTR_API ntr_status ntr_batch_ticket(ntr_batch* batch, uint64_t ticket, uint32_t*
             return NTR_OK;
         }
     return fail(NTR_E_INVALID, "unknown ticket");
+}
+
+NTR_API ntr_status ntr_batch_profile(ntr_batch* batch, uint32_t n, char* report, size_t cap, size_t* len) {
+    BGUARD(batch);
+    Prof prof;
+    uint32_t active = 0;
+    ntr_status r = batch_step(B, n, active, &prof);
+    if (r != NTR_OK) return r;
+    return prof_report(prof, report, cap, len);
 }
 
 NTR_API ntr_status ntr_batch_step(ntr_batch* batch, uint32_t n, uint32_t* active) {

@@ -2,6 +2,7 @@
 (src/sim.rs:594-614, 670-689) as a command:
 
     python -m natray_b200.prof [--resolution 124] [--warmup 3] [--steps 5] [--graph-steps 10] [--keyframes 0]
+    python -m natray_b200.prof --batch 64 [--warmup 8] [--graph-steps 16] [--steps 4]
 
 Builds the 1M-particle scene of the benchmark (or another resolution), runs warm-up batches,
 times `--graph-steps` steps through the step's CUDA graph, then runs `--steps` steps kernel by
@@ -26,7 +27,10 @@ def main():
     ap.add_argument("--graph-steps", type=int, default=10)
     ap.add_argument("--speed", type=float, default=350.0)
     ap.add_argument("--keyframes", type=int, default=0)
+    ap.add_argument("--batch", type=int, default=0, help="profile a batch of this many mixed scenes instead")
     args = ap.parse_args()
+    if args.batch:
+        return batch_profile(args)
     w = build_world(Params(resolution=args.resolution, mesh_level=args.mesh_level, dt_max=2e-6, bullet=6, caliber=8,
                            bullet_speed=args.speed))
     s = Sim(world=w)
@@ -57,6 +61,32 @@ def main():
             c.show(0.5 * (a["t"] + b["t"]))
             print(f"show at {0.5 * (a['t'] + b['t']) * 1e3:.4f} ms: {c.last_times()[2] * 1e3:.1f} us")
         c.close()
+
+
+def batch_profile(args):
+    """The batch engine on the bench's mixed scenes: graph-timed batch steps, then one call of
+    `--steps` steps kernel by kernel (ntr_batch_profile)."""
+    import time
+
+    from .batch import Batch
+    from .serve import build_worlds, mixed_scenes
+    worlds = build_worlds(mixed_scenes(args.batch, 7))
+    n_p = sum(w.h.n_particles for w in worlds)
+    with Batch(max_scenes=max(64, args.batch)) as b:
+        for w in worlds:
+            assert b.admit(w, 100000) is not None
+        b.step(args.warmup)
+        t0 = time.perf_counter()
+        b.step(args.graph_steps)
+        dt = time.perf_counter() - t0
+        print(f"{len(worlds)} scenes, {n_p} particles: {dt / max(args.graph_steps, 1) * 1e3:.3f} ms per batch step (graph, "
+              f"host-timed, states read back once)")
+        if args.steps:
+            p = b.profile(args.steps)
+            tot = sum(v[1] for v in p.values())
+            print(f"kernel by kernel: {tot / args.steps:.3f} ms per batch step")
+            for k, (c, t) in sorted(p.items(), key=lambda kv: -kv[1][1]):
+                print(f"  {k:24s} {c:5d} launches {t / args.steps * 1e3:9.1f} us/step {100 * t / tot:5.1f}%")
 
 
 if __name__ == "__main__":
