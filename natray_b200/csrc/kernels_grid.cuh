@@ -663,30 +663,39 @@ __device__ __forceinline__ uint32_t tile_cell(const uint32_t* links, uint32_t t)
 // P2G by stencil groups. Particles of one cell whose stencils on a lattice start at the same
 // node add to the same 27 nodes of the tile: for a face lattice these are the particles of the
 // cell on one side of its middle along that lattice's axis (the half decides whether the
-// stencil starts at the cell below or at the cell itself), for the cell-centred lattice every
-// particle of the cell. A thread owns one such group (a lattice, a cell, a half) and sums its
-// particles' rounded i32 contributions to the 27 nodes in registers, then adds each node's sum
-// to the tile with one shared atomic, instead of one atomic per particle and node. Integer sums
-// do not depend on the order of the adds, so the tile is the same as the particle-by-particle
-// splat's, bit for bit.
+// stencil starts at the cell below or at the cell itself); the cell-centred lattice's stencil is
+// the same for the whole cell, which is split in two by its x half. A thread owns one such group
+// (a lattice, a cell, a half) and sums its particles' rounded i32 contributions to the 27 nodes
+// in registers, then adds each node's sum to the tile with one shared atomic, instead of one
+// atomic per particle and node. Integer sums do not depend on the order of the adds, so the tile
+// is the same as the particle-by-particle splat's, bit for bit.
 //
 // A block's particles are taken in chunks of P2G_CHUNK. Each chunk's particles are counted by
 // (cell, octant) (octant = the particle's half of its cell along each axis, from the same float
-// expressions as the stencils' first nodes), their cells' counts scanned, and their values
-// staged in shared memory in that order: position in cells and the cell-centred value, and per
-// face lattice the velocity component and h times the affine row. The group of (cell, lattice,
-// half) is then a run of octants: 4 consecutive ones for x, two pairs for y, four singles for z.
-// A particle whose values would leave the range in which the rounding by addition is exact on
-// any lattice (or that are not finite) takes the particle-by-particle splat instead.
+// expressions as the stencils' first nodes), the counts scanned, and the particles' values
+// staged in shared memory in (cell, x half, y half, z half) order: position in cells and the
+// cell-centred value, and per face lattice the velocity component and h times the affine row.
+// Two lists of staged indices put the same particles in (cell, y half, x half, z half) and
+// (cell, z half, x half, y half) order, so that every group is one contiguous run: in the staged
+// order for the x faces and the cell centres, in those lists for the y and z faces. Each
+// lattice's non-empty groups are listed most particles first, and its threads take them in that
+// order: the lanes of a warp, all on one lattice, loop over similar counts. A particle whose
+// values would leave the range in which the rounding by addition is exact on any lattice (or that
+// are not finite) takes the particle-by-particle splat instead.
 constexpr uint32_t P2G_CHUNK = 2 * P2G_T;
 constexpr uint32_t P2G_KEYS = 64 * 8;  // (cell, octant)
-constexpr uint32_t P2G_ODD = 0xffffffffu;
+constexpr uint16_t P2G_ODD = 0xffffu;
+constexpr uint32_t P2G_BUCKETS = 16;   // groups sorted by min(particles, 15), most first
 
 struct P2GShared {
     float4 x[P2G_CHUNK];      // position in cells, w = the cell-centred value (pressure / 1e6)
     float4 g[3][P2G_CHUNK];   // per face lattice: h * affine row, w = velocity component
     int32_t tile[8 * TPF];
-    uint32_t start[P2G_KEYS + 1];
+    uint32_t start[P2G_KEYS + 1];         // key counts, then where each key's run starts
+    uint16_t lst[2][P2G_CHUNK];           // staged indices in y-half and in z-half order
+    uint8_t pre[2][64][8];                // per cell and octant: where its run starts in those orders, in the cell
+    uint16_t items[4][128];               // per lattice: its groups (cell * 2 + half), most particles first
+    uint32_t bucket[4][P2G_BUCKETS + 1];  // per lattice: groups per count, then where they start
     uint32_t odd[P2G_CHUNK];
     uint32_t own[64];
     uint32_t warp_sum[P2G_T / 32];
@@ -701,66 +710,65 @@ __device__ __forceinline__ bool p2g_fast(float val, V3 hg, V3 fx, float scale) {
     return bound * scale < 4.0e6f && fabsf(fx.x) + fabsf(fx.y) + fabsf(fx.z) < 8.0f;
 }
 
+// Octant o = (x half, y half, z half) as bits 2, 1, 0; its place in the y-half and z-half orders.
+__device__ __forceinline__ uint32_t oct_y_first(uint32_t o) { return ((o >> 1) & 1u) << 2 | (o >> 2) << 1 | (o & 1u); }
+__device__ __forceinline__ uint32_t oct_z_first(uint32_t o) { return (o & 1u) << 2 | (o >> 2) << 1 | ((o >> 1) & 1u); }
+
 // One group's sums. Lattice L: 0, 1, 2 the faces along x, y, z (offset 0 along that axis, 0.5
-// along the others), 3 the cell centres. The group is the staged particles of the cell's
-// octants (keys k0 .. k0 + 7) whose bit `bit` is h; `b` is the stencil's first node (domain
-// cells, as floats), `t0` its tile index.
+// along the others), 3 the cell centres. The group is the run [lo, hi) of the staged order (x
+// faces, cell centres) or of the y-half or z-half list; `b` is the stencil's first node
+// (domain cells, as floats), `t0` its tile index.
 template <int L>
-__device__ __forceinline__ void p2g_group(P2GShared& S, uint32_t k0, uint32_t bit, uint32_t h, V3 b, uint32_t t0) {
+__device__ __forceinline__ void p2g_group(P2GShared& S, uint32_t lo, uint32_t hi, V3 b, uint32_t t0) {
     int32_t sv[27], sw[27];
 #pragma unroll
     for (int k = 0; k < 27; k++) sv[k] = 0, sw[k] = 0;
-    uint32_t n = 0;
 #pragma unroll 1
-    for (uint32_t oc = 0; oc < 8; oc++) {
-        if (((oc >> bit) & 1u) != h) continue;
-        const uint32_t hi = S.start[k0 + oc + 1];
-#pragma unroll 1
-        for (uint32_t j = S.start[k0 + oc]; j < hi; j++) {
-            const float4 X = S.x[j];
-            // x - o per axis (x - 0 is x), then the offset from the stencil's first node.
-            const V3 xo = {L == 0 ? X.x : X.x - 0.5f, L == 1 ? X.y : X.y - 0.5f, L == 2 ? X.z : X.z - 0.5f};
-            const V3 fx = xo - b;
-            const V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
-            if (L < 3) {
-                const float4 G = S.g[L][j];
-                // hg . ((a, b, c) - fx) as the splat sums it: (x term + y term) + z term.
-                const float px[3] = {G.x * (0.0f - fx.x), G.x * (1.0f - fx.x), G.x * (2.0f - fx.x)};
-                const float py[3] = {G.y * (0.0f - fx.y), G.y * (1.0f - fx.y), G.y * (2.0f - fx.y)};
-                const float pz[3] = {G.z * (0.0f - fx.z), G.z * (1.0f - fx.z), G.z * (2.0f - fx.z)};
+    for (uint32_t q = lo; q < hi; q++) {
+        const uint32_t j = (L == 1 || L == 2) ? (uint32_t)S.lst[L - 1][q] : q;
+        const float4 X = S.x[j];
+        // x - o per axis (x - 0 is x), then the offset from the stencil's first node.
+        const V3 xo = {L == 0 ? X.x : X.x - 0.5f, L == 1 ? X.y : X.y - 0.5f, L == 2 ? X.z : X.z - 0.5f};
+        const V3 fx = xo - b;
+        const V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
+        if (L < 3) {
+            const float4 G = S.g[L][j];
+            // hg . ((a, b, c) - fx) as the splat sums it: (x term + y term) + z term.
+            const float px[3] = {G.x * (0.0f - fx.x), G.x * (1.0f - fx.x), G.x * (2.0f - fx.x)};
+            const float py[3] = {G.y * (0.0f - fx.y), G.y * (1.0f - fx.y), G.y * (2.0f - fx.y)};
+            const float pz[3] = {G.z * (0.0f - fx.z), G.z * (1.0f - fx.z), G.z * (2.0f - fx.z)};
 #pragma unroll
-                for (int a = 0; a < 3; a++)
+            for (int a = 0; a < 3; a++)
 #pragma unroll
-                    for (int bb = 0; bb < 3; bb++) {
-                        const float wab = wx[a] * wy[bb];
-                        const float sab = px[a] + py[bb];
+                for (int bb = 0; bb < 3; bb++) {
+                    const float wab = wx[a] * wy[bb];
+                    const float sab = px[a] + py[bb];
 #pragma unroll
-                        for (int c = 0; c < 3; c++) {
-                            const float weight = wab * wz[c];
-                            const float node = G.w + (sab + pz[c]);
-                            sv[a * 9 + bb * 3 + c] += __float_as_int(__fadd_rn(__fmul_rn(weight * node, FP_M), 12582912.0f));
-                            sw[a * 9 + bb * 3 + c] += __float_as_int(__fadd_rn(__fmul_rn(weight, FP_W), 8388608.0f));
-                        }
+                    for (int c = 0; c < 3; c++) {
+                        const float weight = wab * wz[c];
+                        const float node = G.w + (sab + pz[c]);
+                        sv[a * 9 + bb * 3 + c] += __float_as_int(__fadd_rn(__fmul_rn(weight * node, FP_M), 12582912.0f));
+                        sw[a * 9 + bb * 3 + c] += __float_as_int(__fadd_rn(__fmul_rn(weight, FP_W), 8388608.0f));
                     }
-            } else {
-                // No affine term: the node value is the particle's (adding the dot product of a
-                // zero gradient changes at most the sign of a zero, which rounds to 0 either way).
+                }
+        } else {
+            // No affine term: the node value is the particle's (adding the dot product of a
+            // zero gradient changes at most the sign of a zero, which rounds to 0 either way).
 #pragma unroll
-                for (int a = 0; a < 3; a++)
+            for (int a = 0; a < 3; a++)
 #pragma unroll
-                    for (int bb = 0; bb < 3; bb++) {
-                        const float wab = wx[a] * wy[bb];
+                for (int bb = 0; bb < 3; bb++) {
+                    const float wab = wx[a] * wy[bb];
 #pragma unroll
-                        for (int c = 0; c < 3; c++) {
-                            const float weight = wab * wz[c];
-                            sv[a * 9 + bb * 3 + c] += __float_as_int(__fadd_rn(__fmul_rn(weight * X.w, FP_P), 12582912.0f));
-                            sw[a * 9 + bb * 3 + c] += __float_as_int(__fadd_rn(__fmul_rn(weight, FP_W), 8388608.0f));
-                        }
+                    for (int c = 0; c < 3; c++) {
+                        const float weight = wab * wz[c];
+                        sv[a * 9 + bb * 3 + c] += __float_as_int(__fadd_rn(__fmul_rn(weight * X.w, FP_P), 12582912.0f));
+                        sw[a * 9 + bb * 3 + c] += __float_as_int(__fadd_rn(__fmul_rn(weight, FP_W), 8388608.0f));
                     }
-            }
-            n++;
+                }
         }
     }
+    const uint32_t n = hi - lo;
     if (n == 0) return;
     // Each sum carries n times the rounding constant's bits; take them off (mod 2^32).
     const int32_t ov = (int32_t)(n * 0x4B400000u), ow = (int32_t)(n * 0x4B000000u);
@@ -776,6 +784,19 @@ __device__ __forceinline__ void p2g_group(P2GShared& S, uint32_t k0, uint32_t bi
                 atomicAdd(&S.tile[fa * TPF + t], sv[k] - ov);
                 atomicAdd(&S.tile[fw * TPF + t], sw[k] - ow);
             }
+}
+
+// Particles of group (lattice L, cell, half h) in its run: the particle count and the run's start.
+__device__ __forceinline__ void p2g_run(const P2GShared& S, uint32_t L, uint32_t cell, uint32_t h, uint32_t& lo, uint32_t& hi) {
+    const uint32_t k0 = cell * 8u, base = S.start[k0];
+    if (L == 0 || L == 3) {  // x half: octants 4h .. 4h + 3 of the staged order
+        lo = S.start[k0 + 4u * h], hi = S.start[k0 + 4u * h + 4u];
+    } else {  // y or z half: the first four places of the cell's run in that order, or the rest
+        const uint32_t n = S.start[k0 + 8u] - base;
+        const uint32_t first_half = h ? n : (uint32_t)S.pre[L - 1][cell][4];
+        lo = base + (h ? (uint32_t)S.pre[L - 1][cell][4] : 0u);
+        hi = base + first_half;
+    }
 }
 
 // One block per iteration of a CTA; the tile is stored whole and k_p2g_gather sums the tiles
@@ -810,6 +831,7 @@ __device__ __forceinline__ void p2g_body(const Dev& D, const CT& C) {
         for (uint32_t chunk = 0; chunk < count; chunk += P2G_CHUNK) {
             const uint32_t n = min(P2G_CHUNK, count - chunk);
             for (uint32_t k = tid; k < P2G_KEYS; k += P2G_T) S.start[k] = 0;
+            if (tid < 4 * (P2G_BUCKETS + 1)) (&S.bucket[0][0])[tid] = 0;
             if (tid == 0) S.n_odd = 0;
             __syncthreads();
             // Each thread's two particles: key, rank in its key, and the staged values, kept in
@@ -853,6 +875,21 @@ __device__ __forceinline__ void p2g_body(const Dev& D, const CT& C) {
                 vg[q][2] = make_float4(hw.x, hw.y, hw.z, vel.z);
             }
             __syncthreads();
+            // Each cell's octant counts in the y-half and z-half orders (threads 0-63), before
+            // the counts become starts.
+            uint32_t cnt8[8];
+            if (tid < 64) {
+#pragma unroll
+                for (int o = 0; o < 8; o++) cnt8[o] = S.start[tid * 8 + o];
+                uint32_t py = 0, pz = 0;
+#pragma unroll
+                for (int r = 0; r < 8; r++)
+#pragma unroll
+                    for (int o = 0; o < 8; o++) {
+                        if (oct_y_first(o) == (uint32_t)r) S.pre[0][tid][o] = (uint8_t)py, py += cnt8[o];
+                        if (oct_z_first(o) == (uint32_t)r) S.pre[1][tid][o] = (uint8_t)pz, pz += cnt8[o];
+                    }
+            }
             // Exclusive scan of the 512 key counts: two a thread, warp scans, then the warps'.
             {
                 const uint32_t c0n = S.start[2 * tid], c1n = S.start[2 * tid + 1];
@@ -872,6 +909,7 @@ __device__ __forceinline__ void p2g_body(const Dev& D, const CT& C) {
                 if (tid == P2G_T - 1) S.start[P2G_KEYS] = ex + c0n + c1n;
             }
             __syncthreads();
+            // Stage the values; the two lists; count each lattice's groups by size.
 #pragma unroll
             for (int q = 0; q < 2; q++) {
                 if (key[q] == P2G_ODD) continue;
@@ -880,34 +918,56 @@ __device__ __forceinline__ void p2g_body(const Dev& D, const CT& C) {
                 S.g[0][at] = vg[q][0];
                 S.g[1][at] = vg[q][1];
                 S.g[2][at] = vg[q][2];
+                const uint32_t cell = key[q] >> 3, o = key[q] & 7u, base = S.start[cell * 8u];
+                S.lst[0][base + S.pre[0][cell][o] + rank[q]] = (uint16_t)at;
+                S.lst[1][base + S.pre[1][cell][o] + rank[q]] = (uint16_t)at;
+            }
+            uint32_t gsz[2], gslot[2];
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const uint32_t it = tid + q * P2G_T, L = it >> 7, cell = (it >> 1) & 63u, h = it & 1u;
+                uint32_t lo, hi;
+                p2g_run(S, L, cell, h, lo, hi);
+                gsz[q] = hi - lo;
+                if (gsz[q]) gslot[q] = atomicAdd(&S.bucket[L][P2G_BUCKETS - 1 - min(gsz[q], P2G_BUCKETS - 1)], 1u);
             }
             __syncthreads();
-            // Groups: thread tid takes (kind tid / 64, cell tid % 64) and (kind + 4, same cell).
-            // Kinds 0-5: the faces along x, y, z, halves 0 and 1; 6-7: the cell centres, split in
-            // two by the x half. The 32 lanes of a warp are 32 cells of one half block with the
-            // same kind, so the tile's strides put their atomics in 32 different banks.
-#pragma unroll 1
+            if (tid < 4) {
+                uint32_t at = 0;
+                for (uint32_t k = 0; k < P2G_BUCKETS; k++) {
+                    const uint32_t c = S.bucket[tid][k];
+                    S.bucket[tid][k] = at;
+                    at += c;
+                }
+                S.bucket[tid][P2G_BUCKETS] = at;
+            }
+            __syncthreads();
+#pragma unroll
             for (int q = 0; q < 2; q++) {
-                const uint32_t item = tid + q * P2G_T;
-                const uint32_t kind = item >> 6, cell = item & 63u;
-                const I3 l = {(int32_t)(cell >> 4), (int32_t)((cell >> 2) & 3u), (int32_t)(cell & 3u)};
-                const uint32_t k0 = cell * 8u;
-                const uint32_t h = kind & 1u;
-                // The octant bit of the half: x (bit 2) for the x faces and the cell centres,
-                // y (bit 1), z (bit 0); the stencil starts one node further along that axis
-                // in the upper half of a face lattice.
-                const uint32_t bit = kind < 2 || kind >= 6 ? 2u : kind < 4 ? 1u : 0u;
-                I3 t = l;
-                if (kind < 2) t.x += (int32_t)h;
-                else if (kind < 4) t.y += (int32_t)h;
-                else if (kind < 6) t.z += (int32_t)h;
+                const uint32_t it = tid + q * P2G_T, L = it >> 7;
+                if (gsz[q]) S.items[L][S.bucket[L][P2G_BUCKETS - 1 - min(gsz[q], P2G_BUCKETS - 1)] + gslot[q]] = (uint16_t)(it & 127u);
+            }
+            __syncthreads();
+            // Two rounds of groups: warps 0-3 take a lattice's groups and warps 4-7 another's,
+            // x faces with y faces, then z faces with the cell centres.
+#pragma unroll 1
+            for (uint32_t round = 0; round < 2; round++) {
+                const uint32_t L = round * 2u + (tid >> 7), k = tid & 127u;
+                if (k >= S.bucket[L][P2G_BUCKETS]) continue;
+                const uint32_t grp = S.items[L][k], cell = grp >> 1, h = grp & 1u;
+                uint32_t lo, hi;
+                p2g_run(S, L, cell, h, lo, hi);
+                I3 t = {(int32_t)(cell >> 4), (int32_t)((cell >> 2) & 3u), (int32_t)(cell & 3u)};
+                if (L == 0) t.x += (int32_t)h;
+                else if (L == 1) t.y += (int32_t)h;
+                else if (L == 2) t.z += (int32_t)h;
                 const V3 base = vf(corner + t);
                 const uint32_t t0 = (uint32_t)t.x * TPX + (uint32_t)t.y * TPY + (uint32_t)t.z;
-                switch (kind) {
-                    case 0: case 1: p2g_group<0>(S, k0, bit, h, base, t0); break;
-                    case 2: case 3: p2g_group<1>(S, k0, bit, h, base, t0); break;
-                    case 4: case 5: p2g_group<2>(S, k0, bit, h, base, t0); break;
-                    default: p2g_group<3>(S, k0, bit, h, base, t0); break;
+                switch (L) {
+                    case 0: p2g_group<0>(S, lo, hi, base, t0); break;
+                    case 1: p2g_group<1>(S, lo, hi, base, t0); break;
+                    case 2: p2g_group<2>(S, lo, hi, base, t0); break;
+                    default: p2g_group<3>(S, lo, hi, base, t0); break;
                 }
             }
             // Particles outside the exact fast range: splatted one by one.
@@ -942,10 +1002,6 @@ __global__ void __launch_bounds__(P2G_T, 2) k_p2g_m(Multi M) {
     p2g_body(sD, c);
 }
 
-// Sums of the P2G tiles at each cell: a cell with local coordinate l along an axis lies in
-// the tile of its own block (at l + 1), in the tile of the block below when l <= 1 (at l + 5)
-// and of the block above when l == 3 (at 0). Integer sums, so the same as adding every tile
-// entry atomically, in any order.
 template <class CT>
 __device__ __forceinline__ void p2g_gather_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
