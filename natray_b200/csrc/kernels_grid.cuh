@@ -731,6 +731,12 @@ __device__ __forceinline__ void p2g_group(P2GShared& S, uint32_t lo, uint32_t hi
         const V3 xo = {L == 0 ? X.x : X.x - 0.5f, L == 1 ? X.y : X.y - 0.5f, L == 2 ? X.z : X.z - 0.5f};
         const V3 fx = xo - b;
         const V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
+        // The fixed-point scales are powers of two, so scaling is exact: weight16 = weight * 2^16
+        // (wx taken times 2^16 first), its value t = weight16 * node = (weight * node) * 2^16, and
+        // weight16 * 2^8 = weight * 2^24, bit for bit the splat's products. Pairs of them go
+        // through the packed FP32 instructions (each lane rounds as the scalar one would).
+        const float wx16[3] = {wx[0] * FP_M, wx[1] * FP_M, wx[2] * FP_M};
+        const float2 mag = make_float2(12582912.0f, 8388608.0f);
         if (L < 3) {
             const float4 G = S.g[L][j];
             // hg . ((a, b, c) - fx) as the splat sums it: (x term + y term) + z term.
@@ -741,30 +747,38 @@ __device__ __forceinline__ void p2g_group(P2GShared& S, uint32_t lo, uint32_t hi
             for (int a = 0; a < 3; a++)
 #pragma unroll
                 for (int bb = 0; bb < 3; bb++) {
-                    const float wab = wx[a] * wy[bb];
+                    const float wab16 = wx16[a] * wy[bb];
                     const float sab = px[a] + py[bb];
-#pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        const float weight = wab * wz[c];
-                        const float node = G.w + (sab + pz[c]);
-                        sv[a * 9 + bb * 3 + c] += __float_as_int(__fadd_rn(__fmul_rn(weight * node, FP_M), 12582912.0f));
-                        sw[a * 9 + bb * 3 + c] += __float_as_int(__fadd_rn(__fmul_rn(weight, FP_W), 8388608.0f));
-                    }
+                    const float2 w01 = __fmul2_rn(make_float2(wab16, wab16), make_float2(wz[0], wz[1]));
+                    const float2 n01 = __fadd2_rn(make_float2(G.w, G.w), __fadd2_rn(make_float2(sab, sab), make_float2(pz[0], pz[1])));
+                    const float w2 = wab16 * wz[2];
+                    const float n2 = G.w + (sab + pz[2]);
+                    const float2 r0 = __fadd2_rn(__fmul2_rn(make_float2(w01.x, w01.x), make_float2(n01.x, 256.0f)), mag);
+                    const float2 r1 = __fadd2_rn(__fmul2_rn(make_float2(w01.y, w01.y), make_float2(n01.y, 256.0f)), mag);
+                    const float2 r2 = __fadd2_rn(__fmul2_rn(make_float2(w2, w2), make_float2(n2, 256.0f)), mag);
+                    const int k = a * 9 + bb * 3;
+                    sv[k] += __float_as_int(r0.x), sw[k] += __float_as_int(r0.y);
+                    sv[k + 1] += __float_as_int(r1.x), sw[k + 1] += __float_as_int(r1.y);
+                    sv[k + 2] += __float_as_int(r2.x), sw[k + 2] += __float_as_int(r2.y);
                 }
         } else {
             // No affine term: the node value is the particle's (adding the dot product of a
             // zero gradient changes at most the sign of a zero, which rounds to 0 either way).
+            const float2 val = make_float2(X.w, 256.0f);
 #pragma unroll
             for (int a = 0; a < 3; a++)
 #pragma unroll
                 for (int bb = 0; bb < 3; bb++) {
-                    const float wab = wx[a] * wy[bb];
-#pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        const float weight = wab * wz[c];
-                        sv[a * 9 + bb * 3 + c] += __float_as_int(__fadd_rn(__fmul_rn(weight * X.w, FP_P), 12582912.0f));
-                        sw[a * 9 + bb * 3 + c] += __float_as_int(__fadd_rn(__fmul_rn(weight, FP_W), 8388608.0f));
-                    }
+                    const float wab16 = wx16[a] * wy[bb];
+                    const float2 w01 = __fmul2_rn(make_float2(wab16, wab16), make_float2(wz[0], wz[1]));
+                    const float w2 = wab16 * wz[2];
+                    const float2 r0 = __fadd2_rn(__fmul2_rn(make_float2(w01.x, w01.x), val), mag);
+                    const float2 r1 = __fadd2_rn(__fmul2_rn(make_float2(w01.y, w01.y), val), mag);
+                    const float2 r2 = __fadd2_rn(__fmul2_rn(make_float2(w2, w2), val), mag);
+                    const int k = a * 9 + bb * 3;
+                    sv[k] += __float_as_int(r0.x), sw[k] += __float_as_int(r0.y);
+                    sv[k + 1] += __float_as_int(r1.x), sw[k + 1] += __float_as_int(r1.y);
+                    sv[k + 2] += __float_as_int(r2.x), sw[k + 2] += __float_as_int(r2.y);
                 }
         }
     }
@@ -791,11 +805,12 @@ __device__ __forceinline__ void p2g_run(const P2GShared& S, uint32_t L, uint32_t
     const uint32_t k0 = cell * 8u, base = S.start[k0];
     if (L == 0 || L == 3) {  // x half: octants 4h .. 4h + 3 of the staged order
         lo = S.start[k0 + 4u * h], hi = S.start[k0 + 4u * h + 4u];
-    } else {  // y or z half: the first four places of the cell's run in that order, or the rest
+    } else {  // y or z half: the cell's run in that order, up to the first octant of the upper half
+        // (octant 2 = y half 1 alone, octant 1 = z half 1 alone, where that order starts it)
         const uint32_t n = S.start[k0 + 8u] - base;
-        const uint32_t first_half = h ? n : (uint32_t)S.pre[L - 1][cell][4];
-        lo = base + (h ? (uint32_t)S.pre[L - 1][cell][4] : 0u);
-        hi = base + first_half;
+        const uint32_t lower = S.pre[L - 1][cell][L == 1 ? 2 : 1];
+        lo = base + (h ? lower : 0u);
+        hi = base + (h ? n : lower);
     }
 }
 
