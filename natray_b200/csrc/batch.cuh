@@ -138,7 +138,6 @@ static ntr_status batch_create(int device, uint32_t max_scenes, uint64_t budget,
         CU(cudaEventCreateWithFlags(&B->ev_fork[k], cudaEventDisableTiming));
         CU(cudaEventCreateWithFlags(&B->ev_join[k], cudaEventDisableTiming));
     }
-    CU(cudaFuncSetAttribute(k_p2g_m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2G_SMEM));
     for (auto& s : B->slots) {
         CU(cudaEventCreateWithFlags(&s.ev_pre, cudaEventDisableTiming));
         CU(cudaMallocHost((void**)&s.h_state, sizeof(DevState)));
@@ -265,9 +264,7 @@ static uint64_t enqueue_step_multi(Batch& B, uint32_t n_jobs, const uint32_t* to
         LM(k_radix_scatter_m, GK_TILES, SCAT_T, s, p);
     }
     LM(k_block_bounds_m, GK_BOUNDS, 256, s);
-    if (tot[GK_BLK]) k_p2g_m<<<tot[GK_BLK], P2G_T, P2G_SMEM, s>>>(M(GK_BLK));
-    nl++;
-    if (prof) prof->mark("k_p2g_m", s);
+    LM(k_p2g_m, GK_BLK, P2G_T, s);
     LM(k_p2g_gather_m, GK_CELL, 256, s);
     join(0, a);
     LM(k_grid_prep_m, GK_CELL, 256, s);

@@ -202,6 +202,24 @@ __device__ __forceinline__ void multi_cta(const Multi& M, Dev& sD, Cta& sC) {
     __syncthreads();
 }
 
+// Packed FP32 multiply and add (two lanes of one 64-bit register pair, sm_100). Written in PTX
+// with an explicit round-to-nearest modifier so that no multiply and add pair is ever fused into a
+// packed FMA: each lane rounds exactly as the scalar __fmul_rn and __fadd_rn would.
+__device__ __forceinline__ float2 mul2_rn(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 add2_rn(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
 // ---- vectors (association as written in the WGSL) ------------------------------------------
 struct V3 {
     float x, y, z;

@@ -660,356 +660,124 @@ __device__ __forceinline__ uint32_t tile_cell(const uint32_t* links, uint32_t t)
     return b * 64u + (uint32_t)l.x * 16u + (uint32_t)l.y * 4u + (uint32_t)l.z;
 }
 
-// P2G by stencil groups. Particles of one cell whose stencils on a lattice start at the same
-// node add to the same 27 nodes of the tile: for a face lattice these are the particles of the
-// cell on one side of its middle along that lattice's axis (the half decides whether the
-// stencil starts at the cell below or at the cell itself); the cell-centred lattice's stencil is
-// the same for the whole cell, which is split in two by its x half. A thread owns one such group
-// (a lattice, a cell, a half) and sums its particles' rounded i32 contributions to the 27 nodes
-// in registers, then adds each node's sum to the tile with one shared atomic, instead of one
-// atomic per particle and node. Integer sums do not depend on the order of the adds, so the tile
-// is the same as the particle-by-particle splat's, bit for bit.
-//
-// A block's particles are taken in chunks of P2G_CHUNK. Each chunk's particles are counted by
-// (cell, octant) (octant = the particle's half of its cell along each axis, from the same float
-// expressions as the stencils' first nodes), the counts scanned, and the particles' values
-// staged in shared memory in (cell, x half, y half, z half) order: position in cells and the
-// cell-centred value, and per face lattice the velocity component and h times the affine row.
-// Two lists of staged indices put the same particles in (cell, y half, x half, z half) and
-// (cell, z half, x half, y half) order, so that every group is one contiguous run: in the staged
-// order for the x faces and the cell centres, in those lists for the y and z faces. Each
-// lattice's non-empty groups are listed most particles first, and its threads take them in that
-// order: the lanes of a warp, all on one lattice, loop over similar counts. A particle whose
-// values would leave the range in which the rounding by addition is exact on any lattice (or that
-// are not finite) takes the particle-by-particle splat instead.
-constexpr uint32_t P2G_CHUNK = 2 * P2G_T;
-constexpr uint32_t P2G_KEYS = 64 * 8;  // (cell, octant)
-constexpr uint16_t P2G_ODD = 0xffffu;
-constexpr uint32_t P2G_BUCKETS = 16;   // groups sorted by min(particles, 15), most first
+constexpr uint32_t P2G_CAP = 1024;  // particles of a block ordered at a time
+constexpr uint32_t P2G_LAYERS = 64;  // ranks within a cell that get the interleaved order
 
-struct P2GShared {
-    float4 x[P2G_CHUNK];      // position in cells, w = the cell-centred value (pressure / 1e6)
-    float4 g[3][P2G_CHUNK];   // per face lattice: h * affine row, w = velocity component
-    int32_t tile[8 * TPF];
-    uint32_t start[P2G_KEYS + 1];         // key counts, then where each key's run starts
-    uint16_t lst[2][P2G_CHUNK];           // staged indices in y-half and in z-half order
-    uint8_t pre[2][64][8];                // per cell and octant: where its run starts in those orders, in the cell
-    uint16_t items[4][128];               // per lattice: its groups (cell * 2 + half), most particles first
-    uint32_t bucket[4][P2G_BUCKETS + 1];  // per lattice: groups per count, then where they start
-    uint32_t odd[P2G_CHUNK];
-    uint32_t own[64];
-    uint32_t warp_sum[P2G_T / 32];
-    uint32_t n_odd;
-};
-constexpr size_t P2G_SMEM = sizeof(P2GShared);
-
-// The fast-path test of splat() for one lattice: the rounding by addition is exact when every
-// node value times the scale is well inside 2^22 and nothing is infinite or NaN.
-__device__ __forceinline__ bool p2g_fast(float val, V3 hg, V3 fx, float scale) {
-    const float bound = fabsf(val) + 1.5f * (fabsf(hg.x) + fabsf(hg.y) + fabsf(hg.z));
-    return bound * scale < 4.0e6f && fabsf(fx.x) + fabsf(fx.y) + fabsf(fx.z) < 8.0f;
-}
-
-// Octant o = (x half, y half, z half) as bits 2, 1, 0; its place in the y-half and z-half orders.
-__device__ __forceinline__ uint32_t oct_y_first(uint32_t o) { return ((o >> 1) & 1u) << 2 | (o >> 2) << 1 | (o & 1u); }
-__device__ __forceinline__ uint32_t oct_z_first(uint32_t o) { return (o & 1u) << 2 | (o >> 2) << 1 | ((o >> 1) & 1u); }
-
-// One group's sums. Lattice L: 0, 1, 2 the faces along x, y, z (offset 0 along that axis, 0.5
-// along the others), 3 the cell centres. The group is the run [lo, hi) of the staged order (x
-// faces, cell centres) or of the y-half or z-half list; `b` is the stencil's first node
-// (domain cells, as floats), `t0` its tile index.
-template <int L>
-__device__ __forceinline__ void p2g_group(P2GShared& S, uint32_t lo, uint32_t hi, V3 b, uint32_t t0) {
-    int32_t sv[27], sw[27];
-#pragma unroll
-    for (int k = 0; k < 27; k++) sv[k] = 0, sw[k] = 0;
-#pragma unroll 1
-    for (uint32_t q = lo; q < hi; q++) {
-        const uint32_t j = (L == 1 || L == 2) ? (uint32_t)S.lst[L - 1][q] : q;
-        const float4 X = S.x[j];
-        // x - o per axis (x - 0 is x), then the offset from the stencil's first node.
-        const V3 xo = {L == 0 ? X.x : X.x - 0.5f, L == 1 ? X.y : X.y - 0.5f, L == 2 ? X.z : X.z - 0.5f};
-        const V3 fx = xo - b;
-        const V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
-        // The fixed-point scales are powers of two, so scaling is exact: weight16 = weight * 2^16
-        // (wx taken times 2^16 first), its value t = weight16 * node = (weight * node) * 2^16, and
-        // weight16 * 2^8 = weight * 2^24, bit for bit the splat's products. Pairs of them go
-        // through the packed FP32 instructions (each lane rounds as the scalar one would).
-        const float wx16[3] = {wx[0] * FP_M, wx[1] * FP_M, wx[2] * FP_M};
-        const float2 mag = make_float2(12582912.0f, 8388608.0f);
-        if (L < 3) {
-            const float4 G = S.g[L][j];
-            // hg . ((a, b, c) - fx) as the splat sums it: (x term + y term) + z term.
-            const float px[3] = {G.x * (0.0f - fx.x), G.x * (1.0f - fx.x), G.x * (2.0f - fx.x)};
-            const float py[3] = {G.y * (0.0f - fx.y), G.y * (1.0f - fx.y), G.y * (2.0f - fx.y)};
-            const float pz[3] = {G.z * (0.0f - fx.z), G.z * (1.0f - fx.z), G.z * (2.0f - fx.z)};
-#pragma unroll
-            for (int a = 0; a < 3; a++)
-#pragma unroll
-                for (int bb = 0; bb < 3; bb++) {
-                    const float wab16 = wx16[a] * wy[bb];
-                    const float sab = px[a] + py[bb];
-                    const float2 w01 = __fmul2_rn(make_float2(wab16, wab16), make_float2(wz[0], wz[1]));
-                    const float2 n01 = __fadd2_rn(make_float2(G.w, G.w), __fadd2_rn(make_float2(sab, sab), make_float2(pz[0], pz[1])));
-                    const float w2 = wab16 * wz[2];
-                    const float n2 = G.w + (sab + pz[2]);
-                    const float2 r0 = __fadd2_rn(__fmul2_rn(make_float2(w01.x, w01.x), make_float2(n01.x, 256.0f)), mag);
-                    const float2 r1 = __fadd2_rn(__fmul2_rn(make_float2(w01.y, w01.y), make_float2(n01.y, 256.0f)), mag);
-                    const float2 r2 = __fadd2_rn(__fmul2_rn(make_float2(w2, w2), make_float2(n2, 256.0f)), mag);
-                    const int k = a * 9 + bb * 3;
-                    sv[k] += __float_as_int(r0.x), sw[k] += __float_as_int(r0.y);
-                    sv[k + 1] += __float_as_int(r1.x), sw[k + 1] += __float_as_int(r1.y);
-                    sv[k + 2] += __float_as_int(r2.x), sw[k + 2] += __float_as_int(r2.y);
-                }
-        } else {
-            // No affine term: the node value is the particle's (adding the dot product of a
-            // zero gradient changes at most the sign of a zero, which rounds to 0 either way).
-            const float2 val = make_float2(X.w, 256.0f);
-#pragma unroll
-            for (int a = 0; a < 3; a++)
-#pragma unroll
-                for (int bb = 0; bb < 3; bb++) {
-                    const float wab16 = wx16[a] * wy[bb];
-                    const float2 w01 = __fmul2_rn(make_float2(wab16, wab16), make_float2(wz[0], wz[1]));
-                    const float w2 = wab16 * wz[2];
-                    const float2 r0 = __fadd2_rn(__fmul2_rn(make_float2(w01.x, w01.x), val), mag);
-                    const float2 r1 = __fadd2_rn(__fmul2_rn(make_float2(w01.y, w01.y), val), mag);
-                    const float2 r2 = __fadd2_rn(__fmul2_rn(make_float2(w2, w2), val), mag);
-                    const int k = a * 9 + bb * 3;
-                    sv[k] += __float_as_int(r0.x), sw[k] += __float_as_int(r0.y);
-                    sv[k + 1] += __float_as_int(r1.x), sw[k + 1] += __float_as_int(r1.y);
-                    sv[k + 2] += __float_as_int(r2.x), sw[k + 2] += __float_as_int(r2.y);
-                }
-        }
-    }
-    const uint32_t n = hi - lo;
-    if (n == 0) return;
-    // Each sum carries n times the rounding constant's bits; take them off (mod 2^32).
-    const int32_t ov = (int32_t)(n * 0x4B400000u), ow = (int32_t)(n * 0x4B000000u);
-    const uint32_t fa = L < 3 ? 2u * L : (uint32_t)A_PC, fw = L < 3 ? 2u * L + 1u : (uint32_t)A_WC;
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-#pragma unroll
-        for (int bb = 0; bb < 3; bb++)
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                const uint32_t t = t0 + a * TPX + bb * TPY + c;
-                const int k = a * 9 + bb * 3 + c;
-                atomicAdd(&S.tile[fa * TPF + t], sv[k] - ov);
-                atomicAdd(&S.tile[fw * TPF + t], sw[k] - ow);
-            }
-}
-
-// Particles of group (lattice L, cell, half h) in its run: the particle count and the run's start.
-__device__ __forceinline__ void p2g_run(const P2GShared& S, uint32_t L, uint32_t cell, uint32_t h, uint32_t& lo, uint32_t& hi) {
-    const uint32_t k0 = cell * 8u, base = S.start[k0];
-    if (L == 0 || L == 3) {  // x half: octants 4h .. 4h + 3 of the staged order
-        lo = S.start[k0 + 4u * h], hi = S.start[k0 + 4u * h + 4u];
-    } else {  // y or z half: the cell's run in that order, up to the first octant of the upper half
-        // (octant 2 = y half 1 alone, octant 1 = z half 1 alone, where that order starts it)
-        const uint32_t n = S.start[k0 + 8u] - base;
-        const uint32_t lower = S.pre[L - 1][cell][L == 1 ? 2 : 1];
-        lo = base + (h ? lower : 0u);
-        hi = base + (h ? n : lower);
-    }
-}
-
-// One block per iteration of a CTA; the tile is stored whole and k_p2g_gather sums the tiles
-// that overlap each cell.
+// One block per iteration of a CTA. Its particles add into a 7^3 x 8-field tile of i32 sums in
+// shared memory, in an order that spreads the 32 lanes of an atomic over 32 different cells:
+// a counting sort by cell gives each particle its rank in its cell, and the particles are
+// taken rank layer by rank layer, cell by cell within a layer (layer r holds the cells with
+// more than r particles). Lanes in different cells add to different nodes of the tile, mostly
+// in different banks; neighbours in the particle list share a cell and would collide. Integer
+// sums do not depend on the order of the adds. The tile is stored whole; k_p2g_gather sums the
+// tiles that overlap each cell.
 template <class CT>
 __device__ __forceinline__ void p2g_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
-    extern __shared__ __align__(16) unsigned char p2g_smem[];
-    P2GShared& S = *reinterpret_cast<P2GShared*>(p2g_smem);
     const Grid g = grid_of(D, cur_of(st));
     const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
-    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    __shared__ __align__(16) int32_t tile[8 * TPF];
+    __shared__ uint32_t own[64], s_cnt[64];
+    __shared__ uint32_t s_pid[P2G_CAP];
+    __shared__ uint8_t s_cell[P2G_CAP];
+    __shared__ uint16_t s_rank[P2G_CAP];
+    __shared__ uint32_t s_mlo[P2G_LAYERS], s_mhi[P2G_LAYERS];  // layer r: cells 0-31, 32-63 with > r particles
+    __shared__ uint32_t s_start[P2G_LAYERS + 1], s_over;
     const float hh = g.h;
     for (uint32_t b = C.x(); b < nb; b += C.nx()) {
         const I3 bc = slot_coord(g, g.list[b]);
-        if (tid < 27) {
-            I3 n = bc + I3{(int32_t)(tid / 9u), (int32_t)((tid / 3u) % 3u), (int32_t)(tid % 3u)} - I3{1, 1, 1};
-            D.block_nb[b * 27u + tid] = block_at(g, n);
+        if (threadIdx.x < 27) {
+            uint32_t li = threadIdx.x;
+            I3 n = bc + I3{(int32_t)(li / 9u), (int32_t)((li / 3u) % 3u), (int32_t)(li % 3u)} - I3{1, 1, 1};
+            D.block_nb[b * 27u + li] = block_at(g, n);
         }
-        if (tid < 64) S.own[tid] = 0;
+        if (threadIdx.x < 64) own[threadIdx.x] = 0;
         const uint32_t first = D.block_start[b];
         const uint32_t count = D.block_start[b + 1] - first;
         if (count == 0) {
-            if (tid < 64) D.acc[(size_t)A_N * D.cap_cells + b * 64u + tid] = 0;
-            if (tid == 0) D.tile_ok[b] = 0u;
+            if (threadIdx.x < 64) D.acc[(size_t)A_N * D.cap_cells + b * 64u + threadIdx.x] = 0;
+            if (threadIdx.x == 0) D.tile_ok[b] = 0u;
             __syncthreads();
             continue;
         }
-        for (uint32_t t = tid; t < 8 * TPF; t += P2G_T) S.tile[t] = 0;
+        for (uint32_t t = threadIdx.x; t < 8 * TPF; t += P2G_T) tile[t] = 0;
         const I3 corner = bc * 4 - I3{1, 1, 1};
-        for (uint32_t chunk = 0; chunk < count; chunk += P2G_CHUNK) {
-            const uint32_t n = min(P2G_CHUNK, count - chunk);
-            for (uint32_t k = tid; k < P2G_KEYS; k += P2G_T) S.start[k] = 0;
-            if (tid < 4 * (P2G_BUCKETS + 1)) (&S.bucket[0][0])[tid] = 0;
-            if (tid == 0) S.n_odd = 0;
+        for (uint32_t chunk = 0; chunk < count; chunk += P2G_CAP) {
+            const uint32_t n = min(P2G_CAP, count - chunk);
+            if (threadIdx.x < 64) s_cnt[threadIdx.x] = 0, s_mlo[threadIdx.x] = 0u, s_mhi[threadIdx.x] = 0u;
+            if (threadIdx.x == 0) s_over = 0;
             __syncthreads();
-            // Each thread's two particles: key, rank in its key, and the staged values, kept in
-            // registers until the keys' starts are known.
-            uint32_t key[2], rank[2];
-            float4 vx[2], vg[2][3];
-#pragma unroll
-            for (int q = 0; q < 2; q++) {
-                const uint32_t j = tid + q * P2G_T;
-                key[q] = P2G_ODD;
-                if (j >= n) continue;
+            // Each particle's cell and rank in its cell.
+            for (uint32_t j = threadIdx.x; j < n; j += P2G_T) {
                 const uint32_t i = D.sorted[first + chunk + j];
-                const float4 pos = D.pos[i], vel = D.vel[i], c0 = D.c0[i], c1 = D.c1[i], c2 = D.c2[i];
-                const V3 x = (xyz(pos) - g.org) / hh;
-                const I3 own = vi(vfloor(x)) - bc * 4;  // own_cell, in the block
-                if ((uint32_t)own.x < 4u && (uint32_t)own.y < 4u && (uint32_t)own.z < 4u)
-                    atomicAdd(&S.own[(uint32_t)(own.x * 16 + own.y * 4 + own.z)], 1u);
-                // First stencil nodes: offset 0 along an axis gives A, offset 0.5 gives B.
-                const V3 xh = {x.x - 0.5f, x.y - 0.5f, x.z - 0.5f};
-                const I3 A = vi(vfloor(xh));
-                const I3 B = vi(vfloor(xh - 0.5f));
-                const I3 l = B - corner;
-                const I3 o = A - B;
-                // fx of the two offsets: (x - 0) - A and (x - 0.5) - B.
-                const V3 fa3 = x - vf(A), fb3 = xh - vf(B);
-                const V3 hu = xyz(c0) * hh, hv = xyz(c1) * hh, hw = xyz(c2) * hh;
-                const float pc = c0.w * 1e-6f;
-                bool ok = l.x == own.x && l.y == own.y && l.z == own.z && (uint32_t)own.x < 4u && (uint32_t)own.y < 4u &&
-                          (uint32_t)own.z < 4u && (uint32_t)o.x <= 1u && (uint32_t)o.y <= 1u && (uint32_t)o.z <= 1u;
-                ok = ok && p2g_fast(vel.x, hu, V3{fa3.x, fb3.y, fb3.z}, FP_M) && p2g_fast(vel.y, hv, V3{fb3.x, fa3.y, fb3.z}, FP_M) &&
-                     p2g_fast(vel.z, hw, V3{fb3.x, fb3.y, fa3.z}, FP_M) && p2g_fast(pc, V3{0.0f, 0.0f, 0.0f}, fb3, FP_P);
-                if (!ok) {
-                    S.odd[atomicAdd(&S.n_odd, 1u)] = i;
-                    continue;
-                }
-                key[q] = (uint32_t)(l.x * 16 + l.y * 4 + l.z) * 8u + (uint32_t)(o.x * 4 + o.y * 2 + o.z);
-                rank[q] = atomicAdd(&S.start[key[q]], 1u);
-                vx[q] = make_float4(x.x, x.y, x.z, pc);
-                vg[q][0] = make_float4(hu.x, hu.y, hu.z, vel.x);
-                vg[q][1] = make_float4(hv.x, hv.y, hv.z, vel.y);
-                vg[q][2] = make_float4(hw.x, hw.y, hw.z, vel.z);
+                const I3 l = own_cell(g, xyz(D.pos[i])) - bc * 4;
+                const uint32_t c = (uint32_t)(l.x * 16 + l.y * 4 + l.z);
+                s_cell[j] = (uint8_t)c;
+                s_rank[j] = (uint16_t)atomicAdd(&s_cnt[c], 1u);
             }
             __syncthreads();
-            // Each cell's octant counts in the y-half and z-half orders (threads 0-63), before
-            // the counts become starts.
-            uint32_t cnt8[8];
-            if (tid < 64) {
-#pragma unroll
-                for (int o = 0; o < 8; o++) cnt8[o] = S.start[tid * 8 + o];
-                uint32_t py = 0, pz = 0;
-#pragma unroll
-                for (int r = 0; r < 8; r++)
-#pragma unroll
-                    for (int o = 0; o < 8; o++) {
-                        if (oct_y_first(o) == (uint32_t)r) S.pre[0][tid][o] = (uint8_t)py, py += cnt8[o];
-                        if (oct_z_first(o) == (uint32_t)r) S.pre[1][tid][o] = (uint8_t)pz, pz += cnt8[o];
-                    }
-            }
-            // Exclusive scan of the 512 key counts: two a thread, warp scans, then the warps'.
-            {
-                const uint32_t c0n = S.start[2 * tid], c1n = S.start[2 * tid + 1];
-                uint32_t inc = c0n + c1n;
-#pragma unroll
-                for (int off = 1; off < 32; off <<= 1) {
-                    const uint32_t v = __shfl_up_sync(0xffffffffu, inc, off);
-                    if (lane >= (uint32_t)off) inc += v;
-                }
-                if (lane == 31) S.warp_sum[warp] = inc;
-                __syncthreads();
-                uint32_t before = 0;
-                for (uint32_t w = 0; w < warp; w++) before += S.warp_sum[w];
-                const uint32_t ex = before + inc - c0n - c1n;
-                S.start[2 * tid] = ex;
-                S.start[2 * tid + 1] = ex + c0n;
-                if (tid == P2G_T - 1) S.start[P2G_KEYS] = ex + c0n + c1n;
-            }
-            __syncthreads();
-            // Stage the values; the two lists; count each lattice's groups by size.
-#pragma unroll
-            for (int q = 0; q < 2; q++) {
-                if (key[q] == P2G_ODD) continue;
-                const uint32_t at = S.start[key[q]] + rank[q];
-                S.x[at] = vx[q];
-                S.g[0][at] = vg[q][0];
-                S.g[1][at] = vg[q][1];
-                S.g[2][at] = vg[q][2];
-                const uint32_t cell = key[q] >> 3, o = key[q] & 7u, base = S.start[cell * 8u];
-                S.lst[0][base + S.pre[0][cell][o] + rank[q]] = (uint16_t)at;
-                S.lst[1][base + S.pre[1][cell][o] + rank[q]] = (uint16_t)at;
-            }
-            uint32_t gsz[2], gslot[2];
-#pragma unroll
-            for (int q = 0; q < 2; q++) {
-                const uint32_t it = tid + q * P2G_T, L = it >> 7, cell = (it >> 1) & 63u, h = it & 1u;
-                uint32_t lo, hi;
-                p2g_run(S, L, cell, h, lo, hi);
-                gsz[q] = hi - lo;
-                if (gsz[q]) gslot[q] = atomicAdd(&S.bucket[L][P2G_BUCKETS - 1 - min(gsz[q], P2G_BUCKETS - 1)], 1u);
-            }
-            __syncthreads();
-            if (tid < 4) {
-                uint32_t at = 0;
-                for (uint32_t k = 0; k < P2G_BUCKETS; k++) {
-                    const uint32_t c = S.bucket[tid][k];
-                    S.bucket[tid][k] = at;
-                    at += c;
-                }
-                S.bucket[tid][P2G_BUCKETS] = at;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int q = 0; q < 2; q++) {
-                const uint32_t it = tid + q * P2G_T, L = it >> 7;
-                if (gsz[q]) S.items[L][S.bucket[L][P2G_BUCKETS - 1 - min(gsz[q], P2G_BUCKETS - 1)] + gslot[q]] = (uint16_t)(it & 127u);
-            }
-            __syncthreads();
-            // Two rounds of groups: warps 0-3 take a lattice's groups and warps 4-7 another's,
-            // x faces with y faces, then z faces with the cell centres.
-#pragma unroll 1
-            for (uint32_t round = 0; round < 2; round++) {
-                const uint32_t L = round * 2u + (tid >> 7), k = tid & 127u;
-                if (k >= S.bucket[L][P2G_BUCKETS]) continue;
-                const uint32_t grp = S.items[L][k], cell = grp >> 1, h = grp & 1u;
-                uint32_t lo, hi;
-                p2g_run(S, L, cell, h, lo, hi);
-                I3 t = {(int32_t)(cell >> 4), (int32_t)((cell >> 2) & 3u), (int32_t)(cell & 3u)};
-                if (L == 0) t.x += (int32_t)h;
-                else if (L == 1) t.y += (int32_t)h;
-                else if (L == 2) t.z += (int32_t)h;
-                const V3 base = vf(corner + t);
-                const uint32_t t0 = (uint32_t)t.x * TPX + (uint32_t)t.y * TPY + (uint32_t)t.z;
-                switch (L) {
-                    case 0: p2g_group<0>(S, lo, hi, base, t0); break;
-                    case 1: p2g_group<1>(S, lo, hi, base, t0); break;
-                    case 2: p2g_group<2>(S, lo, hi, base, t0); break;
-                    default: p2g_group<3>(S, lo, hi, base, t0); break;
+            // The layers' cell masks (a ballot per layer by the two warps of the 64 cells), then
+            // where each layer starts (a scan by one warp).
+            if (threadIdx.x < 64) {
+                const uint32_t cnt = s_cnt[threadIdx.x];
+                own[threadIdx.x] += cnt;
+                uint32_t* m = threadIdx.x < 32 ? s_mlo : s_mhi;
+                for (uint32_t r = 0; r < P2G_LAYERS; r++) {
+                    const uint32_t bits = __ballot_sync(0xffffffffu, cnt > r);
+                    if (bits == 0u) break;
+                    if (lane == 0) m[r] = bits;
                 }
             }
-            // Particles outside the exact fast range: splatted one by one.
-            for (uint32_t k = tid; k < S.n_odd; k += P2G_T) {
-                const uint32_t i = S.odd[k];
+            __syncthreads();
+            if (threadIdx.x < 32) {
+                const uint32_t p = __popc(s_mlo[2 * lane]) + __popc(s_mhi[2 * lane]);
+                const uint32_t q = __popc(s_mlo[2 * lane + 1]) + __popc(s_mhi[2 * lane + 1]);
+                uint32_t inc = p + q;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (lane >= (uint32_t)o) inc += v;
+                }
+                s_start[2 * lane] = inc - p - q, s_start[2 * lane + 1] = inc - q;
+                if (lane == 31) s_start[P2G_LAYERS] = inc;
+            }
+            __syncthreads();
+            for (uint32_t j = threadIdx.x; j < n; j += P2G_T) {
+                const uint32_t c = s_cell[j], r = s_rank[j];
+                uint32_t pos;
+                if (r < P2G_LAYERS)
+                    pos = s_start[r] + (c < 32u ? __popc(s_mlo[r] & ((1u << c) - 1u)) : __popc(s_mlo[r]) + __popc(s_mhi[r] & ((1u << (c - 32u)) - 1u)));
+                else
+                    pos = s_start[P2G_LAYERS] + atomicAdd(&s_over, 1u);
+                s_pid[pos] = D.sorted[first + chunk + j];
+            }
+            __syncthreads();
+            for (uint32_t j = threadIdx.x; j < n; j += P2G_T) {
+                const uint32_t i = s_pid[j];
                 float4 pos = D.pos[i], vel = D.vel[i], c0 = D.c0[i], c1 = D.c1[i], c2 = D.c2[i];
                 V3 x = (xyz(pos) - g.org) / hh;
-                splat(S.tile, x, v3(0.0f, 0.5f, 0.5f), corner, 0, vel.x, xyz(c0), 1, FP_M, hh);
-                splat(S.tile, x, v3(0.5f, 0.0f, 0.5f), corner, 2, vel.y, xyz(c1), 3, FP_M, hh);
-                splat(S.tile, x, v3(0.5f, 0.5f, 0.0f), corner, 4, vel.z, xyz(c2), 5, FP_M, hh);
-                splat(S.tile, x, v3(0.5f, 0.5f, 0.5f), corner, A_PC, c0.w * 1e-6f, v3(0.0f, 0.0f, 0.0f), A_WC, FP_P, hh);
+                splat(tile, x, v3(0.0f, 0.5f, 0.5f), corner, 0, vel.x, xyz(c0), 1, FP_M, hh);
+                splat(tile, x, v3(0.5f, 0.0f, 0.5f), corner, 2, vel.y, xyz(c1), 3, FP_M, hh);
+                splat(tile, x, v3(0.5f, 0.5f, 0.0f), corner, 4, vel.z, xyz(c2), 5, FP_M, hh);
+                splat(tile, x, v3(0.5f, 0.5f, 0.5f), corner, A_PC, c0.w * 1e-6f, v3(0.0f, 0.0f, 0.0f), A_WC, FP_P, hh);
             }
             __syncthreads();
         }
         // Stored in the packed layout (8 fields x 343, strides 49, 7, 1) k_p2g_gather reads.
         int32_t* dst = D.tiles + (size_t)b * 8 * TILE;
-        for (uint32_t e = tid; e < 8 * TILE; e += P2G_T) {
+        for (uint32_t e = threadIdx.x; e < 8 * TILE; e += P2G_T) {
             const uint32_t f = e / TILE, r = e - f * TILE, x = r / 49u, y = (r - x * 49u) / 7u, z = r - x * 49u - y * 7u;
-            dst[e] = S.tile[f * TPF + x * TPX + y * TPY + z];
+            dst[e] = tile[f * TPF + x * TPX + y * TPY + z];
         }
-        if (tid < 64) D.acc[(size_t)A_N * D.cap_cells + b * 64u + tid] = (int32_t)S.own[tid];
-        if (tid == 0) D.tile_ok[b] = 1u;
+        if (threadIdx.x < 64) D.acc[(size_t)A_N * D.cap_cells + b * 64u + threadIdx.x] = (int32_t)own[threadIdx.x];
+        if (threadIdx.x == 0) D.tile_ok[b] = 1u;
         __syncthreads();
     }
 }
-__global__ void __launch_bounds__(P2G_T, 2) k_p2g(Dev D) { p2g_body(D, HwCta{}); }
-__global__ void __launch_bounds__(P2G_T, 2) k_p2g_m(Multi M) {
+__global__ void __launch_bounds__(P2G_T, 3) k_p2g(Dev D) { p2g_body(D, HwCta{}); }
+__global__ void __launch_bounds__(P2G_T, 3) k_p2g_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);

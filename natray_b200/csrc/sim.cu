@@ -550,10 +550,7 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
         }
     }
     L(k_block_bounds, (D.Np + 1 + 255) / 256, 256, D);
-    // P2G takes its staging area as dynamic shared memory.
-    k_p2g<<<G_blk, P2G_T, P2G_SMEM, s>>>(D);
-    n++;
-    if (prof) prof->mark("k_p2g", s);
+    L(k_p2g, G_blk, P2G_T, D);
     L(k_p2g_gather, G_cell, 256, D);
     join(0);
     L(k_grid_prep, G_cell, 256, D);
@@ -722,9 +719,6 @@ static ntr_status create_from(const World& w, int device, Sim*& out, uint8_t* ar
     cudaDeviceProp prop;
     CU(cudaGetDeviceProperties(&prop, device));
     S->sms = prop.multiProcessorCount;
-    // P2G stages a chunk of particles, its tile and its keys in more shared memory than the
-    // 48 KB a kernel gets without asking.
-    CU(cudaFuncSetAttribute(k_p2g, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2G_SMEM));
     {
         // The persistent solver's grid must be co-resident: at most what occupancy allows.
         int occ_a = 0, occ_b = 0;
