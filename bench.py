@@ -420,11 +420,11 @@ def main():
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=30, help="steps of the CPU baseline sample")
     ap.add_argument("--batch-scenes", type=int, default=64, help="scenes of the batched run (0: skip)")
-    ap.add_argument("--batch-steps", type=int, default=100)
+    ap.add_argument("--batch-steps", type=int, default=500)
     ap.add_argument("--batch-chunk", type=int, default=8, help="steps per batch call (state read back between)")
-    ap.add_argument("--serve-requests", type=int, default=64, help="requests of the serving loop (0: skip)")
-    ap.add_argument("--serve-steps", type=int, default=100)
-    ap.add_argument("--serve-rate", type=float, default=20.0, help="request arrivals per second")
+    ap.add_argument("--serve-requests", type=int, default=200, help="requests of the serving loop (0: skip)")
+    ap.add_argument("--serve-steps", type=int, default=200)
+    ap.add_argument("--serve-rate", type=float, default=15.0, help="request arrivals per second")
     ap.add_argument("--keyframes", type=int, default=16, help="keyframes stored and shown at the bench scene (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
