@@ -141,38 +141,62 @@ __device__ __forceinline__ void mem_splat_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
-    uint32_t i = C.x() * blockDim.x + threadIdx.x;
-    if (i >= D.Nv || D.mem_mass[i] == 0.0f) return;
-    float2 pa = D.mem_push[i];
-    if (pa.y <= 0.0f) return;
-    float4 x4 = D.mem_x[0][i];
-    uint32_t own = cell_at(g, own_cell(g, xyz(x4)));
-    if (own != NONE) {
-        float a = pa.y * 1e6f;
-        atomicAdd(accp(D, A_MW, own), to_fp(a, FP_A));
-        float4 mv = D.mem_v[0][i];
-        atomicAdd(accp(D, A_MV + 0, own), to_fp(a * mv.x, FP_A));
-        atomicAdd(accp(D, A_MV + 1, own), to_fp(a * mv.y, FP_A));
-        atomicAdd(accp(D, A_MV + 2, own), to_fp(a * mv.z, FP_A));
+    // Every lane of the warp takes part in the merges below (a lane without a vertex adds
+    // nothing): vertices are in the mesh's spatial order, so the lanes of a warp mostly add to the
+    // same cells, and the lanes of each target cell sum their i32 terms (a match, then a reduction
+    // over the matching lanes) before one of them adds the sum with one atomic. Integer sums:
+    // the same as an atomic per term.
+    const uint32_t i = C.x() * blockDim.x + threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31u;
+    bool valid = i < D.Nv && D.mem_mass[i] != 0.0f;
+    float2 pa = make_float2(0.0f, 0.0f);
+    float4 x4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (valid) {
+        pa = D.mem_push[i];
+        valid = pa.y > 0.0f;
+        x4 = D.mem_x[0][i];
     }
-    bool on_water = D.mem_water[i].w >= CONTACT_F;
-    if (!on_water) return;
+    uint32_t own = valid ? cell_at(g, own_cell(g, xyz(x4))) : NONE;
+    {
+        const uint32_t peers = __match_any_sync(0xffffffffu, own);
+        if (own != NONE) {
+            const float a = pa.y * 1e6f;
+            const float4 mv = D.mem_v[0][i];
+            const int32_t vw = __reduce_add_sync(peers, to_fp(a, FP_A));
+            const int32_t vx = __reduce_add_sync(peers, to_fp(a * mv.x, FP_A));
+            const int32_t vy = __reduce_add_sync(peers, to_fp(a * mv.y, FP_A));
+            const int32_t vz = __reduce_add_sync(peers, to_fp(a * mv.z, FP_A));
+            if ((uint32_t)(__ffs(peers) - 1) == lane) {
+                atomicAdd(accp(D, A_MW, own), vw);
+                atomicAdd(accp(D, A_MV + 0, own), vx);
+                atomicAdd(accp(D, A_MV + 1, own), vy);
+                atomicAdd(accp(D, A_MV + 2, own), vz);
+            }
+        }
+    }
+    const bool on_water = valid && D.mem_water[i].w >= CONTACT_F;
+    if (!__any_sync(0xffffffffu, on_water)) return;  // warp-uniform
     V3 x = (xyz(x4) - g.org) / g.h - 0.5f;
     I3 base = vi(vfloor(x - 0.5f));
     V3 fx = x - vf(base);
     V3 wx = axis_weights(fx.x), wy = axis_weights(fx.y), wz = axis_weights(fx.z);
-    const Stencil27 sc = stencil_of(g, near_of(g, base), base);
+    const Stencil27 sc = stencil_of(g, near_of(g, on_water ? base : I3{0, 0, 0}), on_water ? base : I3{0, 0, 0});
 #pragma unroll
     for (int a = 0; a < 3; a++)
 #pragma unroll
         for (int b = 0; b < 3; b++)
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                uint32_t cell = sc.cell(a, b, c);
+                const uint32_t cell = on_water ? sc.cell(a, b, c) : NONE;
+                const uint32_t peers = __match_any_sync(0xffffffffu, cell);
                 if (cell == NONE) continue;
-                float w = wx[a] * wy[b] * wz[c];
-                atomicAdd(accp(D, A_MF, cell), to_fp(w * pa.x, FP_F));
-                atomicAdd(accp(D, A_MA, cell), to_fp(w * pa.y * 1e6f, FP_A));
+                const float w = wx[a] * wy[b] * wz[c];
+                const int32_t sf = __reduce_add_sync(peers, to_fp(w * pa.x, FP_F));
+                const int32_t sa = __reduce_add_sync(peers, to_fp(w * pa.y * 1e6f, FP_A));
+                if ((uint32_t)(__ffs(peers) - 1) == lane) {
+                    atomicAdd(accp(D, A_MF, cell), sf);
+                    atomicAdd(accp(D, A_MA, cell), sa);
+                }
             }
 }
 __global__ void k_mem_splat(Dev D) { mem_splat_body(D, HwCta{}); }
