@@ -9,7 +9,7 @@ reference's, src/sim.rs:20) and with a tight one (1e-7) on both sides, which sep
 arithmetic's own error from the difference the stopping tolerance leaves between two runs that
 stop at different iterates.
 
-    python tests/precision_study.py [--resolution 124] [--steps 1000] [--every 100] [--out FILE]
+    python tests/precision_study.py [--resolution 124] [--steps 1000] [--every 100] [--speed 350] [--out FILE]
 
 Prints a table per tolerance and writes all figures as JSON to --out. Test infrastructure: it
 drives the oracle. Needs a GPU.
@@ -63,8 +63,8 @@ def compare(a: World, b: World) -> dict:
             "iters": [int(a.h.iters), int(b.h.iters)]}
 
 
-def study(resolution: int, steps: int, every: int, tol: float, mesh_level: int = 6) -> list[dict]:
-    params = Params(resolution=resolution, mesh_level=mesh_level, dt_max=2e-6, bullet=6, caliber=8, bullet_speed=350,
+def study(resolution: int, steps: int, every: int, tol: float, mesh_level: int = 6, speed: float = 350.0) -> list[dict]:
+    params = Params(resolution=resolution, mesh_level=mesh_level, dt_max=2e-6, bullet=6, caliber=8, bullet_speed=speed,
                     solve_tol=tol)
     w = World(Oracle(build_world(params).blob).snapshot())  # the measuring substep on the CPU: both start alike
     sim, ref = Sim(world=w), Oracle(w.blob, real64=True)
@@ -89,13 +89,14 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--every", type=int, default=100)
     ap.add_argument("--tols", default="1e-5,1e-7")
+    ap.add_argument("--speed", type=float, default=350.0, help="the sphere's speed (1 m/s: it does not reach the balloon)")
     ap.add_argument("--out", default="")
     args = ap.parse_args()
-    out = {"resolution": args.resolution, "mesh_level": args.mesh_level, "steps": args.steps, "runs": {}}
+    out = {"resolution": args.resolution, "mesh_level": args.mesh_level, "steps": args.steps, "speed": args.speed, "runs": {}}
     for tol in [float(t) for t in args.tols.split(",")]:
         print(f"solver tolerance {tol:g}: relative L2 against FP64")
         print("   step   t (us)      x          v          p        mem_x     stretch    torn (product, FP64)")
-        out["runs"][f"{tol:g}"] = study(args.resolution, args.steps, args.every, tol, args.mesh_level)
+        out["runs"][f"{tol:g}"] = study(args.resolution, args.steps, args.every, tol, args.mesh_level, args.speed)
     if args.out:
         Path(args.out).write_text(json.dumps(out, indent=1))
 
