@@ -29,7 +29,6 @@ enum GridKind { GK_ONE, GK_CELL, GK_WORDS, GK_MARK, GK_SCAN, GK_TILES, GK_RSCAN,
 struct BatchSlot {
     std::unique_ptr<Sim> sim;
     uint32_t target = 0, done = 0;
-    cudaEvent_t ev_pre = nullptr;  // the scene's part before the solve is done
     // The slot's device region and pinned state buffer, kept across the scenes it holds; the
     // region grows (and only then is reallocated) when a scene needs more.
     uint8_t* arena = nullptr;
@@ -48,7 +47,6 @@ struct Batch {
     std::vector<BatchSlot> slots;
     cudaStream_t solve_stream = nullptr;  // the batch step's main stream
     cudaStream_t aux = nullptr, aux2 = nullptr;  // its side streams (as a one-scene step's)
-    cudaEvent_t ev_solve = nullptr;
     cudaEvent_t ev_fork[3] = {nullptr, nullptr, nullptr}, ev_join[3] = {nullptr, nullptr, nullptr};
     std::vector<cudaEvent_t> ev_sub;
     Dev* d_jobs = nullptr;  // the pointer tables of the scenes in the current step's order
@@ -86,13 +84,11 @@ struct Batch {
         if (d_first) cudaFree(d_first);
         for (auto& s : slots) {
             s.sim.reset();
-            if (s.ev_pre) cudaEventDestroy(s.ev_pre);
             if (s.arena) cudaFree(s.arena);
             if (s.h_state) cudaFreeHost(s.h_state);
         }
         slots.clear();
         if (d_jobs) cudaFree(d_jobs);
-        if (ev_solve) cudaEventDestroy(ev_solve);
         if (solve_stream) cudaStreamDestroy(solve_stream);
     }
 };
@@ -133,13 +129,11 @@ static ntr_status batch_create(int device, uint32_t max_scenes, uint64_t budget,
     CU(cudaStreamCreateWithFlags(&B->solve_stream, cudaStreamNonBlocking));
     CU(cudaStreamCreateWithFlags(&B->aux, cudaStreamNonBlocking));
     CU(cudaStreamCreateWithFlags(&B->aux2, cudaStreamNonBlocking));
-    CU(cudaEventCreateWithFlags(&B->ev_solve, cudaEventDisableTiming));
     for (int k = 0; k < 3; k++) {
         CU(cudaEventCreateWithFlags(&B->ev_fork[k], cudaEventDisableTiming));
         CU(cudaEventCreateWithFlags(&B->ev_join[k], cudaEventDisableTiming));
     }
     for (auto& s : B->slots) {
-        CU(cudaEventCreateWithFlags(&s.ev_pre, cudaEventDisableTiming));
         CU(cudaMallocHost((void**)&s.h_state, sizeof(DevState)));
     }
     CU(cudaMalloc((void**)&B->d_jobs, sizeof(Dev) * max_scenes));

@@ -37,9 +37,9 @@ namespace ntr {
     } while (0)
 
 struct GraphKey {
-    uint32_t n_mem, n_air, fp64, part, size;
+    uint32_t n_mem, n_air, fp64, size;
     bool operator<(const GraphKey& o) const {
-        return std::tie(n_mem, n_air, fp64, part, size) < std::tie(o.n_mem, o.n_air, o.fp64, o.part, o.size);
+        return std::tie(n_mem, n_air, fp64, size) < std::tie(o.n_mem, o.n_air, o.fp64, o.size);
     }
 };
 
@@ -428,7 +428,7 @@ static ntr_status prof_report(Prof& prof, char* report, size_t cap, size_t* len)
 
 // The pressure solve as one cooperative launch of `ctas` CTAs on `s`: of S alone (jobs == NULL),
 // or of the `n_jobs` simulations whose pointer tables are at `jobs` on the device. Each job's
-// barrier counter must be zero (the pre-solve part resets it).
+// barrier counter must be zero (the step resets it before the launch).
 static uint64_t enqueue_solve(Sim& S, cudaStream_t s, const Dev* jobs, uint32_t n_jobs, bool fp64, Prof* prof, uint32_t ctas) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ctas);
@@ -449,8 +449,6 @@ static uint64_t enqueue_solve(Sim& S, cudaStream_t s, const Dev* jobs, uint32_t 
     if (prof) prof->mark(fp64 ? "k_solve<true>" : "k_solve<false>", s);
     return 1;
 }
-
-enum { PART_PRE = 1, PART_POST = 2, PART_FULL = 3 };
 
 // Launch grids sized to the scene. The per-cell, per-block and solver kernels loop over their
 // work, so any grid gives the same results, bit for bit; a scene of a few hundred blocks gets as
@@ -478,9 +476,8 @@ static uint32_t size_class_of(uint32_t n_blocks) {
     return c;
 }
 
-// The step on stream `s`: the part before the pressure solve (PART_PRE), the part after it
-// (PART_POST), or both with the solve between (PART_FULL).
-static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_air, bool fp64, Prof* prof, int part = PART_FULL) {
+// One step on stream `s`, with the side streams forked from and joined back into it.
+static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_air, bool fp64, Prof* prof) {
     Dev& D = S.D;
     uint64_t n = 0;
     const Grids grids = launch_grids(S);
@@ -512,8 +509,7 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
         n++;                                            \
         if (prof) prof->mark(#kern, a);                 \
     } while (0)
-    if (prof && (part & PART_PRE)) prof->mark("start", s);
-    if (part & PART_PRE) {
+    if (prof) prof->mark("start", s);
     L(k_begin_step, 1, 32, D);
     // The side stream clears the last step's sums while the blocks are found and the particles
     // sorted; it then splats the rubber and carries the air (which need the block set but touch
@@ -564,9 +560,7 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     L(k_bullet_apply, G_cell, 256, D);
     // The pressure solve's grid barrier counter starts from zero.
     cudaMemsetAsync(&D.st->bar_count, 0, 4, s);
-    }
-    if (part == PART_FULL) n += enqueue_solve(S, s, nullptr, 1u, fp64, prof, grids.solve);
-    if (part & PART_POST) {
+    n += enqueue_solve(S, s, nullptr, 1u, fp64, prof, grids.solve);
     L(k_project, G_cell, 256, D);
     L(k_extend_1, G_cell, 256, D);
     L(k_extend_2, G_cell, 256, D);
@@ -620,17 +614,16 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     L(k_spray_scan, 1, 1024, D);
     L(k_spray_emit, G_cell, 256, D);
     L(k_spray_commit, 1, 32, D);
-    }
 #undef L
 #undef LA
     return n;
 }
 
-// The step (or a part of it, for a batch) captured as a graph, cached by its shape.
-static ntr_status get_graph(Sim& S, StepGraph*& out, int part = 3) {
+// The step captured as a graph, cached by its shape.
+static ntr_status get_graph(Sim& S, StepGraph*& out) {
     // The size class follows the block count the last read-back saw.
     if (S.h_state) S.size_class = size_class_of(std::max(S.h_state->s.n_blocks, S.h_state->s.n_blocks_prev));
-    GraphKey key{part == 1 ? 0u : S.host.h.substeps, part == 1 ? 0u : S.host.h.air_substeps, S.fp64, (uint32_t)part, S.size_class};
+    GraphKey key{S.host.h.substeps, S.host.h.air_substeps, S.fp64, S.size_class};
     auto it = S.graphs.find(key);
     if (it != S.graphs.end()) {
         out = &it->second;
@@ -646,7 +639,7 @@ static ntr_status get_graph(Sim& S, StepGraph*& out, int part = 3) {
     StepGraph g;
     S.launch_err = cudaSuccess;
     CU(cudaStreamBeginCapture(S.stream, cudaStreamCaptureModeThreadLocal));
-    g.launches = enqueue_step(S, S.stream, key.n_mem, key.n_air, key.fp64 != 0, nullptr, part);
+    g.launches = enqueue_step(S, S.stream, key.n_mem, key.n_air, key.fp64 != 0, nullptr);
     cudaError_t le = cudaGetLastError();
     cudaError_t ce = cudaStreamEndCapture(S.stream, &g.graph);
     if (S.launch_err != cudaSuccess) le = S.launch_err;
