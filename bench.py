@@ -394,7 +394,8 @@ def batch_and_serve(args) -> dict:
                         f"{args.batch_steps} steps each, dt 2 us, FP64 solver sums",
             "scenes_per_s": b["scenes_per_s"], "particle_steps_per_s": b["particle_steps_per_s"], "seconds": b["seconds"],
             "sequential_scenes_per_s": q["scenes_per_s"], "sequential_seconds": q["seconds"],
-            "speedup_vs_sequential": q["seconds"] / b["seconds"], "chunk": args.batch_chunk}
+            "speedup_vs_sequential": q["seconds"] / b["seconds"], "chunk": args.batch_chunk, "calls": b["calls"],
+            "graph_captures": b["graph_captures"], "graph_instantiations": b["graph_instantiations"]}
     if args.serve_requests:
         from natray_b200 import build_world
         ps = sv.mixed_scenes(args.serve_requests, 11, lo=16_000, hi=2_000_000, lognormal_median=128_000)

@@ -458,10 +458,11 @@ NTR_API ntr_status ntr_sim_autotune(ntr_sim* s, uint32_t steps, ntr_tuning* best
  * No counterpart in the reference (it runs one Sim at a time, src/sim.rs:149-205): a serving
  * engine for many scenes of uneven size on one GPU. Each admitted scene keeps its state on the
  * device in its own slot. ntr_batch_step advances every unfinished scene by n steps: per step
- * each scene's work before and after the pressure solve runs on its own stream, overlapping
- * the others', and the pressure systems of all of them are solved by ONE cooperative launch
- * that splits the GPU over them. A scene's results are bit for bit those of the same scene run
- * alone with ntr_sim_step(n) calls of the same n.
+ * one launch per kernel covers every scene (each its own range of CTAs, sized to it), and the
+ * pressure systems of all of them are solved by ONE cooperative launch that splits the GPU
+ * over them; the step is a CUDA graph, captured again only when the set of scenes or their
+ * size classes change. A scene's results are bit for bit those of the same scene run alone
+ * with ntr_sim_step(n) calls of the same n.
  *
  *   ntr_batch_create  max_scenes (at most NTR_BATCH_MAX) slots; hbm_budget bytes the batch may
  *                     hold on the device (0: no limit but the free memory)
@@ -485,11 +486,15 @@ typedef struct {
     ntr_state state;
 } ntr_batch_slot;
 typedef struct {
-    uint32_t max_scenes, in_use, active, pad;
+    uint32_t max_scenes, in_use, active;
+    uint32_t captures;     /* step graphs captured (for a new set of scenes or shapes) */
     uint64_t held_bytes;   /* device memory the slots hold (a slot keeps its region for its next scene) */
     uint64_t budget_bytes;
     uint64_t free_bytes;   /* free device memory now */
     uint64_t steps;        /* batch steps taken */
+    uint32_t instantiations; /* of the captures, those that needed a new executable graph (the
+                                others updated the last one in place) */
+    uint32_t pad;
 } ntr_batch_info;
 NTR_API ntr_status ntr_batch_create(int device, uint32_t max_scenes, uint64_t hbm_budget, ntr_batch** out);
 NTR_API ntr_status ntr_batch_destroy(ntr_batch* b);

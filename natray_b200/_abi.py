@@ -119,9 +119,9 @@ class BatchSlot(C.Structure):
 
 
 class BatchInfo(C.Structure):
-    _fields_ = [("max_scenes", C.c_uint32), ("in_use", C.c_uint32), ("active", C.c_uint32), ("pad", C.c_uint32),
+    _fields_ = [("max_scenes", C.c_uint32), ("in_use", C.c_uint32), ("active", C.c_uint32), ("captures", C.c_uint32),
                 ("held_bytes", C.c_uint64), ("budget_bytes", C.c_uint64), ("free_bytes", C.c_uint64),
-                ("steps", C.c_uint64)]
+                ("steps", C.c_uint64), ("instantiations", C.c_uint32), ("pad", C.c_uint32)]
 
 
 MAX_SHOTS = 4

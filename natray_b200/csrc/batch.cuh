@@ -10,9 +10,11 @@
 // for the batch's current scenes and shapes and replayed per step; scenes differ in their
 // rubber and air substep counts (each scene's kernels skip the substeps past its own) and in
 // how many steps they take in a call (each scene's step budget stops it, as a stop time would).
-// The host reads the scenes' states back once per ntr_batch_step call and adapts each one's
-// solver iterations and substeps as ntr_sim_step does, so a scene's results are those of the
-// scene run alone with the same chunks of steps.
+// A call moves its host data in one copy each way: the pointer tables, grid prefixes, each
+// scene's parameters and step budget go up together (k_batch_begin puts the parameters and
+// budgets in place), and k_batch_end gathers the scenes' states into one buffer that comes
+// back. The host then adapts each scene's solver iterations and substeps as ntr_sim_step does,
+// so a scene's results are those of the scene run alone with the same chunks of steps.
 //
 // Included at the end of sim.cu (it uses the Sim internals there).
 #pragma once
@@ -25,6 +27,44 @@ namespace ntr {
 // The kinds of per-scene grids a step's launches use (enqueue_step's grid expressions).
 enum GridKind { GK_ONE, GK_CELL, GK_WORDS, GK_MARK, GK_SCAN, GK_TILES, GK_RSCAN, GK_BOUNDS, GK_BLK, GK_SHOTS, GK_PATCH,
                 GK_VERT, GK_VERT4, GK_TRI, GK_COUNT };
+
+// A scene's parameters for a batch call (Sim::run sets the same before a one-scene call).
+struct BatchJobIn {
+    ntr_gpu_params U;
+    uint32_t budget, pad[3];
+};
+
+// Each scene's parameters and step budget into place, and its solver counters of the call
+// (iters_max, unconverged) cleared: one CTA a scene.
+__global__ void k_batch_begin(const Dev* __restrict__ jobs, const BatchJobIn* __restrict__ in) {
+    const Dev& D = jobs[blockIdx.x];
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&in[blockIdx.x].U);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(const_cast<ntr_gpu_params*>(D.U));
+    for (uint32_t t = threadIdx.x; t < sizeof(ntr_gpu_params) / 4; t += blockDim.x) dst[t] = src[t];
+    if (threadIdx.x == 0) {
+        D.st->step_budget = in[blockIdx.x].budget;
+        D.st->s.iters_max = 0u;
+        D.st->s.unconverged = 0u;
+    }
+}
+
+// After a call's steps: a scene parked for the end of the call gets its last step length back
+// (its state is then what its own last step left, as after ntr_sim_step of its steps), its
+// budget goes back to no limit, and its state is gathered into out[scene].
+__global__ void k_batch_end(const Dev* __restrict__ jobs, DevState* __restrict__ out) {
+    DevState* st = jobs[blockIdx.x].st;
+    if (threadIdx.x == 0) {
+        if (st->parked) {
+            st->s.dt_ns = st->parked_dt;
+            st->parked = 0u;
+        }
+        st->step_budget = 0xFFFFFFFFu;
+    }
+    __syncthreads();
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(st);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(out + blockIdx.x);
+    for (uint32_t t = threadIdx.x; t < sizeof(DevState) / 4; t += blockDim.x) dst[t] = src[t];
+}
 
 struct BatchSlot {
     std::unique_ptr<Sim> sim;
@@ -49,9 +89,21 @@ struct Batch {
     cudaStream_t aux = nullptr, aux2 = nullptr;  // its side streams (as a one-scene step's)
     cudaEvent_t ev_fork[3] = {nullptr, nullptr, nullptr}, ev_join[3] = {nullptr, nullptr, nullptr};
     std::vector<cudaEvent_t> ev_sub;
-    Dev* d_jobs = nullptr;  // the pointer tables of the scenes in the current step's order
-    uint32_t* d_first = nullptr;  // per kind of grid, the scenes' first CTAs (GK_COUNT x (max_scenes + 1))
+    // What a call sends up, in one buffer on each side (pinned on the host): the pointer tables
+    // of the scenes in the current step's order, per kind of grid the scenes' first CTAs
+    // (GK_COUNT x (max_scenes + 1)), and each scene's parameters; and what comes back: the
+    // scenes' states.
+    uint8_t* d_stage = nullptr;
+    uint8_t* h_stage = nullptr;
+    size_t off_first = 0, off_in = 0, stage_bytes = 0;
+    Dev* d_jobs = nullptr;
+    uint32_t* d_first = nullptr;
+    BatchJobIn* d_in = nullptr;
+    DevState* d_out = nullptr;
+    DevState* h_out = nullptr;
     uint32_t n_jobs_cap = 0;
+    uint32_t captures = 0;        // step graphs captured (a new set of scenes or shapes)
+    uint32_t instantiations = 0;  // of them, those that needed a new executable graph
     // The captured step of the current scenes and shapes, and what it was captured for.
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -81,14 +133,16 @@ struct Batch {
             if (e) cudaEventDestroy(e);
         if (aux) cudaStreamDestroy(aux);
         if (aux2) cudaStreamDestroy(aux2);
-        if (d_first) cudaFree(d_first);
         for (auto& s : slots) {
             s.sim.reset();
             if (s.arena) cudaFree(s.arena);
             if (s.h_state) cudaFreeHost(s.h_state);
         }
         slots.clear();
-        if (d_jobs) cudaFree(d_jobs);
+        if (d_stage) cudaFree(d_stage);
+        if (h_stage) cudaFreeHost(h_stage);
+        if (d_out) cudaFree(d_out);
+        if (h_out) cudaFreeHost(h_out);
         if (solve_stream) cudaStreamDestroy(solve_stream);
     }
 };
@@ -136,8 +190,17 @@ static ntr_status batch_create(int device, uint32_t max_scenes, uint64_t budget,
     for (auto& s : B->slots) {
         CU(cudaMallocHost((void**)&s.h_state, sizeof(DevState)));
     }
-    CU(cudaMalloc((void**)&B->d_jobs, sizeof(Dev) * max_scenes));
-    CU(cudaMalloc((void**)&B->d_first, sizeof(uint32_t) * GK_COUNT * (max_scenes + 1)));
+    auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    B->off_first = up16(sizeof(Dev) * max_scenes);
+    B->off_in = up16(B->off_first + sizeof(uint32_t) * GK_COUNT * (max_scenes + 1));
+    B->stage_bytes = B->off_in + sizeof(BatchJobIn) * max_scenes;
+    CU(cudaMalloc((void**)&B->d_stage, B->stage_bytes));
+    CU(cudaMallocHost((void**)&B->h_stage, B->stage_bytes));
+    B->d_jobs = reinterpret_cast<Dev*>(B->d_stage);
+    B->d_first = reinterpret_cast<uint32_t*>(B->d_stage + B->off_first);
+    B->d_in = reinterpret_cast<BatchJobIn*>(B->d_stage + B->off_in);
+    CU(cudaMalloc((void**)&B->d_out, sizeof(DevState) * max_scenes));
+    CU(cudaMallocHost((void**)&B->h_out, sizeof(DevState) * max_scenes));
     B->n_jobs_cap = max_scenes;
     out = B.release();
     return NTR_OK;
@@ -323,10 +386,13 @@ static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active, Prof* prof 
     if (order.empty() || n == 0) return NTR_OK;
     const uint32_t n_jobs = (uint32_t)order.size();
     cudaStream_t s = B.solve_stream;
-    // Each scene's parameters for this call (Sim::run) and its step budget, then the pointer
-    // tables and the grids of the scenes in order.
-    std::vector<Dev> jobs(n_jobs);
-    std::vector<uint32_t> first((size_t)GK_COUNT * (B.max_scenes + 1), 0u), tot(GK_COUNT, 0u);
+    // Each scene's parameters for this call (Sim::run) and its step budget, the pointer tables
+    // and the grids of the scenes in order, staged in the pinned buffer and sent in one copy.
+    Dev* jobs = reinterpret_cast<Dev*>(B.h_stage);
+    uint32_t* first = reinterpret_cast<uint32_t*>(B.h_stage + B.off_first);
+    BatchJobIn* in = reinterpret_cast<BatchJobIn*>(B.h_stage + B.off_in);
+    std::fill(first, first + (size_t)GK_COUNT * (B.max_scenes + 1), 0u);
+    uint32_t tot[GK_COUNT] = {};
     std::vector<uint32_t> key;
     uint32_t fp64 = B.slots[order[0]].sim->fp64, max_shots = 1, n_mem = 0, n_air = 0, steps = 0;
     for (uint32_t j = 0; j < n_jobs; j++) {
@@ -337,9 +403,8 @@ static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active, Prof* prof 
         S.U.limits[3] = 0xFFFFFFFFu;
         S.U.mem[1] = h.substeps;
         S.U.mem[2] = h.air_substeps;
-        CU(cudaMemcpyAsync((void*)S.D.U, &S.U, sizeof(ntr_gpu_params), cudaMemcpyHostToDevice, s));
-        CU(cudaMemsetAsync(&S.D.st->s.iters_max, 0, 8, s));
-        CU(cudaMemcpyAsync(&S.D.st->step_budget, &todo[order[j]], 4, cudaMemcpyHostToDevice, s));
+        in[j].U = S.U;
+        in[j].budget = todo[order[j]];
         S.size_class = size_class_of(std::max(S.h_state->s.n_blocks, S.h_state->s.n_blocks_prev));
         jobs[j] = S.D;
         uint32_t g[GK_COUNT];
@@ -357,33 +422,50 @@ static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active, Prof* prof 
     }
     for (int k = 0; k < GK_COUNT; k++) first[(size_t)k * (B.max_scenes + 1) + n_jobs] = tot[k];
     key.insert(key.end(), {n_jobs, fp64, max_shots, n_mem, n_air});
-    CU(cudaMemcpyAsync(B.d_jobs, jobs.data(), sizeof(Dev) * n_jobs, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(B.d_first, first.data(), sizeof(uint32_t) * first.size(), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(B.d_stage, B.h_stage, B.off_in + sizeof(BatchJobIn) * n_jobs, cudaMemcpyHostToDevice, s));
+    k_batch_begin<<<n_jobs, 64, 0, s>>>(B.d_jobs, B.d_in);
+    CU(cudaGetLastError());
     // The step graph of these scenes and shapes (captured again when they change).
     Sim& S0 = *B.slots[order[0]].sim;
     if (!prof && (!B.exec || key != B.graph_key)) {
-        if (B.exec) cudaGraphExecDestroy(B.exec), B.exec = nullptr;
         if (B.graph) cudaGraphDestroy(B.graph), B.graph = nullptr;
-        CU(cudaStreamSynchronize(s));
         S0.launch_err = cudaSuccess;
         CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        enqueue_step_multi(B, n_jobs, tot.data(), max_shots, n_mem, n_air, fp64 != 0, S0);
+        enqueue_step_multi(B, n_jobs, tot, max_shots, n_mem, n_air, fp64 != 0, S0);
         cudaError_t le = cudaGetLastError();
         cudaError_t ce = cudaStreamEndCapture(s, &B.graph);
         if (S0.launch_err != cudaSuccess) le = S0.launch_err;
         if (le != cudaSuccess) {
             if (B.graph) cudaGraphDestroy(B.graph), B.graph = nullptr;
+            if (B.exec) cudaGraphExecDestroy(B.exec), B.exec = nullptr;
             return fail(NTR_E_CUDA, std::string("kernel launch during capture: ") + cudaGetErrorString(le));
         }
-        if (ce != cudaSuccess) return fail(NTR_E_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce));
-        CU(cudaGraphInstantiate(&B.exec, B.graph, 0));
+        if (ce != cudaSuccess) {
+            if (B.exec) cudaGraphExecDestroy(B.exec), B.exec = nullptr;
+            return fail(NTR_E_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(ce));
+        }
+        // Most changes are only of grid sizes (a scene's size class): the executable graph
+        // takes the new launch shapes in place. A changed sequence (substep counts, an empty
+        // grid) needs a new one.
+        bool updated = false;
+        if (B.exec) {
+            cudaGraphExecUpdateResultInfo info;
+            updated = cudaGraphExecUpdate(B.exec, B.graph, &info) == cudaSuccess;
+            if (!updated) {
+                cudaGetLastError();
+                cudaGraphExecDestroy(B.exec), B.exec = nullptr;
+            }
+        }
+        if (!updated) CU(cudaGraphInstantiate(&B.exec, B.graph, 0));
         B.graph_key = key;
+        B.captures++;
+        B.instantiations += updated ? 0u : 1u;
     }
     std::vector<uint32_t> before(n_jobs);
     for (uint32_t j = 0; j < n_jobs; j++) before[j] = B.slots[order[j]].sim->h_state->s.step;
     if (prof) {
         S0.launch_err = cudaSuccess;
-        for (uint32_t k = 0; k < steps; k++) enqueue_step_multi(B, n_jobs, tot.data(), max_shots, n_mem, n_air, fp64 != 0, S0, prof);
+        for (uint32_t k = 0; k < steps; k++) enqueue_step_multi(B, n_jobs, tot, max_shots, n_mem, n_air, fp64 != 0, S0, prof);
         CU(cudaGetLastError());
         CU(S0.launch_err);
         CU(prof->err);
@@ -391,24 +473,17 @@ static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active, Prof* prof 
         for (uint32_t k = 0; k < steps; k++) CU(cudaGraphLaunch(B.exec, s));
     }
     B.steps += steps;
-    // States back, then the host control of each scene (Sim::run).
-    for (uint32_t j = 0; j < n_jobs; j++) {
-        Sim& S = *B.slots[order[j]].sim;
-        CU(cudaMemcpyAsync(S.h_state, S.D.st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
-    }
+    // The states back in one copy (parked scenes' step lengths restored, budgets back to no
+    // limit on the device), then the host control of each scene (Sim::run).
+    k_batch_end<<<n_jobs, 64, 0, s>>>(B.d_jobs, B.d_out);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(B.h_out, B.d_out, sizeof(DevState) * n_jobs, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     ntr_status first_err = NTR_OK;
     for (uint32_t j = 0; j < n_jobs; j++) {
         BatchSlot& sl = B.slots[order[j]];
         Sim& S = *sl.sim;
-        // A scene parked for the end of the call gets its last step length back: its state is
-        // what its own last step left, as after ntr_sim_step of its steps.
-        if (S.h_state->parked) {
-            S.h_state->s.dt_ns = S.h_state->parked_dt;
-            S.h_state->parked = 0u;
-            CU(cudaMemcpyAsync(&S.D.st->s.dt_ns, &S.h_state->s.dt_ns, 4, cudaMemcpyHostToDevice, s));
-            CU(cudaMemcpyAsync(&S.D.st->parked, &S.h_state->parked, 4, cudaMemcpyHostToDevice, s));
-        }
+        *S.h_state = B.h_out[j];
         const ntr_state& st = S.h_state->s;
         sl.done += st.step - before[j];
         if (st.overflow && first_err == NTR_OK)
@@ -416,13 +491,6 @@ static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active, Prof* prof 
         if (S.h_state->err && first_err == NTR_OK) first_err = fail(NTR_E_TIMEOUT, "a bounded device-side wait gave up");
         if (!st.overflow && !S.h_state->err) adapt_after_batch(S.host.h, st);
     }
-    // Each scene's budget back to no limit, for its own calls.
-    const uint32_t unlimited = 0xFFFFFFFFu;
-    for (uint32_t j = 0; j < n_jobs; j++) {
-        Sim& S = *B.slots[order[j]].sim;
-        CU(cudaMemcpyAsync(&S.D.st->step_budget, &unlimited, 4, cudaMemcpyHostToDevice, s));
-    }
-    CU(cudaStreamSynchronize(s));
     return first_err;
 }
 

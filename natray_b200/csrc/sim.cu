@@ -1459,6 +1459,7 @@ NTR_API ntr_status ntr_batch_info_get(ntr_batch* batch, ntr_batch_info* out) {
             if (sl.done < sl.target) out->active++;
         }
     out->held_bytes = B.held, out->budget_bytes = B.budget, out->steps = B.steps;
+    out->captures = B.captures, out->instantiations = B.instantiations;
     size_t f = 0, t = 0;
     if (cudaMemGetInfo(&f, &t) == cudaSuccess) out->free_bytes = f;
     return NTR_OK;

@@ -61,12 +61,15 @@ def run_batched(worlds: list[World], steps: int, chunk: int = 4, max_scenes: int
         if None in slots:
             raise RuntimeError("the batch could not hold every scene")
         t0 = time.perf_counter()
+        calls = 0
         while b.step(chunk):
-            pass
+            calls += 1
         wall = time.perf_counter() - t0
         done = [b.poll(s)["steps_done"] for s in slots]
+        info = b.info()
     n_ps = sum(w.h.n_particles * d for w, d in zip(worlds, done))
-    return {"seconds": wall, "scenes_per_s": len(worlds) / wall, "particle_steps_per_s": n_ps / wall}
+    return {"seconds": wall, "scenes_per_s": len(worlds) / wall, "particle_steps_per_s": n_ps / wall, "calls": calls,
+            "graph_captures": info["captures"], "graph_instantiations": info["instantiations"]}
 
 
 def run_sequential(worlds, steps: int, chunk: int = 4, build=None) -> dict:

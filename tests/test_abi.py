@@ -56,7 +56,7 @@ def test_no_silent_cpu_fallback():
 
 def test_batch_structs_and_null_handles():
     assert C.sizeof(_abi.BatchSlot) == 24 + 96
-    assert C.sizeof(_abi.BatchInfo) == 48
+    assert C.sizeof(_abi.BatchInfo) == 56
     for name, args in [("ntr_batch_step", (None, 1, None)), ("ntr_batch_retire", (None, 0)),
                        ("ntr_batch_info_get", (None, None))]:
         assert getattr(lib(), name)(*args) == 1  # NTR_E_INVALID

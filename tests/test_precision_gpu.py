@@ -1,43 +1,46 @@
-"""The precision study of the 1M configuration, scaled down to a scene the all-FP64 oracle
-runs in seconds: the product (FP32 state, FP64 solver sums, on the GPU) against the oracle with
-every real in FP64, from the same start, relative L2 errors at checkpoints through the impact.
+"""The precision study of the 1M-particle scene (976,915 particles, a level-6 membrane, an 8 mm
+sphere at 350 m/s): the product (FP32 state and grid arithmetic, FP64 solver sums, on the GPU)
+against the oracle with every real in FP64, from the same start, relative L2 errors of positions,
+velocities, particle pressure, membrane positions and the membrane's major principal stretch.
 
-Positions stay within 1e-4 of FP64. Before the impact the velocity fields agree to the pressure
-solve's tolerance (its relative residual of 1e-5 leaves differences near 1e-3); after it they
-differ where a triangle tears a substep earlier or later on one side, a discrete event, so the
-velocity bound is only checked before the impact. Run with -s to see the table."""
-import numpy as np
+The bounds are the measured errors (tests/precision_study.py, 1000 steps at solver tolerances
+1e-5 and 1e-7 alike) with a margin of three to five:
+
+- before the sphere reaches the membrane (step 70), and in the same scene with the sphere at
+  1 m/s (it never arrives): positions within 2e-7 (measured 5e-8), membrane positions within
+  3e-6 (6e-7), velocities and pressure within 3e-3 (8e-4 and 6e-4: the same at the tight
+  tolerance, so FP32 rounding and not the solver's stopping point), stretch within 1e-3 (2e-4);
+- after it the membrane tears at different substeps and triangles on the two sides, a discrete
+  event (12 torn triangles against 13 at step 80), and the velocity and pressure fields differ
+  where it does (0.33 and 0.43 at step 80, 0.14 and 0.06 at step 100); positions stay within
+  1e-4 (1.4e-5 at step 100), membrane positions within 5e-4 (5e-5), stretch within 3e-2 (4.5e-3)
+  and the torn counts within a quarter of each other.
+
+Run with -s to see the tables."""
 import pytest
 
-from natray_b200 import Params, World, build_world
-from natray_b200.sim import Sim
-from oracle.py import Oracle
+from precision_study import study
 
 pytestmark = pytest.mark.gpu
 
 
-def rel(x, y):
-    x, y = np.asarray(x, np.float64), np.asarray(y, np.float64)
-    return float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-30))
+def test_fp32_product_tracks_fp64_through_the_impact(oracle_threads):
+    rows = study(124, 100, 20, 1e-5)
+    for r in rows:
+        if r["step"] <= 60:
+            assert r["torn"] == [0, 0]
+            assert r["x"] < 2e-7 and r["mem_x"] < 3e-6, r
+            assert r["v"] < 3e-3 and r["p"] < 3e-3 and r["stretch"] < 1e-3, r
+        else:
+            assert r["x"] < 1e-4 and r["mem_x"] < 5e-4 and r["stretch"] < 3e-2, r
+            a, b = r["torn"]
+            assert abs(a - b) <= max(3, 0.25 * max(a, b)), r
+    assert rows[-1]["torn"][0] > 0  # the step range covers the impact
 
 
-def test_fp32_product_tracks_fp64(oracle_threads):
-    w0 = build_world(Params(resolution=40, mesh_level=4, block_cap=8192, spray_cap=200000, dt_max=2e-6, bullet=6,
-                            caliber=8, bullet_speed=350))
-    w = World(Oracle(w0.blob).snapshot())  # the measuring substep on the CPU: both start alike
-    sim, ref = Sim(world=w), Oracle(w.blob, real64=True)
-    print(f"\n{w.h.n_particles} particles; relative L2 against FP64")
-    print(" step   t (us)      x          v          p        membrane   torn (product, FP64)")
-    for k in range(4):
-        sim.step(25)
-        ref.step(25)
-        a, b = sim.snapshot(), World(ref.snapshot())
-        pa, pb = a.particles, b.particles
-        ex, ev, ep = rel(pa[:, :3], pb[:, :3]), rel(pa[:, 4:7], pb[:, 4:7]), rel(pa[:, 11], pb[:, 11])
-        em = rel(a.sec("MEM_X")[:, :3], b.sec("MEM_X")[:, :3])
-        torn = (int((a.sec("ALIVE") == 0).sum()), int((b.sec("ALIVE") == 0).sum()))
-        print(f" {25 * (k + 1):4d} {a.state['t_ns'] * 1e-3:8.1f}  {ex:.2e}  {ev:.2e}  {ep:.2e}  {em:.2e}  {torn}")
-        assert ex < 1e-4 and em < 1e-3
-        if torn == (0, 0):
-            assert ev < 1e-2
-    sim.close()
+def test_fp32_product_tracks_fp64_at_rest(oracle_threads):
+    rows = study(124, 200, 100, 1e-5, speed=1.0)
+    for r in rows:
+        assert r["torn"] == [0, 0]
+        assert r["x"] < 1e-6 and r["mem_x"] < 1e-5, r
+        assert r["v"] < 3e-3 and r["p"] < 5e-3 and r["stretch"] < 1e-3, r
