@@ -136,16 +136,38 @@ __global__ void k_air_carry_m(Multi M) {
 }
 
 // ---- mem_splat, membrane.wgsl:182-217 -------------------------------------------------------------
+// Sums of runs of equal keys among the lanes of a warp: the lanes of a run (consecutive lanes
+// with the same key) hold their run's sum in its last lane, which `last` tells. Every lane takes
+// part; the shuffles are uniform (a segmented scan over the run boundaries from a ballot).
+struct WarpRuns {
+    uint32_t start;  // first lane of this lane's run
+    bool last;       // this lane ends its run
+    __device__ __forceinline__ WarpRuns(uint32_t key, uint32_t lane) {
+        const uint32_t prev = __shfl_up_sync(0xffffffffu, key, 1), next = __shfl_down_sync(0xffffffffu, key, 1);
+        const uint32_t heads = __ballot_sync(0xffffffffu, lane == 0 || prev != key);
+        start = 31u - __clz(heads & (0xffffffffu >> (31u - lane)));
+        last = lane == 31 || next != key;
+    }
+    __device__ __forceinline__ int32_t sum(int32_t x, uint32_t lane) const {
+#pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+            const int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= start + o) x += y;
+        }
+        return x;
+    }
+};
+
+// The rubber's splat: per vertex its area-weighted velocity into its own
+// cell, and where it touches water its push and area over the 27 cells around it. Vertices are
+// in the mesh's spatial order, so neighbouring lanes of a warp mostly add to the same cells: each
+// run of lanes with one target cell sums its i32 terms across the lanes and its last lane adds
+// the sums with one atomic each. Integer sums: the same as an atomic per term, in any grouping.
 template <class CT>
 __device__ __forceinline__ void mem_splat_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
     const Grid g = grid_of(D, cur_of(st));
-    // Every lane of the warp takes part in the merges below (a lane without a vertex adds
-    // nothing): vertices are in the mesh's spatial order, so the lanes of a warp mostly add to the
-    // same cells, and the lanes of each target cell sum their i32 terms (a match, then a reduction
-    // over the matching lanes) before one of them adds the sum with one atomic. Integer sums:
-    // the same as an atomic per term.
     const uint32_t i = C.x() * blockDim.x + threadIdx.x;
     const uint32_t lane = threadIdx.x & 31u;
     bool valid = i < D.Nv && D.mem_mass[i] != 0.0f;
@@ -156,22 +178,22 @@ __device__ __forceinline__ void mem_splat_body(const Dev& D, const CT& C) {
         valid = pa.y > 0.0f;
         x4 = D.mem_x[0][i];
     }
-    uint32_t own = valid ? cell_at(g, own_cell(g, xyz(x4))) : NONE;
+    if (!__any_sync(0xffffffffu, valid)) return;  // warp-uniform
+    const uint32_t own = valid ? cell_at(g, own_cell(g, xyz(x4))) : NONE;
     {
-        const uint32_t peers = __match_any_sync(0xffffffffu, own);
+        const WarpRuns r(own, lane);
+        int32_t vw = 0, vx = 0, vy = 0, vz = 0;
         if (own != NONE) {
             const float a = pa.y * 1e6f;
             const float4 mv = D.mem_v[0][i];
-            const int32_t vw = __reduce_add_sync(peers, to_fp(a, FP_A));
-            const int32_t vx = __reduce_add_sync(peers, to_fp(a * mv.x, FP_A));
-            const int32_t vy = __reduce_add_sync(peers, to_fp(a * mv.y, FP_A));
-            const int32_t vz = __reduce_add_sync(peers, to_fp(a * mv.z, FP_A));
-            if ((uint32_t)(__ffs(peers) - 1) == lane) {
-                atomicAdd(accp(D, A_MW, own), vw);
-                atomicAdd(accp(D, A_MV + 0, own), vx);
-                atomicAdd(accp(D, A_MV + 1, own), vy);
-                atomicAdd(accp(D, A_MV + 2, own), vz);
-            }
+            vw = to_fp(a, FP_A), vx = to_fp(a * mv.x, FP_A), vy = to_fp(a * mv.y, FP_A), vz = to_fp(a * mv.z, FP_A);
+        }
+        vw = r.sum(vw, lane), vx = r.sum(vx, lane), vy = r.sum(vy, lane), vz = r.sum(vz, lane);
+        if (r.last && own != NONE) {
+            atomicAdd(accp(D, A_MW, own), vw);
+            atomicAdd(accp(D, A_MV + 0, own), vx);
+            atomicAdd(accp(D, A_MV + 1, own), vy);
+            atomicAdd(accp(D, A_MV + 2, own), vz);
         }
     }
     const bool on_water = valid && D.mem_water[i].w >= CONTACT_F;
@@ -188,12 +210,14 @@ __device__ __forceinline__ void mem_splat_body(const Dev& D, const CT& C) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 const uint32_t cell = on_water ? sc.cell(a, b, c) : NONE;
-                const uint32_t peers = __match_any_sync(0xffffffffu, cell);
-                if (cell == NONE) continue;
-                const float w = wx[a] * wy[b] * wz[c];
-                const int32_t sf = __reduce_add_sync(peers, to_fp(w * pa.x, FP_F));
-                const int32_t sa = __reduce_add_sync(peers, to_fp(w * pa.y * 1e6f, FP_A));
-                if ((uint32_t)(__ffs(peers) - 1) == lane) {
+                const WarpRuns r(cell, lane);
+                int32_t sf = 0, sa = 0;
+                if (cell != NONE) {
+                    const float w = wx[a] * wy[b] * wz[c];
+                    sf = to_fp(w * pa.x, FP_F), sa = to_fp(w * pa.y * 1e6f, FP_A);
+                }
+                sf = r.sum(sf, lane), sa = r.sum(sa, lane);
+                if (r.last && cell != NONE) {
                     atomicAdd(accp(D, A_MF, cell), sf);
                     atomicAdd(accp(D, A_MA, cell), sa);
                 }
