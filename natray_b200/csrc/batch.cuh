@@ -74,6 +74,7 @@ struct BatchSlot {
     uint8_t* arena = nullptr;
     size_t arena_cap = 0;
     DevState* h_state = nullptr;
+    SimHandles hs;  // its scenes' streams and events, made at its first scene
 };
 
 struct Batch {
@@ -135,6 +136,7 @@ struct Batch {
         if (aux2) cudaStreamDestroy(aux2);
         for (auto& s : slots) {
             s.sim.reset();
+            free_handles(s.hs);
             if (s.arena) cudaFree(s.arena);
             if (s.h_state) cudaFreeHost(s.h_state);
         }
@@ -164,13 +166,10 @@ static ntr_status batch_create(int device, uint32_t max_scenes, uint64_t budget,
     if (max_scenes == 0 || max_scenes > NTR_BATCH_MAX) return fail(NTR_E_INVALID, "max_scenes is 1.." + std::to_string(NTR_BATCH_MAX));
     DeviceScope scope(device);
     if (!scope.ok) return fail(NTR_E_CUDA, "cudaSetDevice failed");
-    cudaDeviceProp prop;
-    CU(cudaGetDeviceProperties(&prop, device));
-    if (prop.major < 10) return fail(NTR_E_NODEVICE, "this library is built for sm_100a (B200)");
-    int occ_a = 0, occ_b = 0;
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_solve_batch<true>, SOLVE_T, 0));
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_solve_batch<false>, SOLVE_T, 0));
-    const uint32_t ctas = (uint32_t)std::min(256, prop.multiProcessorCount * std::min(occ_a, occ_b));
+    DevFacts f;
+    if ((r = device_facts(device, f)) != NTR_OK) return r;
+    if (f.major < 10) return fail(NTR_E_NODEVICE, "this library is built for sm_100a (B200)");
+    const uint32_t ctas = f.coop_ctas;
     // Every scene needs a CTA of the joint solve.
     if (max_scenes > ctas) return fail(NTR_E_INVALID, "max_scenes is at most " + std::to_string(ctas) + " on this device");
     std::unique_ptr<Batch> B(new Batch);
@@ -225,12 +224,16 @@ static ntr_status batch_admit(Batch& B, const void* blob, size_t len, uint32_t n
     }
     if (fits != NONE) free_slot = fits;
     if (free_slot == NONE) return fail(NTR_E_BUSY, "every slot of the batch is in use");
-    size_t free_b = 0, total_b = 0;
-    CU(cudaMemGetInfo(&free_b, &total_b));
     BatchSlot& sl = B.slots[free_slot];
     const uint64_t grow = need > sl.arena_cap ? need + need / 4 - sl.arena_cap : 0;  // 25 % headroom
     if (B.budget && B.held + grow > B.budget) return fail(NTR_E_BUSY, "the scene's " + std::to_string(need) + " bytes exceed the batch's budget now");
-    if (grow && (uint64_t)free_b < grow + B.reserve) return fail(NTR_E_BUSY, "the scene's " + std::to_string(need) + " bytes do not fit the free device memory now");
+    if (grow) {
+        // The free device memory is asked only when the slot's region must grow (the query
+        // takes milliseconds).
+        size_t free_b = 0, total_b = 0;
+        CU(cudaMemGetInfo(&free_b, &total_b));
+        if ((uint64_t)free_b < grow + B.reserve) return fail(NTR_E_BUSY, "the scene's " + std::to_string(need) + " bytes do not fit the free device memory now");
+    }
     if (grow) {
         if (sl.arena) CU(cudaFree(sl.arena));
         B.held -= sl.arena_cap;
@@ -239,8 +242,12 @@ static ntr_status batch_admit(Batch& B, const void* blob, size_t len, uint32_t n
         sl.arena_cap = need + need / 4;
         B.held += sl.arena_cap;
     }
+    if (!sl.hs.stream && (r = make_handles(sl.hs)) != NTR_OK) {
+        free_handles(sl.hs);
+        return r;
+    }
     Sim* s = nullptr;
-    if ((r = create_from(w, B.device, s, sl.arena, sl.arena_cap, sl.h_state)) != NTR_OK) return r;
+    if ((r = create_from(w, B.device, s, sl.arena, sl.arena_cap, sl.h_state, &sl.hs)) != NTR_OK) return r;
     sl.sim.reset(s);
     sl.target = n_steps;
     sl.done = 0;

@@ -95,6 +95,7 @@ struct Sim {
     uint32_t batch_steps = 0;  // ntr_sim_set_batch_steps: fixed steps per ntr_sim_advance batch (0: by time)
     uint32_t fp64 = 1;
     ntr_tuning tune{0u, 8u, 8u, 0u};  // launch shapes (ntr_sim_set_tuning)
+    bool own_streams = true;  // false: the streams and events are a batch slot's, kept across its scenes
 
     ~Sim() {
         DeviceScope scope(device);
@@ -106,14 +107,15 @@ struct Sim {
         if (stats_mem) cudaFree(stats_mem);
         if (ev_out) cudaEventDestroy(ev_out);
         if (h_state && own_h_state) cudaFreeHost(h_state);
+        for (cudaEvent_t e : ev_sub)
+            if (e) cudaEventDestroy(e);
+        if (!own_streams) return;
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         for (int k = 0; k < 3; k++) {
             if (ev_fork[k]) cudaEventDestroy(ev_fork[k]);
             if (ev_join[k]) cudaEventDestroy(ev_join[k]);
         }
-        for (cudaEvent_t e : ev_sub)
-            if (e) cudaEventDestroy(e);
         if (aux2) cudaStreamDestroy(aux2);
         if (aux) cudaStreamDestroy(aux);
         if (stream) cudaStreamDestroy(stream);
@@ -162,6 +164,46 @@ static ntr_status check_device(int device) {
         return fail(NTR_E_NODEVICE, "no CUDA device available");
     }
     if (device < 0 || device >= n) return fail(NTR_E_INVALID, "device index out of range");
+    return NTR_OK;
+}
+
+// What the library needs to know of a device, asked once per device (cudaGetDeviceProperties
+// takes milliseconds, which a serving loop admitting scenes would pay every time).
+struct DevFacts {
+    int sms = 0, major = 0, minor = 0;
+    uint32_t coop_ctas = 0;  // CTAs of a persistent solve that the device holds at once (at most 256)
+    bool known = false;
+};
+static ntr_status device_facts(int device, DevFacts& out) {
+    static std::mutex mu;
+    static DevFacts cache[64];
+    if (device < 0 || device >= 64) return fail(NTR_E_INVALID, "device index out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    DevFacts& f = cache[device];
+    if (!f.known) {
+        DeviceScope scope(device);
+        if (!scope.ok) return fail(NTR_E_CUDA, "cudaSetDevice failed");
+        CU(cudaDeviceGetAttribute(&f.sms, cudaDevAttrMultiProcessorCount, device));
+        CU(cudaDeviceGetAttribute(&f.major, cudaDevAttrComputeCapabilityMajor, device));
+        CU(cudaDeviceGetAttribute(&f.minor, cudaDevAttrComputeCapabilityMinor, device));
+        if (f.major >= 10) {
+            // The persistent solver's grid must be co-resident: at most what occupancy allows,
+            // for the one-scene and the many-scene solve alike. CTA c owns the blocks c (mod 256)
+            // (and c + G, ... with fewer CTAs): at most 256.
+            int occ = 1 << 30, o = 0;
+            CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_solve<true>, SOLVE_T, 0));
+            occ = std::min(occ, o);
+            CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_solve<false>, SOLVE_T, 0));
+            occ = std::min(occ, o);
+            CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_solve_batch<true>, SOLVE_T, 0));
+            occ = std::min(occ, o);
+            CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_solve_batch<false>, SOLVE_T, 0));
+            occ = std::min(occ, o);
+            f.coop_ctas = (uint32_t)std::min(256, f.sms * occ);
+        }
+        f.known = true;
+    }
+    out = f;
     return NTR_OK;
 }
 
@@ -279,33 +321,33 @@ static ntr_status upload_state(Sim& S, const World& w) {
         for (uint32_t i = 0; i < D.Np; i++)
             for (int k = 0; k < 5; k++) a[k][i] = make_float4(p[20 * (size_t)i + 4 * k], p[20 * (size_t)i + 4 * k + 1], p[20 * (size_t)i + 4 * k + 2], p[20 * (size_t)i + 4 * k + 3]);
         float4* dst[5] = {D.pos, D.vel, D.c0, D.c1, D.c2};
-        for (int k = 0; k < 5; k++) CU(cudaMemcpy(dst[k], a[k].data(), (size_t)D.Np * 16, cudaMemcpyHostToDevice));
+        for (int k = 0; k < 5; k++) CU(cudaMemcpyAsync(dst[k], a[k].data(), (size_t)D.Np * 16, cudaMemcpyHostToDevice, S.stream));
     }
-    CU(cudaMemcpy(D.mem_x[0], w.sec[NTR_SEC_MEM_X].data(), (size_t)D.Nv * 16, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(D.mem_x[1], w.sec[NTR_SEC_MEM_X].data(), (size_t)D.Nv * 16, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(D.mem_v[0], w.sec[NTR_SEC_MEM_V].data(), (size_t)D.Nv * 16, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(D.mem_v[1], w.sec[NTR_SEC_MEM_V].data(), (size_t)D.Nv * 16, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(D.mem_water, w.sec[NTR_SEC_MEM_WATER].data(), (size_t)D.Nv * 16, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(D.mem_layer, w.sec[NTR_SEC_MEM_LAYER].data(), (size_t)D.Nv * 96, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(D.mem_push, w.sec[NTR_SEC_MEM_PUSH].data(), (size_t)D.Nv * 8, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(D.alive, w.sec[NTR_SEC_ALIVE].data(), (size_t)D.Nt * 4, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(D.bullets, w.sec[NTR_SEC_BULLETS].data(), w.sec[NTR_SEC_BULLETS].size(), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(D.sections, w.sec[NTR_SEC_SECTIONS].data(), w.sec[NTR_SEC_SECTIONS].size(), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(D.bullet_hit, w.sec[NTR_SEC_BULLET_HIT].data(), w.sec[NTR_SEC_BULLET_HIT].size(), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(D.pose_log, w.sec[NTR_SEC_POSE_LOG].data(), w.sec[NTR_SEC_POSE_LOG].size(), cudaMemcpyHostToDevice));
-    CU(cudaMemset(D.spray, 0, (size_t)D.spray_cap * 48));
-    CU(cudaMemset(D.landed, 0, (size_t)D.spray_cap * 16));
+    CU(cudaMemcpyAsync(D.mem_x[0], w.sec[NTR_SEC_MEM_X].data(), (size_t)D.Nv * 16, cudaMemcpyHostToDevice, S.stream));
+    CU(cudaMemcpyAsync(D.mem_x[1], w.sec[NTR_SEC_MEM_X].data(), (size_t)D.Nv * 16, cudaMemcpyHostToDevice, S.stream));
+    CU(cudaMemcpyAsync(D.mem_v[0], w.sec[NTR_SEC_MEM_V].data(), (size_t)D.Nv * 16, cudaMemcpyHostToDevice, S.stream));
+    CU(cudaMemcpyAsync(D.mem_v[1], w.sec[NTR_SEC_MEM_V].data(), (size_t)D.Nv * 16, cudaMemcpyHostToDevice, S.stream));
+    CU(cudaMemcpyAsync(D.mem_water, w.sec[NTR_SEC_MEM_WATER].data(), (size_t)D.Nv * 16, cudaMemcpyHostToDevice, S.stream));
+    CU(cudaMemcpyAsync(D.mem_layer, w.sec[NTR_SEC_MEM_LAYER].data(), (size_t)D.Nv * 96, cudaMemcpyHostToDevice, S.stream));
+    CU(cudaMemcpyAsync(D.mem_push, w.sec[NTR_SEC_MEM_PUSH].data(), (size_t)D.Nv * 8, cudaMemcpyHostToDevice, S.stream));
+    CU(cudaMemcpyAsync(D.alive, w.sec[NTR_SEC_ALIVE].data(), (size_t)D.Nt * 4, cudaMemcpyHostToDevice, S.stream));
+    CU(cudaMemcpyAsync(D.bullets, w.sec[NTR_SEC_BULLETS].data(), w.sec[NTR_SEC_BULLETS].size(), cudaMemcpyHostToDevice, S.stream));
+    CU(cudaMemcpyAsync(D.sections, w.sec[NTR_SEC_SECTIONS].data(), w.sec[NTR_SEC_SECTIONS].size(), cudaMemcpyHostToDevice, S.stream));
+    CU(cudaMemcpyAsync(D.bullet_hit, w.sec[NTR_SEC_BULLET_HIT].data(), w.sec[NTR_SEC_BULLET_HIT].size(), cudaMemcpyHostToDevice, S.stream));
+    CU(cudaMemcpyAsync(D.pose_log, w.sec[NTR_SEC_POSE_LOG].data(), w.sec[NTR_SEC_POSE_LOG].size(), cudaMemcpyHostToDevice, S.stream));
+    CU(cudaMemsetAsync(D.spray, 0, (size_t)D.spray_cap * 48, S.stream));
+    CU(cudaMemsetAsync(D.landed, 0, (size_t)D.spray_cap * 16, S.stream));
     if (h.n_spray) {
-        CU(cudaMemcpy(D.spray, w.sec[NTR_SEC_SPRAY].data(), (size_t)h.n_spray * 48, cudaMemcpyHostToDevice));
-        CU(cudaMemcpy(D.landed, w.sec[NTR_SEC_LANDED].data(), (size_t)h.n_spray * 16, cudaMemcpyHostToDevice));
+        CU(cudaMemcpyAsync(D.spray, w.sec[NTR_SEC_SPRAY].data(), (size_t)h.n_spray * 48, cudaMemcpyHostToDevice, S.stream));
+        CU(cudaMemcpyAsync(D.landed, w.sec[NTR_SEC_LANDED].data(), (size_t)h.n_spray * 16, cudaMemcpyHostToDevice, S.stream));
     }
-    CU(cudaMemcpy(D.touch, w.sec[NTR_SEC_TOUCH].data(), (size_t)D.wet_res * D.wet_res * 4, cudaMemcpyHostToDevice));
+    CU(cudaMemcpyAsync(D.touch, w.sec[NTR_SEC_TOUCH].data(), (size_t)D.wet_res * D.wet_res * 4, cudaMemcpyHostToDevice, S.stream));
     // Grid: the last step's blocks become the "current" ones of parity step & 1.
-    CU(cudaMemset(D.acc, 0, (size_t)NTR_ACC_FIELDS * D.cap_cells * 4));
-    CU(cudaMemset(D.cf, 0, (size_t)NTR_CELL_FIELDS * D.cap_cells * 4));
-    CU(cudaMemset(D.air[0], 0, (size_t)NTR_AIR_FIELDS * D.cap_cells * 4));
-    CU(cudaMemset(D.air[1], 0, (size_t)NTR_AIR_FIELDS * D.cap_cells * 4));
-    CU(cudaMemset(D.block_active, 0, (size_t)D.cap_blocks * 4));
+    CU(cudaMemsetAsync(D.acc, 0, (size_t)NTR_ACC_FIELDS * D.cap_cells * 4, S.stream));
+    CU(cudaMemsetAsync(D.cf, 0, (size_t)NTR_CELL_FIELDS * D.cap_cells * 4, S.stream));
+    CU(cudaMemsetAsync(D.air[0], 0, (size_t)NTR_AIR_FIELDS * D.cap_cells * 4, S.stream));
+    CU(cudaMemsetAsync(D.air[1], 0, (size_t)NTR_AIR_FIELDS * D.cap_cells * 4, S.stream));
+    CU(cudaMemsetAsync(D.block_active, 0, (size_t)D.cap_blocks * 4, S.stream));
     const int cur = (int)(h.state.step & 1u);
     const uint32_t nbp = h.n_blocks_prev;
     {
@@ -322,16 +364,16 @@ static ntr_status upload_state(Sim& S, const World& w) {
             run += __builtin_popcount(mask[k]);
         }
         prefix[D.nwords] = run;
-        CU(cudaMemcpy(D.mask[cur], mask.data(), (size_t)D.nwords * 4, cudaMemcpyHostToDevice));
-        CU(cudaMemcpy(D.prefix[cur], prefix.data(), ((size_t)D.nwords + 1) * 4, cudaMemcpyHostToDevice));
-        CU(cudaMemset(D.mask[cur ^ 1], 0, (size_t)D.nwords * 4));
-        CU(cudaMemset(D.prefix[cur ^ 1], 0, ((size_t)D.nwords + 1) * 4));
+        CU(cudaMemcpyAsync(D.mask[cur], mask.data(), (size_t)D.nwords * 4, cudaMemcpyHostToDevice, S.stream));
+        CU(cudaMemcpyAsync(D.prefix[cur], prefix.data(), ((size_t)D.nwords + 1) * 4, cudaMemcpyHostToDevice, S.stream));
+        CU(cudaMemsetAsync(D.mask[cur ^ 1], 0, (size_t)D.nwords * 4, S.stream));
+        CU(cudaMemsetAsync(D.prefix[cur ^ 1], 0, ((size_t)D.nwords + 1) * 4, S.stream));
         if (nbp) {
-            CU(cudaMemcpy(D.block_list[cur], bl, (size_t)nbp * 4, cudaMemcpyHostToDevice));
-            CU(cudaMemcpy(D.block_active, w.sec[NTR_SEC_BLOCK_ACTIVE].data(), (size_t)nbp * 4, cudaMemcpyHostToDevice));
+            CU(cudaMemcpyAsync(D.block_list[cur], bl, (size_t)nbp * 4, cudaMemcpyHostToDevice, S.stream));
+            CU(cudaMemcpyAsync(D.block_active, w.sec[NTR_SEC_BLOCK_ACTIVE].data(), (size_t)nbp * 4, cudaMemcpyHostToDevice, S.stream));
             const float* af = w.as<float>(NTR_SEC_AIR);
             for (uint32_t f = 0; f < NTR_AIR_FIELDS; f++)
-                CU(cudaMemcpy(D.air[0] + (size_t)f * D.cap_cells, af + (size_t)f * nbp * 64, (size_t)nbp * 64 * 4, cudaMemcpyHostToDevice));
+                CU(cudaMemcpyAsync(D.air[0] + (size_t)f * D.cap_cells, af + (size_t)f * nbp * 64, (size_t)nbp * 64 * 4, cudaMemcpyHostToDevice, S.stream));
         }
     }
     DevState ds;
@@ -340,15 +382,15 @@ static ntr_status upload_state(Sim& S, const World& w) {
     ds.s = h.state;
     ds.s.n_blocks = nbp;
     ds.rz = h.state.rz, ds.alpha = h.state.alpha, ds.beta = h.state.beta, ds.b_norm = h.state.b_norm, ds.r_norm = h.state.r_norm;
-    CU(cudaMemcpy(D.st, &ds, sizeof ds, cudaMemcpyHostToDevice));
+    CU(cudaMemcpyAsync(D.st, &ds, sizeof ds, cudaMemcpyHostToDevice, S.stream));
     return NTR_OK;
 }
 
 static ntr_status upload_static(Sim& S, const World& w) {
     Dev& D = S.D;
-    CU(cudaMemcpy((void*)D.tris, w.sec[NTR_SEC_TRIS].data(), (size_t)D.Nt * 32, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(D.vtri_off, w.sec[NTR_SEC_VTRI_OFF].data(), ((size_t)D.Nv + 1) * 4, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(D.vtri, w.sec[NTR_SEC_VTRI].data(), w.sec[NTR_SEC_VTRI].size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpyAsync((void*)D.tris, w.sec[NTR_SEC_TRIS].data(), (size_t)D.Nt * 32, cudaMemcpyHostToDevice, S.stream));
+    CU(cudaMemcpyAsync(D.vtri_off, w.sec[NTR_SEC_VTRI_OFF].data(), ((size_t)D.Nv + 1) * 4, cudaMemcpyHostToDevice, S.stream));
+    CU(cudaMemcpyAsync(D.vtri, w.sec[NTR_SEC_VTRI].data(), w.sec[NTR_SEC_VTRI].size(), cudaMemcpyHostToDevice, S.stream));
     {
         // Which corner of each of its triangles a vertex is: the first of v0, v1, v2 that it
         // equals (the order in which membrane.wgsl's vertex_force tests them).
@@ -362,11 +404,11 @@ static ntr_status upload_static(Sim& S, const World& w) {
                 const uint32_t t = vt[k];
                 if (t < D.Nt) corner[k] = tr[t].v0 == i ? 0 : tr[t].v1 == i ? 1 : 2;
             }
-        if (n_vt) CU(cudaMemcpy(D.vtri_c, corner.data(), n_vt, cudaMemcpyHostToDevice));
+        if (n_vt) CU(cudaMemcpyAsync(D.vtri_c, corner.data(), n_vt, cudaMemcpyHostToDevice, S.stream));
     }
-    CU(cudaMemcpy(D.mem_mass, w.sec[NTR_SEC_MEM_MASS].data(), (size_t)D.Nv * 4, cudaMemcpyHostToDevice));
-    CU(cudaMemcpy((void*)D.patches, w.sec[NTR_SEC_PATCHES].data(), w.sec[NTR_SEC_PATCHES].size(), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy((void*)D.outlines, w.sec[NTR_SEC_OUTLINES].data(), w.sec[NTR_SEC_OUTLINES].size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpyAsync(D.mem_mass, w.sec[NTR_SEC_MEM_MASS].data(), (size_t)D.Nv * 4, cudaMemcpyHostToDevice, S.stream));
+    CU(cudaMemcpyAsync((void*)D.patches, w.sec[NTR_SEC_PATCHES].data(), w.sec[NTR_SEC_PATCHES].size(), cudaMemcpyHostToDevice, S.stream));
+    CU(cudaMemcpyAsync((void*)D.outlines, w.sec[NTR_SEC_OUTLINES].data(), w.sec[NTR_SEC_OUTLINES].size(), cudaMemcpyHostToDevice, S.stream));
     return NTR_OK;
 }
 
@@ -699,43 +741,64 @@ static ntr_status run_batch(Sim& S, uint32_t n, uint32_t stop, uint32_t* taken, 
     return NTR_OK;
 }
 
+// A batch slot's streams and events, kept across the scenes it holds (creating them is a
+// driver call each, which admitting a scene would otherwise pay).
+struct SimHandles {
+    cudaStream_t stream = nullptr, aux = nullptr, aux2 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_fork[3] = {nullptr, nullptr, nullptr}, ev_join[3] = {nullptr, nullptr, nullptr};
+};
+static ntr_status make_handles(SimHandles& h) {
+    CU(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+    CU(cudaStreamCreateWithFlags(&h.aux, cudaStreamNonBlocking));
+    CU(cudaStreamCreateWithFlags(&h.aux2, cudaStreamNonBlocking));
+    for (int k = 0; k < 3; k++) {
+        CU(cudaEventCreateWithFlags(&h.ev_fork[k], cudaEventDisableTiming));
+        CU(cudaEventCreateWithFlags(&h.ev_join[k], cudaEventDisableTiming));
+    }
+    CU(cudaEventCreate(&h.ev0));
+    CU(cudaEventCreate(&h.ev1));
+    return NTR_OK;
+}
+static void free_handles(SimHandles& h) {
+    if (h.ev0) cudaEventDestroy(h.ev0);
+    if (h.ev1) cudaEventDestroy(h.ev1);
+    for (int k = 0; k < 3; k++) {
+        if (h.ev_fork[k]) cudaEventDestroy(h.ev_fork[k]);
+        if (h.ev_join[k]) cudaEventDestroy(h.ev_join[k]);
+    }
+    if (h.aux2) cudaStreamDestroy(h.aux2);
+    if (h.aux) cudaStreamDestroy(h.aux);
+    if (h.stream) cudaStreamDestroy(h.stream);
+    h = SimHandles{};
+}
+
 static ntr_status create_from(const World& w, int device, Sim*& out, uint8_t* arena = nullptr, size_t arena_cap = 0,
-                              DevState* h_state = nullptr) {
+                              DevState* h_state = nullptr, const SimHandles* borrowed = nullptr) {
     ntr_status r = check_device(device);
     if (r != NTR_OK) return r;
     DeviceScope scope(device);
     if (!scope.ok) return fail(NTR_E_CUDA, "cudaSetDevice failed");
+    DevFacts f;
+    if ((r = device_facts(device, f)) != NTR_OK) return r;
+    if (f.major < 10) return fail(NTR_E_NODEVICE, "this library is built for sm_100a (B200); device is sm_" + std::to_string(f.major * 10 + f.minor));
     std::unique_ptr<Sim> S(new Sim);
     S->device = device;
     S->host.h = w.h;
     S->U = w.h.params;
-    cudaDeviceProp prop;
-    CU(cudaGetDeviceProperties(&prop, device));
-    S->sms = prop.multiProcessorCount;
-    {
-        // The persistent solver's grid must be co-resident: at most what occupancy allows.
-        int occ_a = 0, occ_b = 0;
-        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_solve<true>, SOLVE_T, 0));
-        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_solve<false>, SOLVE_T, 0));
-        int occ = std::min(occ_a, occ_b);
-        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_solve_batch<true>, SOLVE_T, 0));
-        CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_solve_batch<false>, SOLVE_T, 0));
-        occ = std::min(occ, std::min(occ_a, occ_b));
-        // CTA c owns the blocks c (mod 256) (and c + G, ... with fewer CTAs): at most 256.
-        S->coop_ctas = (uint32_t)std::min(256, S->sms * occ);
-        if (S->coop_ctas < 1) return fail(NTR_E_NODEVICE, "the device cannot hold a solver CTA");
-    }
+    S->sms = f.sms;
+    S->coop_ctas = f.coop_ctas;
+    if (S->coop_ctas < 1) return fail(NTR_E_NODEVICE, "the device cannot hold a solver CTA");
     if (w.h.block_cap > 65535u) return fail(NTR_E_INVALID, "block_cap is at most 65535");
-    if (prop.major < 10) return fail(NTR_E_NODEVICE, "this library is built for sm_100a (B200); device is sm_" + std::to_string(prop.major * 10 + prop.minor));
-    CU(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
-    CU(cudaStreamCreateWithFlags(&S->aux, cudaStreamNonBlocking));
-    CU(cudaStreamCreateWithFlags(&S->aux2, cudaStreamNonBlocking));
-    for (int k = 0; k < 3; k++) {
-        CU(cudaEventCreateWithFlags(&S->ev_fork[k], cudaEventDisableTiming));
-        CU(cudaEventCreateWithFlags(&S->ev_join[k], cudaEventDisableTiming));
+    SimHandles hs;
+    if (borrowed) {
+        hs = *borrowed;
+        S->own_streams = false;
+    } else if ((r = make_handles(hs)) != NTR_OK) {
+        free_handles(hs);
+        return r;
     }
-    CU(cudaEventCreate(&S->ev0));
-    CU(cudaEventCreate(&S->ev1));
+    S->stream = hs.stream, S->aux = hs.aux, S->aux2 = hs.aux2, S->ev0 = hs.ev0, S->ev1 = hs.ev1;
+    for (int k = 0; k < 3; k++) S->ev_fork[k] = hs.ev_fork[k], S->ev_join[k] = hs.ev_join[k];
     if (h_state)
         S->h_state = h_state, S->own_h_state = false;
     else

@@ -173,6 +173,10 @@ def serve(worlds, arrivals: list[float], steps: int, chunk: int = 4, max_scenes:
     queue: list[tuple[int, object]] = []  # (request, its world or the future building it)
     slot_req: dict[int, int] = {}
     pool = ThreadPoolExecutor(max_workers=max(1, build_threads)) if build else None
+    # Where the loop's time goes: admitting scenes, stepping, polling and retiring, waiting with
+    # nothing to step; and how full the batch was, step call by step call.
+    t_admit = t_step = t_poll = t_idle = 0.0
+    calls, occupancy = 0, 0
     try:
         with batch_factory() as b:
             t0 = clock()
@@ -184,6 +188,7 @@ def serve(worlds, arrivals: list[float], steps: int, chunk: int = 4, max_scenes:
                     if i is None:
                         break
                     queue.append((i, pool.submit(build, worlds[i]) if build else worlds[i]))
+                ta = clock()
                 while queue:
                     i, w = queue[0]
                     if build:
@@ -195,23 +200,35 @@ def serve(worlds, arrivals: list[float], steps: int, chunk: int = 4, max_scenes:
                         break
                     slot_req[sl] = i
                     queue.pop(0)
+                tb = clock()
+                t_admit += tb - ta
                 if not slot_req:
                     time.sleep(min(requests.wait_hint(clock() - t0), 0.002) if not queue else 0.0005)
+                    t_idle += clock() - tb
                     continue
                 b.step(chunk)
-                now = clock() - t0
+                tc = clock()
+                t_step += tc - tb
+                calls += 1
+                occupancy += len(slot_req)
+                now = tc - t0
                 for sl in list(slot_req):
                     if b.poll(sl)["finished"]:
                         finish[slot_req.pop(sl)] = now
                         b.retire(sl)
+                t_poll += clock() - tc
             makespan = clock() - t0
+            info = b.info() if hasattr(b, "info") else {}
     finally:
         if pool:
             pool.shutdown(wait=True)
     served = sorted(finish)
     lat = np.array([finish[i] - arrivals[i] for i in served])
     out = {"requests": len(served), "seconds": makespan, "scenes_per_s": len(served) / makespan if makespan > 0 else 0.0,
-           "latencies": [float(x) for x in lat], "requests_served": served}
+           "latencies": [float(x) for x in lat], "requests_served": served,
+           "loop": {"admit_s": t_admit, "step_s": t_step, "poll_s": t_poll, "idle_s": t_idle, "step_calls": calls,
+                    "mean_scenes_per_call": occupancy / calls if calls else 0.0,
+                    "graph_captures": info.get("captures"), "graph_instantiations": info.get("instantiations")}}
     if lat.size:
         out.update({"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean())})
     return out
