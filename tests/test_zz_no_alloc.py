@@ -79,3 +79,36 @@ def test_noalloc_sort_rejects_sizes_beyond_its_scratch():
     with pytest.raises(NatrayError) as e:
         check(lib().ntr_sort_by_block_noalloc(small.data_ptr(), 4, 65536, small.data_ptr(), small.data_ptr(), None))
     assert e.value.status == 1 and "at most 65535" in str(e.value)
+
+
+def expected_sort(keys: np.ndarray, n_blocks: int):
+    """The stable sort by block of numpy: particle indices grouped by key (NONE last), and where
+    each block's particles start."""
+    order = np.argsort(keys.astype(np.int64), kind="stable").astype(np.uint32)
+    valid = np.sort(keys[keys != NONE].astype(np.int64))
+    starts = np.searchsorted(valid, np.arange(n_blocks + 1), side="left").astype(np.uint32)
+    return order[: len(valid)], starts
+
+
+@pytest.mark.parametrize("n,n_blocks", [(3 * 4096 + 17, 300), (1048576, 60000)])
+def test_noalloc_sort_two_passes_up_to_the_key_limit(n, n_blocks):
+    # More than 255 blocks: two 8-bit passes (through the scratch's alternate keys and values);
+    # partial last tiles; about 5 % of the particles taking no part; the largest n it takes.
+    import torch
+    torch.cuda.init()
+    rng = np.random.default_rng(n)
+    keys = rng.integers(0, n_blocks, size=n, dtype=np.int64).astype(np.uint32)
+    keys[rng.random(n) < 0.05] = NONE
+    srt, bs = sort_noalloc(keys, n_blocks)
+    want_srt, want_bs = expected_sort(keys, n_blocks)
+    assert np.array_equal(bs, want_bs)
+    assert np.array_equal(srt[: bs[-1]], want_srt)
+
+
+def test_noalloc_sort_of_no_keys():
+    import torch
+    dev = torch.device("cuda:0")
+    bs = torch.full((65,), -1, dtype=torch.int32, device=dev)
+    check(lib().ntr_sort_by_block_noalloc(None, 0, 64, None, bs.data_ptr(), None))
+    torch.cuda.synchronize(dev)
+    assert np.array_equal(bs.cpu().numpy(), np.zeros(65, dtype=np.int32))
