@@ -127,6 +127,38 @@ __device__ __forceinline__ Gathered gather(const float* tg, V3 X, V3 o, I3 corne
     return r;
 }
 
+// Asynchronous 4-byte copies global -> shared (cp.async; a source of size 0 fills zeros), in
+// groups a thread commits and later waits for.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, bool valid) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(sa), "l"(gmem), "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// The raw fields of a block's 7^3 tile on their way to shared memory: per node the three
+// velocities and the three weight sums, the cell type and the pressure (zeros where no block
+// is), and the block's own 64 cells' rubber area sums.
+constexpr uint32_t G2P_RAW = 8;
+__device__ __forceinline__ void g2p_stage(const Dev& D, uint32_t b, uint32_t* links, uint32_t* raw, uint32_t* raw_cov, uint32_t nthreads) {
+    if (threadIdx.x < 27) links[threadIdx.x] = D.block_nb[b * 27u + threadIdx.x];
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < TILE; t += nthreads) {
+        const uint32_t cell = tile_cell(links, t);
+        const bool ok = cell != NONE;
+        const uint32_t c = ok ? cell : 0u;
+#pragma unroll
+        for (uint32_t d = 0; d < 3; d++) {
+            cp_async4(raw + d * TILE + t, D.cf + (size_t)(F_U + d) * D.cap_cells + c, ok);
+            cp_async4(raw + (3 + d) * TILE + t, D.acc + (size_t)a_wt(d) * D.cap_cells + c, ok);
+        }
+        cp_async4(raw + 6 * TILE + t, D.cf + (size_t)F_TYPE * D.cap_cells + c, ok);
+        cp_async4(raw + 7 * TILE + t, D.cf + (size_t)F_P * D.cap_cells + c, ok);
+    }
+    if (threadIdx.x < 64) cp_async4(raw_cov + threadIdx.x, D.acc + (size_t)A_MA * D.cap_cells + b * 64u + threadIdx.x, true);
+    cp_async_commit();
+}
+
 // G2P_T threads a CTA, 768 / G2P_T CTAs an SM. With many blocks (the 1M-particle scene: 128
 // threads, six CTAs an SM) a block's few hundred particles take 3 rounds with a short last one,
 // and the SM has more CTAs to switch to while one waits on its loads or barriers. With few
@@ -148,20 +180,31 @@ __device__ __forceinline__ void g2p_body(const Dev& D, const CT& C) {
     const float cs = 4.0f / (hh * hh);
     const uint32_t step_no = st->s.step;
     __shared__ float tg[8 * TILE];
-    __shared__ uint32_t links[27];
+    __shared__ uint32_t raw[G2P_RAW * TILE];  // the next block's fields, arriving (g2p_stage)
+    __shared__ uint32_t raw_cov[64];
+    __shared__ uint32_t s_links[2][27];       // the current block's neighbours, and the next's
     __shared__ uint8_t s_cov[64];  // the block's own cells: rubber over them (A_MA > 0)
     __shared__ uint32_t s_wcount[G2P_T / 32];
     __shared__ uint32_t s_brk;
     float fastest = 0.0f;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    for (uint32_t b = C.x(); b < nb; b += C.nx()) {
+    // The CTA's blocks that hold particles, in turn (an empty one only gets its count of break-ups).
+    auto next_full = [&](uint32_t x) {
+        while (x < nb && D.block_start[x + 1] == D.block_start[x]) {
+            if (threadIdx.x == 0) D.brk_count[x] = 0;
+            x += C.nx();
+        }
+        return x;
+    };
+    // Each block's tile is staged while the block before it is processed: its fields come in by
+    // asynchronous copies behind that block's particles, and only the first block's wait is bare.
+    uint32_t b = next_full(C.x()), cur = 0;
+    if (b < nb) g2p_stage(D, b, s_links[0], raw, raw_cov, G2P_T);
+    while (b < nb) {
+        const uint32_t* links = s_links[cur];
         const uint32_t first = D.block_start[b];
         const uint32_t count = D.block_start[b + 1] - first;
-        if (count == 0) {
-            if (threadIdx.x == 0) D.brk_count[b] = 0;
-            continue;
-        }
-        // This thread's particle of the first round, loaded before the tile so that the two
+        // This thread's particle of the first round, loaded before the tile is made so that the
         // waits overlap; each round then loads the next round's particle before its gathers.
         uint32_t i_next = 0u;
         float4 pos_next = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -171,27 +214,24 @@ __device__ __forceinline__ void g2p_body(const Dev& D, const CT& C) {
             pos_next = D.pos[i_next];
             c1w_next = D.c1[i_next].w;
         }
-        if (threadIdx.x < 27) links[threadIdx.x] = D.block_nb[b * 27u + threadIdx.x];
-        if (threadIdx.x < 64) s_cov[threadIdx.x] = accv(D, A_MA, b * 64u + threadIdx.x) > 0 ? 1 : 0;
-        if (threadIdx.x == 0) s_brk = 0;
+        cp_async_wait_all();
         __syncthreads();
         for (uint32_t t = threadIdx.x; t < TILE; t += G2P_T) {
-            uint32_t cell = tile_cell(links, t);
-            bool water = cell != NONE && cfv(D, F_TYPE, cell) == WATER_T;
+            const float ty = __uint_as_float(raw[6 * TILE + t]);
+            const bool water = ty == WATER_T;  // zeros (gas) where no block is
 #pragma unroll
             for (uint32_t d = 0; d < 3; d++) {
-                float u = 0.0f, w = 0.0f;
-                if (cell != NONE) {
-                    u = cfv(D, F_U + d, cell);
-                    w = from_fp(accv(D, a_wt(d), cell), FP_W);
-                }
-                tg[a_mom(d) * TILE + t] = u;
-                tg[a_wt(d) * TILE + t] = w;
+                tg[a_mom(d) * TILE + t] = __uint_as_float(raw[d * TILE + t]);
+                tg[a_wt(d) * TILE + t] = from_fp((int32_t)raw[(3 + d) * TILE + t], FP_W);
             }
-            tg[A_PC * TILE + t] = water ? pressure_of(D, cell) : 0.0f;
+            tg[A_PC * TILE + t] = water ? mx(__uint_as_float(raw[7 * TILE + t]), P_VAPOUR - P_ATM) : 0.0f;
             tg[A_WC * TILE + t] = water ? 1.0f : 0.0f;
         }
+        if (threadIdx.x < 64) s_cov[threadIdx.x] = (int32_t)raw_cov[threadIdx.x] > 0 ? 1 : 0;
+        if (threadIdx.x == 0) s_brk = 0;
         __syncthreads();
+        const uint32_t nxt = next_full(b + C.nx());
+        if (nxt < nb) g2p_stage(D, nxt, s_links[cur ^ 1u], raw, raw_cov, G2P_T);
         const I3 corner = slot_coord(g, g.list[b]) * 4 - I3{1, 1, 1};
         // Rounds of G2P_T particles keep the sorted order for ranking the break-ups.
         for (uint32_t base = 0; base < count; base += G2P_T) {
@@ -278,6 +318,8 @@ __device__ __forceinline__ void g2p_body(const Dev& D, const CT& C) {
         }
         if (threadIdx.x == 0) D.brk_count[b] = s_brk;
         __syncthreads();
+        b = nxt;
+        cur ^= 1u;
     }
     for (int o = 16; o > 0; o >>= 1) fastest = fmaxf(fastest, __shfl_down_sync(0xffffffffu, fastest, o));
     if (lane == 0 && fastest > 0.0f) atomicMax((unsigned int*)&st->s.max_speed, __float_as_uint(fastest));
