@@ -169,7 +169,9 @@ static ntr_status batch_create(int device, uint32_t max_scenes, uint64_t budget,
     DevFacts f;
     if ((r = device_facts(device, f)) != NTR_OK) return r;
     if (f.major < 10) return fail(NTR_E_NODEVICE, "this library is built for sm_100a (B200)");
-    const uint32_t ctas = f.coop_ctas;
+    // Each system of the joint solve takes at most 256 CTAs (the residues of the reference's
+    // summation tree); together they may use every CTA the device holds at once.
+    const uint32_t ctas = f.coop_all;
     // Every scene needs a CTA of the joint solve.
     if (max_scenes > ctas) return fail(NTR_E_INVALID, "max_scenes is at most " + std::to_string(ctas) + " on this device");
     std::unique_ptr<Batch> B(new Batch);

@@ -90,7 +90,7 @@ struct DevState {
     uint32_t nbrk;       // break-ups of this step
     uint32_t err;        // bit 0: a bounded grid barrier gave up
     uint32_t bar_count;  // grid barrier of the persistent solver: arrivals (reset per launch)
-    uint32_t bar_gen;    // unused
+    uint32_t iters_prev;  // the last solve's iterations, kept for a joint solve's split (k_solve_reset_m)
     uint32_t pad[3];
     // The step's work, for its algorithmic bytes: this step's water and free-gas cells (counted
     // by k_project), and totals since ntr_sim_work last cleared them (added by the step's last

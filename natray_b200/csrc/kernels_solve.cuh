@@ -208,12 +208,13 @@ constexpr uint32_t SOLVE_MAX_JOBS = 128;  // systems solved by one launch, at mo
 constexpr uint32_t SOLVE_PART_SH = 512;   // partial sums per quantity kept in shared memory
 
 // The CTAs of a launch split over its jobs (independent systems, each a simulation's step):
-// every job that steps gets one CTA and the rest go by block count, at most 256 each. Every CTA
-// computes the same split. c0[j] .. c0[j + 1] are job j's CTAs.
+// every job that steps gets one CTA and the rest go by expected work, its blocks times its last
+// solve's iterations, at most 256 each. Every CTA computes the same split. c0[j] .. c0[j + 1]
+// are job j's CTAs. (A job's result does not depend on how many CTAs it gets.)
 __device__ __forceinline__ void solve_split(const Dev* jobs, uint32_t n_jobs, uint32_t* w, uint32_t* c0) {
     for (uint32_t j = threadIdx.x; j < n_jobs; j += blockDim.x) {
         const DevState* st = jobs[j].st;
-        w[j] = st->s.dt_ns == 0u ? NONE : min(st->s.n_blocks, jobs[j].cap_blocks);
+        w[j] = st->s.dt_ns == 0u ? NONE : min(st->s.n_blocks, jobs[j].cap_blocks) * max(min(st->iters_prev, 4096u), 1u);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -559,12 +560,13 @@ __global__ void __launch_bounds__(SOLVE_T, 2) k_solve_batch(const Dev* __restric
 }
 
 // Every scene's grid barrier counter back to zero before the joint solve (a one-scene step
-// clears its own with a memset).
+// clears its own with a memset), and its last solve's iterations set aside for the split: the
+// solve itself rewrites them, and every CTA must compute the same split.
 __global__ void k_solve_reset_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
-    if (threadIdx.x == 0) sD.st->bar_count = 0u;
+    if (threadIdx.x == 0) sD.st->bar_count = 0u, sD.st->iters_prev = sD.st->s.solve_iters;
 }
 
 }  // namespace ntr

@@ -172,6 +172,7 @@ static ntr_status check_device(int device) {
 struct DevFacts {
     int sms = 0, major = 0, minor = 0;
     uint32_t coop_ctas = 0;  // CTAs of a persistent solve that the device holds at once (at most 256)
+    uint32_t coop_all = 0;   // CTAs of the solve the device holds at once, uncapped (a joint solve of many systems)
     bool known = false;
 };
 static ntr_status device_facts(int device, DevFacts& out) {
@@ -200,6 +201,7 @@ static ntr_status device_facts(int device, DevFacts& out) {
             CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_solve_batch<false>, SOLVE_T, 0));
             occ = std::min(occ, o);
             f.coop_ctas = (uint32_t)std::min(256, f.sms * occ);
+            f.coop_all = (uint32_t)(f.sms * occ);
         }
         f.known = true;
     }
