@@ -75,6 +75,7 @@ struct BatchSlot {
     size_t arena_cap = 0;
     DevState* h_state = nullptr;
     SimHandles hs;  // its scenes' streams and events, made at its first scene
+    bool reserved = false;  // a scene is being created in it (ntr_batch_admit, outside the lock)
 };
 
 struct Batch {
@@ -109,8 +110,12 @@ struct Batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::vector<uint32_t> graph_key;
-    // Every call on the batch holds this lock: calls from several host threads take turns.
+    // Every call on the batch holds this lock: calls from several host threads take turns. A
+    // batch step lets it go while it waits for the GPU (in_flight): then only admissions, which
+    // touch free slots alone, may proceed; every other call waits for the step to end.
     std::mutex mu;
+    std::condition_variable cv;
+    bool in_flight = false;
     // Scenes queued by any thread (ntr_batch_enqueue), admitted in order at the start of the
     // next ntr_batch_step; where each ticket went (a slot, or BATCH_REJECTED).
     struct Queued {
@@ -207,20 +212,14 @@ static ntr_status batch_create(int device, uint32_t max_scenes, uint64_t budget,
     return NTR_OK;
 }
 
-static ntr_status batch_admit(Batch& B, const void* blob, size_t len, uint32_t n_steps, uint32_t& slot) {
-    CU(cudaSetDevice(B.device));
-    World w;
-    std::string err;
-    if (!deserialize(blob, len, w, err)) return fail(NTR_E_INVALID, err);
-    uint64_t need = 0;
-    ntr_status r = world_device_bytes(w, need);
-    if (r != NTR_OK) return r;
-    // A free slot whose region already holds the scene (the smallest such), else the free slot
-    // with the largest region.
+// Picks and prepares a free slot for a scene of `need` device bytes (its region grown if it must
+// be, its streams made): a free slot whose region already holds the scene (the smallest such),
+// else the free slot with the largest region. Under the batch's lock.
+static ntr_status batch_reserve(Batch& B, uint64_t need, uint32_t& slot) {
     uint32_t free_slot = NONE, fits = NONE;
     for (uint32_t i = 0; i < B.max_scenes; i++) {
         const BatchSlot& c = B.slots[i];
-        if (c.sim) continue;
+        if (c.sim || c.reserved) continue;
         if (c.arena_cap >= need && (fits == NONE || c.arena_cap < B.slots[fits].arena_cap)) fits = i;
         if (free_slot == NONE || c.arena_cap > B.slots[free_slot].arena_cap) free_slot = i;
     }
@@ -244,16 +243,64 @@ static ntr_status batch_admit(Batch& B, const void* blob, size_t len, uint32_t n
         sl.arena_cap = need + need / 4;
         B.held += sl.arena_cap;
     }
+    ntr_status r;
     if (!sl.hs.stream && (r = make_handles(sl.hs)) != NTR_OK) {
         free_handles(sl.hs);
         return r;
     }
+    slot = free_slot;
+    return NTR_OK;
+}
+
+// Admission with the batch's lock held throughout (the queued scenes of a batch step).
+static ntr_status batch_admit(Batch& B, const void* blob, size_t len, uint32_t n_steps, uint32_t& slot) {
+    CU(cudaSetDevice(B.device));
+    World w;
+    std::string err;
+    if (!deserialize(blob, len, w, err)) return fail(NTR_E_INVALID, err);
+    uint64_t need = 0;
+    ntr_status r = world_device_bytes(w, need);
+    if (r != NTR_OK) return r;
+    uint32_t k = 0;
+    if ((r = batch_reserve(B, need, k)) != NTR_OK) return r;
+    BatchSlot& sl = B.slots[k];
     Sim* s = nullptr;
     if ((r = create_from(w, B.device, s, sl.arena, sl.arena_cap, sl.h_state, &sl.hs)) != NTR_OK) return r;
     sl.sim.reset(s);
     sl.target = n_steps;
     sl.done = 0;
-    slot = free_slot;
+    slot = k;
+    return NTR_OK;
+}
+
+// Admission from any thread, beside a batch step: the world is checked and sized without the
+// lock, a slot reserved under it, the scene created in the slot without it (its uploads and
+// measuring substep on the slot's own stream, overlapping the step's work on the GPU), and the
+// scene placed under it again. Only the reservation and the placing wait for the lock, which a
+// batch step lets go while it waits for the GPU.
+static ntr_status batch_admit_overlapped(Batch& B, const void* blob, size_t len, uint32_t n_steps, uint32_t& slot) {
+    World w;
+    std::string err;
+    if (!deserialize(blob, len, w, err)) return fail(NTR_E_INVALID, err);
+    uint64_t need = 0;
+    ntr_status r = world_device_bytes(w, need);
+    if (r != NTR_OK) return r;
+    uint32_t k = 0;
+    {
+        std::lock_guard<std::mutex> lk(B.mu);
+        if ((r = batch_reserve(B, need, k)) != NTR_OK) return r;
+        B.slots[k].reserved = true;
+    }
+    BatchSlot& sl = B.slots[k];
+    Sim* s = nullptr;
+    r = create_from(w, B.device, s, sl.arena, sl.arena_cap, sl.h_state, &sl.hs);
+    std::lock_guard<std::mutex> lk(B.mu);
+    sl.reserved = false;
+    if (r != NTR_OK) return r;
+    sl.sim.reset(s);
+    sl.target = n_steps;
+    sl.done = 0;
+    slot = k;
     return NTR_OK;
 }
 
@@ -382,7 +429,8 @@ static uint64_t enqueue_step_multi(Batch& B, uint32_t n_jobs, const uint32_t* to
 
 // n steps of every unfinished scene: each scene takes min(n, its steps left) (its step budget
 // stops it after those), all of them in the same replays of the batch's step graph.
-static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active, Prof* prof = nullptr) {
+// `lk` (the batch's lock, held by the caller) is let go while the step waits for the GPU.
+static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active, Prof* prof = nullptr, std::unique_lock<std::mutex>* lk = nullptr) {
     std::vector<uint32_t> order;
     std::vector<uint32_t> todo(B.max_scenes, 0u);
     for (uint32_t i = 0; i < B.max_scenes; i++) {
@@ -487,7 +535,20 @@ static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active, Prof* prof 
     k_batch_end<<<n_jobs, 64, 0, s>>>(B.d_jobs, B.d_out);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(B.h_out, B.d_out, sizeof(DevState) * n_jobs, cudaMemcpyDeviceToHost, s));
-    CU(cudaStreamSynchronize(s));
+    {
+        // Admissions may reserve and fill free slots meanwhile; every other call waits.
+        if (lk) {
+            B.in_flight = true;
+            lk->unlock();
+        }
+        const cudaError_t e = cudaStreamSynchronize(s);
+        if (lk) {
+            lk->lock();
+            B.in_flight = false;
+            B.cv.notify_all();
+        }
+        CU(e);
+    }
     ntr_status first_err = NTR_OK;
     for (uint32_t j = 0; j < n_jobs; j++) {
         BatchSlot& sl = B.slots[order[j]];

@@ -14,6 +14,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <condition_variable>
 #include <mutex>
 #include <string>
 #include <tuple>
@@ -1380,7 +1381,8 @@ struct ntr_batch {
 #define BGUARD(batch)                                                                   \
     if (!(batch) || !(batch)->b) return fail(NTR_E_INVALID, "null batch handle");        \
     Batch& B = *(batch)->b;                                                             \
-    std::lock_guard<std::mutex> batch_lock_(B.mu);                                      \
+    std::unique_lock<std::mutex> batch_lock_(B.mu);                                     \
+    B.cv.wait(batch_lock_, [&] { return !B.in_flight; });                               \
     DeviceScope device_scope_(B.device);                                                \
     if (!device_scope_.ok) return fail(NTR_E_CUDA, "cudaSetDevice failed")
 
@@ -1405,9 +1407,12 @@ NTR_API ntr_status ntr_batch_destroy(ntr_batch* batch) {
 }
 
 NTR_API ntr_status ntr_batch_admit(ntr_batch* batch, const void* blob, size_t len, uint32_t n_steps, uint32_t* slot) {
-    BGUARD(batch);
+    if (!batch || !batch->b) return fail(NTR_E_INVALID, "null batch handle");
     if (!blob || !slot) return fail(NTR_E_INVALID, "null argument");
-    return batch_admit(B, blob, len, n_steps, *slot);
+    Batch& B = *batch->b;
+    DeviceScope scope(B.device);
+    if (!scope.ok) return fail(NTR_E_CUDA, "cudaSetDevice failed");
+    return batch_admit_overlapped(B, blob, len, n_steps, *slot);
 }
 
 NTR_API ntr_status ntr_world_device_bytes(const void* blob, size_t len, uint64_t* bytes) {
@@ -1475,7 +1480,7 @@ NTR_API ntr_status ntr_batch_step(ntr_batch* batch, uint32_t n, uint32_t* active
         B.queue.pop_front();
     }
     uint32_t a = 0;
-    ntr_status r = batch_step(B, n, a);
+    ntr_status r = batch_step(B, n, a, nullptr, &batch_lock_);
     if (active) *active = a;
     return r;
 }

@@ -157,67 +157,118 @@ def serve(worlds, arrivals: list[float], steps: int, chunk: int = 4, max_scenes:
     """Continuous batching: a request enters the batch when it has arrived (and, with `build`,
     its scene has been built on a host thread, which its latency includes) and a slot and the
     device memory are free, runs `steps` steps among the others, and leaves. Latency = completion
-    - arrival.
+    - arrival. Scenes are admitted by a thread of their own, in arrival order, while the batch
+    steps: ntr_batch_admit creates a scene in a free slot beside a running batch step (its
+    uploads on the slot's own stream), so admitting does not hold up the GPU.
 
     worlds         the requests' worlds, or their parameters when `build` (a function of them
                    returning a World, natray_b200.build_world) builds each on its arrival
     requests       where requests come from: LocalRequests(arrivals) by default, SharedRequests
                    when several servers share one stream
     batch_factory  makes the batch (natray_b200.batch.Batch); tests pass a stand-in"""
+    import threading
+    from collections import deque
     from concurrent.futures import ThreadPoolExecutor
 
     requests = requests or LocalRequests(arrivals)
     batch_factory = batch_factory or (lambda: Batch(max_scenes=max_scenes))
     clock = clock or time.perf_counter
     finish: dict[int, float] = {}
-    queue: list[tuple[int, object]] = []  # (request, its world or the future building it)
     slot_req: dict[int, int] = {}
     pool = ThreadPoolExecutor(max_workers=max(1, build_threads)) if build else None
-    # Where the loop's time goes: admitting scenes, stepping, polling and retiring, waiting with
-    # nothing to step; and how full the batch was, step call by step call.
-    t_admit = t_step = t_poll = t_idle = 0.0
+    # The admission thread's queue (requests taken, in arrival order, with their worlds or the
+    # builds of them) and its output (requests placed, with their slots); `room` wakes it when a
+    # slot frees up.
+    pending: deque = deque()
+    placed: deque = deque()
+    cv = threading.Condition()
+    stop = [False]
+    errors: list = []
+    # Where the time goes: admitting scenes (on the admission thread), stepping, polling and
+    # retiring, waiting with nothing to step; and how full the batch was, step call by step call.
+    t_admit = [0.0]
+    t_step = t_poll = t_idle = 0.0
     calls, occupancy = 0, 0
+
+    def admitter(b):
+        try:
+            while True:
+                with cv:
+                    while not pending and not stop[0]:
+                        cv.wait()
+                    if not pending:
+                        return
+                    i, w = pending[0]
+                if build:
+                    w = w.result()
+                while True:
+                    ta = clock()
+                    sl = b.admit(w, steps)
+                    t_admit[0] += clock() - ta
+                    if sl is not None:
+                        break
+                    with cv:  # no room: wait for a slot to free up
+                        if stop[0]:
+                            return
+                        cv.wait(timeout=0.005)
+                with cv:
+                    pending.popleft()
+                    placed.append((i, sl))
+        except BaseException as e:  # surfaced on the serving thread
+            errors.append(e)
+
     try:
         with batch_factory() as b:
+            th = threading.Thread(target=admitter, args=(b,), daemon=True)
+            th.start()
             t0 = clock()
-            while not requests.exhausted() or queue or slot_req:
-                now = clock() - t0
-                # Take requests while the batch has room for them (queued ones count).
-                while len(slot_req) + len(queue) < max_scenes:
-                    i = requests.claim(now)
-                    if i is None:
-                        break
-                    queue.append((i, pool.submit(build, worlds[i]) if build else worlds[i]))
-                ta = clock()
-                while queue:
-                    i, w = queue[0]
-                    if build:
-                        if not w.done():
+            try:
+                while True:
+                    if errors:
+                        raise errors[0]
+                    now = clock() - t0
+                    with cv:
+                        while placed:
+                            i, sl = placed.popleft()
+                            slot_req[sl] = i
+                        # Take requests while the batch has room for them (queued ones count).
+                        while len(slot_req) + len(pending) < max_scenes:
+                            i = requests.claim(now)
+                            if i is None:
+                                break
+                            pending.append((i, pool.submit(build, worlds[i]) if build else worlds[i]))
+                            cv.notify_all()
+                        waiting = len(pending)
+                    if not slot_req:
+                        if requests.exhausted() and not waiting:
                             break
-                        w = w.result()
-                    sl = b.admit(w, steps)
-                    if sl is None:
-                        break
-                    slot_req[sl] = i
-                    queue.pop(0)
-                tb = clock()
-                t_admit += tb - ta
-                if not slot_req:
-                    time.sleep(min(requests.wait_hint(clock() - t0), 0.002) if not queue else 0.0005)
-                    t_idle += clock() - tb
-                    continue
-                b.step(chunk)
-                tc = clock()
-                t_step += tc - tb
-                calls += 1
-                occupancy += len(slot_req)
-                now = tc - t0
-                for sl in list(slot_req):
-                    if b.poll(sl)["finished"]:
-                        finish[slot_req.pop(sl)] = now
-                        b.retire(sl)
-                t_poll += clock() - tc
-            makespan = clock() - t0
+                        tb = clock()
+                        time.sleep(min(requests.wait_hint(clock() - t0), 0.002) if not waiting else 0.0005)
+                        t_idle += clock() - tb
+                        continue
+                    tb = clock()
+                    b.step(chunk)
+                    tc = clock()
+                    t_step += tc - tb
+                    calls += 1
+                    occupancy += len(slot_req)
+                    now = tc - t0
+                    freed = False
+                    for sl in list(slot_req):
+                        if b.poll(sl)["finished"]:
+                            finish[slot_req.pop(sl)] = now
+                            b.retire(sl)
+                            freed = True
+                    if freed:
+                        with cv:
+                            cv.notify_all()
+                    t_poll += clock() - tc
+                makespan = clock() - t0
+            finally:
+                with cv:
+                    stop[0] = True
+                    cv.notify_all()
+                th.join()
             info = b.info() if hasattr(b, "info") else {}
     finally:
         if pool:
@@ -226,7 +277,7 @@ def serve(worlds, arrivals: list[float], steps: int, chunk: int = 4, max_scenes:
     lat = np.array([finish[i] - arrivals[i] for i in served])
     out = {"requests": len(served), "seconds": makespan, "scenes_per_s": len(served) / makespan if makespan > 0 else 0.0,
            "latencies": [float(x) for x in lat], "requests_served": served,
-           "loop": {"admit_s": t_admit, "step_s": t_step, "poll_s": t_poll, "idle_s": t_idle, "step_calls": calls,
+           "loop": {"admit_s": t_admit[0], "step_s": t_step, "poll_s": t_poll, "idle_s": t_idle, "step_calls": calls,
                     "mean_scenes_per_call": occupancy / calls if calls else 0.0,
                     "graph_captures": info.get("captures"), "graph_instantiations": info.get("instantiations")}}
     if lat.size:

@@ -4,13 +4,18 @@ with a stand-in batch that finishes a scene after its steps, each of its steps t
 `step_ms[rank]` milliseconds, so that a slower rank has its slots free less often."""
 import json
 import os
+import threading
 import time
 
 
 class FakeBatch:
+    """Admission comes from the serving loop's admission thread, the rest from its own: a lock
+    keeps the slots consistent, as the library's batch lock does."""
+
     def __init__(self, max_scenes: int, step_s: float):
         self.max_scenes, self.step_s = max_scenes, step_s
         self.slots: dict[int, list[int]] = {}
+        self.mu = threading.Lock()
 
     def __enter__(self):
         return self
@@ -19,24 +24,28 @@ class FakeBatch:
         pass
 
     def admit(self, world, steps):
-        if len(self.slots) >= self.max_scenes:
-            return None
-        k = min(set(range(self.max_scenes)) - set(self.slots))
-        self.slots[k] = [0, steps]
-        return k
+        with self.mu:
+            if len(self.slots) >= self.max_scenes:
+                return None
+            k = min(set(range(self.max_scenes)) - set(self.slots))
+            self.slots[k] = [0, steps]
+            return k
 
     def step(self, n):
         time.sleep(self.step_s)
-        for v in self.slots.values():
-            v[0] = min(v[0] + n, v[1])
-        return sum(1 for v in self.slots.values() if v[0] < v[1])
+        with self.mu:
+            for v in self.slots.values():
+                v[0] = min(v[0] + n, v[1])
+            return sum(1 for v in self.slots.values() if v[0] < v[1])
 
     def poll(self, k):
-        v = self.slots[k]
-        return {"finished": v[0] >= v[1], "steps_done": v[0]}
+        with self.mu:
+            v = self.slots[k]
+            return {"finished": v[0] >= v[1], "steps_done": v[0]}
 
     def retire(self, k):
-        del self.slots[k]
+        with self.mu:
+            del self.slots[k]
 
 
 def run(rank, port, n_requests, arrivals, step_ms, max_scenes, out_dir):
