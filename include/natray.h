@@ -468,7 +468,10 @@ NTR_API ntr_status ntr_sim_autotune(ntr_sim* s, uint32_t steps, ntr_tuning* best
  *                     hold on the device (0: no limit but the free memory)
  *   ntr_batch_admit   a world blob (ntr_world_build, ntr_sim_snapshot) into a free slot, to run
  *                     n_steps steps; NTR_E_BUSY when no slot is free or the scene's device memory
- *                     does not fit the budget or the free HBM (less a reserve): admit it later
+ *                     does not fit the budget or the free HBM (less a reserve): admit it later.
+ *                     From any thread, also while another thread's ntr_batch_step runs: the
+ *                     scene is created in a reserved slot outside the batch's lock, its uploads
+ *                     on the slot's own stream beside the step's work
  *   ntr_batch_step    n steps of every unfinished scene (fewer for a scene that reaches its
  *                     target); *active (may be NULL) = scenes that stepped
  *   ntr_batch_poll    a slot's state and progress
@@ -514,7 +517,9 @@ NTR_API ntr_status ntr_batch_info_get(ntr_batch* b, ntr_batch_info* out);
 NTR_API ntr_status ntr_world_device_bytes(const void* world_blob, size_t len, uint64_t* bytes);
 /* Admission from any thread. Every ntr_batch_* call holds the batch's lock, so calls from
  * several host threads take turns (a call waits at most for the one in progress, such as a
- * batch step). ntr_batch_enqueue checks the world blob, queues a copy and returns a ticket; the
+ * batch step), except that a batch step lets the lock go while it waits for the GPU, during
+ * which only ntr_batch_admit proceeds, and ntr_batch_admit holds it only to reserve a slot and
+ * to place the scene. ntr_batch_enqueue checks the world blob, queues a copy and returns a ticket; the
  * queued scenes are admitted in order at the start of the next ntr_batch_step, as far as slots
  * and memory allow (a scene that does not fit yet stays at the head of the queue).
  * ntr_batch_ticket gives the ticket's slot once admitted, NTR_BATCH_MAX while it waits, and
