@@ -372,6 +372,7 @@ def cpu_baseline(sample_steps: int, threads: int | None = None, warmup: int = 1)
     n = o.step(sample_steps)
     dt = time.perf_counter() - t0
     return {"value": w.h.n_particles * n / dt, "unit": "particle-substeps/s", "cores": nthreads(), "kind": "port",
+            "n_particles": int(w.h.n_particles),
             "sample": f"steps {max(warmup, 1) + 1}-{max(warmup, 1) + n} of the 1M-particle scene (after {max(warmup, 1)} untimed "
                       f"steps), oracle FP32 with the reference's FP32 sums, OpenMP; the scene built by the library's CPU "
                       f"scene builder before timing"}
@@ -439,7 +440,7 @@ def main():
         line = {"metric": METRIC, "value": cb["value"], "unit": "particle-substeps/s", "n_gpus": args.gpus, "steps": steps,
                 "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded scene builder of the reference)", "impl": "reference",
-                "config": {"workload": WORKLOAD, "parallelism": "host cores", "n_particles": None},
+                "config": {"workload": WORKLOAD, "parallelism": "host cores", "n_particles": cb["n_particles"]},
                 "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "particle-substeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                 "note": "the reference's wgpu/WGSL step needs a graphics adapter (none on this box, no Rust toolchain); this is the C++ restatement of its step kernels"}
         print(json.dumps(line), flush=True)
