@@ -387,7 +387,7 @@ def batch_and_serve(args) -> dict:
     out = {}
     if args.batch_scenes:
         ws = sv.build_worlds(sv.mixed_scenes(args.batch_scenes, 7))
-        b = sv.run_batched(ws, args.batch_steps, args.batch_chunk, max_scenes=max(64, args.batch_scenes))
+        b = sv.run_batched(ws, args.batch_steps, args.batch_chunk, max_scenes=max(64, args.batch_scenes), tune_steps=args.batch_tune)
         q = sv.run_sequential(ws, args.batch_steps, args.batch_chunk)
         out["batched"] = {
             "workload": f"{len(ws)} scenes, particles log-uniform 16k-512k (seeded; {sum(w.h.n_particles for w in ws)} in all), "
@@ -396,7 +396,9 @@ def batch_and_serve(args) -> dict:
             "scenes_per_s": b["scenes_per_s"], "particle_steps_per_s": b["particle_steps_per_s"], "seconds": b["seconds"],
             "sequential_scenes_per_s": q["scenes_per_s"], "sequential_seconds": q["seconds"],
             "speedup_vs_sequential": q["seconds"] / b["seconds"], "chunk": args.batch_chunk, "calls": b["calls"],
-            "graph_captures": b["graph_captures"], "graph_instantiations": b["graph_instantiations"]}
+            "graph_captures": b["graph_captures"], "graph_instantiations": b["graph_instantiations"],
+            "tuning": b["tuning"], "tuning_note": "launch shapes chosen by the batch autotuner on a throwaway batch of the same scenes"
+                                                  if b["tuning"] else "default launch shapes"}
     if args.serve_requests:
         from natray_b200 import build_world
         ps = sv.mixed_scenes(args.serve_requests, 11, lo=16_000, hi=2_000_000, lognormal_median=128_000)
@@ -424,6 +426,7 @@ def main():
     ap.add_argument("--batch-scenes", type=int, default=64, help="scenes of the batched run (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=500)
     ap.add_argument("--batch-chunk", type=int, default=8, help="steps per batch call (state read back between)")
+    ap.add_argument("--batch-tune", type=int, default=4, help="timed steps per autotuner candidate before the batched run (0: default shapes)")
     ap.add_argument("--serve-requests", type=int, default=200, help="requests of the serving loop (0: skip)")
     ap.add_argument("--serve-steps", type=int, default=200)
     ap.add_argument("--serve-rate", type=float, default=15.0, help="request arrivals per second")

@@ -512,6 +512,15 @@ NTR_API ntr_status ntr_batch_poll(ntr_batch* b, uint32_t slot, ntr_batch_slot* o
 NTR_API ntr_status ntr_batch_snapshot(ntr_batch* b, uint32_t slot, void* buf, size_t cap, size_t* len);
 NTR_API ntr_status ntr_batch_retire(ntr_batch* b, uint32_t slot);
 NTR_API ntr_status ntr_batch_info_get(ntr_batch* b, ntr_batch_info* out);
+/* The batch's launch shapes (ntr_tuning: the per-SM caps of every scene's cell and transfer
+ * kernel grids, and the CTAs of the joint solve, at least one per scene; zero fields take the
+ * defaults), for every scene in it and every scene it admits; a scene's results do not depend
+ * on them. ntr_batch_autotune searches them as ntr_sim_autotune does, on the batch's own scenes:
+ * one untimed and `steps` timed batch steps per candidate, which are steps of the scenes (they
+ * are not put back), and keeps the fastest. */
+NTR_API ntr_status ntr_batch_set_tuning(ntr_batch* b, const ntr_tuning* t);
+NTR_API ntr_status ntr_batch_get_tuning(ntr_batch* b, ntr_tuning* out);
+NTR_API ntr_status ntr_batch_autotune(ntr_batch* b, uint32_t steps, ntr_tuning* best, double* best_ms_per_step);
 /* The device memory a simulation of this world takes (what admission to a batch checks against
  * its budget and the free memory; a server placing scenes on GPUs uses it). CPU only. */
 NTR_API ntr_status ntr_world_device_bytes(const void* world_blob, size_t len, uint64_t* bytes);

@@ -207,6 +207,9 @@ _SIGS = {
     "ntr_sim_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "ntr_sim_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "ntr_sim_autotune": (C.c_int, [_P, C.c_uint32, C.POINTER(Tuning), C.POINTER(C.c_double)]),
+    "ntr_batch_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "ntr_batch_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "ntr_batch_autotune": (C.c_int, [_P, C.c_uint32, C.POINTER(Tuning), C.POINTER(C.c_double)]),
     "ntr_batch_create": (C.c_int, [C.c_int, C.c_uint32, C.c_uint64, C.POINTER(_P)]),
     "ntr_batch_destroy": (C.c_int, [_P]),
     "ntr_batch_admit": (C.c_int, [_P, _P, C.c_size_t, C.c_uint32, C.POINTER(C.c_uint32)]),

@@ -106,5 +106,24 @@ class Batch:
         check(lib().ntr_batch_info_get(self._h, C.byref(i)))
         return {k: getattr(i, k) for k, _ in i._fields_ if k != "pad"}
 
+    @property
+    def tuning(self) -> dict:
+        """The launch shapes of every scene's grids and of the joint solve."""
+        t = _abi.Tuning()
+        check(lib().ntr_batch_get_tuning(self._h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in t._fields_ if k != "pad"}
+
+    @tuning.setter
+    def tuning(self, v: dict) -> None:
+        t = _abi.Tuning(**{k: int(x) for k, x in v.items()})
+        check(lib().ntr_batch_set_tuning(self._h, C.byref(t)))
+
+    def autotune(self, steps: int = 4) -> tuple[dict, float]:
+        """Times candidate launch shapes on the batch's scenes (the tuning steps are steps of
+        theirs) and keeps the fastest; returns it and its ms per batch step."""
+        t, ms = _abi.Tuning(), C.c_double()
+        check(lib().ntr_batch_autotune(self._h, steps, C.byref(t), C.byref(ms)))
+        return {k: getattr(t, k) for k, _ in t._fields_ if k != "pad"}, ms.value
+
 
 __all__ = ["Batch", "NatrayError"]

@@ -85,7 +85,10 @@ struct Batch {
     uint64_t reserve = 0;  // free device memory that admission leaves
     uint64_t held = 0;
     uint64_t steps = 0;
-    uint32_t ctas = 0;  // CTAs of the joint solve
+    uint32_t ctas = 0;  // CTAs of the joint solve (every co-resident one)
+    // Launch shapes of every scene's grids and the joint solve (ntr_batch_set_tuning): the
+    // per-SM caps of the cell and transfer kernels, and the joint solve's CTAs (0: all).
+    ntr_tuning tune{0u, 8u, 8u, 0u};
     std::vector<BatchSlot> slots;
     cudaStream_t solve_stream = nullptr;  // the batch step's main stream
     cudaStream_t aux = nullptr, aux2 = nullptr;  // its side streams (as a one-scene step's)
@@ -266,6 +269,7 @@ static ntr_status batch_admit(Batch& B, const void* blob, size_t len, uint32_t n
     BatchSlot& sl = B.slots[k];
     Sim* s = nullptr;
     if ((r = create_from(w, B.device, s, sl.arena, sl.arena_cap, sl.h_state, &sl.hs)) != NTR_OK) return r;
+    s->tune = B.tune;
     sl.sim.reset(s);
     sl.target = n_steps;
     sl.done = 0;
@@ -297,6 +301,7 @@ static ntr_status batch_admit_overlapped(Batch& B, const void* blob, size_t len,
     std::lock_guard<std::mutex> lk(B.mu);
     sl.reserved = false;
     if (r != NTR_OK) return r;
+    s->tune = B.tune;
     sl.sim.reset(s);
     sl.target = n_steps;
     sl.done = 0;
@@ -390,7 +395,9 @@ static uint64_t enqueue_step_multi(Batch& B, uint32_t n_jobs, const uint32_t* to
     LM(k_bullet_apply_m, GK_CELL, 256, s);
     // Every scene's grid barrier counter starts from zero (k_solve_batch keeps one per scene).
     LM(k_solve_reset_m, GK_ONE, 32, s);
-    nl += enqueue_solve(S0, s, B.d_jobs, n_jobs, fp64, prof, B.ctas);
+    // Every scene needs a CTA of the joint solve.
+    const uint32_t solve_ctas = B.tune.solve_ctas ? std::min(B.ctas, std::max(B.tune.solve_ctas, n_jobs)) : B.ctas;
+    nl += enqueue_solve(S0, s, B.d_jobs, n_jobs, fp64, prof, solve_ctas);
     LM(k_project_m, GK_CELL, 256, s);
     LM(k_extend_1_m, GK_CELL, 256, s);
     LM(k_extend_2_m, GK_CELL, 256, s);
@@ -478,7 +485,7 @@ static ntr_status batch_step(Batch& B, uint32_t n, uint32_t& active, Prof* prof 
         key.push_back(S.size_class);
     }
     for (int k = 0; k < GK_COUNT; k++) first[(size_t)k * (B.max_scenes + 1) + n_jobs] = tot[k];
-    key.insert(key.end(), {n_jobs, fp64, max_shots, n_mem, n_air});
+    key.insert(key.end(), {n_jobs, fp64, max_shots, n_mem, n_air, B.tune.cell_ctas_per_sm, B.tune.block_ctas_per_sm, B.tune.solve_ctas});
     CU(cudaMemcpyAsync(B.d_stage, B.h_stage, B.off_in + sizeof(BatchJobIn) * n_jobs, cudaMemcpyHostToDevice, s));
     k_batch_begin<<<n_jobs, 64, 0, s>>>(B.d_jobs, B.d_in);
     CU(cudaGetLastError());

@@ -1518,6 +1518,82 @@ NTR_API ntr_status ntr_batch_retire(ntr_batch* batch, uint32_t slot) {
     return batch_retire(B, slot);
 }
 
+NTR_API ntr_status ntr_batch_set_tuning(ntr_batch* batch, const ntr_tuning* t) {
+    BGUARD(batch);
+    if (!t) return fail(NTR_E_INVALID, "null argument");
+    ntr_tuning n = *t;
+    if (n.solve_ctas > B.ctas) return fail(NTR_E_INVALID, "solve_ctas is at most " + std::to_string(B.ctas) + " (co-resident) on this device");
+    if (n.cell_ctas_per_sm > 64 || n.block_ctas_per_sm > 64) return fail(NTR_E_INVALID, "at most 64 CTAs per SM");
+    if (!n.cell_ctas_per_sm) n.cell_ctas_per_sm = 8;
+    if (!n.block_ctas_per_sm) n.block_ctas_per_sm = 8;
+    n.pad = 0;
+    B.tune = n;
+    for (auto& sl : B.slots)
+        if (sl.sim) sl.sim->tune = n;
+    return NTR_OK;  // the step graph is captured again at the next step (the shapes are in its key)
+}
+
+NTR_API ntr_status ntr_batch_get_tuning(ntr_batch* batch, ntr_tuning* out) {
+    BGUARD(batch);
+    if (!out) return fail(NTR_E_INVALID, "null argument");
+    *out = B.tune;
+    if (!out->solve_ctas) out->solve_ctas = B.ctas;
+    return NTR_OK;
+}
+
+// A coordinate search over the batch's launch shapes, as ntr_sim_autotune's, on the batch's own
+// scenes: each candidate takes one untimed batch step (its graph) and `steps` timed ones. The
+// scenes are not put back: the tuning steps are steps of theirs (the results do not depend on
+// the shapes). The batch keeps the fastest.
+NTR_API ntr_status ntr_batch_autotune(ntr_batch* batch, uint32_t steps, ntr_tuning* best, double* best_ms) {
+    if (!batch || !batch->b) return fail(NTR_E_INVALID, "null batch handle");
+    if (steps == 0) return fail(NTR_E_INVALID, "steps must be positive");
+    Batch& B = *batch->b;
+    ntr_tuning cur;
+    ntr_status r = ntr_batch_get_tuning(batch, &cur);
+    if (r != NTR_OK) return r;
+    auto trial = [&](const ntr_tuning& t, double& ms) -> ntr_status {
+        ntr_status q;
+        if ((q = ntr_batch_set_tuning(batch, &t)) != NTR_OK) return q;
+        uint32_t active = 0;
+        if ((q = ntr_batch_step(batch, 1, &active)) != NTR_OK) return q;
+        const auto t0 = std::chrono::steady_clock::now();
+        if ((q = ntr_batch_step(batch, steps, &active)) != NTR_OK) return q;
+        ms = active ? std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count() / steps : 1e300;
+        return NTR_OK;
+    };
+    double cur_ms = 1e300;
+    if ((r = trial(cur, cur_ms)) != NTR_OK) return r;
+    const uint32_t blocks[] = {4, 6, 12, 16}, cells[] = {4, 6, 12, 16};
+    const uint32_t solves[] = {B.ctas * 7 / 8, B.ctas * 3 / 4, B.ctas / 2};
+    for (uint32_t v : blocks) {
+        ntr_tuning t = cur;
+        t.block_ctas_per_sm = v;
+        double ms;
+        if ((r = trial(t, ms)) != NTR_OK) return r;
+        if (ms < cur_ms) cur = t, cur_ms = ms;
+    }
+    for (uint32_t v : cells) {
+        ntr_tuning t = cur;
+        t.cell_ctas_per_sm = v;
+        double ms;
+        if ((r = trial(t, ms)) != NTR_OK) return r;
+        if (ms < cur_ms) cur = t, cur_ms = ms;
+    }
+    for (uint32_t v : solves) {
+        if (v == 0) continue;
+        ntr_tuning t = cur;
+        t.solve_ctas = v;
+        double ms;
+        if ((r = trial(t, ms)) != NTR_OK) return r;
+        if (ms < cur_ms) cur = t, cur_ms = ms;
+    }
+    if ((r = ntr_batch_set_tuning(batch, &cur)) != NTR_OK) return r;
+    if (best) *best = cur;
+    if (best_ms) *best_ms = cur_ms;
+    return NTR_OK;
+}
+
 NTR_API ntr_status ntr_batch_info_get(ntr_batch* batch, ntr_batch_info* out) {
     BGUARD(batch);
     if (!out) return fail(NTR_E_INVALID, "null argument");

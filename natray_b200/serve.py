@@ -54,9 +54,19 @@ def build_worlds(params: list[Params], threads: int = 16) -> list[World]:
         return list(ex.map(build_world, params))
 
 
-def run_batched(worlds: list[World], steps: int, chunk: int = 4, max_scenes: int = 64) -> dict:
-    """All scenes admitted into one batch and stepped together to `steps` steps each."""
+def run_batched(worlds: list[World], steps: int, chunk: int = 4, max_scenes: int = 64, tune_steps: int = 0) -> dict:
+    """All scenes admitted into one batch and stepped together to `steps` steps each. With
+    `tune_steps`, the launch shapes are first chosen by the batch autotuner on a throwaway batch
+    of the same scenes (its tuning steps are not part of the timed run)."""
+    tuning = None
+    if tune_steps:
+        with Batch(max_scenes=max_scenes) as tb:
+            for w in worlds:
+                tb.admit(w, 1 << 30)
+            tuning, _ = tb.autotune(tune_steps)
     with Batch(max_scenes=max_scenes) as b:
+        if tuning:
+            b.tuning = tuning
         slots = [b.admit(w, steps) for w in worlds]
         if None in slots:
             raise RuntimeError("the batch could not hold every scene")
@@ -69,7 +79,7 @@ def run_batched(worlds: list[World], steps: int, chunk: int = 4, max_scenes: int
         info = b.info()
     n_ps = sum(w.h.n_particles * d for w, d in zip(worlds, done))
     return {"seconds": wall, "scenes_per_s": len(worlds) / wall, "particle_steps_per_s": n_ps / wall, "calls": calls,
-            "graph_captures": info["captures"], "graph_instantiations": info["instantiations"]}
+            "graph_captures": info["captures"], "graph_instantiations": info["instantiations"], "tuning": tuning}
 
 
 def run_sequential(worlds, steps: int, chunk: int = 4, build=None) -> dict:

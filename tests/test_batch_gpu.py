@@ -160,3 +160,28 @@ def test_queue_from_other_threads(worlds):
     for k, r in got.items():
         d = first_difference(solo(worlds[k], 8, 4), r)
         assert d is None, f"scene {k}: {d}"
+
+
+def test_launch_shapes_do_not_change_results(worlds):
+    # The same scenes and calls under the default shapes, under odd ones (3 and 5 CTAs an SM,
+    # the joint solve on one CTA a scene) and after the autotuner's search: the same bits.
+    targets = [12, 8, 16]
+    runs = []
+    for tuning in (None, {"cell_ctas_per_sm": 3, "block_ctas_per_sm": 5, "solve_ctas": 3}):
+        with Batch(max_scenes=4) as b:
+            if tuning:
+                b.tuning = tuning
+                got = b.tuning
+                assert (got["cell_ctas_per_sm"], got["block_ctas_per_sm"], got["solve_ctas"]) == (3, 5, 3)
+            slots = [b.admit(w, t) for w, t in zip(worlds, targets)]
+            while b.step(4):
+                pass
+            runs.append([b.snapshot(sl) for sl in slots])
+    for a, c in zip(*runs):
+        assert first_difference(a, c) is None
+    with Batch(max_scenes=4) as b:
+        slots = [b.admit(w, 200) for w in worlds]
+        best, ms = b.autotune(steps=2)
+        assert ms > 0 and 1 <= best["cell_ctas_per_sm"] <= 64 and 1 <= best["block_ctas_per_sm"] <= 64
+        assert best["solve_ctas"] >= 3 and b.tuning == best
+        assert all(b.poll(sl)["steps_done"] == 12 * 3 for sl in slots)  # 12 candidates, 1 + 2 steps each
