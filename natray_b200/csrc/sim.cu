@@ -87,6 +87,7 @@ struct Sim {
     size_t device_bytes = 0;
     DevState* h_state = nullptr;  // pinned
     bool own_h_state = true;      // false: a batch slot's, kept across its scenes
+    ntr_gpu_params* h_params = nullptr;  // pinned staging of the parameters a step call uploads
     std::map<GraphKey, StepGraph> graphs;
     uint64_t last_launches = 0;
     double last_ms = 0.0;
@@ -96,7 +97,7 @@ struct Sim {
     uint32_t batch_steps = 0;  // ntr_sim_set_batch_steps: fixed steps per ntr_sim_advance batch (0: by time)
     uint32_t fp64 = 1;
     ntr_tuning tune{0u, 8u, 8u, 0u};  // launch shapes (ntr_sim_set_tuning)
-    bool own_streams = true;  // false: the streams and events are a batch slot's, kept across its scenes
+    bool own_streams = true;  // false: the streams, events and h_params are a batch slot's, kept across its scenes
 
     ~Sim() {
         DeviceScope scope(device);
@@ -111,6 +112,7 @@ struct Sim {
         for (cudaEvent_t e : ev_sub)
             if (e) cudaEventDestroy(e);
         if (!own_streams) return;
+        if (h_params) cudaFreeHost(h_params);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         for (int k = 0; k < 3; k++) {
@@ -415,8 +417,11 @@ static ntr_status upload_static(Sim& S, const World& w) {
     return NTR_OK;
 }
 
+// The parameters of a step call, through a pinned buffer so that the copy is an asynchronous
+// DMA (the call before has read its state back, so the buffer is free).
 static ntr_status push_params(Sim& S) {
-    CU(cudaMemcpyAsync((void*)S.D.U, &S.U, sizeof(ntr_gpu_params), cudaMemcpyHostToDevice, S.stream));
+    *S.h_params = S.U;
+    CU(cudaMemcpyAsync((void*)S.D.U, S.h_params, sizeof(ntr_gpu_params), cudaMemcpyHostToDevice, S.stream));
     return NTR_OK;
 }
 
@@ -749,8 +754,10 @@ static ntr_status run_batch(Sim& S, uint32_t n, uint32_t stop, uint32_t* taken, 
 struct SimHandles {
     cudaStream_t stream = nullptr, aux = nullptr, aux2 = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_fork[3] = {nullptr, nullptr, nullptr}, ev_join[3] = {nullptr, nullptr, nullptr};
+    ntr_gpu_params* h_params = nullptr;
 };
 static ntr_status make_handles(SimHandles& h) {
+    CU(cudaMallocHost((void**)&h.h_params, sizeof(ntr_gpu_params)));
     CU(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
     CU(cudaStreamCreateWithFlags(&h.aux, cudaStreamNonBlocking));
     CU(cudaStreamCreateWithFlags(&h.aux2, cudaStreamNonBlocking));
@@ -763,6 +770,7 @@ static ntr_status make_handles(SimHandles& h) {
     return NTR_OK;
 }
 static void free_handles(SimHandles& h) {
+    if (h.h_params) cudaFreeHost(h.h_params);
     if (h.ev0) cudaEventDestroy(h.ev0);
     if (h.ev1) cudaEventDestroy(h.ev1);
     for (int k = 0; k < 3; k++) {
@@ -800,7 +808,7 @@ static ntr_status create_from(const World& w, int device, Sim*& out, uint8_t* ar
         free_handles(hs);
         return r;
     }
-    S->stream = hs.stream, S->aux = hs.aux, S->aux2 = hs.aux2, S->ev0 = hs.ev0, S->ev1 = hs.ev1;
+    S->stream = hs.stream, S->aux = hs.aux, S->aux2 = hs.aux2, S->ev0 = hs.ev0, S->ev1 = hs.ev1, S->h_params = hs.h_params;
     for (int k = 0; k < 3; k++) S->ev_fork[k] = hs.ev_fork[k], S->ev_join[k] = hs.ev_join[k];
     if (h_state)
         S->h_state = h_state, S->own_h_state = false;
