@@ -185,3 +185,33 @@ def test_launch_shapes_do_not_change_results(worlds):
         assert ms > 0 and 1 <= best["cell_ctas_per_sm"] <= 64 and 1 <= best["block_ctas_per_sm"] <= 64
         assert best["solve_ctas"] >= 3 and b.tuning == best
         assert all(b.poll(sl)["steps_done"] == 12 * 3 for sl in slots)  # 12 candidates, 1 + 2 steps each
+
+
+def test_admission_beside_a_running_step(worlds):
+    # One scene steps while another thread admits the other two (ntr_batch_admit lets the
+    # step run: it creates the scene outside the batch's lock); every scene still ends as alone.
+    import threading
+    import time
+    targets = [40, 12, 16]
+    with Batch(max_scenes=4) as b:
+        slots = {0: b.admit(worlds[0], targets[0])}
+
+        def admit_rest():
+            for k in (1, 2):
+                time.sleep(0.01)
+                slots[k] = b.admit(worlds[k], targets[k])
+
+        th = threading.Thread(target=admit_rest)
+        th.start()
+        while True:
+            active = b.step(4)
+            if not active and not th.is_alive():
+                break
+        th.join()
+        while b.step(4):
+            pass
+        for k, (w, t) in enumerate(zip(worlds, targets)):
+            p = b.poll(slots[k])
+            assert p["finished"] and p["steps_done"] == t
+            d = first_difference(solo(w, t, 4), b.snapshot(slots[k]))
+            assert d is None, f"scene {k}: {d}"
