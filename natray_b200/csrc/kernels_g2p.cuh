@@ -159,6 +159,42 @@ __device__ __forceinline__ void g2p_stage(const Dev& D, uint32_t b, uint32_t* li
     cp_async_commit();
 }
 
+// The break-ups of one segment of a block's particles (sorted positions seg .. seg + G2P_SEG),
+// written at their own positions and flagged in `bits`, moved to their ranks: after the block's
+// earlier ones (`brk`), in sorted order. One warp moves them a word (up to 32) at a time in
+// ascending order, so a move never lands on a break-up still to be moved (a rank is at most its
+// position, and the positions still to come are above it). `any`: this thread flagged one in the
+// segment. Every thread of the CTA calls it (it has barriers).
+constexpr uint32_t G2P_SEG = 1024;
+__device__ __forceinline__ void g2p_rank_breakups(const Dev& D, uint32_t first, uint32_t seg, uint32_t* bits, uint32_t& brk,
+                                                  bool any, uint32_t warp, uint32_t lane) {
+    if (!__syncthreads_or(any)) return;  // most segments have none
+    if (warp == 0) {
+        uint32_t n = brk;
+        for (uint32_t w0 = 0; w0 < G2P_SEG / 32; w0++) {
+            const uint32_t word = bits[w0];
+            if (!word) continue;
+            const uint32_t cnt = (uint32_t)__popc(word);
+            const uint32_t at = lane < cnt ? (uint32_t)__fns(word, 0u, (int)lane + 1) : 0u;
+            float4 x = make_float4(0.0f, 0.0f, 0.0f, 0.0f), v = x;
+            if (lane < cnt) {
+                x = D.brk_x[first + seg + w0 * 32u + at];
+                v = D.brk_v[first + seg + w0 * 32u + at];
+            }
+            __syncwarp();
+            if (lane < cnt) {
+                D.brk_x[first + n + lane] = x;
+                D.brk_v[first + n + lane] = v;
+            }
+            __syncwarp();
+            n += cnt;
+            bits[w0] = 0u;
+        }
+        if (lane == 0) brk = n;
+    }
+    __syncthreads();
+}
+
 // G2P_T threads a CTA, 768 / G2P_T CTAs an SM. With many blocks (the 1M-particle scene: 128
 // threads, six CTAs an SM) a block's few hundred particles take 3 rounds with a short last one,
 // and the SM has more CTAs to switch to while one waits on its loads or barriers. With few
@@ -184,7 +220,7 @@ __device__ __forceinline__ void g2p_body(const Dev& D, const CT& C) {
     __shared__ uint32_t raw_cov[64];
     __shared__ uint32_t s_links[2][27];       // the current block's neighbours, and the next's
     __shared__ uint8_t s_cov[64];  // the block's own cells: rubber over them (A_MA > 0)
-    __shared__ uint32_t s_wcount[G2P_T / 32];
+    __shared__ uint32_t s_bits[G2P_SEG / 32];  // the segment's break-up flags, a bit per particle
     __shared__ uint32_t s_brk;
     float fastest = 0.0f;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -229,11 +265,14 @@ __device__ __forceinline__ void g2p_body(const Dev& D, const CT& C) {
         }
         if (threadIdx.x < 64) s_cov[threadIdx.x] = (int32_t)raw_cov[threadIdx.x] > 0 ? 1 : 0;
         if (threadIdx.x == 0) s_brk = 0;
+        for (uint32_t w = threadIdx.x; w < G2P_SEG / 32; w += G2P_T) s_bits[w] = 0u;
         __syncthreads();
         const uint32_t nxt = next_full(b + C.nx());
         if (nxt < nb) g2p_stage(D, nxt, s_links[cur ^ 1u], raw, raw_cov, G2P_T);
         const I3 corner = slot_coord(g, g.list[b]) * 4 - I3{1, 1, 1};
-        // Rounds of G2P_T particles keep the sorted order for ranking the break-ups.
+        // Rounds of G2P_T particles; the break-ups are ranked in sorted order per segment.
+        uint32_t seg = 0;
+        bool seg_any = false;
         for (uint32_t base = 0; base < count; base += G2P_T) {
             const uint32_t k = base + threadIdx.x;
             bool brk = false;
@@ -294,26 +333,20 @@ __device__ __forceinline__ void g2p_body(const Dev& D, const CT& C) {
                     fastest = mx(fastest, length(vv));
                 }
             }
-            // Rank this round's break-ups in sorted order and put them after the earlier ones
-            // (most rounds have none).
-            if (__syncthreads_or(brk)) {
-                uint32_t bal = __ballot_sync(0xffffffffu, brk);
-                if (lane == 0) s_wcount[warp] = __popc(bal);
-                __syncthreads();
-                uint32_t before = s_brk;
-                for (uint32_t w = 0; w < warp; w++) before += s_wcount[w];
-                if (brk) {
-                    uint32_t r = before + __popc(bal & ((1u << lane) - 1u));
-                    D.brk_x[first + r] = f4(bx, __uint_as_float(bid));
-                    D.brk_v[first + r] = f4(bv, 0.0f);
-                }
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    uint32_t t = 0;
-                    for (uint32_t w = 0; w < G2P_T / 32; w++) t += s_wcount[w];
-                    s_brk += t;
-                }
-                __syncthreads();
+            // A break-up goes to scratch at its own sorted position and is flagged, a bit per
+            // particle; the flags are ranked (in sorted order) a segment of G2P_SEG particles at a
+            // time, so that the rounds need no barrier.
+            const uint32_t bal = __ballot_sync(0xffffffffu, brk);
+            if (lane == 0) s_bits[((base - seg) >> 5) + warp] = bal;
+            if (brk) {
+                D.brk_x[first + k] = f4(bx, __uint_as_float(bid));
+                D.brk_v[first + k] = f4(bv, 0.0f);
+            }
+            seg_any = seg_any || brk;
+            if (base + G2P_T >= count || base + G2P_T - seg >= G2P_SEG) {
+                g2p_rank_breakups(D, first, seg, s_bits, s_brk, seg_any, warp, lane);
+                seg = base + G2P_T;
+                seg_any = false;
             }
         }
         if (threadIdx.x == 0) D.brk_count[b] = s_brk;
