@@ -6,7 +6,7 @@ step against these, so a change to any of them that alters a result shows up as 
     python tests/golden/make_golden.py
 
 The reference's own step has no recorded outputs to pin against (its tests cover the scene
-construction only); these are regression fixtures of this build's canonical form.
+construction only); these are regression fixtures of this library's canonical form.
 """
 from __future__ import annotations
 
