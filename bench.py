@@ -33,6 +33,9 @@ FALLBACK_HBM_GBS = 6650.0
 METRIC = "particle-substeps/s @1M"
 SCENE = dict(resolution=124, mesh_level=6, dt_max=2e-6, bullet=6, caliber=8, bullet_speed=350)
 WORKLOAD = "single scene 1M particles: d=16 cm balloon, res 124 (976,915 particles), icosphere(6) 81,920 tris, 8 mm steel sphere at 350 m/s, dt=2 us"
+# The small scene (d 8 cm, about 70k particles, 5,120 triangles, rubber 0.2 mm, 8 mm sphere at
+# 300 m/s), timed over its 200 fixed steps of 2 us.
+SMALL = dict(diameter=8, resolution=51, mesh_level=4, thickness=0.2, bullet=6, caliber=8, bullet_speed=300, dt_max=2e-6)
 
 
 def log(*a):
@@ -378,6 +381,33 @@ def cpu_baseline(sample_steps: int, threads: int | None = None, warmup: int = 1)
                       f"scene builder before timing"}
 
 
+def small_scene(steps: int = 200) -> dict:
+    """The small scene's 200 fixed steps: device-timed in one call (CUDA events), and end to end
+    with one ntr_sim_step call a step, after 5 warm-up steps of a separate simulation of it."""
+    from natray_b200 import Params, build_world
+    from natray_b200.sim import Sim
+    w = build_world(Params(**SMALL))
+    warm = Sim(world=w)
+    for _ in range(5):
+        warm.step(1)
+    warm.close()
+    s = Sim(world=w)
+    assert s.step(steps) == steps
+    _, ms = s.last_launches()
+    s.close()
+    s = Sim(world=w)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s.step(1)
+    e2e_s = time.perf_counter() - t0
+    s.close()
+    n = w.h.n_particles
+    return {"workload": f"small scene: d=8 cm balloon, res 51 ({n} particles), icosphere(4) 5,120 tris, rubber 0.2 mm, "
+                        f"8 mm steel sphere at 300 m/s, {steps} fixed steps of 2 us",
+            "particle_steps_per_s": n * steps / (ms * 1e-3), "ms_per_step": ms / steps,
+            "e2e_particle_steps_per_s": n * steps / e2e_s, "e2e_ms_per_step": e2e_s * 1e3 / steps}
+
+
 def batch_and_serve(args) -> dict:
     """The batched workload (many mixed scenes stepped together, against the same scenes one at a
     time) and the serving loop (Poisson arrivals, continuous batching, against one request at a
@@ -452,6 +482,7 @@ def main():
     res = run_native(args, rank, world, local)
     if rank == 0 and res is not None:
         if world == 1:
+            res["small"] = small_scene()
             res.update(batch_and_serve(args))
             res["cpu_baseline"] = cpu_baseline(args.cpu_sample, warmup=args.warmup)
         print(json.dumps(res), flush=True)
