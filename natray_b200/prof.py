@@ -26,13 +26,20 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--graph-steps", type=int, default=10)
     ap.add_argument("--speed", type=float, default=350.0)
+    ap.add_argument("--diameter", type=float, default=0.0, help="balloon diameter in cm (0: the scene default)")
+    ap.add_argument("--thickness", type=float, default=0.0, help="rubber thickness in mm (0: the scene default)")
     ap.add_argument("--keyframes", type=int, default=0)
     ap.add_argument("--batch", type=int, default=0, help="profile a batch of this many mixed scenes instead")
     args = ap.parse_args()
     if args.batch:
         return batch_profile(args)
+    extra = {}
+    if args.diameter:
+        extra["diameter"] = args.diameter
+    if args.thickness:
+        extra["thickness"] = args.thickness
     w = build_world(Params(resolution=args.resolution, mesh_level=args.mesh_level, dt_max=2e-6, bullet=6, caliber=8,
-                           bullet_speed=args.speed))
+                           bullet_speed=args.speed, **extra))
     s = Sim(world=w)
     s.step(args.warmup)
     n = s.step(args.graph_steps)
