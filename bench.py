@@ -302,6 +302,19 @@ def run_native(args, rank, world, local):
                 except ValueError:
                     pass
 
+    # P2G's limit is its shared-memory atomics: 216 lane additions a particle (4 lattices x 27
+    # nodes x value and weight), against the device's measured rate for them at their best.
+    atomics = None
+    if top.startswith("k_p2g"):
+        import ctypes as C
+        from natray_b200._abi import check, lib
+        peak_at = C.c_double()
+        check(lib().ntr_probe_shared_atomics(local, 16384, C.byref(peak_at)))
+        rate = 216.0 * n_particles / per_launch_s
+        atomics = {"achieved": rate, "peak": peak_at.value, "unit": "lane atomic adds/s", "frac": rate / peak_at.value,
+                   "per_launch": 216 * n_particles,
+                   "note": "peak: ntr_probe_shared_atomics, conflict-free adds in P2G's CTA shape on this GPU"}
+
     result = None
     if rank == 0:
         h2d = 192  # the Params uniform per call
@@ -338,7 +351,7 @@ def run_native(args, rank, world, local):
             "roofline": {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind, "traffic": traffic,
                          "traffic_source": traffic_src, "algorithmic_bytes_per_launch": alg,
-                         "launch_ms": per_launch_s * 1e3, "share": round(kms / tot, 4)},
+                         "launch_ms": per_launch_s * 1e3, "share": round(kms / tot, 4), "shared_atomics": atomics},
             "step_roofline": {"bound": "hbm", "achieved": step_bytes / t_dev / 1e9 * world, "peak": peak, "unit": "GB/s",
                               "frac": step_bytes / t_dev / 1e9 / peak, "peak_kind": peak_kind,
                               "algorithmic_bytes_per_step": step_bytes / max(work["steps"], 1), "work": work,

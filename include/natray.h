@@ -438,6 +438,11 @@ NTR_API ntr_status ntr_sim_pack_particles(ntr_sim* s, void* dst_device, size_t b
  * particle mass, out[5..7] = sum of positions. */
 NTR_API ntr_status ntr_sim_conservation(ntr_sim* s, double out[8]);
 
+/* The device's sustained rate of shared-memory atomic adds (lane additions per second) at their
+ * best, in P2G's CTA shape: the peak against which P2G, bound by its 216 such adds a particle,
+ * is measured. No counterpart in the reference. */
+NTR_API ntr_status ntr_probe_shared_atomics(int device, uint32_t iters, double* lane_atomics_per_s);
+
 /* --- Launch shapes and their autotuner ----------------------------------------------------
  * No counterpart in the reference (wgpu picks nothing of the kind). How many CTAs the step's
  * kernels use; the results do not depend on it, bit for bit. Zero fields take the defaults.

@@ -207,6 +207,7 @@ _SIGS = {
     "ntr_sim_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "ntr_sim_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "ntr_sim_autotune": (C.c_int, [_P, C.c_uint32, C.POINTER(Tuning), C.POINTER(C.c_double)]),
+    "ntr_probe_shared_atomics": (C.c_int, [C.c_int, C.c_uint32, C.POINTER(C.c_double)]),
     "ntr_batch_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "ntr_batch_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "ntr_batch_autotune": (C.c_int, [_P, C.c_uint32, C.POINTER(Tuning), C.POINTER(C.c_double)]),

@@ -1285,6 +1285,65 @@ NTR_API ntr_status ntr_sim_conservation(ntr_sim* sim, double out[8]) {
 
 }  // extern "C"
 
+// ---- the shared-memory atomic peak (ntr_probe_shared_atomics) -----------------------------------
+// P2G's limit is its shared-memory atomic adds. This kernel measures the rate the SMs sustain
+// for them at their best: P2G's CTA shape (256 threads, its tile's 15.2 KB of shared memory,
+// three CTAs an SM), every lane of a warp on its own bank and node, integer adds in a chain of
+// `iters` per lane whose sums are kept (so that none is optimised away).
+namespace ntr {
+__global__ void __launch_bounds__(256, 3) k_probe_shared_atomics(uint32_t iters, int32_t* out) {
+    __shared__ int32_t tile[8 * 476];
+    for (uint32_t t = threadIdx.x; t < 8 * 476; t += blockDim.x) tile[t] = 0;
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    int32_t* mine = tile + (warp * 32u) % (8u * 476u - 32u) + lane;
+    for (uint32_t k = 0; k < iters; k++) {
+        atomicAdd(mine, (int32_t)k);
+        atomicAdd(mine + 256, (int32_t)(k ^ lane));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int32_t sum = 0;
+        for (uint32_t t = 0; t < 8 * 476; t++) sum += tile[t];
+        out[blockIdx.x] = sum;
+    }
+}
+}  // namespace ntr
+
+extern "C" NTR_API ntr_status ntr_probe_shared_atomics(int device, uint32_t iters, double* lane_atomics_per_s) {
+    using namespace ntr;
+    if (!lane_atomics_per_s || iters == 0) return fail(NTR_E_INVALID, "null argument or no iterations");
+    ntr_status r = check_device(device);
+    if (r != NTR_OK) return r;
+    DeviceScope scope(device);
+    if (!scope.ok) return fail(NTR_E_CUDA, "cudaSetDevice failed");
+    DevFacts f;
+    if ((r = device_facts(device, f)) != NTR_OK) return r;
+    const uint32_t grid = (uint32_t)f.sms * 3u;
+    int32_t* out = nullptr;
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CU(cudaMallocAsync((void**)&out, sizeof(int32_t) * grid, s));
+    CU(cudaEventCreate(&e0));
+    CU(cudaEventCreate(&e1));
+    k_probe_shared_atomics<<<grid, 256, 0, s>>>(iters, out);  // warm-up
+    CU(cudaEventRecord(e0, s));
+    k_probe_shared_atomics<<<grid, 256, 0, s>>>(iters, out);
+    CU(cudaEventRecord(e1, s));
+    CU(cudaGetLastError());
+    CU(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    CU(cudaEventElapsedTime(&ms, e0, e1));
+    cudaFreeAsync(out, s);
+    cudaStreamSynchronize(s);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    *lane_atomics_per_s = (double)grid * 256.0 * 2.0 * iters / (ms * 1e-3);
+    return NTR_OK;
+}
+
 // ---- sorting by block without allocating (ntr_sort_by_block_noalloc) --------------------------
 // For callers that cannot allocate device memory (a framework that has reserved the GPU's
 // memory for its own pool, a frame loop that must not make the device-wide synchronising
