@@ -612,6 +612,7 @@ constexpr int P2G_T = 256;
 // 16, 24, z 0-3), where the packed strides put pairs of them in one bank.
 constexpr uint32_t TPX = 68, TPY = 8, TPF = 7 * TPX;
 
+static_assert(FP_M == 65536.0f && FP_P == 65536.0f && FP_W == 16777216.0f, "splat's fused rounding needs power-of-two scales");
 __device__ __forceinline__ void splat(int32_t* tile, V3 x, V3 o, I3 corner, uint32_t fa, float val, V3 grad, uint32_t fw, float scale, float hh) {
     I3 base = vi(vfloor(x - o - 0.5f));
     V3 fx = x - o - vf(base);
@@ -634,8 +635,11 @@ __device__ __forceinline__ void splat(int32_t* tile, V3 x, V3 o, I3 corner, uint
                     float weight = wx[a] * wy[b] * wz[c];
                     uint32_t tt = t0 + a * TPX + b * TPY + c;
                     float node = val + dot(hg, v3((float)a, (float)b, (float)c) - fx);
-                    atomicAdd(&tile[fa * TPF + tt], fp_round(__fmul_rn(weight * node, scale)));
-                    atomicAdd(&tile[fw * TPF + tt], fp_round_pos(__fmul_rn(weight, FP_W)));
+                    // The scales are powers of two (FP_M, FP_P, FP_W), so the scaling is exact and
+                    // one fused multiply-add with the rounding constant rounds once, as the add
+                    // after the multiply does: fp_round(x * scale) in one instruction fewer.
+                    atomicAdd(&tile[fa * TPF + tt], __float_as_int(__fmaf_rn(weight * node, scale, 12582912.0f)) - 0x4B400000);
+                    atomicAdd(&tile[fw * TPF + tt], __float_as_int(__fmaf_rn(weight, FP_W, 8388608.0f)) - 0x4B000000);
                 }
     } else {
 #pragma unroll 1
