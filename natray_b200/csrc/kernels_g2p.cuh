@@ -63,10 +63,12 @@ __device__ __forceinline__ void ground_touch(const Dev& D, V3 p, float now) {
     atomicMin(D.touch + (size_t)cz * res + cx, __float_as_uint(now));
 }
 
-__device__ void carve(const Dev& D, V3& x, V3& v, uint32_t id, float t, float hh, uint32_t step_no) {
+// `reach`: the bullets' reach spheres (DBullet::reach), `n_shots` of them, read once per CTA.
+__device__ void carve(const Dev& D, const float4* reach_of, uint32_t n_shots, V3& x, V3& v, uint32_t id, float t, float hh,
+                      uint32_t step_no) {
     const float hand2 = R_HAND * R_HAND * hh * hh;
-    for (uint32_t bi = 0; bi < D.U->mem[3]; bi++) {
-        float4 reach = D.bullets[bi].reach;
+    for (uint32_t bi = 0; bi < n_shots; bi++) {
+        const float4 reach = reach_of[bi];
         if (reach.w <= 0.0f || distance(x, xyz(reach)) > reach.w) continue;
         for (uint32_t k = 0; k < NTR_N_SEC; k++) {
             const DSection s = D.sections[bi * NTR_N_SEC + k];
@@ -222,6 +224,9 @@ __device__ __forceinline__ void g2p_body(const Dev& D, const CT& C) {
     __shared__ uint8_t s_cov[64];  // the block's own cells: rubber over them (A_MA > 0)
     __shared__ uint32_t s_bits[G2P_SEG / 32];  // the segment's break-up flags, a bit per particle
     __shared__ uint32_t s_brk;
+    __shared__ float4 s_reach[NTR_MAX_SHOTS];
+    const uint32_t n_shots = min(U->mem[3], (uint32_t)NTR_MAX_SHOTS);
+    if (threadIdx.x < n_shots) s_reach[threadIdx.x] = D.bullets[threadIdx.x].reach;  // barriers follow before its use
     float fastest = 0.0f;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     // The CTA's blocks that hold particles, in turn (an empty one only gets its count of break-ups).
@@ -295,7 +300,7 @@ __device__ __forceinline__ void g2p_body(const Dev& D, const CT& C) {
                 V3 v = {gu.s, gv.s, gw.s};
                 float m_near = gu.w + gv.w + gw.w;
                 V3 x = xyz(pos) + step * v;
-                if (U->mem[3] > 0u) carve(D, x, v, i, now, hh, step_no);
+                if (n_shots > 0u) carve(D, s_reach, n_shots, x, v, i, now, hh, step_no);
                 bool escaped = x.x < lo.x || x.z < lo.z || x.x > hi.x || x.z > hi.z || x.y > hi.y;
                 float fill = m_near / 24.0f;
                 bool on_ground = x.y < 1.5f * spacing;
