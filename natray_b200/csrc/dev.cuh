@@ -91,7 +91,9 @@ struct DevState {
     uint32_t err;        // bit 0: a bounded grid barrier gave up
     uint32_t bar_count;  // grid barrier of the persistent solver: arrivals (reset per launch)
     uint32_t iters_prev;  // the last solve's iterations, kept for a joint solve's split (k_solve_reset_m)
-    uint32_t pad[3];
+    // The next block P2G (0) and G2P (1) hand out in a one-scene launch, zeroed by k_begin_step.
+    uint32_t next_block[2];
+    uint32_t pad;
     // The step's work, for its algorithmic bytes: this step's water and free-gas cells (counted
     // by k_project), and totals since ntr_sim_work last cleared them (added by the step's last
     // kernel): NTR_WORK_STEPS .. NTR_WORK_SPRAY of include/natray.h.
@@ -160,12 +162,16 @@ struct Dev {
 // that the same body runs in a launch for one scene (HwCta: the hardware's indices, read where
 // used) and in one launch for many scenes (Cta: a batch, where each scene owns a contiguous
 // range of the launch's CTAs).
+// A CTA of a one-scene launch. `dynamic`: the per-block kernels may hand their blocks out from
+// a counter (a many-scene launch's CTAs are tied to their scenes' blocks).
 struct HwCta {
+    static constexpr bool dynamic = true;
     __device__ __forceinline__ uint32_t x() const { return blockIdx.x; }
     __device__ __forceinline__ uint32_t nx() const { return gridDim.x; }
     __device__ __forceinline__ uint32_t y() const { return blockIdx.y; }
 };
 struct Cta {
+    static constexpr bool dynamic = false;
     uint32_t x_, nx_, y_;
     __device__ __forceinline__ uint32_t x() const { return x_; }
     __device__ __forceinline__ uint32_t nx() const { return nx_; }

@@ -237,11 +237,30 @@ __device__ __forceinline__ void g2p_body(const Dev& D, const CT& C) {
         }
         return x;
     };
+    // A one-scene launch hands the blocks out from a counter as CTAs come free (thread 0 takes
+    // them, the empty ones in passing); a CTA takes its next block at the start of this one, in
+    // time to stage it, into the slot of its turn's parity.
+    __shared__ uint32_t s_next[2];
+    auto take = [&]() {
+        uint32_t x = atomicAdd(&D.st->next_block[1], 1u);
+        while (x < nb && D.block_start[x + 1] == D.block_start[x]) {
+            D.brk_count[x] = 0;
+            x = atomicAdd(&D.st->next_block[1], 1u);
+        }
+        return x;
+    };
+    uint32_t turn = 0;
+    if constexpr (CT::dynamic) {
+        if (threadIdx.x == 0) s_next[0] = take();
+        __syncthreads();
+    }
     // Each block's tile is staged while the block before it is processed: its fields come in by
     // asynchronous copies behind that block's particles, and only the first block's wait is bare.
-    uint32_t b = next_full(C.x()), cur = 0;
+    uint32_t b = CT::dynamic ? s_next[0] : next_full(C.x()), cur = 0;
     if (b < nb) g2p_stage(D, b, s_links[0], raw, raw_cov, G2P_T);
     while (b < nb) {
+        turn++;
+        if (CT::dynamic && threadIdx.x == 0) s_next[turn & 1u] = take();
         const uint32_t* links = s_links[cur];
         const uint32_t first = D.block_start[b];
         const uint32_t count = D.block_start[b + 1] - first;
@@ -272,7 +291,7 @@ __device__ __forceinline__ void g2p_body(const Dev& D, const CT& C) {
         if (threadIdx.x == 0) s_brk = 0;
         for (uint32_t w = threadIdx.x; w < G2P_SEG / 32; w += G2P_T) s_bits[w] = 0u;
         __syncthreads();
-        const uint32_t nxt = next_full(b + C.nx());
+        const uint32_t nxt = CT::dynamic ? s_next[turn & 1u] : next_full(b + C.nx());
         if (nxt < nb) g2p_stage(D, nxt, s_links[cur ^ 1u], raw, raw_cov, G2P_T);
         const I3 corner = slot_coord(g, g.list[b]) * 4 - I3{1, 1, 1};
         // Rounds of G2P_T particles; the break-ups are ranked in sorted order per segment.

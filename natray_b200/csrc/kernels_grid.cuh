@@ -13,6 +13,7 @@ namespace ntr {
 template <class CT>
 __device__ __forceinline__ void begin_step_body(const Dev& D, const CT& C) {
     if (threadIdx.x != 0 || C.x() != 0) return;
+    D.st->next_block[0] = D.st->next_block[1] = 0u;
     const ntr_gpu_params* U = D.U;
     ntr_state& s = D.st->s;
     if (D.st->step_budget == 0u) {  // a batch scene that has taken its steps of the call
@@ -691,8 +692,19 @@ __device__ __forceinline__ void p2g_body(const Dev& D, const CT& C) {
     __shared__ uint16_t s_rank[P2G_CAP];
     __shared__ uint32_t s_mlo[P2G_LAYERS], s_mhi[P2G_LAYERS];  // layer r: cells 0-31, 32-63 with > r particles
     __shared__ uint32_t s_start[P2G_LAYERS + 1], s_over;
+    __shared__ uint32_t s_next[2];  // the block after this one, by the parity of the CTA's turn
     const float hh = g.h;
-    for (uint32_t b = C.x(); b < nb; b += C.nx()) {
+    // A one-scene launch hands the blocks out from a counter as CTAs come free (their particle
+    // counts differ, and a fixed stride leaves some CTAs a block more than others); a CTA takes
+    // its next block at the start of this one, so the fetch is off the critical path.
+    uint32_t turn = 0;
+    if constexpr (CT::dynamic) {
+        if (threadIdx.x == 0) s_next[0] = atomicAdd(&D.st->next_block[0], 1u);
+        __syncthreads();
+    }
+    for (uint32_t b = CT::dynamic ? s_next[0] : C.x(); b < nb; b = CT::dynamic ? s_next[turn & 1u] : b + C.nx()) {
+        turn++;
+        if (CT::dynamic && threadIdx.x == 0) s_next[turn & 1u] = atomicAdd(&D.st->next_block[0], 1u);
         const I3 bc = slot_coord(g, g.list[b]);
         if (threadIdx.x < 27) {
             uint32_t li = threadIdx.x;

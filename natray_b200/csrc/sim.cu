@@ -70,6 +70,7 @@ struct Sim {
     int device = 0;
     int sms = 148;
     uint32_t coop_ctas = 148;
+    uint32_t p2g_occ = 1, g2p128_occ = 1, g2p256_occ = 1;  // DevFacts
     // The scene's size class for its launch grids: its block count at the last read-back with a
     // quarter to spare, rounded up to a power of two (0: not known yet, full grids).
     uint32_t size_class = 0;
@@ -176,6 +177,9 @@ struct DevFacts {
     int sms = 0, major = 0, minor = 0;
     uint32_t coop_ctas = 0;  // CTAs of a persistent solve that the device holds at once (at most 256)
     uint32_t coop_all = 0;   // CTAs of the solve the device holds at once, uncapped (a joint solve of many systems)
+    // CTAs an SM holds at once of the one-scene P2G and G2P (of 128 and 256 threads), which hand
+    // their blocks out from a counter: more than that only wait for the counter to run out.
+    uint32_t p2g_occ = 1, g2p128_occ = 1, g2p256_occ = 1;
     bool known = false;
 };
 static ntr_status device_facts(int device, DevFacts& out) {
@@ -205,6 +209,12 @@ static ntr_status device_facts(int device, DevFacts& out) {
             occ = std::min(occ, o);
             f.coop_ctas = (uint32_t)std::min(256, f.sms * occ);
             f.coop_all = (uint32_t)(f.sms * occ);
+            CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_p2g, P2G_T, 0));
+            f.p2g_occ = (uint32_t)std::max(o, 1);
+            CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_g2p<128>, 128, 0));
+            f.g2p128_occ = (uint32_t)std::max(o, 1);
+            CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_g2p<256>, 256, 0));
+            f.g2p256_occ = (uint32_t)std::max(o, 1);
         }
         f.known = true;
     }
@@ -506,15 +516,22 @@ static uint64_t enqueue_solve(Sim& S, cudaStream_t s, const Dev* jobs, uint32_t 
 // warp) instead of the GPU's worth its kernels would otherwise spend launching CTAs with nothing
 // to do. The launch-shape tuning (ntr_sim_set_tuning) caps them.
 struct Grids {
-    uint32_t cell, blk, solve;
+    uint32_t cell, p2g, g2p, solve;
+    bool g2p_wide;  // G2P in CTAs of 256 threads (scenes under 300k particles), else 128
+    uint32_t blk;   // CTAs of a scene's per-block kernels in a many-scene launch (a fixed stride)
 };
 static Grids launch_grids(const Sim& S) {
-    Grids g{(uint32_t)S.sms * S.tune.cell_ctas_per_sm, (uint32_t)S.sms * S.tune.block_ctas_per_sm,
-            S.tune.solve_ctas ? S.tune.solve_ctas : S.coop_ctas};
+    const bool wide = S.D.Np < 300000u;
+    const uint32_t per_sm = S.tune.block_ctas_per_sm;
+    Grids g{(uint32_t)S.sms * S.tune.cell_ctas_per_sm, (uint32_t)S.sms * std::min(per_sm, S.p2g_occ),
+            (uint32_t)S.sms * std::min(per_sm, wide ? S.g2p256_occ : S.g2p128_occ),
+            S.tune.solve_ctas ? S.tune.solve_ctas : S.coop_ctas, wide, (uint32_t)S.sms * per_sm};
     const uint32_t nb = S.size_class;
     if (nb) {
         g.cell = std::max(1u, std::min(g.cell, (nb * 64u + 255u) / 256u));
         g.blk = std::max(1u, std::min(g.blk, nb));
+        g.p2g = std::max(1u, std::min(g.p2g, nb));
+        g.g2p = std::max(1u, std::min(g.g2p, nb));
         if (!S.tune.solve_ctas) g.solve = std::max(1u, std::min(g.solve, (nb + SOLVE_T / 32 - 1) / (SOLVE_T / 32)));
     }
     return g;
@@ -531,7 +548,7 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     Dev& D = S.D;
     uint64_t n = 0;
     const Grids grids = launch_grids(S);
-    const uint32_t G_cell = grids.cell, G_blk = grids.blk;
+    const uint32_t G_cell = grids.cell;
     const uint32_t g_vert = (D.Nv + 255) / 256 ? (D.Nv + 255) / 256 : 1;
     const uint32_t g_tri = std::max((D.Nt + 255) / 256, 1u);
     const uint32_t n_shots = S.U.mem[3] ? S.U.mem[3] : 1;
@@ -596,7 +613,7 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
         }
     }
     L(k_block_bounds, (D.Np + 1 + 255) / 256, 256, D);
-    L(k_p2g, G_blk, P2G_T, D);
+    L(k_p2g, grids.p2g, P2G_T, D);
     L(k_p2g_gather, G_cell, 256, D);
     join(0);
     L(k_grid_prep, G_cell, 256, D);
@@ -652,10 +669,10 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     }
     LA(k_spray_update, G_cell, 256, D);
     // Past 300k particles the blocks outnumber the resident CTAs: smaller CTAs, more of them.
-    if (D.Np >= 300000u)
-        L(k_g2p<128>, G_blk, 128, D);
+    if (!grids.g2p_wide)
+        L(k_g2p<128>, grids.g2p, 128, D);
     else
-        L(k_g2p<256>, G_blk, 256, D);
+        L(k_g2p<256>, grids.g2p, 256, D);
     join(1);
     if (a2 != s) {
         cudaEventRecord(S.ev_join[2], a2);
@@ -798,6 +815,7 @@ static ntr_status create_from(const World& w, int device, Sim*& out, uint8_t* ar
     S->U = w.h.params;
     S->sms = f.sms;
     S->coop_ctas = f.coop_ctas;
+    S->p2g_occ = f.p2g_occ, S->g2p128_occ = f.g2p128_occ, S->g2p256_occ = f.g2p256_occ;
     if (S->coop_ctas < 1) return fail(NTR_E_NODEVICE, "the device cannot hold a solver CTA");
     if (w.h.block_cap > 65535u) return fail(NTR_E_INVALID, "block_cap is at most 65535");
     SimHandles hs;
