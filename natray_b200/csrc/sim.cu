@@ -583,6 +583,10 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     // none of what the sort and P2G read or write).
     fork(0);
     LA(k_clear_acc, G_cell, 256, D);
+    // The first rubber substep's triangle records need only the membrane as the last step left
+    // it (nothing before that substep writes its positions or `alive`): made here, beside the
+    // sort, instead of in the rubber's chain after the pressure solve.
+    if (n_mem > 0) LA(k_mem_tri, g_tri, 256, D, 0);
     L(k_clear_mask, std::max((D.nwords + 255) / 256, 1u), 256, D);
     L(k_mark, (uint32_t)(((uint64_t)warp_round(D.Np) + warp_round(D.cap_blocks) + warp_round(D.Nv) + 255) / 256), 256, D);
     L(k_scan_words_a, D.scan_ctas, SCAN_T, D);
@@ -651,11 +655,11 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
         cudaEventRecord(S.ev_fork[2], s);
         cudaStreamWaitEvent(a2, S.ev_fork[2], 0);
     }
-    LA(k_mem_sample, (uint32_t)(((uint64_t)D.Nv * 4 + 255) / 256), 256, D);
+    LA(k_mem_sample, (uint32_t)(((uint64_t)D.Nv * 4 + 127) / 128), 128, D);
     for (uint32_t i = 0; i < n_sub; i++) {
         if (i < n_mem) {
             if (a != s && i >= 1 && i - 1 < n_air) cudaStreamWaitEvent(a, S.ev_sub[2 * (i - 1) + 1], 0);
-            LA(k_mem_tri, g_tri, 256, D, (int)(i % 2));
+            if (i > 0) LA(k_mem_tri, g_tri, 256, D, (int)(i % 2));
             LA(k_mem_substep, g_vert, 256, D, i, (int)(i % 2));
             if (a != s) cudaEventRecord(S.ev_sub[2 * i], a);
         }
