@@ -367,6 +367,7 @@ static uint64_t enqueue_step_multi(Batch& B, uint32_t n_jobs, const uint32_t* to
     LM(k_begin_step_m, GK_ONE, 32, s);
     fork(0, a);
     LM(k_clear_acc_m, GK_CELL, 256, a);
+    LM(k_spray_update_m, GK_CELL, 256, a);  // beside the sort, as in enqueue_step
     LM(k_clear_mask_m, GK_WORDS, 256, s);
     LM(k_mark_m, GK_MARK, 256, s);
     LM(k_scan_words_a_m, GK_SCAN, SCAN_T, s);
@@ -383,9 +384,8 @@ static uint64_t enqueue_step_multi(Batch& B, uint32_t n_jobs, const uint32_t* to
     }
     LM(k_block_bounds_m, GK_BOUNDS, 256, s);
     LM(k_p2g_m, GK_BLK, P2G_T, s);
-    LM(k_p2g_gather_m, GK_CELL, 256, s);
     join(0, a);
-    LM(k_grid_prep_m, GK_CELL, 256, s);
+    LM(k_gather_prep_m, GK_CELL, 256, s);
     LM(k_air_fill_m, GK_CELL, 256, s);
     LM(k_bullet_prep_m, GK_SHOTS, 32, s);
     if (tot[GK_PATCH]) k_bullet_patch_m<<<dim3(tot[GK_PATCH], max_shots), BULLET_PW * 32, 0, s>>>(M(GK_PATCH));
@@ -425,13 +425,11 @@ static uint64_t enqueue_step_multi(Batch& B, uint32_t n_jobs, const uint32_t* to
             if (a2 != s) cudaEventRecord(B.ev_sub[2 * i + 1], a2);
         }
     }
-    LM(k_spray_update_m, GK_CELL, 256, a);
     LM(k_g2p_m<128>, GK_BLK, 128, s);
-    join(1, a);
-    join(2, a2);
     LM(k_spray_scan_m, GK_ONE, 1024, s);
     LM(k_spray_emit_m, GK_CELL, 256, s);
-    LM(k_spray_commit_m, GK_ONE, 32, s);
+    join(1, a);
+    join(2, a2);
 #undef LM
     return nl;
 }

@@ -233,55 +233,39 @@ __global__ void k_mem_splat_m(Multi M) {
 }
 
 // ---- grid_prep, fluid.wgsl:305-356 -----------------------------------------------------------------
-template <class CT>
-__device__ __forceinline__ void grid_prep_body(const Dev& D, const CT& C) {
-    const DevState* st = D.st;
-    if (st->s.dt_ns == 0) return;
-    const Grid g = grid_of(D, cur_of(st));
-    const ntr_gpu_params* U = D.U;
+// One cell: its type, velocities and pressure from the transfer sums. `s8`: its sums of fields
+// 0-7 (momenta and weights of the three face lattices, A_WC, A_PC); the rest are read here.
+__device__ __forceinline__ void grid_prep_cell(const Dev& D, const Grid& g, V3 knot, float kr, float dt, const float (&grav)[3], uint32_t cell,
+                                               const int32_t (&s8)[8]) {
     const float hh = g.h;
-    const V3 knot = {U->knot[0], U->knot[1], U->knot[2]};
-    const float kr = U->knot[3] + 0.5f * hh;
-    const float dt = dt_of(st);
-    const float grav[3] = {U->gravity[0], U->gravity[1], U->gravity[2]};
-    CELL_LOOP(D, st) {
-        float ty = GAS_T;
-        I3 c = cell_coord(g, cell);
-        bool ground = g.org.y + ((float)c.y + 0.5f) * hh < 0.0f;
-        V3 p = g.org + (vf(c) + 0.5f) * hh - knot;
-        bool knot_c = p.y > 0.0f && p.y < 2.0f * kr && sqrtf(p.x * p.x + p.z * p.z) < kr;
-        if (ground || knot_c)
-            ty = SOLID_T;
-        else if (accv(D, A_N, cell) > 0)
-            ty = WATER_T;
+    float ty = GAS_T;
+    I3 c = cell_coord(g, cell);
+    bool ground = g.org.y + ((float)c.y + 0.5f) * hh < 0.0f;
+    V3 p = g.org + (vf(c) + 0.5f) * hh - knot;
+    bool knot_c = p.y > 0.0f && p.y < 2.0f * kr && sqrtf(p.x * p.x + p.z * p.z) < kr;
+    if (ground || knot_c)
+        ty = SOLID_T;
+    else if (accv(D, A_N, cell) > 0)
+        ty = WATER_T;
 #pragma unroll
-        for (uint32_t d = 0; d < 3; d++) {
-            float w = from_fp(accv(D, a_wt(d), cell), FP_W);
-            float u = 0.0f;
-            if (w > 1e-6f) u = from_fp(accv(D, a_mom(d), cell), FP_M) / w + dt * grav[d];
-            *cfp(D, F_U + d, cell) = u;
-        }
-        float wc = from_fp(accv(D, A_WC, cell), FP_W);
-        float ma = from_fp(accv(D, A_MA, cell), FP_A);
-        if (ty == GAS_T && accv(D, A_MW, cell) > 0) ty = RUBBER_T;
-        float pr = 0.0f;
-        if (ty == WATER_T && wc > 1e-6f) {
-            pr = from_fp(accv(D, A_PC, cell), FP_P) / wc * 1e6f;
-        } else if (ty != WATER_T && ty != SOLID_T && ma > 0.0f) {
-            ty = COVERED_T;
-            pr = from_fp(accv(D, A_MF, cell), FP_F) / ma * 1e6f;
-        }
-        *cfp(D, F_TYPE, cell) = ty;
-        *cfp(D, F_P, cell) = pr;
+    for (uint32_t d = 0; d < 3; d++) {
+        float w = from_fp(s8[a_wt(d)], FP_W);
+        float u = 0.0f;
+        if (w > 1e-6f) u = from_fp(s8[a_mom(d)], FP_M) / w + dt * grav[d];
+        *cfp(D, F_U + d, cell) = u;
     }
-}
-__global__ void k_grid_prep(Dev D) { grid_prep_body(D, HwCta{}); }
-__global__ void k_grid_prep_m(Multi M) {
-    __shared__ Dev sD;
-    __shared__ Cta c;
-    multi_cta(M, sD, c);
-    if (sD.st->parked) return;
-    grid_prep_body(sD, c);
+    float wc = from_fp(s8[A_WC], FP_W);
+    float ma = from_fp(accv(D, A_MA, cell), FP_A);
+    if (ty == GAS_T && accv(D, A_MW, cell) > 0) ty = RUBBER_T;
+    float pr = 0.0f;
+    if (ty == WATER_T && wc > 1e-6f) {
+        pr = from_fp(s8[A_PC], FP_P) / wc * 1e6f;
+    } else if (ty != WATER_T && ty != SOLID_T && ma > 0.0f) {
+        ty = COVERED_T;
+        pr = from_fp(accv(D, A_MF, cell), FP_F) / ma * 1e6f;
+    }
+    *cfp(D, F_TYPE, cell) = ty;
+    *cfp(D, F_P, cell) = pr;
 }
 
 __constant__ int8_t E6[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};

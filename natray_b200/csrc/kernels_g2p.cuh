@@ -392,6 +392,23 @@ __global__ void __launch_bounds__(G2P_T, 768 / G2P_T) k_g2p_m(Multi M) {
     g2p_body<G2P_T>(sD, c);
 }
 
+// The step's last bookkeeping (what the reference's break_up leaves in its counters): the spray
+// count advanced by the step's break-ups (5 slots each), and the step's work, whose algorithmic
+// bytes are counted from these: blocks, water cells times solver iterations, rubber substeps,
+// free-gas cells times air substeps, spray slots in use. By k_spray_scan, once it has the
+// step's break-ups; k_spray_emit takes its first slot as the count less those.
+__device__ __forceinline__ void spray_commit(const Dev& D, DevState* st) {
+    st->s.spray_count += 5u * st->nbrk;
+    const ntr_gpu_params* U = D.U;
+    st->work[0] += 1ull;
+    st->work[1] += 64ull * min(st->s.n_blocks, D.cap_blocks);
+    st->work[2] += (unsigned long long)st->n_water * st->s.solve_iters;
+    st->work[3] += U->mem[1];
+    st->work[4] += (unsigned long long)st->n_gas * U->mem[2];
+    st->work[5] += min(st->s.spray_count, D.spray_cap);
+    st->n_water = st->n_gas = 0u;
+}
+
 // Exclusive scan of the blocks' break-up counts (one CTA); advances the spray count.
 template <class CT>
 __device__ __forceinline__ void spray_scan_body(const Dev& D, const CT& C) {
@@ -428,6 +445,7 @@ __device__ __forceinline__ void spray_scan_body(const Dev& D, const CT& C) {
     if (threadIdx.x == 0) {
         uint32_t total = ws[31];
         st->nbrk = total;
+        spray_commit(D, st);
     }
 }
 __global__ void __launch_bounds__(1024) k_spray_scan(Dev D) { spray_scan_body(D, HwCta{}); }
@@ -446,7 +464,7 @@ __device__ __forceinline__ void spray_emit_body(const Dev& D, const CT& C) {
     if (st->s.dt_ns == 0) return;
     const uint32_t nb = min(st->s.n_blocks, D.cap_blocks);
     const uint32_t cap = D.spray_cap;
-    const uint32_t base_count = st->s.spray_count;
+    const uint32_t base_count = st->s.spray_count - 5u * st->nbrk;  // k_spray_scan advanced it
     const float hs = D.U->fluid[3], rhow = D.U->fluid[0];
     const float now = now_of(st);
     const uint32_t step_no = st->s.step;
@@ -521,34 +539,6 @@ __global__ void k_spray_emit_m(Multi M) {
 }
 
 // The spray count moves on by five slots per break-up, capacity or not (fluid.wgsl:726).
-template <class CT>
-__device__ __forceinline__ void spray_commit_body(const Dev& D, const CT& C) {
-    DevState* st = D.st;
-    if (st->s.dt_ns == 0) return;
-    if (threadIdx.x == 0 && C.x() == 0) {
-        st->s.spray_count += 5u * st->nbrk;
-        // The step's work (its algorithmic bytes are counted from these): blocks, water cells
-        // times solver iterations, rubber substeps, free-gas cells times air substeps, spray
-        // slots in use.
-        const ntr_gpu_params* U = D.U;
-        st->work[0] += 1ull;
-        st->work[1] += 64ull * min(st->s.n_blocks, D.cap_blocks);
-        st->work[2] += (unsigned long long)st->n_water * st->s.solve_iters;
-        st->work[3] += U->mem[1];
-        st->work[4] += (unsigned long long)st->n_gas * U->mem[2];
-        st->work[5] += min(st->s.spray_count, D.spray_cap);
-        st->n_water = st->n_gas = 0u;
-    }
-}
-__global__ void k_spray_commit(Dev D) { spray_commit_body(D, HwCta{}); }
-__global__ void k_spray_commit_m(Multi M) {
-    __shared__ Dev sD;
-    __shared__ Cta c;
-    multi_cta(M, sD, c);
-    if (sD.st->parked) return;
-    spray_commit_body(sD, c);
-}
-
 // ---- the zero-length measuring substep and diagnostics --------------------------------------------
 // Conservation sums over live particles in FP64: count, momentum, kinetic energy (per particle
 // mass) and the sum of positions.

@@ -6,6 +6,7 @@
 #pragma once
 
 #include "dev.cuh"
+#include "kernels_cells.cuh"
 
 namespace ntr {
 
@@ -783,7 +784,7 @@ __device__ __forceinline__ void p2g_body(const Dev& D, const CT& C) {
             }
             __syncthreads();
         }
-        // Stored in the packed layout (8 fields x 343, strides 49, 7, 1) k_p2g_gather reads.
+        // Stored in the packed layout (8 fields x 343, strides 49, 7, 1) gather_cell reads.
         int32_t* dst = D.tiles + (size_t)b * 8 * TILE;
         for (uint32_t e = threadIdx.x; e < 8 * TILE; e += P2G_T) {
             const uint32_t f = e / TILE, r = e - f * TILE, x = r / 49u, y = (r - x * 49u) / 7u, z = r - x * 49u - y * 7u;
@@ -803,50 +804,68 @@ __global__ void __launch_bounds__(P2G_T, 4) k_p2g_m(Multi M) {
     p2g_body(sD, c);
 }
 
+// The transfer sums of fields 0-7 of `cell`: the entries of the tiles over it, added.
+__device__ __forceinline__ void gather_cell(const Dev& D, uint32_t cell, int32_t (&out)[8]) {
+    const uint32_t b = cell >> 6;
+    const I3 l = local_coord(cell);
+    // The up to 2 x 2 x 2 tiles over the cell: per axis its own block (offset 0) and the one
+    // below (l <= 1) or above (l == 3). Their indices, then whether they hold sums, then all
+    // their entries, each step's loads in flight together.
+    const int ax[2] = {0, l.x <= 1 ? -1 : 1}, ay[2] = {0, l.y <= 1 ? -1 : 1}, az[2] = {0, l.z <= 1 ? -1 : 1};
+    const int nx = l.x == 2 ? 1 : 2, ny = l.y == 2 ? 1 : 2, nz = l.z == 2 ? 1 : 2;
+    const uint32_t* nbt = D.block_nb + (size_t)b * 27u;
+    uint32_t src[8], tix[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int ix = i & 1, iy = (i >> 1) & 1, iz = i >> 2;
+        const int ox = ax[ix], oy = ay[iy], oz = az[iz];
+        src[i] = (ix < nx && iy < ny && iz < nz) ? nbt[(ox + 1) * 9 + (oy + 1) * 3 + oz + 1] : NONE;
+        tix[i] = (uint32_t)(l.x + 1 - 4 * ox) * 49u + (uint32_t)(l.y + 1 - 4 * oy) * 7u + (uint32_t)(l.z + 1 - 4 * oz);
+    }
+    bool ok[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) ok[i] = src[i] != NONE && D.tile_ok[src[i] != NONE ? src[i] : b] != 0u;
+    // Integer sums: the same in any order.
+    uint32_t s[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const int32_t* tp = D.tiles + (size_t)(ok[i] ? src[i] : b) * 8 * TILE + (ok[i] ? tix[i] : 0u);
+#pragma unroll
+        for (int f = 0; f < 8; f++) s[f] += ok[i] ? (uint32_t)tp[f * TILE] : 0u;
+    }
+#pragma unroll
+    for (int f = 0; f < 8; f++) out[f] = (int32_t)s[f];
+}
+
+// The tiles' flush and grid_prep (fluid.wgsl:305-356) in one pass over the cells: grid_prep
+// reads only the cell's own sums, so each cell's are used as they are gathered. The rubber's
+// splat (fields A_MF and up) must be complete.
 template <class CT>
-__device__ __forceinline__ void p2g_gather_body(const Dev& D, const CT& C) {
+__device__ __forceinline__ void gather_prep_body(const Dev& D, const CT& C) {
     const DevState* st = D.st;
     if (st->s.dt_ns == 0) return;
+    const Grid g = grid_of(D, cur_of(st));
+    const ntr_gpu_params* U = D.U;
+    const V3 knot = {U->knot[0], U->knot[1], U->knot[2]};
+    const float kr = U->knot[3] + 0.5f * g.h;
+    const float dt = dt_of(st);
+    const float grav[3] = {U->gravity[0], U->gravity[1], U->gravity[2]};
     const uint32_t n_cells = min(st->s.n_blocks, D.cap_blocks) * 64u;
     for (uint32_t cell = C.x() * blockDim.x + threadIdx.x; cell < n_cells; cell += C.nx() * blockDim.x) {
-        const uint32_t b = cell >> 6;
-        const I3 l = local_coord(cell);
-        // The up to 2 x 2 x 2 tiles over the cell: per axis its own block (offset 0) and the one
-        // below (l <= 1) or above (l == 3). Their indices, then whether they hold sums, then all
-        // their entries, each step's loads in flight together.
-        const int ax[2] = {0, l.x <= 1 ? -1 : 1}, ay[2] = {0, l.y <= 1 ? -1 : 1}, az[2] = {0, l.z <= 1 ? -1 : 1};
-        const int nx = l.x == 2 ? 1 : 2, ny = l.y == 2 ? 1 : 2, nz = l.z == 2 ? 1 : 2;
-        const uint32_t* nbt = D.block_nb + (size_t)b * 27u;
-        uint32_t src[8], tix[8];
+        int32_t s8[8];
+        gather_cell(D, cell, s8);
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int ix = i & 1, iy = (i >> 1) & 1, iz = i >> 2;
-            const int ox = ax[ix], oy = ay[iy], oz = az[iz];
-            src[i] = (ix < nx && iy < ny && iz < nz) ? nbt[(ox + 1) * 9 + (oy + 1) * 3 + oz + 1] : NONE;
-            tix[i] = (uint32_t)(l.x + 1 - 4 * ox) * 49u + (uint32_t)(l.y + 1 - 4 * oy) * 7u + (uint32_t)(l.z + 1 - 4 * oz);
-        }
-        bool ok[8];
-#pragma unroll
-        for (int i = 0; i < 8; i++) ok[i] = src[i] != NONE && D.tile_ok[src[i] != NONE ? src[i] : b] != 0u;
-        // Integer sums: the same in any order.
-        uint32_t s[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
-#pragma unroll
-        for (int i = 0; i < 8; i++) {
-            const int32_t* tp = D.tiles + (size_t)(ok[i] ? src[i] : b) * 8 * TILE + (ok[i] ? tix[i] : 0u);
-#pragma unroll
-            for (int f = 0; f < 8; f++) s[f] += ok[i] ? (uint32_t)tp[f * TILE] : 0u;
-        }
-#pragma unroll
-        for (int f = 0; f < 8; f++) D.acc[(size_t)f * D.cap_cells + cell] = (int32_t)s[f];
+        for (int f = 0; f < 8; f++) D.acc[(size_t)f * D.cap_cells + cell] = s8[f];
+        grid_prep_cell(D, g, knot, kr, dt, grav, cell, s8);
     }
 }
-__global__ void k_p2g_gather(Dev D) { p2g_gather_body(D, HwCta{}); }
-__global__ void k_p2g_gather_m(Multi M) {
+__global__ void k_gather_prep(Dev D) { gather_prep_body(D, HwCta{}); }
+__global__ void k_gather_prep_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;
     multi_cta(M, sD, c);
     if (sD.st->parked) return;
-    p2g_gather_body(sD, c);
+    gather_prep_body(sD, c);
 }
 
 }  // namespace ntr

@@ -587,6 +587,9 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     // it (nothing before that substep writes its positions or `alive`): made here, beside the
     // sort, instead of in the rubber's chain after the pressure solve.
     if (n_mem > 0) LA(k_mem_tri, g_tri, 256, D, 0);
+    // The spray's flight reads only the spray, the step length and the spray count from before
+    // this step's break-ups (k_spray_scan advances it): beside the sort too.
+    LA(k_spray_update, G_cell, 256, D);
     L(k_clear_mask, std::max((D.nwords + 255) / 256, 1u), 256, D);
     L(k_mark, (uint32_t)(((uint64_t)warp_round(D.Np) + warp_round(D.cap_blocks) + warp_round(D.Nv) + 255) / 256), 256, D);
     L(k_scan_words_a, D.scan_ctas, SCAN_T, D);
@@ -618,9 +621,10 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     }
     L(k_block_bounds, (D.Np + 1 + 255) / 256, 256, D);
     L(k_p2g, grids.p2g, P2G_T, D);
-    L(k_p2g_gather, G_cell, 256, D);
+    // The side stream (the rubber's splat, the air's carry) is long done by now; the gather of
+    // the tiles and the cells' grid_prep then go in one pass.
     join(0);
-    L(k_grid_prep, G_cell, 256, D);
+    L(k_gather_prep, G_cell, 256, D);
     L(k_air_fill, G_cell, 256, D);
     L(k_bullet_prep, n_shots, 32, D);
     {
@@ -635,8 +639,7 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     L(k_project, G_cell, 256, D);
     L(k_extend_1, G_cell, 256, D);
     L(k_extend_2, G_cell, 256, D);
-    // G2P shares nothing with the rubber and air substeps or the spray's flight: they run
-    // side by side.
+    // G2P shares nothing with the rubber and air substeps: they run side by side.
     // The rubber substeps on one side stream and the air substeps on another: rubber substep i
     // reads the air buffer that air substep i - 1 writes, and air substep i overwrites the one
     // rubber substep i - 1 reads, so substep i of the two runs side by side and each waits for
@@ -671,20 +674,20 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
             if (a2 != s) cudaEventRecord(S.ev_sub[2 * i + 1], a2);
         }
     }
-    LA(k_spray_update, G_cell, 256, D);
     // Past 300k particles the blocks outnumber the resident CTAs: smaller CTAs, more of them.
     if (!grids.g2p_wide)
         L(k_g2p<128>, grids.g2p, 128, D);
     else
         L(k_g2p<256>, grids.g2p, 256, D);
+    // The break-ups' drops go into spray slots past the old count, which nothing on the side
+    // streams touches: they follow G2P while the rubber and the air finish.
+    L(k_spray_scan, 1, 1024, D);
+    L(k_spray_emit, G_cell, 256, D);
     join(1);
     if (a2 != s) {
         cudaEventRecord(S.ev_join[2], a2);
         cudaStreamWaitEvent(s, S.ev_join[2], 0);
     }
-    L(k_spray_scan, 1, 1024, D);
-    L(k_spray_emit, G_cell, 256, D);
-    L(k_spray_commit, 1, 32, D);
 #undef L
 #undef LA
     return n;
