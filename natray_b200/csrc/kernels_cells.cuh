@@ -338,7 +338,12 @@ __device__ __forceinline__ void bullet_apply_body(const Dev& D, const CT& C) {
         }
     }
 }
-__global__ void k_bullet_apply(Dev D) { bullet_apply_body(D, HwCta{}); }
+// A one-scene step's: CTA 0 also starts the pressure solve's grid barrier counter from zero
+// (one graph node fewer than a memset; a many-scene step has k_solve_reset_m).
+__global__ void k_bullet_apply(Dev D) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) D.st->bar_count = 0u;
+    bullet_apply_body(D, HwCta{});
+}
 __global__ void k_bullet_apply_m(Multi M) {
     __shared__ Dev sD;
     __shared__ Cta c;

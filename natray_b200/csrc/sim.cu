@@ -633,8 +633,7 @@ static uint64_t enqueue_step(Sim& S, cudaStream_t s, uint32_t n_mem, uint32_t n_
     }
     L(k_bullet_finish, n_shots, 256, D);
     L(k_bullet_apply, G_cell, 256, D);
-    // The pressure solve's grid barrier counter starts from zero.
-    cudaMemsetAsync(&D.st->bar_count, 0, 4, s);
+    // (k_bullet_apply has set the pressure solve's grid barrier counter to zero.)
     n += enqueue_solve(S, s, nullptr, 1u, fp64, prof, grids.solve);
     L(k_project, G_cell, 256, D);
     L(k_extend_1, G_cell, 256, D);
