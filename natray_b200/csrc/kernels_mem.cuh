@@ -634,6 +634,51 @@ __device__ __forceinline__ float2 warp_sample_pressure(const Dev& D, const Grid&
     return fold27(present, wp, w);
 }
 
+// The five samples of a bullet patch at X (grid units) by a warp: the water velocity of the
+// three face lattices (warp_sample_grid with F_U + d, a_wt(d)), the fill (F_TYPE, A_WC at
+// X - 0.5) and the gas pressure (warp_sample_pressure at X - 0.5, gas only, the fill's stencil).
+// Each lane's four cell lookups and then all their loads go out together, instead of one
+// sample's dependent chain after another's; the folds are the same, in the same order.
+__device__ __forceinline__ void warp_patch_samples(const Dev& D, const Grid& g, V3 X, int lane, float2 (&s)[4], float2& gs) {
+    const int a = lane / 9, b = (lane / 3) % 3, c = lane % 3;
+    V3 wx[4], wy[4], wz[4];
+    uint32_t cell[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const V3 x = k < 3 ? X - lattice_offset((uint32_t)k) : X - 0.5f;
+        const I3 base = vi(vfloor(x - 0.5f));
+        const V3 fx = x - vf(base);
+        wx[k] = axis_weights(fx.x), wy[k] = axis_weights(fx.y), wz[k] = axis_weights(fx.z);
+        cell[k] = lane < 27 ? cell_at(g, base + I3{a, b, c}) : NONE;
+    }
+    int32_t wv[4];
+    float uv[4], pv = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const bool in = cell[k] != NONE;
+        wv[k] = in ? accv(D, k < 3 ? a_wt((uint32_t)k) : (uint32_t)A_WC, cell[k]) : 0;
+        uv[k] = in ? cfv(D, k < 3 ? F_U + (uint32_t)k : (uint32_t)F_TYPE, cell[k]) : 0.0f;
+    }
+    if (cell[3] != NONE) pv = cfv(D, F_P, cell[3]);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        float w = 0.0f, wu = 0.0f;
+        if (cell[k] != NONE) {
+            w = wsel(wx[k], a) * wsel(wy[k], b) * wsel(wz[k], c) * from_fp(wv[k], FP_W);
+            wu = w * uv[k];
+        }
+        s[k] = fold27(cell[k] != NONE, wu, w);
+    }
+    // The pressure sample: cells that are not solid and not water (uv[3] is the cell's type).
+    const bool pp = cell[3] != NONE && !(uv[3] == SOLID_T || uv[3] == WATER_T);
+    float w = 0.0f, wp = 0.0f;
+    if (pp) {
+        w = wsel(wx[3], a) * wsel(wy[3], b) * wsel(wz[3], c);
+        wp = w * pv;
+    }
+    gs = fold27(pp, wp, w);
+}
+
 // push_water by a warp (integer sums: the lanes add their cells' shares in any order).
 __device__ __forceinline__ void warp_push_water(const Dev& D, const Grid& g, V3 x, uint32_t d, float j, float sw, int lane) {
     if (sw <= 1e-6f || j == 0.0f) return;
@@ -766,14 +811,13 @@ __device__ __forceinline__ void bullet_patch_body(const Dev& D, const CT& C) {
     V3 n = qrot(b.q, xyz(pn));
     float area = pp.w;
     V3 X = (p - g.org) / hh;
-    float2 s0 = warp_sample_grid(D, g, X - lattice_offset(0), F_U + 0, a_wt(0), lane);
-    float2 s1 = warp_sample_grid(D, g, X - lattice_offset(1), F_U + 1, a_wt(1), lane);
-    float2 s2 = warp_sample_grid(D, g, X - lattice_offset(2), F_U + 2, a_wt(2), lane);
+    float2 sm[4], gs;
+    warp_patch_samples(D, g, X, lane, sm, gs);
+    const float2 s0 = sm[0], s1 = sm[1], s2 = sm[2];
     V3 uw = {s0.y > 1e-6f ? s0.x / s0.y : 0.0f, s1.y > 1e-6f ? s1.x / s1.y : 0.0f, s2.y > 1e-6f ? s2.x / s2.y : 0.0f};
     V3 sw = {s0.y, s1.y, s2.y};
-    float fill = clampf_(warp_sample_grid(D, g, X - 0.5f, F_TYPE, A_WC, lane).y / 8.0f, 0.0f, 1.0f);
+    float fill = clampf_(sm[3].y / 8.0f, 0.0f, 1.0f);
     if (warp_in_cavity(D, hh, bi, p, t_end - step, lane) || dot(r, xyz(side)) > side.w) fill = 0.0f;
-    float2 gs = warp_sample_pressure(D, g, X - 0.5f, true, lane);
     float p_gas = gs.y > 1e-6f ? gs.x / gs.y : 0.0f;
     V3 vp = xyz(b.v) + cross(w, r);
     V3 rel = vp - uw;
