@@ -439,8 +439,8 @@ NTR_API ntr_status ntr_sim_pack_particles(ntr_sim* s, void* dst_device, size_t b
 NTR_API ntr_status ntr_sim_conservation(ntr_sim* s, double out[8]);
 
 /* The device's sustained rate of shared-memory atomic adds (lane additions per second) at their
- * best, in P2G's CTA shape: the peak against which P2G, bound by its 216 such adds a particle,
- * is measured. No counterpart in the reference. */
+ * best, in P2G's CTA shape: the peak against which P2G's 216 such adds a particle are measured.
+ * No counterpart in the reference. */
 NTR_API ntr_status ntr_probe_shared_atomics(int device, uint32_t iters, double* lane_atomics_per_s);
 
 /* --- Launch shapes and their autotuner ----------------------------------------------------

@@ -1310,12 +1310,12 @@ NTR_API ntr_status ntr_sim_conservation(ntr_sim* sim, double out[8]) {
 }  // extern "C"
 
 // ---- the shared-memory atomic peak (ntr_probe_shared_atomics) -----------------------------------
-// P2G's limit is its shared-memory atomic adds. This kernel measures the rate the SMs sustain
-// for them at their best: P2G's CTA shape (256 threads, its tile's 15.2 KB of shared memory,
-// three CTAs an SM), every lane of a warp on its own bank and node, integer adds in a chain of
+// P2G makes 216 shared-memory atomic adds a particle. This kernel measures the rate the SMs
+// sustain for them at their best: P2G's CTA shape (256 threads, its tile's 15.2 KB of shared
+// memory, as many CTAs an SM as P2G runs), every lane of a warp on its own bank and node, integer adds in a chain of
 // `iters` per lane whose sums are kept (so that none is optimised away).
 namespace ntr {
-__global__ void __launch_bounds__(256, 3) k_probe_shared_atomics(uint32_t iters, int32_t* out) {
+__global__ void __launch_bounds__(256, 4) k_probe_shared_atomics(uint32_t iters, int32_t* out) {
     __shared__ int32_t tile[8 * 476];
     for (uint32_t t = threadIdx.x; t < 8 * 476; t += blockDim.x) tile[t] = 0;
     __syncthreads();
@@ -1343,7 +1343,7 @@ extern "C" NTR_API ntr_status ntr_probe_shared_atomics(int device, uint32_t iter
     if (!scope.ok) return fail(NTR_E_CUDA, "cudaSetDevice failed");
     DevFacts f;
     if ((r = device_facts(device, f)) != NTR_OK) return r;
-    const uint32_t grid = (uint32_t)f.sms * 3u;
+    const uint32_t grid = (uint32_t)f.sms * f.p2g_occ;  // P2G's CTAs an SM
     int32_t* out = nullptr;
     cudaStream_t s = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
