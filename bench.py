@@ -302,17 +302,20 @@ def run_native(args, rank, world, local):
                 except ValueError:
                     pass
 
-    # P2G's limit is its shared-memory atomics: 216 lane additions a particle (4 lattices x 27
-    # nodes x value and weight), against the device's measured rate for them at their best.
+    # P2G's shared-memory atomics: 216 lane additions a particle (4 lattices x 27 nodes x value
+    # and weight), against the device's measured rate for them at their best. Reported whichever
+    # kernel has the largest share (P2G and the solve are within a point of each other).
     atomics = None
-    if top.startswith("k_p2g"):
+    p2g = prof.get("k_p2g")
+    if p2g:
         import ctypes as C
         from natray_b200._abi import check, lib
         peak_at = C.c_double()
         check(lib().ntr_probe_shared_atomics(local, 16384, C.byref(peak_at)))
-        rate = 216.0 * n_particles / per_launch_s
-        atomics = {"achieved": rate, "peak": peak_at.value, "unit": "lane atomic adds/s", "frac": rate / peak_at.value,
-                   "per_launch": 216 * n_particles,
+        p2g_s = p2g[1] / p2g[0] * 1e-3
+        rate = 216.0 * n_particles / p2g_s
+        atomics = {"kernel": "k_p2g", "achieved": rate, "peak": peak_at.value, "unit": "lane atomic adds/s",
+                   "frac": rate / peak_at.value, "per_launch": 216 * n_particles, "launch_ms": p2g_s * 1e3,
                    "note": "peak: ntr_probe_shared_atomics, conflict-free adds in P2G's CTA shape on this GPU"}
 
     result = None
