@@ -434,9 +434,17 @@ __device__ __forceinline__ void extend_1_body(const Dev& D, const CT& C) {
         }
         // Types of the 3^3 cells around (GAS outside the grid), of the cells two down each axis,
         // and the face velocities of the cell and its six neighbours.
+        // face_set below reads 16 of the 27: the cell, its 6 face neighbours and the 9 edge
+        // neighbours with a step down along some axis (o - e_d for a face offset o); the 8
+        // corners and the 3 edges up along both axes are neither looked up nor loaded.
+        auto read = [](int k) {
+            const int x = k / 9 - 1, y = (k / 3) % 3 - 1, z = k % 3 - 1;
+            const int nnz = (x != 0) + (y != 0) + (z != 0);
+            return nnz <= 1 || (nnz == 2 && (x < 0 || y < 0 || z < 0));
+        };
         uint32_t nc[27], n2[3];
 #pragma unroll
-        for (int k = 0; k < 27; k++) nc[k] = k == 13 ? cell : neighbour(g, cell, I3{k / 9 - 1, (k / 3) % 3 - 1, k % 3 - 1});
+        for (int k = 0; k < 27; k++) nc[k] = k == 13 ? cell : (read(k) ? neighbour(g, cell, I3{k / 9 - 1, (k / 3) % 3 - 1, k % 3 - 1}) : NONE);
 #pragma unroll
         for (int d = 0; d < 3; d++) n2[d] = neighbour(g, cell, ed((uint32_t)d, -2));
         float T[27], T2[3], un[6][3], uo[3];

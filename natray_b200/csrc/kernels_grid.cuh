@@ -249,13 +249,19 @@ __device__ __forceinline__ void scan_words_b_body(const Dev& D, const CT& C) {
         for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
         if (threadIdx.x == 0) s_base = t;
     }
-    // Each thread owns SCAN_W consecutive words.
+    // Each thread owns SCAN_W consecutive words (two 16-byte loads where all are in range).
+    static_assert(SCAN_W == 8, "two uint4 per thread");
     uint32_t w0 = C.x() * SCAN_T * SCAN_W + threadIdx.x * SCAN_W;
     uint32_t words[SCAN_W], cnt = 0;
-    for (int k = 0; k < SCAN_W; k++) {
-        words[k] = (w0 + k < D.nwords) ? m[w0 + k] : 0u;
-        cnt += __popc(words[k]);
+    if (w0 + SCAN_W <= D.nwords) {
+        const uint4 a = *reinterpret_cast<const uint4*>(m + w0), b = *reinterpret_cast<const uint4*>(m + w0 + 4);
+        words[0] = a.x, words[1] = a.y, words[2] = a.z, words[3] = a.w;
+        words[4] = b.x, words[5] = b.y, words[6] = b.z, words[7] = b.w;
+    } else {
+        for (int k = 0; k < SCAN_W; k++) words[k] = (w0 + k < D.nwords) ? m[w0 + k] : 0u;
     }
+#pragma unroll
+    for (int k = 0; k < SCAN_W; k++) cnt += __popc(words[k]);
     uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     uint32_t inc = cnt;
     for (int o = 1; o < 32; o <<= 1) {
@@ -271,8 +277,10 @@ __device__ __forceinline__ void scan_words_b_body(const Dev& D, const CT& C) {
     for (int k = 0; k < SCAN_W; k++) {
         uint32_t w = w0 + k;
         if (w >= D.nwords) break;
-        prefix[w] = run;
+        // lookup() reads a word's prefix only for a set bit of it: the empty words (nearly all
+        // of the domain) are not written.
         uint32_t bits = words[k];
+        if (bits) prefix[w] = run;
         while (bits) {
             uint32_t b = __ffs(bits) - 1;
             bits &= bits - 1;
