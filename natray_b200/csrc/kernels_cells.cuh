@@ -721,7 +721,10 @@ __device__ __forceinline__ void air_substep_body(const Dev& D, const CT& C, int 
     // The reference lowers air_dt once per workgroup, so only when there are cells.
     if ((threadIdx.x & 31) == 0 && n_cells_ > 0) atomicMin((unsigned int*)&st->s.air_dt, __float_as_uint(lim));
 }
-__global__ void __launch_bounds__(256, 3) k_air_substep(Dev D, int par) { air_substep_body(D, HwCta{}, par); }
+// A one-scene step's at four CTAs an SM (64 registers, a few spilled): alone it is slower than at
+// three (35.5 against 34.0 us a step at 1M particles), but beside G2P and the rubber substeps the
+// step's graph is faster (0.493 against 0.495 ms).
+__global__ void __launch_bounds__(256, 4) k_air_substep(Dev D, int par) { air_substep_body(D, HwCta{}, par); }
 
 // The air's substep over many scenes: substep i, for the scenes whose step has that many.
 __global__ void __launch_bounds__(256, 3) k_air_substep_m(Multi M, uint32_t i, int par) {
