@@ -671,7 +671,8 @@ __global__ void k_mem_sample_m(Multi M) {
 }
 
 // ---- air_substep, air.wgsl:237-269 --------------------------------------------------------------------
-// Three CTAs an SM (80 registers, from 84 and two CTAs): 38.5 -> 34.8 us a step at 1M particles.
+// Three CTAs an SM (80 registers, from 84 and two CTAs): 38.5 -> 34.8 us a step at 1M particles
+// (the many-scene kernel's shape; the one-scene kernel's is below).
 template <class CT>
 __device__ __forceinline__ void air_substep_body(const Dev& D, const CT& C, int par) {
     DevState* st = D.st;
