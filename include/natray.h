@@ -452,8 +452,9 @@ NTR_API ntr_status ntr_probe_shared_atomics(int device, uint32_t iters, double* 
 typedef struct {
     uint32_t solve_ctas;        /* CTAs of the cooperative pressure solve, 1..256 (default: all that fit, at most 256) */
     uint32_t cell_ctas_per_sm;  /* CTAs of 256 threads per SM of the per-cell kernels (default 8) */
-    uint32_t block_ctas_per_sm; /* CTAs per SM of the per-block transfer kernels P2G and G2P (default 8; a one-scene
-                                   step takes at most what an SM holds at once, its CTAs taking blocks as they come free) */
+    uint32_t block_ctas_per_sm; /* CTAs per SM of the per-block transfer kernels P2G and G2P (default 8 in a batch, 5 in
+                                   a simulation: its step takes at most what an SM holds at once, its CTAs taking blocks as
+                                   they come free, and 5 leaves G2P room for the rubber's kernels beside it) */
     uint32_t pad;
 } ntr_tuning;
 NTR_API ntr_status ntr_sim_get_tuning(ntr_sim* s, ntr_tuning* out);

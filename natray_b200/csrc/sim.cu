@@ -66,6 +66,12 @@ struct DeviceScope {
     }
 };
 
+// A one-scene step's default cap on P2G's and G2P's CTAs an SM. Each takes at most what an SM
+// holds at once (P2G four, G2P six at 1M particles); five leaves G2P one CTA's registers short of
+// that on every SM, where the rubber's substep and sampling CTAs run beside it instead of waiting
+// for G2P's end: 0.524 -> 0.515 ms a step over the bench's 300 steps of the 1M scene (four: 0.524).
+constexpr uint32_t SIM_BLOCK_CTAS = 5;
+
 struct Sim {
     int device = 0;
     int sms = 148;
@@ -97,7 +103,7 @@ struct Sim {
     cudaEvent_t ev_out = nullptr;  // ntr_sim_pack_particles: the caller's stream waits on it
     uint32_t batch_steps = 0;  // ntr_sim_set_batch_steps: fixed steps per ntr_sim_advance batch (0: by time)
     uint32_t fp64 = 1;
-    ntr_tuning tune{0u, 8u, 8u, 0u};  // launch shapes (ntr_sim_set_tuning)
+    ntr_tuning tune{0u, 8u, SIM_BLOCK_CTAS, 0u};  // launch shapes (ntr_sim_set_tuning)
     bool own_streams = true;  // false: the streams, events and h_params are a batch slot's, kept across its scenes
 
     ~Sim() {
@@ -1179,7 +1185,7 @@ NTR_API ntr_status ntr_sim_set_tuning(ntr_sim* sim, const ntr_tuning* t) {
     if (n.solve_ctas > S.coop_ctas) return fail(NTR_E_INVALID, "solve_ctas is at most " + std::to_string(S.coop_ctas) + " (co-resident) on this device");
     if (n.cell_ctas_per_sm > 64 || n.block_ctas_per_sm > 64) return fail(NTR_E_INVALID, "at most 64 CTAs per SM");
     if (!n.cell_ctas_per_sm) n.cell_ctas_per_sm = 8;
-    if (!n.block_ctas_per_sm) n.block_ctas_per_sm = 8;
+    if (!n.block_ctas_per_sm) n.block_ctas_per_sm = SIM_BLOCK_CTAS;
     n.pad = 0;
     CU(cudaStreamSynchronize(S.stream));
     S.tune = n;
